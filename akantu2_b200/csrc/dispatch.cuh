@@ -1,0 +1,63 @@
+// Dispatch from runtime (element type, quadrature rule, law) to the kernel
+// template instances; shared by the FP64 and the mixed translation units.
+#pragma once
+
+#include <type_traits>
+
+#include "fe_kernels.cuh"
+#include "launch.h"
+
+namespace akb {
+
+namespace {
+constexpr int kThreads = 256;
+inline unsigned grid_for(int64_t n, int threads = kThreads) {
+  return (unsigned)((n + threads - 1) / threads);
+}
+}  // namespace
+
+// ---- dispatch helpers ------------------------------------------------------
+#define AKB_DISPATCH_ELEM(g, ...)                                        \
+  do {                                                                    \
+    if ((g).et == ET_TET4) {                                              \
+      constexpr int ET = ET_TET4, D = 3, NN = 4, NQ = 1;                  \
+      __VA_ARGS__;                                                        \
+    } else if ((g).et == ET_HEX8) {                                       \
+      constexpr int ET = ET_HEX8, D = 3, NN = 8, NQ = 8;                  \
+      __VA_ARGS__;                                                        \
+    } else if ((g).et == ET_TRI6 && (g).NQ == 3) {                        \
+      constexpr int ET = ET_TRI6, D = 2, NN = 6, NQ = 3;                  \
+      __VA_ARGS__;                                                        \
+    } else if ((g).et == ET_TRI6 && (g).NQ == 6) {                        \
+      constexpr int ET = ET_TRI6, D = 2, NN = 6, NQ = 6;                  \
+      __VA_ARGS__;                                                        \
+    } else {                                                              \
+      return cudaErrorInvalidValue;                                       \
+    }                                                                     \
+  } while (0)
+
+template <class T, class RT>
+inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                       const T *B, const T *wJ, const double *u,
+                                       const MatParams &mp, const PlasticState &ps, RT *re,
+                                       cudaStream_t s) {
+  if (ne == 0) return cudaSuccess;
+  AKB_DISPATCH_ELEM(g, {
+    (void)ET;
+    constexpr int EB = EPB<NQ>::value;
+    const unsigned grid = (unsigned)((ne + EB - 1) / EB);
+    if (law == LAW_ELASTIC)
+      k_element_forces<D, NN, NQ, LAW_ELASTIC, T, RT>
+          <<<grid, EB * NQ, 0, s>>>(e0, ne, g.E, g.conn, B, wJ, u, mp, ps, re);
+    else if (law == LAW_NEOHOOKEAN)
+      k_element_forces<D, NN, NQ, LAW_NEOHOOKEAN, T, RT>
+          <<<grid, EB * NQ, 0, s>>>(e0, ne, g.E, g.conn, B, wJ, u, mp, ps, re);
+    else
+      k_element_forces<D, NN, NQ, LAW_PLASTIC, T, RT>
+          <<<grid, EB * NQ, 0, s>>>(e0, ne, g.E, g.conn, B, wJ, u, mp, ps, re);
+  });
+  return cudaGetLastError();
+}
+
+
+}  // namespace akb

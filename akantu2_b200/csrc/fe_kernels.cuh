@@ -1,0 +1,499 @@
+// Kernel templates of the explicit step.  Instantiated by kernels_fp64.cu
+// (T = double, compiled --fmad=false) and kernels_mixed.cu (T = float).
+//
+// HBM layout (all arrays in internal element order: elements grouped by
+// material, ascending original id inside a material):
+//   conn  int32 [NN][E]              node ids, component-major
+//   B     T     [NN*D][E*NQ]         dN_a/dx_j at (a*D + j), per (e, q)
+//   wJ    T     [E*NQ]               det J * w_q
+//   re    RT    [E*NN][D]            elemental internal force, read by the
+//                                    node gather in ascending slot order
+//   u,v,a,fext,fint double [N][D]    user node order (reference layout)
+//   mass  double [N]                 one lumped mass per node
+//   blocked uint8 [N]                bit c = component c blocked
+// The node -> slot CSR (ptr [N+1], ent [E*NN]) lists slots (e*NN + a) in
+// increasing order, which is the order of the reference's serial scatter
+// (dof_manager.cc:65-120), so the gather reproduces its sums exactly.
+#pragma once
+
+#include "fe_device.cuh"
+
+namespace akb {
+
+constexpr int kMaxNQ = 8;
+constexpr int kMaxNN = 8;
+
+// natural-coordinate tables evaluated on the host
+struct QuadTable {
+  double dnds[kMaxNQ * 3 * kMaxNN];  // [q][k][a]
+  double N[kMaxNQ * kMaxNN];         // [q][a]
+  double w[kMaxNQ];
+};
+
+// per-material plastic internals, SoA [comp][nqp_m], ping-pong prev/cur
+struct PlasticState {
+  const double *sig_prev, *gu_prev, *eps_prev, *iso_prev;
+  const double *iso_cur_in;  // "current" hardening read by the yield test
+  double *sig, *gu, *eps, *iso;
+  double *pe;                // cumulative plastic energy density
+  int64_t nqp;               // quadrature points of the material
+  int update_energy;         // 1 inside solveStep (afterSolveStep), 0 otherwise
+};
+
+// ---------------------------------------------------------------------------
+// K0: dN/dx and det J * w  (element_class_tmpl.hh:296-395,
+// integrator_gauss_inline_impl.hh:176-195,378-398).  One thread per (e, q).
+template <int D, int NN, int NQ>
+__global__ void k_precompute(const double *__restrict__ X, const int32_t *__restrict__ conn,
+                             int64_t E, QuadTable tab, double *__restrict__ B,
+                             double *__restrict__ wJ, unsigned long long *__restrict__ bad) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * NQ) return;
+  const int64_t e = t / NQ;
+  const int q = (int)(t - e * NQ);
+  double Xe[NN * D];
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < D; ++i) Xe[a * D + i] = X[node * D + i];
+  }
+  const double *dn = &tab.dnds[q * 3 * kMaxNN];
+  double J[D * D], Ji[D * D];
+#pragma unroll
+  for (int k = 0; k < D; ++k)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      double s = dn[k * kMaxNN] * Xe[j];
+#pragma unroll
+      for (int a = 1; a < NN; ++a) s = s + dn[k * kMaxNN + a] * Xe[a * D + j];
+      J[k + D * j] = s;
+    }
+  double det;
+  if constexpr (D == 3) {
+    det = det3(J);
+    inv3(J, Ji);
+  } else {
+    det = det2(J);
+    inv2(J, Ji);
+  }
+  const int64_t EQ = E * NQ;
+#pragma unroll
+  for (int a = 0; a < NN; ++a)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      double s = Ji[j] * dn[a];
+#pragma unroll
+      for (int k = 1; k < D; ++k) s = s + Ji[j + D * k] * dn[k * kMaxNN + a];
+      B[(int64_t)(a * D + j) * EQ + t] = s;
+    }
+  if (det < 0) atomicMin(bad, (unsigned long long)t);
+  wJ[t] = det * tab.w[q];
+}
+
+// ---------------------------------------------------------------------------
+// K1a: elemental lumped mass into the slot array (ncomp 1)
+// row sum sum_q (rho N_a(q)) wJ_q, or for _triangle_6 rho V_e * (1/12 | 1/4)
+// (fe_engine_template_tmpl_field.hh:112-242)
+template <int NN, int NQ, bool DIAG>
+__global__ void k_mass_elem(int64_t e_begin, int64_t e_count, int64_t E, double rho,
+                            QuadTable tab, const double *__restrict__ wJ,
+                            double *__restrict__ me) {
+  const int64_t le = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (le >= e_count) return;
+  const int64_t e = e_begin + le;
+  if constexpr (DIAG) {
+    double vol = rho * wJ[e * NQ];
+#pragma unroll
+    for (int q = 1; q < NQ; ++q) vol = vol + rho * wJ[e * NQ + q];
+#pragma unroll
+    for (int a = 0; a < NN; ++a) me[e * NN + a] = vol * (a < 3 ? 1. / 12. : 1. / 4.);
+  } else {
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      double acc = rho * tab.N[a] * wJ[e * NQ];
+#pragma unroll
+      for (int q = 1; q < NQ; ++q) acc = acc + rho * tab.N[q * kMaxNN + a] * wJ[e * NQ + q];
+      me[e * NN + a] = acc;
+    }
+  }
+}
+
+// K1b: M_i = sum over the node's slots, ascending
+static __global__ void k_gather_scalar(int64_t N, const int32_t *__restrict__ ptr,
+                                const int32_t *__restrict__ ent, const double *__restrict__ me,
+                                double *__restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double acc = 0.;
+  for (int32_t p = ptr[i]; p < ptr[i + 1]; ++p) acc += 1. * me[ent[p]];
+  out[i] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// K2: element inradius / celerity at the current position X + u
+// (solid_mechanics_model.cc:436-473, fe_engine_inline_impl.hh:35-45)
+__device__ __forceinline__ double dist3(const double *a, const double *b) {
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double t = a[i] - b[i];
+    s += t * t;
+  }
+  return sqrt(s);
+}
+__device__ __forceinline__ double dist2(const double *a, const double *b) {
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    double t = a[i] - b[i];
+    s += t * t;
+  }
+  return sqrt(s);
+}
+__device__ __forceinline__ double det3cols(const double *c0, const double *c1,
+                                           const double *c2) {
+  double m[9] = {c0[0], c0[1], c0[2], c1[0], c1[1], c1[2], c2[0], c2[1], c2[2]};
+  return det3(m);
+}
+template <int ET> __device__ double element_inradius(const double *X);
+template <> __device__ inline double element_inradius<ET_TET4>(const double *X) {
+  const double *p1 = X, *p2 = X + 3, *p3 = X + 6, *p4 = X + 9;
+  double l12 = dist3(p1, p2), l13 = dist3(p1, p3), l14 = dist3(p1, p4);
+  double l23 = dist3(p2, p3), l24 = dist3(p2, p4), l34 = dist3(p3, p4);
+  double s1 = (l12 + l23 + l13) * 0.5;
+  s1 = sqrt(s1 * (s1 - l12) * (s1 - l23) * (s1 - l13));
+  double s2 = (l12 + l24 + l14) * 0.5;
+  s2 = sqrt(s2 * (s2 - l12) * (s2 - l24) * (s2 - l14));
+  double s3 = (l23 + l34 + l24) * 0.5;
+  s3 = sqrt(s3 * (s3 - l23) * (s3 - l34) * (s3 - l24));
+  double s4 = (l13 + l34 + l14) * 0.5;
+  s4 = sqrt(s4 * (s4 - l13) * (s4 - l34) * (s4 - l14));
+  double vol = det3cols(p2, p3, p4);
+  vol -= det3cols(p1, p3, p4);
+  vol += det3cols(p1, p2, p4);
+  vol -= det3cols(p1, p2, p3);
+  vol /= 6;
+  return 2. * (3 * vol / (s1 + s2 + s3 + s4));
+}
+template <> __device__ inline double element_inradius<ET_HEX8>(const double *X) {
+  const int ed[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 5},
+                         {2, 6}, {3, 7}, {4, 5}, {5, 6}, {6, 7}, {7, 4}};
+  double p = dist3(X + 3 * ed[0][0], X + 3 * ed[0][1]);
+#pragma unroll
+  for (int k = 1; k < 12; ++k) p = fmin(p, dist3(X + 3 * ed[k][0], X + 3 * ed[k][1]));
+  return p;
+}
+template <> __device__ inline double element_inradius<ET_TRI6>(const double *X) {
+  const int tr[4][3] = {{0, 3, 5}, {3, 1, 4}, {3, 4, 5}, {5, 4, 2}};
+  double r = 1.7976931348623157e308;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double *p1 = X + 2 * tr[k][0], *p2 = X + 2 * tr[k][1], *p3 = X + 2 * tr[k][2];
+    double a = dist2(p1, p2), b = dist2(p2, p3), c = dist2(p1, p3);
+    double s = (a + b + c) / 2.;
+    r = fmin(sqrt((s - a) * (s - b) * (s - c) / s), r);
+  }
+  return 2. * r;
+}
+
+template <int ET, int D, int NN>
+__global__ void k_element_dt(int64_t e_begin, int64_t e_count, int64_t E, double celerity,
+                             const int32_t *__restrict__ conn, const double *__restrict__ X,
+                             const double *__restrict__ u, double *__restrict__ out) {
+  const int64_t le = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (le >= e_count) return;
+  const int64_t e = e_begin + le;
+  double Xe[NN * D];
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < D; ++i) Xe[a * D + i] = X[node * D + i] + u[node * D + i];
+  }
+  out[e] = element_inradius<ET>(Xe) / celerity;
+}
+
+// ---------------------------------------------------------------------------
+// K3: NewmarkBeta::predictor, alpha = 0, beta = 1/2 (newmark-beta.cc:47-76)
+//   u += dt v + (dt/2)(dt a);  v += dt a   on non-blocked dofs
+template <int D>
+__global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked, double *__restrict__ u,
+                          double *__restrict__ v, const double *__restrict__ a, double dt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * D) return;
+  const int64_t node = i / D;
+  const int c = (int)(i - node * D);
+  if ((blocked[node] >> c) & 1) return;
+  const double hdt = .5 * dt;
+  const double dta = dt * a[i];
+  u[i] = u[i] + (dt * v[i] + hdt * dta);
+  v[i] = v[i] + dta;
+}
+
+// ---------------------------------------------------------------------------
+// K4: gradient at quadrature points, material law, B^T sigma integration.
+// One thread per (element, quadrature point); the NQ threads of an element
+// share its gathered displacement and sum their contributions in q order.
+template <int NQ> struct EPB {
+  static constexpr int value = NQ == 1 ? 128 : (NQ == 8 ? 16 : (128 / NQ));
+};
+
+template <int D, int NN, int NQ, int LAW, class T, class RT>
+__global__ void __launch_bounds__(EPB<NQ>::value * NQ)
+    k_element_forces(int64_t e_begin, int64_t e_count, int64_t E,
+                     const int32_t *__restrict__ conn, const T *__restrict__ B,
+                     const T *__restrict__ wJ, const double *__restrict__ u, MatParams mp,
+                     PlasticState ps, RT *__restrict__ re) {
+  constexpr int ND = NN * D;
+  constexpr int EB = EPB<NQ>::value;
+  constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
+  __shared__ double us[EB][ND];
+  __shared__ T red[NQ > 1 ? EB : 1][NQ > 1 ? NQ : 1][ND];
+
+  const int eb = threadIdx.x / NQ;
+  const int q = threadIdx.x - eb * NQ;
+  const int64_t le = (int64_t)blockIdx.x * EB + eb;
+  const bool active = le < e_count;
+  const int64_t e = e_begin + le;
+
+  if (active) {
+    for (int a = q; a < NN; a += NQ) {
+      const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+      for (int i = 0; i < D; ++i) us[eb][a * D + i] = u[node * D + i];
+    }
+  }
+  if constexpr (NQ > 1) __syncthreads();
+
+  T t[ND];
+  if (active) {
+    const int64_t EQ = E * NQ;
+    const int64_t eq = e * NQ + q;
+    T b[ND];
+#pragma unroll
+    for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)c * EQ + eq];
+    const T w = wJ[eq];
+    T ue[ND];
+    if constexpr (REL) {
+#pragma unroll
+      for (int c = 0; c < ND; ++c) ue[c] = (T)(us[eb][c] - us[eb][c % D]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < ND; ++c) ue[c] = us[eb][c];
+    }
+    // grad u = u B^T  (shape_functions_inline_impl.hh:303-310)
+    T g[D * D];
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        T s = ue[i] * b[j];
+#pragma unroll
+        for (int a = 1; a < NN; ++a) s = s + ue[a * D + i] * b[a * D + j];
+        g[i + D * j] = s;
+      }
+    if constexpr (LAW == LAW_NEOHOOKEAN) {
+      T S[D * D], Sv[D == 3 ? 6 : 3];
+      neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
+      to_voigt<D, T>(S, Sv);
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+          t[a * D + k] = finite_force_component<D, T>(&b[a * D], g, Sv, k) * w;
+    } else {
+      T sig[D * D];
+      if constexpr (LAW == LAW_ELASTIC) {
+        elastic_stress<D, T>((T)mp.lambda, (T)mp.mu, g, (T)mp.sigma_th, sig);
+      } else {
+        constexpr int DD = D * D;
+        const int64_t lq = le * NQ + q;
+        double gd[DD], gp[DD], sp[DD], epp[DD], s[DD], ep[DD], iso;
+#pragma unroll
+        for (int k = 0; k < DD; ++k) {
+          gd[k] = (double)g[k];
+          gp[k] = ps.gu_prev[k * ps.nqp + lq];
+          sp[k] = ps.sig_prev[k * ps.nqp + lq];
+          epp[k] = ps.eps_prev[k * ps.nqp + lq];
+        }
+        const double isop = ps.iso_prev[lq];
+        const double isoc = ps.iso_cur_in[lq];
+        plastic_update<D>(mp.lambda, mp.mu, mp.sigma_y, mp.h, gd, gp, sp, epp, isoc, isop, 0.,
+                          s, ep, &iso);
+        if (ps.update_energy) {
+          // MaterialPlastic::updateEnergies (material_plastic.cc:85-103)
+          double wp = 0.;
+#pragma unroll
+          for (int k = 0; k < DD; ++k) {
+            const double de = ep[k] - epp[k];
+            const double sh = s[k] + sp[k];
+            wp = (k == 0) ? sh * de : wp + sh * de;
+          }
+          wp = wp / 2.;
+          ps.pe[lq] = ps.pe[lq] + wp;
+        }
+#pragma unroll
+        for (int k = 0; k < DD; ++k) {
+          ps.gu[k * ps.nqp + lq] = gd[k];
+          ps.sig[k * ps.nqp + lq] = s[k];
+          ps.eps[k * ps.nqp + lq] = ep[k];
+          sig[k] = (T)s[k];
+        }
+        ps.iso[lq] = iso;
+      }
+      // sigma B, d x n  (shape_lagrange_inline_impl.hh:402-408), times wJ_q
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          T s = sig[i] * b[a * D];
+#pragma unroll
+          for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * b[a * D + j];
+          t[a * D + i] = s * w;
+        }
+    }
+  }
+
+  if constexpr (NQ == 1) {
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < ND; ++c) re[e * ND + c] = (RT)t[c];
+    }
+  } else {
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < ND; ++c) red[eb][q][c] = t[c];
+    }
+    __syncthreads();
+    if (active) {
+      // integrate: sum over q in increasing order (integrator_gauss_inline_impl.hh:401-418)
+      for (int c = q; c < ND; c += NQ) {
+        if constexpr (std::is_same<T, double>::value) {
+          T s = red[eb][0][c];
+#pragma unroll
+          for (int qq = 1; qq < NQ; ++qq) s = s + red[eb][qq][c];
+          re[e * ND + c] = (RT)s;
+        } else {
+          float s = red[eb][0][c];
+#pragma unroll
+          for (int qq = 1; qq < NQ; ++qq) s = s + red[eb][qq][c];
+          re[e * ND + c] = (RT)s;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5: node gather + residual + lumped solve + corrector
+//   f_int = sum_slots (-1) r_e           (dof_manager.cc:65-120)
+//   r = (0 + f_ext + f_int) + M (0 - a)  (solid_mechanics_model.cc:235-249,
+//                                         dof_manager_default.cc:260-277)
+//   x = r / M; v += (dt/2) x; a += x     (non_linear_solver_lumped.cc:76-87,
+//                                         newmark-beta.cc:163-197)
+// The displacement coefficient of the corrector is alpha*beta*dt^2 = 0.
+// KAHAN selects a compensated FP64 sum (mixed path).
+template <int D, class RT, bool KAHAN>
+__global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
+                              const int32_t *__restrict__ ent, const RT *__restrict__ re,
+                              const double *__restrict__ fext, const double *__restrict__ mass,
+                              const uint8_t *__restrict__ blocked, double *__restrict__ fint,
+                              double *__restrict__ a, double *__restrict__ v, double dt,
+                              int do_correct, unsigned int *__restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double acc[D], comp[D];
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    acc[c] = 0.;
+    comp[c] = 0.;
+  }
+  const int32_t p0 = ptr[i], p1 = ptr[i + 1];
+  for (int32_t p = p0; p < p1; ++p) {
+    const int64_t s = ent[p];
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      const double val = -1. * (double)re[s * D + c];
+      if constexpr (KAHAN) {
+        const double y = val - comp[c];
+        const double tt = acc[c] + y;
+        comp[c] = (tt - acc[c]) - y;
+        acc[c] = tt;
+      } else {
+        acc[c] = acc[c] + val;
+      }
+    }
+  }
+  const double m = mass[i];
+  const uint8_t bl = blocked[i];
+  const double hdt = .5 * dt;
+  bool bad = false;
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const int64_t k = i * D + c;
+    fint[k] = acc[c];
+    if (!do_correct) continue;
+    double r = 0. + 1. * fext[k];
+    r = r + 1. * acc[c];
+    const double ak = a[k];
+    const double ma = 0. + -1. * ak;
+    r = r + m * ma;
+    if (!((bl >> c) & 1)) {
+      const double x = 1. * (r / m);
+      v[k] = v[k] + hdt * x;
+      const double an = ak + 1. * x;
+      a[k] = an;
+      bad |= !isfinite(an);
+    }
+  }
+  if (bad) atomicOr(status, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// quadrature-point fields of elastic / neohookean materials, evaluated from a
+// displacement snapshot (the reference keeps them as internals,
+// material.cc:128-154).  Output SoA [D*D][nqp_m].
+template <int D, int NN, int NQ, int LAW>
+__global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
+                            const int32_t *__restrict__ conn, const double *__restrict__ B,
+                            const double *__restrict__ u, MatParams mp,
+                            double *__restrict__ grad_out, double *__restrict__ stress_out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e_count * NQ) return;
+  const int64_t le = t / NQ;
+  const int q = (int)(t - le * NQ);
+  const int64_t e = e_begin + le;
+  const int64_t EQ = E * NQ, eq = e * NQ + q;
+  double ue[NN * D], b[NN * D];
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < D; ++i) ue[a * D + i] = u[node * D + i];
+  }
+#pragma unroll
+  for (int c = 0; c < NN * D; ++c) b[c] = B[(int64_t)c * EQ + eq];
+  double g[D * D], s[D * D];
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      double acc = ue[i] * b[j];
+#pragma unroll
+      for (int a = 1; a < NN; ++a) acc = acc + ue[a * D + i] * b[a * D + j];
+      g[i + D * j] = acc;
+    }
+  if constexpr (LAW == LAW_NEOHOOKEAN)
+    neohookean_pk2<D, double>(mp.lambda, mp.mu, g, s);
+  else
+    elastic_stress<D, double>(mp.lambda, mp.mu, g, mp.sigma_th, s);
+  const int64_t nqp = e_count * NQ;
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) {
+    grad_out[k * nqp + t] = g[k];
+    stress_out[k * nqp + t] = s[k];
+  }
+}
+
+}  // namespace akb

@@ -1,0 +1,288 @@
+// FP64 kernels and their launchers.  Built with --fmad=false: no contraction,
+// so the arithmetic matches the CPU path operation for operation.
+#include <type_traits>
+
+#include "dispatch.cuh"
+
+namespace akb {
+
+// ---- init ------------------------------------------------------------------
+cudaError_t launch_precompute(const DevGeom &g, const QuadTable &tab, double *B, double *wJ,
+                              unsigned long long *bad, cudaStream_t s) {
+  if (g.E == 0) return cudaSuccess;
+  AKB_DISPATCH_ELEM(g, {
+    (void)ET;
+    k_precompute<D, NN, NQ><<<grid_for(g.E * NQ), kThreads, 0, s>>>(g.X, g.conn, g.E, tab, B,
+                                                                      wJ, bad);
+  });
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mass_elem(const DevGeom &g, int64_t e0, int64_t ne, double rho,
+                             const QuadTable &tab, const double *wJ, double *me,
+                             cudaStream_t s) {
+  if (ne == 0) return cudaSuccess;
+  AKB_DISPATCH_ELEM(g, {
+    (void)D;
+    k_mass_elem<NN, NQ, ET == ET_TRI6><<<grid_for(ne), kThreads, 0, s>>>(e0, ne, g.E, rho, tab,
+                                                                         wJ, me);
+  });
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_scalar(const DevGeom &g, const double *me, double *out,
+                                 cudaStream_t s) {
+  if (g.N == 0) return cudaSuccess;
+  k_gather_scalar<<<grid_for(g.N), kThreads, 0, s>>>(g.N, g.ptr, g.ent, me, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_element_dt(const DevGeom &g, int64_t e0, int64_t ne, double celerity,
+                              const double *u, double *out, cudaStream_t s) {
+  if (ne == 0) return cudaSuccess;
+  AKB_DISPATCH_ELEM(g, {
+    (void)NQ;
+    k_element_dt<ET, D, NN><<<grid_for(ne), kThreads, 0, s>>>(e0, ne, g.E, celerity, g.conn,
+                                                              g.X, u, out);
+  });
+  return cudaGetLastError();
+}
+
+__global__ void k_to_float(const double *__restrict__ in, float *__restrict__ out, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (float)in[i];
+}
+cudaError_t launch_to_float(const double *in, float *out, int64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_to_float<<<grid_for(n), kThreads, 0, s>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+// ---- step ------------------------------------------------------------------
+cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, double *u, double *v,
+                           const double *a, double dt, cudaStream_t s) {
+  if (g.N == 0) return cudaSuccess;
+  if (g.D == 3)
+    k_predict<3><<<grid_for(g.N * 3), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt);
+  else
+    k_predict<2><<<grid_for(g.N * 2), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                       const double *B, const double *wJ, const double *u,
+                                       const MatParams &mp, const PlasticState &ps,
+                                       double *re, cudaStream_t s) {
+  return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, s);
+}
+
+cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
+                                    const double *mass, const uint8_t *blocked, double *fint,
+                                    double *a, double *v, double dt, int do_correct,
+                                    unsigned int *status, cudaStream_t s) {
+  if (g.N == 0) return cudaSuccess;
+  if (g.D == 3)
+    k_node_update<3, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
+        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+  else
+    k_node_update<2, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
+        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+  return cudaGetLastError();
+}
+
+// ---- fields and energies ---------------------------------------------------
+cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                             const double *B, const double *u, const MatParams &mp,
+                             double *grad, double *stress, cudaStream_t s) {
+  if (ne == 0) return cudaSuccess;
+  AKB_DISPATCH_ELEM(g, {
+    (void)ET;
+    if (law == LAW_NEOHOOKEAN)
+      k_qp_fields<D, NN, NQ, LAW_NEOHOOKEAN><<<grid_for(ne * NQ), kThreads, 0, s>>>(
+          e0, ne, g.E, g.conn, B, u, mp, grad, stress);
+    else
+      k_qp_fields<D, NN, NQ, LAW_ELASTIC><<<grid_for(ne * NQ), kThreads, 0, s>>>(
+          e0, ne, g.E, g.conn, B, u, mp, grad, stress);
+  });
+  return cudaGetLastError();
+}
+
+// kinetic energy terms (solid_mechanics_model.cc:476-527): per node
+// mv2 = sum_c (m > eps ? v v m : 0)
+template <int D>
+__global__ void k_ekin_terms(int64_t N, const double *__restrict__ v,
+                             const double *__restrict__ mass, double *__restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double m = mass[i];
+  double mv2 = 0.;
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const double vv = v[i * D + c];
+    if (m > 2.220446049250313080847e-16) mv2 += vv * vv * m;
+  }
+  out[i] = mv2;
+}
+cudaError_t launch_ekin_terms(const DevGeom &g, const double *v, const double *mass,
+                              double *out, cudaStream_t s) {
+  if (g.N == 0) return cudaSuccess;
+  if (g.D == 3)
+    k_ekin_terms<3><<<grid_for(g.N), kThreads, 0, s>>>(g.N, v, mass, out);
+  else
+    k_ekin_terms<2><<<grid_for(g.N), kThreads, 0, s>>>(g.N, v, mass, out);
+  return cudaGetLastError();
+}
+
+// external work terms (solid_mechanics_model.cc:556-598)
+template <int D>
+__global__ void k_work_terms(int64_t N, const double *__restrict__ fext,
+                             const double *__restrict__ fint, const double *__restrict__ v,
+                             const uint8_t *__restrict__ blocked, double *__restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double w = 0.;
+  const uint8_t bl = blocked[i];
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const int64_t k = i * D + c;
+    if ((bl >> c) & 1)
+      w -= fint[k] * v[k];
+    else
+      w += fext[k] * v[k];
+  }
+  out[i] = w;
+}
+cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double *fint,
+                              const double *v, const uint8_t *blocked, double *out,
+                              cudaStream_t s) {
+  if (g.N == 0) return cudaSuccess;
+  if (g.D == 3)
+    k_work_terms<3><<<grid_for(g.N), kThreads, 0, s>>>(g.N, fext, fint, v, blocked, out);
+  else
+    k_work_terms<2><<<grid_for(g.N), kThreads, 0, s>>>(g.N, fext, fint, v, blocked, out);
+  return cudaGetLastError();
+}
+
+// per-element integral of an energy density (Material::getPotentialEnergy,
+// material.cc:604-619; MaterialPlastic::getPlasticEnergy, material_plastic.cc:47-69)
+template <int D, int NQ, int LAW>
+__global__ void k_energy_elem(int which, int64_t e0, int64_t ne, const double *__restrict__ wJ,
+                              const double *__restrict__ grad, const double *__restrict__ stress,
+                              const double *__restrict__ eps_p, const double *__restrict__ pe,
+                              MatParams mp, double *__restrict__ out) {
+  const int64_t le = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (le >= ne) return;
+  constexpr int DD = D * D;
+  const int64_t nqp = ne * NQ;
+  double el = 0.;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const int64_t lq = le * NQ + q;
+    double dens;
+    if (which == 1) {
+      dens = pe[lq];
+    } else if (LAW == LAW_NEOHOOKEAN) {
+      double F[DD];
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+#pragma unroll
+        for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? 1. : 0.) + grad[(i + D * j) * nqp + lq];
+      double trC = 0.;
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        double tt = F[0 + D * i] * F[0 + D * i];
+#pragma unroll
+        for (int k = 1; k < D; ++k) tt = tt + F[k + D * i] * F[k + D * i];
+        trC = (i == 0) ? tt : trC + tt;
+      }
+      double J;
+      if constexpr (D == 3) J = det3(F); else J = det2(F);
+      dens = mp.lambda * pow(log(J), 2.) + mp.mu * (-log(J) + (trC - D) / 2.) / 2.;
+    } else {
+      double dot = 0.;
+#pragma unroll
+      for (int k = 0; k < DD; ++k) {
+        double ge = grad[k * nqp + lq];
+        if (LAW == LAW_PLASTIC) ge = ge - eps_p[k * nqp + lq];
+        const double sk = stress[k * nqp + lq];
+        dot = (k == 0) ? sk * ge : dot + sk * ge;
+      }
+      dens = .5 * dot;
+    }
+    const double w = wJ[(e0 + le) * NQ + q];
+    el = (q == 0) ? dens * w : el + dens * w;
+  }
+  out[le] = el;
+}
+cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0, int64_t ne,
+                               const double *wJ, const double *grad, const double *stress,
+                               const double *eps_p, const double *pe, const MatParams &mp,
+                               double *out, cudaStream_t s) {
+  if (ne == 0) return cudaSuccess;
+  AKB_DISPATCH_ELEM(g, {
+    (void)ET;
+    (void)NN;
+    if (law == LAW_NEOHOOKEAN)
+      k_energy_elem<D, NQ, LAW_NEOHOOKEAN><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, wJ, grad, stress, eps_p, pe, mp, out);
+    else if (law == LAW_PLASTIC)
+      k_energy_elem<D, NQ, LAW_PLASTIC><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, wJ, grad, stress, eps_p, pe, mp, out);
+    else
+      k_energy_elem<D, NQ, LAW_ELASTIC><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, wJ, grad, stress, eps_p, pe, mp, out);
+  });
+  return cudaGetLastError();
+}
+
+// deterministic two-level reduction: block b sums the strided set
+// {i : i % gridDim == b} in increasing i per thread, then a fixed smem tree
+template <int OPMIN>
+__global__ void k_reduce_partial(const double *__restrict__ x, int64_t n,
+                                 double *__restrict__ partials) {
+  __shared__ double sm[256];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double acc = OPMIN ? 1.7976931348623157e308 : 0.;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    acc = OPMIN ? fmin(acc, x[i]) : acc + x[i];
+  sm[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      sm[threadIdx.x] = OPMIN ? fmin(sm[threadIdx.x], sm[threadIdx.x + w])
+                              : sm[threadIdx.x] + sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
+}
+template <int OPMIN>
+__global__ void k_reduce_final(const double *__restrict__ partials, int np,
+                               double *__restrict__ out) {
+  __shared__ double sm[1024];
+  double acc = OPMIN ? 1.7976931348623157e308 : 0.;
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    acc = OPMIN ? fmin(acc, partials[i]) : acc + partials[i];
+  sm[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      sm[threadIdx.x] = OPMIN ? fmin(sm[threadIdx.x], sm[threadIdx.x + w])
+                              : sm[threadIdx.x] + sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sm[0];
+}
+cudaError_t launch_reduce(const double *x, int64_t n, int op_min, double *partials,
+                          double *out, cudaStream_t s) {
+  const int nb = kReducePartials;
+  if (op_min) {
+    k_reduce_partial<1><<<nb, 256, 0, s>>>(x, n, partials);
+    k_reduce_final<1><<<1, 1024, 0, s>>>(partials, nb, out);
+  } else {
+    k_reduce_partial<0><<<nb, 256, 0, s>>>(x, n, partials);
+    k_reduce_final<0><<<1, 1024, 0, s>>>(partials, nb, out);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace akb

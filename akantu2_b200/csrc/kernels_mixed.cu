@@ -1,0 +1,29 @@
+// Mixed-precision kernels: FP32 element kinematics, stress and B^T sigma,
+// FP64 nodal state with a compensated (Kahan) FP64 gather of the FP32
+// elemental forces.  Contraction (FMA) is allowed in this translation unit.
+#include "dispatch.cuh"
+
+namespace akb {
+
+cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                        const float *B, const float *wJ, const double *u,
+                                        const MatParams &mp, const PlasticState &ps,
+                                        float *re, cudaStream_t s) {
+  return element_forces_impl<float, float>(g, law, e0, ne, B, wJ, u, mp, ps, re, s);
+}
+
+cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
+                                     const double *mass, const uint8_t *blocked,
+                                     double *fint, double *a, double *v, double dt,
+                                     int do_correct, unsigned int *status, cudaStream_t s) {
+  if (g.N == 0) return cudaSuccess;
+  if (g.D == 3)
+    k_node_update<3, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
+        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+  else
+    k_node_update<2, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
+        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+  return cudaGetLastError();
+}
+
+}  // namespace akb

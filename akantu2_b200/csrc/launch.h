@@ -1,0 +1,81 @@
+// Host-side launchers of the explicit-step kernels (one translation unit per
+// arithmetic: kernels_fp64.cu is built with --fmad=false, kernels_mixed.cu
+// with contraction allowed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fe_device.cuh"
+
+namespace akb {
+
+struct QuadTable;
+struct PlasticState;
+
+// device view of the mesh, internal element order
+struct DevGeom {
+  int et, D, NN, NQ;
+  int64_t E, N;
+  const int32_t *conn;  // [NN][E]
+  const double *X;      // [N][D]
+  const int32_t *ptr;   // [N+1]
+  const int32_t *ent;   // [E*NN]
+};
+
+// ---- init ------------------------------------------------------------------
+cudaError_t launch_precompute(const DevGeom &g, const QuadTable &tab, double *B, double *wJ,
+                              unsigned long long *bad, cudaStream_t s);
+cudaError_t launch_mass_elem(const DevGeom &g, int64_t e0, int64_t ne, double rho,
+                             const QuadTable &tab, const double *wJ, double *me,
+                             cudaStream_t s);
+cudaError_t launch_gather_scalar(const DevGeom &g, const double *me, double *out,
+                                 cudaStream_t s);
+cudaError_t launch_element_dt(const DevGeom &g, int64_t e0, int64_t ne, double celerity,
+                              const double *u, double *out, cudaStream_t s);
+cudaError_t launch_to_float(const double *in, float *out, int64_t n, cudaStream_t s);
+
+// ---- step ------------------------------------------------------------------
+cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, double *u, double *v,
+                           const double *a, double dt, cudaStream_t s);
+cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                       const double *B, const double *wJ, const double *u,
+                                       const MatParams &mp, const PlasticState &ps,
+                                       double *re, cudaStream_t s);
+cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                        const float *B, const float *wJ, const double *u,
+                                        const MatParams &mp, const PlasticState &ps,
+                                        float *re, cudaStream_t s);
+cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
+                                    const double *mass, const uint8_t *blocked, double *fint,
+                                    double *a, double *v, double dt, int do_correct,
+                                    unsigned int *status, cudaStream_t s);
+cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
+                                     const double *mass, const uint8_t *blocked,
+                                     double *fint, double *a, double *v, double dt,
+                                     int do_correct, unsigned int *status, cudaStream_t s);
+
+// ---- fields and energies ---------------------------------------------------
+cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                             const double *B, const double *u, const MatParams &mp,
+                             double *grad, double *stress, cudaStream_t s);
+// per-dof kinetic terms (m > eps ? v v m : 0) summed per node -> out[N]
+cudaError_t launch_ekin_terms(const DevGeom &g, const double *v, const double *mass,
+                              double *out, cudaStream_t s);
+// per-dof external work terms -> out[N]
+cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double *fint,
+                              const double *v, const uint8_t *blocked, double *out,
+                              cudaStream_t s);
+// per-element sum_q density_q wJ_q of one material -> out[ne]
+// which: 0 potential, 1 plastic
+cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0, int64_t ne,
+                               const double *wJ, const double *grad, const double *stress,
+                               const double *eps_p, const double *pe, const MatParams &mp,
+                               double *out, cudaStream_t s);
+// deterministic reductions (fixed grid, fixed tree): result written to *out
+// (device); partials needs kReducePartials doubles
+constexpr int kReducePartials = 1024;
+cudaError_t launch_reduce(const double *x, int64_t n, int op_min, double *partials,
+                          double *out, cudaStream_t s);
+
+}  // namespace akb

@@ -1,0 +1,999 @@
+// Host runtime behind the C ABI (include/akb_capi.h): model construction,
+// material instantiation from .dat sections, device memory, the explicit
+// step pipeline and the field / energy getters.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "akb_capi.h"
+#include "dat_parser.h"
+#include "fe_kernels.cuh"
+#include "host_common.h"
+#include "launch.h"
+
+namespace akb {
+static thread_local std::string g_last_error;
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+}  // namespace akb
+
+using namespace akb;
+
+#define AKB_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t err_ = (call);                                                           \
+    if (err_ != cudaSuccess)                                                             \
+      return fail(AKB_ECUDA, std::string(#call) + ": " + cudaGetErrorString(err_));      \
+  } while (0)
+
+#define AKB_TRY(call)                                                                    \
+  do {                                                                                   \
+    int rc_ = (call);                                                                    \
+    if (rc_ != AKB_OK) return rc_;                                                       \
+  } while (0)
+
+namespace {
+
+struct Material {
+  std::string type, name;
+  int law = LAW_ELASTIC;
+  double rho = 0., E = 0., nu = 0.5, sigma_y = 0., h = 0., alpha = 0., delta_T = 0.;
+  bool plane_stress = false, finite_deformation = false;
+  double lambda = 0., mu = 0., sigma_th = 0.;
+  int64_t e_begin = 0, e_count = 0;
+  // plastic internals (SoA [comp][nqp]), ping-pong prev / cur
+  double *sig[2] = {nullptr, nullptr}, *gu[2] = {nullptr, nullptr};
+  double *eps[2] = {nullptr, nullptr}, *iso[2] = {nullptr, nullptr};
+  double *pe = nullptr;
+
+  // Lame update (material_elastic.cc:53-78, material_neohookean.cc:61-67),
+  // thermal stress (material_thermal.hh:89-95)
+  void update(int dim) {
+    lambda = nu * E / ((1 + nu) * (1 - 2 * nu));
+    mu = E / (2 * (1 + nu));
+    if (dim == 2 && plane_stress && law != LAW_NEOHOOKEAN)
+      lambda = nu * E / ((1 + nu) * (1 - nu));
+    sigma_th = -E / (1. - 2. * nu) * alpha * delta_T;
+  }
+  MatParams params() const { return MatParams{lambda, mu, sigma_y, h, sigma_th, rho}; }
+  double celerity() const { return std::sqrt((lambda + 2 * mu) / rho); }
+};
+
+int nodes_per_element(int et) {
+  return et == AKB_TETRAHEDRON_4 ? 4 : (et == AKB_HEXAHEDRON_8 ? 8 : 6);
+}
+int dim_of(int et) { return et == AKB_TRIANGLE_6 ? 2 : 3; }
+
+// quadrature tables (gauss_integration.cc) and the natural-coordinate shape
+// functions / derivatives of the element files, evaluated at the points
+int quadrature(int et, int rule, double *pts, double *w) {
+  if (et == AKB_TETRAHEDRON_4) {
+    pts[0] = pts[1] = pts[2] = 1. / 4.;
+    w[0] = 1. / 6.;
+    return 1;
+  }
+  if (et == AKB_HEXAHEDRON_8) {
+    const double g[2] = {-1. / std::sqrt(3.), 1. / std::sqrt(3.)};
+    for (int q = 0; q < 8; ++q) {
+      pts[q * 3 + 0] = g[q & 1];
+      pts[q * 3 + 1] = g[(q >> 1) & 1];
+      pts[q * 3 + 2] = g[(q >> 2) & 1];
+      w[q] = 1.;
+    }
+    return 8;
+  }
+  if (rule == 0) {
+    const double p[6] = {1. / 6., 1. / 6., 2. / 3., 1. / 6., 1. / 6., 2. / 3.};
+    std::copy(p, p + 6, pts);
+    w[0] = w[1] = w[2] = 1. / 6.;
+    return 3;
+  }
+  const double a = (8. - std::sqrt(10.) + std::sqrt(38. - 44. * std::sqrt(2. / 5.))) / 18.;
+  const double b = (8. - std::sqrt(10.) - std::sqrt(38. - 44. * std::sqrt(2. / 5.))) / 18.;
+  const double w1 = (620. - std::sqrt(213125. - 53320. * std::sqrt(10.))) / 7440.;
+  const double w2 = (620. + std::sqrt(213125. - 53320. * std::sqrt(10.))) / 7440.;
+  const double p[12] = {b, b, 1. - 2. * b, b, b, 1. - 2. * b, a, 1. - 2. * a, a, a, 1. - 2. * a, a};
+  std::copy(p, p + 12, pts);
+  w[0] = w[1] = w[2] = w1;
+  w[3] = w[4] = w[5] = w2;
+  return 6;
+}
+
+void fill_tables(int et, int rule, QuadTable &tab, int &nq) {
+  std::memset(&tab, 0, sizeof(tab));
+  double pts[24], w[8];
+  nq = quadrature(et, rule, pts, w);
+  const int d = dim_of(et);
+  for (int q = 0; q < nq; ++q) {
+    const double *c = &pts[q * d];
+    double *N = &tab.N[q * kMaxNN];
+    double *r0 = &tab.dnds[q * 3 * kMaxNN], *r1 = r0 + kMaxNN, *r2 = r1 + kMaxNN;
+    tab.w[q] = w[q];
+    if (et == AKB_TETRAHEDRON_4) {
+      double c0 = 1 - c[0] - c[1] - c[2];
+      N[0] = c0; N[1] = c[1]; N[2] = c[2]; N[3] = c[0];
+      const double v0[4] = {-1., 0., 0., 1.}, v1[4] = {-1., 1., 0., 0.}, v2[4] = {-1., 0., 1., 0.};
+      for (int a = 0; a < 4; ++a) { r0[a] = v0[a]; r1[a] = v1[a]; r2[a] = v2[a]; }
+    } else if (et == AKB_HEXAHEDRON_8) {
+      // node a at (sx, sy, sz) in {-1, 1}^3, element_class_hexahedron_8_inline_impl.hh
+      static const int s[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                  {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+      for (int a = 0; a < 8; ++a) {
+        const double fx = s[a][0] < 0 ? (1 - c[0]) : (1 + c[0]);
+        const double fy = s[a][1] < 0 ? (1 - c[1]) : (1 + c[1]);
+        const double fz = s[a][2] < 0 ? (1 - c[2]) : (1 + c[2]);
+        N[a] = .125 * fx * fy * fz;
+        r0[a] = (s[a][0] < 0 ? -.125 : .125) * fy * fz;
+        r1[a] = (s[a][1] < 0 ? -.125 : .125) * fx * fz;
+        r2[a] = (s[a][2] < 0 ? -.125 : .125) * fx * fy;
+      }
+    } else {
+      double c0 = 1 - c[0] - c[1], c1 = c[0], c2 = c[1];
+      N[0] = c0 * (2 * c0 - 1.); N[1] = c1 * (2 * c1 - 1.); N[2] = c2 * (2 * c2 - 1.);
+      N[3] = 4 * c0 * c1; N[4] = 4 * c1 * c2; N[5] = 4 * c2 * c0;
+      r0[0] = 1 - 4 * c0; r0[1] = 4 * c1 - 1.; r0[2] = 0.;
+      r0[3] = 4 * (c0 - c1); r0[4] = 4 * c2; r0[5] = -4 * c2;
+      r1[0] = 1 - 4 * c0; r1[1] = 0.; r1[2] = 4 * c2 - 1.;
+      r1[3] = -4 * c1; r1[4] = 4 * c1; r1[5] = 4 * (c0 - c2);
+    }
+  }
+}
+
+}  // namespace
+
+struct akb_model {
+  int dim = 3, et = 0, nn = 4, nq = 1, rule = 0, precision = AKB_PRECISION_FP64;
+  int64_t N = 0, E = 0;
+  std::vector<double> X;
+  std::vector<int32_t> conn;        // user order [E][nn]
+  std::vector<int32_t> mat_user;    // user element -> material
+  std::vector<Material> mats;
+  std::vector<int64_t> perm;        // internal element -> user element
+  bool initialized = false, forces_evaluated = false, snap_valid = false;
+  int cur = 0;  // ping-pong index of the latest plastic state
+  int64_t steps_done = 0;
+  double dt = 0.;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // device arrays
+  double *dX = nullptr, *dB = nullptr, *dwJ = nullptr;
+  float *fB = nullptr, *fwJ = nullptr;
+  int32_t *dconn = nullptr, *dptr = nullptr, *dent = nullptr;
+  double *du = nullptr, *dv = nullptr, *da = nullptr, *dfext = nullptr, *dfint = nullptr;
+  double *dmass = nullptr, *dusnap = nullptr;
+  uint8_t *dblocked = nullptr;
+  void *dre = nullptr;
+  double *dscratch = nullptr, *dpartials = nullptr, *dresult = nullptr;
+  double *dqp_a = nullptr, *dqp_b = nullptr;
+  int64_t qp_scratch_size = 0;
+  unsigned int *dstatus = nullptr;
+  unsigned long long *dbad = nullptr;
+  std::vector<void *> allocs;
+
+  DevGeom geom() const {
+    DevGeom g;
+    g.et = et; g.D = dim; g.NN = nn; g.NQ = nq; g.E = E; g.N = N;
+    g.conn = dconn; g.X = dX; g.ptr = dptr; g.ent = dent;
+    return g;
+  }
+  template <class P> int alloc(P **p, size_t bytes) {
+    void *q = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? AKB_ENOMEM : AKB_ECUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(q);
+    *p = (P *)q;
+    return AKB_OK;
+  }
+  ~akb_model() {
+    for (void *p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int apply_param(Material &m, const std::string &key, const std::string &val) {
+  if (key == "name") {
+    m.name = val;
+    return AKB_OK;
+  }
+  double v;
+  if (!eval_value(val, v))
+    return fail(AKB_EPARSE, "material parameter '" + key + "' has a non-numeric value '" + val + "'");
+  if (key == "rho") m.rho = v;
+  else if (key == "E") m.E = v;
+  else if (key == "nu") m.nu = v;
+  else if (key == "sigma_y") m.sigma_y = v;
+  else if (key == "h") m.h = v;
+  else if (key == "alpha") m.alpha = v;
+  else if (key == "delta_T") m.delta_T = v;
+  else if (key == "Plane_Stress") m.plane_stress = v != 0.;
+  else if (key == "finite_deformation") m.finite_deformation = v != 0.;
+  else if (key == "eigen_grad_u") {
+    if (v != 0.) return fail(AKB_EUNSUPPORTED, "a non-zero eigen_grad_u is not supported");
+  } else
+    return fail(AKB_EPARSE, "unknown material parameter '" + key + "'");
+  return AKB_OK;
+}
+
+int make_material(akb_model *m, const std::string &type, const std::string &name,
+                  const std::vector<std::pair<std::string, std::string>> &kv, bool permissive) {
+  Material mat;
+  mat.type = type;
+  if (type == "elastic") mat.law = LAW_ELASTIC;
+  else if (type == "neohookean") { mat.law = LAW_NEOHOOKEAN; mat.finite_deformation = true; }
+  else if (type == "plastic_linear_isotropic_hardening") mat.law = LAW_PLASTIC;
+  else return fail(AKB_EMATERIAL, "unknown material type '" + type + "'");
+  mat.name = name;
+  for (auto &p : kv) {
+    int rc = apply_param(mat, p.first, p.second);
+    if (rc == AKB_EPARSE && permissive && p.first != "rho" && p.first != "E" && p.first != "nu")
+      continue;
+    if (rc != AKB_OK) return rc;
+  }
+  if (mat.law == LAW_ELASTIC && mat.finite_deformation)
+    return fail(AKB_EUNSUPPORTED, "finite_deformation elastic is not supported by this path");
+  if (mat.law == LAW_PLASTIC && mat.finite_deformation)
+    return fail(AKB_EUNSUPPORTED, "finite-strain plasticity is not supported by this path");
+  if (mat.law == LAW_NEOHOOKEAN && mat.plane_stress)
+    return fail(AKB_EUNSUPPORTED, "plane-stress neohookean is not supported by this path");
+  if (mat.law == LAW_PLASTIC && mat.alpha * mat.delta_T != 0.)
+    return fail(AKB_EUNSUPPORTED, "thermal stress with plasticity is not supported");
+  m->mats.push_back(mat);
+  return AKB_OK;
+}
+
+int check_model(akb_model *m, bool need_init) {
+  if (!m) return fail(AKB_EINVAL, "null model");
+  if (need_init && !m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  return AKB_OK;
+}
+
+int64_t nodal_doubles(const akb_model *m) { return m->N * m->dim; }
+
+// snapshot of u used by the elastic / neohookean quadrature-point getters
+// when the displacement is overwritten after the last force evaluation
+int snapshot_u(akb_model *m) {
+  if (!m->forces_evaluated || m->snap_valid) return AKB_OK;
+  bool need = false;
+  for (auto &mt : m->mats) need |= mt.law != LAW_PLASTIC;
+  if (!need) return AKB_OK;
+  if (!m->dusnap) AKB_TRY(m->alloc(&m->dusnap, sizeof(double) * nodal_doubles(m)));
+  AKB_CUDA(cudaMemcpyAsync(m->dusnap, m->du, sizeof(double) * nodal_doubles(m),
+                           cudaMemcpyDeviceToDevice, m->stream));
+  m->snap_valid = true;
+  return AKB_OK;
+}
+
+PlasticState plastic_state(akb_model *m, const Material &mt, bool in_step) {
+  PlasticState ps;
+  std::memset(&ps, 0, sizeof(ps));
+  if (mt.law != LAW_PLASTIC) return ps;
+  const int c = m->cur;
+  // inside a step the new state goes to the other buffer; a standalone
+  // assembly recomputes the current state from the previous one
+  const int prev = in_step ? c : 1 - c;
+  const int out = in_step ? 1 - c : c;
+  ps.sig_prev = mt.sig[prev];
+  ps.gu_prev = mt.gu[prev];
+  ps.eps_prev = mt.eps[prev];
+  ps.iso_prev = mt.iso[prev];
+  ps.iso_cur_in = mt.iso[c];
+  ps.sig = mt.sig[out];
+  ps.gu = mt.gu[out];
+  ps.eps = mt.eps[out];
+  ps.iso = mt.iso[out];
+  ps.pe = mt.pe;
+  ps.nqp = mt.e_count * m->nq;
+  ps.update_energy = in_step ? 1 : 0;
+  return ps;
+}
+
+int element_forces(akb_model *m, bool in_step) {
+  DevGeom g = m->geom();
+  for (auto &mt : m->mats) {
+    PlasticState ps = plastic_state(m, mt, in_step);
+    cudaError_t e;
+    if (m->precision == AKB_PRECISION_MIXED)
+      e = launch_element_forces_mixed(g, mt.law, mt.e_begin, mt.e_count, m->fB, m->fwJ, m->du,
+                                      mt.params(), ps, (float *)m->dre, m->stream);
+    else
+      e = launch_element_forces_fp64(g, mt.law, mt.e_begin, mt.e_count, m->dB, m->dwJ, m->du,
+                                     mt.params(), ps, (double *)m->dre, m->stream);
+    if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("element forces: ") + cudaGetErrorString(e));
+  }
+  return AKB_OK;
+}
+
+int node_update(akb_model *m, bool correct) {
+  DevGeom g = m->geom();
+  cudaError_t e;
+  if (m->precision == AKB_PRECISION_MIXED)
+    e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass, m->dblocked,
+                                 m->dfint, m->da, m->dv, m->dt, correct ? 1 : 0, m->dstatus,
+                                 m->stream);
+  else
+    e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass, m->dblocked,
+                                m->dfint, m->da, m->dv, m->dt, correct ? 1 : 0, m->dstatus,
+                                m->stream);
+  if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
+  return AKB_OK;
+}
+
+int ensure_qp_scratch(akb_model *m) {
+  int64_t need = 0;
+  for (auto &mt : m->mats) need = std::max(need, mt.e_count * m->nq * m->dim * m->dim);
+  if (need <= m->qp_scratch_size) return AKB_OK;
+  AKB_TRY(m->alloc(&m->dqp_a, sizeof(double) * need));
+  AKB_TRY(m->alloc(&m->dqp_b, sizeof(double) * need));
+  m->qp_scratch_size = need;
+  return AKB_OK;
+}
+
+// grad u and stress (or PK2) of an elastic / neohookean material into the
+// qp scratch buffers, SoA [dd][nqp]
+int eval_qp_fields(akb_model *m, const Material &mt) {
+  AKB_TRY(ensure_qp_scratch(m));
+  const int64_t n = mt.e_count * m->nq * m->dim * m->dim;
+  if (!m->forces_evaluated) {
+    AKB_CUDA(cudaMemsetAsync(m->dqp_a, 0, sizeof(double) * std::max<int64_t>(n, 1), m->stream));
+    AKB_CUDA(cudaMemsetAsync(m->dqp_b, 0, sizeof(double) * std::max<int64_t>(n, 1), m->stream));
+    return AKB_OK;
+  }
+  const double *u = m->snap_valid ? m->dusnap : m->du;
+  AKB_CUDA(launch_qp_fields(m->geom(), mt.law, mt.e_begin, mt.e_count, m->dB, u, mt.params(),
+                            m->dqp_a, m->dqp_b, m->stream));
+  return AKB_OK;
+}
+
+int reduce_to_host(akb_model *m, const double *x, int64_t n, bool op_min, double *out) {
+  AKB_CUDA(launch_reduce(x, n, op_min ? 1 : 0, m->dpartials, m->dresult, m->stream));
+  AKB_CUDA(cudaMemcpyAsync(out, m->dresult, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------------ */
+/* C ABI                                                                    */
+/* ------------------------------------------------------------------------ */
+extern "C" {
+
+const char *akb_last_error(void) { return g_last_error.c_str(); }
+int akb_version(void) { return 100; }
+
+int akb_device_count(int *count) {
+  if (!count) return fail(AKB_EINVAL, "null argument");
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return fail(AKB_ECUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  *count = c;
+  return AKB_OK;
+}
+
+int akb_set_device(int device) {
+  AKB_CUDA(cudaSetDevice(device));
+  return AKB_OK;
+}
+
+int akb_host_alloc(size_t bytes, void **ptr) {
+  if (!ptr) return fail(AKB_EINVAL, "null argument");
+  AKB_CUDA(cudaHostAlloc(ptr, bytes ? bytes : 16, cudaHostAllocDefault));
+  return AKB_OK;
+}
+
+int akb_host_free(void *ptr) {
+  if (ptr) AKB_CUDA(cudaFreeHost(ptr));
+  return AKB_OK;
+}
+
+int akb_model_create(int dim, int et, const double *nodes, int64_t N, const int32_t *conn,
+                     int64_t E, akb_model **out) {
+  if (!out) return fail(AKB_EINVAL, "null output pointer");
+  *out = nullptr;
+  if (et < AKB_TETRAHEDRON_4 || et > AKB_TRIANGLE_6) return fail(AKB_EINVAL, "unknown element type");
+  if (dim != dim_of(et)) return fail(AKB_EINVAL, "spatial dimension does not match the element type");
+  if (N < 0 || E < 0 || (N > 0 && !nodes) || (E > 0 && !conn))
+    return fail(AKB_EINVAL, "bad mesh arrays");
+  const int nn = nodes_per_element(et);
+  if (E * nn >= (int64_t)std::numeric_limits<int32_t>::max())
+    return fail(AKB_EINVAL, "mesh too large for 32-bit slot indices");
+  for (int64_t k = 0; k < E * nn; ++k)
+    if (conn[k] < 0 || conn[k] >= N) return fail(AKB_EINVAL, "connectivity refers to a missing node");
+  auto *m = new akb_model();
+  m->dim = dim;
+  m->et = et;
+  m->nn = nn;
+  m->N = N;
+  m->E = E;
+  m->X.assign(nodes, nodes + N * dim);
+  m->conn.assign(conn, conn + E * nn);
+  *out = m;
+  return AKB_OK;
+}
+
+int akb_model_destroy(akb_model *m) {
+  if (!m) return AKB_OK;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  delete m;
+  return AKB_OK;
+}
+
+int akb_model_load_materials(akb_model *m, const char *text) {
+  AKB_TRY(check_model(m, false));
+  if (!text) return fail(AKB_EINVAL, "null text");
+  if (m->initialized) return fail(AKB_ESTATE, "materials must be loaded before initFull");
+  ParsedFile pf;
+  std::string err;
+  if (!parse_dat(text, pf, err)) return fail(AKB_EPARSE, ".dat: " + err);
+  bool permissive = false;
+  auto it = pf.globals.find("permissive_parser");
+  if (it != pf.globals.end()) {
+    double v;
+    permissive = eval_value(it->second, v) && v != 0.;
+  }
+  for (auto &pm : pf.materials) {
+    std::vector<std::pair<std::string, std::string>> kv(pm.raw.begin(), pm.raw.end());
+    AKB_TRY(make_material(m, pm.type, pm.name, kv, permissive));
+  }
+  return AKB_OK;
+}
+
+int akb_model_add_material(akb_model *m, const char *type, const char *params) {
+  AKB_TRY(check_model(m, false));
+  if (!type) return fail(AKB_EINVAL, "null type");
+  if (m->initialized) return fail(AKB_ESTATE, "materials must be added before initFull");
+  std::string text = std::string("material ") + type + " [\n";
+  if (params) {
+    for (const char *p = params; *p; ++p) text.push_back(*p == ';' ? '\n' : *p);
+  }
+  text += "\n]\n";
+  ParsedFile pf;
+  std::string err;
+  if (!parse_dat(text, pf, err)) return fail(AKB_EPARSE, "material parameters: " + err);
+  auto &pm = pf.materials.at(0);
+  std::vector<std::pair<std::string, std::string>> kv(pm.raw.begin(), pm.raw.end());
+  return make_material(m, pm.type, pm.name, kv, false);
+}
+
+int akb_model_set_element_materials(akb_model *m, const int32_t *mat) {
+  AKB_TRY(check_model(m, false));
+  if (m->initialized) return fail(AKB_ESTATE, "element materials must be set before initFull");
+  if (!mat && m->E > 0) return fail(AKB_EINVAL, "null array");
+  m->mat_user.assign(mat, mat + m->E);
+  return AKB_OK;
+}
+
+int akb_model_set_quadrature_rule(akb_model *m, int rule) {
+  AKB_TRY(check_model(m, false));
+  if (m->initialized) return fail(AKB_ESTATE, "the quadrature rule must be set before initFull");
+  if (rule != 0 && !(rule == 1 && m->et == AKB_TRIANGLE_6))
+    return fail(AKB_EUNSUPPORTED, "only _triangle_6 has an alternative (6-point) rule");
+  m->rule = rule;
+  return AKB_OK;
+}
+
+int akb_model_init_full(akb_model *m, int method, int precision) {
+  AKB_TRY(check_model(m, false));
+  if (m->initialized) return fail(AKB_ESTATE, "initFull called twice");
+  if (method != AKB_EXPLICIT_LUMPED_MASS)
+    return fail(AKB_EUNSUPPORTED, "only _explicit_lumped_mass is provided");
+  if (precision != AKB_PRECISION_FP64 && precision != AKB_PRECISION_MIXED)
+    return fail(AKB_EINVAL, "unknown precision");
+  if (m->mats.empty()) return fail(AKB_EMATERIAL, "no material defined (parse a .dat first)");
+  if (m->mat_user.empty()) m->mat_user.assign(m->E, 0);
+  for (int32_t k : m->mat_user)
+    if (k < 0 || k >= (int32_t)m->mats.size()) return fail(AKB_EINVAL, "element material index out of range");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(AKB_ECUDA, "no CUDA device available");
+  for (auto &mt : m->mats) mt.update(m->dim);
+  m->precision = precision;
+  AKB_CUDA(cudaGetDevice(&m->device));
+  AKB_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+
+  const int nn = m->nn, d = m->dim;
+  const int64_t E = m->E, N = m->N;
+  QuadTable tab;
+  fill_tables(m->et, m->rule, tab, m->nq);
+  const int nq = m->nq;
+
+  // internal element order: grouped by material, ascending user id inside
+  m->perm.resize(E);
+  {
+    std::vector<int64_t> count(m->mats.size() + 1, 0);
+    for (int64_t e = 0; e < E; ++e) count[m->mat_user[e] + 1]++;
+    for (size_t k = 0; k < m->mats.size(); ++k) {
+      count[k + 1] += count[k];
+      m->mats[k].e_begin = count[k];
+      m->mats[k].e_count = count[k + 1] - count[k];
+    }
+    for (int64_t e = 0; e < E; ++e) m->perm[count[m->mat_user[e]]++] = e;
+  }
+  std::vector<int32_t> conn_soa((size_t)nn * E);
+  for (int64_t ie = 0; ie < E; ++ie)
+    for (int a = 0; a < nn; ++a) conn_soa[(size_t)a * E + ie] = m->conn[m->perm[ie] * nn + a];
+  // node -> slot CSR, slots ascending (= material, user element, local node)
+  std::vector<int32_t> ptr(N + 1, 0), ent((size_t)E * nn);
+  for (int64_t ie = 0; ie < E; ++ie)
+    for (int a = 0; a < nn; ++a) ptr[conn_soa[(size_t)a * E + ie] + 1]++;
+  for (int64_t i = 0; i < N; ++i) ptr[i + 1] += ptr[i];
+  {
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int64_t ie = 0; ie < E; ++ie)
+      for (int a = 0; a < nn; ++a) ent[fill[conn_soa[(size_t)a * E + ie]]++] = (int32_t)(ie * nn + a);
+  }
+
+  AKB_TRY(m->alloc(&m->dX, sizeof(double) * N * d));
+  AKB_TRY(m->alloc(&m->dconn, sizeof(int32_t) * E * nn));
+  AKB_TRY(m->alloc(&m->dptr, sizeof(int32_t) * (N + 1)));
+  AKB_TRY(m->alloc(&m->dent, sizeof(int32_t) * E * nn));
+  AKB_TRY(m->alloc(&m->dB, sizeof(double) * E * nq * nn * d));
+  AKB_TRY(m->alloc(&m->dwJ, sizeof(double) * E * nq));
+  for (double **p : {&m->du, &m->dv, &m->da, &m->dfext, &m->dfint})
+    AKB_TRY(m->alloc(p, sizeof(double) * N * d));
+  AKB_TRY(m->alloc(&m->dmass, sizeof(double) * N));
+  AKB_TRY(m->alloc(&m->dblocked, N));
+  const size_t re_bytes = (precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double)) *
+                          (size_t)E * nn * d;
+  AKB_TRY(m->alloc(&m->dre, std::max(re_bytes, sizeof(double) * (size_t)E * nn)));
+  AKB_TRY(m->alloc(&m->dscratch, sizeof(double) * std::max<int64_t>(std::max(E, N), 1)));
+  AKB_TRY(m->alloc(&m->dpartials, sizeof(double) * kReducePartials));
+  AKB_TRY(m->alloc(&m->dresult, sizeof(double)));
+  AKB_TRY(m->alloc(&m->dstatus, sizeof(unsigned int)));
+  AKB_TRY(m->alloc(&m->dbad, sizeof(unsigned long long)));
+  cudaStream_t s = m->stream;
+  AKB_CUDA(cudaMemcpyAsync(m->dX, m->X.data(), sizeof(double) * N * d, cudaMemcpyHostToDevice, s));
+  AKB_CUDA(cudaMemcpyAsync(m->dconn, conn_soa.data(), sizeof(int32_t) * E * nn, cudaMemcpyHostToDevice, s));
+  AKB_CUDA(cudaMemcpyAsync(m->dptr, ptr.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, s));
+  AKB_CUDA(cudaMemcpyAsync(m->dent, ent.data(), sizeof(int32_t) * E * nn, cudaMemcpyHostToDevice, s));
+  for (double *p : {m->du, m->dv, m->da, m->dfext, m->dfint})
+    AKB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * N * d, s));
+  AKB_CUDA(cudaMemsetAsync(m->dblocked, 0, N, s));
+  AKB_CUDA(cudaMemsetAsync(m->dstatus, 0, sizeof(unsigned int), s));
+  AKB_CUDA(cudaMemsetAsync(m->dbad, 0xff, sizeof(unsigned long long), s));
+
+  DevGeom g = m->geom();
+  AKB_CUDA(launch_precompute(g, tab, m->dB, m->dwJ, m->dbad, s));
+  unsigned long long bad = 0;
+  AKB_CUDA(cudaMemcpyAsync(&bad, m->dbad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+  AKB_CUDA(cudaStreamSynchronize(s));
+  if (bad != ~0ull) {
+    const int64_t ie = (int64_t)(bad / nq);
+    return fail(AKB_ENEGJAC, "Negative jacobian computed, possible problem in the element node "
+                             "ordering (Quadrature Point " + std::to_string(bad % nq) + ":" +
+                             std::to_string(m->perm[ie]) + ")");
+  }
+  // lumped mass
+  double *me = (double *)m->dre;
+  for (auto &mt : m->mats)
+    AKB_CUDA(launch_mass_elem(g, mt.e_begin, mt.e_count, mt.rho, tab, m->dwJ, me, s));
+  AKB_CUDA(launch_gather_scalar(g, me, m->dmass, s));
+  if (precision == AKB_PRECISION_MIXED) {
+    AKB_TRY(m->alloc(&m->fB, sizeof(float) * E * nq * nn * d));
+    AKB_TRY(m->alloc(&m->fwJ, sizeof(float) * E * nq));
+    AKB_CUDA(launch_to_float(m->dB, m->fB, E * nq * nn * d, s));
+    AKB_CUDA(launch_to_float(m->dwJ, m->fwJ, E * nq, s));
+  }
+  for (auto &mt : m->mats) {
+    if (mt.law != LAW_PLASTIC) continue;
+    const int64_t nqp = mt.e_count * nq, dd = (int64_t)d * d;
+    for (int b = 0; b < 2; ++b) {
+      AKB_TRY(m->alloc(&mt.sig[b], sizeof(double) * nqp * dd));
+      AKB_TRY(m->alloc(&mt.gu[b], sizeof(double) * nqp * dd));
+      AKB_TRY(m->alloc(&mt.eps[b], sizeof(double) * nqp * dd));
+      AKB_TRY(m->alloc(&mt.iso[b], sizeof(double) * nqp));
+      for (double *p : {mt.sig[b], mt.gu[b], mt.eps[b]})
+        AKB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * std::max<int64_t>(nqp * dd, 1), s));
+      AKB_CUDA(cudaMemsetAsync(mt.iso[b], 0, sizeof(double) * std::max<int64_t>(nqp, 1), s));
+    }
+    AKB_TRY(m->alloc(&mt.pe, sizeof(double) * nqp));
+    AKB_CUDA(cudaMemsetAsync(mt.pe, 0, sizeof(double) * std::max<int64_t>(nqp, 1), s));
+  }
+  AKB_CUDA(cudaStreamSynchronize(s));
+  m->initialized = true;
+  return AKB_OK;
+}
+
+int akb_model_nb_materials(const akb_model *m, int *count) {
+  if (!m || !count) return fail(AKB_EINVAL, "null argument");
+  *count = (int)m->mats.size();
+  return AKB_OK;
+}
+
+int akb_model_get_material_param(const akb_model *m, int k, const char *name, double *v) {
+  if (!m || !name || !v) return fail(AKB_EINVAL, "null argument");
+  if (k < 0 || k >= (int)m->mats.size()) return fail(AKB_EINVAL, "material index out of range");
+  Material mt = m->mats[k];
+  mt.update(m->dim);
+  std::string n(name);
+  if (n == "rho") *v = mt.rho;
+  else if (n == "E") *v = mt.E;
+  else if (n == "nu") *v = mt.nu;
+  else if (n == "lambda") *v = mt.lambda;
+  else if (n == "mu") *v = mt.mu;
+  else if (n == "sigma_y") *v = mt.sigma_y;
+  else if (n == "h") *v = mt.h;
+  else if (n == "alpha") *v = mt.alpha;
+  else if (n == "delta_T") *v = mt.delta_T;
+  else if (n == "kapa") *v = mt.lambda + 2. / 3. * mt.mu;
+  else if (n == "Plane_Stress") *v = mt.plane_stress ? 1. : 0.;
+  else if (n == "finite_deformation") *v = mt.finite_deformation ? 1. : 0.;
+  else return fail(AKB_EINVAL, "unknown parameter '" + n + "'");
+  return AKB_OK;
+}
+
+int akb_model_get_material_name(const akb_model *m, int k, char *buf, size_t size) {
+  if (!m || !buf || size == 0) return fail(AKB_EINVAL, "null argument");
+  if (k < 0 || k >= (int)m->mats.size()) return fail(AKB_EINVAL, "material index out of range");
+  std::snprintf(buf, size, "%s", m->mats[k].name.c_str());
+  return AKB_OK;
+}
+
+int akb_model_nb_quadrature_points(const akb_model *m, int *nq) {
+  if (!m || !nq) return fail(AKB_EINVAL, "null argument");
+  if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  *nq = m->nq;
+  return AKB_OK;
+}
+
+int akb_model_get_fe_data(akb_model *m, int which, double *host, int64_t count) {
+  AKB_TRY(check_model(m, true));
+  const int64_t EQ = m->E * m->nq, comps = which == 0 ? (int64_t)m->nn * m->dim : 1;
+  if (which != 0 && which != 1) return fail(AKB_EINVAL, "which must be 0 (dN/dx) or 1 (det J w)");
+  if (count != EQ * comps) return fail(AKB_EINVAL, "count does not match the field size");
+  if (!host && count > 0) return fail(AKB_EINVAL, "null host buffer");
+  std::vector<double> soa((size_t)EQ * comps);
+  AKB_CUDA(cudaMemcpyAsync(soa.data(), which == 0 ? m->dB : m->dwJ, sizeof(double) * soa.size(),
+                           cudaMemcpyDeviceToHost, m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  for (int64_t ie = 0; ie < m->E; ++ie) {
+    const int64_t ue = m->perm[ie];
+    for (int q = 0; q < m->nq; ++q)
+      for (int64_t c = 0; c < comps; ++c)
+        host[(ue * m->nq + q) * comps + c] = soa[(size_t)c * EQ + ie * m->nq + q];
+  }
+  return AKB_OK;
+}
+
+int akb_model_get_stable_time_step(akb_model *m, double *dt) {
+  AKB_TRY(check_model(m, true));
+  if (!dt) return fail(AKB_EINVAL, "null argument");
+  DevGeom g = m->geom();
+  for (auto &mt : m->mats)
+    AKB_CUDA(launch_element_dt(g, mt.e_begin, mt.e_count, mt.celerity(), m->du, m->dscratch, m->stream));
+  return reduce_to_host(m, m->dscratch, m->E, true, dt);
+}
+
+int akb_model_set_time_step(akb_model *m, double dt) {
+  AKB_TRY(check_model(m, false));
+  m->dt = dt;
+  return AKB_OK;
+}
+int akb_model_get_time_step(const akb_model *m, double *dt) {
+  if (!m || !dt) return fail(AKB_EINVAL, "null argument");
+  *dt = m->dt;
+  return AKB_OK;
+}
+
+int akb_model_set_nodal(akb_model *m, int field, const void *host, int64_t nbytes) {
+  AKB_TRY(check_model(m, true));
+  const int64_t nd = nodal_doubles(m);
+  if (!host && nd > 0) return fail(AKB_EINVAL, "null host buffer");
+  if (field == AKB_BLOCKED_DOFS) {
+    if (nbytes != nd) return fail(AKB_EINVAL, "blocked dofs: size must be N*dim bytes");
+    const uint8_t *b = (const uint8_t *)host;
+    std::vector<uint8_t> mask(m->N, 0);
+    for (int64_t i = 0; i < m->N; ++i)
+      for (int c = 0; c < m->dim; ++c)
+        if (b[i * m->dim + c]) mask[i] |= (uint8_t)(1u << c);
+    AKB_CUDA(cudaMemcpyAsync(m->dblocked, mask.data(), m->N, cudaMemcpyHostToDevice, m->stream));
+    AKB_CUDA(cudaStreamSynchronize(m->stream));
+    return AKB_OK;
+  }
+  if (nbytes != nd * (int64_t)sizeof(double)) return fail(AKB_EINVAL, "size must be N*dim doubles");
+  double *dst = nullptr;
+  switch (field) {
+  case AKB_DISPLACEMENT:
+    AKB_TRY(snapshot_u(m));
+    dst = m->du;
+    break;
+  case AKB_VELOCITY: dst = m->dv; break;
+  case AKB_ACCELERATION: dst = m->da; break;
+  case AKB_EXTERNAL_FORCE: dst = m->dfext; break;
+  default: return fail(AKB_EINVAL, "field is read-only or unknown");
+  }
+  AKB_CUDA(cudaMemcpyAsync(dst, host, nbytes, cudaMemcpyHostToDevice, m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+int akb_model_get_nodal(akb_model *m, int field, void *host, int64_t nbytes) {
+  AKB_TRY(check_model(m, true));
+  const int64_t nd = nodal_doubles(m);
+  if (!host && nd > 0) return fail(AKB_EINVAL, "null host buffer");
+  cudaStream_t s = m->stream;
+  if (field == AKB_BLOCKED_DOFS) {
+    if (nbytes != nd) return fail(AKB_EINVAL, "blocked dofs: size must be N*dim bytes");
+    std::vector<uint8_t> mask(m->N);
+    AKB_CUDA(cudaMemcpyAsync(mask.data(), m->dblocked, m->N, cudaMemcpyDeviceToHost, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
+    uint8_t *b = (uint8_t *)host;
+    for (int64_t i = 0; i < m->N; ++i)
+      for (int c = 0; c < m->dim; ++c) b[i * m->dim + c] = (mask[i] >> c) & 1;
+    return AKB_OK;
+  }
+  if (nbytes != nd * (int64_t)sizeof(double)) return fail(AKB_EINVAL, "size must be N*dim doubles");
+  double *out = (double *)host;
+  switch (field) {
+  case AKB_MASS: {
+    std::vector<double> mass(m->N);
+    AKB_CUDA(cudaMemcpyAsync(mass.data(), m->dmass, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < m->N; ++i)
+      for (int c = 0; c < m->dim; ++c) out[i * m->dim + c] = mass[i];
+    return AKB_OK;
+  }
+  case AKB_CURRENT_POSITION: {
+    AKB_CUDA(cudaMemcpyAsync(out, m->du, nbytes, cudaMemcpyDeviceToHost, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
+    for (int64_t k = 0; k < nd; ++k) out[k] = m->X[k] + out[k];
+    return AKB_OK;
+  }
+  default: break;
+  }
+  const double *src = nullptr;
+  switch (field) {
+  case AKB_DISPLACEMENT: src = m->du; break;
+  case AKB_VELOCITY: src = m->dv; break;
+  case AKB_ACCELERATION: src = m->da; break;
+  case AKB_EXTERNAL_FORCE: src = m->dfext; break;
+  case AKB_INTERNAL_FORCE: src = m->dfint; break;
+  default: return fail(AKB_EINVAL, "unknown nodal field");
+  }
+  AKB_CUDA(cudaMemcpyAsync(out, src, nbytes, cudaMemcpyDeviceToHost, s));
+  AKB_CUDA(cudaStreamSynchronize(s));
+  return AKB_OK;
+}
+
+int akb_model_nodal_device_pointer(akb_model *m, int field, void **p) {
+  AKB_TRY(check_model(m, true));
+  if (!p) return fail(AKB_EINVAL, "null argument");
+  switch (field) {
+  case AKB_DISPLACEMENT: *p = m->du; break;
+  case AKB_VELOCITY: *p = m->dv; break;
+  case AKB_ACCELERATION: *p = m->da; break;
+  case AKB_EXTERNAL_FORCE: *p = m->dfext; break;
+  case AKB_INTERNAL_FORCE: *p = m->dfint; break;
+  default: return fail(AKB_EINVAL, "no device pointer for this field");
+  }
+  return AKB_OK;
+}
+
+int akb_model_qp_field_size(akb_model *m, int field, int k, int64_t *count) {
+  AKB_TRY(check_model(m, true));
+  if (!count) return fail(AKB_EINVAL, "null argument");
+  if (k < 0 || k >= (int)m->mats.size()) return fail(AKB_EINVAL, "material index out of range");
+  const int64_t nqp = m->mats[k].e_count * m->nq;
+  switch (field) {
+  case AKB_GRAD_U: case AKB_STRESS: case AKB_PIOLA_KIRCHHOFF_2: case AKB_INELASTIC_STRAIN:
+    *count = nqp * m->dim * m->dim;
+    return AKB_OK;
+  case AKB_ISO_HARDENING: case AKB_PLASTIC_ENERGY:
+    *count = nqp;
+    return AKB_OK;
+  default: return fail(AKB_EINVAL, "unknown quadrature-point field");
+  }
+}
+
+int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t count) {
+  int64_t need = 0;
+  AKB_TRY(akb_model_qp_field_size(m, field, k, &need));
+  if (count != need) return fail(AKB_EINVAL, "count does not match the field size");
+  if (!host && need > 0) return fail(AKB_EINVAL, "null host buffer");
+  const Material &mt = m->mats[k];
+  const int64_t nqp = mt.e_count * m->nq;
+  const int dd = m->dim * m->dim;
+  const double *src = nullptr;
+  int comps = dd;
+  if (mt.law == LAW_PLASTIC) {
+    const int c = m->cur;
+    switch (field) {
+    case AKB_GRAD_U: src = mt.gu[c]; break;
+    case AKB_STRESS: src = mt.sig[c]; break;
+    case AKB_INELASTIC_STRAIN: src = mt.eps[c]; break;
+    case AKB_ISO_HARDENING: src = mt.iso[c]; comps = 1; break;
+    case AKB_PLASTIC_ENERGY: src = mt.pe; comps = 1; break;
+    default: return fail(AKB_EINVAL, "field not defined for plastic_linear_isotropic_hardening");
+    }
+  } else {
+    if (field != AKB_GRAD_U && field != AKB_STRESS && field != AKB_PIOLA_KIRCHHOFF_2)
+      return fail(AKB_EINVAL, "field not defined for this material");
+    if (field == AKB_PIOLA_KIRCHHOFF_2 && mt.law != LAW_NEOHOOKEAN)
+      return fail(AKB_EINVAL, "piola_kirchhoff_2 exists only for finite deformation");
+    if (field == AKB_STRESS && mt.law == LAW_NEOHOOKEAN) {
+      // the Cauchy stress of a finite-deformation material is only filled
+      // on dump (Material::onDump); the internal stays zero during stepping
+      std::fill(host, host + need, 0.);
+      return AKB_OK;
+    }
+    AKB_TRY(eval_qp_fields(m, mt));
+    src = (field == AKB_GRAD_U) ? m->dqp_a : m->dqp_b;
+  }
+  std::vector<double> soa((size_t)nqp * comps);
+  AKB_CUDA(cudaMemcpyAsync(soa.data(), src, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  for (int64_t q = 0; q < nqp; ++q)
+    for (int c = 0; c < comps; ++c) host[q * comps + c] = soa[(size_t)c * nqp + q];
+  return AKB_OK;
+}
+
+int akb_model_solve_step(akb_model *m, int64_t nsteps) {
+  AKB_TRY(check_model(m, true));
+  if (nsteps < 0) return fail(AKB_EINVAL, "negative step count");
+  DevGeom g = m->geom();
+  bool any_plastic = false;
+  for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
+  for (int64_t s = 0; s < nsteps; ++s) {
+    AKB_CUDA(launch_predict(g, m->dblocked, m->du, m->dv, m->da, m->dt, m->stream));
+    AKB_TRY(element_forces(m, true));
+    AKB_TRY(node_update(m, true));
+    if (any_plastic) m->cur = 1 - m->cur;
+    m->steps_done++;
+  }
+  if (nsteps > 0) {
+    m->forces_evaluated = true;
+    m->snap_valid = false;
+  }
+  return AKB_OK;
+}
+
+int akb_model_time_steps(akb_model *m, int64_t nsteps, double *ms) {
+  AKB_TRY(check_model(m, true));
+  if (!ms || nsteps < 0) return fail(AKB_EINVAL, "bad argument");
+  cudaEvent_t e0, e1;
+  AKB_CUDA(cudaEventCreate(&e0));
+  AKB_CUDA(cudaEventCreate(&e1));
+  AKB_CUDA(cudaEventRecord(e0, m->stream));
+  int rc = akb_model_solve_step(m, nsteps);
+  cudaError_t e = cudaEventRecord(e1, m->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float f = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != AKB_OK) return rc;
+  if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("timing: ") + cudaGetErrorString(e));
+  *ms = f;
+  return AKB_OK;
+}
+
+int akb_model_profile_steps(akb_model *m, int64_t nsteps, double *total_ms, double *phase_ms) {
+  AKB_TRY(check_model(m, true));
+  if (!total_ms || !phase_ms || nsteps < 1 || nsteps > 4096) return fail(AKB_EINVAL, "bad argument");
+  std::vector<cudaEvent_t> ev((size_t)nsteps * 3 + 1);
+  for (auto &x : ev) AKB_CUDA(cudaEventCreate(&x));
+  DevGeom g = m->geom();
+  bool any_plastic = false;
+  for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
+  int rc = AKB_OK;
+  AKB_CUDA(cudaEventRecord(ev[0], m->stream));
+  for (int64_t s = 0; s < nsteps && rc == AKB_OK; ++s) {
+    cudaError_t e = launch_predict(g, m->dblocked, m->du, m->dv, m->da, m->dt, m->stream);
+    if (e != cudaSuccess) { rc = fail(AKB_ECUDA, cudaGetErrorString(e)); break; }
+    cudaEventRecord(ev[s * 3 + 1], m->stream);
+    rc = element_forces(m, true);
+    if (rc != AKB_OK) break;
+    cudaEventRecord(ev[s * 3 + 2], m->stream);
+    rc = node_update(m, true);
+    if (rc != AKB_OK) break;
+    cudaEventRecord(ev[s * 3 + 3], m->stream);
+    if (any_plastic) m->cur = 1 - m->cur;
+    m->steps_done++;
+  }
+  cudaError_t e = cudaStreamSynchronize(m->stream);
+  if (rc == AKB_OK && e == cudaSuccess) {
+    m->forces_evaluated = true;
+    m->snap_valid = false;
+    phase_ms[0] = phase_ms[1] = phase_ms[2] = 0.;
+    for (int64_t s = 0; s < nsteps; ++s)
+      for (int p = 0; p < 3; ++p) {
+        float f = 0.f;
+        cudaEventElapsedTime(&f, ev[s * 3 + p], ev[s * 3 + p + 1]);
+        phase_ms[p] += f;
+      }
+    float f = 0.f;
+    cudaEventElapsedTime(&f, ev[0], ev[(size_t)nsteps * 3]);
+    *total_ms = f;
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (rc != AKB_OK) return rc;
+  if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("profile: ") + cudaGetErrorString(e));
+  return AKB_OK;
+}
+
+int akb_model_synchronize(akb_model *m) {
+  AKB_TRY(check_model(m, true));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+int akb_model_assemble_internal_forces(akb_model *m) {
+  AKB_TRY(check_model(m, true));
+  AKB_TRY(element_forces(m, false));
+  AKB_TRY(node_update(m, false));
+  m->forces_evaluated = true;
+  m->snap_valid = false;
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+int akb_model_get_energy(akb_model *m, const char *id, double *value) {
+  AKB_TRY(check_model(m, true));
+  if (!id || !value) return fail(AKB_EINVAL, "null argument");
+  std::string which(id);
+  DevGeom g = m->geom();
+  if (which == "kinetic") {
+    AKB_CUDA(launch_ekin_terms(g, m->dv, m->dmass, m->dscratch, m->stream));
+    double s = 0.;
+    AKB_TRY(reduce_to_host(m, m->dscratch, m->N, false, &s));
+    *value = s / 2.;
+    return AKB_OK;
+  }
+  if (which == "external work") {
+    AKB_CUDA(launch_work_terms(g, m->dfext, m->dfint, m->dv, m->dblocked, m->dscratch, m->stream));
+    double s = 0.;
+    AKB_TRY(reduce_to_host(m, m->dscratch, m->N, false, &s));
+    *value = s * m->dt;
+    return AKB_OK;
+  }
+  if (which != "potential" && which != "plastic")
+    return fail(AKB_EINVAL, "unknown energy '" + which + "'");
+  const int kind = which == "plastic" ? 1 : 0;
+  double total = 0.;
+  for (auto &mt : m->mats) {
+    if (kind == 1 && mt.law != LAW_PLASTIC) continue;
+    const double *grad = nullptr, *stress = nullptr, *eps = nullptr;
+    if (mt.law == LAW_PLASTIC) {
+      grad = mt.gu[m->cur];
+      stress = mt.sig[m->cur];
+      eps = mt.eps[m->cur];
+    } else {
+      AKB_TRY(eval_qp_fields(m, mt));
+      grad = m->dqp_a;
+      stress = m->dqp_b;
+    }
+    AKB_CUDA(launch_energy_elem(g, mt.law, kind, mt.e_begin, mt.e_count, m->dwJ, grad, stress,
+                                eps, mt.pe, mt.params(), m->dscratch, m->stream));
+    double s = 0.;
+    AKB_TRY(reduce_to_host(m, m->dscratch, mt.e_count, false, &s));
+    total += s;
+  }
+  *value = total;
+  return AKB_OK;
+}
+
+int akb_model_get_status(akb_model *m, int *flags) {
+  AKB_TRY(check_model(m, true));
+  if (!flags) return fail(AKB_EINVAL, "null argument");
+  unsigned int st = 0;
+  AKB_CUDA(cudaMemcpyAsync(&st, m->dstatus, sizeof(st), cudaMemcpyDeviceToHost, m->stream));
+  AKB_CUDA(cudaMemsetAsync(m->dstatus, 0, sizeof(st), m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  *flags = (int)st;
+  return AKB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,332 @@
+"""SolidMechanicsModel for the explicit lumped-mass path, over libakb.
+
+Mirrors the reference's Python binding (python/py_solid_mechanics_model.cc:
+57-173, python/py_model.cc:131-137): initFull, getStableTimeStep,
+setTimeStep, solveStep and the nodal-array getters.  The arrays live on the
+GPU; the getters return host copies that the model refreshes after each step
+and uploads again before the next step, so a script that edits the array it
+got (boundary values, initial velocity, external force) behaves as with the
+reference's zero-copy views.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from .mesh import Mesh, TYPE_IDS
+
+_explicit_lumped_mass = "_explicit_lumped_mass"
+_x, _y, _z = 0, 1, 2
+
+_FIELDS = {
+    "displacement": _capi.DISPLACEMENT, "velocity": _capi.VELOCITY,
+    "acceleration": _capi.ACCELERATION, "external_force": _capi.EXTERNAL_FORCE,
+    "internal_force": _capi.INTERNAL_FORCE, "mass": _capi.MASS,
+    "blocked_dofs": _capi.BLOCKED_DOFS, "current_position": _capi.CURRENT_POSITION,
+}
+_WRITABLE = ("displacement", "velocity", "acceleration", "external_force", "blocked_dofs")
+
+
+class _Parser:
+    """getStaticParser(): the parsed .dat texts, in parse order."""
+
+    def __init__(self):
+        self.texts = []
+
+    def parse(self, path):
+        with open(path) as f:
+            self.texts.append(f.read())
+
+    def parse_text(self, text):
+        self.texts.append(text)
+
+    def clear(self):
+        self.texts = []
+
+
+_static_parser = _Parser()
+
+
+def getStaticParser():
+    return _static_parser
+
+
+def parseInput(path):
+    """akantu.parseInput: add the sections of a .dat file to the static parser."""
+    _static_parser.parse(path)
+
+
+class FixedValue:
+    """BC::Dirichlet::FixedValue(value, axis)  (boundary_condition_functor_inline_impl.hh:53-61)."""
+
+    def __init__(self, value, axis):
+        self.value = value
+        self.axis = axis
+
+
+class Material:
+    """View of one material of a model (src/model/solid_mechanics/material.hh)."""
+
+    def __init__(self, model, index):
+        self._model = model
+        self._index = index
+
+    def get(self, name):
+        v = ctypes.c_double()
+        _capi.check(_capi.lib().akb_model_get_material_param(
+            self._model._h, self._index, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    getParam = get
+
+    def getRho(self):
+        return self.get("rho")
+
+    def getName(self):
+        buf = ctypes.create_string_buffer(256)
+        _capi.check(_capi.lib().akb_model_get_material_name(self._model._h, self._index, buf, 256))
+        return buf.value.decode()
+
+    def _qp(self, field):
+        m = self._model
+        m._sync_up()
+        n = ctypes.c_int64()
+        L = _capi.lib()
+        _capi.check(L.akb_model_qp_field_size(m._h, field, self._index, ctypes.byref(n)))
+        out = np.zeros(n.value)
+        _capi.check(L.akb_model_get_qp_field(m._h, field, self._index, _capi.ptr(out), n.value))
+        if field in (_capi.ISO_HARDENING, _capi.PLASTIC_ENERGY):
+            return out.reshape(-1, 1)
+        return out.reshape(-1, m.dim * m.dim)
+
+    def getStress(self, element_type=None):
+        return self._qp(_capi.STRESS)
+
+    def getGradU(self, element_type=None):
+        return self._qp(_capi.GRAD_U)
+
+    def getInternal(self, name):
+        ids = {"stress": _capi.STRESS, "grad_u": _capi.GRAD_U,
+               "piola_kirchhoff_2": _capi.PIOLA_KIRCHHOFF_2,
+               "inelastic_strain": _capi.INELASTIC_STRAIN,
+               "iso_hardening": _capi.ISO_HARDENING, "plastic_energy": _capi.PLASTIC_ENERGY}
+        fid = ids[name]
+        return lambda element_type=None: self._qp(fid)
+
+
+class SolidMechanicsModel:
+    """Explicit lumped-mass SolidMechanicsModel on one GPU."""
+
+    def __init__(self, mesh, dim=None, id="solid_mechanics_model"):
+        if not isinstance(mesh, Mesh):
+            raise TypeError("mesh must be an akantu2_b200.Mesh")
+        self.mesh = mesh
+        self.dim = mesh.spatial_dimension if dim is None else dim
+        self.id = id
+        L = _capi.lib()
+        h = ctypes.c_void_p()
+        _capi.check(L.akb_model_create(self.dim, TYPE_IDS[mesh.element_type],
+                                       _capi.ptr(mesh.nodes), mesh.getNbNodes(),
+                                       _capi.ptr(mesh.connectivity), mesh.getNbElement(),
+                                       ctypes.byref(h)))
+        self._h = h
+        self._mirrors = {}
+        self._handed_out = set()
+        self._initialized = False
+        self._materials_added = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _capi.lib().akb_model_destroy(h)
+            self._h = None
+
+    # -- set-up ------------------------------------------------------------------
+    def addMaterial(self, type, **params):
+        """Adds one material (alternative to a parsed .dat file)."""
+        text = "\n".join(f"{k} = {v}" for k, v in params.items())
+        _capi.check(_capi.lib().akb_model_add_material(self._h, type.encode(), text.encode()))
+        self._materials_added = True
+
+    def setElementMaterials(self, material_of_element):
+        self._mat = np.ascontiguousarray(material_of_element, dtype=np.int32)
+        _capi.check(_capi.lib().akb_model_set_element_materials(self._h, _capi.ptr(self._mat)))
+
+    def setQuadratureRule(self, rule):
+        """0: the reference's default order; 1: the 6-point rule of _triangle_6."""
+        _capi.check(_capi.lib().akb_model_set_quadrature_rule(self._h, rule))
+
+    def initFull(self, _analysis_method=_explicit_lumped_mass, precision="fp64"):
+        if _analysis_method != _explicit_lumped_mass:
+            raise _capi.AkbError(8, "only _explicit_lumped_mass is provided")
+        L = _capi.lib()
+        if not self._materials_added:
+            for text in _static_parser.texts:
+                _capi.check(L.akb_model_load_materials(self._h, text.encode()))
+        prec = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}[precision]
+        _capi.check(L.akb_model_init_full(self._h, _capi.EXPLICIT_LUMPED_MASS, prec))
+        self._initialized = True
+        self.precision = precision
+
+    # -- nodal arrays ----------------------------------------------------------------
+    def _get(self, name):
+        a = self._mirrors.get(name)
+        if a is None:
+            shape = (self.mesh.getNbNodes(), self.dim)
+            a = np.zeros(shape, dtype=np.bool_ if name == "blocked_dofs" else np.float64)
+            view = a.view(np.uint8) if name == "blocked_dofs" else a
+            _capi.check(_capi.lib().akb_model_get_nodal(self._h, _FIELDS[name], _capi.ptr(view),
+                                                        view.nbytes))
+            self._mirrors[name] = a
+        if name in _WRITABLE:
+            self._handed_out.add(name)
+        return a
+
+    def _sync_up(self):
+        """Uploads the host arrays handed out since the last step."""
+        L = _capi.lib()
+        for name in list(self._handed_out):
+            a = self._mirrors[name]
+            view = np.ascontiguousarray(a).view(np.uint8) if name == "blocked_dofs" else \
+                np.ascontiguousarray(a, dtype=np.float64)
+            _capi.check(L.akb_model_set_nodal(self._h, _FIELDS[name], _capi.ptr(view), view.nbytes))
+        self._handed_out.clear()
+
+    def _invalidate(self, names=None):
+        if names is None:
+            self._mirrors.clear()
+        else:
+            for n in names:
+                self._mirrors.pop(n, None)
+
+    def getDisplacement(self):
+        return self._get("displacement")
+
+    def getVelocity(self):
+        return self._get("velocity")
+
+    def getAcceleration(self):
+        return self._get("acceleration")
+
+    def getExternalForce(self):
+        return self._get("external_force")
+
+    def getInternalForce(self):
+        self._sync_up()
+        return self._get("internal_force")
+
+    def getMass(self):
+        return self._get("mass")
+
+    def getBlockedDOFs(self):
+        return self._get("blocked_dofs")
+
+    def getCurrentPosition(self):
+        self._sync_up()
+        self._invalidate(["current_position"])
+        return self._get("current_position")
+
+    def setNodal(self, name, values):
+        """Direct upload of a whole nodal array."""
+        self._sync_up()
+        a = np.ascontiguousarray(values, dtype=np.uint8 if name == "blocked_dofs" else np.float64)
+        _capi.check(_capi.lib().akb_model_set_nodal(self._h, _FIELDS[name], _capi.ptr(a), a.nbytes))
+        self._invalidate([name, "current_position"])
+
+    def applyBC(self, bc, group):
+        """applyBC(FixedValue(v, axis), group): blocks the axis of the group's
+        nodes and sets their displacement (boundary_condition_tmpl.hh)."""
+        nodes = self.mesh.getNodeGroup(group) if isinstance(group, str) else np.asarray(group)
+        if not isinstance(bc, FixedValue):
+            raise TypeError("only BC::Dirichlet::FixedValue is provided")
+        self.getBlockedDOFs()[nodes, bc.axis] = True
+        self.getDisplacement()[nodes, bc.axis] = bc.value
+
+    # -- time stepping -----------------------------------------------------------------
+    def getStableTimeStep(self):
+        self._sync_up()
+        dt = ctypes.c_double()
+        _capi.check(_capi.lib().akb_model_get_stable_time_step(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def setTimeStep(self, dt, solver_id=""):
+        _capi.check(_capi.lib().akb_model_set_time_step(self._h, float(dt)))
+
+    def getTimeStep(self, solver_id=""):
+        dt = ctypes.c_double()
+        _capi.check(_capi.lib().akb_model_get_time_step(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def solveStep(self, nsteps=1):
+        """ModelSolver::solveStep; nsteps > 1 enqueues several steps at once."""
+        self._sync_up()
+        _capi.check(_capi.lib().akb_model_solve_step(self._h, int(nsteps)))
+        self._invalidate()
+
+    def timeSteps(self, nsteps):
+        """Runs nsteps steps between two CUDA events on the model's stream;
+        returns the device time in milliseconds."""
+        self._sync_up()
+        ms = ctypes.c_double()
+        _capi.check(_capi.lib().akb_model_time_steps(self._h, int(nsteps), ctypes.byref(ms)))
+        self._invalidate()
+        return ms.value
+
+    def profileSteps(self, nsteps):
+        """Like timeSteps with events between phases; returns (total_ms,
+        [predictor_ms, element_forces_ms, node_update_ms]) summed over steps."""
+        self._sync_up()
+        total = ctypes.c_double()
+        phases = (ctypes.c_double * 3)()
+        _capi.check(_capi.lib().akb_model_profile_steps(self._h, int(nsteps), ctypes.byref(total),
+                                                        phases))
+        self._invalidate()
+        return total.value, list(phases)
+
+    def synchronize(self):
+        _capi.check(_capi.lib().akb_model_synchronize(self._h))
+
+    def assembleInternalForces(self):
+        self._sync_up()
+        _capi.check(_capi.lib().akb_model_assemble_internal_forces(self._h))
+        self._invalidate(["internal_force"])
+
+    def getEnergy(self, energy_id):
+        self._sync_up()
+        v = ctypes.c_double()
+        _capi.check(_capi.lib().akb_model_get_energy(self._h, energy_id.encode(), ctypes.byref(v)))
+        return v.value
+
+    def getStatus(self):
+        f = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_status(self._h, ctypes.byref(f)))
+        return f.value
+
+    def getFEData(self):
+        """(dN/dx [E, nq, n, dim], det J * w [E, nq]) in user element order."""
+        L = _capi.lib()
+        nq = ctypes.c_int()
+        _capi.check(L.akb_model_nb_quadrature_points(self._h, ctypes.byref(nq)))
+        E, n = self.mesh.getNbElement(), self.mesh.connectivity.shape[1]
+        B = np.zeros((E, nq.value, n, self.dim))
+        j = np.zeros((E, nq.value))
+        _capi.check(L.akb_model_get_fe_data(self._h, 0, _capi.ptr(B), B.size))
+        _capi.check(L.akb_model_get_fe_data(self._h, 1, _capi.ptr(j), j.size))
+        return B, j
+
+    # -- materials ------------------------------------------------------------------
+    def getNbMaterials(self):
+        c = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_nb_materials(self._h, ctypes.byref(c)))
+        return c.value
+
+    def getMaterial(self, which=0):
+        if isinstance(which, str):
+            for i in range(self.getNbMaterials()):
+                if Material(self, i).getName() == which:
+                    return Material(self, i)
+            raise _capi.AkbError(10, f"no material named '{which}'")
+        return Material(self, which)
+
+    def getSpatialDimension(self):
+        return self.dim

@@ -1,0 +1,373 @@
+"""Benchmark of the explicit solid-dynamics step (element-steps/s).
+
+Workload (default): the single-large-mesh configuration -- a 128 x 128 x 128
+structured _hexahedron_8 box (2,097,152 elements, 2,146,689 nodes, 8 Gauss
+points), neohookean (rho = 1, E = 1, nu = 0.3), z = 0 face blocked, seeded
+Gaussian random initial velocity (correlation length 0.1, std 0.02),
+dt = 0.8 x stable.  One step = one central-difference step of the whole mesh.
+
+  value      device time (CUDA events on the model's stream) of K steps of the
+             mixed-precision path (FP32 element math, FP64 state); inputs are
+             resident in HBM and far larger than L2 (no flush needed)
+  fp64       the same for the plain FP64 path
+  e2e        through the C ABI with host buffers: every step uploads the
+             external force from pinned memory, runs the step and reads the
+             displacement back (wall clock, synchronised)
+  roofline   element-force kernel: algorithmic bytes / its event-timed duration
+  cpu_baseline  the CPU oracle (restatement of the reference path) on the host
+             cores, bounded sample of the same workload
+
+--impl reference times the reference's CPU algorithm (the oracle: the
+reference cannot be built here) on all host threads and prints its line.
+N > 1 (torchrun): independent replicas, one mesh per GPU, weak scaling.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "element-steps/s"
+UNIT = "element-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="hex8", choices=["hex8", "tet", "tri6"])
+    p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--precisions", default="mixed,fp64")
+    return p.parse_args()
+
+
+# ---- workloads ---------------------------------------------------------------------
+def workload(config, cells):
+    import akantu2_b200 as akb
+    if config == "hex8":
+        n = cells or 128
+        mesh = akb.box_hex8(n)
+        mat = dict(type="neohookean", rho=1.0, E=1.0, nu=0.3)
+        desc = f"hex8 neohookean {n}^3 box"
+    elif config == "tet":
+        n = cells or 20
+        mesh = akb.box_tet4(n)
+        mat = dict(type="elastic", rho=1.0, E=1.0, nu=0.3)
+        desc = f"tet4 elastic {n}^3 x 6 cube"
+    else:
+        n = cells or 512
+        mesh = akb.square_tri6(n)
+        mat = dict(type="plastic_linear_isotropic_hardening", rho=1.0, E=1.0, nu=0.3,
+                   sigma_y=1e-3, h=0.1)
+        desc = f"tri6 plastic {n}^2 x 2 square"
+    return mesh, mat, desc
+
+
+def initial_state(config, mesh):
+    from akantu2_b200 import gaussian_random_field
+    x = mesh.nodes
+    blocked = np.zeros(x.shape, dtype=np.uint8)
+    if config == "tri6":
+        blocked[np.isclose(x[:, 0], 0.0)] = 1
+        v0 = np.zeros_like(x)
+        v0[:, 0] = 1e-3 * x[:, 0]
+    else:
+        blocked[np.isclose(x[:, 2], 0.0)] = 1
+        if config == "hex8":
+            v0 = gaussian_random_field(x, seed=2024, corr_length=0.1, std=0.02)
+        else:
+            v0 = np.zeros_like(x)
+            v0[:, 2] = 0.01 * np.sin(np.pi * x[:, 0]) * np.sin(np.pi * x[:, 1]) * x[:, 2]
+    return v0, blocked
+
+
+# algorithmic bytes (formula of the specification, per element-step), and the
+# element-force kernel's own share
+def algorithmic_bytes(config, mesh, precision):
+    E, N = mesh.getNbElement(), mesh.getNbNodes()
+    n = mesh.connectivity.shape[1]
+    d = mesh.spatial_dimension
+    Q = {"hex8": 8, "tet": 1, "tri6": 3}[config]
+    s_e = 8 if precision == "fp64" else 4
+    S = (3 * d * d + 1) * 8 if config == "tri6" else 0
+    elem = E * (4 * n + Q * (d * n + 1) * s_e + 2 * Q * S)
+    nodal = N * (64 * d + 9)
+    step = elem + nodal
+    kernel = elem + N * 8 * d  # the element kernel also gathers u
+    return step, kernel
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(config, precision):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(f"{config}_{precision}")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        except Exception:
+            return None
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---- CPU legs --------------------------------------------------------------------------
+def cpu_rate(config, mesh, mat, v0, blocked, budget_s, max_steps, threads):
+    """Element-steps/s of the oracle on `threads` host threads."""
+    from oracle import oracle as orc
+    otype = {"hex8": orc.HEX8, "tet": orc.TET4, "tri6": orc.TRI6}[config]
+    o = orc.OracleModel(otype, mesh.nodes, mesh.connectivity, [mat], threads=threads)
+    o.set(orc.V, v0)
+    o.set(orc.BLOCKED, blocked)
+    o.set_dt(0.8 * o.stable_dt())
+    o.step(1)  # warm
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps:
+        o.step(1)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return mesh.getNbElement() * steps / dt, steps, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    mesh, mat, desc = workload(args.config, args.cells)
+    v0, blocked = initial_state(args.config, mesh)
+    # each timed step is one full step of the workload; the count is bounded
+    # so that the whole run stays within a few minutes
+    rate, steps, secs = cpu_rate(args.config, mesh, mat, v0, blocked, budget_s=60.0,
+                                 max_steps=max(1, args.steps), threads=threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": steps, "warmup": 1,
+        "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "elements": mesh.getNbElement(),
+                   "nodes": mesh.getNbNodes(), "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} full steps of the {desc} (oracle restatement; "
+                                   "the reference cannot be built without Eigen/Boost)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU leg ----------------------------------------------------------------------------
+def run_ours(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    import akantu2_b200 as akb
+    from akantu2_b200 import _capi
+    _capi.check(_capi.lib().akb_set_device(local))
+
+    mesh, mat, desc = workload(args.config, args.cells)
+    v0, blocked = initial_state(args.config, mesh)
+    E = mesh.getNbElement()
+    results = {}
+    precisions = [p for p in args.precisions.split(",") if p]
+
+    def barrier():
+        if dist is not None:
+            import torch
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for prec in precisions:
+        m = akb.SolidMechanicsModel(mesh)
+        m.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+        m.initFull(akb._explicit_lumped_mass, precision=prec)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", blocked)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.timeSteps(max(3, args.warmup))
+        barrier()
+        with ClockSampler(local) as clk:
+            ms = m.timeSteps(args.steps)
+        barrier()
+        ms = max_over_ranks(ms)
+        nprof = min(args.steps, 20)
+        tot, phases = m.profileSteps(nprof)
+        step_b, kern_b = algorithmic_bytes(args.config, mesh, prec)
+        elem_ms = phases[1] / nprof
+        peak, peak_kind = read_peaks()
+        results[prec] = {
+            "ms_per_step": ms / args.steps,
+            "value": world * E * args.steps / (ms / 1e3),
+            "phase_ms_per_step": {"predictor": phases[0] / nprof,
+                                  "element_forces": phases[1] / nprof,
+                                  "node_update": phases[2] / nprof},
+            "roofline": {"bound": "hbm", "kernel": "k_element_forces",
+                         "achieved": kern_b / (elem_ms / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": kern_b / (elem_ms / 1e3) / 1e9 / peak,
+                         "traffic": read_traffic(args.config, prec),
+                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "roofline_step": {"bytes_per_element_step": step_b / E,
+                              "achieved": step_b / (ms / args.steps / 1e3) / 1e9,
+                              "frac": step_b / (ms / args.steps / 1e3) / 1e9 / peak},
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps * 3,
+        }
+        if prec == precisions[0]:
+            # end to end through the C ABI with host buffers
+            from akantu2_b200._capi import PinnedArray
+            L = _capi.lib()
+            fext = PinnedArray(mesh.nodes.shape)
+            fext.array[:] = 0.0
+            uout = PinnedArray(mesh.nodes.shape)
+            nb = fext.array.nbytes
+            k_e2e = max(1, min(args.steps, 100))
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(k_e2e):
+                _capi.check(L.akb_model_set_nodal(m._h, _capi.EXTERNAL_FORCE, _capi.ptr(fext.array), nb))
+                _capi.check(L.akb_model_solve_step(m._h, 1))
+                _capi.check(L.akb_model_get_nodal(m._h, _capi.DISPLACEMENT, _capi.ptr(uout.array), nb))
+            secs = max_over_ranks(time.perf_counter() - t0)
+            results[prec]["e2e"] = {"value": world * E * k_e2e / secs, "unit": UNIT,
+                                    "steps": k_e2e, "h2d_bytes_per_step": nb,
+                                    "d2h_bytes_per_step": nb}
+        del m
+    head = results[precisions[0]]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, steps, secs = cpu_rate(args.config, mesh, mat, v0, blocked, budget_s=20.0,
+                                     max_steps=50, threads=threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{steps} steps of the full {desc} in {secs:.1f} s "
+                         f"(CPU oracle, {threads} threads)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 element math / f64 state" if precisions[0] == "mixed" else "f64",
+            "data": "synthetic (seeded random-field initial velocity)",
+            "config": {"workload": desc, "elements": E, "nodes": mesh.getNbNodes(),
+                       "quadrature_points": {"hex8": 8, "tet": 1, "tri6": 3}[args.config],
+                       "precision": precisions[0], "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (no flush)"},
+            "e2e": head.get("e2e"), "roofline": head["roofline"],
+            "roofline_step": head["roofline_step"], "clocks": head["clocks"],
+            "gpu_launches": head["gpu_launches"],
+            "phase_ms_per_step": head["phase_ms_per_step"],
+            "cpu_baseline": cpu,
+        }
+        for prec in precisions[1:]:
+            r = results[prec]
+            line[prec] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                          "roofline": r["roofline"], "roofline_step": r["roofline_step"],
+                          "phase_ms_per_step": r["phase_ms_per_step"]}
+        if "fp64" in results and precisions[0] != "fp64":
+            line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,195 @@
+/*
+ * akb_capi.h -- C ABI of the B200 explicit solid-dynamics step.
+ *
+ * This is the drop-in boundary for the explicit, lumped-mass, central-
+ * difference time step of Akantu's SolidMechanicsModel.  Every entry point is
+ * `extern "C"`, takes plain pointers and sizes, and returns an int status
+ * (AKB_OK == 0).  On error, akb_last_error() returns a thread-local message.
+ *
+ * Each function names the reference interface it replaces (paths relative to
+ * the Akantu source tree).  Host buffers are owned by the caller, device
+ * memory by the library.  One model belongs to one host thread and one CUDA
+ * stream; different models may be driven from different threads.  There is
+ * no CPU fallback: without a usable CUDA device every compute entry point
+ * fails with AKB_ECUDA.
+ */
+#ifndef AKB_CAPI_H_
+#define AKB_CAPI_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define AKB_OK 0
+#define AKB_EINVAL 1       /* bad argument (size, index, enum)                 */
+#define AKB_ENOMEM 2       /* device or host allocation failed                 */
+#define AKB_ECUDA 3        /* CUDA runtime error / no device                   */
+#define AKB_ENEGJAC 4      /* negative Jacobian at initialisation              */
+#define AKB_ENAN 5         /* non-finite value detected on the device          */
+#define AKB_EPARSE 6       /* .dat or .msh syntax error                        */
+#define AKB_ESTATE 7       /* call out of order (e.g. step before init)        */
+#define AKB_EUNSUPPORTED 8 /* option the explicit path does not provide        */
+#define AKB_EIO 9          /* file could not be read                           */
+#define AKB_EMATERIAL 10   /* unknown material type / name                     */
+
+/* ---- enumerations ------------------------------------------------------- */
+/* element types, src/common/aka_element_classes_info.hh (_tetrahedron_4 ...) */
+enum akb_element_type {
+  AKB_TETRAHEDRON_4 = 0,
+  AKB_HEXAHEDRON_8 = 1,
+  AKB_TRIANGLE_6 = 2
+};
+
+/* src/model/model_solver.hh AnalysisMethod: only _explicit_lumped_mass */
+enum akb_analysis_method { AKB_EXPLICIT_LUMPED_MASS = 0 };
+
+/* arithmetic of the element kernels; nodal state is FP64 in both */
+enum akb_precision {
+  AKB_PRECISION_FP64 = 0,  /* plain FP64, same operation order as the CPU path */
+  AKB_PRECISION_MIXED = 1  /* FP32 element math, FP64 nodal state + gather   */
+};
+
+/* nodal arrays, src/model/solid_mechanics/solid_mechanics_model.hh:270-321 */
+enum akb_nodal_field {
+  AKB_DISPLACEMENT = 0,     /* double [N][dim] getDisplacement()             */
+  AKB_VELOCITY = 1,         /* double [N][dim] getVelocity()                 */
+  AKB_ACCELERATION = 2,     /* double [N][dim] getAcceleration()             */
+  AKB_EXTERNAL_FORCE = 3,   /* double [N][dim] getExternalForce()            */
+  AKB_INTERNAL_FORCE = 4,   /* double [N][dim] getInternalForce() (read only)*/
+  AKB_MASS = 5,             /* double [N][dim] getMass()         (read only) */
+  AKB_BLOCKED_DOFS = 6,     /* uint8  [N][dim] getBlockedDOFs()              */
+  AKB_CURRENT_POSITION = 7  /* double [N][dim] getCurrentPosition() (r/o)    */
+};
+
+/* quadrature-point internals of one material, material-local element order,
+ * src/model/solid_mechanics/material.hh getStress / getGradU / getInternal */
+enum akb_qp_field {
+  AKB_GRAD_U = 0,               /* [nq_m][dim*dim] column-major               */
+  AKB_STRESS = 1,               /* [nq_m][dim*dim] Cauchy (small strain)      */
+  AKB_PIOLA_KIRCHHOFF_2 = 2,    /* [nq_m][dim*dim] neohookean                 */
+  AKB_INELASTIC_STRAIN = 3,     /* [nq_m][dim*dim] plastic                    */
+  AKB_ISO_HARDENING = 4,        /* [nq_m]          plastic                    */
+  AKB_PLASTIC_ENERGY = 5        /* [nq_m]          plastic, cumulative        */
+};
+
+/* ---- library ------------------------------------------------------------ */
+/* thread-local description of the last failed call on this thread */
+const char *akb_last_error(void);
+/* library version, e.g. 100 for 0.1.0 */
+int akb_version(void);
+/* number of CUDA devices visible to the library */
+int akb_device_count(int *count);
+
+/* selects the CUDA device used by models created afterwards on this thread */
+int akb_set_device(int device);
+/* page-locked host buffers, for host <-> device copies at full PCIe rate */
+int akb_host_alloc(size_t bytes, void **ptr);
+int akb_host_free(void *ptr);
+
+/* ---- mesh input (src/io/mesh_io/mesh_io_msh.cc, gmsh 2.x ASCII) ---------- */
+typedef struct akb_mesh akb_mesh;
+/* reads the nodes and the elements of `element_type` from a .msh file
+ * (Mesh::read, src/mesh/mesh.hh:121); node order is the file's, elements are
+ * numbered in order of appearance; physical tags are kept per element */
+int akb_mesh_read_msh(const char *path, int spatial_dimension, int element_type,
+                      akb_mesh **mesh);
+int akb_mesh_sizes(const akb_mesh *mesh, int64_t *nb_nodes, int64_t *nb_elements,
+                   int *nodes_per_element);
+/* copies nodes [N][dim], connectivity [E][n] and physical tag [E] */
+int akb_mesh_copy(const akb_mesh *mesh, double *nodes, int32_t *connectivity,
+                  int32_t *physical_tag);
+void akb_mesh_free(akb_mesh *mesh);
+
+/* ---- model --------------------------------------------------------------- */
+typedef struct akb_model akb_model;
+
+/* SolidMechanicsModel(Mesh &, Int dim)  solid_mechanics_model.hh:61-64.
+ * nodes [N][dim] double, connectivity [E][n] int32 (reference node order) */
+int akb_model_create(int spatial_dimension, int element_type, const double *nodes,
+                     int64_t nb_nodes, const int32_t *connectivity,
+                     int64_t nb_elements, akb_model **model);
+int akb_model_destroy(akb_model *model);
+
+/* material sections of a .dat text (getStaticParser().parse(file),
+ * src/io/parser/parser.hh:344-432); types: elastic, neohookean,
+ * plastic_linear_isotropic_hardening.  Materials are appended in file order. */
+int akb_model_load_materials(akb_model *model, const char *dat_text);
+/* one material, params as "name = value" pairs separated by newlines or ';' */
+int akb_model_add_material(akb_model *model, const char *type, const char *params);
+/* element -> material index (ConstitutiveLawSelector, default all 0) */
+int akb_model_set_element_materials(akb_model *model, const int32_t *material_of_element);
+/* quadrature rule of _triangle_6: 0 = reference default (3 points), 1 = 6 points */
+int akb_model_set_quadrature_rule(akb_model *model, int rule);
+
+/* Model::initFull(_analysis_method = _explicit_lumped_mass)
+ * src/model/model.hh:74-131, solid_mechanics_model.cc:123-232.
+ * Precomputes dN/dx and det J w (AKB_ENEGJAC on an inverted element,
+ * integrator_gauss_inline_impl.hh:176-195) and assembles the lumped mass. */
+int akb_model_init_full(akb_model *model, int analysis_method, int precision);
+
+int akb_model_nb_materials(const akb_model *model, int *count);
+/* Material::getParam / get("E"), returns the parsed or derived value
+ * (rho, E, nu, lambda, mu, sigma_y, h, alpha, delta_T) */
+int akb_model_get_material_param(const akb_model *model, int material, const char *name,
+                                 double *value);
+int akb_model_get_material_name(const akb_model *model, int material, char *buffer,
+                                size_t size);
+
+/* precomputed element data in user element order
+ * (ShapeLagrange::getShapesDerivatives, shape_lagrange.hh, and
+ * IntegratorGauss::getJacobians, integrator_gauss.hh):
+ * which 0: dN/dx  [E][nq][n][dim] (dN_a/dx_j at a*dim + j), which 1: det J * w [E][nq] */
+int akb_model_get_fe_data(akb_model *model, int which, double *host, int64_t count);
+/* number of quadrature points per element */
+int akb_model_nb_quadrature_points(const akb_model *model, int *nq);
+
+/* SolidMechanicsModel::getStableTimeStep  solid_mechanics_model.cc:423-473 */
+int akb_model_get_stable_time_step(akb_model *model, double *dt);
+/* Model::setTimeStep / getTimeStep */
+int akb_model_set_time_step(akb_model *model, double dt);
+int akb_model_get_time_step(const akb_model *model, double *dt);
+
+/* host <-> device copies of a nodal array (the getters of
+ * solid_mechanics_model.hh:270-321 return the same arrays by reference);
+ * nbytes must be N*dim*sizeof(double), or N*dim for AKB_BLOCKED_DOFS */
+int akb_model_set_nodal(akb_model *model, int field, const void *host, int64_t nbytes);
+int akb_model_get_nodal(akb_model *model, int field, void *host, int64_t nbytes);
+/* device address of a nodal array, for callers that keep data on the GPU */
+int akb_model_nodal_device_pointer(akb_model *model, int field, void **device_ptr);
+
+/* Material::getStress/getGradU/getInternal<Real>(id)(type): count is the
+ * number of doubles (akb_model_qp_field_size) */
+int akb_model_qp_field_size(akb_model *model, int field, int material, int64_t *count);
+int akb_model_get_qp_field(akb_model *model, int field, int material, double *host,
+                           int64_t count);
+
+/* ModelSolver::solveStep  model_solver.cc:267-280: enqueues nsteps explicit
+ * steps on the model's stream (asynchronous; getters synchronise) */
+int akb_model_solve_step(akb_model *model, int64_t nsteps);
+int akb_model_synchronize(akb_model *model);
+/* SolidMechanicsModel::assembleInternalForces  solid_mechanics_model.cc:333-370 */
+int akb_model_assemble_internal_forces(akb_model *model);
+/* SolidMechanicsModel::getEnergy("kinetic" | "potential" | "external work" |
+ * "plastic")  solid_mechanics_model.cc:601-621 */
+int akb_model_get_energy(akb_model *model, const char *energy_id, double *value);
+/* timing on the device: enqueues nsteps steps between two CUDA events
+ * recorded on the model's stream and returns the elapsed milliseconds */
+int akb_model_time_steps(akb_model *model, int64_t nsteps, double *elapsed_ms);
+/* the same with an event between the phases of every step; phase_ms[0..2]
+ * receive the summed durations of predictor, element forces (all materials)
+ * and node update (gather + corrector); nsteps <= 4096 */
+int akb_model_profile_steps(akb_model *model, int64_t nsteps, double *total_ms,
+                            double *phase_ms);
+/* device status word: bit 0 = non-finite acceleration seen since the last
+ * call (the flag is cleared by reading it) */
+int akb_model_get_status(akb_model *model, int *flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AKB_CAPI_H_ */

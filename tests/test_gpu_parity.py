@@ -1,0 +1,319 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+The FP64 kernels are compiled without contraction and follow the oracle's
+operation order, so elastic and plastic runs are expected to be bit-identical;
+the neohookean law calls log(), whose last bit may differ between the CUDA
+and glibc implementations, so those runs are held to the 1e-12 relative bar
+of the specification (max |gpu - cpu| / max |cpu| over each nodal array).
+"""
+import numpy as np
+import pytest
+
+import akantu2_b200 as akb
+from oracle import oracle as orc
+from scenarios import (OR_TYPE, STEEL_PLANE_STRAIN, STEEL_PLANE_STRESS, UNIT_ELASTIC,
+                       UNIT_NEOHOOKEAN, UNIT_PLASTIC, blocked_face, golden, oracle_model,
+                       random_field_velocity, sinusoidal_velocity)
+from test_oracle_golden import _patch_mesh, check_patch_results, run_patch_test
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+NODAL = [("displacement", orc.U), ("velocity", orc.V), ("acceleration", orc.A),
+         ("internal_force", orc.FINT)]
+
+
+def rel_err(a, b):
+    scale = np.max(np.abs(b))
+    return np.max(np.abs(a - b)) / scale if scale > 0 else np.max(np.abs(a - b))
+
+
+def gpu_model(mesh, materials, mat_of_elem=None, precision="fp64", qp_rule=0):
+    m = akb.SolidMechanicsModel(mesh)
+    for mat in materials:
+        params = {k: v for k, v in mat.items() if k != "type"}
+        m.addMaterial(mat["type"], **params)
+    if mat_of_elem is not None:
+        m.setElementMaterials(mat_of_elem)
+    if qp_rule:
+        m.setQuadratureRule(qp_rule)
+    m.initFull(akb._explicit_lumped_mass, precision=precision)
+    return m
+
+
+def setup_pair(mesh, materials, v0, blocked, mat_of_elem=None, qp_rule=0, precision="fp64",
+               dt_factor=0.8):
+    g = gpu_model(mesh, materials, mat_of_elem, precision, qp_rule)
+    o = oracle_model(mesh, materials, mat_of_elem, qp_rule)
+    g.setNodal("velocity", v0)
+    g.setNodal("blocked_dofs", blocked)
+    o.set(orc.V, v0)
+    o.set(orc.BLOCKED, blocked)
+    dt_g, dt_o = g.getStableTimeStep(), o.stable_dt()
+    assert dt_g == dt_o
+    g.setTimeStep(dt_factor * dt_g)
+    o.set_dt(dt_factor * dt_o)
+    return g, o
+
+
+def compare(g, o, exact, tol=REL):
+    errs = {}
+    for name, fid in NODAL:
+        a, b = getattr(g, "get" + "".join(w.capitalize() for w in name.split("_")))(), o.get(fid)
+        if exact:
+            assert np.array_equal(a, b), f"{name} differs: rel {rel_err(a, b):.3e}"
+        errs[name] = rel_err(a, b)
+        assert errs[name] <= tol, f"{name}: {errs[name]:.3e}"
+    return errs
+
+
+# ---- element data -----------------------------------------------------------------
+@pytest.mark.parametrize("etype", ["_tetrahedron_4", "_hexahedron_8", "_triangle_6"])
+def test_fe_data_bitwise_and_py_engine(etype):
+    gold = golden(f"fe{etype}.npz")
+    mesh = akb.Mesh(gold["nodes"].shape[1], gold["nodes"], gold["conn"], etype)
+    m = gpu_model(mesh, [UNIT_ELASTIC])
+    B, j = m.getFEData()
+    _, Bo, jo, _ = orc.precompute(OR_TYPE[etype], mesh.nodes[mesh.connectivity])
+    assert np.array_equal(B, Bo) and np.array_equal(j, jo)
+    assert np.max(np.abs(B - gold["B"])) < 1e-10 and np.max(np.abs(j - gold["j"])) < 1e-10
+
+
+@pytest.mark.parametrize("etype", ["_tetrahedron_4", "_hexahedron_8", "_triangle_6"])
+def test_mass_and_stable_dt_bitwise(etype):
+    mesh = {"_tetrahedron_4": akb.box_tet4(4), "_hexahedron_8": akb.box_hex8(4),
+            "_triangle_6": akb.square_tri6(5)}[etype]
+    mesh.nodes += 0.01 * np.sin(7 * mesh.nodes)  # distorted, still valid
+    g = gpu_model(mesh, [UNIT_ELASTIC])
+    o = oracle_model(mesh, [UNIT_ELASTIC])
+    assert np.array_equal(g.getMass(), o.get(orc.MASS))
+    assert g.getStableTimeStep() == o.stable_dt()
+
+
+def test_inradius_fixtures_through_stable_dt():
+    for etype in ["_tetrahedron_4", "_hexahedron_8", "_triangle_6"]:
+        gold = golden(f"fe{etype}.npz")
+        mesh = akb.Mesh(gold["nodes"].shape[1], gold["nodes"], gold["conn"], etype)
+        m = gpu_model(mesh, [dict(UNIT_ELASTIC, nu=0.0)])  # celerity 1
+        assert abs(m.getStableTimeStep() - gold["inradius"].min()) < 1e-6
+
+
+# ---- trajectories -------------------------------------------------------------------
+def test_tet4_elastic_bitwise():
+    mesh = akb.box_tet4(5)
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], sinusoidal_velocity(mesh.nodes),
+                      blocked_face(mesh.nodes))
+    g.solveStep(150)
+    o.step(150)
+    compare(g, o, exact=True)
+    for f in (orc.GRAD_U, orc.STRESS):
+        got = g.getMaterial(0).getGradU() if f == orc.GRAD_U else g.getMaterial(0).getStress()
+        assert np.array_equal(got, o.qp(0, f))
+
+
+def test_hex8_neohookean_parity():
+    mesh = akb.box_hex8(6)
+    v0 = random_field_velocity(mesh.nodes, seed=7, corr_length=0.3, std=0.05)
+    g, o = setup_pair(mesh, [UNIT_NEOHOOKEAN], v0, blocked_face(mesh.nodes))
+    g.solveStep(150)
+    o.step(150)
+    compare(g, o, exact=False)
+    assert rel_err(g.getMaterial(0).getInternal("piola_kirchhoff_2")(), o.qp(0, orc.PK2)) < REL
+    assert rel_err(g.getMaterial(0).getGradU(), o.qp(0, orc.GRAD_U)) < REL
+
+
+def test_hex8_elastic_bitwise():
+    mesh = akb.box_hex8(5)
+    v0 = random_field_velocity(mesh.nodes, seed=3)
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], v0, blocked_face(mesh.nodes))
+    g.solveStep(100)
+    o.step(100)
+    compare(g, o, exact=True)
+
+
+@pytest.mark.parametrize("qp_rule", [0, 1])
+def test_tri6_plastic_ramp_bitwise(qp_rule):
+    """Left edge blocked, right edge pulled with a velocity ramp written
+    into the displacement before every step (the imposed-motion loop of
+    test_solid_mechanics_model_dynamics.cc:243-244)."""
+    mesh = akb.square_tri6(6)
+    x = mesh.nodes
+    left, right = np.isclose(x[:, 0], 0.0), np.isclose(x[:, 0], 1.0)
+    blocked = np.zeros(x.shape, dtype=np.uint8)
+    blocked[left] = 1
+    blocked[right, 0] = 1
+    mat = dict(UNIT_PLASTIC, sigma_y=2e-3)
+    g, o = setup_pair(mesh, [mat], np.zeros_like(x), blocked, qp_rule=qp_rule)
+    nsteps, target = 120, 2e-2
+    u = np.zeros_like(x)
+    for s in range(nsteps):
+        u = o.get(orc.U)
+        u[right, 0] = target * min(1.0, (s + 1) / nsteps)
+        o.set(orc.U, u)
+        g.setNodal("displacement", u)
+        g.solveStep()
+        o.step()
+    compare(g, o, exact=True)
+    mg, eps = g.getMaterial(0), o.qp(0, orc.EPS_P)
+    assert np.max(np.abs(eps)) > 0, "the ramp must reach the yield stress"
+    assert np.array_equal(mg.getInternal("inelastic_strain")(), eps)
+    assert np.array_equal(mg.getInternal("iso_hardening")(), o.qp(0, orc.ISO))
+    assert np.array_equal(mg.getStress(), o.qp(0, orc.STRESS))
+    assert np.array_equal(mg.getInternal("plastic_energy")(), o.qp(0, orc.PLASTIC_ENERGY))
+
+
+def test_multi_material_hex8():
+    mesh = akb.box_hex8(4)
+    centers = mesh.nodes[mesh.connectivity].mean(axis=1)
+    mat_of_elem = (centers[:, 0] > 0.5).astype(np.int32)  # elements interleaved by x
+    mats = [dict(UNIT_ELASTIC, name="soft", E=0.5), dict(UNIT_ELASTIC, name="stiff", E=2.0)]
+    v0 = random_field_velocity(mesh.nodes, seed=11)
+    g, o = setup_pair(mesh, mats, v0, blocked_face(mesh.nodes), mat_of_elem=mat_of_elem)
+    g.solveStep(80)
+    o.step(80)
+    compare(g, o, exact=True)
+    for k in range(2):
+        assert np.array_equal(g.getMaterial(k).getStress(), o.qp(k, orc.STRESS))
+
+
+def test_energies_match_oracle():
+    mesh = akb.box_tet4(4)
+    f_ext = np.zeros_like(mesh.nodes)
+    f_ext[:, 0] = 1e-4
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], sinusoidal_velocity(mesh.nodes),
+                      blocked_face(mesh.nodes))
+    g.setNodal("external_force", f_ext)
+    o.set(orc.FEXT, f_ext)
+    g.solveStep(60)
+    o.step(60)
+    for name, which in [("kinetic", orc.EKIN), ("potential", orc.EPOT),
+                        ("external work", orc.EXT_WORK)]:
+        a, b = g.getEnergy(name), o.energy(which)
+        assert abs(a - b) <= 1e-12 * abs(b), name
+
+
+def test_plastic_energy_matches_oracle():
+    mesh = akb.square_tri6(4)
+    x = mesh.nodes
+    blocked = np.zeros(x.shape, dtype=np.uint8)
+    blocked[np.isclose(x[:, 0], 0.0)] = 1
+    v0 = np.zeros_like(x)
+    v0[:, 0] = 0.02 * x[:, 0]
+    g, o = setup_pair(mesh, [UNIT_PLASTIC], v0, blocked)
+    g.solveStep(80)
+    o.step(80)
+    for name, which in [("plastic", orc.EPLASTIC), ("potential", orc.EPOT)]:
+        a, b = g.getEnergy(name), o.energy(which)
+        assert b != 0 and abs(a - b) <= 1e-12 * abs(b), name
+
+
+@pytest.mark.parametrize("etype,material", [
+    ("_tetrahedron_4", STEEL_PLANE_STRAIN), ("_hexahedron_8", STEEL_PLANE_STRAIN),
+    ("_triangle_6", STEEL_PLANE_STRAIN), ("_triangle_6", STEEL_PLANE_STRESS)])
+def test_gpu_explicit_patch_test(etype, material):
+    mesh, model, blocked, u = run_patch_test(lambda m, mat: gpu_model(m, [mat]), etype, material)
+    model.getBlockedDOFs()[:] = blocked.astype(bool)
+    model.getDisplacement()[:] = u
+    model.setTimeStep(0.8 * model.getStableTimeStep())
+    for _ in range(100):
+        model.solveStep()
+    check_patch_results(mesh, model.getDisplacement(), model.getMaterial(0).getGradU(),
+                        model.getMaterial(0).getStress(), material, model.getInternalForce(),
+                        model.getEnergy("kinetic"))
+
+
+# ---- full-size tet-cube configuration ---------------------------------------------------
+def test_tet_cube_48k_1000_steps():
+    """Unit cube, 20^3 cells x 6 tetrahedra, elastic, z = 0 blocked,
+    v_z = 0.01 sin(pi x) sin(pi y) z, dt = 0.8 stable, 1000 steps."""
+    mesh = akb.box_tet4(20)
+    assert mesh.getNbElement() == 48000 and mesh.getNbNodes() == 9261
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], sinusoidal_velocity(mesh.nodes),
+                      blocked_face(mesh.nodes))
+    g.solveStep(1000)
+    o.step(1000)
+    errs = compare(g, o, exact=True)
+    assert max(errs.values()) == 0.0
+
+
+def test_mixed_precision_error_tet_cube():
+    mesh = akb.box_tet4(12)
+    v0, bl = sinusoidal_velocity(mesh.nodes), blocked_face(mesh.nodes)
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], v0, bl, precision="mixed")
+    g.solveStep(1000)
+    o.step(1000)
+    u, uo = g.getDisplacement(), o.get(orc.U)
+    l2 = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert l2 < 1e-5
+
+
+# ---- edge cases ---------------------------------------------------------------------------
+def test_negative_jacobian_is_reported():
+    mesh = akb.box_tet4(2)
+    c = mesh.connectivity
+    c[3, [1, 2]] = c[3, [2, 1]]  # invert one element
+    with pytest.raises(akb.AkbError) as e:
+        gpu_model(mesh, [UNIT_ELASTIC])
+    assert e.value.name == "AKB_ENEGJAC" and ":3)" in str(e.value)
+
+
+def test_empty_mesh():
+    mesh = akb.Mesh(3, np.zeros((0, 3)), np.zeros((0, 4), np.int32), "_tetrahedron_4")
+    m = gpu_model(mesh, [UNIT_ELASTIC])
+    m.setTimeStep(1e-3)
+    m.solveStep(3)
+    assert m.getDisplacement().shape == (0, 3)
+    assert m.getEnergy("kinetic") == 0.0
+
+
+def test_single_element_and_unconnected_node():
+    nodes = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [5, 5, 5]], dtype=float)
+    conn = np.array([[0, 1, 2, 3]], dtype=np.int32)
+    mesh = akb.Mesh(3, nodes, conn, "_tetrahedron_4")
+    g = gpu_model(mesh, [UNIT_ELASTIC])
+    o = oracle_model(mesh, [UNIT_ELASTIC])
+    assert np.array_equal(g.getMass(), o.get(orc.MASS))
+    v0 = np.zeros((5, 3))
+    v0[1, 0] = 0.1
+    for m in (g,):
+        m.setNodal("velocity", v0)
+    o.set(orc.V, v0)
+    dt = 0.5 * g.getStableTimeStep()
+    g.setTimeStep(dt)
+    o.set_dt(dt)
+    g.solveStep(10)
+    o.step(10)
+    # node 4 has zero mass: its acceleration is r / 0 (non-finite) in both
+    a_g, a_o = g.getAcceleration(), o.get(orc.A)
+    assert np.array_equal(np.isfinite(a_g), np.isfinite(a_o))
+    fin = np.isfinite(a_o)
+    assert np.array_equal(a_g[fin], a_o[fin])
+    assert g.getStatus() & 1
+
+
+def test_nonfinite_state_sets_status():
+    mesh = akb.box_tet4(2)
+    m = gpu_model(mesh, [UNIT_ELASTIC])
+    v0 = np.zeros_like(mesh.nodes)
+    m.setTimeStep(0.5 * m.getStableTimeStep())
+    m.solveStep(2)
+    assert m.getStatus() == 0
+    v0[3, 1] = np.nan
+    m.setNodal("velocity", v0)
+    m.solveStep(2)
+    assert m.getStatus() & 1
+    assert m.getStatus() == 0  # reading clears the flag
+
+
+def test_user_writes_between_steps_keep_reference_semantics():
+    """Elastic grad_u / stress are those of the last force assembly even
+    if the displacement array is written afterwards."""
+    mesh = akb.box_tet4(3)
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], sinusoidal_velocity(mesh.nodes, 0.1),
+                      blocked_face(mesh.nodes))
+    g.solveStep(5)
+    o.step(5)
+    u = g.getDisplacement()
+    u[:] += 0.01
+    ref = o.qp(0, orc.GRAD_U)
+    assert np.array_equal(g.getMaterial(0).getGradU(), ref)

@@ -1,0 +1,261 @@
+"""Pins the CPU oracle against the reference's own fixtures and known-answer
+tests (no GPU needed).
+
+  - FE precomputation vs the reference's independent numpy engine
+    (test/test_fe_engine/test_fe_engine_precomputation.cc, tol 1e-10)
+  - element inradius vs test/test_fe_engine/_<type>.csv (tol 1e-6)
+  - gradient of a linear field (test_gradient.cc, tol 5e-13)
+  - lumped mass sum (test/test_model/patch_tests/test_lumped_mass.cc, tol 2e-15)
+  - explicit linear patch tests (patch_test_linear_elastic_explicit.cc)
+  - elastic and plastic material KATs (test_elastic_materials.cc,
+    test_plastic_materials.cc)
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from scenarios import (OR_TYPE, PATCH_ALPHA, STEEL_LUMPED, STEEL_PLANE_STRAIN,
+                       STEEL_PLANE_STRESS, TYPES, golden, linear_field)
+
+from akantu2_b200.mesh import Mesh, boundary_nodes
+
+
+@pytest.mark.parametrize("etype", TYPES)
+def test_precompute_matches_py_engine(etype):
+    g = golden(f"fe{etype}.npz")
+    Xe = g["nodes"][g["conn"]]
+    N, B, j, rc = orc.precompute(OR_TYPE[etype], Xe)
+    assert rc == 0
+    assert np.max(np.abs(N - g["N"])) < 1e-10
+    assert np.max(np.abs(B - g["B"])) < 1e-10
+    assert np.max(np.abs(j - g["j"])) < 1e-10
+    # and in fact far tighter than the reference's own tolerance
+    scale = np.max(np.abs(g["B"]))
+    assert np.max(np.abs(B - g["B"])) < 1e-12 * scale
+
+
+@pytest.mark.parametrize("etype", TYPES)
+def test_quadrature_matches_py_engine(etype):
+    g = golden(f"fe{etype}.npz")
+    pts, w = orc.quadrature(OR_TYPE[etype])
+    assert np.allclose(pts, g["quad_points"], rtol=0, atol=1e-15)
+    assert np.allclose(w, g["quad_weights"], rtol=0, atol=1e-15)
+
+
+def test_triangle_six_point_rule_integrates_quartics():
+    pts, w = orc.quadrature(orc.TRI6, rule=1)
+    assert len(w) == 6
+    # int over the reference triangle of x^a y^b = a! b! / (a + b + 2)!
+    from math import factorial
+    for a in range(5):
+        for b in range(5 - a):
+            exact = factorial(a) * factorial(b) / factorial(a + b + 2)
+            got = np.sum(w * pts[:, 0] ** a * pts[:, 1] ** b)
+            assert abs(got - exact) < 1e-15
+
+
+@pytest.mark.parametrize("etype", TYPES)
+def test_inradius_matches_reference_csv(etype):
+    g = golden(f"fe{etype}.npz")
+    got = np.array([orc.inradius(OR_TYPE[etype], g["nodes"][c]) for c in g["conn"]])
+    assert np.max(np.abs(got - g["inradius"])) < 1e-6
+
+
+@pytest.mark.parametrize("etype", TYPES)
+def test_gradient_of_linear_field_is_exact(etype):
+    g = golden(f"fe{etype}.npz")
+    nodes, conn = g["nodes"], g["conn"]
+    d = nodes.shape[1]
+    alpha = np.array([[13, 23, 31], [11, 7, 5]], dtype=np.float64)[:, :d]
+    field = nodes @ alpha.T  # two components
+    _, B, _, _ = orc.precompute(OR_TYPE[etype], nodes[conn])
+    ue = field[conn]  # [E, n, 2]
+    grad = np.einsum("ean,eqaj->eqnj", ue, B)
+    assert np.max(np.abs(grad - alpha[None, None])) < 5e-13
+
+
+def _patch_mesh(etype):
+    g = golden(f"patch{etype}.npz")
+    d = g["nodes"].shape[1]
+    return Mesh(d, g["nodes"], g["conn"], etype)
+
+
+@pytest.mark.parametrize("etype", TYPES)
+def test_lumped_mass_sums_to_total_mass(etype):
+    mesh = _patch_mesh(etype)
+    m = orc.OracleModel(OR_TYPE[etype], mesh.nodes, mesh.connectivity, [STEEL_LUMPED])
+    _, _, j, _ = orc.precompute(OR_TYPE[etype], mesh.nodes[mesh.connectivity])
+    total = 7800.0 * j.sum()
+    masses = m.get(orc.MASS)
+    for c in range(masses.shape[1]):
+        assert abs((total - masses[:, c].sum()) / total) < 2e-15
+
+
+def run_patch_test(mk_model, etype, material, nsteps=100):
+    """The explicit linear patch test: static linear field imposed on all
+    nodes, boundary blocked, 100 steps at 0.8 * stable dt
+    (patch_test_linear_elastic_explicit.cc:25-46)."""
+    mesh = _patch_mesh(etype)
+    d = mesh.spatial_dimension
+    model = mk_model(mesh, material)
+    bnodes = boundary_nodes(etype, mesh.connectivity)
+    blocked = np.zeros((mesh.getNbNodes(), d), dtype=np.uint8)
+    blocked[bnodes] = 1
+    u = linear_field(mesh.nodes)
+    return mesh, model, blocked, u
+
+
+def check_patch_results(mesh, u, grad, stress, material, fint, ekin):
+    d = mesh.spatial_dimension
+    # kinetic energy, dofs, gradient and stress tolerances of
+    # patch_test_linear_fixture.hh:163-165 and the explicit test
+    assert abs(ekin) < 1e-16
+    ref_u = linear_field(mesh.nodes)
+    assert np.max(np.abs(u - ref_u)) < 1e-15
+    pgrad = PATCH_ALPHA[:d, 1:1 + d]
+    for row in grad:
+        gmat = row.reshape(d, d, order="F")
+        assert np.max(np.abs(gmat - pgrad)) / np.max(np.abs(gmat)) < 1e-13
+    E, nu = material["E"], material["nu"]
+    strain = 0.5 * (pgrad + pgrad.T)
+    lam = nu * E / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    if material.get("Plane_Stress"):
+        lam = nu * E / (1 - nu * nu)
+    psig = np.eye(d) * lam * np.trace(strain) + 2 * mu * strain
+    for sq in stress:
+        smat = sq.reshape(d, d, order="F")
+        assert np.max(np.abs(smat - psig)) / np.max(np.abs(psig)) < 1e-13
+    # internal forces are self-equilibrated (checkForces, total force part)
+    total = fint.sum(axis=0)
+    assert np.max(np.abs(total)) / np.max(np.abs(fint)) < 1e-9
+
+
+@pytest.mark.parametrize("etype,material", [
+    ("_tetrahedron_4", STEEL_PLANE_STRAIN), ("_hexahedron_8", STEEL_PLANE_STRAIN),
+    ("_triangle_6", STEEL_PLANE_STRAIN), ("_triangle_6", STEEL_PLANE_STRESS)])
+def test_oracle_explicit_patch_test(etype, material):
+    def mk(mesh, mat):
+        return orc.OracleModel(OR_TYPE[etype], mesh.nodes, mesh.connectivity, [mat])
+    mesh, model, blocked, u = run_patch_test(mk, etype, material)
+    model.set(orc.BLOCKED, blocked)
+    model.set(orc.U, u)
+    model.set_dt(0.8 * model.stable_dt())
+    model.step(100)
+    check_patch_results(mesh, model.get(orc.U), model.qp(0, orc.GRAD_U), model.qp(0, orc.STRESS),
+                        material, model.get(orc.FINT), model.energy(orc.EKIN))
+
+
+# ---- material KATs --------------------------------------------------------------
+def _random_rotation(rng, d):
+    q, r = np.linalg.qr(rng.standard_normal((d, d)))
+    q = q * np.sign(np.diag(r))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    return q
+
+
+def _composed_strain(t):
+    dev = np.array([[0., 1., 2.], [1., 0., 3.], [2., 3., 0.]]) * t
+    hyd = np.eye(3) * t
+    return (hyd + dev) * t
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_elastic_3d_kat(seed):
+    # test_elastic_materials.cc:206-245
+    E, nu = 1.0, 0.3
+    K = E / 3. / (1 - 2. * nu)
+    mu = 0.5 * E / (1 + nu)
+    R = _random_rotation(np.random.default_rng(seed), 3)
+    g = _composed_strain(1.)
+    s_rot = orc.elastic_stress(R @ g @ R.T, E, nu)
+    s = R.T @ s_rot @ R
+    strain = 0.5 * (g + g.T)
+    dev = strain - np.trace(strain) / 3. * np.eye(3)
+    expected = 2 * mu * dev + K * np.trace(strain) * np.eye(3)
+    assert np.max(np.abs(s - expected)) < 1e-14
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_elastic_2d_kat(seed):
+    # test_elastic_materials.cc:95-135 (plane strain, sigma_th = 0)
+    E, nu = 1.0, 0.3
+    lam = nu * E / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    R = _random_rotation(np.random.default_rng(seed), 2)
+    g = _composed_strain(1.)[:2, :2]
+    s = R.T @ orc.elastic_stress(R @ g @ R.T, E, nu) @ R
+    strain = 0.5 * (g + g.T)
+    expected = 2 * mu * strain + lam * np.trace(strain) * np.eye(2)
+    err = np.max(np.abs(s - expected)) / np.max(np.abs(expected))
+    assert err < 1e-13
+
+
+def test_elastic_thermal_stress_adds_to_diagonal():
+    s0 = orc.elastic_stress(np.zeros((3, 3)), 1.0, 0.3, sigma_th=2.0)
+    assert np.allclose(s0, 2.0 * np.eye(3), atol=0, rtol=0)
+
+
+def test_plastic_3d_kat():
+    # test_plastic_materials.cc:38-173: E = 1, nu = 0, sigma_y = 1, h = 0
+    E, nu, sy, h = 1., 0., 1., 0.
+    K = E / 3. / (1 - 2. * nu)
+    mu = 0.5 * E / (1 + nu)
+    R = _random_rotation(np.random.default_rng(42), 3)
+    dt = 10. / 100
+    steps = np.arange(100.)
+    prev_g = np.zeros((3, 3)); prev_s = np.zeros((3, 3)); prev_e = np.zeros((3, 3))
+    iso = 0.; prev_iso = 0.
+    for i in steps:  # hydrostatic loading: no plastic flow
+        t = i * dt
+        g = R @ (np.eye(3) * t) @ R.T
+        s, e, iso = orc.plastic_stress(g, prev_g, prev_s, prev_e, iso, prev_iso, E, nu, sy, h)
+        sig = R.T @ s @ R
+        assert np.max(np.abs(sig - t * 3. * K * np.eye(3))) < 1e-13
+        assert np.max(np.abs(e)) < 1e-13
+        prev_g, prev_s, prev_e, prev_iso = g, s, e, iso
+    beta = np.sqrt(42)
+    t_p = sy / 2. / mu / beta
+    prev_sigma = None
+    prev_eps_unrot = np.zeros((3, 3))
+    dev0 = np.array([[0., 1., 2.], [1., 0., 3.], [2., 3., 0.]])
+    for i in steps:  # deviatoric loading: plastic flow
+        t = i * dt
+        gu = dev0 * t
+        g = R @ gu @ R.T
+        s, e, _ = orc.plastic_stress(g, prev_g, prev_s, prev_e, 0., 0., E, nu, sy, h)
+        sig = R.T @ s @ R
+        eps = R.T @ e @ R
+        if t < t_p:
+            assert np.max(np.abs(sig - mu * (gu + gu.T))) < 1e-13
+            assert np.max(np.abs(e)) < 1e-13
+        elif t > t_p + dt:
+            dl = dt / t * np.sum(prev_sigma * (gu + gu.T)) / 2.
+            deps = dl * 3. / 2. / sy * prev_sigma
+            assert np.max(np.abs(eps - (deps + prev_eps_unrot))) < 1e-13
+            dsig = 2. * mu * (0.5 * dt / t * (gu + gu.T) - deps)
+            assert np.max(np.abs(dsig - (sig - prev_sigma))) < 1e-13
+        prev_sigma = sig
+        prev_eps_unrot = eps
+        prev_g, prev_s, prev_e = g, s, e
+
+
+def test_neohookean_reference_state_and_objectivity():
+    # all neohookean tests of the reference are disabled; these are
+    # self-consistency checks of the restated law
+    S0 = orc.neohookean_stress(np.zeros((3, 3)), 1.0, 0.3)
+    assert np.max(np.abs(S0)) < 1e-15
+    rng = np.random.default_rng(3)
+    g = 0.05 * rng.standard_normal((3, 3))
+    F = np.eye(3) + g
+    R = _random_rotation(rng, 3)
+    S1 = orc.neohookean_stress(g, 1.0, 0.3)
+    S2 = orc.neohookean_stress(R @ F - np.eye(3), 1.0, 0.3)  # PK2 is invariant under F -> R F
+    assert np.max(np.abs(S1 - S2)) < 1e-13
+    # small-strain limit: S -> lambda tr(eps) I + 2 mu eps
+    eps = 1e-7 * (g + g.T) / 2
+    S = orc.neohookean_stress(eps, 1.0, 0.3)
+    lam, mu = 0.3 / (1.3 * 0.4), 1 / 2.6
+    lin = lam * np.trace(eps) * np.eye(3) + 2 * mu * eps
+    assert np.max(np.abs(S - lin)) < 1e-12
