@@ -80,14 +80,16 @@ __device__ __forceinline__ void neohookean_pk2(T lambda, T mu, const T *g, T *S)
   for (int j = 0; j < D; ++j)
 #pragma unroll
     for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? T(1) : T(0)) + g[i + D * j];
+  // C is symmetric term by term (same products, same order): fill j >= i
 #pragma unroll
   for (int j = 0; j < D; ++j)
 #pragma unroll
-    for (int i = 0; i < D; ++i) {
+    for (int i = 0; i <= j; ++i) {
       T s = F[0 + D * i] * F[0 + D * j];
 #pragma unroll
       for (int k = 1; k < D; ++k) s = s + F[k + D * i] * F[k + D * j];
       C[i + D * j] = s;
+      C[j + D * i] = s;
     }
   T J;
   if constexpr (D == 3) {
@@ -165,49 +167,62 @@ __device__ __forceinline__ void plastic_update(double lambda, double mu, double 
 }
 
 // r_q(a*D + k) = sum_I (B_L0 + B_L2(grad u))(I, a*D + k) S_voigt(I)
-// (material.cc:547-565, aka_voigthelper_tmpl.hh:99-140,180-235)
+// (material.cc:547-565, aka_voigthelper_tmpl.hh:99-140,180-235).
+// The reference builds the full 6 x 3n matrices; here the entries that are
+// structurally zero are not added (x + 0 == x), every non-zero term keeps its
+// operand order, so the result is the same number.  k must be a compile-time
+// constant after unrolling.
 template <int D, class T>
 __device__ __forceinline__ T finite_force_component(const T *b /* dN_a/dx */, const T *g,
                                                     const T *Sv, int k) {
-  T acc = T(0);
   if constexpr (D == 3) {
-#pragma unroll
-    for (int I = 0; I < 6; ++I) {
-      T bl0 = T(0), bl2;
-      if (I < 3) {
-        if (k == I) bl0 = b[I];
-        bl2 = g[k + 3 * I] * b[I];
-      } else {
-        if (I == 3) { if (k == 1) bl0 = b[2]; else if (k == 2) bl0 = b[1]; }
-        if (I == 4) { if (k == 0) bl0 = b[2]; else if (k == 2) bl0 = b[0]; }
-        if (I == 5) { if (k == 0) bl0 = b[1]; else if (k == 1) bl0 = b[0]; }
-        const int aux = I - 3;
-        bl2 = T(0);
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-          if (m != aux) bl2 += g[k + 3 * m] * b[3 - m - aux];
-      }
-      const T bf = bl0 + bl2;
-      acc = (I == 0) ? bf * Sv[I] : acc + bf * Sv[I];
-    }
-  } else {
+    // rows 0..2: B_L0(I, k) = b_I if k == I; B_L2(I, k) = g(k, I) b_I
+    T bf[6];
 #pragma unroll
     for (int I = 0; I < 3; ++I) {
-      T bl0 = T(0), bl2;
-      if (I < 2) {
-        if (k == I) bl0 = b[I];
-        bl2 = g[k + 2 * I] * b[I];
-      } else {
-        bl0 = (k == 1) ? b[0] : b[1];
-        bl2 = T(0);
-#pragma unroll
-        for (int m = 0; m < 2; ++m) bl2 += g[k + 2 * m] * b[1 - m];
-      }
-      const T bf = bl0 + bl2;
-      acc = (I == 0) ? bf * Sv[I] : acc + bf * Sv[I];
+      const T bl2 = g[k + 3 * I] * b[I];
+      bf[I] = (k == I) ? b[I] + bl2 : bl2;
     }
+    // shear rows: B_L2(3+aux, k) = sum_{m != aux} g(k, m) b_{3-m-aux}
+    const T s3 = g[k + 3 * 1] * b[2] + g[k + 3 * 2] * b[1];
+    const T s4 = g[k + 3 * 0] * b[2] + g[k + 3 * 2] * b[0];
+    const T s5 = g[k + 3 * 0] * b[1] + g[k + 3 * 1] * b[0];
+    bf[3] = (k == 1) ? b[2] + s3 : ((k == 2) ? b[1] + s3 : s3);
+    bf[4] = (k == 0) ? b[2] + s4 : ((k == 2) ? b[0] + s4 : s4);
+    bf[5] = (k == 0) ? b[1] + s5 : ((k == 1) ? b[0] + s5 : s5);
+    T acc = bf[0] * Sv[0];
+#pragma unroll
+    for (int I = 1; I < 6; ++I) acc = acc + bf[I] * Sv[I];
+    return acc;
+  } else {
+    T bf[3];
+#pragma unroll
+    for (int I = 0; I < 2; ++I) {
+      const T bl2 = g[k + 2 * I] * b[I];
+      bf[I] = (k == I) ? b[I] + bl2 : bl2;
+    }
+    const T s2 = g[k + 2 * 0] * b[1] + g[k + 2 * 1] * b[0];
+    bf[2] = ((k == 1) ? b[0] : b[1]) + s2;
+    T acc = bf[0] * Sv[0];
+    acc = acc + bf[1] * Sv[1];
+    acc = acc + bf[2] * Sv[2];
+    return acc;
   }
-  return acc;
+}
+
+// first Piola-Kirchhoff form of the same force, P = F S, r(a, k) = P(k, :) . dN_a/dx,
+// used by the mixed-precision path (equal in exact arithmetic, fewer operations)
+template <int D, class T>
+__device__ __forceinline__ void first_piola(const T *g, const T *S, T w, T *P) {
+#pragma unroll
+  for (int J = 0; J < D; ++J)
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      T s = S[k + D * J];
+#pragma unroll
+      for (int m = 0; m < D; ++m) s += g[k + D * m] * S[m + D * J];
+      P[k + D * J] = s * w;
+    }
 }
 
 template <int D, class T> __device__ __forceinline__ void to_voigt(const T *S, T *Sv) {

@@ -294,14 +294,30 @@ __global__ void __launch_bounds__(EPB<NQ>::value * NQ)
         g[i + D * j] = s;
       }
     if constexpr (LAW == LAW_NEOHOOKEAN) {
-      T S[D * D], Sv[D == 3 ? 6 : 3];
+      T S[D * D];
       neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
-      to_voigt<D, T>(S, Sv);
+      if constexpr (REL) {
+        // mixed path: r = (F S w) . dN/dx
+        T P[D * D];
+        first_piola<D, T>(g, S, w, P);
 #pragma unroll
-      for (int a = 0; a < NN; ++a)
+        for (int a = 0; a < NN; ++a)
 #pragma unroll
-        for (int k = 0; k < D; ++k)
-          t[a * D + k] = finite_force_component<D, T>(&b[a * D], g, Sv, k) * w;
+          for (int k = 0; k < D; ++k) {
+            T s = P[k] * b[a * D];
+#pragma unroll
+            for (int J = 1; J < D; ++J) s += P[k + D * J] * b[a * D + J];
+            t[a * D + k] = s;
+          }
+      } else {
+        T Sv[D == 3 ? 6 : 3];
+        to_voigt<D, T>(S, Sv);
+#pragma unroll
+        for (int a = 0; a < NN; ++a)
+#pragma unroll
+          for (int k = 0; k < D; ++k)
+            t[a * D + k] = finite_force_component<D, T>(&b[a * D], g, Sv, k) * w;
+      }
     } else {
       T sig[D * D];
       if constexpr (LAW == LAW_ELASTIC) {
@@ -343,15 +359,30 @@ __global__ void __launch_bounds__(EPB<NQ>::value * NQ)
         ps.iso[lq] = iso;
       }
       // sigma B, d x n  (shape_lagrange_inline_impl.hh:402-408), times wJ_q
+      if constexpr (REL) {
+        // mixed path: (sigma w) B
 #pragma unroll
-      for (int a = 0; a < NN; ++a)
+        for (int k = 0; k < D * D; ++k) sig[k] *= w;
 #pragma unroll
-        for (int i = 0; i < D; ++i) {
-          T s = sig[i] * b[a * D];
+        for (int a = 0; a < NN; ++a)
 #pragma unroll
-          for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * b[a * D + j];
-          t[a * D + i] = s * w;
-        }
+          for (int i = 0; i < D; ++i) {
+            T s = sig[i] * b[a * D];
+#pragma unroll
+            for (int j = 1; j < D; ++j) s += sig[i + D * j] * b[a * D + j];
+            t[a * D + i] = s;
+          }
+      } else {
+#pragma unroll
+        for (int a = 0; a < NN; ++a)
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            T s = sig[i] * b[a * D];
+#pragma unroll
+            for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * b[a * D + j];
+            t[a * D + i] = s * w;
+          }
+      }
     }
   }
 

@@ -144,7 +144,11 @@ class SolidMechanicsModel:
     # -- set-up ------------------------------------------------------------------
     def addMaterial(self, type, **params):
         """Adds one material (alternative to a parsed .dat file)."""
-        text = "\n".join(f"{k} = {v}" for k, v in params.items())
+        def fmt(v):
+            if isinstance(v, (bool, np.bool_)):
+                return "true" if v else "false"
+            return repr(float(v)) if isinstance(v, (int, float, np.floating)) else str(v)
+        text = "\n".join(f"{k} = {fmt(v)}" for k, v in params.items())
         _capi.check(_capi.lib().akb_model_add_material(self._h, type.encode(), text.encode()))
         self._materials_added = True
 

@@ -301,6 +301,8 @@ def run_ours(args):
                               "frac": step_b / (ms / args.steps / 1e3) / 1e9 / peak},
             "clocks": clk.summary(),
             "gpu_launches": args.steps * 3,
+            # the state after the timed steps must be finite (device status word)
+            "state_finite": m.getStatus() == 0 and bool(np.all(np.isfinite(m.getDisplacement()))),
         }
         if prec == precisions[0]:
             # end to end through the C ABI with host buffers
@@ -345,7 +347,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (no flush)"},
             "e2e": head.get("e2e"), "roofline": head["roofline"],
             "roofline_step": head["roofline_step"], "clocks": head["clocks"],
-            "gpu_launches": head["gpu_launches"],
+            "gpu_launches": head["gpu_launches"], "state_finite": head["state_finite"],
             "phase_ms_per_step": head["phase_ms_per_step"],
             "cpu_baseline": cpu,
         }
