@@ -44,17 +44,32 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
-    constexpr int EB = EPB<NQ>::value;
-    const unsigned grid = (unsigned)((ne + EB - 1) / EB);
-    if (law == LAW_ELASTIC)
-      k_element_forces<D, NN, NQ, LAW_ELASTIC, T, RT>
-          <<<grid, EB * NQ, 0, s>>>(e0, ne, g.E, g.conn, B, wJ, u, mp, ps, re);
-    else if (law == LAW_NEOHOOKEAN)
-      k_element_forces<D, NN, NQ, LAW_NEOHOOKEAN, T, RT>
-          <<<grid, EB * NQ, 0, s>>>(e0, ne, g.E, g.conn, B, wJ, u, mp, ps, re);
-    else
-      k_element_forces<D, NN, NQ, LAW_PLASTIC, T, RT>
-          <<<grid, EB * NQ, 0, s>>>(e0, ne, g.E, g.conn, B, wJ, u, mp, ps, re);
+    // FP64 hexahedra: one thread per (element, point); otherwise one thread
+    // per element looping over its points
+    constexpr bool PQ = std::is_same<T, double>::value && NQ == 8;
+    if constexpr (PQ) {
+      const unsigned grid = (unsigned)((ne + 31) / 32);
+      if (law == LAW_ELASTIC)
+        k_element_forces_pq<D, NN, NQ, LAW_ELASTIC>
+            <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      else if (law == LAW_NEOHOOKEAN)
+        k_element_forces_pq<D, NN, NQ, LAW_NEOHOOKEAN>
+            <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      else
+        k_element_forces_pq<D, NN, NQ, LAW_PLASTIC>
+            <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+    } else {
+      const unsigned grid = (unsigned)((ne + kPeThreads - 1) / kPeThreads);
+      if (law == LAW_ELASTIC)
+        k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT>
+            <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      else if (law == LAW_NEOHOOKEAN)
+        k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT>
+            <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      else
+        k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT>
+            <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+    }
   });
   return cudaGetLastError();
 }

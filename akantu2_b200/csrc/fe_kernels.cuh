@@ -4,8 +4,9 @@
 // HBM layout (all arrays in internal element order: elements grouped by
 // material, ascending original id inside a material):
 //   conn  int32 [NN][E]              node ids, component-major
-//   B     T     [NN*D][E*NQ]         dN_a/dx_j at (a*D + j), per (e, q)
-//   wJ    T     [E*NQ]               det J * w_q
+//   B     T     [NQ][NN*D][E]        dN_a/dx_j of point q at ((q*NN + a)*D + j)*E + e
+//   wJ    T     [NQ][E]              det J * w_q
+//   per-material quadrature-point internals [NQ][comp][ne] (element fastest)
 //   re    RT    [E*NN][D]            elemental internal force, read by the
 //                                    node gather in ascending slot order
 //   u,v,a,fext,fint double [N][D]    user node order (reference layout)
@@ -30,27 +31,27 @@ struct QuadTable {
   double w[kMaxNQ];
 };
 
-// per-material plastic internals, SoA [comp][nqp_m], ping-pong prev/cur
+// per-material plastic internals, [q][comp][ne], ping-pong prev/cur
 struct PlasticState {
   const double *sig_prev, *gu_prev, *eps_prev, *iso_prev;
   const double *iso_cur_in;  // "current" hardening read by the yield test
   double *sig, *gu, *eps, *iso;
   double *pe;                // cumulative plastic energy density
-  int64_t nqp;               // quadrature points of the material
   int update_energy;         // 1 inside solveStep (afterSolveStep), 0 otherwise
 };
 
 // ---------------------------------------------------------------------------
 // K0: dN/dx and det J * w  (element_class_tmpl.hh:296-395,
-// integrator_gauss_inline_impl.hh:176-195,378-398).  One thread per (e, q).
+// integrator_gauss_inline_impl.hh:176-195,378-398).  One thread per (e, q),
+// element fastest.  bad receives the smallest e*NQ + q with det J < 0.
 template <int D, int NN, int NQ>
 __global__ void k_precompute(const double *__restrict__ X, const int32_t *__restrict__ conn,
                              int64_t E, QuadTable tab, double *__restrict__ B,
                              double *__restrict__ wJ, unsigned long long *__restrict__ bad) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= E * NQ) return;
-  const int64_t e = t / NQ;
-  const int q = (int)(t - e * NQ);
+  const int q = (int)(t / E);
+  const int64_t e = t - (int64_t)q * E;
   double Xe[NN * D];
 #pragma unroll
   for (int a = 0; a < NN; ++a) {
@@ -77,7 +78,6 @@ __global__ void k_precompute(const double *__restrict__ X, const int32_t *__rest
     det = det2(J);
     inv2(J, Ji);
   }
-  const int64_t EQ = E * NQ;
 #pragma unroll
   for (int a = 0; a < NN; ++a)
 #pragma unroll
@@ -85,9 +85,9 @@ __global__ void k_precompute(const double *__restrict__ X, const int32_t *__rest
       double s = Ji[j] * dn[a];
 #pragma unroll
       for (int k = 1; k < D; ++k) s = s + Ji[j + D * k] * dn[k * kMaxNN + a];
-      B[(int64_t)(a * D + j) * EQ + t] = s;
+      B[(int64_t)((q * NN + a) * D + j) * E + e] = s;
     }
-  if (det < 0) atomicMin(bad, (unsigned long long)t);
+  if (det < 0) atomicMin(bad, (unsigned long long)(e * NQ + q));
   wJ[t] = det * tab.w[q];
 }
 
@@ -103,17 +103,17 @@ __global__ void k_mass_elem(int64_t e_begin, int64_t e_count, int64_t E, double 
   if (le >= e_count) return;
   const int64_t e = e_begin + le;
   if constexpr (DIAG) {
-    double vol = rho * wJ[e * NQ];
+    double vol = rho * wJ[e];
 #pragma unroll
-    for (int q = 1; q < NQ; ++q) vol = vol + rho * wJ[e * NQ + q];
+    for (int q = 1; q < NQ; ++q) vol = vol + rho * wJ[q * E + e];
 #pragma unroll
     for (int a = 0; a < NN; ++a) me[e * NN + a] = vol * (a < 3 ? 1. / 12. : 1. / 4.);
   } else {
 #pragma unroll
     for (int a = 0; a < NN; ++a) {
-      double acc = rho * tab.N[a] * wJ[e * NQ];
+      double acc = rho * tab.N[a] * wJ[e];
 #pragma unroll
-      for (int q = 1; q < NQ; ++q) acc = acc + rho * tab.N[q * kMaxNN + a] * wJ[e * NQ + q];
+      for (int q = 1; q < NQ; ++q) acc = acc + rho * tab.N[q * kMaxNN + a] * wJ[q * E + e];
       me[e * NN + a] = acc;
     }
   }
@@ -216,203 +216,269 @@ __global__ void k_element_dt(int64_t e_begin, int64_t e_count, int64_t E, double
 
 // ---------------------------------------------------------------------------
 // K3: NewmarkBeta::predictor, alpha = 0, beta = 1/2 (newmark-beta.cc:47-76)
-//   u += dt v + (dt/2)(dt a);  v += dt a   on non-blocked dofs
+//   u_pred = u + (dt v + (dt/2)(dt a)) on non-blocked dofs, u elsewhere.
+// The displacement goes to a second buffer; the predicted velocity v + dt a is
+// formed again by the node update (same arithmetic), so v and a keep the
+// corrected values of the last step.  Only launched when the prediction made
+// by the previous node update is not valid (first step, or the host wrote u,
+// v, a, the blocked dofs or the time step in between).
 template <int D>
-__global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked, double *__restrict__ u,
-                          double *__restrict__ v, const double *__restrict__ a, double dt) {
+__global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
+                          const double *__restrict__ u, const double *__restrict__ v,
+                          const double *__restrict__ a, double dt, double *__restrict__ u_pred) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N * D) return;
   const int64_t node = i / D;
   const int c = (int)(i - node * D);
-  if ((blocked[node] >> c) & 1) return;
+  if ((blocked[node] >> c) & 1) {
+    u_pred[i] = u[i];
+    return;
+  }
   const double hdt = .5 * dt;
   const double dta = dt * a[i];
-  u[i] = u[i] + (dt * v[i] + hdt * dta);
-  v[i] = v[i] + dta;
+  u_pred[i] = u[i] + (dt * v[i] + hdt * dta);
 }
 
 // ---------------------------------------------------------------------------
 // K4: gradient at quadrature points, material law, B^T sigma integration.
-// One thread per (element, quadrature point); the NQ threads of an element
-// share its gathered displacement and sum their contributions in q order.
-template <int NQ> struct EPB {
-  static constexpr int value = NQ == 1 ? 128 : (NQ == 8 ? 16 : (128 / NQ));
-};
+//
+// element_law<...>() evaluates one (element, quadrature point): the gradient
+// u B^T, the law, and the weighted elemental force t = (B^T sigma or
+// B(grad u)^T S) * wJ_q.  Two launch shapes use it:
+//  - k_element_forces_pe: one thread per element, loop over q, accumulate t
+//    in registers in increasing q (all mixed kernels; FP64 tet4 / tri6);
+//  - k_element_forces_pq: one thread per (element, q) for FP64 hexahedra,
+//    32 elements per warp (lanes = elements, warps = quadrature points), the
+//    per-q contributions summed in increasing q through shared memory laid
+//    out [q][component][lane], which is free of bank conflicts.
+
+// plastic internals of one quadrature point: loads previous state, runs the
+// radial return, stores the new state (and the plastic energy in a step)
+template <int D>
+__device__ __forceinline__ void plastic_point(const MatParams &mp, const PlasticState &ps,
+                                              int64_t ne, int64_t le, int q,
+                                              const double *gd, double *s) {
+  constexpr int DD = D * D;
+  double gp[DD], sp[DD], epp[DD], ep[DD], iso;
+#pragma unroll
+  for (int k = 0; k < DD; ++k) {
+    const int64_t idx = (int64_t)(q * DD + k) * ne + le;
+    gp[k] = ps.gu_prev[idx];
+    sp[k] = ps.sig_prev[idx];
+    epp[k] = ps.eps_prev[idx];
+  }
+  const int64_t qi = (int64_t)q * ne + le;
+  plastic_update<D>(mp.lambda, mp.mu, mp.sigma_y, mp.h, gd, gp, sp, epp, ps.iso_cur_in[qi],
+                    ps.iso_prev[qi], 0., s, ep, &iso);
+  if (ps.update_energy) {
+    // MaterialPlastic::updateEnergies (material_plastic.cc:85-103)
+    double wp = 0.;
+#pragma unroll
+    for (int k = 0; k < DD; ++k) {
+      const double de = ep[k] - epp[k];
+      const double sh = s[k] + sp[k];
+      wp = (k == 0) ? sh * de : wp + sh * de;
+    }
+    wp = wp / 2.;
+    ps.pe[qi] = ps.pe[qi] + wp;
+  }
+#pragma unroll
+  for (int k = 0; k < DD; ++k) {
+    const int64_t idx = (int64_t)(q * DD + k) * ne + le;
+    ps.gu[idx] = gd[k];
+    ps.sig[idx] = s[k];
+    ps.eps[idx] = ep[k];
+  }
+  ps.iso[qi] = iso;
+}
+
+template <int D, int NN, int LAW, class T, bool REL>
+__device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const MatParams &mp,
+                                            const PlasticState &ps, int64_t ne, int64_t le,
+                                            int q, T *t) {
+  // grad u = u B^T  (shape_functions_inline_impl.hh:303-310)
+  T g[D * D];
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T s = ue[i] * b[j];
+#pragma unroll
+      for (int a = 1; a < NN; ++a) s = s + ue[a * D + i] * b[a * D + j];
+      g[i + D * j] = s;
+    }
+  if constexpr (LAW == LAW_NEOHOOKEAN) {
+    T S[D * D];
+    neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
+    if constexpr (REL) {
+      // mixed path: r = (F S w) . dN/dx
+      T P[D * D];
+      first_piola<D, T>(g, S, w, P);
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          T s = P[k] * b[a * D];
+#pragma unroll
+          for (int J = 1; J < D; ++J) s += P[k + D * J] * b[a * D + J];
+          t[a * D + k] = s;
+        }
+    } else {
+      T Sv[D == 3 ? 6 : 3];
+      to_voigt<D, T>(S, Sv);
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+          t[a * D + k] = finite_force_component<D, T>(&b[a * D], g, Sv, k) * w;
+    }
+  } else {
+    T sig[D * D];
+    if constexpr (LAW == LAW_ELASTIC) {
+      elastic_stress<D, T>((T)mp.lambda, (T)mp.mu, g, (T)mp.sigma_th, sig);
+    } else {
+      double gd[D * D], s[D * D];
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) gd[k] = (double)g[k];
+      plastic_point<D>(mp, ps, ne, le, q, gd, s);
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) sig[k] = (T)s[k];
+    }
+    // sigma B, d x n  (shape_lagrange_inline_impl.hh:402-408), times wJ_q
+    if constexpr (REL) {
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) sig[k] *= w;
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          T s = sig[i] * b[a * D];
+#pragma unroll
+          for (int j = 1; j < D; ++j) s += sig[i + D * j] * b[a * D + j];
+          t[a * D + i] = s;
+        }
+    } else {
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          T s = sig[i] * b[a * D];
+#pragma unroll
+          for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * b[a * D + j];
+          t[a * D + i] = s * w;
+        }
+    }
+  }
+}
+
+constexpr int kPeThreads = 128;
 
 template <int D, int NN, int NQ, int LAW, class T, class RT>
-__global__ void __launch_bounds__(EPB<NQ>::value * NQ)
-    k_element_forces(int64_t e_begin, int64_t e_count, int64_t E,
-                     const int32_t *__restrict__ conn, const T *__restrict__ B,
-                     const T *__restrict__ wJ, const double *__restrict__ u, MatParams mp,
-                     PlasticState ps, RT *__restrict__ re) {
+__global__ void __launch_bounds__(kPeThreads)
+    k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
+                        const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                        const T *__restrict__ B, const T *__restrict__ wJ,
+                        const double *__restrict__ u, MatParams mp, PlasticState ps,
+                        RT *__restrict__ re) {
   constexpr int ND = NN * D;
-  constexpr int EB = EPB<NQ>::value;
   constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
-  __shared__ double us[EB][ND];
-  __shared__ T red[NQ > 1 ? EB : 1][NQ > 1 ? NQ : 1][ND];
+  const int64_t le = (int64_t)blockIdx.x * kPeThreads + threadIdx.x;
+  if (le >= e_count) return;
+  const int64_t e = e_begin + le;
+  T ue[ND];
+  double u0[D];
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const double x = u[node * D + i];
+      if constexpr (REL) {
+        if (a == 0) u0[i] = x;
+        ue[a * D + i] = (T)(x - u0[i]);
+      } else {
+        ue[a * D + i] = x;
+      }
+    }
+  }
+  T r[ND];
+#pragma unroll 1
+  for (int q = 0; q < NQ; ++q) {
+    T b[ND];
+#pragma unroll
+    for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)(q * ND + c) * E + e];
+    const T w = wJ[(int64_t)q * E + e];
+    T t[ND];
+    element_law<D, NN, LAW, T, REL>(ue, b, w, mp, ps, e_count, le, q, t);
+    // integrate: sum over q in increasing order (integrator_gauss_inline_impl.hh:401-418)
+#pragma unroll
+    for (int c = 0; c < ND; ++c) r[c] = (q == 0) ? t[c] : r[c] + t[c];
+  }
+  // elemental force of node a goes to its position in the node CSR
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    const int64_t p = pos[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < D; ++i) re[p * D + i] = (RT)r[a * D + i];
+  }
+}
 
-  const int eb = threadIdx.x / NQ;
-  const int q = threadIdx.x - eb * NQ;
-  const int64_t le = (int64_t)blockIdx.x * EB + eb;
+// FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q
+template <int D, int NN, int NQ, int LAW>
+__global__ void __launch_bounds__(32 * NQ)
+    k_element_forces_pq(int64_t e_begin, int64_t e_count, int64_t E,
+                        const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                        const double *__restrict__ B, const double *__restrict__ wJ,
+                        const double *__restrict__ u, MatParams mp, PlasticState ps,
+                        double *__restrict__ re) {
+  constexpr int ND = NN * D;
+  constexpr int CH = (ND + NQ - 1) / NQ;  // components reduced per round and thread
+  __shared__ double us[ND][32];
+  __shared__ double red[NQ][NQ][32];
+  const int lane = threadIdx.x & 31;
+  const int q = threadIdx.x >> 5;
+  const int64_t le = (int64_t)blockIdx.x * 32 + lane;
   const bool active = le < e_count;
   const int64_t e = e_begin + le;
-
   if (active) {
     for (int a = q; a < NN; a += NQ) {
       const int64_t node = conn[(int64_t)a * E + e];
 #pragma unroll
-      for (int i = 0; i < D; ++i) us[eb][a * D + i] = u[node * D + i];
+      for (int i = 0; i < D; ++i) us[a * D + i][lane] = u[node * D + i];
     }
   }
-  if constexpr (NQ > 1) __syncthreads();
-
-  T t[ND];
+  __syncthreads();
+  double t[ND];
   if (active) {
-    const int64_t EQ = E * NQ;
-    const int64_t eq = e * NQ + q;
-    T b[ND];
+    double ue[ND], b[ND];
 #pragma unroll
-    for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)c * EQ + eq];
-    const T w = wJ[eq];
-    T ue[ND];
-    if constexpr (REL) {
-#pragma unroll
-      for (int c = 0; c < ND; ++c) ue[c] = (T)(us[eb][c] - us[eb][c % D]);
-    } else {
-#pragma unroll
-      for (int c = 0; c < ND; ++c) ue[c] = us[eb][c];
+    for (int c = 0; c < ND; ++c) {
+      ue[c] = us[c][lane];
+      b[c] = B[(int64_t)(q * ND + c) * E + e];
     }
-    // grad u = u B^T  (shape_functions_inline_impl.hh:303-310)
-    T g[D * D];
-#pragma unroll
-    for (int j = 0; j < D; ++j)
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        T s = ue[i] * b[j];
-#pragma unroll
-        for (int a = 1; a < NN; ++a) s = s + ue[a * D + i] * b[a * D + j];
-        g[i + D * j] = s;
-      }
-    if constexpr (LAW == LAW_NEOHOOKEAN) {
-      T S[D * D];
-      neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
-      if constexpr (REL) {
-        // mixed path: r = (F S w) . dN/dx
-        T P[D * D];
-        first_piola<D, T>(g, S, w, P);
-#pragma unroll
-        for (int a = 0; a < NN; ++a)
-#pragma unroll
-          for (int k = 0; k < D; ++k) {
-            T s = P[k] * b[a * D];
-#pragma unroll
-            for (int J = 1; J < D; ++J) s += P[k + D * J] * b[a * D + J];
-            t[a * D + k] = s;
-          }
-      } else {
-        T Sv[D == 3 ? 6 : 3];
-        to_voigt<D, T>(S, Sv);
-#pragma unroll
-        for (int a = 0; a < NN; ++a)
-#pragma unroll
-          for (int k = 0; k < D; ++k)
-            t[a * D + k] = finite_force_component<D, T>(&b[a * D], g, Sv, k) * w;
-      }
-    } else {
-      T sig[D * D];
-      if constexpr (LAW == LAW_ELASTIC) {
-        elastic_stress<D, T>((T)mp.lambda, (T)mp.mu, g, (T)mp.sigma_th, sig);
-      } else {
-        constexpr int DD = D * D;
-        const int64_t lq = le * NQ + q;
-        double gd[DD], gp[DD], sp[DD], epp[DD], s[DD], ep[DD], iso;
-#pragma unroll
-        for (int k = 0; k < DD; ++k) {
-          gd[k] = (double)g[k];
-          gp[k] = ps.gu_prev[k * ps.nqp + lq];
-          sp[k] = ps.sig_prev[k * ps.nqp + lq];
-          epp[k] = ps.eps_prev[k * ps.nqp + lq];
-        }
-        const double isop = ps.iso_prev[lq];
-        const double isoc = ps.iso_cur_in[lq];
-        plastic_update<D>(mp.lambda, mp.mu, mp.sigma_y, mp.h, gd, gp, sp, epp, isoc, isop, 0.,
-                          s, ep, &iso);
-        if (ps.update_energy) {
-          // MaterialPlastic::updateEnergies (material_plastic.cc:85-103)
-          double wp = 0.;
-#pragma unroll
-          for (int k = 0; k < DD; ++k) {
-            const double de = ep[k] - epp[k];
-            const double sh = s[k] + sp[k];
-            wp = (k == 0) ? sh * de : wp + sh * de;
-          }
-          wp = wp / 2.;
-          ps.pe[lq] = ps.pe[lq] + wp;
-        }
-#pragma unroll
-        for (int k = 0; k < DD; ++k) {
-          ps.gu[k * ps.nqp + lq] = gd[k];
-          ps.sig[k * ps.nqp + lq] = s[k];
-          ps.eps[k * ps.nqp + lq] = ep[k];
-          sig[k] = (T)s[k];
-        }
-        ps.iso[lq] = iso;
-      }
-      // sigma B, d x n  (shape_lagrange_inline_impl.hh:402-408), times wJ_q
-      if constexpr (REL) {
-        // mixed path: (sigma w) B
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) sig[k] *= w;
-#pragma unroll
-        for (int a = 0; a < NN; ++a)
-#pragma unroll
-          for (int i = 0; i < D; ++i) {
-            T s = sig[i] * b[a * D];
-#pragma unroll
-            for (int j = 1; j < D; ++j) s += sig[i + D * j] * b[a * D + j];
-            t[a * D + i] = s;
-          }
-      } else {
-#pragma unroll
-        for (int a = 0; a < NN; ++a)
-#pragma unroll
-          for (int i = 0; i < D; ++i) {
-            T s = sig[i] * b[a * D];
-#pragma unroll
-            for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * b[a * D + j];
-            t[a * D + i] = s * w;
-          }
-      }
-    }
+    const double w = wJ[(int64_t)q * E + e];
+    element_law<D, NN, LAW, double, false>(ue, b, w, mp, ps, e_count, le, q, t);
   }
-
-  if constexpr (NQ == 1) {
+  // sum over q in increasing order, NQ components per round
+#pragma unroll
+  for (int round = 0; round < CH; ++round) {
     if (active) {
 #pragma unroll
-      for (int c = 0; c < ND; ++c) re[e * ND + c] = (RT)t[c];
-    }
-  } else {
-    if (active) {
-#pragma unroll
-      for (int c = 0; c < ND; ++c) red[eb][q][c] = t[c];
+      for (int k = 0; k < NQ; ++k) {
+        const int c = round * NQ + k;
+        if (c < ND) red[q][k][lane] = t[c];
+      }
     }
     __syncthreads();
-    if (active) {
-      // integrate: sum over q in increasing order (integrator_gauss_inline_impl.hh:401-418)
-      for (int c = q; c < ND; c += NQ) {
-        if constexpr (std::is_same<T, double>::value) {
-          T s = red[eb][0][c];
+    const int c = round * NQ + q;
+    if (active && c < ND) {
+      double s = red[0][q][lane];
 #pragma unroll
-          for (int qq = 1; qq < NQ; ++qq) s = s + red[eb][qq][c];
-          re[e * ND + c] = (RT)s;
-        } else {
-          float s = red[eb][0][c];
-#pragma unroll
-          for (int qq = 1; qq < NQ; ++qq) s = s + red[eb][qq][c];
-          re[e * ND + c] = (RT)s;
-        }
-      }
+      for (int qq = 1; qq < NQ; ++qq) s = s + red[qq][q][lane];
+      const int a = c / D;
+      re[(int64_t)pos[(int64_t)a * E + e] * D + (c - a * D)] = s;
     }
+    __syncthreads();
   }
 }
 
@@ -424,14 +490,20 @@ __global__ void __launch_bounds__(EPB<NQ>::value * NQ)
 //   x = r / M; v += (dt/2) x; a += x     (non_linear_solver_lumped.cc:76-87,
 //                                         newmark-beta.cc:163-197)
 // The displacement coefficient of the corrector is alpha*beta*dt^2 = 0.
+// The elemental forces are stored in node-CSR order, so node i reads
+// re[ptr[i] .. ptr[i+1]) contiguously, in increasing slot order.
+// mode 0: internal force only; 1: + residual, solve and corrector, where the
+// predicted velocity v + dt a of the reference predictor is formed here;
+// 2: + the predictor of the next step, u_next = u + (dt v + (dt/2)(dt a)).
 // KAHAN selects a compensated FP64 sum (mixed path).
 template <int D, class RT, bool KAHAN>
 __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
-                              const int32_t *__restrict__ ent, const RT *__restrict__ re,
-                              const double *__restrict__ fext, const double *__restrict__ mass,
+                              const RT *__restrict__ re, const double *__restrict__ fext,
+                              const double *__restrict__ mass,
                               const uint8_t *__restrict__ blocked, double *__restrict__ fint,
-                              double *__restrict__ a, double *__restrict__ v, double dt,
-                              int do_correct, unsigned int *__restrict__ status) {
+                              double *__restrict__ a, double *__restrict__ v,
+                              const double *__restrict__ u, double *__restrict__ u_next,
+                              double dt, int mode, unsigned int *__restrict__ status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[D], comp[D];
@@ -442,10 +514,9 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
   }
   const int32_t p0 = ptr[i], p1 = ptr[i + 1];
   for (int32_t p = p0; p < p1; ++p) {
-    const int64_t s = ent[p];
 #pragma unroll
     for (int c = 0; c < D; ++c) {
-      const double val = -1. * (double)re[s * D + c];
+      const double val = -1. * (double)re[(int64_t)p * D + c];
       if constexpr (KAHAN) {
         const double y = val - comp[c];
         const double tt = acc[c] + y;
@@ -464,18 +535,27 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
   for (int c = 0; c < D; ++c) {
     const int64_t k = i * D + c;
     fint[k] = acc[c];
-    if (!do_correct) continue;
+    if (mode == 0) continue;
+    const bool free_dof = !((bl >> c) & 1);
+    const double ak = a[k];
+    double vk = v[k];
+    if (free_dof) vk = vk + dt * ak;  // predicted velocity (newmark-beta.cc:69)
     double r = 0. + 1. * fext[k];
     r = r + 1. * acc[c];
-    const double ak = a[k];
     const double ma = 0. + -1. * ak;
     r = r + m * ma;
-    if (!((bl >> c) & 1)) {
+    double an = ak;
+    if (free_dof) {
       const double x = 1. * (r / m);
-      v[k] = v[k] + hdt * x;
-      const double an = ak + 1. * x;
+      vk = vk + hdt * x;
+      an = ak + 1. * x;
+      v[k] = vk;
       a[k] = an;
       bad |= !isfinite(an);
+    }
+    if (mode == 2) {
+      const double uk = u[k];
+      u_next[k] = free_dof ? uk + (dt * vk + hdt * (dt * an)) : uk;
     }
   }
   if (bad) atomicOr(status, 1u);
@@ -484,7 +564,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
 // ---------------------------------------------------------------------------
 // quadrature-point fields of elastic / neohookean materials, evaluated from a
 // displacement snapshot (the reference keeps them as internals,
-// material.cc:128-154).  Output SoA [D*D][nqp_m].
+// material.cc:128-154).  Output [q][D*D][ne].
 template <int D, int NN, int NQ, int LAW>
 __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const double *__restrict__ B,
@@ -492,10 +572,9 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
                             double *__restrict__ grad_out, double *__restrict__ stress_out) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e_count * NQ) return;
-  const int64_t le = t / NQ;
-  const int q = (int)(t - le * NQ);
+  const int q = (int)(t / e_count);
+  const int64_t le = t - (int64_t)q * e_count;
   const int64_t e = e_begin + le;
-  const int64_t EQ = E * NQ, eq = e * NQ + q;
   double ue[NN * D], b[NN * D];
 #pragma unroll
   for (int a = 0; a < NN; ++a) {
@@ -504,7 +583,7 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
     for (int i = 0; i < D; ++i) ue[a * D + i] = u[node * D + i];
   }
 #pragma unroll
-  for (int c = 0; c < NN * D; ++c) b[c] = B[(int64_t)c * EQ + eq];
+  for (int c = 0; c < NN * D; ++c) b[c] = B[(int64_t)(q * NN * D + c) * E + e];
   double g[D * D], s[D * D];
 #pragma unroll
   for (int j = 0; j < D; ++j)
@@ -519,11 +598,10 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
     neohookean_pk2<D, double>(mp.lambda, mp.mu, g, s);
   else
     elastic_stress<D, double>(mp.lambda, mp.mu, g, mp.sigma_th, s);
-  const int64_t nqp = e_count * NQ;
 #pragma unroll
   for (int k = 0; k < D * D; ++k) {
-    grad_out[k * nqp + t] = g[k];
-    stress_out[k * nqp + t] = s[k];
+    grad_out[(int64_t)(q * D * D + k) * e_count + le] = g[k];
+    stress_out[(int64_t)(q * D * D + k) * e_count + le] = s[k];
   }
 }
 

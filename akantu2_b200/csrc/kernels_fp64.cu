@@ -59,13 +59,14 @@ cudaError_t launch_to_float(const double *in, float *out, int64_t n, cudaStream_
 }
 
 // ---- step ------------------------------------------------------------------
-cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, double *u, double *v,
-                           const double *a, double dt, cudaStream_t s) {
+cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const double *u,
+                           const double *v, const double *a, double dt, double *u_pred,
+                           cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
-    k_predict<3><<<grid_for(g.N * 3), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt);
+    k_predict<3><<<grid_for(g.N * 3), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, u_pred);
   else
-    k_predict<2><<<grid_for(g.N * 2), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt);
+    k_predict<2><<<grid_for(g.N * 2), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, u_pred);
   return cudaGetLastError();
 }
 
@@ -78,15 +79,15 @@ cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, in
 
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
-                                    double *a, double *v, double dt, int do_correct,
-                                    unsigned int *status, cudaStream_t s) {
+                                    double *a, double *v, const double *u, double *u_next,
+                                    double dt, int mode, unsigned int *status, cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
     k_node_update<3, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, mode, status);
   else
     k_node_update<2, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, mode, status);
   return cudaGetLastError();
 }
 
@@ -164,29 +165,30 @@ cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double
 }
 
 // per-element integral of an energy density (Material::getPotentialEnergy,
-// material.cc:604-619; MaterialPlastic::getPlasticEnergy, material_plastic.cc:47-69)
+// material.cc:604-619; MaterialPlastic::getPlasticEnergy, material_plastic.cc:47-69).
+// Quadrature-point inputs are [q][comp][ne]; wJ is [q][E].
 template <int D, int NQ, int LAW>
-__global__ void k_energy_elem(int which, int64_t e0, int64_t ne, const double *__restrict__ wJ,
-                              const double *__restrict__ grad, const double *__restrict__ stress,
+__global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t E,
+                              const double *__restrict__ wJ, const double *__restrict__ grad,
+                              const double *__restrict__ stress,
                               const double *__restrict__ eps_p, const double *__restrict__ pe,
                               MatParams mp, double *__restrict__ out) {
   const int64_t le = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (le >= ne) return;
   constexpr int DD = D * D;
-  const int64_t nqp = ne * NQ;
   double el = 0.;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    const int64_t lq = le * NQ + q;
+    auto at = [&](int k) { return (int64_t)(q * DD + k) * ne + le; };
     double dens;
     if (which == 1) {
-      dens = pe[lq];
+      dens = pe[(int64_t)q * ne + le];
     } else if (LAW == LAW_NEOHOOKEAN) {
       double F[DD];
 #pragma unroll
       for (int j = 0; j < D; ++j)
 #pragma unroll
-        for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? 1. : 0.) + grad[(i + D * j) * nqp + lq];
+        for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? 1. : 0.) + grad[at(i + D * j)];
       double trC = 0.;
 #pragma unroll
       for (int i = 0; i < D; ++i) {
@@ -202,14 +204,14 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, const double *_
       double dot = 0.;
 #pragma unroll
       for (int k = 0; k < DD; ++k) {
-        double ge = grad[k * nqp + lq];
-        if (LAW == LAW_PLASTIC) ge = ge - eps_p[k * nqp + lq];
-        const double sk = stress[k * nqp + lq];
+        double ge = grad[at(k)];
+        if (LAW == LAW_PLASTIC) ge = ge - eps_p[at(k)];
+        const double sk = stress[at(k)];
         dot = (k == 0) ? sk * ge : dot + sk * ge;
       }
       dens = .5 * dot;
     }
-    const double w = wJ[(e0 + le) * NQ + q];
+    const double w = wJ[(int64_t)q * E + e0 + le];
     el = (q == 0) ? dens * w : el + dens * w;
   }
   out[le] = el;
@@ -224,13 +226,13 @@ cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0,
     (void)NN;
     if (law == LAW_NEOHOOKEAN)
       k_energy_elem<D, NQ, LAW_NEOHOOKEAN><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, wJ, grad, stress, eps_p, pe, mp, out);
+          which, e0, ne, g.E, wJ, grad, stress, eps_p, pe, mp, out);
     else if (law == LAW_PLASTIC)
       k_energy_elem<D, NQ, LAW_PLASTIC><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, wJ, grad, stress, eps_p, pe, mp, out);
+          which, e0, ne, g.E, wJ, grad, stress, eps_p, pe, mp, out);
     else
       k_energy_elem<D, NQ, LAW_ELASTIC><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, wJ, grad, stress, eps_p, pe, mp, out);
+          which, e0, ne, g.E, wJ, grad, stress, eps_p, pe, mp, out);
   });
   return cudaGetLastError();
 }

@@ -14,15 +14,16 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
 
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
-                                     double *fint, double *a, double *v, double dt,
-                                     int do_correct, unsigned int *status, cudaStream_t s) {
+                                     double *fint, double *a, double *v, const double *u,
+                                     double *u_next, double dt, int mode,
+                                     unsigned int *status, cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
     k_node_update<3, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, mode, status);
   else
     k_node_update<2, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, g.ent, re, fext, mass, blocked, fint, a, v, dt, do_correct, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, mode, status);
   return cudaGetLastError();
 }
 

@@ -20,7 +20,8 @@ struct DevGeom {
   const int32_t *conn;  // [NN][E]
   const double *X;      // [N][D]
   const int32_t *ptr;   // [N+1]
-  const int32_t *ent;   // [E*NN]
+  const int32_t *ent;   // [E*NN] slot (e*NN + a) of each CSR position
+  const int32_t *pos;   // [NN][E] CSR position of each slot
 };
 
 // ---- init ------------------------------------------------------------------
@@ -36,8 +37,10 @@ cudaError_t launch_element_dt(const DevGeom &g, int64_t e0, int64_t ne, double c
 cudaError_t launch_to_float(const double *in, float *out, int64_t n, cudaStream_t s);
 
 // ---- step ------------------------------------------------------------------
-cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, double *u, double *v,
-                           const double *a, double dt, cudaStream_t s);
+// u_pred = predictor displacement of (u, v, a); v and a are not modified
+cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const double *u,
+                           const double *v, const double *a, double dt, double *u_pred,
+                           cudaStream_t s);
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
                                        const MatParams &mp, const PlasticState &ps,
@@ -46,14 +49,17 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
                                         const float *B, const float *wJ, const double *u,
                                         const MatParams &mp, const PlasticState &ps,
                                         float *re, cudaStream_t s);
+// mode 0: internal force only; 1: + corrector; 2: + predictor of the next
+// step from u into u_next
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
-                                    double *a, double *v, double dt, int do_correct,
-                                    unsigned int *status, cudaStream_t s);
+                                    double *a, double *v, const double *u, double *u_next,
+                                    double dt, int mode, unsigned int *status, cudaStream_t s);
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
-                                     double *fint, double *a, double *v, double dt,
-                                     int do_correct, unsigned int *status, cudaStream_t s);
+                                     double *fint, double *a, double *v, const double *u,
+                                     double *u_next, double dt, int mode,
+                                     unsigned int *status, cudaStream_t s);
 
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,

@@ -163,8 +163,13 @@ struct akb_model {
   // device arrays
   double *dX = nullptr, *dB = nullptr, *dwJ = nullptr;
   float *fB = nullptr, *fwJ = nullptr;
-  int32_t *dconn = nullptr, *dptr = nullptr, *dent = nullptr;
-  double *du = nullptr, *dv = nullptr, *da = nullptr, *dfext = nullptr, *dfint = nullptr;
+  int32_t *dconn = nullptr, *dptr = nullptr, *dent = nullptr, *dpos = nullptr;
+  // displacement ping-pong: dU[ucur] is the model's u, dU[1 - ucur] the
+  // prediction of the next step (valid when `predicted`)
+  double *dU[2] = {nullptr, nullptr};
+  int ucur = 0;
+  bool predicted = false;
+  double *dv = nullptr, *da = nullptr, *dfext = nullptr, *dfint = nullptr;
   double *dmass = nullptr, *dusnap = nullptr;
   uint8_t *dblocked = nullptr;
   void *dre = nullptr;
@@ -175,10 +180,12 @@ struct akb_model {
   unsigned long long *dbad = nullptr;
   std::vector<void *> allocs;
 
+  double *u() const { return dU[ucur]; }
+  double *u_pred() const { return dU[1 - ucur]; }
   DevGeom geom() const {
     DevGeom g;
     g.et = et; g.D = dim; g.NN = nn; g.NQ = nq; g.E = E; g.N = N;
-    g.conn = dconn; g.X = dX; g.ptr = dptr; g.ent = dent;
+    g.conn = dconn; g.X = dX; g.ptr = dptr; g.ent = dent; g.pos = dpos;
     return g;
   }
   template <class P> int alloc(P **p, size_t bytes) {
@@ -267,7 +274,7 @@ int snapshot_u(akb_model *m) {
   for (auto &mt : m->mats) need |= mt.law != LAW_PLASTIC;
   if (!need) return AKB_OK;
   if (!m->dusnap) AKB_TRY(m->alloc(&m->dusnap, sizeof(double) * nodal_doubles(m)));
-  AKB_CUDA(cudaMemcpyAsync(m->dusnap, m->du, sizeof(double) * nodal_doubles(m),
+  AKB_CUDA(cudaMemcpyAsync(m->dusnap, m->u(), sizeof(double) * nodal_doubles(m),
                            cudaMemcpyDeviceToDevice, m->stream));
   m->snap_valid = true;
   return AKB_OK;
@@ -292,39 +299,66 @@ PlasticState plastic_state(akb_model *m, const Material &mt, bool in_step) {
   ps.eps = mt.eps[out];
   ps.iso = mt.iso[out];
   ps.pe = mt.pe;
-  ps.nqp = mt.e_count * m->nq;
   ps.update_energy = in_step ? 1 : 0;
   return ps;
 }
 
+// elemental forces at the predicted displacement (inside a step) or at the
+// model's displacement (standalone assembly)
 int element_forces(akb_model *m, bool in_step) {
   DevGeom g = m->geom();
+  const double *u = in_step ? m->u_pred() : m->u();
   for (auto &mt : m->mats) {
     PlasticState ps = plastic_state(m, mt, in_step);
     cudaError_t e;
     if (m->precision == AKB_PRECISION_MIXED)
-      e = launch_element_forces_mixed(g, mt.law, mt.e_begin, mt.e_count, m->fB, m->fwJ, m->du,
+      e = launch_element_forces_mixed(g, mt.law, mt.e_begin, mt.e_count, m->fB, m->fwJ, u,
                                       mt.params(), ps, (float *)m->dre, m->stream);
     else
-      e = launch_element_forces_fp64(g, mt.law, mt.e_begin, mt.e_count, m->dB, m->dwJ, m->du,
+      e = launch_element_forces_fp64(g, mt.law, mt.e_begin, mt.e_count, m->dB, m->dwJ, u,
                                      mt.params(), ps, (double *)m->dre, m->stream);
     if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("element forces: ") + cudaGetErrorString(e));
   }
   return AKB_OK;
 }
 
+// correct == false: internal force only.  correct == true: corrector, then
+// the predictor of the next step from the new displacement u_pred into the
+// other buffer (which held the displacement of the previous step)
 int node_update(akb_model *m, bool correct) {
   DevGeom g = m->geom();
   cudaError_t e;
+  const int mode = correct ? 2 : 0;
+  const double *u = m->u_pred();
+  double *u_next = m->u();
   if (m->precision == AKB_PRECISION_MIXED)
     e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass, m->dblocked,
-                                 m->dfint, m->da, m->dv, m->dt, correct ? 1 : 0, m->dstatus,
+                                 m->dfint, m->da, m->dv, u, u_next, m->dt, mode, m->dstatus,
                                  m->stream);
   else
     e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass, m->dblocked,
-                                m->dfint, m->da, m->dv, m->dt, correct ? 1 : 0, m->dstatus,
+                                m->dfint, m->da, m->dv, u, u_next, m->dt, mode, m->dstatus,
                                 m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
+  return AKB_OK;
+}
+
+// one explicit step: [predictor,] element forces, node update (+ next
+// predictor); afterwards the prediction buffer becomes the model's u
+int one_step(akb_model *m, bool any_plastic, cudaEvent_t e1 = nullptr,
+             cudaEvent_t e2 = nullptr) {
+  DevGeom g = m->geom();
+  if (!m->predicted) {
+    AKB_CUDA(launch_predict(g, m->dblocked, m->u(), m->dv, m->da, m->dt, m->u_pred(), m->stream));
+    m->predicted = true;
+  }
+  if (e1) AKB_CUDA(cudaEventRecord(e1, m->stream));
+  AKB_TRY(element_forces(m, true));
+  if (e2) AKB_CUDA(cudaEventRecord(e2, m->stream));
+  AKB_TRY(node_update(m, true));
+  m->ucur = 1 - m->ucur;  // u_{n+1} is now the model's displacement
+  if (any_plastic) m->cur = 1 - m->cur;
+  m->steps_done++;
   return AKB_OK;
 }
 
@@ -348,7 +382,7 @@ int eval_qp_fields(akb_model *m, const Material &mt) {
     AKB_CUDA(cudaMemsetAsync(m->dqp_b, 0, sizeof(double) * std::max<int64_t>(n, 1), m->stream));
     return AKB_OK;
   }
-  const double *u = m->snap_valid ? m->dusnap : m->du;
+  const double *u = m->snap_valid ? m->dusnap : m->u();
   AKB_CUDA(launch_qp_fields(m->geom(), mt.law, mt.e_begin, mt.e_count, m->dB, u, mt.params(),
                             m->dqp_a, m->dqp_b, m->stream));
   return AKB_OK;
@@ -526,23 +560,30 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   for (int64_t ie = 0; ie < E; ++ie)
     for (int a = 0; a < nn; ++a) conn_soa[(size_t)a * E + ie] = m->conn[m->perm[ie] * nn + a];
   // node -> slot CSR, slots ascending (= material, user element, local node)
-  std::vector<int32_t> ptr(N + 1, 0), ent((size_t)E * nn);
+  // pos: CSR position of slot (a, e), where the element kernel writes the
+  // force of its node a, so the node gather reads its forces contiguously
+  std::vector<int32_t> ptr(N + 1, 0), ent((size_t)E * nn), pos((size_t)E * nn);
   for (int64_t ie = 0; ie < E; ++ie)
     for (int a = 0; a < nn; ++a) ptr[conn_soa[(size_t)a * E + ie] + 1]++;
   for (int64_t i = 0; i < N; ++i) ptr[i + 1] += ptr[i];
   {
     std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
     for (int64_t ie = 0; ie < E; ++ie)
-      for (int a = 0; a < nn; ++a) ent[fill[conn_soa[(size_t)a * E + ie]]++] = (int32_t)(ie * nn + a);
+      for (int a = 0; a < nn; ++a) {
+        const int32_t p = fill[conn_soa[(size_t)a * E + ie]]++;
+        ent[p] = (int32_t)(ie * nn + a);
+        pos[(size_t)a * E + ie] = p;
+      }
   }
 
   AKB_TRY(m->alloc(&m->dX, sizeof(double) * N * d));
   AKB_TRY(m->alloc(&m->dconn, sizeof(int32_t) * E * nn));
   AKB_TRY(m->alloc(&m->dptr, sizeof(int32_t) * (N + 1)));
   AKB_TRY(m->alloc(&m->dent, sizeof(int32_t) * E * nn));
+  AKB_TRY(m->alloc(&m->dpos, sizeof(int32_t) * E * nn));
   AKB_TRY(m->alloc(&m->dB, sizeof(double) * E * nq * nn * d));
   AKB_TRY(m->alloc(&m->dwJ, sizeof(double) * E * nq));
-  for (double **p : {&m->du, &m->dv, &m->da, &m->dfext, &m->dfint})
+  for (double **p : {&m->dU[0], &m->dU[1], &m->dv, &m->da, &m->dfext, &m->dfint})
     AKB_TRY(m->alloc(p, sizeof(double) * N * d));
   AKB_TRY(m->alloc(&m->dmass, sizeof(double) * N));
   AKB_TRY(m->alloc(&m->dblocked, N));
@@ -559,7 +600,8 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   AKB_CUDA(cudaMemcpyAsync(m->dconn, conn_soa.data(), sizeof(int32_t) * E * nn, cudaMemcpyHostToDevice, s));
   AKB_CUDA(cudaMemcpyAsync(m->dptr, ptr.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, s));
   AKB_CUDA(cudaMemcpyAsync(m->dent, ent.data(), sizeof(int32_t) * E * nn, cudaMemcpyHostToDevice, s));
-  for (double *p : {m->du, m->dv, m->da, m->dfext, m->dfint})
+  AKB_CUDA(cudaMemcpyAsync(m->dpos, pos.data(), sizeof(int32_t) * E * nn, cudaMemcpyHostToDevice, s));
+  for (double *p : {m->dU[0], m->dU[1], m->dv, m->da, m->dfext, m->dfint})
     AKB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * N * d, s));
   AKB_CUDA(cudaMemsetAsync(m->dblocked, 0, N, s));
   AKB_CUDA(cudaMemsetAsync(m->dstatus, 0, sizeof(unsigned int), s));
@@ -663,7 +705,7 @@ int akb_model_get_fe_data(akb_model *m, int which, double *host, int64_t count) 
     const int64_t ue = m->perm[ie];
     for (int q = 0; q < m->nq; ++q)
       for (int64_t c = 0; c < comps; ++c)
-        host[(ue * m->nq + q) * comps + c] = soa[(size_t)c * EQ + ie * m->nq + q];
+        host[(ue * m->nq + q) * comps + c] = soa[(size_t)(q * comps + c) * m->E + ie];
   }
   return AKB_OK;
 }
@@ -673,12 +715,13 @@ int akb_model_get_stable_time_step(akb_model *m, double *dt) {
   if (!dt) return fail(AKB_EINVAL, "null argument");
   DevGeom g = m->geom();
   for (auto &mt : m->mats)
-    AKB_CUDA(launch_element_dt(g, mt.e_begin, mt.e_count, mt.celerity(), m->du, m->dscratch, m->stream));
+    AKB_CUDA(launch_element_dt(g, mt.e_begin, mt.e_count, mt.celerity(), m->u(), m->dscratch, m->stream));
   return reduce_to_host(m, m->dscratch, m->E, true, dt);
 }
 
 int akb_model_set_time_step(akb_model *m, double dt) {
   AKB_TRY(check_model(m, false));
+  if (dt != m->dt) m->predicted = false;
   m->dt = dt;
   return AKB_OK;
 }
@@ -701,6 +744,7 @@ int akb_model_set_nodal(akb_model *m, int field, const void *host, int64_t nbyte
         if (b[i * m->dim + c]) mask[i] |= (uint8_t)(1u << c);
     AKB_CUDA(cudaMemcpyAsync(m->dblocked, mask.data(), m->N, cudaMemcpyHostToDevice, m->stream));
     AKB_CUDA(cudaStreamSynchronize(m->stream));
+    m->predicted = false;
     return AKB_OK;
   }
   if (nbytes != nd * (int64_t)sizeof(double)) return fail(AKB_EINVAL, "size must be N*dim doubles");
@@ -708,10 +752,11 @@ int akb_model_set_nodal(akb_model *m, int field, const void *host, int64_t nbyte
   switch (field) {
   case AKB_DISPLACEMENT:
     AKB_TRY(snapshot_u(m));
-    dst = m->du;
+    dst = m->u();
+    m->predicted = false;
     break;
-  case AKB_VELOCITY: dst = m->dv; break;
-  case AKB_ACCELERATION: dst = m->da; break;
+  case AKB_VELOCITY: dst = m->dv; m->predicted = false; break;
+  case AKB_ACCELERATION: dst = m->da; m->predicted = false; break;
   case AKB_EXTERNAL_FORCE: dst = m->dfext; break;
   default: return fail(AKB_EINVAL, "field is read-only or unknown");
   }
@@ -747,7 +792,7 @@ int akb_model_get_nodal(akb_model *m, int field, void *host, int64_t nbytes) {
     return AKB_OK;
   }
   case AKB_CURRENT_POSITION: {
-    AKB_CUDA(cudaMemcpyAsync(out, m->du, nbytes, cudaMemcpyDeviceToHost, s));
+    AKB_CUDA(cudaMemcpyAsync(out, m->u(), nbytes, cudaMemcpyDeviceToHost, s));
     AKB_CUDA(cudaStreamSynchronize(s));
     for (int64_t k = 0; k < nd; ++k) out[k] = m->X[k] + out[k];
     return AKB_OK;
@@ -756,7 +801,7 @@ int akb_model_get_nodal(akb_model *m, int field, void *host, int64_t nbytes) {
   }
   const double *src = nullptr;
   switch (field) {
-  case AKB_DISPLACEMENT: src = m->du; break;
+  case AKB_DISPLACEMENT: src = m->u(); break;
   case AKB_VELOCITY: src = m->dv; break;
   case AKB_ACCELERATION: src = m->da; break;
   case AKB_EXTERNAL_FORCE: src = m->dfext; break;
@@ -772,7 +817,7 @@ int akb_model_nodal_device_pointer(akb_model *m, int field, void **p) {
   AKB_TRY(check_model(m, true));
   if (!p) return fail(AKB_EINVAL, "null argument");
   switch (field) {
-  case AKB_DISPLACEMENT: *p = m->du; break;
+  case AKB_DISPLACEMENT: *p = m->u(); break;
   case AKB_VELOCITY: *p = m->dv; break;
   case AKB_ACCELERATION: *p = m->da; break;
   case AKB_EXTERNAL_FORCE: *p = m->dfext; break;
@@ -835,24 +880,21 @@ int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t
   std::vector<double> soa((size_t)nqp * comps);
   AKB_CUDA(cudaMemcpyAsync(soa.data(), src, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, m->stream));
   AKB_CUDA(cudaStreamSynchronize(m->stream));
-  for (int64_t q = 0; q < nqp; ++q)
-    for (int c = 0; c < comps; ++c) host[q * comps + c] = soa[(size_t)c * nqp + q];
+  // device [q][comp][ne] -> reference order [element][q][comp]
+  const int64_t ne = mt.e_count;
+  for (int64_t le = 0; le < ne; ++le)
+    for (int q = 0; q < m->nq; ++q)
+      for (int c = 0; c < comps; ++c)
+        host[(le * m->nq + q) * comps + c] = soa[(size_t)(q * comps + c) * ne + le];
   return AKB_OK;
 }
 
 int akb_model_solve_step(akb_model *m, int64_t nsteps) {
   AKB_TRY(check_model(m, true));
   if (nsteps < 0) return fail(AKB_EINVAL, "negative step count");
-  DevGeom g = m->geom();
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
-  for (int64_t s = 0; s < nsteps; ++s) {
-    AKB_CUDA(launch_predict(g, m->dblocked, m->du, m->dv, m->da, m->dt, m->stream));
-    AKB_TRY(element_forces(m, true));
-    AKB_TRY(node_update(m, true));
-    if (any_plastic) m->cur = 1 - m->cur;
-    m->steps_done++;
-  }
+  for (int64_t s = 0; s < nsteps; ++s) AKB_TRY(one_step(m, any_plastic));
   if (nsteps > 0) {
     m->forces_evaluated = true;
     m->snap_valid = false;
@@ -885,23 +927,14 @@ int akb_model_profile_steps(akb_model *m, int64_t nsteps, double *total_ms, doub
   if (!total_ms || !phase_ms || nsteps < 1 || nsteps > 4096) return fail(AKB_EINVAL, "bad argument");
   std::vector<cudaEvent_t> ev((size_t)nsteps * 3 + 1);
   for (auto &x : ev) AKB_CUDA(cudaEventCreate(&x));
-  DevGeom g = m->geom();
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
   int rc = AKB_OK;
   AKB_CUDA(cudaEventRecord(ev[0], m->stream));
   for (int64_t s = 0; s < nsteps && rc == AKB_OK; ++s) {
-    cudaError_t e = launch_predict(g, m->dblocked, m->du, m->dv, m->da, m->dt, m->stream);
-    if (e != cudaSuccess) { rc = fail(AKB_ECUDA, cudaGetErrorString(e)); break; }
-    cudaEventRecord(ev[s * 3 + 1], m->stream);
-    rc = element_forces(m, true);
-    if (rc != AKB_OK) break;
-    cudaEventRecord(ev[s * 3 + 2], m->stream);
-    rc = node_update(m, true);
-    if (rc != AKB_OK) break;
-    cudaEventRecord(ev[s * 3 + 3], m->stream);
-    if (any_plastic) m->cur = 1 - m->cur;
-    m->steps_done++;
+    // phases: [predictor if needed], element forces, node update (+ predictor)
+    rc = one_step(m, any_plastic, ev[s * 3 + 1], ev[s * 3 + 2]);
+    if (rc == AKB_OK) cudaEventRecord(ev[s * 3 + 3], m->stream);
   }
   cudaError_t e = cudaStreamSynchronize(m->stream);
   if (rc == AKB_OK && e == cudaSuccess) {

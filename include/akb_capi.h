@@ -158,7 +158,10 @@ int akb_model_get_time_step(const akb_model *model, double *dt);
  * nbytes must be N*dim*sizeof(double), or N*dim for AKB_BLOCKED_DOFS */
 int akb_model_set_nodal(akb_model *model, int field, const void *host, int64_t nbytes);
 int akb_model_get_nodal(akb_model *model, int field, void *host, int64_t nbytes);
-/* device address of a nodal array, for callers that keep data on the GPU */
+/* device address of a nodal array, for callers that keep data on the GPU.
+ * The displacement alternates between two buffers (the step writes the next
+ * step's prediction into the other one): its address is valid until the next
+ * akb_model_solve_step; the other arrays keep their address. */
 int akb_model_nodal_device_pointer(akb_model *model, int field, void **device_ptr);
 
 /* Material::getStress/getGradU/getInternal<Real>(id)(type): count is the
@@ -180,8 +183,10 @@ int akb_model_get_energy(akb_model *model, const char *energy_id, double *value)
  * recorded on the model's stream and returns the elapsed milliseconds */
 int akb_model_time_steps(akb_model *model, int64_t nsteps, double *elapsed_ms);
 /* the same with an event between the phases of every step; phase_ms[0..2]
- * receive the summed durations of predictor, element forces (all materials)
- * and node update (gather + corrector); nsteps <= 4096 */
+ * receive the summed durations of the standalone predictor (only run when the
+ * host changed u, v, a, the blocked dofs or dt since the last step), element
+ * forces (all materials) and node update (gather, corrector and the next
+ * step's predictor); nsteps <= 4096 */
 int akb_model_profile_steps(akb_model *model, int64_t nsteps, double *total_ms,
                             double *phase_ms);
 /* device status word: bit 0 = non-finite acceleration seen since the last
