@@ -24,12 +24,30 @@ namespace akb {
 constexpr int kMaxNQ = 8;
 constexpr int kMaxNN = 8;
 
-// natural-coordinate tables evaluated on the host
+// natural-coordinate tables evaluated on the host (passed by value: they sit
+// in the kernel-parameter constant bank)
 struct QuadTable {
   double dnds[kMaxNQ * 3 * kMaxNN];  // [q][k][a]
   double N[kMaxNQ * kMaxNN];         // [q][a]
   double w[kMaxNQ];
+  float fdnds[kMaxNQ * 3 * kMaxNN];  // FP32 copies for the mixed path
+  float fw[kMaxNQ];
 };
+
+// elemental-force slots: the D components of one (element, node) force,
+// stored contiguously at slot p (D values, no padding)
+template <int D> struct SlotStride { static constexpr int value = D; };
+
+template <int D, class RT, class V>
+__device__ __forceinline__ void store_slot(RT *re, int64_t p, const V *v) {
+#pragma unroll
+  for (int i = 0; i < D; ++i) re[p * D + i] = (RT)v[i];
+}
+template <int D, class RT>
+__device__ __forceinline__ void load_slot(const RT *re, int64_t p, double *v) {
+#pragma unroll
+  for (int i = 0; i < D; ++i) v[i] = (double)__ldg(re + p * D + i);
+}
 
 // per-material plastic internals, [q][comp][ne], ping-pong prev/cur
 struct PlasticState {
@@ -416,11 +434,82 @@ __global__ void __launch_bounds__(kPeThreads)
   }
   // elemental force of node a goes to its position in the node CSR
 #pragma unroll
-  for (int a = 0; a < NN; ++a) {
-    const int64_t p = pos[(int64_t)a * E + e];
+  for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
+}
+
+// Mixed path: FP32 element math with the shape derivatives recomputed from
+// the gathered nodal coordinates instead of streamed from HBM.  Per point:
+// J = dN/ds X^T, dN/dx = J^-1 dN/ds, w = det J * w_q (the arithmetic of
+// k_precompute, in FP32, with coordinates and displacements taken relative
+// to the element's first node -- dN/ds sums to zero over the nodes, so the
+// Jacobian and the gradient are unchanged in exact arithmetic).
+template <int D, int NN, int NQ, int LAW>
+__global__ void __launch_bounds__(kPeThreads)
+    k_element_forces_geo(int64_t e_begin, int64_t e_count, int64_t E,
+                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                         const double *__restrict__ X, QuadTable tab,
+                         const double *__restrict__ u, MatParams mp, PlasticState ps,
+                         float *__restrict__ re) {
+  constexpr int ND = NN * D;
+  const int64_t le = (int64_t)blockIdx.x * kPeThreads + threadIdx.x;
+  if (le >= e_count) return;
+  const int64_t e = e_begin + le;
+  float xe[ND], ue[ND];
+  double x0[D], u0[D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) re[p * D + i] = (RT)r[a * D + i];
+  for (int a = 0; a < NN; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const double x = X[node * D + i], uu = u[node * D + i];
+      if (a == 0) {
+        x0[i] = x;
+        u0[i] = uu;
+      }
+      xe[a * D + i] = (float)(x - x0[i]);
+      ue[a * D + i] = (float)(uu - u0[i]);
+    }
   }
+  float r[ND];
+#pragma unroll 1
+  for (int q = 0; q < NQ; ++q) {
+    const float *dn = &tab.fdnds[q * 3 * kMaxNN];
+    float J[D * D], Ji[D * D];
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        float s = dn[k * kMaxNN] * xe[j];
+#pragma unroll
+        for (int a = 1; a < NN; ++a) s += dn[k * kMaxNN + a] * xe[a * D + j];
+        J[k + D * j] = s;
+      }
+    float det;
+    if constexpr (D == 3) {
+      det = det3(J);
+      inv3(J, Ji);
+    } else {
+      det = det2(J);
+      inv2(J, Ji);
+    }
+    float b[ND];
+#pragma unroll
+    for (int a = 0; a < NN; ++a)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        float s = Ji[j] * dn[a];
+#pragma unroll
+        for (int k = 1; k < D; ++k) s += Ji[j + D * k] * dn[k * kMaxNN + a];
+        b[a * D + j] = s;
+      }
+    const float w = det * tab.fw[q];
+    float t[ND];
+    element_law<D, NN, LAW, float, true>(ue, b, w, mp, ps, e_count, le, q, t);
+#pragma unroll
+    for (int c = 0; c < ND; ++c) r[c] = (q == 0) ? t[c] : r[c] + t[c];
+  }
+#pragma unroll
+  for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
 }
 
 // FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q
@@ -476,7 +565,7 @@ __global__ void __launch_bounds__(32 * NQ)
 #pragma unroll
       for (int qq = 1; qq < NQ; ++qq) s = s + red[qq][q][lane];
       const int a = c / D;
-      re[(int64_t)pos[(int64_t)a * E + e] * D + (c - a * D)] = s;
+      re[(int64_t)pos[(int64_t)a * E + e] * SlotStride<D>::value + (c - a * D)] = s;
     }
     __syncthreads();
   }
@@ -490,12 +579,19 @@ __global__ void __launch_bounds__(32 * NQ)
 //   x = r / M; v += (dt/2) x; a += x     (non_linear_solver_lumped.cc:76-87,
 //                                         newmark-beta.cc:163-197)
 // The displacement coefficient of the corrector is alpha*beta*dt^2 = 0.
-// The elemental forces are stored in node-CSR order, so node i reads
-// re[ptr[i] .. ptr[i+1]) contiguously, in increasing slot order.
-// mode 0: internal force only; 1: + residual, solve and corrector, where the
-// predicted velocity v + dt a of the reference predictor is formed here;
-// 2: + the predictor of the next step, u_next = u + (dt v + (dt/2)(dt a)).
+// The elemental forces are stored in node-CSR order, so node i reads slots
+// ptr[i] .. ptr[i+1] contiguously, in increasing slot order.
+// flags: NU_CORRECT   residual, solve and corrector; the predicted velocity
+//                     v + dt a of the reference predictor is formed here
+//        NU_PREDICT   + the predictor of the next step,
+//                     u_next = u + (dt v + (dt/2)(dt a))
+//        NU_FINT      store the internal force (else it is gathered again on
+//                     request by a flags == NU_FINT launch)
+//        NU_FEXT_ZERO the external force is identically zero: not read
+//                     (0 + f_ext + f_int == f_int)
 // KAHAN selects a compensated FP64 sum (mixed path).
+enum { NU_CORRECT = 1, NU_PREDICT = 2, NU_FINT = 4, NU_FEXT_ZERO = 8 };
+
 template <int D, class RT, bool KAHAN>
 __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               const RT *__restrict__ re, const double *__restrict__ fext,
@@ -503,7 +599,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               const uint8_t *__restrict__ blocked, double *__restrict__ fint,
                               double *__restrict__ a, double *__restrict__ v,
                               const double *__restrict__ u, double *__restrict__ u_next,
-                              double dt, int mode, unsigned int *__restrict__ status) {
+                              double dt, int flags, unsigned int *__restrict__ status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[D], comp[D];
@@ -513,10 +609,13 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
     comp[c] = 0.;
   }
   const int32_t p0 = ptr[i], p1 = ptr[i + 1];
+#pragma unroll 4
   for (int32_t p = p0; p < p1; ++p) {
+    double rv[D];
+    load_slot<D>(re, p, rv);
 #pragma unroll
     for (int c = 0; c < D; ++c) {
-      const double val = -1. * (double)re[(int64_t)p * D + c];
+      const double val = -1. * rv[c];
       if constexpr (KAHAN) {
         const double y = val - comp[c];
         const double tt = acc[c] + y;
@@ -527,6 +626,11 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
       }
     }
   }
+  if (flags & NU_FINT) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) fint[i * D + c] = acc[c];
+  }
+  if (!(flags & NU_CORRECT)) return;
   const double m = mass[i];
   const uint8_t bl = blocked[i];
   const double hdt = .5 * dt;
@@ -534,14 +638,17 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
 #pragma unroll
   for (int c = 0; c < D; ++c) {
     const int64_t k = i * D + c;
-    fint[k] = acc[c];
-    if (mode == 0) continue;
     const bool free_dof = !((bl >> c) & 1);
     const double ak = a[k];
     double vk = v[k];
     if (free_dof) vk = vk + dt * ak;  // predicted velocity (newmark-beta.cc:69)
-    double r = 0. + 1. * fext[k];
-    r = r + 1. * acc[c];
+    double r;
+    if (flags & NU_FEXT_ZERO) {
+      r = acc[c];
+    } else {
+      r = 0. + 1. * fext[k];
+      r = r + 1. * acc[c];
+    }
     const double ma = 0. + -1. * ak;
     r = r + m * ma;
     double an = ak;
@@ -553,7 +660,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
       a[k] = an;
       bad |= !isfinite(an);
     }
-    if (mode == 2) {
+    if (flags & NU_PREDICT) {
       const double uk = u[k];
       u_next[k] = free_dof ? uk + (dt * vk + hdt * (dt * an)) : uk;
     }

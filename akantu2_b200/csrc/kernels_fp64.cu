@@ -80,14 +80,14 @@ cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, in
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
-                                    double dt, int mode, unsigned int *status, cudaStream_t s) {
+                                    double dt, int flags, unsigned int *status, cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
     k_node_update<3, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, mode, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, flags, status);
   else
     k_node_update<2, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, mode, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, flags, status);
   return cudaGetLastError();
 }
 

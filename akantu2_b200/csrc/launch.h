@@ -45,20 +45,24 @@ cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, in
                                        const double *B, const double *wJ, const double *u,
                                        const MatParams &mp, const PlasticState &ps,
                                        double *re, cudaStream_t s);
+// mixed path: 3D elements recompute their shape derivatives in FP32 from g.X
+// and the table; 2D elements stream FP32 copies (fB, fwJ) of the precomputed
+// ones (their state traffic dominates, the recomputation would not pay)
 cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, int64_t ne,
-                                        const float *B, const float *wJ, const double *u,
+                                        const QuadTable &tab, const float *fB,
+                                        const float *fwJ, const double *u,
                                         const MatParams &mp, const PlasticState &ps,
                                         float *re, cudaStream_t s);
-// mode 0: internal force only; 1: + corrector; 2: + predictor of the next
-// step from u into u_next
+// flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
+// the predictor of the next step reads u and writes u_next
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
-                                    double dt, int mode, unsigned int *status, cudaStream_t s);
+                                    double dt, int flags, unsigned int *status, cudaStream_t s);
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,
-                                     double *u_next, double dt, int mode,
+                                     double *u_next, double dt, int flags,
                                      unsigned int *status, cudaStream_t s);
 
 // ---- fields and energies ---------------------------------------------------

@@ -142,6 +142,8 @@ void fill_tables(int et, int rule, QuadTable &tab, int &nq) {
       r1[3] = -4 * c1; r1[4] = 4 * c1; r1[5] = 4 * (c0 - c2);
     }
   }
+  for (int k = 0; k < kMaxNQ * 3 * kMaxNN; ++k) tab.fdnds[k] = (float)tab.dnds[k];
+  for (int q = 0; q < kMaxNQ; ++q) tab.fw[q] = (float)tab.w[q];
 }
 
 }  // namespace
@@ -162,13 +164,16 @@ struct akb_model {
   cudaStream_t stream = nullptr;
   // device arrays
   double *dX = nullptr, *dB = nullptr, *dwJ = nullptr;
-  float *fB = nullptr, *fwJ = nullptr;
+  float *fB = nullptr, *fwJ = nullptr;  // FP32 copies (mixed path, 2D elements)
+  QuadTable tab;  // quadrature tables of the element type
   int32_t *dconn = nullptr, *dptr = nullptr, *dent = nullptr, *dpos = nullptr;
   // displacement ping-pong: dU[ucur] is the model's u, dU[1 - ucur] the
   // prediction of the next step (valid when `predicted`)
   double *dU[2] = {nullptr, nullptr};
   int ucur = 0;
   bool predicted = false;
+  bool fint_valid = true;  // dfint holds the internal force of the last evaluation
+  bool fext_zero = true;   // the external force is identically zero
   double *dv = nullptr, *da = nullptr, *dfext = nullptr, *dfint = nullptr;
   double *dmass = nullptr, *dusnap = nullptr;
   uint8_t *dblocked = nullptr;
@@ -312,8 +317,8 @@ int element_forces(akb_model *m, bool in_step) {
     PlasticState ps = plastic_state(m, mt, in_step);
     cudaError_t e;
     if (m->precision == AKB_PRECISION_MIXED)
-      e = launch_element_forces_mixed(g, mt.law, mt.e_begin, mt.e_count, m->fB, m->fwJ, u,
-                                      mt.params(), ps, (float *)m->dre, m->stream);
+      e = launch_element_forces_mixed(g, mt.law, mt.e_begin, mt.e_count, m->tab, m->fB, m->fwJ,
+                                      u, mt.params(), ps, (float *)m->dre, m->stream);
     else
       e = launch_element_forces_fp64(g, mt.law, mt.e_begin, mt.e_count, m->dB, m->dwJ, u,
                                      mt.params(), ps, (double *)m->dre, m->stream);
@@ -322,24 +327,36 @@ int element_forces(akb_model *m, bool in_step) {
   return AKB_OK;
 }
 
-// correct == false: internal force only.  correct == true: corrector, then
-// the predictor of the next step from the new displacement u_pred into the
-// other buffer (which held the displacement of the previous step)
+// node update after the element forces.  In a step (correct == true): the
+// corrector, then the predictor of the next step from the new displacement
+// u_pred into the other buffer (which held the displacement of the previous
+// step); the internal force is only gathered when asked for (ensure_fint).
+// Standalone (correct == false): the internal force only.
 int node_update(akb_model *m, bool correct) {
   DevGeom g = m->geom();
   cudaError_t e;
-  const int mode = correct ? 2 : 0;
+  int flags = correct ? (NU_CORRECT | NU_PREDICT) : NU_FINT;
+  if (correct && m->fext_zero) flags |= NU_FEXT_ZERO;
   const double *u = m->u_pred();
   double *u_next = m->u();
   if (m->precision == AKB_PRECISION_MIXED)
     e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass, m->dblocked,
-                                 m->dfint, m->da, m->dv, u, u_next, m->dt, mode, m->dstatus,
+                                 m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
                                  m->stream);
   else
     e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass, m->dblocked,
-                                m->dfint, m->da, m->dv, u, u_next, m->dt, mode, m->dstatus,
+                                m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
                                 m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
+  m->fint_valid = !correct;
+  return AKB_OK;
+}
+
+// the internal force of the last force evaluation, gathered again from the
+// elemental forces it left in the slot array
+int ensure_fint(akb_model *m) {
+  if (m->fint_valid || !m->forces_evaluated) return AKB_OK;
+  AKB_TRY(node_update(m, false));
   return AKB_OK;
 }
 
@@ -540,7 +557,7 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
 
   const int nn = m->nn, d = m->dim;
   const int64_t E = m->E, N = m->N;
-  QuadTable tab;
+  QuadTable &tab = m->tab;
   fill_tables(m->et, m->rule, tab, m->nq);
   const int nq = m->nq;
 
@@ -587,8 +604,9 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_TRY(m->alloc(p, sizeof(double) * N * d));
   AKB_TRY(m->alloc(&m->dmass, sizeof(double) * N));
   AKB_TRY(m->alloc(&m->dblocked, N));
+  // one padded slot per (element, node): 3D slots hold 4 values, 2D slots 2
   const size_t re_bytes = (precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double)) *
-                          (size_t)E * nn * d;
+                          (size_t)E * nn * (d == 3 ? 4 : 2);
   AKB_TRY(m->alloc(&m->dre, std::max(re_bytes, sizeof(double) * (size_t)E * nn)));
   AKB_TRY(m->alloc(&m->dscratch, sizeof(double) * std::max<int64_t>(std::max(E, N), 1)));
   AKB_TRY(m->alloc(&m->dpartials, sizeof(double) * kReducePartials));
@@ -623,7 +641,7 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   for (auto &mt : m->mats)
     AKB_CUDA(launch_mass_elem(g, mt.e_begin, mt.e_count, mt.rho, tab, m->dwJ, me, s));
   AKB_CUDA(launch_gather_scalar(g, me, m->dmass, s));
-  if (precision == AKB_PRECISION_MIXED) {
+  if (precision == AKB_PRECISION_MIXED && d == 2) {
     AKB_TRY(m->alloc(&m->fB, sizeof(float) * E * nq * nn * d));
     AKB_TRY(m->alloc(&m->fwJ, sizeof(float) * E * nq));
     AKB_CUDA(launch_to_float(m->dB, m->fB, E * nq * nn * d, s));
@@ -757,7 +775,11 @@ int akb_model_set_nodal(akb_model *m, int field, const void *host, int64_t nbyte
     break;
   case AKB_VELOCITY: dst = m->dv; m->predicted = false; break;
   case AKB_ACCELERATION: dst = m->da; m->predicted = false; break;
-  case AKB_EXTERNAL_FORCE: dst = m->dfext; break;
+  case AKB_EXTERNAL_FORCE: {
+    dst = m->dfext;
+    const double *h = (const double *)host;
+    m->fext_zero = std::all_of(h, h + nd, [](double x) { return x == 0.; });
+  } break;
   default: return fail(AKB_EINVAL, "field is read-only or unknown");
   }
   AKB_CUDA(cudaMemcpyAsync(dst, host, nbytes, cudaMemcpyHostToDevice, m->stream));
@@ -805,7 +827,10 @@ int akb_model_get_nodal(akb_model *m, int field, void *host, int64_t nbytes) {
   case AKB_VELOCITY: src = m->dv; break;
   case AKB_ACCELERATION: src = m->da; break;
   case AKB_EXTERNAL_FORCE: src = m->dfext; break;
-  case AKB_INTERNAL_FORCE: src = m->dfint; break;
+  case AKB_INTERNAL_FORCE:
+    AKB_TRY(ensure_fint(m));
+    src = m->dfint;
+    break;
   default: return fail(AKB_EINVAL, "unknown nodal field");
   }
   AKB_CUDA(cudaMemcpyAsync(out, src, nbytes, cudaMemcpyDeviceToHost, s));
@@ -821,7 +846,11 @@ int akb_model_nodal_device_pointer(akb_model *m, int field, void **p) {
   case AKB_VELOCITY: *p = m->dv; break;
   case AKB_ACCELERATION: *p = m->da; break;
   case AKB_EXTERNAL_FORCE: *p = m->dfext; break;
-  case AKB_INTERNAL_FORCE: *p = m->dfint; break;
+  case AKB_INTERNAL_FORCE:
+    AKB_TRY(ensure_fint(m));
+    AKB_CUDA(cudaStreamSynchronize(m->stream));
+    *p = m->dfint;
+    break;
   default: return fail(AKB_EINVAL, "no device pointer for this field");
   }
   return AKB_OK;
@@ -986,6 +1015,7 @@ int akb_model_get_energy(akb_model *m, const char *id, double *value) {
     return AKB_OK;
   }
   if (which == "external work") {
+    AKB_TRY(ensure_fint(m));
     AKB_CUDA(launch_work_terms(g, m->dfext, m->dfint, m->dv, m->dblocked, m->dscratch, m->stream));
     double s = 0.;
     AKB_TRY(reduce_to_host(m, m->dscratch, m->N, false, &s));
