@@ -89,6 +89,7 @@ def lib():
         "akb_model_assemble_internal_forces": (c_int, [vp]),
         "akb_model_get_energy": (c_int, [vp, ctypes.c_char_p, ctypes.POINTER(c_dbl)]),
         "akb_model_get_status": (c_int, [vp, ctypes.POINTER(c_int)]),
+        "akb_stable_time_step_noalloc": (c_int, [c_int, vp, vp, vp, i64, c_dbl, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -193,6 +193,32 @@ int akb_model_profile_steps(akb_model *model, int64_t nsteps, double *total_ms,
  * call (the flag is cleared by reading it) */
 int akb_model_get_status(akb_model *model, int *flags);
 
+/* ---- stable time step without allocation -------------------------------- */
+/* This entry point has no counterpart in the reference.  It computes the
+ * same value as akb_model_get_stable_time_step for the elements of one
+ * material, for callers that cannot let the library call cudaMalloc: an
+ * application whose device memory all comes from its own pool or arena, or
+ * code computing the time step inside a loop where runtime allocation is not
+ * allowed.  All arguments are device pointers owned by the caller:
+ *   nodes, displacement  double [N][dim]; connectivity int32 [E][n] (the
+ *   reference's node order); dt_out one double, receives min_e h_e / celerity
+ *   (DBL_MAX when nb_elements == 0); stream a cudaStream_t (NULL: default).
+ * The work is enqueued on `stream`; synchronise it before reading dt_out.
+ * The scratch (per-element values and reduction partials) is a file-scope
+ * device array of AKB_NOALLOC_MAX_ELEMENTS + 1024 doubles (8 MiB) that every
+ * GPU loading the library holds until the process exits; larger element
+ * counts are rejected with AKB_EINVAL.  Every call shares that array and
+ * overwrites all of it that it reads, so nothing carries over between calls,
+ * but calls that overlap on the GPU (different streams, threads or
+ * processes sharing the module) race on it.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device
+ * current); make that first call before any stream capture begins. */
+#define AKB_NOALLOC_MAX_ELEMENTS (1 << 20)
+int akb_stable_time_step_noalloc(int element_type, const double *nodes,
+                                 const double *displacement, const int32_t *connectivity,
+                                 int64_t nb_elements, double celerity, double *dt_out,
+                                 void *stream);
+
 #ifdef __cplusplus
 }
 #endif
