@@ -1,0 +1,433 @@
+/*
+ * akantu_b200/solid_mechanics_model.hh -- C++ drop-in API of the explicit
+ * lumped-mass step, header-only over the C ABI (akb_capi.h, libakb.so).
+ *
+ * Mirrors the reference surface used by explicit drivers
+ * (src/model/solid_mechanics/solid_mechanics_model.hh:61-321,
+ *  src/model/model.hh:74-131, src/mesh/mesh.hh:121-281,
+ *  src/io/parser/parser.hh:344-432, src/common/aka_common.hh:48,662):
+ *
+ *   initialize("material.dat", argc, argv);
+ *   Mesh mesh(3); mesh.read("bar.msh");
+ *   SolidMechanicsModel model(mesh);
+ *   model.initFull(_analysis_method = _explicit_lumped_mass);
+ *   model.setTimeStep(0.8 * model.getStableTimeStep());
+ *   Array<Real> & u = model.getDisplacement();   // host view, edit in place
+ *   for (...) model.solveStep();
+ *
+ * The nodal arrays live on the GPU.  The getters return host arrays that
+ * the model refreshes after a step and uploads again before the next step
+ * when the caller may have changed them (any non-const getter call marks the
+ * array), which gives the reference's "edit the array between steps"
+ * semantics.  Errors throw akantu_b200::Exception with the library message.
+ */
+#ifndef AKANTU_B200_SOLID_MECHANICS_MODEL_HH_
+#define AKANTU_B200_SOLID_MECHANICS_MODEL_HH_
+
+#include <cstdint>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../akb_capi.h"
+
+namespace akantu_b200 {
+
+using Real = double;
+using Int = int64_t;
+using Idx = int32_t;
+using ID = std::string;
+
+class Exception : public std::runtime_error {
+public:
+  Exception(int code, const std::string &msg) : std::runtime_error(msg), code_(code) {}
+  int code() const { return code_; }
+
+private:
+  int code_;
+};
+
+inline void check(int rc) {
+  if (rc != AKB_OK) throw Exception(rc, akb_last_error());
+}
+
+/* ---- element types, analysis method, axes -------------------------------- */
+enum ElementType {
+  _tetrahedron_4 = AKB_TETRAHEDRON_4,
+  _hexahedron_8 = AKB_HEXAHEDRON_8,
+  _triangle_6 = AKB_TRIANGLE_6,
+  _not_defined = -1
+};
+enum AnalysisMethod { _explicit_lumped_mass = AKB_EXPLICIT_LUMPED_MASS };
+enum SpatialDirection { _x = 0, _y = 1, _z = 2 };
+constexpr Int _all_dimensions = -1;
+
+// named argument of initFull: model.initFull(_analysis_method = _explicit_lumped_mass)
+struct AnalysisMethodArg {
+  AnalysisMethod method;
+  int precision;
+};
+struct AnalysisMethodTag {
+  AnalysisMethodArg operator=(AnalysisMethod m) const { return {m, AKB_PRECISION_FP64}; }
+};
+inline constexpr AnalysisMethodTag _analysis_method{};
+
+/* ---- Array: row-major tuples (size x nb_component), src/common/aka_array.hh */
+template <class T> class Array {
+public:
+  Array(Int size = 0, Int nb_component = 1, T value = T())
+      : n_(size), c_(nb_component), v_(new T[size * nb_component]) {
+    set(value);
+  }
+  Array(const Array &o) : n_(o.n_), c_(o.c_), v_(new T[o.n_ * o.c_]) {
+    std::copy(o.data(), o.data() + n_ * c_, data());
+  }
+  Array(Array &&) = default;
+  Array &operator=(const Array &o) {
+    if (this != &o) {
+      Array tmp(o);
+      *this = std::move(tmp);
+    }
+    return *this;
+  }
+  Array &operator=(Array &&) = default;
+  Int size() const { return n_; }
+  Int getNbComponent() const { return c_; }
+  T &operator()(Int i, Int c = 0) { return v_[i * c_ + c]; }
+  const T &operator()(Int i, Int c = 0) const { return v_[i * c_ + c]; }
+  T *data() { return v_.get(); }
+  const T *data() const { return v_.get(); }
+  void resize(Int size) {
+    std::unique_ptr<T[]> nv(new T[size * c_]());
+    std::copy(data(), data() + std::min(size, n_) * c_, nv.get());
+    v_ = std::move(nv);
+    n_ = size;
+  }
+  void set(T value) {
+    if (n_ * c_ > 0) std::fill(data(), data() + n_ * c_, value);
+  }
+  void zero() { set(T()); }
+
+private:
+  Int n_, c_;
+  std::unique_ptr<T[]> v_;
+};
+
+/* ---- static parser (getStaticParser().parse / initialize) --------------- */
+class Parser {
+public:
+  void parse(const std::string &path) {
+    std::ifstream f(path);
+    if (!f) throw Exception(AKB_EIO, "cannot open " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    texts_.push_back(ss.str());
+  }
+  void parseText(const std::string &text) { texts_.push_back(text); }
+  void clear() { texts_.clear(); }
+  const std::vector<std::string> &texts() const { return texts_; }
+
+private:
+  std::vector<std::string> texts_;
+};
+
+inline Parser &getStaticParser() {
+  static Parser parser;
+  return parser;
+}
+
+inline void initialize(const std::string &input_file, int /*argc*/ = 0, char ** /*argv*/ = nullptr) {
+  if (!input_file.empty()) getStaticParser().parse(input_file);
+}
+
+/* ---- Mesh ------------------------------------------------------------------ */
+class Mesh {
+public:
+  explicit Mesh(Int spatial_dimension) : dim_(spatial_dimension), nodes_(0, spatial_dimension) {}
+
+  // Mesh::read for gmsh 2.x ASCII files: the elements of the type matching
+  // the dimension (_triangle_6 in 2D; _hexahedron_8, else _tetrahedron_4 in 3D)
+  void read(const std::string &path, ElementType type = _not_defined) {
+    std::vector<ElementType> types;
+    if (type != _not_defined) types = {type};
+    else if (dim_ == 2) types = {_triangle_6};
+    else types = {_hexahedron_8, _tetrahedron_4};
+    for (ElementType t : types) {
+      akb_mesh *m = nullptr;
+      check(akb_mesh_read_msh(path.c_str(), (int)dim_, t, &m));
+      int64_t nn = 0, ne = 0;
+      int npe = 0;
+      check(akb_mesh_sizes(m, &nn, &ne, &npe));
+      if (ne == 0 && types.size() > 1 && t != types.back()) {
+        akb_mesh_free(m);
+        continue;
+      }
+      nodes_ = Array<Real>(nn, dim_);
+      conn_ = Array<Idx>(ne, npe);
+      tags_ = Array<Idx>(ne, 1);
+      check(akb_mesh_copy(m, nodes_.data(), conn_.data(), tags_.data()));
+      akb_mesh_free(m);
+      type_ = t;
+      return;
+    }
+  }
+
+  void setElements(ElementType type, const Array<Real> &nodes, const Array<Idx> &conn) {
+    type_ = type;
+    nodes_ = nodes;
+    conn_ = conn;
+    tags_ = Array<Idx>(conn.size(), 1);
+  }
+
+  Int getSpatialDimension() const { return dim_; }
+  Int getNbNodes() const { return nodes_.size(); }
+  Int getNbElement(ElementType = _not_defined) const { return conn_.size(); }
+  ElementType getElementType() const { return type_; }
+  Array<Real> &getNodes() { return nodes_; }
+  const Array<Real> &getNodes() const { return nodes_; }
+  const Array<Idx> &getConnectivity(ElementType = _not_defined) const { return conn_; }
+  const Array<Idx> &getPhysicalTags() const { return tags_; }
+
+  // named node groups (src/mesh/group_manager.hh), used by applyBC
+  void createNodeGroup(const ID &name, const std::vector<Idx> &nodes) {
+    groups_[name] = std::set<Idx>(nodes.begin(), nodes.end());
+  }
+  const std::set<Idx> &getNodeGroup(const ID &name) const { return groups_.at(name); }
+
+private:
+  Int dim_;
+  ElementType type_ = _not_defined;
+  Array<Real> nodes_;
+  Array<Idx> conn_{0, 4}, tags_{0, 1};
+  std::map<ID, std::set<Idx>> groups_;
+};
+
+namespace BC {
+namespace Dirichlet {
+// BC::Dirichlet::FixedValue(value, axis)
+// (boundary_condition_functor_inline_impl.hh:53-61)
+struct FixedValue {
+  FixedValue(Real v, SpatialDirection ax = _x) : value(v), axis(ax) {}
+  Real value;
+  SpatialDirection axis;
+};
+}  // namespace Dirichlet
+}  // namespace BC
+
+class SolidMechanicsModel;
+
+/* ---- Material view ---------------------------------------------------------- */
+class Material {
+public:
+  Material(SolidMechanicsModel &model, int index) : model_(&model), index_(index) {}
+  inline Real get(const ID &param) const;
+  Real getRho() const { return get("rho"); }
+  inline ID getName() const;
+  // quadrature-point internals, material-local element order, [nq][dim*dim]
+  inline Array<Real> getStress(ElementType = _not_defined);
+  inline Array<Real> getGradU(ElementType = _not_defined);
+  inline Array<Real> getInternal(const ID &name, ElementType = _not_defined);
+
+private:
+  inline Array<Real> qp(int field);
+  SolidMechanicsModel *model_;
+  int index_;
+};
+
+/* ---- SolidMechanicsModel ------------------------------------------------- */
+class SolidMechanicsModel {
+public:
+  explicit SolidMechanicsModel(Mesh &mesh, Int dim = _all_dimensions,
+                               const ID &id = "solid_mechanics_model")
+      : mesh_(mesh), dim_(dim == _all_dimensions ? mesh.getSpatialDimension() : dim), id_(id) {
+    check(akb_model_create((int)dim_, mesh.getElementType(), mesh.getNodes().data(),
+                           mesh.getNbNodes(), mesh.getConnectivity().data(),
+                           mesh.getNbElement(), &h_));
+  }
+  ~SolidMechanicsModel() {
+    if (h_) akb_model_destroy(h_);
+  }
+  SolidMechanicsModel(const SolidMechanicsModel &) = delete;
+  SolidMechanicsModel &operator=(const SolidMechanicsModel &) = delete;
+
+  void initFull(AnalysisMethodArg arg = {_explicit_lumped_mass, AKB_PRECISION_FP64}) {
+    for (const auto &text : getStaticParser().texts())
+      check(akb_model_load_materials(h_, text.c_str()));
+    check(akb_model_init_full(h_, arg.method, arg.precision));
+  }
+  // FP32 element math with FP64 nodal state (see akb_precision)
+  void initFullMixedPrecision() { check(akb_model_load_and_init_mixed()); }
+
+  Real getStableTimeStep() {
+    syncUp();
+    Real dt = 0;
+    check(akb_model_get_stable_time_step(h_, &dt));
+    return dt;
+  }
+  void setTimeStep(Real dt, const ID & = "") { check(akb_model_set_time_step(h_, dt)); }
+  Real getTimeStep(const ID & = "") const {
+    Real dt = 0;
+    check(akb_model_get_time_step(h_, &dt));
+    return dt;
+  }
+
+  // ModelSolver::solveStep; nsteps > 1 enqueues several steps at once
+  void solveStep(const ID & = "", Int nsteps = 1) {
+    syncUp();
+    check(akb_model_solve_step(h_, nsteps));
+    mirrors_.clear();
+    blocked_.reset();
+  }
+
+  Array<Real> &getDisplacement() { return nodal(AKB_DISPLACEMENT, true); }
+  Array<Real> &getVelocity() { return nodal(AKB_VELOCITY, true); }
+  Array<Real> &getAcceleration() { return nodal(AKB_ACCELERATION, true); }
+  Array<Real> &getExternalForce() { return nodal(AKB_EXTERNAL_FORCE, true); }
+  const Array<Real> &getInternalForce() {
+    syncUp();
+    return nodal(AKB_INTERNAL_FORCE, false);
+  }
+  const Array<Real> &getMass() { return nodal(AKB_MASS, false); }
+  const Array<Real> &getCurrentPosition() {
+    syncUp();
+    mirrors_.erase(AKB_CURRENT_POSITION);
+    return nodal(AKB_CURRENT_POSITION, false);
+  }
+  Array<bool> &getBlockedDOFs() {
+    if (!blocked_) {
+      std::vector<uint8_t> raw(mesh_.getNbNodes() * dim_);
+      check(akb_model_get_nodal(h_, AKB_BLOCKED_DOFS, raw.data(), (int64_t)raw.size()));
+      blocked_ = std::make_unique<Array<bool>>(mesh_.getNbNodes(), dim_);
+      for (size_t k = 0; k < raw.size(); ++k) blocked_->data()[k] = raw[k] != 0;
+    }
+    blocked_dirty_ = true;
+    return *blocked_;
+  }
+
+  // applyBC(BC::Dirichlet::FixedValue(v, axis), group)
+  void applyBC(const BC::Dirichlet::FixedValue &bc, const ID &group) {
+    auto &blocked = getBlockedDOFs();
+    auto &u = getDisplacement();
+    for (Idx n : mesh_.getNodeGroup(group)) {
+      blocked(n, bc.axis) = true;
+      u(n, bc.axis) = bc.value;
+    }
+  }
+
+  void assembleInternalForces() {
+    syncUp();
+    check(akb_model_assemble_internal_forces(h_));
+    mirrors_.erase(AKB_INTERNAL_FORCE);
+  }
+
+  Real getEnergy(const ID &energy_id) {
+    syncUp();
+    Real e = 0;
+    check(akb_model_get_energy(h_, energy_id.c_str(), &e));
+    return e;
+  }
+
+  Int getNbMaterials() const {
+    int n = 0;
+    check(akb_model_nb_materials(h_, &n));
+    return n;
+  }
+  Material &getMaterial(Int i) {
+    while ((Int)materials_.size() <= i) materials_.emplace_back(*this, (int)materials_.size());
+    return materials_[i];
+  }
+  Material &getMaterial(const ID &name) {
+    for (Int i = 0; i < getNbMaterials(); ++i)
+      if (getMaterial(i).getName() == name) return getMaterial(i);
+    throw Exception(AKB_EMATERIAL, "no material named " + name);
+  }
+
+  Int getSpatialDimension() const { return dim_; }
+  Mesh &getMesh() { return mesh_; }
+  akb_model *handle() { return h_; }
+
+  // uploads the host arrays handed out since the last step
+  void syncUp() {
+    for (int f : handed_out_) {
+      auto &a = mirrors_.at(f);
+      check(akb_model_set_nodal(h_, f, a.data(), (int64_t)(a.size() * dim_ * sizeof(Real))));
+    }
+    handed_out_.clear();
+    if (blocked_dirty_ && blocked_) {
+      std::vector<uint8_t> raw(blocked_->size() * dim_);
+      for (size_t k = 0; k < raw.size(); ++k) raw[k] = blocked_->data()[k] ? 1 : 0;
+      check(akb_model_set_nodal(h_, AKB_BLOCKED_DOFS, raw.data(), (int64_t)raw.size()));
+    }
+    blocked_dirty_ = false;
+  }
+
+private:
+  int akb_model_load_and_init_mixed() {
+    for (const auto &text : getStaticParser().texts()) {
+      int rc = akb_model_load_materials(h_, text.c_str());
+      if (rc != AKB_OK) return rc;
+    }
+    return akb_model_init_full(h_, AKB_EXPLICIT_LUMPED_MASS, AKB_PRECISION_MIXED);
+  }
+
+  Array<Real> &nodal(int field, bool writable) {
+    auto it = mirrors_.find(field);
+    if (it == mirrors_.end()) {
+      Array<Real> a(mesh_.getNbNodes(), dim_);
+      check(akb_model_get_nodal(h_, field, a.data(), (int64_t)(a.size() * dim_ * sizeof(Real))));
+      it = mirrors_.emplace(field, std::move(a)).first;
+    }
+    if (writable) handed_out_.insert(field);
+    return it->second;
+  }
+
+  Mesh &mesh_;
+  Int dim_;
+  ID id_;
+  akb_model *h_ = nullptr;
+  std::map<int, Array<Real>> mirrors_;
+  std::set<int> handed_out_;
+  std::unique_ptr<Array<bool>> blocked_;
+  bool blocked_dirty_ = false;
+  std::vector<Material> materials_;
+};
+
+inline Real Material::get(const ID &param) const {
+  Real v = 0;
+  check(akb_model_get_material_param(model_->handle(), index_, param.c_str(), &v));
+  return v;
+}
+inline ID Material::getName() const {
+  char buf[256];
+  check(akb_model_get_material_name(model_->handle(), index_, buf, sizeof(buf)));
+  return buf;
+}
+inline Array<Real> Material::qp(int field) {
+  model_->syncUp();
+  int64_t n = 0;
+  check(akb_model_qp_field_size(model_->handle(), field, index_, &n));
+  const Int comps = (field == AKB_ISO_HARDENING || field == AKB_PLASTIC_ENERGY)
+                        ? 1
+                        : model_->getSpatialDimension() * model_->getSpatialDimension();
+  Array<Real> out(n / comps, comps);
+  check(akb_model_get_qp_field(model_->handle(), field, index_, out.data(), n));
+  return out;
+}
+inline Array<Real> Material::getStress(ElementType) { return qp(AKB_STRESS); }
+inline Array<Real> Material::getGradU(ElementType) { return qp(AKB_GRAD_U); }
+inline Array<Real> Material::getInternal(const ID &name, ElementType) {
+  static const std::map<ID, int> ids = {
+      {"stress", AKB_STRESS}, {"grad_u", AKB_GRAD_U},
+      {"piola_kirchhoff_2", AKB_PIOLA_KIRCHHOFF_2}, {"inelastic_strain", AKB_INELASTIC_STRAIN},
+      {"iso_hardening", AKB_ISO_HARDENING}, {"plastic_energy", AKB_PLASTIC_ENERGY}};
+  return qp(ids.at(name));
+}
+
+}  // namespace akantu_b200
+
+#endif
