@@ -81,11 +81,11 @@ inline constexpr AnalysisMethodTag _analysis_method{};
 template <class T> class Array {
 public:
   Array(Int size = 0, Int nb_component = 1, T value = T())
-      : n_(size), c_(nb_component), v_(new T[size * nb_component]) {
+      : n_(size), c_(nb_component), v_(allocate(size * nb_component)) {
     set(value);
   }
-  Array(const Array &o) : n_(o.n_), c_(o.c_), v_(new T[o.n_ * o.c_]) {
-    std::copy(o.data(), o.data() + n_ * c_, data());
+  Array(const Array &o) : n_(o.n_), c_(o.c_), v_(allocate(o.n_ * o.c_)) {
+    for (Int k = 0; k < n_ * c_; ++k) v_[k] = o.v_[k];
   }
   Array(Array &&) = default;
   Array &operator=(const Array &o) {
@@ -103,17 +103,19 @@ public:
   T *data() { return v_.get(); }
   const T *data() const { return v_.get(); }
   void resize(Int size) {
-    std::unique_ptr<T[]> nv(new T[size * c_]());
-    std::copy(data(), data() + std::min(size, n_) * c_, nv.get());
+    std::unique_ptr<T[]> nv = allocate(size * c_);
+    for (Int k = 0; k < std::min(size, n_) * c_; ++k) nv[k] = v_[k];
     v_ = std::move(nv);
     n_ = size;
   }
   void set(T value) {
-    if (n_ * c_ > 0) std::fill(data(), data() + n_ * c_, value);
+    for (Int k = 0; k < n_ * c_; ++k) v_[k] = value;
   }
   void zero() { set(T()); }
 
 private:
+  // never a zero-length allocation, so data() is always a valid pointer
+  static std::unique_ptr<T[]> allocate(Int n) { return std::unique_ptr<T[]>(new T[n > 0 ? n : 1]()); }
   Int n_, c_;
   std::unique_ptr<T[]> v_;
 };

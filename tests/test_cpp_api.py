@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def build_example(tmp_path):
     exe = tmp_path / "explicit_dynamic"
-    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-Wno-array-bounds",
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror",
            "-I", os.path.join(ROOT, "include"),
            os.path.join(ROOT, "examples", "explicit_dynamic.cc"),
            "-L", os.path.join(ROOT, "akantu2_b200"), "-lakb",
