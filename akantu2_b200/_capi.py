@@ -82,6 +82,7 @@ def lib():
         "akb_model_qp_field_size": (c_int, [vp, c_int, c_int, ctypes.POINTER(i64)]),
         "akb_model_get_qp_field": (c_int, [vp, c_int, c_int, vp, i64]),
         "akb_model_solve_step": (c_int, [vp, i64]),
+        "akb_model_set_graph_steps": (c_int, [vp, i64]),
         "akb_model_synchronize": (c_int, [vp]),
         "akb_model_time_steps": (c_int, [vp, i64, ctypes.POINTER(c_dbl)]),
         "akb_model_profile_steps": (c_int, [vp, i64, ctypes.POINTER(c_dbl),

@@ -184,6 +184,18 @@ struct akb_model {
   unsigned int *dstatus = nullptr;
   unsigned long long *dbad = nullptr;
   std::vector<void *> allocs;
+  // captured multi-step graphs, keyed by the buffer parities they start from
+  // (an even number of steps returns to the same parities) and by the values
+  // baked into their launches
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int ucur = 0, cur = 0;
+    double dt = 0.;
+    bool fext_zero = true;
+    int64_t steps = 0;
+  };
+  std::vector<StepGraph> graphs;
+  int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
 
   double *u() const { return dU[ucur]; }
   double *u_pred() const { return dU[1 - ucur]; }
@@ -205,6 +217,7 @@ struct akb_model {
     return AKB_OK;
   }
   ~akb_model() {
+    for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
     for (void *p : allocs) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -376,6 +389,50 @@ int one_step(akb_model *m, bool any_plastic, cudaEvent_t e1 = nullptr,
   m->ucur = 1 - m->ucur;  // u_{n+1} is now the model's displacement
   if (any_plastic) m->cur = 1 - m->cur;
   m->steps_done++;
+  return AKB_OK;
+}
+
+// graph_steps steps (even) as one CUDA graph launch.  The graph is captured
+// from one_step the first time a (parity, dt, f_ext == 0) combination is
+// met; capturing does not execute, so the host-side step state is restored
+// afterwards and advanced when the graph is launched.
+int run_graph(akb_model *m, bool any_plastic) {
+  akb_model::StepGraph *g = nullptr;
+  for (auto &x : m->graphs)
+    if (x.ucur == m->ucur && x.cur == m->cur && x.dt == m->dt && x.fext_zero == m->fext_zero &&
+        x.steps == m->graph_steps)
+      g = &x;
+  if (!g) {
+    const int ucur0 = m->ucur, cur0 = m->cur;
+    const int64_t steps0 = m->steps_done;
+    AKB_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = AKB_OK;
+    for (int64_t s = 0; s < m->graph_steps && rc == AKB_OK; ++s) rc = one_step(m, any_plastic);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(m->stream, &graph);
+    m->ucur = ucur0;
+    m->cur = cur0;
+    m->steps_done = steps0;
+    if (rc != AKB_OK || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc != AKB_OK) return rc;
+      return fail(AKB_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+      return fail(AKB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    if (m->graphs.size() >= 8) {  // keep the cache small: drop the oldest
+      cudaGraphExecDestroy(m->graphs.front().exec);
+      m->graphs.erase(m->graphs.begin());
+    }
+    m->graphs.push_back({exec, ucur0, cur0, m->dt, m->fext_zero, m->graph_steps});
+    g = &m->graphs.back();
+  }
+  AKB_CUDA(cudaGraphLaunch(g->exec, m->stream));
+  m->steps_done += g->steps;
+  m->fint_valid = false;
   return AKB_OK;
 }
 
@@ -923,11 +980,29 @@ int akb_model_solve_step(akb_model *m, int64_t nsteps) {
   if (nsteps < 0) return fail(AKB_EINVAL, "negative step count");
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
-  for (int64_t s = 0; s < nsteps; ++s) AKB_TRY(one_step(m, any_plastic));
+  int64_t left = nsteps;
+  // a step whose prediction is stale runs eagerly (it launches the predictor)
+  if (left > 0 && !m->predicted) {
+    AKB_TRY(one_step(m, any_plastic));
+    --left;
+  }
+  const int64_t G = m->graph_steps;
+  while (G > 0 && left >= G) {
+    AKB_TRY(run_graph(m, any_plastic));
+    left -= G;
+  }
+  for (; left > 0; --left) AKB_TRY(one_step(m, any_plastic));
   if (nsteps > 0) {
     m->forces_evaluated = true;
     m->snap_valid = false;
   }
+  return AKB_OK;
+}
+
+int akb_model_set_graph_steps(akb_model *m, int64_t steps) {
+  AKB_TRY(check_model(m, false));
+  if (steps < 0 || steps % 2) return fail(AKB_EINVAL, "graph length must be even and >= 0");
+  m->graph_steps = steps;
   return AKB_OK;
 }
 

@@ -287,6 +287,10 @@ class SolidMechanicsModel:
         self._invalidate()
         return total.value, list(phases)
 
+    def setGraphSteps(self, steps):
+        """Multi-step runs are replayed as CUDA graphs of `steps` steps (even; 0 disables)."""
+        _capi.check(_capi.lib().akb_model_set_graph_steps(self._h, int(steps)))
+
     def synchronize(self):
         _capi.check(_capi.lib().akb_model_synchronize(self._h))
 

@@ -173,6 +173,11 @@ int akb_model_get_qp_field(akb_model *model, int field, int material, double *ho
 /* ModelSolver::solveStep  model_solver.cc:267-280: enqueues nsteps explicit
  * steps on the model's stream (asynchronous; getters synchronise) */
 int akb_model_solve_step(akb_model *model, int64_t nsteps);
+/* runs of solve_step are issued as CUDA graphs of `steps` steps (even; 0 =
+ * plain launches; default 100).  A graph is captured once per (buffer
+ * parity, dt, zero external force) and replayed; steps that follow a host
+ * edit of u, v, a, the blocked dofs or dt run eagerly first. */
+int akb_model_set_graph_steps(akb_model *model, int64_t steps);
 int akb_model_synchronize(akb_model *model);
 /* SolidMechanicsModel::assembleInternalForces  solid_mechanics_model.cc:333-370 */
 int akb_model_assemble_internal_forces(akb_model *model);
