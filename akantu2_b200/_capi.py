@@ -91,6 +91,23 @@ def lib():
         "akb_model_get_energy": (c_int, [vp, ctypes.c_char_p, ctypes.POINTER(c_dbl)]),
         "akb_model_get_status": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_stable_time_step_noalloc": (c_int, [c_int, vp, vp, vp, i64, c_dbl, vp, vp]),
+        "akb_model_prepare_graphs": (c_int, [vp]),
+        "akb_model_stream": (c_int, [vp, pp]),
+        "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
+        "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,
+                                              ctypes.POINTER(i64)]),
+        "akb_server_create": (c_int, [vp, pp]),
+        "akb_server_submit": (c_int, [vp, vp, ctypes.POINTER(i64)]),
+        "akb_server_poll": (c_int, [vp, vp, c_int, ctypes.POINTER(c_int), c_dbl]),
+        "akb_server_get_stats": (c_int, [vp, vp]),
+        "akb_server_destroy": (c_int, [vp]),
+        "akb_batch_create": (c_int, [c_int, c_int, c_int, vp, vp, vp, vp, pp]),
+        "akb_batch_nb_instances": (c_int, [vp, ctypes.POINTER(c_int)]),
+        "akb_batch_instance_offsets": (c_int, [vp, vp, vp]),
+        "akb_batch_set_instance_materials": (c_int, [vp, vp]),
+        "akb_batch_get_stable_time_steps": (c_int, [vp, vp]),
+        "akb_batch_set_time_steps": (c_int, [vp, vp]),
+        "akb_batch_get_time_steps": (c_int, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -39,7 +39,7 @@ inline unsigned grid_for(int64_t n, int threads = kThreads) {
 template <class T, class RT>
 inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const T *B, const T *wJ, const double *u,
-                                       const MatParams &mp, const PlasticState &ps, RT *re,
+                                       const MatParams &mp, const GroupArgs &ps, RT *re,
                                        cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {

@@ -50,13 +50,25 @@ __device__ __forceinline__ void load_slot(const RT *re, int64_t p, double *v) {
 }
 
 // per-material plastic internals, [q][comp][ne], ping-pong prev/cur
-struct PlasticState {
+// One launch covers a law group: the elements of all materials with the same
+// law, contiguous in internal order.  With several materials, each element
+// reads its parameters from mtab[mslot[le]]; with one, from the launch's
+// MatParams.  Plastic internals of the group are [q][comp][ne] arrays,
+// ping-pong prev / cur.
+struct GroupArgs {
+  const MatParams *mtab;     // per-material parameters, or null
+  const int32_t *mslot;      // [ne] index into mtab
   const double *sig_prev, *gu_prev, *eps_prev, *iso_prev;
   const double *iso_cur_in;  // "current" hardening read by the yield test
   double *sig, *gu, *eps, *iso;
   double *pe;                // cumulative plastic energy density
   int update_energy;         // 1 inside solveStep (afterSolveStep), 0 otherwise
 };
+
+__device__ __forceinline__ MatParams group_params(const MatParams &mp, const GroupArgs &ga,
+                                                  int64_t le) {
+  return ga.mtab ? ga.mtab[ga.mslot[le]] : mp;
+}
 
 // ---------------------------------------------------------------------------
 // K0: dN/dx and det J * w  (element_class_tmpl.hh:296-395,
@@ -215,10 +227,12 @@ template <> __device__ inline double element_inradius<ET_TRI6>(const double *X) 
   return 2. * r;
 }
 
+// out[perm ? perm[e] : e] = h_e / c
 template <int ET, int D, int NN>
 __global__ void k_element_dt(int64_t e_begin, int64_t e_count, int64_t E, double celerity,
                              const int32_t *__restrict__ conn, const double *__restrict__ X,
-                             const double *__restrict__ u, double *__restrict__ out) {
+                             const double *__restrict__ u, const int32_t *__restrict__ perm,
+                             double *__restrict__ out) {
   const int64_t le = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (le >= e_count) return;
   const int64_t e = e_begin + le;
@@ -229,7 +243,30 @@ __global__ void k_element_dt(int64_t e_begin, int64_t e_count, int64_t E, double
 #pragma unroll
     for (int i = 0; i < D; ++i) Xe[a * D + i] = X[node * D + i] + u[node * D + i];
   }
-  out[e] = element_inradius<ET>(Xe) / celerity;
+  out[perm ? (int64_t)perm[e] : e] = element_inradius<ET>(Xe) / celerity;
+}
+
+// minimum of each segment [off[k], off[k+1]) of x, one block per segment
+static __global__ void k_segment_min(const double *__restrict__ x, const int64_t *__restrict__ off,
+                                     double *__restrict__ out) {
+  __shared__ double sm[256];
+  const int k = blockIdx.x;
+  double acc = 1.7976931348623157e308;
+  for (int64_t i = off[k] + threadIdx.x; i < off[k + 1]; i += blockDim.x) acc = fmin(acc, x[i]);
+  sm[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] = fmin(sm[threadIdx.x], sm[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = sm[0];
+}
+
+// time step of node i: one value for the model, or the value of the node's
+// instance when several independent meshes advance together
+__device__ __forceinline__ double node_dt(double dt, const int32_t *node_inst,
+                                          const double *inst_dt, int64_t i) {
+  return node_inst ? inst_dt[node_inst[i]] : dt;
 }
 
 // ---------------------------------------------------------------------------
@@ -243,7 +280,9 @@ __global__ void k_element_dt(int64_t e_begin, int64_t e_count, int64_t E, double
 template <int D>
 __global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
                           const double *__restrict__ u, const double *__restrict__ v,
-                          const double *__restrict__ a, double dt, double *__restrict__ u_pred) {
+                          const double *__restrict__ a, double dt,
+                          const int32_t *__restrict__ node_inst,
+                          const double *__restrict__ inst_dt, double *__restrict__ u_pred) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N * D) return;
   const int64_t node = i / D;
@@ -252,6 +291,7 @@ __global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
     u_pred[i] = u[i];
     return;
   }
+  dt = node_dt(dt, node_inst, inst_dt, node);
   const double hdt = .5 * dt;
   const double dta = dt * a[i];
   u_pred[i] = u[i] + (dt * v[i] + hdt * dta);
@@ -273,7 +313,7 @@ __global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
 // plastic internals of one quadrature point: loads previous state, runs the
 // radial return, stores the new state (and the plastic energy in a step)
 template <int D>
-__device__ __forceinline__ void plastic_point(const MatParams &mp, const PlasticState &ps,
+__device__ __forceinline__ void plastic_point(const MatParams &mp, const GroupArgs &ps,
                                               int64_t ne, int64_t le, int q,
                                               const double *gd, double *s) {
   constexpr int DD = D * D;
@@ -312,7 +352,7 @@ __device__ __forceinline__ void plastic_point(const MatParams &mp, const Plastic
 
 template <int D, int NN, int LAW, class T, bool REL>
 __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const MatParams &mp,
-                                            const PlasticState &ps, int64_t ne, int64_t le,
+                                            const GroupArgs &ps, int64_t ne, int64_t le,
                                             int q, T *t) {
   // grad u = u B^T  (shape_functions_inline_impl.hh:303-310)
   T g[D * D];
@@ -396,13 +436,14 @@ __global__ void __launch_bounds__(kPeThreads)
     k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const T *__restrict__ B, const T *__restrict__ wJ,
-                        const double *__restrict__ u, MatParams mp, PlasticState ps,
+                        const double *__restrict__ u, MatParams mp, GroupArgs ps,
                         RT *__restrict__ re) {
   constexpr int ND = NN * D;
   constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
   const int64_t le = (int64_t)blockIdx.x * kPeThreads + threadIdx.x;
   if (le >= e_count) return;
   const int64_t e = e_begin + le;
+  const MatParams mpe = group_params(mp, ps, le);
   T ue[ND];
   double u0[D];
 #pragma unroll
@@ -427,7 +468,7 @@ __global__ void __launch_bounds__(kPeThreads)
     for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)(q * ND + c) * E + e];
     const T w = wJ[(int64_t)q * E + e];
     T t[ND];
-    element_law<D, NN, LAW, T, REL>(ue, b, w, mp, ps, e_count, le, q, t);
+    element_law<D, NN, LAW, T, REL>(ue, b, w, mpe, ps, e_count, le, q, t);
     // integrate: sum over q in increasing order (integrator_gauss_inline_impl.hh:401-418)
 #pragma unroll
     for (int c = 0; c < ND; ++c) r[c] = (q == 0) ? t[c] : r[c] + t[c];
@@ -448,12 +489,13 @@ __global__ void __launch_bounds__(kPeThreads)
     k_element_forces_geo(int64_t e_begin, int64_t e_count, int64_t E,
                          const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                          const double *__restrict__ X, QuadTable tab,
-                         const double *__restrict__ u, MatParams mp, PlasticState ps,
+                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
                          float *__restrict__ re) {
   constexpr int ND = NN * D;
   const int64_t le = (int64_t)blockIdx.x * kPeThreads + threadIdx.x;
   if (le >= e_count) return;
   const int64_t e = e_begin + le;
+  const MatParams mpe = group_params(mp, ps, le);
   float xe[ND], ue[ND];
   double x0[D], u0[D];
 #pragma unroll
@@ -504,7 +546,7 @@ __global__ void __launch_bounds__(kPeThreads)
       }
     const float w = det * tab.fw[q];
     float t[ND];
-    element_law<D, NN, LAW, float, true>(ue, b, w, mp, ps, e_count, le, q, t);
+    element_law<D, NN, LAW, float, true>(ue, b, w, mpe, ps, e_count, le, q, t);
 #pragma unroll
     for (int c = 0; c < ND; ++c) r[c] = (q == 0) ? t[c] : r[c] + t[c];
   }
@@ -518,7 +560,7 @@ __global__ void __launch_bounds__(32 * NQ)
     k_element_forces_pq(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const double *__restrict__ B, const double *__restrict__ wJ,
-                        const double *__restrict__ u, MatParams mp, PlasticState ps,
+                        const double *__restrict__ u, MatParams mp, GroupArgs ps,
                         double *__restrict__ re) {
   constexpr int ND = NN * D;
   constexpr int CH = (ND + NQ - 1) / NQ;  // components reduced per round and thread
@@ -546,7 +588,8 @@ __global__ void __launch_bounds__(32 * NQ)
       b[c] = B[(int64_t)(q * ND + c) * E + e];
     }
     const double w = wJ[(int64_t)q * E + e];
-    element_law<D, NN, LAW, double, false>(ue, b, w, mp, ps, e_count, le, q, t);
+    const MatParams mpe = group_params(mp, ps, le);
+    element_law<D, NN, LAW, double, false>(ue, b, w, mpe, ps, e_count, le, q, t);
   }
   // sum over q in increasing order, NQ components per round
 #pragma unroll
@@ -599,7 +642,9 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               const uint8_t *__restrict__ blocked, double *__restrict__ fint,
                               double *__restrict__ a, double *__restrict__ v,
                               const double *__restrict__ u, double *__restrict__ u_next,
-                              double dt, int flags, unsigned int *__restrict__ status) {
+                              double dt, const int32_t *__restrict__ node_inst,
+                              const double *__restrict__ inst_dt, int flags,
+                              unsigned int *__restrict__ status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double acc[D], comp[D];
@@ -633,6 +678,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
   if (!(flags & NU_CORRECT)) return;
   const double m = mass[i];
   const uint8_t bl = blocked[i];
+  dt = node_dt(dt, node_inst, inst_dt, i);
   const double hdt = .5 * dt;
   bool bad = false;
 #pragma unroll

@@ -38,13 +38,21 @@ cudaError_t launch_gather_scalar(const DevGeom &g, const double *me, double *out
 }
 
 cudaError_t launch_element_dt(const DevGeom &g, int64_t e0, int64_t ne, double celerity,
-                              const double *u, double *out, cudaStream_t s) {
+                              const double *u, const int32_t *perm, double *out,
+                              cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {
     (void)NQ;
     k_element_dt<ET, D, NN><<<grid_for(ne), kThreads, 0, s>>>(e0, ne, g.E, celerity, g.conn,
-                                                              g.X, u, out);
+                                                              g.X, u, perm, out);
   });
+  return cudaGetLastError();
+}
+
+cudaError_t launch_segment_min(const double *x, const int64_t *off, int nseg, double *out,
+                               cudaStream_t s) {
+  if (nseg == 0) return cudaSuccess;
+  k_segment_min<<<nseg, 256, 0, s>>>(x, off, out);
   return cudaGetLastError();
 }
 
@@ -64,15 +72,17 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
                            cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
-    k_predict<3><<<grid_for(g.N * 3), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, u_pred);
+    k_predict<3><<<grid_for(g.N * 3), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, g.node_inst,
+                                                        g.inst_dt, u_pred);
   else
-    k_predict<2><<<grid_for(g.N * 2), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, u_pred);
+    k_predict<2><<<grid_for(g.N * 2), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, g.node_inst,
+                                                        g.inst_dt, u_pred);
   return cudaGetLastError();
 }
 
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
-                                       const MatParams &mp, const PlasticState &ps,
+                                       const MatParams &mp, const GroupArgs &ps,
                                        double *re, cudaStream_t s) {
   return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, s);
 }
@@ -84,10 +94,12 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
     k_node_update<3, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, flags, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
+        flags, status);
   else
     k_node_update<2, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, flags, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
+        flags, status);
   return cudaGetLastError();
 }
 
@@ -168,7 +180,7 @@ cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double
 // material.cc:604-619; MaterialPlastic::getPlasticEnergy, material_plastic.cc:47-69).
 // Quadrature-point inputs are [q][comp][ne]; wJ is [q][E].
 template <int D, int NQ, int LAW>
-__global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t E,
+__global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t ld, int64_t E,
                               const double *__restrict__ wJ, const double *__restrict__ grad,
                               const double *__restrict__ stress,
                               const double *__restrict__ eps_p, const double *__restrict__ pe,
@@ -179,10 +191,10 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t E,
   double el = 0.;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    auto at = [&](int k) { return (int64_t)(q * DD + k) * ne + le; };
+    auto at = [&](int k) { return (int64_t)(q * DD + k) * ld + le; };
     double dens;
     if (which == 1) {
-      dens = pe[(int64_t)q * ne + le];
+      dens = pe[(int64_t)q * ld + le];
     } else if (LAW == LAW_NEOHOOKEAN) {
       double F[DD];
 #pragma unroll
@@ -217,7 +229,7 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t E,
   out[le] = el;
 }
 cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0, int64_t ne,
-                               const double *wJ, const double *grad, const double *stress,
+                               int64_t ld, const double *wJ, const double *grad, const double *stress,
                                const double *eps_p, const double *pe, const MatParams &mp,
                                double *out, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
@@ -226,13 +238,13 @@ cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0,
     (void)NN;
     if (law == LAW_NEOHOOKEAN)
       k_energy_elem<D, NQ, LAW_NEOHOOKEAN><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, g.E, wJ, grad, stress, eps_p, pe, mp, out);
+          which, e0, ne, ld, g.E, wJ, grad, stress, eps_p, pe, mp, out);
     else if (law == LAW_PLASTIC)
       k_energy_elem<D, NQ, LAW_PLASTIC><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, g.E, wJ, grad, stress, eps_p, pe, mp, out);
+          which, e0, ne, ld, g.E, wJ, grad, stress, eps_p, pe, mp, out);
     else
       k_energy_elem<D, NQ, LAW_ELASTIC><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, g.E, wJ, grad, stress, eps_p, pe, mp, out);
+          which, e0, ne, ld, g.E, wJ, grad, stress, eps_p, pe, mp, out);
   });
   return cudaGetLastError();
 }

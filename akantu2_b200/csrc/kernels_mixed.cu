@@ -8,7 +8,7 @@ namespace akb {
 cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                         const QuadTable &tab, const float *fB,
                                         const float *fwJ, const double *u,
-                                        const MatParams &mp, const PlasticState &ps,
+                                        const MatParams &mp, const GroupArgs &ps,
                                         float *re, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   if (g.D == 2) return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, s);
@@ -36,10 +36,12 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
     k_node_update<3, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, flags, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
+        flags, status);
   else
     k_node_update<2, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, flags, status);
+        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
+        flags, status);
   return cudaGetLastError();
 }
 

@@ -11,7 +11,7 @@
 namespace akb {
 
 struct QuadTable;
-struct PlasticState;
+struct GroupArgs;
 
 // device view of the mesh, internal element order
 struct DevGeom {
@@ -22,6 +22,10 @@ struct DevGeom {
   const int32_t *ptr;   // [N+1]
   const int32_t *ent;   // [E*NN] slot (e*NN + a) of each CSR position
   const int32_t *pos;   // [NN][E] CSR position of each slot
+  // several independent meshes in one model: instance of each node and the
+  // time step of each instance (both null for a single mesh)
+  const int32_t *node_inst = nullptr;  // [N]
+  const double *inst_dt = nullptr;     // [instances]
 };
 
 // ---- init ------------------------------------------------------------------
@@ -32,8 +36,13 @@ cudaError_t launch_mass_elem(const DevGeom &g, int64_t e0, int64_t ne, double rh
                              cudaStream_t s);
 cudaError_t launch_gather_scalar(const DevGeom &g, const double *me, double *out,
                                  cudaStream_t s);
+// out[perm ? perm[e] : e] = h_e / celerity for the elements e0 .. e0 + ne
 cudaError_t launch_element_dt(const DevGeom &g, int64_t e0, int64_t ne, double celerity,
-                              const double *u, double *out, cudaStream_t s);
+                              const double *u, const int32_t *perm, double *out,
+                              cudaStream_t s);
+// out[k] = min of x[off[k] .. off[k+1]) (off on the device)
+cudaError_t launch_segment_min(const double *x, const int64_t *off, int nseg, double *out,
+                               cudaStream_t s);
 cudaError_t launch_to_float(const double *in, float *out, int64_t n, cudaStream_t s);
 
 // ---- step ------------------------------------------------------------------
@@ -43,7 +52,7 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
                            cudaStream_t s);
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
-                                       const MatParams &mp, const PlasticState &ps,
+                                       const MatParams &mp, const GroupArgs &ps,
                                        double *re, cudaStream_t s);
 // mixed path: 3D elements recompute their shape derivatives in FP32 from g.X
 // and the table; 2D elements stream FP32 copies (fB, fwJ) of the precomputed
@@ -51,7 +60,7 @@ cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, in
 cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                         const QuadTable &tab, const float *fB,
                                         const float *fwJ, const double *u,
-                                        const MatParams &mp, const PlasticState &ps,
+                                        const MatParams &mp, const GroupArgs &ps,
                                         float *re, cudaStream_t s);
 // flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
 // the predictor of the next step reads u and writes u_next
@@ -76,10 +85,11 @@ cudaError_t launch_ekin_terms(const DevGeom &g, const double *v, const double *m
 cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double *fint,
                               const double *v, const uint8_t *blocked, double *out,
                               cudaStream_t s);
-// per-element sum_q density_q wJ_q of one material -> out[ne]
-// which: 0 potential, 1 plastic
+// per-element sum_q density_q wJ_q of one material -> out[ne]; the
+// quadrature-point inputs are [q][comp][ld] with the material's elements at
+// 0 .. ne.  which: 0 potential, 1 plastic
 cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0, int64_t ne,
-                               const double *wJ, const double *grad, const double *stress,
+                               int64_t ld, const double *wJ, const double *grad, const double *stress,
                                const double *eps_p, const double *pe, const MatParams &mp,
                                double *out, cudaStream_t s);
 // deterministic reductions (fixed grid, fixed tree): result written to *out

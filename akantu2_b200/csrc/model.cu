@@ -45,11 +45,8 @@ struct Material {
   double rho = 0., E = 0., nu = 0.5, sigma_y = 0., h = 0., alpha = 0., delta_T = 0.;
   bool plane_stress = false, finite_deformation = false;
   double lambda = 0., mu = 0., sigma_th = 0.;
-  int64_t e_begin = 0, e_count = 0;
-  // plastic internals (SoA [comp][nqp]), ping-pong prev / cur
-  double *sig[2] = {nullptr, nullptr}, *gu[2] = {nullptr, nullptr};
-  double *eps[2] = {nullptr, nullptr}, *iso[2] = {nullptr, nullptr};
-  double *pe = nullptr;
+  int64_t e_begin = 0, e_count = 0;  // internal element range
+  int group = 0;                     // law group holding the range
 
   // Lame update (material_elastic.cc:53-78, material_neohookean.cc:61-67),
   // thermal stress (material_thermal.hh:89-95)
@@ -62,6 +59,21 @@ struct Material {
   }
   MatParams params() const { return MatParams{lambda, mu, sigma_y, h, sigma_th, rho}; }
   double celerity() const { return std::sqrt((lambda + 2 * mu) / rho); }
+};
+
+// Law group: the elements of all materials with one constitutive law, one
+// contiguous internal range, advanced by one kernel launch per step.  Its
+// plastic internals are [q][comp][e_count] arrays (group-local element
+// fastest), ping-pong prev / cur; a material's part starts at column
+// (material e_begin - group e_begin).
+struct Group {
+  int law = LAW_ELASTIC;
+  int mat0 = 0;  // first material of the group
+  int nmat = 0;
+  int64_t e_begin = 0, e_count = 0;
+  double *sig[2] = {nullptr, nullptr}, *gu[2] = {nullptr, nullptr};
+  double *eps[2] = {nullptr, nullptr}, *iso[2] = {nullptr, nullptr};
+  double *pe = nullptr;
 };
 
 int nodes_per_element(int et) {
@@ -155,7 +167,13 @@ struct akb_model {
   std::vector<int32_t> conn;        // user order [E][nn]
   std::vector<int32_t> mat_user;    // user element -> material
   std::vector<Material> mats;
+  std::vector<Group> groups;
   std::vector<int64_t> perm;        // internal element -> user element
+  // independent meshes advanced together (batch): node and element ranges of
+  // each instance in user order, and the time step of each
+  int ninst = 1;
+  std::vector<int64_t> inst_node_off{0, 0}, inst_elem_off{0, 0};
+  std::vector<double> inst_dt;
   bool initialized = false, forces_evaluated = false, snap_valid = false;
   int cur = 0;  // ping-pong index of the latest plastic state
   int64_t steps_done = 0;
@@ -167,6 +185,11 @@ struct akb_model {
   float *fB = nullptr, *fwJ = nullptr;  // FP32 copies (mixed path, 2D elements)
   QuadTable tab;  // quadrature tables of the element type
   int32_t *dconn = nullptr, *dptr = nullptr, *dent = nullptr, *dpos = nullptr;
+  MatParams *dmtab = nullptr;  // all materials, for groups of several
+  int32_t *dmslot = nullptr;   // [E] material of each internal element
+  int32_t *dnode_inst = nullptr, *dperm = nullptr;  // batch: [N] instance, [E] user id
+  double *dinst_dt = nullptr, *dinst_min = nullptr;  // batch: [ninst]
+  int64_t *dinst_eoff = nullptr;                     // batch: [ninst + 1]
   // displacement ping-pong: dU[ucur] is the model's u, dU[1 - ucur] the
   // prediction of the next step (valid when `predicted`)
   double *dU[2] = {nullptr, nullptr};
@@ -203,22 +226,28 @@ struct akb_model {
     DevGeom g;
     g.et = et; g.D = dim; g.NN = nn; g.NQ = nq; g.E = E; g.N = N;
     g.conn = dconn; g.X = dX; g.ptr = dptr; g.ent = dent; g.pos = dpos;
+    g.node_inst = dnode_inst;
+    g.inst_dt = dinst_dt;
     return g;
   }
+  // stream-ordered allocations on the model's stream: neither allocating
+  // nor freeing waits for the work of other models on the device
   template <class P> int alloc(P **p, size_t bytes) {
     void *q = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(&q, bytes);
+    cudaError_t e = cudaMallocAsync(&q, bytes, stream);
     if (e != cudaSuccess)
       return fail(e == cudaErrorMemoryAllocation ? AKB_ENOMEM : AKB_ECUDA,
-                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+                  std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     allocs.push_back(q);
+    device_bytes += bytes;
     *p = (P *)q;
     return AKB_OK;
   }
+  size_t device_bytes = 0;
   ~akb_model() {
     for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
-    for (void *p : allocs) cudaFree(p);
+    for (void *p : allocs) cudaFreeAsync(p, stream);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -298,9 +327,13 @@ int snapshot_u(akb_model *m) {
   return AKB_OK;
 }
 
-PlasticState plastic_state(akb_model *m, const Material &mt, bool in_step) {
-  PlasticState ps;
+GroupArgs group_args(akb_model *m, const Group &mt, bool in_step) {
+  GroupArgs ps;
   std::memset(&ps, 0, sizeof(ps));
+  if (mt.nmat > 1) {
+    ps.mtab = m->dmtab;
+    ps.mslot = m->dmslot + mt.e_begin;
+  }
   if (mt.law != LAW_PLASTIC) return ps;
   const int c = m->cur;
   // inside a step the new state goes to the other buffer; a standalone
@@ -326,15 +359,16 @@ PlasticState plastic_state(akb_model *m, const Material &mt, bool in_step) {
 int element_forces(akb_model *m, bool in_step) {
   DevGeom g = m->geom();
   const double *u = in_step ? m->u_pred() : m->u();
-  for (auto &mt : m->mats) {
-    PlasticState ps = plastic_state(m, mt, in_step);
+  for (auto &gr : m->groups) {
+    GroupArgs ps = group_args(m, gr, in_step);
+    const MatParams mp = m->mats[gr.mat0].params();
     cudaError_t e;
     if (m->precision == AKB_PRECISION_MIXED)
-      e = launch_element_forces_mixed(g, mt.law, mt.e_begin, mt.e_count, m->tab, m->fB, m->fwJ,
-                                      u, mt.params(), ps, (float *)m->dre, m->stream);
+      e = launch_element_forces_mixed(g, gr.law, gr.e_begin, gr.e_count, m->tab, m->fB, m->fwJ,
+                                      u, mp, ps, (float *)m->dre, m->stream);
     else
-      e = launch_element_forces_fp64(g, mt.law, mt.e_begin, mt.e_count, m->dB, m->dwJ, u,
-                                     mt.params(), ps, (double *)m->dre, m->stream);
+      e = launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ, u, mp,
+                                     ps, (double *)m->dre, m->stream);
     if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("element forces: ") + cudaGetErrorString(e));
   }
   return AKB_OK;
@@ -396,10 +430,14 @@ int one_step(akb_model *m, bool any_plastic, cudaEvent_t e1 = nullptr,
 // from one_step the first time a (parity, dt, f_ext == 0) combination is
 // met; capturing does not execute, so the host-side step state is restored
 // afterwards and advanced when the graph is launched.
-int run_graph(akb_model *m, bool any_plastic) {
+// the graph for the model's current parities, dt and f_ext flag, captured
+// (not launched) if it does not exist yet
+int capture_graph(akb_model *m, bool any_plastic, akb_model::StepGraph **out = nullptr) {
   akb_model::StepGraph *g = nullptr;
+  // a batch reads its time steps from device memory: they are not baked in
+  const double key_dt = m->ninst > 1 ? 0. : m->dt;
   for (auto &x : m->graphs)
-    if (x.ucur == m->ucur && x.cur == m->cur && x.dt == m->dt && x.fext_zero == m->fext_zero &&
+    if (x.ucur == m->ucur && x.cur == m->cur && x.dt == key_dt && x.fext_zero == m->fext_zero &&
         x.steps == m->graph_steps)
       g = &x;
   if (!g) {
@@ -427,9 +465,16 @@ int run_graph(akb_model *m, bool any_plastic) {
       cudaGraphExecDestroy(m->graphs.front().exec);
       m->graphs.erase(m->graphs.begin());
     }
-    m->graphs.push_back({exec, ucur0, cur0, m->dt, m->fext_zero, m->graph_steps});
+    m->graphs.push_back({exec, ucur0, cur0, key_dt, m->fext_zero, m->graph_steps});
     g = &m->graphs.back();
   }
+  if (out) *out = g;
+  return AKB_OK;
+}
+
+int run_graph(akb_model *m, bool any_plastic) {
+  akb_model::StepGraph *g = nullptr;
+  AKB_TRY(capture_graph(m, any_plastic, &g));
   AKB_CUDA(cudaGraphLaunch(g->exec, m->stream));
   m->steps_done += g->steps;
   m->fint_valid = false;
@@ -528,8 +573,73 @@ int akb_model_create(int dim, int et, const double *nodes, int64_t N, const int3
   m->E = E;
   m->X.assign(nodes, nodes + N * dim);
   m->conn.assign(conn, conn + E * nn);
+  m->inst_node_off = {0, N};
+  m->inst_elem_off = {0, E};
   *out = m;
   return AKB_OK;
+}
+
+int akb_batch_create(int dim, int et, int nb_instances, const int64_t *nb_nodes,
+                     const int64_t *nb_elements, const double *nodes, const int32_t *conn,
+                     akb_model **out) {
+  if (!out) return fail(AKB_EINVAL, "null output pointer");
+  *out = nullptr;
+  if (nb_instances < 1 || !nb_nodes || !nb_elements)
+    return fail(AKB_EINVAL, "a batch needs at least one instance and its sizes");
+  if (et < AKB_TETRAHEDRON_4 || et > AKB_TRIANGLE_6) return fail(AKB_EINVAL, "unknown element type");
+  const int nn = nodes_per_element(et);
+  std::vector<int64_t> noff(nb_instances + 1, 0), eoff(nb_instances + 1, 0);
+  for (int k = 0; k < nb_instances; ++k) {
+    if (nb_nodes[k] < 0 || nb_elements[k] < 0) return fail(AKB_EINVAL, "negative instance size");
+    noff[k + 1] = noff[k] + nb_nodes[k];
+    eoff[k + 1] = eoff[k] + nb_elements[k];
+  }
+  const int64_t N = noff.back(), E = eoff.back();
+  if (N >= (int64_t)std::numeric_limits<int32_t>::max())
+    return fail(AKB_EINVAL, "batch too large for 32-bit node indices");
+  if ((N > 0 && !nodes) || (E > 0 && !conn)) return fail(AKB_EINVAL, "bad mesh arrays");
+  // instance-local node ids -> ids in the concatenated node array
+  std::vector<int32_t> gconn((size_t)E * nn);
+  for (int k = 0; k < nb_instances; ++k)
+    for (int64_t j = eoff[k] * nn; j < eoff[k + 1] * nn; ++j) {
+      if (conn[j] < 0 || conn[j] >= nb_nodes[k])
+        return fail(AKB_EINVAL, "instance " + std::to_string(k) +
+                                    ": connectivity refers to a missing node");
+      gconn[j] = (int32_t)(conn[j] + noff[k]);
+    }
+  akb_model *m = nullptr;
+  AKB_TRY(akb_model_create(dim, et, nodes, N, gconn.data(), E, &m));
+  m->ninst = nb_instances;
+  m->inst_node_off = noff;
+  m->inst_elem_off = eoff;
+  m->inst_dt.assign(nb_instances, 0.);
+  *out = m;
+  return AKB_OK;
+}
+
+int akb_batch_nb_instances(const akb_model *m, int *count) {
+  if (!m || !count) return fail(AKB_EINVAL, "null argument");
+  *count = m->ninst;
+  return AKB_OK;
+}
+
+int akb_batch_instance_offsets(const akb_model *m, int64_t *node_offsets,
+                               int64_t *element_offsets) {
+  if (!m) return fail(AKB_EINVAL, "null model");
+  if (node_offsets) std::copy(m->inst_node_off.begin(), m->inst_node_off.end(), node_offsets);
+  if (element_offsets)
+    std::copy(m->inst_elem_off.begin(), m->inst_elem_off.end(), element_offsets);
+  return AKB_OK;
+}
+
+int akb_batch_set_instance_materials(akb_model *m, const int32_t *material_of_instance) {
+  AKB_TRY(check_model(m, false));
+  if (!material_of_instance) return fail(AKB_EINVAL, "null array");
+  std::vector<int32_t> mat(m->E);
+  for (int k = 0; k < m->ninst; ++k)
+    for (int64_t e = m->inst_elem_off[k]; e < m->inst_elem_off[k + 1]; ++e)
+      mat[e] = material_of_instance[k];
+  return akb_model_set_element_materials(m, mat.data());
 }
 
 int akb_model_destroy(akb_model *m) {
@@ -618,36 +728,68 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   fill_tables(m->et, m->rule, tab, m->nq);
   const int nq = m->nq;
 
-  // internal element order: grouped by material, ascending user id inside
+  // internal element order: grouped by law, then material, ascending user
+  // id inside a material; a law group is one launch per step
+  const int nm = (int)m->mats.size();
+  std::vector<int> mat_order(nm);  // materials sorted by (law, index)
+  for (int k = 0; k < nm; ++k) mat_order[k] = k;
+  std::stable_sort(mat_order.begin(), mat_order.end(),
+                   [&](int x, int y) { return m->mats[x].law < m->mats[y].law; });
   m->perm.resize(E);
   {
-    std::vector<int64_t> count(m->mats.size() + 1, 0);
-    for (int64_t e = 0; e < E; ++e) count[m->mat_user[e] + 1]++;
-    for (size_t k = 0; k < m->mats.size(); ++k) {
-      count[k + 1] += count[k];
-      m->mats[k].e_begin = count[k];
-      m->mats[k].e_count = count[k + 1] - count[k];
+    std::vector<int64_t> count(nm, 0), start(nm, 0);
+    for (int64_t e = 0; e < E; ++e) count[m->mat_user[e]]++;
+    int64_t off = 0;
+    m->groups.clear();
+    for (int k : mat_order) {
+      Material &mt = m->mats[k];
+      start[k] = off;
+      mt.e_begin = off;
+      mt.e_count = count[k];
+      off += count[k];
+      if (m->groups.empty() || m->groups.back().law != mt.law) {
+        Group gr;
+        gr.law = mt.law;
+        gr.mat0 = k;
+        gr.e_begin = mt.e_begin;
+        m->groups.push_back(gr);
+      }
+      Group &gr = m->groups.back();
+      gr.nmat++;
+      gr.e_count += mt.e_count;
+      mt.group = (int)m->groups.size() - 1;
     }
-    for (int64_t e = 0; e < E; ++e) m->perm[count[m->mat_user[e]]++] = e;
+    for (int64_t e = 0; e < E; ++e) m->perm[start[m->mat_user[e]]++] = e;
   }
+  std::vector<int64_t> iperm(E);  // user element -> internal element
+  for (int64_t ie = 0; ie < E; ++ie) iperm[m->perm[ie]] = ie;
   std::vector<int32_t> conn_soa((size_t)nn * E);
   for (int64_t ie = 0; ie < E; ++ie)
     for (int a = 0; a < nn; ++a) conn_soa[(size_t)a * E + ie] = m->conn[m->perm[ie] * nn + a];
-  // node -> slot CSR, slots ascending (= material, user element, local node)
-  // pos: CSR position of slot (a, e), where the element kernel writes the
-  // force of its node a, so the node gather reads its forces contiguously
+  // node -> slot CSR.  A node's slots follow the reference's scatter order of
+  // the internal force: material by material in index order, ascending user
+  // element inside a material (dof_manager.cc:65-120 called per material from
+  // solid_mechanics_model.cc:333-370).  pos: CSR position of slot (a, e),
+  // where the element kernel writes the force of its node a, so the node
+  // gather reads its forces contiguously.  ent: the slots of each node in
+  // the order of the lumped-mass assembly, which runs over all elements of
+  // the type in user order (solid_mechanics_model_mass.cc:115-128).
   std::vector<int32_t> ptr(N + 1, 0), ent((size_t)E * nn), pos((size_t)E * nn);
   for (int64_t ie = 0; ie < E; ++ie)
     for (int a = 0; a < nn; ++a) ptr[conn_soa[(size_t)a * E + ie] + 1]++;
   for (int64_t i = 0; i < N; ++i) ptr[i + 1] += ptr[i];
   {
     std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
-    for (int64_t ie = 0; ie < E; ++ie)
-      for (int a = 0; a < nn; ++a) {
-        const int32_t p = fill[conn_soa[(size_t)a * E + ie]]++;
-        ent[p] = (int32_t)(ie * nn + a);
-        pos[(size_t)a * E + ie] = p;
-      }
+    for (int k = 0; k < nm; ++k) {
+      const Material &mt = m->mats[k];
+      for (int64_t ie = mt.e_begin; ie < mt.e_begin + mt.e_count; ++ie)
+        for (int a = 0; a < nn; ++a) pos[(size_t)a * E + ie] = fill[conn_soa[(size_t)a * E + ie]]++;
+    }
+    std::copy(ptr.begin(), ptr.end() - 1, fill.begin());
+    for (int64_t e = 0; e < E; ++e) {
+      const int64_t ie = iperm[e];
+      for (int a = 0; a < nn; ++a) ent[fill[conn_soa[(size_t)a * E + ie]]++] = (int32_t)(ie * nn + a);
+    }
   }
 
   AKB_TRY(m->alloc(&m->dX, sizeof(double) * N * d));
@@ -704,7 +846,7 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_CUDA(launch_to_float(m->dB, m->fB, E * nq * nn * d, s));
     AKB_CUDA(launch_to_float(m->dwJ, m->fwJ, E * nq, s));
   }
-  for (auto &mt : m->mats) {
+  for (auto &mt : m->groups) {
     if (mt.law != LAW_PLASTIC) continue;
     const int64_t nqp = mt.e_count * nq, dd = (int64_t)d * d;
     for (int b = 0; b < 2; ++b) {
@@ -718,6 +860,39 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     }
     AKB_TRY(m->alloc(&mt.pe, sizeof(double) * nqp));
     AKB_CUDA(cudaMemsetAsync(mt.pe, 0, sizeof(double) * std::max<int64_t>(nqp, 1), s));
+  }
+  // groups of several materials read per-element parameters
+  bool multi = false;
+  for (auto &gr : m->groups) multi |= gr.nmat > 1;
+  if (multi) {
+    std::vector<MatParams> mtab(nm);
+    for (int k = 0; k < nm; ++k) mtab[k] = m->mats[k].params();
+    std::vector<int32_t> mslot(E);
+    for (int64_t ie = 0; ie < E; ++ie) mslot[ie] = m->mat_user[m->perm[ie]];
+    AKB_TRY(m->alloc(&m->dmtab, sizeof(MatParams) * nm));
+    AKB_TRY(m->alloc(&m->dmslot, sizeof(int32_t) * E));
+    AKB_CUDA(cudaMemcpyAsync(m->dmtab, mtab.data(), sizeof(MatParams) * nm, cudaMemcpyHostToDevice, s));
+    AKB_CUDA(cudaMemcpyAsync(m->dmslot, mslot.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
+  }
+  // batch: instance of each node, per-instance time steps, element ranges
+  if (m->ninst > 1) {
+    const int ni = m->ninst;
+    std::vector<int32_t> node_inst(N), perm32(E);
+    for (int k = 0; k < ni; ++k)
+      for (int64_t i = m->inst_node_off[k]; i < m->inst_node_off[k + 1]; ++i) node_inst[i] = k;
+    for (int64_t ie = 0; ie < E; ++ie) perm32[ie] = (int32_t)m->perm[ie];
+    AKB_TRY(m->alloc(&m->dnode_inst, sizeof(int32_t) * N));
+    AKB_TRY(m->alloc(&m->dperm, sizeof(int32_t) * E));
+    AKB_TRY(m->alloc(&m->dinst_dt, sizeof(double) * ni));
+    AKB_TRY(m->alloc(&m->dinst_min, sizeof(double) * ni));
+    AKB_TRY(m->alloc(&m->dinst_eoff, sizeof(int64_t) * (ni + 1)));
+    AKB_CUDA(cudaMemcpyAsync(m->dnode_inst, node_inst.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+    AKB_CUDA(cudaMemcpyAsync(m->dperm, perm32.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice, s));
+    AKB_CUDA(cudaMemcpyAsync(m->dinst_dt, m->inst_dt.data(), sizeof(double) * ni, cudaMemcpyHostToDevice, s));
+    AKB_CUDA(cudaMemcpyAsync(m->dinst_eoff, m->inst_elem_off.data(), sizeof(int64_t) * (ni + 1),
+                             cudaMemcpyHostToDevice, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
   }
   AKB_CUDA(cudaStreamSynchronize(s));
   m->initialized = true;
@@ -790,12 +965,59 @@ int akb_model_get_stable_time_step(akb_model *m, double *dt) {
   if (!dt) return fail(AKB_EINVAL, "null argument");
   DevGeom g = m->geom();
   for (auto &mt : m->mats)
-    AKB_CUDA(launch_element_dt(g, mt.e_begin, mt.e_count, mt.celerity(), m->u(), m->dscratch, m->stream));
+    AKB_CUDA(launch_element_dt(g, mt.e_begin, mt.e_count, mt.celerity(), m->u(), nullptr,
+                               m->dscratch, m->stream));
   return reduce_to_host(m, m->dscratch, m->E, true, dt);
+}
+
+int akb_batch_get_stable_time_steps(akb_model *m, double *dt) {
+  AKB_TRY(check_model(m, true));
+  if (!dt) return fail(AKB_EINVAL, "null argument");
+  if (m->ninst == 1) return akb_model_get_stable_time_step(m, dt);
+  DevGeom g = m->geom();
+  // per-element values in user order, then the minimum over each instance
+  for (auto &mt : m->mats)
+    AKB_CUDA(launch_element_dt(g, mt.e_begin, mt.e_count, mt.celerity(), m->u(), m->dperm,
+                               m->dscratch, m->stream));
+  AKB_CUDA(launch_segment_min(m->dscratch, m->dinst_eoff, m->ninst, m->dinst_min, m->stream));
+  AKB_CUDA(cudaMemcpyAsync(dt, m->dinst_min, sizeof(double) * m->ninst, cudaMemcpyDeviceToHost,
+                           m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+int akb_batch_set_time_steps(akb_model *m, const double *dt) {
+  AKB_TRY(check_model(m, false));
+  if (!dt) return fail(AKB_EINVAL, "null argument");
+  if (m->ninst == 1) return akb_model_set_time_step(m, dt[0]);
+  if (m->inst_dt.empty() || !std::equal(m->inst_dt.begin(), m->inst_dt.end(), dt))
+    m->predicted = false;
+  m->inst_dt.assign(dt, dt + m->ninst);
+  m->dt = *std::min_element(m->inst_dt.begin(), m->inst_dt.end());
+  if (m->dinst_dt) {
+    AKB_CUDA(cudaMemcpyAsync(m->dinst_dt, m->inst_dt.data(), sizeof(double) * m->ninst,
+                             cudaMemcpyHostToDevice, m->stream));
+    AKB_CUDA(cudaStreamSynchronize(m->stream));
+  }
+  return AKB_OK;
+}
+
+int akb_batch_get_time_steps(const akb_model *m, double *dt) {
+  if (!m || !dt) return fail(AKB_EINVAL, "null argument");
+  if (m->ninst == 1) {
+    dt[0] = m->dt;
+    return AKB_OK;
+  }
+  std::copy(m->inst_dt.begin(), m->inst_dt.end(), dt);
+  return AKB_OK;
 }
 
 int akb_model_set_time_step(akb_model *m, double dt) {
   AKB_TRY(check_model(m, false));
+  if (m->ninst > 1) {
+    std::vector<double> all(m->ninst, dt);
+    return akb_batch_set_time_steps(m, all.data());
+  }
   if (dt != m->dt) m->predicted = false;
   m->dt = dt;
   return AKB_OK;
@@ -939,16 +1161,20 @@ int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t
   const int dd = m->dim * m->dim;
   const double *src = nullptr;
   int comps = dd;
+  int64_t ld = mt.e_count;  // row length of the device array [q][comp][ld]
   if (mt.law == LAW_PLASTIC) {
+    const Group &gr = m->groups[mt.group];
     const int c = m->cur;
     switch (field) {
-    case AKB_GRAD_U: src = mt.gu[c]; break;
-    case AKB_STRESS: src = mt.sig[c]; break;
-    case AKB_INELASTIC_STRAIN: src = mt.eps[c]; break;
-    case AKB_ISO_HARDENING: src = mt.iso[c]; comps = 1; break;
-    case AKB_PLASTIC_ENERGY: src = mt.pe; comps = 1; break;
+    case AKB_GRAD_U: src = gr.gu[c]; break;
+    case AKB_STRESS: src = gr.sig[c]; break;
+    case AKB_INELASTIC_STRAIN: src = gr.eps[c]; break;
+    case AKB_ISO_HARDENING: src = gr.iso[c]; comps = 1; break;
+    case AKB_PLASTIC_ENERGY: src = gr.pe; comps = 1; break;
     default: return fail(AKB_EINVAL, "field not defined for plastic_linear_isotropic_hardening");
     }
+    src += mt.e_begin - gr.e_begin;
+    ld = gr.e_count;
   } else {
     if (field != AKB_GRAD_U && field != AKB_STRESS && field != AKB_PIOLA_KIRCHHOFF_2)
       return fail(AKB_EINVAL, "field not defined for this material");
@@ -964,7 +1190,10 @@ int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t
     src = (field == AKB_GRAD_U) ? m->dqp_a : m->dqp_b;
   }
   std::vector<double> soa((size_t)nqp * comps);
-  AKB_CUDA(cudaMemcpyAsync(soa.data(), src, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, m->stream));
+  if (nqp > 0)
+    AKB_CUDA(cudaMemcpy2DAsync(soa.data(), sizeof(double) * mt.e_count, src, sizeof(double) * ld,
+                               sizeof(double) * mt.e_count, (size_t)m->nq * comps,
+                               cudaMemcpyDeviceToHost, m->stream));
   AKB_CUDA(cudaStreamSynchronize(m->stream));
   // device [q][comp][ne] -> reference order [element][q][comp]
   const int64_t ne = mt.e_count;
@@ -996,6 +1225,58 @@ int akb_model_solve_step(akb_model *m, int64_t nsteps) {
     m->forces_evaluated = true;
     m->snap_valid = false;
   }
+  return AKB_OK;
+}
+
+int akb_model_prepare_graphs(akb_model *m) {
+  AKB_TRY(check_model(m, true));
+  if (m->graph_steps == 0) return AKB_OK;
+  bool any_plastic = false;
+  for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
+  if (!m->predicted) {
+    AKB_CUDA(launch_predict(m->geom(), m->dblocked, m->u(), m->dv, m->da, m->dt, m->u_pred(),
+                            m->stream));
+    m->predicted = true;
+  }
+  // captured, not launched: the next solve_step launches it
+  return capture_graph(m, any_plastic);
+}
+
+int akb_model_stream(const akb_model *m, void **stream) {
+  if (!m || !stream) return fail(AKB_EINVAL, "null argument");
+  if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  *stream = m->stream;
+  return AKB_OK;
+}
+
+int akb_model_device_bytes(const akb_model *m, int64_t *bytes) {
+  if (!m || !bytes) return fail(AKB_EINVAL, "null argument");
+  *bytes = (int64_t)m->device_bytes;
+  return AKB_OK;
+}
+
+int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, int precision,
+                              int64_t *bytes) {
+  if (!bytes) return fail(AKB_EINVAL, "null argument");
+  if (et < AKB_TETRAHEDRON_4 || et > AKB_TRIANGLE_6) return fail(AKB_EINVAL, "unknown element type");
+  if (law < LAW_ELASTIC || law > LAW_PLASTIC) return fail(AKB_EINVAL, "unknown law");
+  if (N < 0 || E < 0) return fail(AKB_EINVAL, "negative size");
+  const int64_t nn = nodes_per_element(et), d = dim_of(et);
+  QuadTable tab;
+  int nq = 0;
+  fill_tables(et, rule, tab, nq);
+  // mirrors the allocations of akb_model_init_full (16-byte minimum each)
+  auto r = [](int64_t b) { return std::max<int64_t>(b, 16); };
+  int64_t t = 0;
+  t += r(8 * N * d) + 3 * r(4 * E * nn) + r(4 * (N + 1));
+  t += r(8 * E * nq * nn * d) + r(8 * E * nq);
+  t += 6 * r(8 * N * d) + r(8 * N) + r(N);
+  const int64_t re_bytes = (precision == AKB_PRECISION_MIXED ? 4 : 8) * E * nn * (d == 3 ? 4 : 2);
+  t += r(std::max(re_bytes, 8 * E * nn));
+  t += r(8 * std::max<int64_t>(std::max(E, N), 1)) + 8 * kReducePartials + 4 * 16;
+  if (precision == AKB_PRECISION_MIXED && d == 2) t += r(4 * E * nq * nn * d) + r(4 * E * nq);
+  if (law == LAW_PLASTIC) t += 2 * (3 * r(8 * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
+  *bytes = t;
   return AKB_OK;
 }
 
@@ -1103,18 +1384,23 @@ int akb_model_get_energy(akb_model *m, const char *id, double *value) {
   double total = 0.;
   for (auto &mt : m->mats) {
     if (kind == 1 && mt.law != LAW_PLASTIC) continue;
-    const double *grad = nullptr, *stress = nullptr, *eps = nullptr;
+    const double *grad = nullptr, *stress = nullptr, *eps = nullptr, *pe = nullptr;
+    int64_t ld = mt.e_count;
     if (mt.law == LAW_PLASTIC) {
-      grad = mt.gu[m->cur];
-      stress = mt.sig[m->cur];
-      eps = mt.eps[m->cur];
+      const Group &gr = m->groups[mt.group];
+      const int64_t off = mt.e_begin - gr.e_begin;
+      grad = gr.gu[m->cur] + off;
+      stress = gr.sig[m->cur] + off;
+      eps = gr.eps[m->cur] + off;
+      pe = gr.pe + off;
+      ld = gr.e_count;
     } else {
       AKB_TRY(eval_qp_fields(m, mt));
       grad = m->dqp_a;
       stress = m->dqp_b;
     }
-    AKB_CUDA(launch_energy_elem(g, mt.law, kind, mt.e_begin, mt.e_count, m->dwJ, grad, stress,
-                                eps, mt.pe, mt.params(), m->dscratch, m->stream));
+    AKB_CUDA(launch_energy_elem(g, mt.law, kind, mt.e_begin, mt.e_count, ld, m->dwJ, grad,
+                                stress, eps, pe, mt.params(), m->dscratch, m->stream));
     double s = 0.;
     AKB_TRY(reduce_to_host(m, m->dscratch, mt.e_count, false, &s));
     total += s;

@@ -305,6 +305,12 @@ class SolidMechanicsModel:
         _capi.check(_capi.lib().akb_model_get_energy(self._h, energy_id.encode(), ctypes.byref(v)))
         return v.value
 
+    def getDeviceBytes(self):
+        """Device memory held by the model."""
+        b = ctypes.c_int64()
+        _capi.check(_capi.lib().akb_model_device_bytes(self._h, ctypes.byref(b)))
+        return b.value
+
     def getStatus(self):
         f = ctypes.c_int()
         _capi.check(_capi.lib().akb_model_get_status(self._h, ctypes.byref(f)))
@@ -338,3 +344,75 @@ class SolidMechanicsModel:
 
     def getSpatialDimension(self):
         return self.dim
+
+
+class BatchModel(SolidMechanicsModel):
+    """Many independent meshes of one element type advanced together
+    (akb_batch_create).  The nodal arrays are the instances' arrays one after
+    the other; ``instance_nodes(k)`` / ``instance_elements(k)`` give the
+    slices of instance k.  Each instance may have its own material
+    (``setInstanceMaterials``) and its own time step (``setTimeSteps``)."""
+
+    def __init__(self, meshes, dim=None, id="solid_mechanics_batch"):
+        meshes = list(meshes)
+        if not meshes or not all(isinstance(m, Mesh) for m in meshes):
+            raise TypeError("meshes must be a non-empty list of akantu2_b200.Mesh")
+        et = meshes[0].element_type
+        if any(m.element_type != et for m in meshes):
+            raise ValueError("all instances of a batch have the same element type")
+        sd = meshes[0].spatial_dimension
+        nn = np.array([m.getNbNodes() for m in meshes], dtype=np.int64)
+        ne = np.array([m.getNbElement() for m in meshes], dtype=np.int64)
+        self.node_offsets = np.concatenate([[0], np.cumsum(nn)]).astype(np.int64)
+        self.element_offsets = np.concatenate([[0], np.cumsum(ne)]).astype(np.int64)
+        nodes = np.ascontiguousarray(np.concatenate([m.nodes for m in meshes]), dtype=np.float64)
+        local = np.ascontiguousarray(np.concatenate([m.connectivity for m in meshes]),
+                                     dtype=np.int32)
+        combined = Mesh(sd)
+        combined.set(nodes, local + np.repeat(self.node_offsets[:-1], ne)[:, None].astype(np.int32),
+                     et)
+        self.mesh = combined
+        self.meshes = meshes
+        self.dim = sd if dim is None else dim
+        self.id = id
+        L = _capi.lib()
+        h = ctypes.c_void_p()
+        _capi.check(L.akb_batch_create(self.dim, TYPE_IDS[et], len(meshes), _capi.ptr(nn),
+                                       _capi.ptr(ne), _capi.ptr(nodes), _capi.ptr(local),
+                                       ctypes.byref(h)))
+        self._h = h
+        self._mirrors = {}
+        self._handed_out = set()
+        self._initialized = False
+        self._materials_added = False
+
+    @property
+    def nb_instances(self):
+        return len(self.meshes)
+
+    def instance_nodes(self, k):
+        return slice(int(self.node_offsets[k]), int(self.node_offsets[k + 1]))
+
+    def instance_elements(self, k):
+        return slice(int(self.element_offsets[k]), int(self.element_offsets[k + 1]))
+
+    def setInstanceMaterials(self, material_of_instance):
+        self._imat = np.ascontiguousarray(material_of_instance, dtype=np.int32)
+        _capi.check(_capi.lib().akb_batch_set_instance_materials(self._h, _capi.ptr(self._imat)))
+
+    def getStableTimeSteps(self):
+        self._sync_up()
+        dt = np.zeros(self.nb_instances)
+        _capi.check(_capi.lib().akb_batch_get_stable_time_steps(self._h, _capi.ptr(dt)))
+        return dt
+
+    def setTimeSteps(self, dt):
+        dt = np.ascontiguousarray(dt, dtype=np.float64)
+        if dt.shape != (self.nb_instances,):
+            raise ValueError("one time step per instance")
+        _capi.check(_capi.lib().akb_batch_set_time_steps(self._h, _capi.ptr(dt)))
+
+    def getTimeSteps(self):
+        dt = np.zeros(self.nb_instances)
+        _capi.check(_capi.lib().akb_batch_get_time_steps(self._h, _capi.ptr(dt)))
+        return dt

@@ -17,6 +17,14 @@ dt = 0.8 x stable.  One step = one central-difference step of the whole mesh.
   cpu_baseline  the CPU oracle (restatement of the reference path) on the host
              cores, bounded sample of the same workload
 
+--config batch: 256 independent linear-elastic tet cubes, n cells per edge
+with n uniform in 8..32 (seeded), E log-uniform in [0.5, 2], nu uniform in
+[0.2, 0.4], rho = 1, z = 0 blocked, sinusoidal initial velocity modes with
+wavenumbers 1..4, each instance at 0.8 x its own stable dt, all advanced
+together (one element launch and one node launch per step, 100-step CUDA
+graphs).  Beside the batched mixed and FP64 rates it times the instances one
+model at a time (FP64, a sample of 16 instances) as the unbatched baseline.
+
 --impl reference times the reference's CPU algorithm (the oracle: the
 reference cannot be built here) on all host threads and prints its line.
 N > 1 (torchrun): independent replicas, one mesh per GPU, weak scaling.
@@ -43,7 +51,8 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", default="hex8", choices=["hex8", "tet", "tri6"])
+    p.add_argument("--config", default="hex8", choices=["hex8", "tet", "tri6", "batch"])
+    p.add_argument("--instances", type=int, default=256, help="batch: number of meshes")
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--precisions", default="mixed,fp64")
@@ -90,13 +99,40 @@ def initial_state(config, mesh):
     return v0, blocked
 
 
+def batch_workload(count, seed=7, n_range=(8, 32)):
+    """The batched-instance configuration: meshes, materials, initial states."""
+    import akantu2_b200 as akb
+    rng = np.random.default_rng(seed)
+    meshes, mats, vels, blocks = [], [], [], []
+    for k in range(count):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        mesh = akb.box_tet4(n)
+        E = float(np.exp(rng.uniform(np.log(0.5), np.log(2.0))))
+        nu = float(rng.uniform(0.2, 0.4))
+        mats.append(dict(type="elastic", name=f"instance{k}", rho=1.0, E=E, nu=nu))
+        x = mesh.nodes
+        v = np.zeros_like(x)
+        for _ in range(2):  # two modes per component, wavenumbers 1..4
+            kx, ky, kz = rng.integers(1, 5, size=3)
+            amp = 0.01 * rng.uniform(-1.0, 1.0, size=3)
+            mode = (np.sin(kx * np.pi * x[:, 0]) * np.sin(ky * np.pi * x[:, 1]) *
+                    np.sin(0.5 * kz * np.pi * x[:, 2]))
+            v += amp[None, :] * mode[:, None]
+        b = np.zeros(x.shape, dtype=np.uint8)
+        b[np.isclose(x[:, 2], 0.0)] = 1
+        meshes.append(mesh)
+        vels.append(v)
+        blocks.append(b)
+    return meshes, mats, vels, blocks
+
+
 # algorithmic bytes (formula of the specification, per element-step), and the
 # element-force kernel's own share
 def algorithmic_bytes(config, mesh, precision):
     E, N = mesh.getNbElement(), mesh.getNbNodes()
     n = mesh.connectivity.shape[1]
     d = mesh.spatial_dimension
-    Q = {"hex8": 8, "tet": 1, "tri6": 3}[config]
+    Q = {"hex8": 8, "tet": 1, "tri6": 3, "batch": 1}[config]
     s_e = 8 if precision == "fp64" else 4
     S = (3 * d * d + 1) * 8 if config == "tri6" else 0
     elem = E * (4 * n + Q * (d * n + 1) * s_e + 2 * Q * S)
@@ -211,6 +247,23 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if args.config == "batch":
+        meshes, mats, vels, blocks = batch_workload(args.instances)
+        cpu = cpu_batch_rate(meshes, mats, vels, blocks, threads, budget_s=60.0)
+        E = sum(m.getNbElement() for m in meshes)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": 20, "warmup": 1, "ms_per_step": 1e3 * E / cpu["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{len(meshes)} tet4 elastic cubes, n in 8..32",
+                       "elements": E, "parallelism": f"{threads} host threads"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     mesh, mat, desc = workload(args.config, args.cells)
     v0, blocked = initial_state(args.config, mesh)
     # each timed step is one full step of the workload; the count is bounded
@@ -363,10 +416,187 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def build_batch(akb, meshes, mats, vels, blocks, precision):
+    b = akb.BatchModel(meshes)
+    for mat in mats:
+        b.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+    b.setInstanceMaterials(np.arange(len(meshes)))
+    b.initFull(akb._explicit_lumped_mass, precision=precision)
+    b.setNodal("velocity", np.concatenate(vels))
+    b.setNodal("blocked_dofs", np.concatenate(blocks))
+    b.setTimeSteps(0.8 * b.getStableTimeSteps())
+    return b
+
+
+def run_batch(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    import akantu2_b200 as akb
+    from akantu2_b200 import _capi
+    _capi.check(_capi.lib().akb_set_device(local))
+
+    def barrier():
+        if dist is not None:
+            import torch
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    meshes, mats, vels, blocks = batch_workload(args.instances)
+    E = sum(m.getNbElement() for m in meshes)
+    N = sum(m.getNbNodes() for m in meshes)
+    desc = (f"{len(meshes)} tet4 elastic cubes, n in 8..32 cells per edge "
+            f"({E} elements, {N} nodes)")
+    peak, peak_kind = read_peaks()
+    precisions = [p for p in args.precisions.split(",") if p]
+    results = {}
+    for prec in precisions:
+        b = build_batch(akb, meshes, mats, vels, blocks, prec)
+        b.timeSteps(max(3, args.warmup))
+        barrier()
+        with ClockSampler(local) as clk:
+            ms = b.timeSteps(args.steps)
+        barrier()
+        ms = max_over_ranks(ms)
+        nprof = min(args.steps, 20)
+        _, phases = b.profileSteps(nprof)
+        step_b, kern_b = algorithmic_bytes("batch", b.mesh, prec)
+        elem_ms = phases[1] / nprof
+        results[prec] = {
+            "ms_per_step": ms / args.steps,
+            "value": world * E * args.steps / (ms / 1e3),
+            "phase_ms_per_step": {"predictor": phases[0] / nprof,
+                                  "element_forces": phases[1] / nprof,
+                                  "node_update": phases[2] / nprof},
+            "roofline": {"bound": "hbm", "kernel": "k_element_forces",
+                         "achieved": kern_b / (elem_ms / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": kern_b / (elem_ms / 1e3) / 1e9 / peak,
+                         "traffic": read_traffic("batch", prec),
+                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "roofline_step": {"bytes_per_element_step": step_b / E,
+                              "achieved": step_b / (ms / args.steps / 1e3) / 1e9,
+                              "frac": step_b / (ms / args.steps / 1e3) / 1e9 / peak},
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps * 2,
+            "state_finite": b.getStatus() == 0 and bool(np.all(np.isfinite(b.getDisplacement()))),
+        }
+        if prec == precisions[0]:
+            from akantu2_b200._capi import PinnedArray
+            L = _capi.lib()
+            fext = PinnedArray((N, 3))
+            fext.array[:] = 0.0
+            uout = PinnedArray((N, 3))
+            nb = fext.array.nbytes
+            k_e2e = max(1, min(args.steps, 100))
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(k_e2e):
+                _capi.check(L.akb_model_set_nodal(b._h, _capi.EXTERNAL_FORCE, _capi.ptr(fext.array), nb))
+                _capi.check(L.akb_model_solve_step(b._h, 1))
+                _capi.check(L.akb_model_get_nodal(b._h, _capi.DISPLACEMENT, _capi.ptr(uout.array), nb))
+            secs = max_over_ranks(time.perf_counter() - t0)
+            results[prec]["e2e"] = {"value": world * E * k_e2e / secs, "unit": UNIT,
+                                    "steps": k_e2e, "h2d_bytes_per_step": nb,
+                                    "d2h_bytes_per_step": nb}
+        del b
+    # unbatched baseline: every 16th instance alone (sizes spread over the
+    # range), FP64, same step count with the same graphs
+    alone_e, alone_ms = 0, 0.0
+    for k in range(0, len(meshes), max(1, len(meshes) // 16)):
+        m = akb.SolidMechanicsModel(meshes[k])
+        m.addMaterial(mats[k]["type"], **{kk: v for kk, v in mats[k].items() if kk != "type"})
+        m.initFull(akb._explicit_lumped_mass, precision="fp64")
+        m.setNodal("velocity", vels[k])
+        m.setNodal("blocked_dofs", blocks[k])
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.timeSteps(max(3, args.warmup))
+        alone_ms += m.timeSteps(args.steps)
+        alone_e += meshes[k].getNbElement()
+        del m
+    unbatched = alone_e * args.steps / (alone_ms / 1e3)
+    head = results[precisions[0]]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cpu = cpu_batch_rate(meshes, mats, vels, blocks, threads, budget_s=20.0)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 element math / f64 state" if precisions[0] == "mixed" else "f64",
+            "data": "synthetic (seeded meshes, materials and sinusoidal modes)",
+            "config": {"workload": desc, "instances": len(meshes), "elements": E, "nodes": N,
+                       "quadrature_points": 1, "precision": precisions[0],
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (no flush)"},
+            "e2e": head.get("e2e"), "roofline": head["roofline"],
+            "roofline_step": head["roofline_step"], "clocks": head["clocks"],
+            "gpu_launches": head["gpu_launches"], "state_finite": head["state_finite"],
+            "phase_ms_per_step": head["phase_ms_per_step"],
+            "unbatched_fp64": {"value": unbatched, "unit": UNIT,
+                               "sample": "every 16th instance run alone, FP64"},
+            "cpu_baseline": cpu,
+        }
+        for prec in precisions[1:]:
+            r = results[prec]
+            line[prec] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                          "roofline": r["roofline"], "roofline_step": r["roofline_step"],
+                          "phase_ms_per_step": r["phase_ms_per_step"]}
+        if "fp64" in results and precisions[0] != "fp64":
+            line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
+        line["speedup_vs_unbatched_fp64"] = head["value"] / unbatched
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_batch_rate(meshes, mats, vels, blocks, threads, budget_s):
+    """Oracle element-steps/s over the instances in turn (bounded time)."""
+    from oracle import oracle as orc
+    elems, secs, steps_total, done = 0, 0.0, 0, 0
+    for k in range(len(meshes)):
+        o = orc.OracleModel(orc.TET4, meshes[k].nodes, meshes[k].connectivity, [mats[k]],
+                            threads=threads)
+        o.set(orc.V, vels[k])
+        o.set(orc.BLOCKED, blocks[k])
+        o.set_dt(0.8 * o.stable_dt())
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(20)
+        secs += time.perf_counter() - t0
+        elems += meshes[k].getNbElement() * 20
+        steps_total += 20
+        done += 1
+        if secs > budget_s:
+            break
+    rate = elems / secs
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"20 steps of each of the first {done} instances "
+                      f"(CPU oracle, {threads} threads, {secs:.1f} s)"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -178,6 +178,20 @@ int akb_model_solve_step(akb_model *model, int64_t nsteps);
  * parity, dt, zero external force) and replayed; steps that follow a host
  * edit of u, v, a, the blocked dofs or dt run eagerly first. */
 int akb_model_set_graph_steps(akb_model *model, int64_t steps);
+/* captures the graph that the next solve_step will launch (and enqueues the
+ * predictor it starts from), so that the capture cost is not paid inside the
+ * first solve_step; optional */
+int akb_model_prepare_graphs(akb_model *model);
+/* the model's CUDA stream (a cudaStream_t), for callers that order their own
+ * work after the model's: every model call enqueues on it */
+int akb_model_stream(const akb_model *model, void **stream);
+/* device memory held by the model (bytes allocated so far) */
+int akb_model_device_bytes(const akb_model *model, int64_t *bytes);
+/* upper bound of the device memory akb_model_init_full allocates for a mesh
+ * of one material of law `law` (0 elastic, 1 neohookean, 2 plastic); used
+ * for admission by memory footprint */
+int akb_estimate_device_bytes(int element_type, int quadrature_rule, int64_t nb_nodes,
+                              int64_t nb_elements, int law, int precision, int64_t *bytes);
 int akb_model_synchronize(akb_model *model);
 /* SolidMechanicsModel::assembleInternalForces  solid_mechanics_model.cc:333-370 */
 int akb_model_assemble_internal_forces(akb_model *model);
@@ -197,6 +211,97 @@ int akb_model_profile_steps(akb_model *model, int64_t nsteps, double *total_ms,
 /* device status word: bit 0 = non-finite acceleration seen since the last
  * call (the flag is cleared by reading it) */
 int akb_model_get_status(akb_model *model, int *flags);
+
+/* ---- batches of independent meshes --------------------------------------- */
+/* A batch is a model whose mesh is the disjoint union of nb_instances
+ * independent meshes of one element type (no reference counterpart: the
+ * reference advances one SolidMechanicsModel per mesh).  Every model entry
+ * point applies to it; the nodal arrays are the instances' arrays one after
+ * the other (akb_batch_instance_offsets).  Each step advances all instances
+ * with one element-force launch per constitutive law and one node-update
+ * launch, each instance with its own time step; the result of an instance is
+ * the result of the same mesh run alone (same kernels, same summation order).
+ *   nb_nodes[k], nb_elements[k]: sizes of instance k;
+ *   nodes: [sum N_k][dim], instance after instance;
+ *   connectivity: [sum E_k][n], instance-local node ids (0 .. N_k - 1). */
+int akb_batch_create(int spatial_dimension, int element_type, int nb_instances,
+                     const int64_t *nb_nodes, const int64_t *nb_elements, const double *nodes,
+                     const int32_t *connectivity, akb_model **model);
+int akb_batch_nb_instances(const akb_model *model, int *count);
+/* first node / element of each instance, arrays of nb_instances + 1 (either
+ * may be NULL) */
+int akb_batch_instance_offsets(const akb_model *model, int64_t *node_offsets,
+                               int64_t *element_offsets);
+/* material index of every element of instance k (before initFull) */
+int akb_batch_set_instance_materials(akb_model *model, const int32_t *material_of_instance);
+/* getStableTimeStep of every instance -> dt[nb_instances] */
+int akb_batch_get_stable_time_steps(akb_model *model, double *dt);
+/* setTimeStep per instance (akb_model_set_time_step sets them all) */
+int akb_batch_set_time_steps(akb_model *model, const double *dt);
+int akb_batch_get_time_steps(const akb_model *model, double *dt);
+
+/* ---- serving: many solves resident on one GPU ---------------------------- */
+/* No reference counterpart (the reference runs one model per process).  A
+ * server admits submitted solves in arrival order while their estimated
+ * device memory (akb_estimate_device_bytes) fits in its budget and fewer
+ * than max_active are resident; each admitted solve gets its own model and
+ * stream, is prepared by a builder thread (tables, lumped mass, stable time
+ * step, step graph) and then advanced chunk by chunk by the scheduler thread
+ * together with every other resident solve, so that their kernels overlap on
+ * the device.  Arrivals are folded into the running set as soon as memory
+ * and a slot are free.  A solve's result does not depend on what else runs
+ * (each solve is computed exactly as by a model of its own). */
+typedef struct akb_server akb_server;
+typedef struct {
+  int device;            /* CUDA device                                        */
+  int max_active;        /* resident solves at most (<= 0: 64)                 */
+  int64_t device_bytes;  /* admission budget (<= 0: 80% of the free memory)    */
+  int64_t chunk_steps;   /* steps enqueued per solve and scheduling pass
+                            (<= 0: 500; multiples of 100 use the step graphs)  */
+  int builders;          /* host threads preparing and finishing solves (<= 0: 4) */
+} akb_server_config;
+
+typedef struct {
+  int element_type, quadrature_rule, precision;
+  int64_t nb_nodes, nb_elements;
+  const double *nodes;           /* [N][dim]                                   */
+  const int32_t *connectivity;   /* [E][n]                                     */
+  const char *material_type;     /* elastic | neohookean | plastic_linear_...  */
+  const char *material_params;   /* "E = 1; nu = 0.3; rho = 1" (may be NULL)   */
+  const double *displacement;    /* initial u [N][dim] or NULL (zero)          */
+  const double *velocity;        /* initial v [N][dim] or NULL (zero)          */
+  const uint8_t *blocked_dofs;   /* [N][dim] or NULL (none)                    */
+  double dt_factor;              /* dt = dt_factor * stable dt (<= 0: 0.8)     */
+  int64_t nb_steps;
+  double *displacement_out;      /* [N][dim] final u, or NULL; caller-owned,
+                                    written before the completion is reported */
+  double *velocity_out;          /* [N][dim] final v, or NULL                 */
+} akb_request;
+
+typedef struct {
+  int64_t id;
+  int status;                    /* AKB_OK or the error of the failed step     */
+  char message[256];
+  double t_submit, t_admit, t_start, t_end; /* seconds on the server's clock   */
+  int64_t nb_elements, nb_steps, device_bytes;
+  double dt;
+} akb_completion;
+
+typedef struct {
+  int64_t queued, building, running, finishing, completed_unpolled;
+  int64_t device_bytes_reserved, device_bytes_budget;
+  double now;                    /* the server's clock, seconds                */
+} akb_server_stats;
+
+int akb_server_create(const akb_server_config *config, akb_server **server);
+/* copies the request's inputs; AKB_ENOMEM if it can never fit the budget */
+int akb_server_submit(akb_server *server, const akb_request *request, int64_t *id);
+/* up to `capacity` completions, waiting at most wait_seconds for the first */
+int akb_server_poll(akb_server *server, akb_completion *out, int capacity, int *count,
+                    double wait_seconds);
+int akb_server_get_stats(akb_server *server, akb_server_stats *stats);
+/* drops queued solves, waits for the admitted ones, joins the threads */
+int akb_server_destroy(akb_server *server);
 
 /* ---- stable time step without allocation -------------------------------- */
 /* This entry point has no counterpart in the reference.  It computes the

@@ -366,7 +366,8 @@ struct or_model {
   std::vector<uint8_t> blocked;
   std::vector<double> re;  // [slot][n][d]
   std::vector<int64_t> node_ptr;
-  std::vector<int64_t> node_ent;
+  std::vector<int64_t> node_ent;       // internal-force scatter order
+  std::vector<int64_t> node_ent_mass;  // lumped-mass scatter order
   double dt = 0.;
   int threads = 1;
 };
@@ -419,16 +420,27 @@ void assign_materials(or_model *m) {
       }
     }
   }
+  // the lumped mass is assembled over all elements of the type in element
+  // order, whatever their material (solid_mechanics_model_mass.cc:115-128)
+  std::vector<int64_t> slot_of_elem(m->E);
+  for (int k = 0; k < nm; ++k)
+    for (size_t le = 0; le < m->st[k].elems.size(); ++le)
+      slot_of_elem[m->st[k].elems[le]] = m->st[k].offset + (long)le;
+  m->node_ent_mass.assign(m->node_ptr[m->N], 0);
+  std::copy(m->node_ptr.begin(), m->node_ptr.end() - 1, fill.begin());
+  for (long e = 0; e < m->E; ++e)
+    for (int a = 0; a < m->n; ++a)
+      m->node_ent_mass[fill[m->conn[e * m->n + a]]++] = slot_of_elem[e] * m->n + a;
   m->re.assign((size_t)m->E * m->n * m->d, 0.);
 }
 
 // gather r_e into a nodal array with factor -1 (internal force) or +1 (mass)
 void gather(or_model *m, double scale, std::vector<double> &out, int ncomp_src,
-            int ncomp_dst) {
+            int ncomp_dst, const std::vector<int64_t> &ent) {
 parallel_for(m->N, m->threads, [&](long i) {
     double acc[3] = {0., 0., 0.};
     for (int64_t p = m->node_ptr[i]; p < m->node_ptr[i + 1]; ++p) {
-      const double *r = &m->re[(size_t)m->node_ent[p] * ncomp_src];
+      const double *r = &m->re[(size_t)ent[p] * ncomp_src];
       for (int c = 0; c < ncomp_src; ++c) acc[c] += scale * r[c];
     }
     for (int c = 0; c < ncomp_dst; ++c)
@@ -461,7 +473,7 @@ parallel_for((long)s.elems.size(), m->threads, [&](long le) {
     });
   }
   m->mass.assign((size_t)m->N * m->d, 0.);
-  gather(m, 1., m->mass, 1, m->d);
+  gather(m, 1., m->mass, 1, m->d, m->node_ent_mass);
 }
 
 // gradient, stress and elemental force of one material's elements
@@ -581,7 +593,7 @@ parallel_for(ne, m->threads, [&](long le) {
 
 void internal_forces(or_model *m, bool history_step) {
   for (size_t k = 0; k < m->st.size(); ++k) element_forces(m, (int)k, history_step);
-  gather(m, -1., m->fint, m->d, m->d);
+  gather(m, -1., m->fint, m->d, m->d, m->node_ent);
 }
 
 void save_previous(or_model *m) {

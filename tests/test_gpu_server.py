@@ -1,0 +1,110 @@
+"""The serving loop: admission by device-memory footprint, overlap of resident
+solves, and results that do not depend on what else was running."""
+import time
+
+import numpy as np
+import pytest
+
+import akantu2_b200 as akb
+from scenarios import UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC
+
+pytestmark = pytest.mark.gpu
+
+LAWS = [UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC]
+
+
+def _request(k, rng):
+    kind = ("tet", "hex", "tri6")[k % 3]
+    n = int(rng.integers(2, 7))
+    mesh = {"tet": akb.box_tet4, "hex": akb.box_hex8, "tri6": akb.square_tri6}[kind](n)
+    mat = dict(LAWS[int(rng.integers(0, 3))])
+    mat.pop("name")
+    x = mesh.nodes
+    d = x.shape[1]
+    v = np.zeros_like(x)
+    v[:, d - 1] = 0.01 * np.sin(np.pi * x[:, 0]) * x[:, d - 1]
+    if kind == "tri6":
+        v[:, 0] = 0.02 * x[:, 0]
+    b = np.zeros(x.shape, dtype=np.uint8)
+    b[np.isclose(x[:, d - 1 if kind != "tri6" else 0], 0.0)] = 1
+    steps = int(rng.integers(50, 450))
+    precision = ("fp64", "mixed")[int(rng.integers(0, 2))]
+    return dict(mesh=mesh, material=mat, steps=steps, velocity=v, blocked=b, precision=precision)
+
+
+def _alone(req):
+    m = akb.SolidMechanicsModel(req["mesh"])
+    mat = req["material"]
+    m.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+    m.initFull(akb._explicit_lumped_mass, precision=req["precision"])
+    m.setNodal("velocity", req["velocity"])
+    m.setNodal("blocked_dofs", req["blocked"])
+    m.setTimeStep(0.8 * m.getStableTimeStep())
+    m.solveStep(req["steps"])
+    return m.getDisplacement(), m.getVelocity()
+
+
+def test_results_same_alone_and_in_the_mix():
+    rng = np.random.default_rng(3)
+    reqs = [_request(k, rng) for k in range(14)]
+    srv = akb.Server(max_active=5, chunk_steps=100, builders=3)
+    ids = {}
+    for k, r in enumerate(reqs):
+        rid, out = srv.submit(r["mesh"], r["material"], r["steps"], velocity=r["velocity"],
+                              blocked=r["blocked"], precision=r["precision"], want_velocity=True)
+        ids[rid] = (k, out)
+        if k == 6:
+            time.sleep(0.05)  # later arrivals join a running set
+    done = srv.drain(timeout=300)
+    srv.close()
+    assert sorted(c["id"] for c in done) == sorted(ids)
+    for c in done:
+        assert c["status"] == 0, c["message"]
+        assert c["t_submit"] <= c["t_admit"] <= c["t_start"] <= c["t_end"]
+        k, out = ids[c["id"]]
+        u, v = _alone(reqs[k])
+        assert np.array_equal(out["displacement"], u), f"request {k}"
+        assert np.array_equal(out["velocity"], v), f"request {k}"
+        assert np.abs(u).max() > 0
+
+
+def test_admission_respects_the_memory_budget():
+    rng = np.random.default_rng(8)
+    reqs = [_request(3 * k, rng) for k in range(8)]  # tet meshes
+    for r in reqs:
+        r["steps"] = 400
+    est = [akb.Server.estimate_bytes(r["mesh"], r["material"], r["precision"]) for r in reqs]
+    budget = int(2.5 * max(est))
+    srv = akb.Server(max_active=16, device_bytes=budget, chunk_steps=100)
+    for r in reqs:
+        srv.submit(r["mesh"], r["material"], r["steps"], velocity=r["velocity"],
+                   blocked=r["blocked"], precision=r["precision"])
+    peak = 0
+    done = []
+    while len(done) < len(reqs):
+        st = srv.stats()
+        assert st["device_bytes_reserved"] <= budget
+        peak = max(peak, st["device_bytes_reserved"])
+        done += srv.poll(wait=0.002)
+    srv.close()
+    assert all(c["status"] == 0 for c in done)
+    assert 0 < peak <= budget
+    too_big = akb.box_tet4(8)
+    srv = akb.Server(device_bytes=1 << 16)
+    with pytest.raises(akb.AkbError) as e:
+        srv.submit(too_big, dict(type="elastic", E=1.0, nu=0.3, rho=1.0), 10)
+    assert e.value.name == "AKB_ENOMEM"
+    srv.close()
+
+
+def test_estimate_bounds_the_allocation():
+    for mesh, mat, prec in [(akb.box_tet4(5), UNIT_ELASTIC, "fp64"),
+                            (akb.box_hex8(4), UNIT_NEOHOOKEAN, "mixed"),
+                            (akb.square_tri6(6), UNIT_PLASTIC, "mixed"),
+                            (akb.square_tri6(6), UNIT_PLASTIC, "fp64")]:
+        m = akb.SolidMechanicsModel(mesh)
+        m.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+        m.initFull(akb._explicit_lumped_mass, precision=prec)
+        used = m.getDeviceBytes()
+        est = akb.Server.estimate_bytes(mesh, mat, prec)
+        assert used <= est <= used + 4096, (mesh.element_type, prec, used, est)

@@ -117,6 +117,28 @@ def test_create_rejects_bad_connectivity():
     assert e.value.name == "AKB_EINVAL"
 
 
+def test_batch_offsets_and_local_connectivity():
+    meshes = [akb.box_tet4(1), akb.box_tet4(2), akb.box_hex8(1)]
+    with pytest.raises(ValueError):
+        akb.BatchModel(meshes)  # mixed element types
+    b = akb.BatchModel(meshes[:2])
+    assert b.nb_instances == 2
+    off_n = np.zeros(3, dtype=np.int64)
+    off_e = np.zeros(3, dtype=np.int64)
+    _capi.check(_capi.lib().akb_batch_instance_offsets(b._h, _capi.ptr(off_n), _capi.ptr(off_e)))
+    assert list(off_n) == [0, 8, 35] and list(off_e) == [0, 6, 54]
+    assert np.array_equal(off_n, b.node_offsets) and np.array_equal(off_e, b.element_offsets)
+    # the combined mesh refers to global node ids
+    assert b.mesh.connectivity[b.instance_elements(1)].min() == 8
+    # an instance-local id past its own nodes is rejected, even when it would
+    # be a valid id of the concatenated array
+    bad = akb.Mesh(3).set(meshes[1].nodes, meshes[1].connectivity, akb._tetrahedron_4)
+    bad.connectivity[0, 0] = meshes[1].getNbNodes()
+    with pytest.raises(akb.AkbError) as e:
+        akb.BatchModel([bad, meshes[0]])
+    assert e.value.name == "AKB_EINVAL"
+
+
 def _write_msh(path, nodes, conn, gtype):
     with open(path, "w") as f:
         f.write("$MeshFormat\n2.1 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(nodes))
