@@ -36,11 +36,26 @@ inline unsigned grid_for(int64_t n, int threads = kThreads) {
     }                                                                     \
   } while (0)
 
+// threads per block of the per-element kernels: 64, 128 or 256
+#define AKB_DISPATCH_BLOCK(b, ...)                                       \
+  do {                                                                    \
+    if ((b) == 64) {                                                      \
+      constexpr int BLOCK = 64;                                           \
+      __VA_ARGS__;                                                        \
+    } else if ((b) == 256) {                                              \
+      constexpr int BLOCK = 256;                                          \
+      __VA_ARGS__;                                                        \
+    } else {                                                              \
+      constexpr int BLOCK = 128;                                          \
+      __VA_ARGS__;                                                        \
+    }                                                                     \
+  } while (0)
+
 template <class T, class RT>
 inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const T *B, const T *wJ, const double *u,
                                        const MatParams &mp, const GroupArgs &ps, RT *re,
-                                       cudaStream_t s) {
+                                       const ElemTuning &tn, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
@@ -59,16 +74,18 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
         k_element_forces_pq<D, NN, NQ, LAW_PLASTIC>
             <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
     } else {
-      const unsigned grid = (unsigned)((ne + kPeThreads - 1) / kPeThreads);
-      if (law == LAW_ELASTIC)
-        k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT>
-            <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
-      else if (law == LAW_NEOHOOKEAN)
-        k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT>
-            <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
-      else
-        k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT>
-            <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      AKB_DISPATCH_BLOCK(tn.block, {
+        const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
+        if (law == LAW_ELASTIC)
+          k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>
+              <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+        else if (law == LAW_NEOHOOKEAN)
+          k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>
+              <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+        else
+          k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>
+              <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      });
     }
   });
   return cudaGetLastError();

@@ -429,10 +429,10 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
   }
 }
 
-constexpr int kPeThreads = 128;
-
-template <int D, int NN, int NQ, int LAW, class T, class RT>
-__global__ void __launch_bounds__(kPeThreads)
+// BLOCK: threads (= elements) per block, one of the launch shapes the
+// autotuner chooses from
+template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
     k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const T *__restrict__ B, const T *__restrict__ wJ,
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(kPeThreads)
                         RT *__restrict__ re) {
   constexpr int ND = NN * D;
   constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
-  const int64_t le = (int64_t)blockIdx.x * kPeThreads + threadIdx.x;
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
@@ -484,15 +484,15 @@ __global__ void __launch_bounds__(kPeThreads)
 // k_precompute, in FP32, with coordinates and displacements taken relative
 // to the element's first node -- dN/ds sums to zero over the nodes, so the
 // Jacobian and the gradient are unchanged in exact arithmetic).
-template <int D, int NN, int NQ, int LAW>
-__global__ void __launch_bounds__(kPeThreads)
+template <int D, int NN, int NQ, int LAW, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
     k_element_forces_geo(int64_t e_begin, int64_t e_count, int64_t E,
                          const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                          const double *__restrict__ X, QuadTable tab,
                          const double *__restrict__ u, MatParams mp, GroupArgs ps,
                          float *__restrict__ re) {
   constexpr int ND = NN * D;
-  const int64_t le = (int64_t)blockIdx.x * kPeThreads + threadIdx.x;
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
@@ -552,6 +552,174 @@ __global__ void __launch_bounds__(kPeThreads)
   }
 #pragma unroll
   for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
+}
+
+// Mixed path, _hexahedron_8: sum factorisation of the trilinear element.
+// With node a at signs (sx, sy, sz) in {-1, 1}^3, N_a = (1 + sx xi)(1 + sy eta)
+// (1 + sz zeta) / 8, so a nodal field f has the modal form
+//   f(xi) = (W_0 + W_1 xi + W_2 eta + W_3 xi eta + W_4 zeta + W_5 xi zeta
+//            + W_6 eta zeta + W_7 xi eta zeta) / 8,
+// W_m = sum_a f_a prod_{d in m} s_{a,d} (m a bit set over x, y, z): an 8-point
+// Walsh-Hadamard transform of the nodal values.  The Jacobian and the
+// displacement derivative at a Gauss point (all coordinates +-1/sqrt(3)) are
+// then a few signed sums of the W_m, and the elemental force
+//   r_a = sum_q P_q J_q^-1 dN_a/dxi(q)
+// (P_q the weighted flux: w sigma, or w F S) is accumulated in the same modal
+// basis and brought back to the nodes by the inverse transform.  Equal to the
+// dN/dx form of k_element_forces_geo in exact arithmetic, with about 40% fewer
+// floating-point operations per point.  The factors 1/8 cancel between the
+// Jacobian and its inverse and are folded into det J.
+__device__ __forceinline__ void wht8(float (*v)[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+      if (!(l & (1 << d))) {
+        const int h = l | (1 << d);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float a = v[l][c], b = v[h][c];
+          v[l][c] = a + b;
+          v[h][c] = b - a;
+        }
+      }
+}
+__device__ __forceinline__ void iwht8(float (*v)[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+      if (!(l & (1 << d))) {
+        const int h = l | (1 << d);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float a = v[l][c], b = v[h][c];
+          v[l][c] = a - b;
+          v[h][c] = a + b;
+        }
+      }
+}
+
+// weighted flux P of one point for the mixed path: r_a = P . dN_a/dx
+template <int D, int LAW>
+__device__ __forceinline__ void mixed_flux(const float *g, float w, const MatParams &mp,
+                                           const GroupArgs &ps, int64_t ne, int64_t le, int q,
+                                           float *P) {
+  if constexpr (LAW == LAW_NEOHOOKEAN) {
+    float S[D * D];
+    neohookean_pk2<D, float>((float)mp.lambda, (float)mp.mu, g, S);
+    first_piola<D, float>(g, S, w, P);
+  } else if constexpr (LAW == LAW_ELASTIC) {
+    float sig[D * D];
+    elastic_stress<D, float>((float)mp.lambda, (float)mp.mu, g, (float)mp.sigma_th, sig);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P[k] = sig[k] * w;
+  } else {
+    double gd[D * D], sd[D * D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) gd[k] = (double)g[k];
+    plastic_point<D>(mp, ps, ne, le, q, gd, sd);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P[k] = (float)sd[k] * w;
+  }
+}
+
+// QU: quadrature points per unrolled iteration (1, 2, 4 or 8)
+template <int LAW, int BLOCK, int QU>
+__global__ void __launch_bounds__(BLOCK)
+    k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
+                            const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                            const double *__restrict__ X, const double *__restrict__ u,
+                            MatParams mp, GroupArgs ps, float *__restrict__ re) {
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count) return;
+  const int64_t e = e_begin + le;
+  const MatParams mpe = group_params(mp, ps, le);
+  // reference node a sits at lexicographic corner lex[a] = [sx>0] + 2[sy>0] + 4[sz>0]
+  constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+  float wx[8][3], wu[8][3];
+  double x0[3], u0[3];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double x = X[node * 3 + i], uu = u[node * 3 + i];
+      if (a == 0) {
+        x0[i] = x;
+        u0[i] = uu;
+      }
+      wx[lex[a]][i] = (float)(x - x0[i]);
+      wu[lex[a]][i] = (float)(uu - u0[i]);
+    }
+  }
+  wht8(wx);
+  wht8(wu);
+  constexpr float g1 = 0.577350269189625764509f;  // Gauss coordinate 1/sqrt(3)
+  constexpr float g2 = 1.f / 3.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    wx[3][c] *= g1; wx[5][c] *= g1; wx[6][c] *= g1; wx[7][c] *= g2;
+    wu[3][c] *= g1; wu[5][c] *= g1; wu[6][c] *= g1; wu[7][c] *= g2;
+  }
+  float A[8][3];
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) A[m][c] = 0.f;
+#pragma unroll 1
+  for (int qo = 0; qo < 8; qo += QU)
+#pragma unroll
+  for (int qi = 0; qi < QU; ++qi) {
+    const int q = qo + qi;
+    // point q at (xi, eta, zeta) = g1 (sx, sy, sz), the order of the rule
+    const float sx = (q & 1) ? 1.f : -1.f, sy = (q & 2) ? 1.f : -1.f, sz = (q & 4) ? 1.f : -1.f;
+    float Jp[9], Dp[9], Ji[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      // 8 d(X_j)/d(xi_k) at row k, 8 d(u_j)/d(xi_k) likewise
+      Jp[0 + 3 * j] = wx[1][j] + sy * wx[3][j] + sz * wx[5][j] + sy * sz * wx[7][j];
+      Jp[1 + 3 * j] = wx[2][j] + sx * wx[3][j] + sz * wx[6][j] + sx * sz * wx[7][j];
+      Jp[2 + 3 * j] = wx[4][j] + sx * wx[5][j] + sy * wx[6][j] + sx * sy * wx[7][j];
+      Dp[0 + 3 * j] = wu[1][j] + sy * wu[3][j] + sz * wu[5][j] + sy * sz * wu[7][j];
+      Dp[1 + 3 * j] = wu[2][j] + sx * wu[3][j] + sz * wu[6][j] + sx * sz * wu[7][j];
+      Dp[2 + 3 * j] = wu[4][j] + sx * wu[5][j] + sy * wu[6][j] + sx * sy * wu[7][j];
+    }
+    const float det8 = det3(Jp);  // 512 det J
+    inv3(Jp, Ji);                 // J^-1 / 8
+    // grad u (i, j) = sum_k J^-1(j, k) du_i/dxi_k  (the factors 8 cancel)
+    float gr[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        gr[i + 3 * j] = Ji[j] * Dp[0 + 3 * i] + Ji[j + 3] * Dp[1 + 3 * i] +
+                        Ji[j + 6] * Dp[2 + 3 * i];
+    const float w = det8 * (1.f / 512.f);  // 2 x 2 x 2 Gauss weights are 1
+    float P[9];
+    mixed_flux<3, LAW>(gr, w, mpe, ps, e_count, le, q, P);
+    // H(k, m) = sum_J P(k, J) J^-1(J, m), accumulated per mode
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float H0 = P[k] * Ji[0] + P[k + 3] * Ji[1] + P[k + 6] * Ji[2];
+      const float H1 = P[k] * Ji[3] + P[k + 3] * Ji[4] + P[k + 6] * Ji[5];
+      const float H2 = P[k] * Ji[6] + P[k + 3] * Ji[7] + P[k + 6] * Ji[8];
+      A[1][k] += H0;
+      A[2][k] += H1;
+      A[4][k] += H2;
+      A[3][k] += sy * H0 + sx * H1;
+      A[5][k] += sz * H0 + sx * H2;
+      A[6][k] += sz * H1 + sy * H2;
+      A[7][k] += sy * sz * H0 + sx * sz * H1 + sx * sy * H2;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    A[3][c] *= g1; A[5][c] *= g1; A[6][c] *= g1; A[7][c] *= g2;
+  }
+  iwht8(A);
+#pragma unroll
+  for (int a = 0; a < 8; ++a) store_slot<3>(re, pos[(int64_t)a * E + e], A[lex[a]]);
 }
 
 // FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q

@@ -83,21 +83,22 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
                                        const MatParams &mp, const GroupArgs &ps,
-                                       double *re, cudaStream_t s) {
-  return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, s);
+                                       double *re, const ElemTuning &tn, cudaStream_t s) {
+  return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, tn, s);
 }
 
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
-                                    double dt, int flags, unsigned int *status, cudaStream_t s) {
+                                    double dt, int flags, unsigned int *status, int node_block,
+                                    cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
-    k_node_update<3, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
+    k_node_update<3, double, false><<<grid_for(g.N, node_block), node_block, 0, s>>>(
         g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
         flags, status);
   else
-    k_node_update<2, double, false><<<grid_for(g.N), kThreads, 0, s>>>(
+    k_node_update<2, double, false><<<grid_for(g.N, node_block), node_block, 0, s>>>(
         g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
         flags, status);
   return cudaGetLastError();

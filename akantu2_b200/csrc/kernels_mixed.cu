@@ -5,25 +5,67 @@
 
 namespace akb {
 
+namespace {
+
+template <int LAW, int BLOCK, int QU>
+void launch_hex8sf(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
+                   const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
+  const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
+  k_element_forces_hex8sf<LAW, BLOCK, QU>
+      <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, u, mp, ps, re);
+}
+
+// the tuned shapes of the sum-factorised kernel: 128 threads with 8, 2 or 1
+// points per iteration, 64 or 256 threads with all 8 unrolled
+template <int LAW>
+void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
+                     const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
+                     cudaStream_t s) {
+  if (tn.qu == 1)
+    launch_hex8sf<LAW, 128, 1>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.qu == 2)
+    launch_hex8sf<LAW, 128, 2>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.block == 64)
+    launch_hex8sf<LAW, 64, 8>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.block == 256)
+    launch_hex8sf<LAW, 256, 8>(g, e0, ne, u, mp, ps, re, s);
+  else
+    launch_hex8sf<LAW, 128, 8>(g, e0, ne, u, mp, ps, re, s);
+}
+
+}  // namespace
+
 cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                         const QuadTable &tab, const float *fB,
                                         const float *fwJ, const double *u,
                                         const MatParams &mp, const GroupArgs &ps,
-                                        float *re, cudaStream_t s) {
+                                        float *re, const ElemTuning &tn, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
-  if (g.D == 2) return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, s);
+  if (g.D == 2)
+    return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, tn, s);
+  if (g.et == ET_HEX8 && tn.qu > 0) {
+    if (law == LAW_ELASTIC)
+      dispatch_hex8sf<LAW_ELASTIC>(tn, g, e0, ne, u, mp, ps, re, s);
+    else if (law == LAW_NEOHOOKEAN)
+      dispatch_hex8sf<LAW_NEOHOOKEAN>(tn, g, e0, ne, u, mp, ps, re, s);
+    else
+      dispatch_hex8sf<LAW_PLASTIC>(tn, g, e0, ne, u, mp, ps, re, s);
+    return cudaGetLastError();
+  }
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
-    const unsigned grid = (unsigned)((ne + kPeThreads - 1) / kPeThreads);
-    if (law == LAW_ELASTIC)
-      k_element_forces_geo<D, NN, NQ, LAW_ELASTIC>
-          <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
-    else if (law == LAW_NEOHOOKEAN)
-      k_element_forces_geo<D, NN, NQ, LAW_NEOHOOKEAN>
-          <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
-    else
-      k_element_forces_geo<D, NN, NQ, LAW_PLASTIC>
-          <<<grid, kPeThreads, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
+    AKB_DISPATCH_BLOCK(tn.block, {
+      const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
+      if (law == LAW_ELASTIC)
+        k_element_forces_geo<D, NN, NQ, LAW_ELASTIC, BLOCK>
+            <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
+      else if (law == LAW_NEOHOOKEAN)
+        k_element_forces_geo<D, NN, NQ, LAW_NEOHOOKEAN, BLOCK>
+            <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
+      else
+        k_element_forces_geo<D, NN, NQ, LAW_PLASTIC, BLOCK>
+            <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
+    });
   });
   return cudaGetLastError();
 }
@@ -32,14 +74,14 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,
                                      double *u_next, double dt, int flags,
-                                     unsigned int *status, cudaStream_t s) {
+                                     unsigned int *status, int node_block, cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
   if (g.D == 3)
-    k_node_update<3, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
+    k_node_update<3, float, true><<<grid_for(g.N, node_block), node_block, 0, s>>>(
         g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
         flags, status);
   else
-    k_node_update<2, float, true><<<grid_for(g.N), kThreads, 0, s>>>(
+    k_node_update<2, float, true><<<grid_for(g.N, node_block), node_block, 0, s>>>(
         g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
         flags, status);
   return cudaGetLastError();

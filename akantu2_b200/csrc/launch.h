@@ -13,6 +13,15 @@ namespace akb {
 struct QuadTable;
 struct GroupArgs;
 
+// launch shape of the element-force kernel of one law group: threads per
+// block (64, 128 or 256) and, for the mixed _hexahedron_8 kernel, the
+// quadrature points per unrolled iteration (1, 2 or 8; 0 selects the dN/dx
+// form).  All shapes give the same arithmetic per element.
+struct ElemTuning {
+  int block = 128;
+  int qu = 8;
+};
+
 // device view of the mesh, internal element order
 struct DevGeom {
   int et, D, NN, NQ;
@@ -53,7 +62,7 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
                                        const MatParams &mp, const GroupArgs &ps,
-                                       double *re, cudaStream_t s);
+                                       double *re, const ElemTuning &tn, cudaStream_t s);
 // mixed path: 3D elements recompute their shape derivatives in FP32 from g.X
 // and the table; 2D elements stream FP32 copies (fB, fwJ) of the precomputed
 // ones (their state traffic dominates, the recomputation would not pay)
@@ -61,18 +70,20 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
                                         const QuadTable &tab, const float *fB,
                                         const float *fwJ, const double *u,
                                         const MatParams &mp, const GroupArgs &ps,
-                                        float *re, cudaStream_t s);
+                                        float *re, const ElemTuning &tn, cudaStream_t s);
 // flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
 // the predictor of the next step reads u and writes u_next
+// node_block: threads per block of the node update (any multiple of 32 up to 1024)
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
-                                    double dt, int flags, unsigned int *status, cudaStream_t s);
+                                    double dt, int flags, unsigned int *status, int node_block,
+                                    cudaStream_t s);
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,
                                      double *u_next, double dt, int flags,
-                                     unsigned int *status, cudaStream_t s);
+                                     unsigned int *status, int node_block, cudaStream_t s);
 
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,

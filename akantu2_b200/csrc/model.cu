@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <string>
 #include <vector>
@@ -68,6 +69,7 @@ struct Material {
 // (material e_begin - group e_begin).
 struct Group {
   int law = LAW_ELASTIC;
+  ElemTuning tune;  // launch shape of the group's element-force kernel
   int mat0 = 0;  // first material of the group
   int nmat = 0;
   int64_t e_begin = 0, e_count = 0;
@@ -219,6 +221,7 @@ struct akb_model {
   };
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
+  int node_block = 256;       // threads per block of the node update
 
   double *u() const { return dU[ucur]; }
   double *u_pred() const { return dU[1 - ucur]; }
@@ -365,10 +368,10 @@ int element_forces(akb_model *m, bool in_step) {
     cudaError_t e;
     if (m->precision == AKB_PRECISION_MIXED)
       e = launch_element_forces_mixed(g, gr.law, gr.e_begin, gr.e_count, m->tab, m->fB, m->fwJ,
-                                      u, mp, ps, (float *)m->dre, m->stream);
+                                      u, mp, ps, (float *)m->dre, gr.tune, m->stream);
     else
       e = launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ, u, mp,
-                                     ps, (double *)m->dre, m->stream);
+                                     ps, (double *)m->dre, gr.tune, m->stream);
     if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("element forces: ") + cudaGetErrorString(e));
   }
   return AKB_OK;
@@ -389,11 +392,11 @@ int node_update(akb_model *m, bool correct) {
   if (m->precision == AKB_PRECISION_MIXED)
     e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass, m->dblocked,
                                  m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
-                                 m->stream);
+                                 m->node_block, m->stream);
   else
     e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass, m->dblocked,
                                 m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
-                                m->stream);
+                                m->node_block, m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
   m->fint_valid = !correct;
   return AKB_OK;
@@ -755,6 +758,8 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
         m->groups.push_back(gr);
       }
       Group &gr = m->groups.back();
+      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED && gr.law == LAW_PLASTIC)
+        gr.tune.qu = 1;
       gr.nmat++;
       gr.e_count += mt.e_count;
       mt.group = (int)m->groups.size() - 1;
@@ -1277,6 +1282,157 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   if (precision == AKB_PRECISION_MIXED && d == 2) t += r(4 * E * nq * nn * d) + r(4 * E * nq);
   if (law == LAW_PLASTIC) t += 2 * (3 * r(8 * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
   *bytes = t;
+  return AKB_OK;
+}
+
+int akb_model_autotune(akb_model *m, int repeats) {
+  AKB_TRY(check_model(m, true));
+  if (repeats < 1) return fail(AKB_EINVAL, "repeats must be >= 1");
+  DevGeom g = m->geom();
+  const int64_t nd = nodal_doubles(m);
+  cudaStream_t s = m->stream;
+  // scratch: plastic outputs of the timed element launches, and a, v, u_next
+  // and the status word of the timed node updates (the model is not touched)
+  int64_t state_n = 0;
+  for (auto &gr : m->groups)
+    if (gr.law == LAW_PLASTIC) state_n = std::max(state_n, gr.e_count * m->nq);
+  const int64_t dd = (int64_t)m->dim * m->dim;
+  double *tmp = nullptr;
+  const size_t tmp_doubles = (size_t)(state_n * (3 * dd + 1) + 3 * nd + 1);
+  AKB_CUDA(cudaMallocAsync((void **)&tmp, sizeof(double) * tmp_doubles, s));
+  double *t_sig = tmp, *t_gu = t_sig + state_n * dd, *t_eps = t_gu + state_n * dd;
+  double *t_iso = t_eps + state_n * dd, *t_a = t_iso + state_n, *t_v = t_a + nd;
+  double *t_u = t_v + nd;
+  unsigned int *t_status = (unsigned int *)(t_u + nd);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = AKB_OK;
+  auto check = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && rc == AKB_OK)
+      rc = fail(AKB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return rc == AKB_OK;
+  };
+  check(cudaEventCreate(&e0), "cudaEventCreate");
+  check(cudaEventCreate(&e1), "cudaEventCreate");
+  auto time_it = [&](const std::function<cudaError_t()> &launch, float *ms) {
+    if (!check(launch(), "autotune launch")) return false;  // warm-up
+    check(cudaEventRecord(e0, s), "cudaEventRecord");
+    for (int r = 0; r < repeats && rc == AKB_OK; ++r) check(launch(), "autotune launch");
+    check(cudaEventRecord(e1, s), "cudaEventRecord");
+    check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    if (check(cudaEventElapsedTime(ms, e0, e1), "cudaEventElapsedTime")) *ms /= repeats;
+    return rc == AKB_OK;
+  };
+  auto elem_launch = [&](Group &gr, const ElemTuning &tn) {
+    GroupArgs ps = group_args(m, gr, false);
+    if (gr.law == LAW_PLASTIC) {
+      ps.sig = t_sig;
+      ps.gu = t_gu;
+      ps.eps = t_eps;
+      ps.iso = t_iso;
+      ps.update_energy = 0;
+    }
+    const MatParams mp = m->mats[gr.mat0].params();
+    if (m->precision == AKB_PRECISION_MIXED)
+      return launch_element_forces_mixed(g, gr.law, gr.e_begin, gr.e_count, m->tab, m->fB,
+                                         m->fwJ, m->u(), mp, ps, (float *)m->dre, tn, s);
+    return launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ,
+                                      m->u(), mp, ps, (double *)m->dre, tn, s);
+  };
+  for (auto &gr : m->groups) {
+    if (rc != AKB_OK) break;
+    std::vector<ElemTuning> cand;
+    if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED)
+      cand = {{128, 8}, {64, 8}, {256, 8}, {128, 2}, {128, 1}};
+    else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64))
+      cand = {{64, 8}, {128, 8}, {256, 8}};
+    float best = 0.f;
+    for (size_t k = 0; k < cand.size() && rc == AKB_OK; ++k) {
+      float ms = 0.f;
+      if (!time_it([&] { return elem_launch(gr, cand[k]); }, &ms)) break;
+      if (k == 0 || ms < best) {
+        best = ms;
+        gr.tune = cand[k];
+      }
+    }
+  }
+  if (rc == AKB_OK) {
+    const int flags = NU_CORRECT | NU_PREDICT | (m->fext_zero ? NU_FEXT_ZERO : 0);
+    check(cudaMemcpyAsync(t_a, m->da, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "copy");
+    check(cudaMemcpyAsync(t_v, m->dv, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "copy");
+    const int blocks[4] = {128, 256, 512, 1024};
+    float best = 0.f;
+    for (int k = 0; k < 4 && rc == AKB_OK; ++k) {
+      float ms = 0.f;
+      auto launch = [&]() {
+        if (m->precision == AKB_PRECISION_MIXED)
+          return launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass,
+                                          m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
+                                          flags, t_status, blocks[k], s);
+        return launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass,
+                                       m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
+                                       flags, t_status, blocks[k], s);
+      };
+      if (!time_it(launch, &ms)) break;
+      if (k == 0 || ms < best) {
+        best = ms;
+        m->node_block = blocks[k];
+      }
+    }
+  }
+  // the slot array again holds the forces of the current state, computed
+  // with the chosen shapes
+  for (auto &gr : m->groups)
+    if (rc == AKB_OK) check(elem_launch(gr, gr.tune), "autotune launch");
+  check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  cudaFreeAsync(tmp, s);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  // captured graphs hold the old launch shapes
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  return rc;
+}
+
+int akb_model_get_launch_shape(const akb_model *m, int law, int *element_block,
+                               int *points_per_iteration, int *node_block) {
+  if (!m) return fail(AKB_EINVAL, "null model");
+  if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  for (auto &gr : m->groups)
+    if (gr.law == law) {
+      if (element_block) *element_block = gr.tune.block;
+      if (points_per_iteration) *points_per_iteration = gr.tune.qu;
+      if (node_block) *node_block = m->node_block;
+      return AKB_OK;
+    }
+  return fail(AKB_EINVAL, "no material of this law in the model");
+}
+
+int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
+                               int points_per_iteration, int node_block) {
+  AKB_TRY(check_model(m, true));
+  if (element_block != 64 && element_block != 128 && element_block != 256)
+    return fail(AKB_EINVAL, "element_block must be 64, 128 or 256");
+  const int q = points_per_iteration;
+  const bool sf = m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED;
+  if (!sf && q != 8)
+    return fail(AKB_EINVAL, "points_per_iteration is 8 except for mixed-precision hexahedra");
+  if (sf && q != 0 && q != 1 && q != 2 && q != 8)
+    return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
+  if (sf && (q == 1 || q == 2) && element_block != 128)
+    return fail(AKB_EINVAL, "1 or 2 points per iteration run with 128 threads");
+  if (node_block < 32 || node_block > 1024 || node_block % 32)
+    return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
+  bool found = false;
+  for (auto &gr : m->groups)
+    if (gr.law == law) {
+      gr.tune = ElemTuning{element_block, q};
+      found = true;
+    }
+  if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
+  m->node_block = node_block;
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
   return AKB_OK;
 }
 

@@ -24,6 +24,8 @@ _FIELDS = {
     "internal_force": _capi.INTERNAL_FORCE, "mass": _capi.MASS,
     "blocked_dofs": _capi.BLOCKED_DOFS, "current_position": _capi.CURRENT_POSITION,
 }
+_LAW_IDS = {"elastic": 0, "neohookean": 1, "plastic_linear_isotropic_hardening": 2,
+            "plastic": 2}
 _WRITABLE = ("displacement", "velocity", "acceleration", "external_force", "blocked_dofs")
 
 
@@ -304,6 +306,26 @@ class SolidMechanicsModel:
         v = ctypes.c_double()
         _capi.check(_capi.lib().akb_model_get_energy(self._h, energy_id.encode(), ctypes.byref(v)))
         return v.value
+
+    def autotune(self, repeats=5):
+        """Picks the fastest launch shapes of the step kernels on the current
+        state (akb_model_autotune); results are unchanged by the choice."""
+        self._sync_up()
+        _capi.check(_capi.lib().akb_model_autotune(self._h, int(repeats)))
+
+    def getLaunchShape(self, law):
+        """(element threads per block, points per iteration, node threads per
+        block) of the law group `law` ("elastic", "neohookean", "plastic...")."""
+        b, q, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_launch_shape(self._h, _LAW_IDS[law], ctypes.byref(b),
+                                                           ctypes.byref(q), ctypes.byref(n)))
+        return b.value, q.value, n.value
+
+    def setLaunchShape(self, law, element_block, points_per_iteration, node_block):
+        _capi.check(_capi.lib().akb_model_set_launch_shape(self._h, _LAW_IDS[law],
+                                                           int(element_block),
+                                                           int(points_per_iteration),
+                                                           int(node_block)))
 
     def getDeviceBytes(self):
         """Device memory held by the model."""

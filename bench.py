@@ -25,6 +25,16 @@ together (one element launch and one node launch per step, 100-step CUDA
 graphs).  Beside the batched mixed and FP64 rates it times the instances one
 model at a time (FP64, a sample of 16 instances) as the unbatched baseline.
 
+--config serve: a stream of solve requests with Poisson arrivals (rate
+--rate per second, seeded).  Each request is a tet4 or hex8 box with an
+element count log-uniform in [1e3, 1e6], a material drawn uniformly among
+elastic, neohookean and plastic_linear_isotropic_hardening (rho = 1, E = 1,
+nu = 0.3; sigma_y = 1e-3, h = 0.1), z = 0 blocked, a sinusoidal initial
+velocity and a step count uniform in 500..5000 at 0.8 x its stable dt.  The
+server admits requests by device-memory footprint and advances the resident
+ones together; value = element-steps/s of the whole stream, with p50 / p99
+of the arrival-to-result latency.
+
 --impl reference times the reference's CPU algorithm (the oracle: the
 reference cannot be built here) on all host threads and prints its line.
 N > 1 (torchrun): independent replicas, one mesh per GPU, weak scaling.
@@ -51,8 +61,12 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", default="hex8", choices=["hex8", "tet", "tri6", "batch"])
+    p.add_argument("--config", default="hex8",
+                   choices=["hex8", "tet", "tri6", "batch", "serve"])
     p.add_argument("--instances", type=int, default=256, help="batch: number of meshes")
+    p.add_argument("--requests", type=int, default=200, help="serve: number of requests")
+    p.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
+    p.add_argument("--max-active", type=int, default=64, help="serve: resident solves")
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--precisions", default="mixed,fp64")
@@ -124,6 +138,50 @@ def batch_workload(count, seed=7, n_range=(8, 32)):
         vels.append(v)
         blocks.append(b)
     return meshes, mats, vels, blocks
+
+
+SERVE_MATERIALS = [
+    dict(type="elastic", rho=1.0, E=1.0, nu=0.3),
+    dict(type="neohookean", rho=1.0, E=1.0, nu=0.3),
+    dict(type="plastic_linear_isotropic_hardening", rho=1.0, E=1.0, nu=0.3, sigma_y=1e-3,
+         h=0.1),
+]
+
+
+def serve_requests(count, rate, seed=11):
+    """Seeded request stream: (arrival time, kind, cells, material, steps)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(count):
+        t += rng.exponential(1.0 / rate)
+        kind = ("tet", "hex")[int(rng.integers(0, 2))]
+        target = float(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        per_cell = 6 if kind == "tet" else 1
+        n = max(2, int(round((target / per_cell) ** (1.0 / 3.0))))
+        nz = max(1, int(round(target / (per_cell * n * n))))
+        mat = SERVE_MATERIALS[int(rng.integers(0, 3))]
+        steps = int(rng.integers(500, 5001))
+        out.append((t, kind, (n, n, nz), mat, steps))
+    return out
+
+
+_MESH_CACHE = {}
+
+
+def serve_mesh(kind, cells):
+    import akantu2_b200 as akb
+    key = (kind, cells)
+    if key not in _MESH_CACHE:
+        nx, ny, nz = cells
+        mesh = (akb.box_tet4 if kind == "tet" else akb.box_hex8)(nx, ny, nz)
+        x = mesh.nodes
+        v = np.zeros_like(x)
+        v[:, 2] = 0.01 * np.sin(np.pi * x[:, 0]) * np.sin(np.pi * x[:, 1]) * x[:, 2]
+        b = np.zeros(x.shape, dtype=np.uint8)
+        b[np.isclose(x[:, 2], 0.0)] = 1
+        _MESH_CACHE[key] = (mesh, v, b)
+    return _MESH_CACHE[key]
 
 
 # algorithmic bytes (formula of the specification, per element-step), and the
@@ -258,6 +316,20 @@ def run_reference(args):
             "data": "synthetic",
             "config": {"workload": f"{len(meshes)} tet4 elastic cubes, n in 8..32",
                        "elements": E, "parallelism": f"{threads} host threads"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+    if args.config == "serve":
+        cpu = cpu_serve_rate(serve_requests(args.requests, args.rate), threads, budget_s=60.0)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": 20, "warmup": 1, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "serving request stream (sample)",
+                                            "parallelism": f"{threads} host threads"},
             "cpu_baseline": cpu,
             "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -566,6 +638,31 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def cpu_serve_rate(reqs, threads, budget_s):
+    """Oracle element-steps/s over the first requests of the stream, 20 steps
+    of each (bounded time)."""
+    from oracle import oracle as orc
+    elems, secs, done = 0, 0.0, 0
+    for (_, kind, cells, mat, _) in reqs:
+        mesh, v, b = serve_mesh(kind, cells)
+        o = orc.OracleModel(orc.TET4 if kind == "tet" else orc.HEX8, mesh.nodes,
+                            mesh.connectivity, [mat], threads=threads)
+        o.set(orc.V, v)
+        o.set(orc.BLOCKED, b)
+        o.set_dt(0.8 * o.stable_dt())
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(20)
+        secs += time.perf_counter() - t0
+        elems += mesh.getNbElement() * 20
+        done += 1
+        if secs > budget_s:
+            break
+    return {"value": elems / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"20 steps of each of the first {done} requests "
+                      f"(CPU oracle, {threads} threads, {secs:.1f} s)"}
+
+
 def cpu_batch_rate(meshes, mats, vels, blocks, threads, budget_s):
     """Oracle element-steps/s over the instances in turn (bounded time)."""
     from oracle import oracle as orc
@@ -591,10 +688,77 @@ def cpu_batch_rate(meshes, mats, vels, blocks, threads, budget_s):
                       f"(CPU oracle, {threads} threads, {secs:.1f} s)"}
 
 
+def run_serve(args):
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    import akantu2_b200 as akb
+    from akantu2_b200 import _capi
+    _capi.check(_capi.lib().akb_set_device(local))
+    reqs = serve_requests(args.requests, args.rate)
+    precision = [p for p in args.precisions.split(",") if p][0]
+    # meshes are generated before the clock starts (the client's work)
+    for _, kind, cells, _, _ in reqs:
+        serve_mesh(kind, cells)
+    # warm the library (context, module load) outside the timed stream
+    warm = akb.Server(device=local, max_active=2)
+    m0, v0, b0 = serve_mesh("tet", (2, 2, 2))
+    warm.submit(m0, SERVE_MATERIALS[0], 100, velocity=v0, blocked=b0, precision=precision)
+    warm.drain()
+    warm.close()
+    srv = akb.Server(device=local, max_active=args.max_active, chunk_steps=500)
+    done = []
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for (t_arr, kind, cells, mat, steps) in reqs:
+            while True:
+                now = time.perf_counter() - t0
+                if now >= t_arr:
+                    break
+                done += srv.poll(wait=min(0.002, t_arr - now))
+            mesh, v, b = serve_mesh(kind, cells)
+            srv.submit(mesh, mat, steps, velocity=v, blocked=b, precision=precision)
+        done += srv.drain(timeout=3600)
+        wall = time.perf_counter() - t0
+    srv.close()
+    bad = [c for c in done if c["status"] != 0]
+    lat = np.array([c["t_end"] - c["t_submit"] for c in done])
+    wait = np.array([c["t_start"] - c["t_submit"] for c in done])
+    work = float(sum(c["nb_elements"] * c["nb_steps"] for c in done))
+    span = max(c["t_end"] for c in done) - min(c["t_submit"] for c in done)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * work / span, "unit": UNIT, "n_gpus": world,
+            "steps": len(done), "warmup": 1, "ms_per_step": 1e3 * span / max(1, len(done)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 element math / f64 state" if precision == "mixed" else "f64",
+            "data": "synthetic (seeded request stream)",
+            "config": {"workload": f"{len(reqs)} solve requests, Poisson arrivals at "
+                                   f"{args.rate}/s, tet4/hex8 boxes of 1e3..1e6 elements, "
+                                   "3 laws, 500..5000 steps",
+                       "precision": precision, "max_active": args.max_active,
+                       "chunk_steps": 500, "parallelism": f"replicas x{world}"},
+            "latency_s": {"p50": float(np.percentile(lat, 50)),
+                          "p99": float(np.percentile(lat, 99)),
+                          "mean": float(lat.mean()), "max": float(lat.max())},
+            "queue_wait_s": {"p50": float(np.percentile(wait, 50)),
+                             "p99": float(np.percentile(wait, 99))},
+            "requests_per_s": len(done) / span, "element_steps": work, "wall_s": wall,
+            "failed": len(bad), "clocks": clk.summary(),
+            "e2e": {"value": world * work / span, "unit": UNIT,
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "each request uploads its mesh and initial state and reads its "
+                            "final displacement; value covers arrival to result"},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "serve":
+        run_serve(args)
     elif args.config == "batch":
         run_batch(args)
     else:

@@ -178,6 +178,22 @@ int akb_model_solve_step(akb_model *model, int64_t nsteps);
  * parity, dt, zero external force) and replayed; steps that follow a host
  * edit of u, v, a, the blocked dofs or dt run eagerly first. */
 int akb_model_set_graph_steps(akb_model *model, int64_t steps);
+/* autotuner: times the candidate launch shapes of each law group's
+ * element-force kernel (threads per block 64 / 128 / 256; for mixed-precision
+ * hexahedra also 8, 2 or 1 quadrature points per unrolled iteration) and of
+ * the node update (128 .. 1024 threads per block) on the model's current
+ * state, `repeats` launches each, and keeps the fastest.  The candidates
+ * compute the same numbers, so the choice changes only the timing; the
+ * model's state is not modified.  Captured step graphs are rebuilt. */
+int akb_model_autotune(akb_model *model, int repeats);
+/* the launch shape in use for the law group of `law` (0 elastic, 1
+ * neohookean, 2 plastic); points_per_iteration is 8 except for mixed
+ * hexahedra, where 0 selects the dN/dx form of the kernel instead of the
+ * sum-factorised one (not bit-identical to it: a different FP32 evaluation) */
+int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
+                               int *points_per_iteration, int *node_block);
+int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
+                               int points_per_iteration, int node_block);
 /* captures the graph that the next solve_step will launch (and enqueues the
  * predictor it starts from), so that the capture cost is not paid inside the
  * first solve_step; optional */

@@ -1,0 +1,110 @@
+"""Launch shapes and the autotuner: every candidate shape computes the same
+numbers, the autotuner leaves the model's state alone, and the sum-factorised
+mixed-precision hexahedron kernel agrees with the dN/dx form and with the
+FP64 oracle."""
+import numpy as np
+import pytest
+
+import akantu2_b200 as akb
+from oracle import oracle as orc
+from scenarios import (UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC, blocked_face,
+                       random_field_velocity, sinusoidal_velocity)
+from test_gpu_parity import gpu_model, setup_pair
+
+pytestmark = pytest.mark.gpu
+
+LAW_NAME = {"elastic": "elastic", "neohookean": "neohookean",
+            "plastic_linear_isotropic_hardening": "plastic"}
+
+
+def _run(mesh, mat, precision, v0, bl, steps, shape=None, autotune_at=None):
+    m = gpu_model(mesh, [mat], precision=precision)
+    m.setNodal("velocity", v0)
+    m.setNodal("blocked_dofs", bl)
+    m.setTimeStep(0.8 * m.getStableTimeStep())
+    if shape is not None:
+        m.setLaunchShape(mat["type"], *shape)
+    if autotune_at is None:
+        m.solveStep(steps)
+    else:
+        m.solveStep(autotune_at)
+        m.autotune(2)
+        m.solveStep(steps - autotune_at)
+    return m
+
+
+HEX_SHAPES = [(128, 8, 256), (64, 8, 128), (256, 8, 512), (128, 2, 1024), (128, 1, 256)]
+PE_SHAPES = [(64, 8, 128), (128, 8, 256), (256, 8, 1024)]
+
+
+@pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC])
+def test_hex8_mixed_shapes_are_bit_identical(mat):
+    mesh = akb.box_hex8(5)
+    v0, bl = random_field_velocity(mesh.nodes, seed=4), blocked_face(mesh.nodes)
+    ref = None
+    for shape in HEX_SHAPES:
+        m = _run(mesh, mat, "mixed", v0, bl, 120, shape)
+        got = (m.getDisplacement(), m.getVelocity(), m.getInternalForce())
+        if ref is None:
+            ref = got
+        else:
+            for a, b in zip(ref, got):
+                assert np.array_equal(a, b), shape
+
+
+@pytest.mark.parametrize("etype,precision,mat", [
+    ("_tetrahedron_4", "fp64", UNIT_ELASTIC), ("_tetrahedron_4", "mixed", UNIT_NEOHOOKEAN),
+    ("_triangle_6", "fp64", UNIT_PLASTIC), ("_triangle_6", "mixed", UNIT_PLASTIC)])
+def test_block_sizes_are_bit_identical(etype, precision, mat):
+    mesh = akb.box_tet4(4) if etype == "_tetrahedron_4" else akb.square_tri6(6)
+    v0 = sinusoidal_velocity(mesh.nodes) if mesh.spatial_dimension == 3 else \
+        np.stack([0.02 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
+    bl = blocked_face(mesh.nodes, axis=mesh.spatial_dimension - 1 if etype != "_triangle_6" else 0)
+    ref = None
+    for shape in PE_SHAPES:
+        m = _run(mesh, mat, precision, v0, bl, 90, shape)
+        got = (m.getDisplacement(), m.getVelocity())
+        if ref is None:
+            ref = got
+        else:
+            for a, b in zip(ref, got):
+                assert np.array_equal(a, b), shape
+
+
+@pytest.mark.parametrize("etype,precision,mat", [
+    ("_hexahedron_8", "mixed", UNIT_NEOHOOKEAN), ("_hexahedron_8", "fp64", UNIT_ELASTIC),
+    ("_triangle_6", "mixed", UNIT_PLASTIC), ("_tetrahedron_4", "fp64", UNIT_ELASTIC)])
+def test_autotune_leaves_the_state_alone(etype, precision, mat):
+    mesh = {"_hexahedron_8": lambda: akb.box_hex8(4), "_triangle_6": lambda: akb.square_tri6(6),
+            "_tetrahedron_4": lambda: akb.box_tet4(4)}[etype]()
+    d = mesh.spatial_dimension
+    v0 = sinusoidal_velocity(mesh.nodes) if d == 3 else \
+        np.stack([0.02 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
+    bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
+    plain = _run(mesh, mat, precision, v0, bl, 150)
+    tuned = _run(mesh, mat, precision, v0, bl, 150, autotune_at=70)
+    for name in ("getDisplacement", "getVelocity", "getAcceleration", "getInternalForce"):
+        assert np.array_equal(getattr(plain, name)(), getattr(tuned, name)()), name
+    if mat is UNIT_PLASTIC:
+        for f in ("inelastic_strain", "iso_hardening", "plastic_energy"):
+            assert np.array_equal(plain.getMaterial(0).getInternal(f)(),
+                                  tuned.getMaterial(0).getInternal(f)()), f
+    b, q, n = tuned.getLaunchShape(mat["type"])
+    assert b in (64, 128, 256) and n in (128, 256, 512, 1024)
+
+
+@pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
+def test_hex8_sum_factorisation_accuracy(mat):
+    """the sum-factorised FP32 kernel against the dN/dx FP32 form and the FP64
+    oracle after 500 steps (relative L2 of the displacement)"""
+    mesh = akb.box_hex8(8)
+    v0, bl = random_field_velocity(mesh.nodes, seed=21), blocked_face(mesh.nodes)
+    g, o = setup_pair(mesh, [mat], v0, bl, precision="mixed")
+    g.solveStep(500)
+    o.step(500)
+    direct = _run(mesh, mat, "mixed", v0, bl, 500, shape=(128, 0, 256))
+    u, ud, uo = g.getDisplacement(), direct.getDisplacement(), o.get(orc.U)
+    err_sf = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    err_direct = np.linalg.norm(ud - uo) / np.linalg.norm(uo)
+    assert err_sf < 1e-5 and err_direct < 1e-5, (err_sf, err_direct)
+    assert np.linalg.norm(u - ud) / np.linalg.norm(uo) < 1e-5
