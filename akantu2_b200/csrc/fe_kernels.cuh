@@ -34,19 +34,34 @@ struct QuadTable {
   float fw[kMaxNQ];
 };
 
-// elemental-force slots: the D components of one (element, node) force,
-// stored contiguously at slot p (D values, no padding)
-template <int D> struct SlotStride { static constexpr int value = D; };
+// elemental-force slots: the D components of one (element, node) force at
+// slot p.  FP32 3D slots are padded to one 16-byte float4 (one vector store
+// in the element kernel, one vector load in the node gather); the others
+// hold D values without padding.
+template <int D, class RT> struct SlotStride {
+  static constexpr int value = (D == 3 && sizeof(RT) == 4) ? 4 : D;
+};
 
 template <int D, class RT, class V>
 __device__ __forceinline__ void store_slot(RT *re, int64_t p, const V *v) {
+  if constexpr (SlotStride<D, RT>::value == 4) {
+    reinterpret_cast<float4 *>(re)[p] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+  } else {
 #pragma unroll
-  for (int i = 0; i < D; ++i) re[p * D + i] = (RT)v[i];
+    for (int i = 0; i < D; ++i) re[p * D + i] = (RT)v[i];
+  }
 }
 template <int D, class RT>
 __device__ __forceinline__ void load_slot(const RT *re, int64_t p, double *v) {
+  if constexpr (SlotStride<D, RT>::value == 4) {
+    const float4 f = __ldg(reinterpret_cast<const float4 *>(re) + p);
+    v[0] = (double)f.x;
+    v[1] = (double)f.y;
+    v[2] = (double)f.z;
+  } else {
 #pragma unroll
-  for (int i = 0; i < D; ++i) v[i] = (double)__ldg(re + p * D + i);
+    for (int i = 0; i < D; ++i) v[i] = (double)__ldg(re + p * D + i);
+  }
 }
 
 // per-material plastic internals, [q][comp][ne], ping-pong prev/cur
@@ -776,7 +791,7 @@ __global__ void __launch_bounds__(32 * NQ)
 #pragma unroll
       for (int qq = 1; qq < NQ; ++qq) s = s + red[qq][q][lane];
       const int a = c / D;
-      re[(int64_t)pos[(int64_t)a * E + e] * SlotStride<D>::value + (c - a * D)] = s;
+      re[(int64_t)pos[(int64_t)a * E + e] * SlotStride<D, double>::value + (c - a * D)] = s;
     }
     __syncthreads();
   }

@@ -104,6 +104,36 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
   return cudaGetLastError();
 }
 
+// prescribed motion: before step k (k = 1, 2, ... since the motion was set)
+// the listed dofs get u = u0 + sum_{j <= k} dt v_max min(1, j / ramp_steps),
+// the cumulative displacement of a velocity ramped linearly to v_max over
+// ramp_steps steps.  One block: thread 0 advances the step counter and the
+// running sum, then the block writes the dofs into the displacement the
+// coming step starts from.
+__global__ void k_prescribe(int64_t count, const int64_t *__restrict__ dofs,
+                            const double *__restrict__ u0, double v_max, double ramp_steps,
+                            double dt, double *__restrict__ acc, int64_t *__restrict__ step,
+                            double *__restrict__ u) {
+  __shared__ double a_sh;
+  if (threadIdx.x == 0) {
+    const int64_t k = *step + 1;
+    const double vk = v_max * fmin(1.0, (double)k / ramp_steps);
+    const double a = *acc + dt * vk;
+    *step = k;
+    *acc = a;
+    a_sh = a;
+  }
+  __syncthreads();
+  const double a = a_sh;
+  for (int64_t i = threadIdx.x; i < count; i += blockDim.x) u[dofs[i]] = u0[i] + a;
+}
+cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u0, double v_max,
+                             int64_t ramp_steps, double dt, double *acc, int64_t *step,
+                             double *u, cudaStream_t s) {
+  k_prescribe<<<1, 512, 0, s>>>(count, dofs, u0, v_max, (double)ramp_steps, dt, acc, step, u);
+  return cudaGetLastError();
+}
+
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,

@@ -85,6 +85,13 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                                      double *u_next, double dt, int flags,
                                      unsigned int *status, int node_block, cudaStream_t s);
 
+// prescribed velocity ramp on a set of dofs (u indices node * D + c), written
+// into the displacement the next step starts from; acc and step live on the
+// device so that captured graphs replay it
+cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u0, double v_max,
+                             int64_t ramp_steps, double dt, double *acc, int64_t *step,
+                             double *u, cudaStream_t s);
+
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,

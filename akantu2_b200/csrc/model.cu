@@ -222,6 +222,11 @@ struct akb_model {
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
   int node_block = 256;       // threads per block of the node update
+  // prescribed velocity ramp on a set of dofs (akb_model_set_prescribed_velocity_ramp)
+  int64_t presc_count = 0, presc_ramp = 1;
+  double presc_vmax = 0.;
+  int64_t *dpresc_dofs = nullptr, *dpresc_step = nullptr;
+  double *dpresc_u0 = nullptr, *dpresc_acc = nullptr;
 
   double *u() const { return dU[ucur]; }
   double *u_pred() const { return dU[1 - ucur]; }
@@ -377,6 +382,25 @@ int element_forces(akb_model *m, bool in_step) {
   return AKB_OK;
 }
 
+// the prescribed dofs of the step that starts from u_start
+int prescribe(akb_model *m, double *u_start) {
+  if (m->presc_count == 0) return AKB_OK;
+  AKB_CUDA(launch_prescribe(m->presc_count, m->dpresc_dofs, m->dpresc_u0, m->presc_vmax,
+                            m->presc_ramp, m->dt, m->dpresc_acc, m->dpresc_step, u_start,
+                            m->stream));
+  return AKB_OK;
+}
+
+// predictor of the coming step from the model's state (when the prediction
+// made by the last node update is stale)
+int predict(akb_model *m) {
+  AKB_CUDA(launch_predict(m->geom(), m->dblocked, m->u(), m->dv, m->da, m->dt, m->u_pred(),
+                          m->stream));
+  AKB_TRY(prescribe(m, m->u_pred()));
+  m->predicted = true;
+  return AKB_OK;
+}
+
 // node update after the element forces.  In a step (correct == true): the
 // corrector, then the predictor of the next step from the new displacement
 // u_pred into the other buffer (which held the displacement of the previous
@@ -398,6 +422,7 @@ int node_update(akb_model *m, bool correct) {
                                 m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
                                 m->node_block, m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
+  if (correct) AKB_TRY(prescribe(m, u_next));
   m->fint_valid = !correct;
   return AKB_OK;
 }
@@ -414,11 +439,7 @@ int ensure_fint(akb_model *m) {
 // predictor); afterwards the prediction buffer becomes the model's u
 int one_step(akb_model *m, bool any_plastic, cudaEvent_t e1 = nullptr,
              cudaEvent_t e2 = nullptr) {
-  DevGeom g = m->geom();
-  if (!m->predicted) {
-    AKB_CUDA(launch_predict(g, m->dblocked, m->u(), m->dv, m->da, m->dt, m->u_pred(), m->stream));
-    m->predicted = true;
-  }
+  if (!m->predicted) AKB_TRY(predict(m));
   if (e1) AKB_CUDA(cudaEventRecord(e1, m->stream));
   AKB_TRY(element_forces(m, true));
   if (e2) AKB_CUDA(cudaEventRecord(e2, m->stream));
@@ -808,9 +829,11 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_TRY(m->alloc(p, sizeof(double) * N * d));
   AKB_TRY(m->alloc(&m->dmass, sizeof(double) * N));
   AKB_TRY(m->alloc(&m->dblocked, N));
-  // one padded slot per (element, node): 3D slots hold 4 values, 2D slots 2
+  // one slot per (element, node): FP32 3D slots are padded to 4 values
+  // (SlotStride); the slot array first holds the elemental lumped masses
+  const size_t slot_vals = (precision == AKB_PRECISION_MIXED && d == 3) ? 4 : (size_t)d;
   const size_t re_bytes = (precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double)) *
-                          (size_t)E * nn * (d == 3 ? 4 : 2);
+                          (size_t)E * nn * slot_vals;
   AKB_TRY(m->alloc(&m->dre, std::max(re_bytes, sizeof(double) * (size_t)E * nn)));
   AKB_TRY(m->alloc(&m->dscratch, sizeof(double) * std::max<int64_t>(std::max(E, N), 1)));
   AKB_TRY(m->alloc(&m->dpartials, sizeof(double) * kReducePartials));
@@ -1238,11 +1261,7 @@ int akb_model_prepare_graphs(akb_model *m) {
   if (m->graph_steps == 0) return AKB_OK;
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
-  if (!m->predicted) {
-    AKB_CUDA(launch_predict(m->geom(), m->dblocked, m->u(), m->dv, m->da, m->dt, m->u_pred(),
-                            m->stream));
-    m->predicted = true;
-  }
+  if (!m->predicted) AKB_TRY(predict(m));
   // captured, not launched: the next solve_step launches it
   return capture_graph(m, any_plastic);
 }
@@ -1276,12 +1295,58 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   t += r(8 * N * d) + 3 * r(4 * E * nn) + r(4 * (N + 1));
   t += r(8 * E * nq * nn * d) + r(8 * E * nq);
   t += 6 * r(8 * N * d) + r(8 * N) + r(N);
-  const int64_t re_bytes = (precision == AKB_PRECISION_MIXED ? 4 : 8) * E * nn * (d == 3 ? 4 : 2);
+  const int64_t slot_vals = (precision == AKB_PRECISION_MIXED && d == 3) ? 4 : d;
+  const int64_t re_bytes = (precision == AKB_PRECISION_MIXED ? 4 : 8) * E * nn * slot_vals;
   t += r(std::max(re_bytes, 8 * E * nn));
   t += r(8 * std::max<int64_t>(std::max(E, N), 1)) + 8 * kReducePartials + 4 * 16;
   if (precision == AKB_PRECISION_MIXED && d == 2) t += r(4 * E * nq * nn * d) + r(4 * E * nq);
   if (law == LAW_PLASTIC) t += 2 * (3 * r(8 * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
   *bytes = t;
+  return AKB_OK;
+}
+
+int akb_model_set_prescribed_velocity_ramp(akb_model *m, const int64_t *dofs, int64_t count,
+                                           double v_max, int64_t ramp_steps) {
+  AKB_TRY(check_model(m, true));
+  if (m->ninst > 1) return fail(AKB_EUNSUPPORTED, "prescribed motion is not provided for batches");
+  if (count < 0 || (count > 0 && !dofs)) return fail(AKB_EINVAL, "bad dof list");
+  if (ramp_steps < 1) return fail(AKB_EINVAL, "ramp_steps must be >= 1");
+  const int64_t nd = nodal_doubles(m);
+  for (int64_t k = 0; k < count; ++k)
+    if (dofs[k] < 0 || dofs[k] >= nd) return fail(AKB_EINVAL, "dof index out of range");
+  cudaStream_t s = m->stream;
+  AKB_CUDA(cudaStreamSynchronize(s));
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  m->presc_count = 0;
+  if (count == 0) return AKB_OK;
+  // the dofs are blocked from now on
+  std::vector<uint8_t> mask(m->N);
+  AKB_CUDA(cudaMemcpyAsync(mask.data(), m->dblocked, m->N, cudaMemcpyDeviceToHost, s));
+  AKB_CUDA(cudaStreamSynchronize(s));
+  for (int64_t k = 0; k < count; ++k) mask[dofs[k] / m->dim] |= (uint8_t)(1u << (dofs[k] % m->dim));
+  AKB_CUDA(cudaMemcpyAsync(m->dblocked, mask.data(), m->N, cudaMemcpyHostToDevice, s));
+  // starting displacement of the dofs
+  std::vector<double> u(nd), u0(count);
+  AKB_CUDA(cudaMemcpyAsync(u.data(), m->u(), sizeof(double) * nd, cudaMemcpyDeviceToHost, s));
+  AKB_CUDA(cudaStreamSynchronize(s));
+  for (int64_t k = 0; k < count; ++k) u0[k] = u[dofs[k]];
+  // buffers are kept for the model's lifetime; a longer list reallocates
+  AKB_TRY(m->alloc(&m->dpresc_dofs, sizeof(int64_t) * count));
+  AKB_TRY(m->alloc(&m->dpresc_u0, sizeof(double) * count));
+  if (!m->dpresc_acc) {
+    AKB_TRY(m->alloc(&m->dpresc_acc, sizeof(double)));
+    AKB_TRY(m->alloc(&m->dpresc_step, sizeof(int64_t)));
+  }
+  AKB_CUDA(cudaMemcpyAsync(m->dpresc_dofs, dofs, sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
+  AKB_CUDA(cudaMemcpyAsync(m->dpresc_u0, u0.data(), sizeof(double) * count, cudaMemcpyHostToDevice, s));
+  AKB_CUDA(cudaMemsetAsync(m->dpresc_acc, 0, sizeof(double), s));
+  AKB_CUDA(cudaMemsetAsync(m->dpresc_step, 0, sizeof(int64_t), s));
+  AKB_CUDA(cudaStreamSynchronize(s));
+  m->presc_count = count;
+  m->presc_vmax = v_max;
+  m->presc_ramp = ramp_steps;
+  m->predicted = false;
   return AKB_OK;
 }
 
@@ -1340,11 +1405,15 @@ int akb_model_autotune(akb_model *m, int repeats) {
   };
   for (auto &gr : m->groups) {
     if (rc != AKB_OK) break;
+    // threads per block only: the points per iteration of the mixed
+    // hexahedron kernel change the FP32 rounding and stay as set
     std::vector<ElemTuning> cand;
-    if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED)
-      cand = {{128, 8}, {64, 8}, {256, 8}, {128, 2}, {128, 1}};
-    else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64))
+    if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
+      if (gr.tune.qu == 8 || gr.tune.qu == 0)
+        cand = {{128, gr.tune.qu}, {64, gr.tune.qu}, {256, gr.tune.qu}};
+    } else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64)) {
       cand = {{64, 8}, {128, 8}, {256, 8}};
+    }
     float best = 0.f;
     for (size_t k = 0; k < cand.size() && rc == AKB_OK; ++k) {
       float ms = 0.f;

@@ -307,6 +307,19 @@ class SolidMechanicsModel:
         _capi.check(_capi.lib().akb_model_get_energy(self._h, energy_id.encode(), ctypes.byref(v)))
         return v.value
 
+    def setPrescribedVelocityRamp(self, nodes, axis, v_max, ramp_steps):
+        """Blocks `axis` of `nodes` and, before every later step k, sets their
+        displacement to u_now + sum_{j<=k} dt v_max min(1, j / ramp_steps) on
+        the device (akb_model_set_prescribed_velocity_ramp)."""
+        self._sync_up()
+        nodes = np.asarray(nodes)
+        if nodes.dtype == np.bool_:
+            nodes = np.nonzero(nodes)[0]
+        dofs = np.ascontiguousarray(nodes.astype(np.int64) * self.dim + int(axis))
+        _capi.check(_capi.lib().akb_model_set_prescribed_velocity_ramp(
+            self._h, _capi.ptr(dofs), dofs.size, float(v_max), int(ramp_steps)))
+        self._invalidate(["blocked_dofs"])
+
     def autotune(self, repeats=5):
         """Picks the fastest launch shapes of the step kernels on the current
         state (akb_model_autotune); results are unchanged by the choice."""

@@ -67,6 +67,7 @@ def parse():
     p.add_argument("--requests", type=int, default=200, help="serve: number of requests")
     p.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     p.add_argument("--max-active", type=int, default=64, help="serve: resident solves")
+    p.add_argument("--builders", type=int, default=8, help="serve: host build threads")
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--precisions", default="mixed,fp64")
@@ -706,7 +707,8 @@ def run_serve(args):
     warm.submit(m0, SERVE_MATERIALS[0], 100, velocity=v0, blocked=b0, precision=precision)
     warm.drain()
     warm.close()
-    srv = akb.Server(device=local, max_active=args.max_active, chunk_steps=500)
+    srv = akb.Server(device=local, max_active=args.max_active, chunk_steps=500,
+                     builders=args.builders)
     done = []
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
@@ -723,7 +725,9 @@ def run_serve(args):
     srv.close()
     bad = [c for c in done if c["status"] != 0]
     lat = np.array([c["t_end"] - c["t_submit"] for c in done])
-    wait = np.array([c["t_start"] - c["t_submit"] for c in done])
+    wait = np.array([c["t_admit"] - c["t_submit"] for c in done])
+    build = np.array([c["t_start"] - c["t_admit"] for c in done])
+    run = np.array([c["t_end"] - c["t_start"] for c in done])
     work = float(sum(c["nb_elements"] * c["nb_steps"] for c in done))
     span = max(c["t_end"] for c in done) - min(c["t_submit"] for c in done)
     if rank == 0:
@@ -743,6 +747,9 @@ def run_serve(args):
                           "mean": float(lat.mean()), "max": float(lat.max())},
             "queue_wait_s": {"p50": float(np.percentile(wait, 50)),
                              "p99": float(np.percentile(wait, 99))},
+            "build_s": {"p50": float(np.percentile(build, 50)),
+                        "p99": float(np.percentile(build, 99))},
+            "run_s": {"p50": float(np.percentile(run, 50)), "p99": float(np.percentile(run, 99))},
             "requests_per_s": len(done) / span, "element_steps": work, "wall_s": wall,
             "failed": len(bad), "clocks": clk.summary(),
             "e2e": {"value": world * work / span, "unit": UNIT,

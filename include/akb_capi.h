@@ -170,6 +170,17 @@ int akb_model_qp_field_size(akb_model *model, int field, int material, int64_t *
 int akb_model_get_qp_field(akb_model *model, int field, int material, double *host,
                            int64_t count);
 
+/* prescribed motion on the device, for the imposed-displacement loop of a
+ * driver (a velocity ramp written into the displacement before each step,
+ * e.g. test_solid_mechanics_model_dynamics.cc:243-244) without a host round
+ * trip per step: the dofs (node * dim + component) become blocked and,
+ * before each later step k = 1, 2, ..., get
+ *   u = u_set + sum_{j=1..k} dt * v_max * min(1, j / ramp_steps)
+ * (u_set: their displacement at this call; the sum is accumulated in that
+ * order).  count == 0 removes the motion (the dofs stay blocked).  Not
+ * available for batches. */
+int akb_model_set_prescribed_velocity_ramp(akb_model *model, const int64_t *dofs,
+                                           int64_t count, double v_max, int64_t ramp_steps);
 /* ModelSolver::solveStep  model_solver.cc:267-280: enqueues nsteps explicit
  * steps on the model's stream (asynchronous; getters synchronise) */
 int akb_model_solve_step(akb_model *model, int64_t nsteps);
@@ -179,12 +190,13 @@ int akb_model_solve_step(akb_model *model, int64_t nsteps);
  * edit of u, v, a, the blocked dofs or dt run eagerly first. */
 int akb_model_set_graph_steps(akb_model *model, int64_t steps);
 /* autotuner: times the candidate launch shapes of each law group's
- * element-force kernel (threads per block 64 / 128 / 256; for mixed-precision
- * hexahedra also 8, 2 or 1 quadrature points per unrolled iteration) and of
- * the node update (128 .. 1024 threads per block) on the model's current
- * state, `repeats` launches each, and keeps the fastest.  The candidates
- * compute the same numbers, so the choice changes only the timing; the
- * model's state is not modified.  Captured step graphs are rebuilt. */
+ * element-force kernel (threads per block 64 / 128 / 256) and of the node
+ * update (128 .. 1024 threads per block) on the model's current state,
+ * `repeats` launches each, and keeps the fastest.  The candidates compute
+ * the same numbers, so the choice changes only the timing; the model's state
+ * is not modified.  Captured step graphs are rebuilt.  The points per
+ * iteration of the mixed hexahedron kernel (set_launch_shape) are not tuned:
+ * they change the FP32 rounding. */
 int akb_model_autotune(akb_model *model, int repeats);
 /* the launch shape in use for the law group of `law` (0 elastic, 1
  * neohookean, 2 plastic); points_per_iteration is 8 except for mixed

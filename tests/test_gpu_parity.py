@@ -344,3 +344,36 @@ def test_user_writes_between_steps_keep_reference_semantics():
     u[:] += 0.01
     ref = o.qp(0, orc.GRAD_U)
     assert np.array_equal(g.getMaterial(0).getGradU(), ref)
+
+
+@pytest.mark.parametrize("graph_steps", [0, 10])
+def test_device_prescribed_velocity_ramp_bitwise(graph_steps):
+    """the right edge pulled by a velocity ramp prescribed on the device
+    matches the host writing the same displacement before every step"""
+    mesh = akb.square_tri6(6)
+    x = mesh.nodes
+    left, right = np.isclose(x[:, 0], 0.0), np.isclose(x[:, 0], 1.0)
+    blocked = np.zeros(x.shape, dtype=np.uint8)
+    blocked[left] = 1
+    mat = dict(UNIT_PLASTIC, sigma_y=2e-3)
+    g, o = setup_pair(mesh, [mat], np.zeros_like(x), blocked)
+    g.setGraphSteps(graph_steps)
+    nsteps, ramp, v_max = 130, 60, 0.4
+    dt = g.getTimeStep()
+    g.setPrescribedVelocityRamp(right, 0, v_max, ramp)
+    ob = blocked.copy()
+    ob[right, 0] = 1
+    o.set(orc.BLOCKED, ob)
+    assert np.array_equal(g.getBlockedDOFs(), ob.astype(bool))
+    u0 = o.get(orc.U)[right, 0].copy()
+    acc = 0.0
+    for k in range(1, nsteps + 1):
+        acc = acc + dt * (v_max * min(1.0, k / ramp))
+        u = o.get(orc.U)
+        u[right, 0] = u0 + acc
+        o.set(orc.U, u)
+        o.step()
+    g.solveStep(nsteps)
+    compare(g, o, exact=True)
+    assert np.max(np.abs(o.qp(0, orc.EPS_P))) > 0, "the ramp must reach the yield stress"
+    assert np.array_equal(g.getMaterial(0).getInternal("inelastic_strain")(), o.qp(0, orc.EPS_P))
