@@ -15,8 +15,19 @@ void launch_hex8sf(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
       <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, u, mp, ps, re);
 }
 
-// the tuned shapes of the sum-factorised kernel: 128 threads with 8, 2 or 1
-// points per iteration, 64 or 256 threads with all 8 unrolled
+// the shapes of the sum-factorised kernel: 64, 128 or 256 threads with 8 or
+// 2 points per iteration, 128 threads with 1
+template <int LAW, int QU>
+void dispatch_hex8sf_block(int block, const DevGeom &g, int64_t e0, int64_t ne,
+                           const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
+                           cudaStream_t s) {
+  if (block == 64)
+    launch_hex8sf<LAW, 64, QU>(g, e0, ne, u, mp, ps, re, s);
+  else if (block == 256)
+    launch_hex8sf<LAW, 256, QU>(g, e0, ne, u, mp, ps, re, s);
+  else
+    launch_hex8sf<LAW, 128, QU>(g, e0, ne, u, mp, ps, re, s);
+}
 template <int LAW>
 void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
                      const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
@@ -24,13 +35,9 @@ void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t
   if (tn.qu == 1)
     launch_hex8sf<LAW, 128, 1>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 2)
-    launch_hex8sf<LAW, 128, 2>(g, e0, ne, u, mp, ps, re, s);
-  else if (tn.block == 64)
-    launch_hex8sf<LAW, 64, 8>(g, e0, ne, u, mp, ps, re, s);
-  else if (tn.block == 256)
-    launch_hex8sf<LAW, 256, 8>(g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf_block<LAW, 2>(tn.block, g, e0, ne, u, mp, ps, re, s);
   else
-    launch_hex8sf<LAW, 128, 8>(g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf_block<LAW, 8>(tn.block, g, e0, ne, u, mp, ps, re, s);
 }
 
 }  // namespace

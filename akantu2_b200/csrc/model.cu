@@ -221,7 +221,7 @@ struct akb_model {
   };
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
-  int node_block = 256;       // threads per block of the node update
+  int node_block = 128;       // threads per block of the node update
   // prescribed velocity ramp on a set of dofs (akb_model_set_prescribed_velocity_ramp)
   int64_t presc_count = 0, presc_ramp = 1;
   double presc_vmax = 0.;
@@ -779,8 +779,10 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
         m->groups.push_back(gr);
       }
       Group &gr = m->groups.back();
-      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED && gr.law == LAW_PLASTIC)
-        gr.tune.qu = 1;
+      // mixed hexahedra: 2 points per unrolled iteration for elastic and
+      // neohookean (fewest cycles at 128^3 on B200), all 8 for plastic
+      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED && gr.law != LAW_PLASTIC)
+        gr.tune.qu = 2;
       gr.nmat++;
       gr.e_count += mt.e_count;
       mt.group = (int)m->groups.size() - 1;
@@ -1409,8 +1411,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
     // hexahedron kernel change the FP32 rounding and stay as set
     std::vector<ElemTuning> cand;
     if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
-      if (gr.tune.qu == 8 || gr.tune.qu == 0)
-        cand = {{128, gr.tune.qu}, {64, gr.tune.qu}, {256, gr.tune.qu}};
+      if (gr.tune.qu != 1) cand = {{128, gr.tune.qu}, {64, gr.tune.qu}, {256, gr.tune.qu}};
     } else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64)) {
       cand = {{64, 8}, {128, 8}, {256, 8}};
     }
@@ -1487,8 +1488,8 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
     return fail(AKB_EINVAL, "points_per_iteration is 8 except for mixed-precision hexahedra");
   if (sf && q != 0 && q != 1 && q != 2 && q != 8)
     return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
-  if (sf && (q == 1 || q == 2) && element_block != 128)
-    return fail(AKB_EINVAL, "1 or 2 points per iteration run with 128 threads");
+  if (sf && q == 1 && element_block != 128)
+    return fail(AKB_EINVAL, "1 point per iteration runs with 128 threads");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   bool found = false;

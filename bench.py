@@ -92,7 +92,8 @@ def workload(config, cells):
         mesh = akb.square_tri6(n)
         mat = dict(type="plastic_linear_isotropic_hardening", rho=1.0, E=1.0, nu=0.3,
                    sigma_y=1e-3, h=0.1)
-        desc = f"tri6 plastic {n}^2 x 2 square"
+        desc = (f"tri6 plastic {n}^2 x 2 square, plane strain, right edge pulled by a "
+                "velocity ramp to 1e-3 over 5000 steps (prescribed on the device)")
     return mesh, mat, desc
 
 
@@ -101,9 +102,11 @@ def initial_state(config, mesh):
     x = mesh.nodes
     blocked = np.zeros(x.shape, dtype=np.uint8)
     if config == "tri6":
+        # left edge blocked; the right edge's x motion is prescribed (run_ours)
         blocked[np.isclose(x[:, 0], 0.0)] = 1
+        blocked[np.isclose(x[:, 0], 1.0), 0] = 1
         v0 = np.zeros_like(x)
-        v0[:, 0] = 1e-3 * x[:, 0]
+        v0[:, 0] = 1e-3 * x[:, 0]  # the ramp's end velocity, linear in x
     else:
         blocked[np.isclose(x[:, 2], 0.0)] = 1
         if config == "hex8":
@@ -400,6 +403,8 @@ def run_ours(args):
         m.setNodal("velocity", v0)
         m.setNodal("blocked_dofs", blocked)
         m.setTimeStep(0.8 * m.getStableTimeStep())
+        if args.config == "tri6":
+            m.setPrescribedVelocityRamp(np.isclose(mesh.nodes[:, 0], 1.0), 0, 1e-3, 5000)
         m.timeSteps(max(3, args.warmup))
         barrier()
         with ClockSampler(local) as clk:
@@ -426,7 +431,9 @@ def run_ours(args):
                               "achieved": step_b / (ms / args.steps / 1e3) / 1e9,
                               "frac": step_b / (ms / args.steps / 1e3) / 1e9 / peak},
             "clocks": clk.summary(),
-            "gpu_launches": args.steps * 3,
+            # per step: the element-force kernel, the node update (with the next
+            # predictor) and, for the ramp, the prescribed-motion kernel
+            "gpu_launches": args.steps * (3 if args.config == "tri6" else 2),
             # the state after the timed steps must be finite (device status word)
             "state_finite": m.getStatus() == 0 and bool(np.all(np.isfinite(m.getDisplacement()))),
         }

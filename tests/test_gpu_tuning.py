@@ -38,14 +38,15 @@ PE_SHAPES = [(64, 8, 128), (128, 8, 256), (256, 8, 1024)]
 
 
 @pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC])
-@pytest.mark.parametrize("qu", [8, 1])
+@pytest.mark.parametrize("qu", [8, 2, 1])
 def test_hex8_mixed_shapes_are_bit_identical(mat, qu):
     """threads per block change nothing (points per iteration are a separate,
     untuned choice)"""
     mesh = akb.box_hex8(5)
     v0, bl = random_field_velocity(mesh.nodes, seed=4), blocked_face(mesh.nodes)
     ref = None
-    shapes = HEX_SHAPES if qu == 8 else [(128, 1, 256), (128, 1, 1024)]
+    shapes = [(b, qu, n) for b, _, n in HEX_SHAPES] if qu != 1 else [(128, 1, 256),
+                                                                       (128, 1, 1024)]
     for shape in shapes:
         m = _run(mesh, mat, "mixed", v0, bl, 120, shape)
         got = (m.getDisplacement(), m.getVelocity(), m.getInternalForce())
