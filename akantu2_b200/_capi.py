@@ -95,8 +95,9 @@ def lib():
         "akb_model_autotune": (c_int, [vp, c_int]),
         "akb_model_set_prescribed_velocity_ramp": (c_int, [vp, vp, i64, c_dbl, i64]),
         "akb_model_get_launch_shape": (c_int, [vp, c_int, ctypes.POINTER(c_int),
-                                               ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
-        "akb_model_set_launch_shape": (c_int, [vp, c_int, c_int, c_int, c_int]),
+                                               ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                               ctypes.POINTER(c_int)]),
+        "akb_model_set_launch_shape": (c_int, [vp, c_int, c_int, c_int, c_int, c_int]),
         "akb_model_stream": (c_int, [vp, pp]),
         "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
         "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,

@@ -225,6 +225,38 @@ __device__ __forceinline__ void first_piola(const T *g, const T *S, T w, T *P) {
     }
 }
 
+// Weighted first Piola-Kirchhoff stress of the neohookean law from the
+// cofactors of F, for the mixed-precision path:
+//   P = F S = mu F + (lambda ln J - mu) F^-T,  F^-T = cof(F) / det F
+// (F C^-1 = F^-T), the same tensor as first_piola(g, neohookean_pk2(g)) in
+// exact arithmetic without forming C, its inverse or the product F S.
+template <int D, class T>
+__device__ __forceinline__ void neohookean_piola_cof(T lambda, T mu, const T *g, T w, T *P) {
+  T F[D * D], cof[D * D];
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+#pragma unroll
+    for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? T(1) : T(0)) + g[i + D * j];
+  if constexpr (D == 3) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) cof[i + 3 * j] = cof3(F, i, j);
+  } else {
+    cof[0] = F[3];
+    cof[1] = -F[2];
+    cof[2] = -F[1];
+    cof[3] = F[0];
+  }
+  T det = F[0] * cof[0];
+#pragma unroll
+  for (int i = 1; i < D; ++i) det += F[i] * cof[i];
+  const T c = (lambda * log(det) - mu) / det;
+  const T mw = mu * w, cw = c * w;
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) P[k] = mw * F[k] + cw * cof[k];
+}
+
 template <int D, class T> __device__ __forceinline__ void to_voigt(const T *S, T *Sv) {
   if constexpr (D == 3) {
     Sv[0] = S[0]; Sv[1] = S[4]; Sv[2] = S[8];

@@ -381,12 +381,10 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
       g[i + D * j] = s;
     }
   if constexpr (LAW == LAW_NEOHOOKEAN) {
-    T S[D * D];
-    neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
     if constexpr (REL) {
-      // mixed path: r = (F S w) . dN/dx
+      // mixed path: r = (F S w) . dN/dx with F S from the cofactors of F
       T P[D * D];
-      first_piola<D, T>(g, S, w, P);
+      neohookean_piola_cof<D, T>((T)mp.lambda, (T)mp.mu, g, w, P);
 #pragma unroll
       for (int a = 0; a < NN; ++a)
 #pragma unroll
@@ -397,6 +395,8 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
           t[a * D + k] = s;
         }
     } else {
+      T S[D * D];
+      neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
       T Sv[D == 3 ? 6 : 3];
       to_voigt<D, T>(S, Sv);
 #pragma unroll
@@ -621,9 +621,7 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
                                            const GroupArgs &ps, int64_t ne, int64_t le, int q,
                                            float *P) {
   if constexpr (LAW == LAW_NEOHOOKEAN) {
-    float S[D * D];
-    neohookean_pk2<D, float>((float)mp.lambda, (float)mp.mu, g, S);
-    first_piola<D, float>(g, S, w, P);
+    neohookean_piola_cof<D, float>((float)mp.lambda, (float)mp.mu, g, w, P);
   } else if constexpr (LAW == LAW_ELASTIC) {
     float sig[D * D];
     elastic_stress<D, float>((float)mp.lambda, (float)mp.mu, g, (float)mp.sigma_th, sig);
@@ -639,9 +637,10 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
   }
 }
 
-// QU: quadrature points per unrolled iteration (1, 2, 4 or 8)
-template <int LAW, int BLOCK, int QU>
-__global__ void __launch_bounds__(BLOCK)
+// QU: quadrature points per unrolled iteration (1, 2, 4 or 8); MINB: blocks
+// per SM the register allocation must allow (1: the compiler's choice)
+template <int LAW, int BLOCK, int QU, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                             const double *__restrict__ X, const double *__restrict__ u,

@@ -7,11 +7,11 @@ namespace akb {
 
 namespace {
 
-template <int LAW, int BLOCK, int QU>
+template <int LAW, int BLOCK, int QU, int MINB = 1>
 void launch_hex8sf(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
                    const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
   const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-  k_element_forces_hex8sf<LAW, BLOCK, QU>
+  k_element_forces_hex8sf<LAW, BLOCK, QU, MINB>
       <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, u, mp, ps, re);
 }
 
@@ -32,7 +32,14 @@ template <int LAW>
 void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
                      const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                      cudaStream_t s) {
-  if (tn.qu == 1)
+  // 128 threads with the registers capped for 5 resident blocks (20 warps)
+  if (tn.minb == 5 && tn.qu == 1)
+    launch_hex8sf<LAW, 128, 1, 5>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.minb == 5 && tn.qu == 2)
+    launch_hex8sf<LAW, 128, 2, 5>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.minb == 5)
+    launch_hex8sf<LAW, 128, 8, 5>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.qu == 1)
     launch_hex8sf<LAW, 128, 1>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 2)
     dispatch_hex8sf_block<LAW, 2>(tn.block, g, e0, ne, u, mp, ps, re, s);

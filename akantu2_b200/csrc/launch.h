@@ -16,10 +16,14 @@ struct GroupArgs;
 // launch shape of the element-force kernel of one law group: threads per
 // block (64, 128 or 256) and, for the mixed _hexahedron_8 kernel, the
 // quadrature points per unrolled iteration (1, 2 or 8; 0 selects the dN/dx
-// form).  All shapes give the same arithmetic per element.
+// form) and the resident blocks per SM its registers are capped for (1: the
+// compiler's choice; 5 with 128 threads).  Threads per block and the
+// register cap leave the arithmetic unchanged; the points per iteration do
+// not (FP32 contraction differs).
 struct ElemTuning {
   int block = 128;
   int qu = 8;
+  int minb = 1;
 };
 
 // device view of the mesh, internal element order

@@ -1411,7 +1411,10 @@ int akb_model_autotune(akb_model *m, int repeats) {
     // hexahedron kernel change the FP32 rounding and stay as set
     std::vector<ElemTuning> cand;
     if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
-      if (gr.tune.qu != 1) cand = {{128, gr.tune.qu}, {64, gr.tune.qu}, {256, gr.tune.qu}};
+      const int q = gr.tune.qu;
+      cand = {{128, q, 1}, {128, q, 5}};
+      if (q != 1) cand.insert(cand.end(), {{64, q, 1}, {256, q, 1}});
+      if (q == 0) cand = {{128, 0, 1}, {64, 0, 1}, {256, 0, 1}};
     } else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64)) {
       cand = {{64, 8}, {128, 8}, {256, 8}};
     }
@@ -1464,13 +1467,14 @@ int akb_model_autotune(akb_model *m, int repeats) {
 }
 
 int akb_model_get_launch_shape(const akb_model *m, int law, int *element_block,
-                               int *points_per_iteration, int *node_block) {
+                               int *points_per_iteration, int *min_blocks, int *node_block) {
   if (!m) return fail(AKB_EINVAL, "null model");
   if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
   for (auto &gr : m->groups)
     if (gr.law == law) {
       if (element_block) *element_block = gr.tune.block;
       if (points_per_iteration) *points_per_iteration = gr.tune.qu;
+      if (min_blocks) *min_blocks = gr.tune.minb;
       if (node_block) *node_block = m->node_block;
       return AKB_OK;
     }
@@ -1478,7 +1482,7 @@ int akb_model_get_launch_shape(const akb_model *m, int law, int *element_block,
 }
 
 int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
-                               int points_per_iteration, int node_block) {
+                               int points_per_iteration, int min_blocks, int node_block) {
   AKB_TRY(check_model(m, true));
   if (element_block != 64 && element_block != 128 && element_block != 256)
     return fail(AKB_EINVAL, "element_block must be 64, 128 or 256");
@@ -1490,12 +1494,14 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
     return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
   if (sf && q == 1 && element_block != 128)
     return fail(AKB_EINVAL, "1 point per iteration runs with 128 threads");
+  if (min_blocks != 1 && !(sf && q != 0 && min_blocks == 5 && element_block == 128))
+    return fail(AKB_EINVAL, "min_blocks is 1, or 5 for the 128-thread mixed hexahedron kernel");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   bool found = false;
   for (auto &gr : m->groups)
     if (gr.law == law) {
-      gr.tune = ElemTuning{element_block, q};
+      gr.tune = ElemTuning{element_block, q, min_blocks};
       found = true;
     }
   if (!found) return fail(AKB_EINVAL, "no material of this law in the model");

@@ -327,18 +327,20 @@ class SolidMechanicsModel:
         _capi.check(_capi.lib().akb_model_autotune(self._h, int(repeats)))
 
     def getLaunchShape(self, law):
-        """(element threads per block, points per iteration, node threads per
-        block) of the law group `law` ("elastic", "neohookean", "plastic...")."""
-        b, q, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _capi.check(_capi.lib().akb_model_get_launch_shape(self._h, _LAW_IDS[law], ctypes.byref(b),
-                                                           ctypes.byref(q), ctypes.byref(n)))
-        return b.value, q.value, n.value
+        """(element threads per block, points per iteration, min blocks per SM,
+        node threads per block) of the law group `law` ("elastic",
+        "neohookean", "plastic...")."""
+        b, q, mb, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_launch_shape(
+            self._h, _LAW_IDS[law], ctypes.byref(b), ctypes.byref(q), ctypes.byref(mb),
+            ctypes.byref(n)))
+        return b.value, q.value, mb.value, n.value
 
-    def setLaunchShape(self, law, element_block, points_per_iteration, node_block):
+    def setLaunchShape(self, law, element_block, points_per_iteration, node_block, min_blocks=1):
         _capi.check(_capi.lib().akb_model_set_launch_shape(self._h, _LAW_IDS[law],
                                                            int(element_block),
                                                            int(points_per_iteration),
-                                                           int(node_block)))
+                                                           int(min_blocks), int(node_block)))
 
     def getDeviceBytes(self):
         """Device memory held by the model."""

@@ -283,6 +283,54 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+class Replicas:
+    """One process per GPU (torchrun): rank and world size from the
+    environment, a process group when world > 1, the barrier and the maximum
+    over ranks of a device-timed value.  The replicas share no data: the only
+    collectives are this barrier and this maximum."""
+
+    def __init__(self, backend="nccl"):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            if self.backend == "nccl":
+                import torch
+                torch.cuda.synchronize()
+
+    def max(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def aggregate_rate(units_per_rank, world, ms_max):
+    """whole-job units/s: every rank processed units_per_rank in at most ms_max"""
+    return world * units_per_rank / (ms_max / 1e3)
+
+
 # ---- CPU legs --------------------------------------------------------------------------
 def cpu_rate(config, mesh, mat, v0, blocked, budget_s, max_steps, threads):
     """Element-steps/s of the oracle on `threads` host threads."""
@@ -363,15 +411,9 @@ def run_reference(args):
 
 # ---- GPU leg ----------------------------------------------------------------------------
 def run_ours(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    rep = Replicas("nccl")
+    world, rank, local = rep.world, rep.rank, rep.local
+    barrier, max_over_ranks = rep.barrier, rep.max
     import akantu2_b200 as akb
     from akantu2_b200 import _capi
     _capi.check(_capi.lib().akb_set_device(local))
@@ -381,20 +423,6 @@ def run_ours(args):
     E = mesh.getNbElement()
     results = {}
     precisions = [p for p in args.precisions.split(",") if p]
-
-    def barrier():
-        if dist is not None:
-            import torch
-            dist.barrier()
-            torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     for prec in precisions:
         m = akb.SolidMechanicsModel(mesh)
@@ -418,7 +446,7 @@ def run_ours(args):
         peak, peak_kind = read_peaks()
         results[prec] = {
             "ms_per_step": ms / args.steps,
-            "value": world * E * args.steps / (ms / 1e3),
+            "value": aggregate_rate(E * args.steps, world, ms),
             "phase_ms_per_step": {"predictor": phases[0] / nprof,
                                   "element_forces": phases[1] / nprof,
                                   "node_update": phases[2] / nprof},
@@ -492,8 +520,7 @@ def run_ours(args):
         if "fp64" in results and precisions[0] != "fp64":
             line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def build_batch(akb, meshes, mats, vels, blocks, precision):
@@ -509,32 +536,12 @@ def build_batch(akb, meshes, mats, vels, blocks, precision):
 
 
 def run_batch(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    rep = Replicas("nccl")
+    world, rank, local = rep.world, rep.rank, rep.local
+    barrier, max_over_ranks = rep.barrier, rep.max
     import akantu2_b200 as akb
     from akantu2_b200 import _capi
     _capi.check(_capi.lib().akb_set_device(local))
-
-    def barrier():
-        if dist is not None:
-            import torch
-            dist.barrier()
-            torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     meshes, mats, vels, blocks = batch_workload(args.instances)
     E = sum(m.getNbElement() for m in meshes)
@@ -558,7 +565,7 @@ def run_batch(args):
         elem_ms = phases[1] / nprof
         results[prec] = {
             "ms_per_step": ms / args.steps,
-            "value": world * E * args.steps / (ms / 1e3),
+            "value": aggregate_rate(E * args.steps, world, ms),
             "phase_ms_per_step": {"predictor": phases[0] / nprof,
                                   "element_forces": phases[1] / nprof,
                                   "node_update": phases[2] / nprof},
@@ -642,8 +649,7 @@ def run_batch(args):
             line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
         line["speedup_vs_unbatched_fp64"] = head["value"] / unbatched
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def cpu_serve_rate(reqs, threads, budget_s):

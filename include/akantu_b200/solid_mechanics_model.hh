@@ -327,6 +327,25 @@ public:
     mirrors_.erase(AKB_INTERNAL_FORCE);
   }
 
+  // the imposed-displacement loop of a driver done on the device: `axis` of
+  // the group's nodes is blocked and, before every later step k, moved to
+  // u_now + sum_{j<=k} dt v_max min(1, j / ramp_steps)
+  void setPrescribedVelocityRamp(const ID &group, Int axis, Real v_max, Int ramp_steps) {
+    syncUp();
+    std::vector<int64_t> dofs;
+    for (Idx n : mesh_.getNodeGroup(group)) dofs.push_back((int64_t)n * dim_ + axis);
+    check(akb_model_set_prescribed_velocity_ramp(h_, dofs.data(), (int64_t)dofs.size(), v_max,
+                                                 ramp_steps));
+    blocked_.reset();
+    blocked_dirty_ = false;
+  }
+
+  // fastest launch shapes on the current state (results unchanged)
+  void autotune(int repeats = 5) {
+    syncUp();
+    check(akb_model_autotune(h_, repeats));
+  }
+
   Real getEnergy(const ID &energy_id) {
     syncUp();
     Real e = 0;
@@ -429,6 +448,42 @@ inline Array<Real> Material::getInternal(const ID &name, ElementType) {
       {"iso_hardening", AKB_ISO_HARDENING}, {"plastic_energy", AKB_PLASTIC_ENERGY}};
   return qp(ids.at(name));
 }
+
+/* ---- Server: many solves resident on one GPU ----------------------------- */
+// RAII wrapper of akb_server_*: submit() copies the request's inputs, the
+// result arrays passed in the request are filled before poll() reports it.
+class Server {
+public:
+  explicit Server(const akb_server_config &cfg = akb_server_config{}) {
+    check(akb_server_create(&cfg, &h_));
+  }
+  ~Server() {
+    if (h_) akb_server_destroy(h_);
+  }
+  Server(const Server &) = delete;
+  Server &operator=(const Server &) = delete;
+
+  int64_t submit(const akb_request &request) {
+    int64_t id = 0;
+    check(akb_server_submit(h_, &request, &id));
+    return id;
+  }
+  std::vector<akb_completion> poll(double wait_seconds = 0., int capacity = 64) {
+    std::vector<akb_completion> out((size_t)capacity);
+    int n = 0;
+    check(akb_server_poll(h_, out.data(), capacity, &n, wait_seconds));
+    out.resize((size_t)n);
+    return out;
+  }
+  akb_server_stats stats() {
+    akb_server_stats st{};
+    check(akb_server_get_stats(h_, &st));
+    return st;
+  }
+
+private:
+  akb_server *h_ = nullptr;
+};
 
 }  // namespace akantu_b200
 

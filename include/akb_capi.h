@@ -190,7 +190,8 @@ int akb_model_solve_step(akb_model *model, int64_t nsteps);
  * edit of u, v, a, the blocked dofs or dt run eagerly first. */
 int akb_model_set_graph_steps(akb_model *model, int64_t steps);
 /* autotuner: times the candidate launch shapes of each law group's
- * element-force kernel (threads per block 64 / 128 / 256) and of the node
+ * element-force kernel (threads per block 64 / 128 / 256; for mixed
+ * hexahedra also a register cap for 5 resident blocks of 128) and of the node
  * update (128 .. 1024 threads per block) on the model's current state,
  * `repeats` launches each, and keeps the fastest.  The candidates compute
  * the same numbers, so the choice changes only the timing; the model's state
@@ -201,11 +202,13 @@ int akb_model_autotune(akb_model *model, int repeats);
 /* the launch shape in use for the law group of `law` (0 elastic, 1
  * neohookean, 2 plastic); points_per_iteration is 8 except for mixed
  * hexahedra, where 0 selects the dN/dx form of the kernel instead of the
- * sum-factorised one (not bit-identical to it: a different FP32 evaluation) */
+ * sum-factorised one (not bit-identical to it: a different FP32 evaluation);
+ * min_blocks is 1 except for the 128-thread mixed hexahedron kernel, which
+ * may cap its registers for 5 resident blocks per SM */
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
-                               int *points_per_iteration, int *node_block);
+                               int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
-                               int points_per_iteration, int node_block);
+                               int points_per_iteration, int min_blocks, int node_block);
 /* captures the graph that the next solve_step will launch (and enqueues the
  * predictor it starts from), so that the capture cost is not paid inside the
  * first solve_step; optional */

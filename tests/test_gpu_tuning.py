@@ -45,8 +45,9 @@ def test_hex8_mixed_shapes_are_bit_identical(mat, qu):
     mesh = akb.box_hex8(5)
     v0, bl = random_field_velocity(mesh.nodes, seed=4), blocked_face(mesh.nodes)
     ref = None
-    shapes = [(b, qu, n) for b, _, n in HEX_SHAPES] if qu != 1 else [(128, 1, 256),
-                                                                       (128, 1, 1024)]
+    shapes = [(b, qu, n, 1) for b, _, n in HEX_SHAPES] if qu != 1 else [(128, 1, 256, 1),
+                                                                          (128, 1, 1024, 1)]
+    shapes.append((128, qu, 256, 5))  # registers capped for 5 blocks per SM
     for shape in shapes:
         m = _run(mesh, mat, "mixed", v0, bl, 120, shape)
         got = (m.getDisplacement(), m.getVelocity(), m.getInternalForce())
@@ -94,8 +95,8 @@ def test_autotune_leaves_the_state_alone(etype, precision, mat):
         for f in ("inelastic_strain", "iso_hardening", "plastic_energy"):
             assert np.array_equal(plain.getMaterial(0).getInternal(f)(),
                                   tuned.getMaterial(0).getInternal(f)()), f
-    b, q, n = tuned.getLaunchShape(mat["type"])
-    assert b in (64, 128, 256) and n in (128, 256, 512, 1024)
+    b, q, mb, n = tuned.getLaunchShape(mat["type"])
+    assert b in (64, 128, 256) and mb in (1, 5) and n in (128, 256, 512, 1024)
 
 
 @pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
