@@ -69,16 +69,37 @@ __device__ __forceinline__ void load_slot(const RT *re, int64_t p, double *v) {
 // law, contiguous in internal order.  With several materials, each element
 // reads its parameters from mtab[mslot[le]]; with one, from the launch's
 // MatParams.  Plastic internals of the group are [q][comp][ne] arrays,
-// ping-pong prev / cur.
+// ping-pong prev / cur.  The stress and the plastic strain are symmetric
+// term by term (every expression that forms them is), so they keep their
+// SymComps<D> independent components; the previous displacement gradient
+// is stored in the element-math type (FP32 on the mixed path, where it is
+// an FP32 value to begin with).
 struct GroupArgs {
   const MatParams *mtab;     // per-material parameters, or null
   const int32_t *mslot;      // [ne] index into mtab
-  const double *sig_prev, *gu_prev, *eps_prev, *iso_prev;
+  const double *sig_prev, *eps_prev, *iso_prev;
+  const void *gu_prev;       // double (FP64 path) or float (mixed path)
   const double *iso_cur_in;  // "current" hardening read by the yield test
-  double *sig, *gu, *eps, *iso;
+  double *sig, *eps, *iso;
+  void *gu;
   double *pe;                // cumulative plastic energy density
   int update_energy;         // 1 inside solveStep (afterSolveStep), 0 otherwise
 };
+
+// symmetric d x d tensors: components (0,0), (1,1), (2,2), (1,2), (0,2), (0,1)
+// in 3D, (0,0), (1,1), (0,1) in 2D
+template <int D> struct SymComps { static constexpr int value = D == 3 ? 6 : 3; };
+// component of column-major entry k = i + D j
+template <int D> __host__ __device__ constexpr int sym_of(int k) {
+  return D == 3 ? (k == 0 ? 0 : k == 4 ? 1 : k == 8 ? 2 : (k == 5 || k == 7) ? 3
+                  : (k == 2 || k == 6) ? 4 : 5)
+                : (k == 0 ? 0 : k == 3 ? 1 : 2);
+}
+// column-major entry stored for component c
+template <int D> __host__ __device__ constexpr int full_of(int c) {
+  return D == 3 ? (c == 0 ? 0 : c == 1 ? 4 : c == 2 ? 8 : c == 3 ? 7 : c == 4 ? 6 : 3)
+                : (c == 0 ? 0 : c == 1 ? 3 : 2);
+}
 
 __device__ __forceinline__ MatParams group_params(const MatParams &mp, const GroupArgs &ga,
                                                   int64_t le) {
@@ -327,18 +348,27 @@ __global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
 
 // plastic internals of one quadrature point: loads previous state, runs the
 // radial return, stores the new state (and the plastic energy in a step)
-template <int D>
+// GT: storage type of the displacement gradient (the element-math type)
+template <int D, class GT>
 __device__ __forceinline__ void plastic_point(const MatParams &mp, const GroupArgs &ps,
                                               int64_t ne, int64_t le, int q,
                                               const double *gd, double *s) {
-  constexpr int DD = D * D;
+  constexpr int DD = D * D, NS = SymComps<D>::value;
+  const GT *gu_prev = static_cast<const GT *>(ps.gu_prev);
   double gp[DD], sp[DD], epp[DD], ep[DD], iso;
+  double sps[NS], epps[NS];
+#pragma unroll
+  for (int k = 0; k < DD; ++k) gp[k] = (double)gu_prev[(int64_t)(q * DD + k) * ne + le];
+#pragma unroll
+  for (int c = 0; c < NS; ++c) {
+    const int64_t idx = (int64_t)(q * NS + c) * ne + le;
+    sps[c] = ps.sig_prev[idx];
+    epps[c] = ps.eps_prev[idx];
+  }
 #pragma unroll
   for (int k = 0; k < DD; ++k) {
-    const int64_t idx = (int64_t)(q * DD + k) * ne + le;
-    gp[k] = ps.gu_prev[idx];
-    sp[k] = ps.sig_prev[idx];
-    epp[k] = ps.eps_prev[idx];
+    sp[k] = sps[sym_of<D>(k)];
+    epp[k] = epps[sym_of<D>(k)];
   }
   const int64_t qi = (int64_t)q * ne + le;
   plastic_update<D>(mp.lambda, mp.mu, mp.sigma_y, mp.h, gd, gp, sp, epp, ps.iso_cur_in[qi],
@@ -355,12 +385,14 @@ __device__ __forceinline__ void plastic_point(const MatParams &mp, const GroupAr
     wp = wp / 2.;
     ps.pe[qi] = ps.pe[qi] + wp;
   }
+  GT *gu = static_cast<GT *>(ps.gu);
 #pragma unroll
-  for (int k = 0; k < DD; ++k) {
-    const int64_t idx = (int64_t)(q * DD + k) * ne + le;
-    ps.gu[idx] = gd[k];
-    ps.sig[idx] = s[k];
-    ps.eps[idx] = ep[k];
+  for (int k = 0; k < DD; ++k) gu[(int64_t)(q * DD + k) * ne + le] = (GT)gd[k];
+#pragma unroll
+  for (int c = 0; c < NS; ++c) {
+    const int64_t idx = (int64_t)(q * NS + c) * ne + le;
+    ps.sig[idx] = s[full_of<D>(c)];
+    ps.eps[idx] = ep[full_of<D>(c)];
   }
   ps.iso[qi] = iso;
 }
@@ -413,7 +445,7 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
       double gd[D * D], s[D * D];
 #pragma unroll
       for (int k = 0; k < D * D; ++k) gd[k] = (double)g[k];
-      plastic_point<D>(mp, ps, ne, le, q, gd, s);
+      plastic_point<D, T>(mp, ps, ne, le, q, gd, s);
 #pragma unroll
       for (int k = 0; k < D * D; ++k) sig[k] = (T)s[k];
     }
@@ -631,7 +663,7 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
     double gd[D * D], sd[D * D];
 #pragma unroll
     for (int k = 0; k < D * D; ++k) gd[k] = (double)g[k];
-    plastic_point<D>(mp, ps, ne, le, q, gd, sd);
+    plastic_point<D, float>(mp, ps, ne, le, q, gd, sd);
 #pragma unroll
     for (int k = 0; k < D * D; ++k) P[k] = (float)sd[k] * w;
   }

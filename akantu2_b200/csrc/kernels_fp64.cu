@@ -209,20 +209,23 @@ cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double
 
 // per-element integral of an energy density (Material::getPotentialEnergy,
 // material.cc:604-619; MaterialPlastic::getPlasticEnergy, material_plastic.cc:47-69).
-// Quadrature-point inputs are [q][comp][ne]; wJ is [q][E].
-template <int D, int NQ, int LAW>
+// Quadrature-point inputs are [q][comp][ld]; wJ is [q][E].  Plastic inputs
+// are the group's internals: the gradient in GT, stress and plastic strain
+// as symmetric components.
+template <int D, int NQ, int LAW, class GT>
 __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t ld, int64_t E,
-                              const double *__restrict__ wJ, const double *__restrict__ grad,
+                              const double *__restrict__ wJ, const GT *__restrict__ grad,
                               const double *__restrict__ stress,
                               const double *__restrict__ eps_p, const double *__restrict__ pe,
                               MatParams mp, double *__restrict__ out) {
   const int64_t le = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (le >= ne) return;
-  constexpr int DD = D * D;
+  constexpr int DD = D * D, NS = SymComps<D>::value;
   double el = 0.;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     auto at = [&](int k) { return (int64_t)(q * DD + k) * ld + le; };
+    auto sym = [&](int k) { return (int64_t)(q * NS + sym_of<D>(k)) * ld + le; };
     double dens;
     if (which == 1) {
       dens = pe[(int64_t)q * ld + le];
@@ -231,7 +234,7 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t ld, int
 #pragma unroll
       for (int j = 0; j < D; ++j)
 #pragma unroll
-        for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? 1. : 0.) + grad[at(i + D * j)];
+        for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? 1. : 0.) + (double)grad[at(i + D * j)];
       double trC = 0.;
 #pragma unroll
       for (int i = 0; i < D; ++i) {
@@ -247,9 +250,9 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t ld, int
       double dot = 0.;
 #pragma unroll
       for (int k = 0; k < DD; ++k) {
-        double ge = grad[at(k)];
-        if (LAW == LAW_PLASTIC) ge = ge - eps_p[at(k)];
-        const double sk = stress[at(k)];
+        double ge = (double)grad[at(k)];
+        if (LAW == LAW_PLASTIC) ge = ge - eps_p[sym(k)];
+        const double sk = LAW == LAW_PLASTIC ? stress[sym(k)] : stress[at(k)];
         dot = (k == 0) ? sk * ge : dot + sk * ge;
       }
       dens = .5 * dot;
@@ -260,22 +263,28 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t ld, int
   out[le] = el;
 }
 cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0, int64_t ne,
-                               int64_t ld, const double *wJ, const double *grad, const double *stress,
-                               const double *eps_p, const double *pe, const MatParams &mp,
-                               double *out, cudaStream_t s) {
+                               int64_t ld, const double *wJ, const void *grad,
+                               bool grad_float, const double *stress, const double *eps_p,
+                               const double *pe, const MatParams &mp, double *out,
+                               cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
+  const double *gd = static_cast<const double *>(grad);
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
     (void)NN;
     if (law == LAW_NEOHOOKEAN)
-      k_energy_elem<D, NQ, LAW_NEOHOOKEAN><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, ld, g.E, wJ, grad, stress, eps_p, pe, mp, out);
+      k_energy_elem<D, NQ, LAW_NEOHOOKEAN, double><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, ld, g.E, wJ, gd, stress, eps_p, pe, mp, out);
+    else if (law == LAW_PLASTIC && grad_float)
+      k_energy_elem<D, NQ, LAW_PLASTIC, float><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, ld, g.E, wJ, static_cast<const float *>(grad), stress, eps_p, pe, mp,
+          out);
     else if (law == LAW_PLASTIC)
-      k_energy_elem<D, NQ, LAW_PLASTIC><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, ld, g.E, wJ, grad, stress, eps_p, pe, mp, out);
+      k_energy_elem<D, NQ, LAW_PLASTIC, double><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, ld, g.E, wJ, gd, stress, eps_p, pe, mp, out);
     else
-      k_energy_elem<D, NQ, LAW_ELASTIC><<<grid_for(ne), kThreads, 0, s>>>(
-          which, e0, ne, ld, g.E, wJ, grad, stress, eps_p, pe, mp, out);
+      k_energy_elem<D, NQ, LAW_ELASTIC, double><<<grid_for(ne), kThreads, 0, s>>>(
+          which, e0, ne, ld, g.E, wJ, gd, stress, eps_p, pe, mp, out);
   });
   return cudaGetLastError();
 }

@@ -109,11 +109,12 @@ cudaError_t launch_work_terms(const DevGeom &g, const double *fext, const double
                               cudaStream_t s);
 // per-element sum_q density_q wJ_q of one material -> out[ne]; the
 // quadrature-point inputs are [q][comp][ld] with the material's elements at
-// 0 .. ne.  which: 0 potential, 1 plastic
+// 0 .. ne (plastic: grad in float when grad_float, stress and eps_p as
+// symmetric components).  which: 0 potential, 1 plastic
 cudaError_t launch_energy_elem(const DevGeom &g, int law, int which, int64_t e0, int64_t ne,
-                               int64_t ld, const double *wJ, const double *grad, const double *stress,
-                               const double *eps_p, const double *pe, const MatParams &mp,
-                               double *out, cudaStream_t s);
+                               int64_t ld, const double *wJ, const void *grad, bool grad_float,
+                               const double *stress, const double *eps_p, const double *pe,
+                               const MatParams &mp, double *out, cudaStream_t s);
 // deterministic reductions (fixed grid, fixed tree): result written to *out
 // (device); partials needs kReducePartials doubles
 constexpr int kReducePartials = 1024;

@@ -73,10 +73,25 @@ struct Group {
   int mat0 = 0;  // first material of the group
   int nmat = 0;
   int64_t e_begin = 0, e_count = 0;
-  double *sig[2] = {nullptr, nullptr}, *gu[2] = {nullptr, nullptr};
-  double *eps[2] = {nullptr, nullptr}, *iso[2] = {nullptr, nullptr};
+  // stress and plastic strain as symmetric components, the gradient in the
+  // element-math type (float on the mixed path)
+  double *sig[2] = {nullptr, nullptr}, *eps[2] = {nullptr, nullptr};
+  void *gu[2] = {nullptr, nullptr};
+  double *iso[2] = {nullptr, nullptr};
   double *pe = nullptr;
 };
+
+// independent components of a symmetric d x d tensor, and the map from
+// column-major entry k to component (the device-side SymComps / sym_of)
+int sym_comps(int d) { return d == 3 ? 6 : 3; }
+int sym_component(int d, int k) {
+  if (d == 3) {
+    static const int m[9] = {0, 5, 4, 5, 1, 3, 4, 3, 2};
+    return m[k];
+  }
+  static const int m2[4] = {0, 2, 2, 1};
+  return m2[k];
+}
 
 int nodes_per_element(int et) {
   return et == AKB_TETRAHEDRON_4 ? 4 : (et == AKB_HEXAHEDRON_8 ? 8 : 6);
@@ -779,10 +794,9 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
         m->groups.push_back(gr);
       }
       Group &gr = m->groups.back();
-      // mixed hexahedra: 2 points per unrolled iteration for elastic and
-      // neohookean (fewest cycles at 128^3 on B200), all 8 for plastic
-      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED && gr.law != LAW_PLASTIC)
-        gr.tune.qu = 2;
+      // mixed hexahedra: 2 points per unrolled iteration (the fastest form
+      // for all three laws at 128^3 on B200)
+      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED) gr.tune.qu = 2;
       gr.nmat++;
       gr.e_count += mt.e_count;
       mt.group = (int)m->groups.size() - 1;
@@ -876,16 +890,18 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_CUDA(launch_to_float(m->dB, m->fB, E * nq * nn * d, s));
     AKB_CUDA(launch_to_float(m->dwJ, m->fwJ, E * nq, s));
   }
+  const size_t gu_size = precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
   for (auto &mt : m->groups) {
     if (mt.law != LAW_PLASTIC) continue;
-    const int64_t nqp = mt.e_count * nq, dd = (int64_t)d * d;
+    const int64_t nqp = mt.e_count * nq, dd = (int64_t)d * d, ns = sym_comps(d);
     for (int b = 0; b < 2; ++b) {
-      AKB_TRY(m->alloc(&mt.sig[b], sizeof(double) * nqp * dd));
-      AKB_TRY(m->alloc(&mt.gu[b], sizeof(double) * nqp * dd));
-      AKB_TRY(m->alloc(&mt.eps[b], sizeof(double) * nqp * dd));
+      AKB_TRY(m->alloc(&mt.sig[b], sizeof(double) * nqp * ns));
+      AKB_TRY(m->alloc(&mt.gu[b], gu_size * nqp * dd));
+      AKB_TRY(m->alloc(&mt.eps[b], sizeof(double) * nqp * ns));
       AKB_TRY(m->alloc(&mt.iso[b], sizeof(double) * nqp));
-      for (double *p : {mt.sig[b], mt.gu[b], mt.eps[b]})
-        AKB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * std::max<int64_t>(nqp * dd, 1), s));
+      for (double *p : {mt.sig[b], mt.eps[b]})
+        AKB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * std::max<int64_t>(nqp * ns, 1), s));
+      AKB_CUDA(cudaMemsetAsync(mt.gu[b], 0, gu_size * std::max<int64_t>(nqp * dd, 1), s));
       AKB_CUDA(cudaMemsetAsync(mt.iso[b], 0, sizeof(double) * std::max<int64_t>(nqp, 1), s));
     }
     AKB_TRY(m->alloc(&mt.pe, sizeof(double) * nqp));
@@ -1195,15 +1211,43 @@ int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t
   if (mt.law == LAW_PLASTIC) {
     const Group &gr = m->groups[mt.group];
     const int c = m->cur;
+    const int64_t off = mt.e_begin - gr.e_begin, ns = sym_comps(m->dim);
+    const double *sym = nullptr;
     switch (field) {
-    case AKB_GRAD_U: src = gr.gu[c]; break;
-    case AKB_STRESS: src = gr.sig[c]; break;
-    case AKB_INELASTIC_STRAIN: src = gr.eps[c]; break;
+    case AKB_GRAD_U: break;
+    case AKB_STRESS: sym = gr.sig[c]; break;
+    case AKB_INELASTIC_STRAIN: sym = gr.eps[c]; break;
     case AKB_ISO_HARDENING: src = gr.iso[c]; comps = 1; break;
     case AKB_PLASTIC_ENERGY: src = gr.pe; comps = 1; break;
     default: return fail(AKB_EINVAL, "field not defined for plastic_linear_isotropic_hardening");
     }
-    src += mt.e_begin - gr.e_begin;
+    const int64_t ne = mt.e_count;
+    if (field == AKB_GRAD_U || sym) {
+      // gradient rows in the storage type, or symmetric rows, then expanded
+      const bool f32 = field == AKB_GRAD_U && m->precision == AKB_PRECISION_MIXED;
+      const size_t es = f32 ? sizeof(float) : sizeof(double);
+      const int64_t rows = (int64_t)m->nq * (field == AKB_GRAD_U ? dd : ns);
+      std::vector<char> raw((size_t)(rows * ne) * es);
+      const char *base = field == AKB_GRAD_U ? static_cast<const char *>(gr.gu[c])
+                                             : reinterpret_cast<const char *>(sym);
+      if (ne > 0)
+        AKB_CUDA(cudaMemcpy2DAsync(raw.data(), es * ne, base + es * off, es * gr.e_count, es * ne,
+                                   (size_t)rows, cudaMemcpyDeviceToHost, m->stream));
+      AKB_CUDA(cudaStreamSynchronize(m->stream));
+      auto at = [&](int64_t row, int64_t le) {
+        return f32 ? (double)reinterpret_cast<const float *>(raw.data())[row * ne + le]
+                   : reinterpret_cast<const double *>(raw.data())[row * ne + le];
+      };
+      for (int64_t le = 0; le < ne; ++le)
+        for (int q = 0; q < m->nq; ++q)
+          for (int kk = 0; kk < dd; ++kk) {
+            const int64_t row = field == AKB_GRAD_U ? (int64_t)q * dd + kk
+                                                    : (int64_t)q * ns + sym_component(m->dim, kk);
+            host[(le * m->nq + q) * dd + kk] = at(row, le);
+          }
+      return AKB_OK;
+    }
+    src += off;
     ld = gr.e_count;
   } else {
     if (field != AKB_GRAD_U && field != AKB_STRESS && field != AKB_PIOLA_KIRCHHOFF_2)
@@ -1302,7 +1346,9 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   t += r(std::max(re_bytes, 8 * E * nn));
   t += r(8 * std::max<int64_t>(std::max(E, N), 1)) + 8 * kReducePartials + 4 * 16;
   if (precision == AKB_PRECISION_MIXED && d == 2) t += r(4 * E * nq * nn * d) + r(4 * E * nq);
-  if (law == LAW_PLASTIC) t += 2 * (3 * r(8 * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
+  const int64_t gs = precision == AKB_PRECISION_MIXED ? 4 : 8, ns = sym_comps((int)d);
+  if (law == LAW_PLASTIC)
+    t += 2 * (2 * r(8 * E * nq * ns) + r(gs * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
   *bytes = t;
   return AKB_OK;
 }
@@ -1363,12 +1409,12 @@ int akb_model_autotune(akb_model *m, int repeats) {
   int64_t state_n = 0;
   for (auto &gr : m->groups)
     if (gr.law == LAW_PLASTIC) state_n = std::max(state_n, gr.e_count * m->nq);
-  const int64_t dd = (int64_t)m->dim * m->dim;
+  const int64_t dd = (int64_t)m->dim * m->dim, ns = sym_comps(m->dim);
   double *tmp = nullptr;
-  const size_t tmp_doubles = (size_t)(state_n * (3 * dd + 1) + 3 * nd + 1);
+  const size_t tmp_doubles = (size_t)(state_n * (2 * ns + dd + 1) + 3 * nd + 1);
   AKB_CUDA(cudaMallocAsync((void **)&tmp, sizeof(double) * tmp_doubles, s));
-  double *t_sig = tmp, *t_gu = t_sig + state_n * dd, *t_eps = t_gu + state_n * dd;
-  double *t_iso = t_eps + state_n * dd, *t_a = t_iso + state_n, *t_v = t_a + nd;
+  double *t_sig = tmp, *t_gu = t_sig + state_n * ns, *t_eps = t_gu + state_n * dd;
+  double *t_iso = t_eps + state_n * ns, *t_a = t_iso + state_n, *t_v = t_a + nd;
   double *t_u = t_v + nd;
   unsigned int *t_status = (unsigned int *)(t_u + nd);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1616,12 +1662,16 @@ int akb_model_get_energy(akb_model *m, const char *id, double *value) {
   double total = 0.;
   for (auto &mt : m->mats) {
     if (kind == 1 && mt.law != LAW_PLASTIC) continue;
-    const double *grad = nullptr, *stress = nullptr, *eps = nullptr, *pe = nullptr;
+    const void *grad = nullptr;
+    const double *stress = nullptr, *eps = nullptr, *pe = nullptr;
     int64_t ld = mt.e_count;
+    bool grad_float = false;
     if (mt.law == LAW_PLASTIC) {
       const Group &gr = m->groups[mt.group];
       const int64_t off = mt.e_begin - gr.e_begin;
-      grad = gr.gu[m->cur] + off;
+      grad_float = m->precision == AKB_PRECISION_MIXED;
+      grad = grad_float ? (const void *)(static_cast<const float *>(gr.gu[m->cur]) + off)
+                        : (const void *)(static_cast<const double *>(gr.gu[m->cur]) + off);
       stress = gr.sig[m->cur] + off;
       eps = gr.eps[m->cur] + off;
       pe = gr.pe + off;
@@ -1632,7 +1682,8 @@ int akb_model_get_energy(akb_model *m, const char *id, double *value) {
       stress = m->dqp_b;
     }
     AKB_CUDA(launch_energy_elem(g, mt.law, kind, mt.e_begin, mt.e_count, ld, m->dwJ, grad,
-                                stress, eps, pe, mt.params(), m->dscratch, m->stream));
+                                grad_float, stress, eps, pe, mt.params(), m->dscratch,
+                                m->stream));
     double s = 0.;
     AKB_TRY(reduce_to_host(m, m->dscratch, mt.e_count, false, &s));
     total += s;
