@@ -2,6 +2,7 @@
 // template instances; shared by the FP64 and the mixed translation units.
 #pragma once
 
+#include <algorithm>
 #include <type_traits>
 
 #include "fe_kernels.cuh"
@@ -50,6 +51,28 @@ inline unsigned grid_for(int64_t n, int threads = kThreads) {
       __VA_ARGS__;                                                        \
     }                                                                     \
   } while (0)
+
+// cooperative launch of a persistent step kernel: as many blocks as fit on
+// the device at once (all resident, so the grid barrier can complete), fewer
+// when the mesh needs fewer
+template <class K>
+inline cudaError_t launch_cooperative(K kernel, int64_t work, const StepArgs &sa,
+                                      const QuadTable &tab, cudaStream_t s) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPersistentThreads, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int64_t want = (work + kPersistentThreads - 1) / kPersistentThreads;
+  const unsigned grid =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * sms));
+  StepArgs a = sa;
+  QuadTable t = tab;
+  void *args[] = {&a, &t};
+  return cudaLaunchCooperativeKernel((const void *)kernel, grid, kPersistentThreads, args, 0, s);
+}
 
 template <class T, class RT>
 inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, int64_t ne,

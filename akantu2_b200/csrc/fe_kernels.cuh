@@ -51,16 +51,19 @@ __device__ __forceinline__ void store_slot(RT *re, int64_t p, const V *v) {
     for (int i = 0; i < D; ++i) re[p * D + i] = (RT)v[i];
   }
 }
+// plain loads: the compiler uses the read-only path where the kernel's
+// parameters allow it, and coherent loads in the persistent kernel, which
+// writes the slots in the same launch
 template <int D, class RT>
 __device__ __forceinline__ void load_slot(const RT *re, int64_t p, double *v) {
   if constexpr (SlotStride<D, RT>::value == 4) {
-    const float4 f = __ldg(reinterpret_cast<const float4 *>(re) + p);
+    const float4 f = reinterpret_cast<const float4 *>(re)[p];
     v[0] = (double)f.x;
     v[1] = (double)f.y;
     v[2] = (double)f.z;
   } else {
 #pragma unroll
-    for (int i = 0; i < D; ++i) v[i] = (double)__ldg(re + p * D + i);
+    for (int i = 0; i < D; ++i) v[i] = (double)re[p * D + i];
   }
 }
 
@@ -476,19 +479,16 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
   }
 }
 
-// BLOCK: threads (= elements) per block, one of the launch shapes the
-// autotuner chooses from
-template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
-    k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
-                        const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                        const T *__restrict__ B, const T *__restrict__ wJ,
-                        const double *__restrict__ u, MatParams mp, GroupArgs ps,
-                        RT *__restrict__ re) {
+// element le of a launch over [e_begin, e_begin + e_count): streamed dN/dx
+template <int D, int NN, int NQ, int LAW, class T, class RT>
+__device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t e_count,
+                                           int64_t E, const int32_t *conn,
+                                           const int32_t *pos,
+                                           const T *B, const T *wJ,
+                                           const double *u, const MatParams &mp,
+                                           const GroupArgs &ps, RT *re) {
   constexpr int ND = NN * D;
   constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
-  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
   T ue[ND];
@@ -525,22 +525,34 @@ __global__ void __launch_bounds__(BLOCK)
   for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
 }
 
+// BLOCK: threads (= elements) per block, one of the launch shapes the
+// autotuner chooses from
+template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+    k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
+                        const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                        const T *__restrict__ B, const T *__restrict__ wJ,
+                        const double *__restrict__ u, MatParams mp, GroupArgs ps,
+                        RT *__restrict__ re) {
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count) return;
+  element_pe<D, NN, NQ, LAW, T, RT>(le, e_begin, e_count, E, conn, pos, B, wJ, u, mp, ps, re);
+}
+
 // Mixed path: FP32 element math with the shape derivatives recomputed from
 // the gathered nodal coordinates instead of streamed from HBM.  Per point:
 // J = dN/ds X^T, dN/dx = J^-1 dN/ds, w = det J * w_q (the arithmetic of
 // k_precompute, in FP32, with coordinates and displacements taken relative
 // to the element's first node -- dN/ds sums to zero over the nodes, so the
 // Jacobian and the gradient are unchanged in exact arithmetic).
-template <int D, int NN, int NQ, int LAW, int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
-    k_element_forces_geo(int64_t e_begin, int64_t e_count, int64_t E,
-                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                         const double *__restrict__ X, QuadTable tab,
-                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
-                         float *__restrict__ re) {
+template <int D, int NN, int NQ, int LAW>
+__device__ __forceinline__ void element_geo(int64_t le, int64_t e_begin, int64_t e_count,
+                                            int64_t E, const int32_t *conn,
+                                            const int32_t *pos,
+                                            const double *X, const QuadTable &tab,
+                                            const double *u, const MatParams &mp,
+                                            const GroupArgs &ps, float *re) {
   constexpr int ND = NN * D;
-  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
   float xe[ND], ue[ND];
@@ -599,6 +611,18 @@ __global__ void __launch_bounds__(BLOCK)
   }
 #pragma unroll
   for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
+}
+
+template <int D, int NN, int NQ, int LAW, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+    k_element_forces_geo(int64_t e_begin, int64_t e_count, int64_t E,
+                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                         const double *__restrict__ X, QuadTable tab,
+                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
+                         float *__restrict__ re) {
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count) return;
+  element_geo<D, NN, NQ, LAW>(le, e_begin, e_count, E, conn, pos, X, tab, u, mp, ps, re);
 }
 
 // Mixed path, _hexahedron_8: sum factorisation of the trilinear element.
@@ -669,16 +693,14 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
   }
 }
 
-// QU: quadrature points per unrolled iteration (1, 2, 4 or 8); MINB: blocks
-// per SM the register allocation must allow (1: the compiler's choice)
-template <int LAW, int BLOCK, int QU, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB)
-    k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
-                            const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                            const double *__restrict__ X, const double *__restrict__ u,
-                            MatParams mp, GroupArgs ps, float *__restrict__ re) {
-  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
+// QU: quadrature points per unrolled iteration (1, 2, 4 or 8)
+template <int LAW, int QU>
+__device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int64_t e_count,
+                                               int64_t E, const int32_t *conn,
+                                               const int32_t *pos,
+                                               const double *X,
+                                               const double *u, const MatParams &mp,
+                                               const GroupArgs &ps, float *re) {
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
   // reference node a sits at lexicographic corner lex[a] = [sx>0] + 2[sy>0] + 4[sz>0]
@@ -768,6 +790,19 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   for (int a = 0; a < 8; ++a) store_slot<3>(re, pos[(int64_t)a * E + e], A[lex[a]]);
 }
 
+// MINB: blocks per SM the register allocation must allow (1: the compiler's
+// choice)
+template <int LAW, int BLOCK, int QU, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
+                            const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                            const double *__restrict__ X, const double *__restrict__ u,
+                            MatParams mp, GroupArgs ps, float *__restrict__ re) {
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count) return;
+  element_hex8sf<LAW, QU>(le, e_begin, e_count, E, conn, pos, X, u, mp, ps, re);
+}
+
 // FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q
 template <int D, int NN, int NQ, int LAW>
 __global__ void __launch_bounds__(32 * NQ)
@@ -850,17 +885,17 @@ __global__ void __launch_bounds__(32 * NQ)
 enum { NU_CORRECT = 1, NU_PREDICT = 2, NU_FINT = 4, NU_FEXT_ZERO = 8 };
 
 template <int D, class RT, bool KAHAN>
-__global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
-                              const RT *__restrict__ re, const double *__restrict__ fext,
-                              const double *__restrict__ mass,
-                              const uint8_t *__restrict__ blocked, double *__restrict__ fint,
-                              double *__restrict__ a, double *__restrict__ v,
-                              const double *__restrict__ u, double *__restrict__ u_next,
-                              double dt, const int32_t *__restrict__ node_inst,
-                              const double *__restrict__ inst_dt, int flags,
-                              unsigned int *__restrict__ status) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+__device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
+                                          const RT *re,
+                                          const double *fext,
+                                          const double *mass,
+                                          const uint8_t *blocked,
+                                          double *fint, double *a,
+                                          double *v, const double *u,
+                                          double *u_next, double dt,
+                                          const int32_t *node_inst,
+                                          const double *inst_dt, int flags,
+                                          unsigned int *status) {
   double acc[D], comp[D];
 #pragma unroll
   for (int c = 0; c < D; ++c) {
@@ -926,6 +961,133 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
     }
   }
   if (bad) atomicOr(status, 1u);
+}
+
+template <int D, class RT, bool KAHAN>
+__global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
+                              const RT *__restrict__ re, const double *__restrict__ fext,
+                              const double *__restrict__ mass,
+                              const uint8_t *__restrict__ blocked, double *__restrict__ fint,
+                              double *__restrict__ a, double *__restrict__ v,
+                              const double *__restrict__ u, double *__restrict__ u_next,
+                              double dt, const int32_t *__restrict__ node_inst,
+                              const double *__restrict__ inst_dt, int flags,
+                              unsigned int *__restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  node_body<D, RT, KAHAN>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst,
+                          inst_dt, flags, status);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent multi-step kernel for small meshes of one law group.  All
+// blocks are resident (cooperative launch); each step runs the element phase
+// and the node phase over grid-stride loops, separated by grid barriers, with
+// the same per-element and per-node functions as the two-kernel path, so the
+// results are bit-identical to it.  The pointers below carry no __restrict__:
+// the displacement, the slots and the state are written and read again in the
+// same launch, so their loads must not take the read-only path.
+struct StepArgs {
+  int64_t E, N;
+  const int32_t *conn, *pos, *ptr;
+  const void *B, *wJ;  // streamed dN/dx and det J w, element-math type
+  const double *X;
+  MatParams mp;
+  GroupArgs ps;        // state buffers of the first step
+  void *re;
+  const double *fext, *mass;
+  const uint8_t *blocked;
+  double *fint, *a, *v;
+  double *u_pred;      // displacement the first step starts from
+  double *u_other;     // receives the prediction of the step after it
+  double dt;
+  const int32_t *node_inst;
+  const double *inst_dt;
+  int flags;           // node-update flags of a step (NU_CORRECT | NU_PREDICT ...)
+  int plastic;         // swap the plastic state buffers after each step
+  int64_t nsteps;
+  unsigned int *status;
+  unsigned int *bar;   // [2]: arrivals, generation
+};
+
+constexpr int kPersistentThreads = 256;
+constexpr unsigned int kBarrierSpinLimit = 1u << 24;  // x 64 ns sleeps: about a second
+constexpr unsigned int ST_BARRIER_TIMEOUT = 2u;
+
+// grid-wide barrier with a bounded wait: false (status bit 1 set) when the
+// other blocks did not all arrive within the limit
+__device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int *status) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *gen = bar + 1;
+    const unsigned int g = *gen;
+    __threadfence();
+    ok = 1;
+    if (atomicAdd(bar, 1u) + 1 == gridDim.x) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned int spins = 0;
+      while (*gen == g) {
+        if (++spins > kBarrierSpinLimit) {
+          atomicOr(status, ST_BARRIER_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*(volatile unsigned int *)status & ST_BARRIER_TIMEOUT) ok = 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__device__ __forceinline__ void swap_state(GroupArgs &ps) {
+  const double *t;
+  t = ps.sig_prev; ps.sig_prev = ps.sig; ps.sig = const_cast<double *>(t);
+  t = ps.eps_prev; ps.eps_prev = ps.eps; ps.eps = const_cast<double *>(t);
+  t = ps.iso_prev; ps.iso_prev = ps.iso; ps.iso = const_cast<double *>(t);
+  const void *tg = ps.gu_prev; ps.gu_prev = ps.gu; ps.gu = const_cast<void *>(tg);
+  ps.iso_cur_in = ps.iso_prev;
+}
+
+// FORM: 0 streamed dN/dx (element_pe, T), 1 recomputed in FP32
+// (element_geo), 2 sum-factorised hexahedron with QU points per iteration
+template <int D, int NN, int NQ, int LAW, int FORM, class T, class RT, bool KAHAN, int QU>
+__global__ void __launch_bounds__(kPersistentThreads)
+    k_persistent_steps(StepArgs sa, QuadTable tab) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  GroupArgs ps = sa.ps;
+  double *up = sa.u_pred, *uo = sa.u_other;
+  RT *re = static_cast<RT *>(sa.re);
+  for (int64_t s = 0; s < sa.nsteps; ++s) {
+    for (int64_t le = t0; le < sa.E; le += stride) {
+      const MatParams &mp = sa.mp;
+      if constexpr (FORM == 0)
+        element_pe<D, NN, NQ, LAW, T, RT>(le, 0, sa.E, sa.E, sa.conn, sa.pos,
+                                          static_cast<const T *>(sa.B),
+                                          static_cast<const T *>(sa.wJ), up, mp, ps, re);
+      else if constexpr (FORM == 1)
+        element_geo<D, NN, NQ, LAW>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, tab, up, mp, ps,
+                                    reinterpret_cast<float *>(re));
+      else
+        element_hex8sf<LAW, QU>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, up, mp, ps,
+                                reinterpret_cast<float *>(re));
+    }
+    if (!grid_barrier(sa.bar, sa.status)) return;
+    for (int64_t i = t0; i < sa.N; i += stride)
+      node_body<D, RT, KAHAN>(i, sa.ptr, re, sa.fext, sa.mass, sa.blocked, sa.fint, sa.a, sa.v,
+                              up, uo, sa.dt, sa.node_inst, sa.inst_dt, sa.flags, sa.status);
+    if (!grid_barrier(sa.bar, sa.status)) return;
+    double *tu = up;
+    up = uo;
+    uo = tu;
+    if (sa.plastic) swap_state(ps);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -87,6 +87,27 @@ cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, in
   return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, tn, s);
 }
 
+cudaError_t launch_persistent_fp64(const DevGeom &g, int law, int qu, const StepArgs &sa,
+                                   const QuadTable &tab, cudaStream_t s) {
+  (void)qu;
+  const int64_t work = std::max(g.E, g.N);
+  AKB_DISPATCH_ELEM(g, {
+    (void)ET;
+    if (law == LAW_ELASTIC)
+      return launch_cooperative(
+          k_persistent_steps<D, NN, NQ, LAW_ELASTIC, 0, double, double, false, 1>, work, sa,
+          tab, s);
+    if (law == LAW_NEOHOOKEAN)
+      return launch_cooperative(
+          k_persistent_steps<D, NN, NQ, LAW_NEOHOOKEAN, 0, double, double, false, 1>, work, sa,
+          tab, s);
+    return launch_cooperative(
+        k_persistent_steps<D, NN, NQ, LAW_PLASTIC, 0, double, double, false, 1>, work, sa, tab,
+        s);
+  });
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,

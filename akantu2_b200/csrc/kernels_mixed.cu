@@ -84,6 +84,35 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
   return cudaGetLastError();
 }
 
+namespace {
+template <int LAW>
+cudaError_t persistent_mixed_law(const DevGeom &g, int qu, const StepArgs &sa,
+                                 const QuadTable &tab, cudaStream_t s) {
+  const int64_t work = std::max(g.E, g.N);
+  if (g.et == ET_TET4)
+    return launch_cooperative(k_persistent_steps<3, 4, 1, LAW, 1, float, float, true, 1>, work,
+                              sa, tab, s);
+  if (g.et == ET_HEX8 && qu == 1)
+    return launch_cooperative(k_persistent_steps<3, 8, 8, LAW, 2, float, float, true, 1>, work,
+                              sa, tab, s);
+  if (g.et == ET_HEX8)
+    return launch_cooperative(k_persistent_steps<3, 8, 8, LAW, 2, float, float, true, 2>, work,
+                              sa, tab, s);
+  if (g.NQ == 3)
+    return launch_cooperative(k_persistent_steps<2, 6, 3, LAW, 0, float, float, true, 1>, work,
+                              sa, tab, s);
+  return launch_cooperative(k_persistent_steps<2, 6, 6, LAW, 0, float, float, true, 1>, work, sa,
+                            tab, s);
+}
+}  // namespace
+
+cudaError_t launch_persistent_mixed(const DevGeom &g, int law, int qu, const StepArgs &sa,
+                                    const QuadTable &tab, cudaStream_t s) {
+  if (law == LAW_ELASTIC) return persistent_mixed_law<LAW_ELASTIC>(g, qu, sa, tab, s);
+  if (law == LAW_NEOHOOKEAN) return persistent_mixed_law<LAW_NEOHOOKEAN>(g, qu, sa, tab, s);
+  return persistent_mixed_law<LAW_PLASTIC>(g, qu, sa, tab, s);
+}
+
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,

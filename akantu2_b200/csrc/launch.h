@@ -96,6 +96,14 @@ cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u
                              int64_t ramp_steps, double dt, double *acc, int64_t *step,
                              double *u, cudaStream_t s);
 
+// persistent multi-step kernel (one law group; sa describes the steps);
+// qu: points per iteration of mixed hexahedra (1 or 2)
+struct StepArgs;
+cudaError_t launch_persistent_fp64(const DevGeom &g, int law, int qu, const StepArgs &sa,
+                                   const QuadTable &tab, cudaStream_t s);
+cudaError_t launch_persistent_mixed(const DevGeom &g, int law, int qu, const StepArgs &sa,
+                                    const QuadTable &tab, cudaStream_t s);
+
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,

@@ -237,6 +237,10 @@ struct akb_model {
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
   int node_block = 128;       // threads per block of the node update
+  // persistent multi-step kernel: 0 never, 1 for small single-group meshes,
+  // 2 whenever the model allows it (akb_model_set_persistent)
+  int persistent = 1;
+  unsigned int *dbar = nullptr;  // grid-barrier counters
   // prescribed velocity ramp on a set of dofs (akb_model_set_prescribed_velocity_ramp)
   int64_t presc_count = 0, presc_ramp = 1;
   double presc_vmax = 0.;
@@ -520,6 +524,86 @@ int run_graph(akb_model *m, bool any_plastic) {
   return AKB_OK;
 }
 
+// small meshes of one law group run whole step sequences in one persistent
+// launch (launch latency dominates the two-kernel step below about this size)
+constexpr int64_t kPersistentMaxElements = 1 << 18;
+
+bool use_persistent(const akb_model *m) {
+  if (m->persistent == 0 || m->groups.size() != 1 || m->presc_count > 0 || m->E == 0) return false;
+  const Group &gr = m->groups[0];
+  // mixed hexahedra: the persistent kernel has the 1- and 2-point forms
+  if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED && gr.tune.qu != 1 &&
+      gr.tune.qu != 2)
+    return false;
+  static int coop = -1;
+  if (coop < 0) {
+    int dev = 0, v = 0;
+    coop = (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && v)
+               ? 1
+               : 0;
+  }
+  if (!coop) return false;
+  return m->persistent == 2 || m->E <= kPersistentMaxElements;
+}
+
+// nsteps steps in persistent launches (up to 10,000 steps each)
+int run_persistent(akb_model *m, int64_t nsteps, bool any_plastic) {
+  if (!m->predicted) AKB_TRY(predict(m));
+  const Group &gr = m->groups[0];
+  DevGeom g = m->geom();
+  int64_t left = nsteps;
+  while (left > 0) {
+    const int64_t n = std::min<int64_t>(left, 10000);
+    StepArgs sa;
+    std::memset(&sa, 0, sizeof(sa));
+    sa.E = m->E;
+    sa.N = m->N;
+    sa.conn = m->dconn;
+    sa.pos = m->dpos;
+    sa.ptr = m->dptr;
+    if (m->precision == AKB_PRECISION_MIXED) {
+      sa.B = m->fB;
+      sa.wJ = m->fwJ;
+    } else {
+      sa.B = m->dB;
+      sa.wJ = m->dwJ;
+    }
+    sa.X = m->dX;
+    sa.mp = m->mats[gr.mat0].params();
+    sa.ps = group_args(m, gr, true);
+    sa.re = m->dre;
+    sa.fext = m->dfext;
+    sa.mass = m->dmass;
+    sa.blocked = m->dblocked;
+    sa.fint = m->dfint;
+    sa.a = m->da;
+    sa.v = m->dv;
+    sa.u_pred = m->u_pred();
+    sa.u_other = m->u();
+    sa.dt = m->dt;
+    sa.node_inst = m->dnode_inst;
+    sa.inst_dt = m->dinst_dt;
+    sa.flags = NU_CORRECT | NU_PREDICT | (m->fext_zero ? NU_FEXT_ZERO : 0);
+    sa.plastic = any_plastic ? 1 : 0;
+    sa.nsteps = n;
+    sa.status = m->dstatus;
+    sa.bar = m->dbar;
+    AKB_CUDA(cudaMemsetAsync(m->dbar, 0, 2 * sizeof(unsigned int), m->stream));
+    cudaError_t e = m->precision == AKB_PRECISION_MIXED
+                        ? launch_persistent_mixed(g, gr.law, gr.tune.qu, sa, m->tab, m->stream)
+                        : launch_persistent_fp64(g, gr.law, gr.tune.qu, sa, m->tab, m->stream);
+    if (e != cudaSuccess)
+      return fail(AKB_ECUDA, std::string("persistent steps: ") + cudaGetErrorString(e));
+    if (n & 1) m->ucur = 1 - m->ucur;
+    if (any_plastic && (n & 1)) m->cur = 1 - m->cur;
+    m->steps_done += n;
+    left -= n;
+  }
+  m->fint_valid = false;
+  return AKB_OK;
+}
+
 int ensure_qp_scratch(akb_model *m) {
   int64_t need = 0;
   for (auto &mt : m->mats) need = std::max(need, mt.e_count * m->nq * m->dim * m->dim);
@@ -794,9 +878,12 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
         m->groups.push_back(gr);
       }
       Group &gr = m->groups.back();
-      // mixed hexahedra: 2 points per unrolled iteration (the fastest form
-      // for all three laws at 128^3 on B200)
-      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED) gr.tune.qu = 2;
+      // mixed hexahedra, fastest forms measured at 128^3 on B200: 2 points
+      // per unrolled iteration (elastic, neohookean); 1 point with registers
+      // capped for 5 blocks per SM (plastic, whose state loads need latency
+      // hiding more than registers)
+      if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED)
+        gr.tune = gr.law == LAW_PLASTIC ? ElemTuning{128, 1, 5} : ElemTuning{128, 2, 1};
       gr.nmat++;
       gr.e_count += mt.e_count;
       mt.group = (int)m->groups.size() - 1;
@@ -855,6 +942,7 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   AKB_TRY(m->alloc(&m->dpartials, sizeof(double) * kReducePartials));
   AKB_TRY(m->alloc(&m->dresult, sizeof(double)));
   AKB_TRY(m->alloc(&m->dstatus, sizeof(unsigned int)));
+  AKB_TRY(m->alloc(&m->dbar, 2 * sizeof(unsigned int)));
   AKB_TRY(m->alloc(&m->dbad, sizeof(unsigned long long)));
   cudaStream_t s = m->stream;
   AKB_CUDA(cudaMemcpyAsync(m->dX, m->X.data(), sizeof(double) * N * d, cudaMemcpyHostToDevice, s));
@@ -1283,6 +1371,12 @@ int akb_model_solve_step(akb_model *m, int64_t nsteps) {
   if (nsteps < 0) return fail(AKB_EINVAL, "negative step count");
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
+  if (nsteps > 0 && use_persistent(m)) {
+    AKB_TRY(run_persistent(m, nsteps, any_plastic));
+    m->forces_evaluated = true;
+    m->snap_valid = false;
+    return AKB_OK;
+  }
   int64_t left = nsteps;
   // a step whose prediction is stale runs eagerly (it launches the predictor)
   if (left > 0 && !m->predicted) {
@@ -1304,6 +1398,10 @@ int akb_model_solve_step(akb_model *m, int64_t nsteps) {
 
 int akb_model_prepare_graphs(akb_model *m) {
   AKB_TRY(check_model(m, true));
+  if (use_persistent(m)) {  // persistent launches need no graph, only the prediction
+    if (!m->predicted) AKB_TRY(predict(m));
+    return AKB_OK;
+  }
   if (m->graph_steps == 0) return AKB_OK;
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
@@ -1395,6 +1493,20 @@ int akb_model_set_prescribed_velocity_ramp(akb_model *m, const int64_t *dofs, in
   m->presc_vmax = v_max;
   m->presc_ramp = ramp_steps;
   m->predicted = false;
+  return AKB_OK;
+}
+
+int akb_model_set_persistent(akb_model *m, int mode) {
+  AKB_TRY(check_model(m, false));
+  if (mode < 0 || mode > 2) return fail(AKB_EINVAL, "mode must be 0, 1 or 2");
+  m->persistent = mode;
+  return AKB_OK;
+}
+
+int akb_model_persistent_active(const akb_model *m, int *active) {
+  if (!m || !active) return fail(AKB_EINVAL, "null argument");
+  if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  *active = use_persistent(m) ? 1 : 0;
   return AKB_OK;
 }
 

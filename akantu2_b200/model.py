@@ -289,6 +289,22 @@ class SolidMechanicsModel:
         self._invalidate()
         return total.value, list(phases)
 
+    def setPersistent(self, mode):
+        """0: never, 1: small single-law meshes (default), 2: whenever allowed
+        -- whole step sequences in one persistent launch (akb_model_set_persistent)."""
+        _capi.check(_capi.lib().akb_model_set_persistent(self._h, int(mode)))
+
+    def persistentActive(self):
+        a = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_persistent_active(self._h, ctypes.byref(a)))
+        return bool(a.value)
+
+    def prepareGraphs(self):
+        """Captures the step graph the next solveStep launches, so that the
+        capture is not paid inside a timed run (akb_model_prepare_graphs)."""
+        self._sync_up()
+        _capi.check(_capi.lib().akb_model_prepare_graphs(self._h))
+
     def setGraphSteps(self, steps):
         """Multi-step runs are replayed as CUDA graphs of `steps` steps (even; 0 disables)."""
         _capi.check(_capi.lib().akb_model_set_graph_steps(self._h, int(steps)))

@@ -189,6 +189,15 @@ int akb_model_solve_step(akb_model *model, int64_t nsteps);
  * parity, dt, zero external force) and replayed; steps that follow a host
  * edit of u, v, a, the blocked dofs or dt run eagerly first. */
 int akb_model_set_graph_steps(akb_model *model, int64_t steps);
+/* persistent multi-step kernel: a model of one law group runs a whole
+ * solve_step in one cooperative launch (all blocks resident, grid barriers
+ * between the element and node phases, bounded waits reported in bit 1 of
+ * the status word), with the arithmetic of the two-kernel step.  mode 0:
+ * never; 1 (default): meshes of at most 2^18 elements, where launch latency
+ * dominates; 2: whenever the model allows it.  Not used with a prescribed
+ * motion or several constitutive laws. */
+int akb_model_set_persistent(akb_model *model, int mode);
+int akb_model_persistent_active(const akb_model *model, int *active);
 /* autotuner: times the candidate launch shapes of each law group's
  * element-force kernel (threads per block 64 / 128 / 256; for mixed
  * hexahedra also a register cap for 5 resident blocks of 128) and of the node
@@ -240,7 +249,8 @@ int akb_model_time_steps(akb_model *model, int64_t nsteps, double *elapsed_ms);
 int akb_model_profile_steps(akb_model *model, int64_t nsteps, double *total_ms,
                             double *phase_ms);
 /* device status word: bit 0 = non-finite acceleration seen since the last
- * call (the flag is cleared by reading it) */
+ * call, bit 1 = a grid barrier of the persistent kernel timed out (the
+ * launch stopped early); the word is cleared by reading it */
 int akb_model_get_status(akb_model *model, int *flags);
 
 /* ---- batches of independent meshes --------------------------------------- */

@@ -115,3 +115,59 @@ def test_hex8_sum_factorisation_accuracy(mat):
         other = _run(mesh, mat, "mixed", v0, bl, 500, shape=(128, qu, 256)).getDisplacement()
         assert np.linalg.norm(other - uo) / np.linalg.norm(uo) < 1e-5, qu
         assert np.linalg.norm(other - u) / np.linalg.norm(uo) < 1e-5, qu
+
+
+@pytest.mark.parametrize("etype,precision,mat", [
+    ("_tetrahedron_4", "fp64", UNIT_ELASTIC), ("_tetrahedron_4", "mixed", UNIT_ELASTIC),
+    ("_hexahedron_8", "mixed", UNIT_NEOHOOKEAN), ("_hexahedron_8", "fp64", UNIT_NEOHOOKEAN),
+    ("_hexahedron_8", "mixed", UNIT_PLASTIC),
+    ("_triangle_6", "fp64", UNIT_PLASTIC), ("_triangle_6", "mixed", UNIT_PLASTIC)])
+def test_persistent_kernel_is_bit_identical(etype, precision, mat):
+    """whole step sequences in one persistent launch give the state of the
+    two-kernel graphs, including an odd step count and a host edit between"""
+    mesh = {"_hexahedron_8": lambda: akb.box_hex8(5), "_triangle_6": lambda: akb.square_tri6(6),
+            "_tetrahedron_4": lambda: akb.box_tet4(5)}[etype]()
+    d = mesh.spatial_dimension
+    v0 = sinusoidal_velocity(mesh.nodes, 0.03) if d == 3 else \
+        np.stack([0.02 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
+    bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
+    runs = []
+    for mode in (0, 2):
+        m = gpu_model(mesh, [mat], precision=precision)
+        m.setPersistent(mode)
+        assert m.persistentActive() == (mode == 2)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.solveStep(137)
+        f = m.getExternalForce()
+        f[:, 0] = 1e-4
+        m.solveStep(100)
+        assert m.getStatus() == 0
+        got = [m.getDisplacement().copy(), m.getVelocity().copy(), m.getAcceleration().copy(),
+               m.getInternalForce().copy()]
+        if mat is UNIT_PLASTIC:
+            got += [m.getMaterial(0).getInternal(f)() for f in ("inelastic_strain",
+                                                                "iso_hardening", "plastic_energy")]
+        runs.append(got)
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+
+
+def test_persistent_batch_with_instance_time_steps():
+    meshes = [akb.box_tet4(n) for n in (2, 3, 4)]
+    outs = []
+    for mode in (0, 2):
+        b = akb.BatchModel(meshes)
+        for k in range(3):
+            b.addMaterial("elastic", name=f"m{k}", rho=1.0, E=0.5 + k, nu=0.3)
+        b.setInstanceMaterials(np.arange(3))
+        b.initFull(akb._explicit_lumped_mass, precision="mixed")
+        b.setPersistent(mode)
+        b.setNodal("velocity", np.concatenate([sinusoidal_velocity(m.nodes) for m in meshes]))
+        b.setNodal("blocked_dofs", np.concatenate([blocked_face(m.nodes) for m in meshes]))
+        b.setTimeSteps(0.8 * b.getStableTimeSteps())
+        b.solveStep(251)
+        outs.append((b.getDisplacement().copy(), b.getVelocity().copy()))
+    for a, c in zip(*outs):
+        assert np.array_equal(a, c)
