@@ -66,8 +66,8 @@ inline cudaError_t launch_cooperative(K kernel, int64_t work, const StepArgs &sa
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   const int64_t want = (work + kPersistentThreads - 1) / kPersistentThreads;
-  const unsigned grid =
-      (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * sms));
+  const unsigned grid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(std::min<int64_t>(want, (int64_t)per_sm * sms), 8192));
   StepArgs a = sa;
   QuadTable t = tab;
   void *args[] = {&a, &t};

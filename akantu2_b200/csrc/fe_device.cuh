@@ -15,9 +15,12 @@ namespace akb {
 enum { ET_TET4 = 0, ET_HEX8 = 1, ET_TRI6 = 2 };
 enum { LAW_ELASTIC = 0, LAW_NEOHOOKEAN = 1, LAW_PLASTIC = 2 };
 
-// Lame constants and the per-material scalars the laws read
+// Lame constants and the per-material scalars the laws read.  svk selects,
+// in the finite-strain kernels, the finite-deformation elastic law
+// (`elastic` with finite_deformation = true) instead of the neohookean one.
 struct MatParams {
   double lambda, mu, sigma_y, h, sigma_th, rho;
+  int svk;
 };
 
 // ---- small dense algebra, column-major m[i + j*D] ---------------------------
@@ -108,6 +111,34 @@ __device__ __forceinline__ void neohookean_pk2(T lambda, T mu, const T *g, T *S)
       const T t = c * Ci[i + D * j];
       S[i + D * j] = (i == j) ? mu + t : t;
     }
+}
+
+// Green-Lagrange strain E = (g^T g + g^T + g) / 2 (material_inline_impl.hh:127-130)
+template <int D, class T>
+__device__ __forceinline__ void green_lagrange(const T *g, T *E) {
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T s = g[0 + D * i] * g[0 + D * j];
+#pragma unroll
+      for (int k = 1; k < D; ++k) s = s + g[k + D * i] * g[k + D * j];
+      E[i + D * j] = ((s + g[j + D * i]) + g[i + D * j]) / T(2);
+    }
+}
+
+// second Piola-Kirchhoff stress of a finite-strain material: the elastic law
+// applied to E (MaterialElastic::computeStress with finite_deformation,
+// material_elastic.cc:82-101), or the neohookean law
+template <int D, class T>
+__device__ __forceinline__ void finite_pk2(const MatParams &mp, const T *g, T *S) {
+  if (mp.svk) {
+    T E[D * D];
+    green_lagrange<D, T>(g, E);
+    elastic_stress<D, T>((T)mp.lambda, (T)mp.mu, E, (T)mp.sigma_th, S);
+  } else {
+    neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
+  }
 }
 
 // radial return with linear isotropic hardening, small strain

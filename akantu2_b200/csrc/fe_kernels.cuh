@@ -419,7 +419,13 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
     if constexpr (REL) {
       // mixed path: r = (F S w) . dN/dx with F S from the cofactors of F
       T P[D * D];
-      neohookean_piola_cof<D, T>((T)mp.lambda, (T)mp.mu, g, w, P);
+      if (mp.svk) {
+        T S[D * D];
+        finite_pk2<D, T>(mp, g, S);
+        first_piola<D, T>(g, S, w, P);
+      } else {
+        neohookean_piola_cof<D, T>((T)mp.lambda, (T)mp.mu, g, w, P);
+      }
 #pragma unroll
       for (int a = 0; a < NN; ++a)
 #pragma unroll
@@ -431,7 +437,7 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
         }
     } else {
       T S[D * D];
-      neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
+      finite_pk2<D, T>(mp, g, S);
       T Sv[D == 3 ? 6 : 3];
       to_voigt<D, T>(S, Sv);
 #pragma unroll
@@ -677,7 +683,13 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
                                            const GroupArgs &ps, int64_t ne, int64_t le, int q,
                                            float *P) {
   if constexpr (LAW == LAW_NEOHOOKEAN) {
-    neohookean_piola_cof<D, float>((float)mp.lambda, (float)mp.mu, g, w, P);
+    if (mp.svk) {
+      float S[D * D];
+      finite_pk2<D, float>(mp, g, S);
+      first_piola<D, float>(g, S, w, P);
+    } else {
+      neohookean_piola_cof<D, float>((float)mp.lambda, (float)mp.mu, g, w, P);
+    }
   } else if constexpr (LAW == LAW_ELASTIC) {
     float sig[D * D];
     elastic_stress<D, float>((float)mp.lambda, (float)mp.mu, g, (float)mp.sigma_th, sig);
@@ -1007,37 +1019,60 @@ struct StepArgs {
   int plastic;         // swap the plastic state buffers after each step
   int64_t nsteps;
   unsigned int *status;
-  unsigned int *bar;   // [2]: arrivals, generation
+  unsigned int *bar;   // [1 + blocks]: release generation, then one arrival flag per block
 };
 
 constexpr int kPersistentThreads = 256;
 constexpr unsigned int kBarrierSpinLimit = 1u << 24;  // x 64 ns sleeps: about a second
 constexpr unsigned int ST_BARRIER_TIMEOUT = 2u;
 
-// grid-wide barrier with a bounded wait: false (status bit 1 set) when the
-// other blocks did not all arrive within the limit
-__device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int *status) {
+// grid-wide barrier number `gen` (1, 2, ... within a launch) with bounded
+// waits: every block publishes its arrival in its own flag (no contended
+// atomic), the first warp of block 0 waits for all flags and then publishes
+// the release, which the other blocks wait for.  Returns false (status bit 1
+// set) when a wait ran out.
+__device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int gen,
+                                             unsigned int *status) {
   __shared__ int ok;
+  volatile unsigned int *release = bar;
+  volatile unsigned int *arrive = bar + 1;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int *gen = bar + 1;
-    const unsigned int g = *gen;
-    __threadfence();
     ok = 1;
-    if (atomicAdd(bar, 1u) + 1 == gridDim.x) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      unsigned int spins = 0;
-      while (*gen == g) {
-        if (++spins > kBarrierSpinLimit) {
-          atomicOr(status, ST_BARRIER_TIMEOUT);
-          break;
+    __threadfence();
+    arrive[blockIdx.x] = gen;
+  }
+  if (blockIdx.x == 0) {
+    if (threadIdx.x < 32) {
+      bool fine = true;
+      for (unsigned int b = threadIdx.x; b < gridDim.x && fine; b += 32) {
+        unsigned int spins = 0;
+        while (arrive[b] != gen) {
+          if (++spins > kBarrierSpinLimit) {
+            fine = false;
+            break;
+          }
+          __nanosleep(32);
         }
-        __nanosleep(64);
+      }
+      fine = __all_sync(0xffffffffu, fine);
+      if (threadIdx.x == 0) {
+        if (!fine) atomicOr(status, ST_BARRIER_TIMEOUT);
+        __threadfence();
+        *release = gen;  // released even after a timeout, so no block waits on
       }
     }
+  } else if (threadIdx.x == 0) {
+    unsigned int spins = 0;
+    while (*release != gen) {
+      if (++spins > kBarrierSpinLimit) {
+        atomicOr(status, ST_BARRIER_TIMEOUT);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  if (threadIdx.x == 0) {
     __threadfence();
     if (*(volatile unsigned int *)status & ST_BARRIER_TIMEOUT) ok = 0;
   }
@@ -1064,6 +1099,7 @@ __global__ void __launch_bounds__(kPersistentThreads)
   GroupArgs ps = sa.ps;
   double *up = sa.u_pred, *uo = sa.u_other;
   RT *re = static_cast<RT *>(sa.re);
+  unsigned int gen = 0;
   for (int64_t s = 0; s < sa.nsteps; ++s) {
     for (int64_t le = t0; le < sa.E; le += stride) {
       const MatParams &mp = sa.mp;
@@ -1078,11 +1114,11 @@ __global__ void __launch_bounds__(kPersistentThreads)
         element_hex8sf<LAW, QU>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, up, mp, ps,
                                 reinterpret_cast<float *>(re));
     }
-    if (!grid_barrier(sa.bar, sa.status)) return;
+    if (!grid_barrier(sa.bar, ++gen, sa.status)) return;
     for (int64_t i = t0; i < sa.N; i += stride)
       node_body<D, RT, KAHAN>(i, sa.ptr, re, sa.fext, sa.mass, sa.blocked, sa.fint, sa.a, sa.v,
                               up, uo, sa.dt, sa.node_inst, sa.inst_dt, sa.flags, sa.status);
-    if (!grid_barrier(sa.bar, sa.status)) return;
+    if (!grid_barrier(sa.bar, ++gen, sa.status)) return;
     double *tu = up;
     up = uo;
     uo = tu;
@@ -1124,7 +1160,7 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
       g[i + D * j] = acc;
     }
   if constexpr (LAW == LAW_NEOHOOKEAN)
-    neohookean_pk2<D, double>(mp.lambda, mp.mu, g, s);
+    finite_pk2<D, double>(mp, g, s);
   else
     elastic_stress<D, double>(mp.lambda, mp.mu, g, mp.sigma_th, s);
 #pragma unroll

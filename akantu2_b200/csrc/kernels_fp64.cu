@@ -264,9 +264,25 @@ __global__ void k_energy_elem(int which, int64_t e0, int64_t ne, int64_t ld, int
         for (int k = 1; k < D; ++k) tt = tt + F[k + D * i] * F[k + D * i];
         trC = (i == 0) ? tt : trC + tt;
       }
-      double J;
-      if constexpr (D == 3) J = det3(F); else J = det2(F);
-      dens = mp.lambda * pow(log(J), 2.) + mp.mu * (-log(J) + (trC - D) / 2.) / 2.;
+      if (mp.svk) {
+        // finite-deformation elastic: .5 S : E (material_elastic.cc:140-157,
+        // material_elastic_inline_impl.hh:113-116), S the stored PK2 stress
+        double g[DD], E[DD];
+#pragma unroll
+        for (int k = 0; k < DD; ++k) g[k] = (double)grad[at(k)];
+        green_lagrange<D, double>(g, E);
+        double dot = 0.;
+#pragma unroll
+        for (int k = 0; k < DD; ++k) {
+          const double sk = stress[at(k)];
+          dot = (k == 0) ? sk * E[k] : dot + sk * E[k];
+        }
+        dens = .5 * dot;
+      } else {
+        double J;
+        if constexpr (D == 3) J = det3(F); else J = det2(F);
+        dens = mp.lambda * pow(log(J), 2.) + mp.mu * (-log(J) + (trC - D) / 2.) / 2.;
+      }
     } else {
       double dot = 0.;
 #pragma unroll

@@ -45,6 +45,9 @@ struct Material {
   int law = LAW_ELASTIC;
   double rho = 0., E = 0., nu = 0.5, sigma_y = 0., h = 0., alpha = 0., delta_T = 0.;
   bool plane_stress = false, finite_deformation = false;
+  // `elastic` with finite_deformation: runs in the finite-strain (neohookean)
+  // kernels with the elastic law applied to the Green-Lagrange strain
+  bool svk = false;
   double lambda = 0., mu = 0., sigma_th = 0.;
   int64_t e_begin = 0, e_count = 0;  // internal element range
   int group = 0;                     // law group holding the range
@@ -54,11 +57,13 @@ struct Material {
   void update(int dim) {
     lambda = nu * E / ((1 + nu) * (1 - 2 * nu));
     mu = E / (2 * (1 + nu));
-    if (dim == 2 && plane_stress && law != LAW_NEOHOOKEAN)
+    if (dim == 2 && plane_stress && (law != LAW_NEOHOOKEAN || svk))
       lambda = nu * E / ((1 + nu) * (1 - nu));
     sigma_th = -E / (1. - 2. * nu) * alpha * delta_T;
   }
-  MatParams params() const { return MatParams{lambda, mu, sigma_y, h, sigma_th, rho}; }
+  MatParams params() const {
+    return MatParams{lambda, mu, sigma_y, h, sigma_th, rho, svk ? 1 : 0};
+  }
   double celerity() const { return std::sqrt((lambda + 2 * mu) / rho); }
 };
 
@@ -320,11 +325,13 @@ int make_material(akb_model *m, const std::string &type, const std::string &name
       continue;
     if (rc != AKB_OK) return rc;
   }
-  if (mat.law == LAW_ELASTIC && mat.finite_deformation)
-    return fail(AKB_EUNSUPPORTED, "finite_deformation elastic is not supported by this path");
+  if (mat.law == LAW_ELASTIC && mat.finite_deformation) {
+    mat.law = LAW_NEOHOOKEAN;
+    mat.svk = true;
+  }
   if (mat.law == LAW_PLASTIC && mat.finite_deformation)
     return fail(AKB_EUNSUPPORTED, "finite-strain plasticity is not supported by this path");
-  if (mat.law == LAW_NEOHOOKEAN && mat.plane_stress)
+  if (mat.law == LAW_NEOHOOKEAN && !mat.svk && mat.plane_stress)
     return fail(AKB_EUNSUPPORTED, "plane-stress neohookean is not supported by this path");
   if (mat.law == LAW_PLASTIC && mat.alpha * mat.delta_T != 0.)
     return fail(AKB_EUNSUPPORTED, "thermal stress with plasticity is not supported");
@@ -524,6 +531,10 @@ int run_graph(akb_model *m, bool any_plastic) {
   return AKB_OK;
 }
 
+// release word + one arrival flag per block of a persistent launch (its grid
+// is at most the resident-block capacity, far below this)
+constexpr int kBarrierWords = 1 + 8192;
+
 // small meshes of one law group run whole step sequences in one persistent
 // launch (launch latency dominates the two-kernel step below about this size)
 constexpr int64_t kPersistentMaxElements = 1 << 18;
@@ -589,7 +600,7 @@ int run_persistent(akb_model *m, int64_t nsteps, bool any_plastic) {
     sa.nsteps = n;
     sa.status = m->dstatus;
     sa.bar = m->dbar;
-    AKB_CUDA(cudaMemsetAsync(m->dbar, 0, 2 * sizeof(unsigned int), m->stream));
+    AKB_CUDA(cudaMemsetAsync(m->dbar, 0, kBarrierWords * sizeof(unsigned int), m->stream));
     cudaError_t e = m->precision == AKB_PRECISION_MIXED
                         ? launch_persistent_mixed(g, gr.law, gr.tune.qu, sa, m->tab, m->stream)
                         : launch_persistent_fp64(g, gr.law, gr.tune.qu, sa, m->tab, m->stream);
@@ -942,7 +953,7 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   AKB_TRY(m->alloc(&m->dpartials, sizeof(double) * kReducePartials));
   AKB_TRY(m->alloc(&m->dresult, sizeof(double)));
   AKB_TRY(m->alloc(&m->dstatus, sizeof(unsigned int)));
-  AKB_TRY(m->alloc(&m->dbar, 2 * sizeof(unsigned int)));
+  AKB_TRY(m->alloc(&m->dbar, kBarrierWords * sizeof(unsigned int)));
   AKB_TRY(m->alloc(&m->dbad, sizeof(unsigned long long)));
   cudaStream_t s = m->stream;
   AKB_CUDA(cudaMemcpyAsync(m->dX, m->X.data(), sizeof(double) * N * d, cudaMemcpyHostToDevice, s));

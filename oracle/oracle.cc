@@ -258,7 +258,7 @@ struct Mat {
     if (plane_stress && law != OR_NEOHOOKEAN) lambda = nu * E / ((1 + nu) * (1 - nu));
     sigma_th = -E / (1. - 2. * nu) * alpha * delta_T;
   }
-  bool finite() const { return law == OR_NEOHOOKEAN; }
+  bool finite() const { return law == OR_NEOHOOKEAN || law == OR_ELASTIC_FD; }
   double celerity() const { return std::sqrt((lambda + 2 * mu) / rho); }
 };
 
@@ -277,6 +277,16 @@ inline void elastic(int d, double lambda, double mu, const double *g, double sth
 }
 
 // material_neohookean_inline_impl.hh:37-48 with gradUToF / rightCauchy
+// Green-Lagrange strain E = (g^T g + g^T + g) / 2 (material_inline_impl.hh:127-130)
+inline void green_lagrange(int d, const double *g, double *E) {
+  for (int j = 0; j < d; ++j)
+    for (int i = 0; i < d; ++i) {
+      double s = g[0 + d * i] * g[0 + d * j];
+      for (int k = 1; k < d; ++k) s = s + g[k + d * i] * g[k + d * j];
+      E[i + d * j] = ((s + g[j + d * i]) + g[i + d * j]) / 2.;
+    }
+}
+
 inline void neohookean(int d, double lambda, double mu, const double *g, double C33,
                        double *S) {
   double F[9], C[9], Ci[9];
@@ -392,7 +402,7 @@ void assign_materials(or_model *m) {
     s.grad_u_prev.assign(nqp * dd, 0.);
     s.stress.assign(nqp * dd, 0.);
     s.stress_prev.assign(nqp * dd, 0.);
-    if (m->mats[k].law == OR_NEOHOOKEAN) s.pk2.assign(nqp * dd, 0.);
+    if (m->mats[k].finite()) s.pk2.assign(nqp * dd, 0.);
     if (m->mats[k].law == OR_PLASTIC) {
       s.eps_p.assign(nqp * dd, 0.);
       s.eps_p_prev.assign(nqp * dd, 0.);
@@ -536,7 +546,14 @@ parallel_for(ne, m->threads, [&](long le) {
           }
       } else {
         double *S = &s.pk2[qp * dd];
-        neohookean(d, mat.lambda, mat.mu, g, 1., S);
+        if (mat.law == OR_ELASTIC_FD) {
+          // MaterialElastic::computeStress, finite deformation (material_elastic.cc:82-101)
+          double Egl[9];
+          green_lagrange(d, g, Egl);
+          elastic(d, mat.lambda, mat.mu, Egl, mat.sigma_th, S);
+        } else {
+          neohookean(d, mat.lambda, mat.mu, g, 1., S);
+        }
         // r_q = (B_L0 + B_L2(grad u))^T S_voigt  (material.cc:547-565)
         const int nv = d == 3 ? 6 : 3;
         double Sv[6];
@@ -850,6 +867,15 @@ double or_model_energy(or_model *m, int which) {
         if (which == OR_EPLASTIC) {
           if (mat.law != OR_PLASTIC) continue;
           dens = s.pe[qp];
+        } else if (mat.law == OR_ELASTIC_FD) {
+          // .5 S : E (material_elastic.cc:140-157)
+          const double *g = &s.grad_u[qp * dd];
+          const double *S = &s.pk2[qp * dd];
+          double Egl[9];
+          green_lagrange(d, g, Egl);
+          double dot = 0.;
+          for (int c = 0; c < dd; ++c) dot = (c == 0) ? S[c] * Egl[c] : dot + S[c] * Egl[c];
+          dens = .5 * dot;
         } else if (mat.law == OR_NEOHOOKEAN) {
           const double *g = &s.grad_u[qp * dd];
           double F[9];

@@ -36,7 +36,9 @@ extern "C" {
 /* element types (same numbering as the product's C-ABI) */
 enum { OR_TET4 = 0, OR_HEX8 = 1, OR_TRI6 = 2 };
 /* constitutive laws */
-enum { OR_ELASTIC = 0, OR_NEOHOOKEAN = 1, OR_PLASTIC = 2 };
+// OR_ELASTIC_FD: `elastic` with finite_deformation = true (the elastic law
+// applied to the Green-Lagrange strain, finite-strain assembly)
+enum { OR_ELASTIC = 0, OR_NEOHOOKEAN = 1, OR_PLASTIC = 2, OR_ELASTIC_FD = 3 };
 /* nodal fields */
 enum {
   OR_U = 0, OR_V = 1, OR_A = 2, OR_FEXT = 3, OR_FINT = 4, OR_MASS = 5,

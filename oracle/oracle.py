@@ -14,7 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 TET4, HEX8, TRI6 = 0, 1, 2
-ELASTIC, NEOHOOKEAN, PLASTIC = 0, 1, 2
+ELASTIC, NEOHOOKEAN, PLASTIC, ELASTIC_FD = 0, 1, 2, 3
 U, V, A, FEXT, FINT, MASS, BLOCKED = range(7)
 GRAD_U, STRESS, PK2, EPS_P, ISO, PLASTIC_ENERGY = range(6)
 EKIN, EPOT, EXT_WORK, EPLASTIC = range(4)
@@ -163,6 +163,8 @@ class OracleModel:
                                     _p(self.conn), self.E)
         for mat in materials:
             law = _LAWS[mat["type"]] if isinstance(mat["type"], str) else mat["type"]
+            if law == ELASTIC and mat.get("finite_deformation", False):
+                law = ELASTIC_FD
             L.or_model_add_material(self._m, law, mat.get("rho", 0.0), mat.get("E", 0.0),
                                     mat.get("nu", 0.5), mat.get("sigma_y", 0.0),
                                     mat.get("h", 0.0), mat.get("alpha", 0.0),

@@ -377,3 +377,50 @@ def test_device_prescribed_velocity_ramp_bitwise(graph_steps):
     compare(g, o, exact=True)
     assert np.max(np.abs(o.qp(0, orc.EPS_P))) > 0, "the ramp must reach the yield stress"
     assert np.array_equal(g.getMaterial(0).getInternal("inelastic_strain")(), o.qp(0, orc.EPS_P))
+
+
+UNIT_ELASTIC_FD = dict(type="elastic", name="svk", rho=1.0, E=1.0, nu=0.3,
+                       finite_deformation=True)
+
+
+@pytest.mark.parametrize("etype,plane_stress", [("_tetrahedron_4", False),
+                                                ("_hexahedron_8", False),
+                                                ("_triangle_6", False), ("_triangle_6", True)])
+def test_finite_deformation_elastic_bitwise(etype, plane_stress):
+    """`elastic` with finite_deformation = true (the JOSS benchmark's material
+    path): FP64 bit-identical to the oracle, mixed within 1e-5"""
+    mesh = {"_tetrahedron_4": lambda: akb.box_tet4(4), "_hexahedron_8": lambda: akb.box_hex8(4),
+            "_triangle_6": lambda: akb.square_tri6(5)}[etype]()
+    mat = dict(UNIT_ELASTIC_FD, Plane_Stress=plane_stress) if plane_stress else UNIT_ELASTIC_FD
+    d = mesh.spatial_dimension
+    v0 = random_field_velocity(mesh.nodes, seed=8) * 5 if d == 3 else \
+        np.stack([0.1 * mesh.nodes[:, 0], 0.05 * mesh.nodes[:, 1]], axis=1)
+    bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
+    g, o = setup_pair(mesh, [mat], v0, bl)
+    g.solveStep(60)
+    o.step(60)
+    compare(g, o, exact=True)
+    assert np.array_equal(g.getMaterial(0).getInternal("piola_kirchhoff_2")(), o.qp(0, orc.PK2))
+    assert np.max(np.abs(g.getMaterial(0).getStress())) == 0.0  # Cauchy: filled on dump only
+    a, b = g.getEnergy("potential"), o.energy(orc.EPOT)
+    assert b > 0 and abs(a - b) <= 1e-12 * b
+    gm, _ = setup_pair(mesh, [mat], v0, bl, precision="mixed")
+    gm.solveStep(60)
+    uo = o.get(orc.U)
+    assert np.linalg.norm(gm.getDisplacement() - uo) / np.linalg.norm(uo) < 1e-5
+
+
+def test_finite_deformation_elastic_shares_the_finite_strain_launch():
+    """neohookean and finite-deformation elastic materials interleaved: one
+    finite-strain law group with per-element parameters, bit-identical"""
+    mesh = akb.box_hex8(4)
+    mat_of_elem = (np.arange(mesh.getNbElement()) % 2).astype(np.int32)
+    mats = [dict(UNIT_NEOHOOKEAN, name="nh"), dict(UNIT_ELASTIC_FD, E=2.0)]
+    v0 = random_field_velocity(mesh.nodes, seed=12)
+    g, o = setup_pair(mesh, mats, v0, blocked_face(mesh.nodes), mat_of_elem=mat_of_elem)
+    g.solveStep(40)
+    o.step(40)
+    compare(g, o, exact=False)
+    for k in range(2):
+        assert np.array_equal(g.getMaterial(k).getInternal("piola_kirchhoff_2")(),
+                              o.qp(k, orc.PK2)) or k == 0

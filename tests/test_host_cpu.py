@@ -82,13 +82,22 @@ def test_dat_parser_reads_materials_and_expressions():
     ("material elastic [ E = 1 ", 6),
     ("material elastic [ E = abc ]", 6),
     ("material elastic [ Youngs = 1 ]", 6),
-    ("material elastic [ E = 1\n finite_deformation = true ]", 8),
+    ("material plastic_linear_isotropic_hardening [ E = 1\n finite_deformation = true ]", 8),
+    ("material neohookean [ E = 1\n Plane_Stress = true ]", 8),
 ])
 def test_dat_parser_errors(text, code):
     _, m = _tiny_model()
     rc = _capi.lib().akb_model_load_materials(m._h, text.encode())
     assert rc == code
     assert _capi.lib().akb_last_error()
+
+
+def test_finite_deformation_elastic_is_accepted():
+    _, m = _tiny_model()
+    text = "material elastic [\n name = svk\n E = 2\n nu = 0.25\n finite_deformation = true\n]\n"
+    _capi.check(_capi.lib().akb_model_load_materials(m._h, text.encode()))
+    mat = m.getMaterial(0)
+    assert mat.get("finite_deformation") == 1.0 and mat.get("E") == 2.0
 
 
 def test_permissive_parser_ignores_unknown_parameters():

@@ -259,3 +259,30 @@ def test_neohookean_reference_state_and_objectivity():
     lam, mu = 0.3 / (1.3 * 0.4), 1 / 2.6
     lin = lam * np.trace(eps) * np.eye(3) + 2 * mu * eps
     assert np.max(np.abs(S - lin)) < 1e-12
+
+
+def test_finite_deformation_elastic_oracle_limits():
+    """`elastic` with finite_deformation: a rigid rotation stores no stress and
+    produces no force (E = 0); a small uniform strain gives the small-strain
+    elastic forces to first order"""
+    from akantu2_b200 import box_hex8
+    mesh = box_hex8(2)
+    x = mesh.nodes
+    mat = dict(type="elastic", rho=1.0, E=1.0, nu=0.3, finite_deformation=True)
+    lin = dict(type="elastic", rho=1.0, E=1.0, nu=0.3)
+    rng = np.random.default_rng(5)
+    R = _random_rotation(rng, 3)
+    o = orc.OracleModel(orc.HEX8, x, mesh.connectivity, [mat])
+    o.set(orc.U, x @ R.T - x)
+    o.assemble_internal_forces()
+    assert np.max(np.abs(o.get(orc.FINT))) < 1e-14
+    assert np.max(np.abs(o.qp(0, orc.PK2))) < 1e-14
+    eps = 1e-7 * rng.standard_normal((3, 3))
+    u = x @ eps.T
+    o.set(orc.U, u)
+    o.assemble_internal_forces()
+    ol = orc.OracleModel(orc.HEX8, x, mesh.connectivity, [lin])
+    ol.set(orc.U, u)
+    ol.assemble_internal_forces()
+    f, fl = o.get(orc.FINT), ol.get(orc.FINT)
+    assert np.max(np.abs(f - fl)) <= 1e-6 * np.max(np.abs(fl))
