@@ -242,9 +242,10 @@ struct akb_model {
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
   int node_block = 128;       // threads per block of the node update
-  // persistent multi-step kernel: 0 never, 1 for small single-group meshes,
-  // 2 whenever the model allows it (akb_model_set_persistent)
-  int persistent = 1;
+  // persistent multi-step kernel: 0 never (default: on B200 the 100-step
+  // graphs of the two-kernel step are faster at every measured size), 1 for
+  // small single-group meshes, 2 whenever the model allows it
+  int persistent = 0;
   unsigned int *dbar = nullptr;  // grid-barrier counters
   // prescribed velocity ramp on a set of dofs (akb_model_set_prescribed_velocity_ramp)
   int64_t presc_count = 0, presc_ramp = 1;
@@ -1454,6 +1455,7 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   const int64_t re_bytes = (precision == AKB_PRECISION_MIXED ? 4 : 8) * E * nn * slot_vals;
   t += r(std::max(re_bytes, 8 * E * nn));
   t += r(8 * std::max<int64_t>(std::max(E, N), 1)) + 8 * kReducePartials + 4 * 16;
+  t += 4 * kBarrierWords;
   if (precision == AKB_PRECISION_MIXED && d == 2) t += r(4 * E * nq * nn * d) + r(4 * E * nq);
   const int64_t gs = precision == AKB_PRECISION_MIXED ? 4 : 8, ns = sym_comps((int)d);
   if (law == LAW_PLASTIC)
