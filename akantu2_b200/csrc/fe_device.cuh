@@ -21,6 +21,7 @@ enum { LAW_ELASTIC = 0, LAW_NEOHOOKEAN = 1, LAW_PLASTIC = 2 };
 struct MatParams {
   double lambda, mu, sigma_y, h, sigma_th, rho;
   int svk;
+  int c33;  // plane-stress neohookean: J includes the out-of-plane stretch sqrt(C33)
 };
 
 // ---- small dense algebra, column-major m[i + j*D] ---------------------------
@@ -74,10 +75,11 @@ __device__ __forceinline__ void elastic_stress(T lambda, T mu, const T *g, T sth
     }
 }
 
-// S = mu I + (lambda ln J - mu) C^-1, F = I + grad u, C = F^T F
+// S = mu I + (lambda ln J - mu) C^-1, F = I + grad u, C = F^T F, J = det F
+// (times sqrt(C33) in plane stress, c33 > 0)
 // (material_neohookean_inline_impl.hh:37-48, material_inline_impl.hh:33-81)
 template <int D, class T>
-__device__ __forceinline__ void neohookean_pk2(T lambda, T mu, const T *g, T *S) {
+__device__ __forceinline__ void neohookean_pk2(T lambda, T mu, const T *g, T *S, double c33 = 0.) {
   T F[D * D], C[D * D], Ci[D * D];
 #pragma unroll
   for (int j = 0; j < D; ++j)
@@ -102,7 +104,8 @@ __device__ __forceinline__ void neohookean_pk2(T lambda, T mu, const T *g, T *S)
     J = det2(F);
     inv2(C, Ci);
   }
-  // J * sqrt(C33) with C33 = 1 (plane strain / 3D)
+  // J * sqrt(C33); C33 = 1 in plane strain and 3D (the product is exact then)
+  if (c33 > 0.) J = J * (T)sqrt(c33);
   const T c = lambda * log(J) - mu;
 #pragma unroll
   for (int j = 0; j < D; ++j)
@@ -127,17 +130,43 @@ __device__ __forceinline__ void green_lagrange(const T *g, T *E) {
     }
 }
 
+// out-of-plane right Cauchy-Green stretch of a plane-stress neohookean
+// point: Newton iterations from the stored value x on
+//   f(x) = lambda/2 (log x + log(C00 C11 - C01^2)) + mu (x - 1),
+//   f'(x) = lambda / (2 x) + mu, tolerance 1e-5, at most 100 iterations
+// (material_neohookean_inline_impl.hh:52-92, aka_math_tmpl.hh:191-208)
+__device__ __forceinline__ double solve_c33(double lambda, double mu, double C00, double C11,
+                                            double C01, double x) {
+  const double lc = log(C00 * C11 - C01 * C01);
+  double fx = lambda / 2. * (log(x) + lc) + mu * (x - 1.);
+  for (int it = 0; fabs(fx) > 1e-5 && it < 100; ++it) {
+    x -= fx / (lambda / (2. * x) + mu);
+    fx = lambda / 2. * (log(x) + lc) + mu * (x - 1.);
+  }
+  return x;
+}
+
+// right Cauchy-Green entries of a 2D point, C = F^T F
+template <class T>
+__device__ __forceinline__ void right_cauchy2(const T *g, double *c00, double *c11, double *c01) {
+  const T F00 = T(1) + g[0], F10 = g[1], F01 = g[2], F11 = T(1) + g[3];
+  *c00 = (double)(F00 * F00 + F10 * F10);
+  *c11 = (double)(F01 * F01 + F11 * F11);
+  *c01 = (double)(F00 * F01 + F10 * F11);
+}
+
 // second Piola-Kirchhoff stress of a finite-strain material: the elastic law
 // applied to E (MaterialElastic::computeStress with finite_deformation,
-// material_elastic.cc:82-101), or the neohookean law
+// material_elastic.cc:82-101), or the neohookean law (c33 > 0: plane stress)
 template <int D, class T>
-__device__ __forceinline__ void finite_pk2(const MatParams &mp, const T *g, T *S) {
+__device__ __forceinline__ void finite_pk2(const MatParams &mp, const T *g, T *S,
+                                           double c33 = 0.) {
   if (mp.svk) {
     T E[D * D];
     green_lagrange<D, T>(g, E);
     elastic_stress<D, T>((T)mp.lambda, (T)mp.mu, E, (T)mp.sigma_th, S);
   } else {
-    neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S);
+    neohookean_pk2<D, T>((T)mp.lambda, (T)mp.mu, g, S, c33);
   }
 }
 
@@ -262,7 +291,8 @@ __device__ __forceinline__ void first_piola(const T *g, const T *S, T w, T *P) {
 // (F C^-1 = F^-T), the same tensor as first_piola(g, neohookean_pk2(g)) in
 // exact arithmetic without forming C, its inverse or the product F S.
 template <int D, class T>
-__device__ __forceinline__ void neohookean_piola_cof(T lambda, T mu, const T *g, T w, T *P) {
+__device__ __forceinline__ void neohookean_piola_cof(T lambda, T mu, const T *g, T w, T *P,
+                                                     double c33 = 0.) {
   T F[D * D], cof[D * D];
 #pragma unroll
   for (int j = 0; j < D; ++j)
@@ -282,7 +312,10 @@ __device__ __forceinline__ void neohookean_piola_cof(T lambda, T mu, const T *g,
   T det = F[0] * cof[0];
 #pragma unroll
   for (int i = 1; i < D; ++i) det += F[i] * cof[i];
-  const T c = (lambda * log(det) - mu) / det;
+  // ln J = ln det F (+ ln C33 / 2 in plane stress)
+  T lnJ = log(det);
+  if (c33 > 0.) lnJ += (T)(0.5 * log(c33));
+  const T c = (lambda * lnJ - mu) / det;
   const T mw = mu * w, cw = c * w;
 #pragma unroll
   for (int k = 0; k < D * D; ++k) P[k] = mw * F[k] + cw * cof[k];

@@ -86,8 +86,29 @@ struct GroupArgs {
   double *sig, *eps, *iso;
   void *gu;
   double *pe;                // cumulative plastic energy density
+  double *c33;               // [q][ne] plane-stress neohookean out-of-plane stretch
+                             // (updated in place by every stress evaluation), or null
   int update_energy;         // 1 inside solveStep (afterSolveStep), 0 otherwise
 };
+
+// plane-stress C33 of point (le, q), solved from its stored value and stored
+// back (PlaneStressToolbox::computeStress runs computeThirdAxisDeformation on
+// every stress evaluation, plane_stress_toolbox_tmpl.hh:68-74); 0 otherwise
+template <int D, class T>
+__device__ __forceinline__ double point_c33(const MatParams &mp, const GroupArgs &ps, int64_t ne,
+                                            int64_t le, int q, const T *g) {
+  if constexpr (D == 2) {
+    if (mp.c33 && ps.c33) {
+      double c00, c11, c01;
+      right_cauchy2<T>(g, &c00, &c11, &c01);
+      double *p = ps.c33 + (int64_t)q * ne + le;
+      const double x = solve_c33(mp.lambda, mp.mu, c00, c11, c01, *p);
+      *p = x;
+      return x;
+    }
+  }
+  return 0.;
+}
 
 // symmetric d x d tensors: components (0,0), (1,1), (2,2), (1,2), (0,2), (0,1)
 // in 3D, (0,0), (1,1), (0,1) in 2D
@@ -424,7 +445,8 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
         finite_pk2<D, T>(mp, g, S);
         first_piola<D, T>(g, S, w, P);
       } else {
-        neohookean_piola_cof<D, T>((T)mp.lambda, (T)mp.mu, g, w, P);
+        const double c33 = point_c33<D, T>(mp, ps, ne, le, q, g);
+        neohookean_piola_cof<D, T>((T)mp.lambda, (T)mp.mu, g, w, P, c33);
       }
 #pragma unroll
       for (int a = 0; a < NN; ++a)
@@ -437,7 +459,7 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
         }
     } else {
       T S[D * D];
-      finite_pk2<D, T>(mp, g, S);
+      finite_pk2<D, T>(mp, g, S, point_c33<D, T>(mp, ps, ne, le, q, g));
       T Sv[D == 3 ? 6 : 3];
       to_voigt<D, T>(S, Sv);
 #pragma unroll
@@ -1131,9 +1153,13 @@ __global__ void __launch_bounds__(kPersistentThreads)
 // displacement snapshot (the reference keeps them as internals,
 // material.cc:128-154).  Output [q][D*D][ne].
 template <int D, int NN, int NQ, int LAW>
+// c33: the stored plane-stress stretches of the material's points at
+// c33[q * c33_ld + le] (read only: the getter reports the stress of the last
+// evaluation), or null
 __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const double *__restrict__ B,
                             const double *__restrict__ u, MatParams mp,
+                            const double *__restrict__ c33, int64_t c33_ld,
                             double *__restrict__ grad_out, double *__restrict__ stress_out) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e_count * NQ) return;
@@ -1160,7 +1186,7 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
       g[i + D * j] = acc;
     }
   if constexpr (LAW == LAW_NEOHOOKEAN)
-    finite_pk2<D, double>(mp, g, s);
+    finite_pk2<D, double>(mp, g, s, (c33 && mp.c33) ? c33[(int64_t)q * c33_ld + le] : 0.);
   else
     elastic_stress<D, double>(mp.lambda, mp.mu, g, mp.sigma_th, s);
 #pragma unroll

@@ -56,6 +56,16 @@ cudaError_t launch_segment_min(const double *x, const int64_t *off, int nseg, do
   return cudaGetLastError();
 }
 
+__global__ void k_fill(double *__restrict__ out, double v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+cudaError_t launch_fill(double *out, double v, int64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_fill<<<grid_for(n), kThreads, 0, s>>>(out, v, n);
+  return cudaGetLastError();
+}
+
 __global__ void k_to_float(const double *__restrict__ in, float *__restrict__ out, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (float)in[i];
@@ -158,16 +168,17 @@ cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,
-                             double *grad, double *stress, cudaStream_t s) {
+                             const double *c33, int64_t c33_ld, double *grad, double *stress,
+                             cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
     if (law == LAW_NEOHOOKEAN)
       k_qp_fields<D, NN, NQ, LAW_NEOHOOKEAN><<<grid_for(ne * NQ), kThreads, 0, s>>>(
-          e0, ne, g.E, g.conn, B, u, mp, grad, stress);
+          e0, ne, g.E, g.conn, B, u, mp, c33, c33_ld, grad, stress);
     else
       k_qp_fields<D, NN, NQ, LAW_ELASTIC><<<grid_for(ne * NQ), kThreads, 0, s>>>(
-          e0, ne, g.E, g.conn, B, u, mp, grad, stress);
+          e0, ne, g.E, g.conn, B, u, mp, c33, c33_ld, grad, stress);
   });
   return cudaGetLastError();
 }

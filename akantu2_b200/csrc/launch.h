@@ -57,6 +57,7 @@ cudaError_t launch_element_dt(const DevGeom &g, int64_t e0, int64_t ne, double c
 cudaError_t launch_segment_min(const double *x, const int64_t *off, int nseg, double *out,
                                cudaStream_t s);
 cudaError_t launch_to_float(const double *in, float *out, int64_t n, cudaStream_t s);
+cudaError_t launch_fill(double *out, double v, int64_t n, cudaStream_t s);
 
 // ---- step ------------------------------------------------------------------
 // u_pred = predictor displacement of (u, v, a); v and a are not modified
@@ -105,9 +106,11 @@ cudaError_t launch_persistent_mixed(const DevGeom &g, int law, int qu, const Ste
                                     const QuadTable &tab, cudaStream_t s);
 
 // ---- fields and energies ---------------------------------------------------
+// c33: stored plane-stress stretches of the material's points ([q][c33_ld]), or null
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,
-                             double *grad, double *stress, cudaStream_t s);
+                             const double *c33, int64_t c33_ld, double *grad, double *stress,
+                             cudaStream_t s);
 // per-dof kinetic terms (m > eps ? v v m : 0) summed per node -> out[N]
 cudaError_t launch_ekin_terms(const DevGeom &g, const double *v, const double *mass,
                               double *out, cudaStream_t s);

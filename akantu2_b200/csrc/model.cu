@@ -62,8 +62,9 @@ struct Material {
     sigma_th = -E / (1. - 2. * nu) * alpha * delta_T;
   }
   MatParams params() const {
-    return MatParams{lambda, mu, sigma_y, h, sigma_th, rho, svk ? 1 : 0};
+    return MatParams{lambda, mu, sigma_y, h, sigma_th, rho, svk ? 1 : 0, c33 ? 1 : 0};
   }
+  bool c33 = false;  // plane-stress neohookean (set by initFull in 2D)
   double celerity() const { return std::sqrt((lambda + 2 * mu) / rho); }
 };
 
@@ -84,6 +85,9 @@ struct Group {
   void *gu[2] = {nullptr, nullptr};
   double *iso[2] = {nullptr, nullptr};
   double *pe = nullptr;
+  // plane-stress neohookean: out-of-plane stretch C33 per point, initially 1
+  // (third_axis_deformation, plane_stress_toolbox_tmpl.hh:46)
+  double *c33 = nullptr;
 };
 
 // independent components of a symmetric d x d tensor, and the map from
@@ -332,8 +336,6 @@ int make_material(akb_model *m, const std::string &type, const std::string &name
   }
   if (mat.law == LAW_PLASTIC && mat.finite_deformation)
     return fail(AKB_EUNSUPPORTED, "finite-strain plasticity is not supported by this path");
-  if (mat.law == LAW_NEOHOOKEAN && !mat.svk && mat.plane_stress)
-    return fail(AKB_EUNSUPPORTED, "plane-stress neohookean is not supported by this path");
   if (mat.law == LAW_PLASTIC && mat.alpha * mat.delta_T != 0.)
     return fail(AKB_EUNSUPPORTED, "thermal stress with plasticity is not supported");
   m->mats.push_back(mat);
@@ -369,6 +371,7 @@ GroupArgs group_args(akb_model *m, const Group &mt, bool in_step) {
     ps.mtab = m->dmtab;
     ps.mslot = m->dmslot + mt.e_begin;
   }
+  ps.c33 = mt.c33;
   if (mt.law != LAW_PLASTIC) return ps;
   const int c = m->cur;
   // inside a step the new state goes to the other buffer; a standalone
@@ -637,8 +640,10 @@ int eval_qp_fields(akb_model *m, const Material &mt) {
     return AKB_OK;
   }
   const double *u = m->snap_valid ? m->dusnap : m->u();
+  const Group &gr = m->groups[mt.group];
+  const double *c33 = gr.c33 ? gr.c33 + (mt.e_begin - gr.e_begin) : nullptr;
   AKB_CUDA(launch_qp_fields(m->geom(), mt.law, mt.e_begin, mt.e_count, m->dB, u, mt.params(),
-                            m->dqp_a, m->dqp_b, m->stream));
+                            c33, gr.e_count, m->dqp_a, m->dqp_b, m->stream));
   return AKB_OK;
 }
 
@@ -852,7 +857,10 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(AKB_ECUDA, "no CUDA device available");
-  for (auto &mt : m->mats) mt.update(m->dim);
+  for (auto &mt : m->mats) {
+    mt.update(m->dim);
+    mt.c33 = m->dim == 2 && mt.law == LAW_NEOHOOKEAN && !mt.svk && mt.plane_stress;
+  }
   m->precision = precision;
   AKB_CUDA(cudaGetDevice(&m->device));
   AKB_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
@@ -1006,6 +1014,15 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     }
     AKB_TRY(m->alloc(&mt.pe, sizeof(double) * nqp));
     AKB_CUDA(cudaMemsetAsync(mt.pe, 0, sizeof(double) * std::max<int64_t>(nqp, 1), s));
+  }
+  // plane-stress neohookean points keep their out-of-plane stretch
+  for (auto &gr : m->groups) {
+    bool need = false;
+    for (auto &mt : m->mats) need |= mt.group == (int)(&gr - m->groups.data()) && mt.c33;
+    if (!need) continue;
+    const int64_t nqp = gr.e_count * nq;
+    AKB_TRY(m->alloc(&gr.c33, sizeof(double) * nqp));
+    AKB_CUDA(launch_fill(gr.c33, 1.0, nqp, s));
   }
   // groups of several materials read per-element parameters
   bool multi = false;
@@ -1460,6 +1477,7 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   const int64_t gs = precision == AKB_PRECISION_MIXED ? 4 : 8, ns = sym_comps((int)d);
   if (law == LAW_PLASTIC)
     t += 2 * (2 * r(8 * E * nq * ns) + r(gs * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
+  if (law == LAW_NEOHOOKEAN && d == 2) t += r(8 * E * nq);  // plane-stress C33
   *bytes = t;
   return AKB_OK;
 }
@@ -1560,8 +1578,16 @@ int akb_model_autotune(akb_model *m, int repeats) {
     if (check(cudaEventElapsedTime(ms, e0, e1), "cudaEventElapsedTime")) *ms /= repeats;
     return rc == AKB_OK;
   };
+  // the stress evaluations of the timed launches update C33 in place: they
+  // get a copy
+  int64_t c33_n = 0;
+  for (auto &gr : m->groups)
+    if (gr.c33) c33_n = std::max(c33_n, gr.e_count * m->nq);
+  double *t_c33 = nullptr;
+  if (c33_n > 0) AKB_CUDA(cudaMallocAsync((void **)&t_c33, sizeof(double) * c33_n, s));
   auto elem_launch = [&](Group &gr, const ElemTuning &tn) {
     GroupArgs ps = group_args(m, gr, false);
+    if (gr.c33) ps.c33 = t_c33;
     if (gr.law == LAW_PLASTIC) {
       ps.sig = t_sig;
       ps.gu = t_gu;
@@ -1578,6 +1604,9 @@ int akb_model_autotune(akb_model *m, int repeats) {
   };
   for (auto &gr : m->groups) {
     if (rc != AKB_OK) break;
+    if (gr.c33)
+      check(cudaMemcpyAsync(t_c33, gr.c33, sizeof(double) * gr.e_count * m->nq,
+                            cudaMemcpyDeviceToDevice, s), "copy");
     // threads per block only: the points per iteration of the mixed
     // hexahedron kernel change the FP32 rounding and stay as set
     std::vector<ElemTuning> cand;
@@ -1629,6 +1658,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
     if (rc == AKB_OK) check(elem_launch(gr, gr.tune), "autotune launch");
   check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   cudaFreeAsync(tmp, s);
+  if (t_c33) cudaFreeAsync(t_c33, s);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   // captured graphs hold the old launch shapes

@@ -71,6 +71,8 @@ def parse():
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--precisions", default="mixed,fp64")
+    p.add_argument("--accuracy-steps", type=int, default=10000,
+                   help="steps of the mixed-vs-FP64 accuracy leg (0: skip)")
     return p.parse_args()
 
 
@@ -487,6 +489,9 @@ def run_ours(args):
                                     "d2h_bytes_per_step": nb}
         del m
     head = results[precisions[0]]
+    accuracy = None
+    if rank == 0 and args.accuracy_steps > 0 and set(precisions) >= {"mixed", "fp64"}:
+        accuracy = accuracy_leg(akb, args.config, mesh, mat, v0, blocked, args.accuracy_steps)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -512,6 +517,7 @@ def run_ours(args):
             "gpu_launches": head["gpu_launches"], "state_finite": head["state_finite"],
             "phase_ms_per_step": head["phase_ms_per_step"],
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
         }
         for prec in precisions[1:]:
             r = results[prec]
@@ -522,6 +528,39 @@ def run_ours(args):
             line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
         print(json.dumps(line), flush=True)
     rep.close()
+
+
+def accuracy_leg(akb, config, mesh, mat, v0, blocked, nsteps):
+    """The mixed path against the plain FP64 path (bit-identical to the CPU
+    oracle for elastic / plastic, within 1e-12 for neohookean) after nsteps
+    steps from the same state: relative L2 of the displacement, and the drift
+    of the total energy (kinetic + potential) of each path."""
+    models = {}
+    e0 = {}
+    for prec in ("mixed", "fp64"):
+        m = akb.SolidMechanicsModel(mesh)
+        m.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+        m.initFull(akb._explicit_lumped_mass, precision=prec)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", blocked)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        if config == "tri6":
+            m.setPrescribedVelocityRamp(np.isclose(mesh.nodes[:, 0], 1.0), 0, 1e-3, 5000)
+        e0[prec] = m.getEnergy("kinetic") + m.getEnergy("potential")
+        models[prec] = m
+    out = {"steps": nsteps}
+    for prec, m in models.items():
+        m.solveStep(nsteps)
+        e = m.getEnergy("kinetic") + m.getEnergy("potential")
+        out[f"energy_drift_{prec}"] = (e - e0[prec]) / e0[prec]
+        out[f"energy_{prec}"] = e
+    u, ud = models["mixed"].getDisplacement(), models["fp64"].getDisplacement()
+    out["rel_l2_displacement"] = float(np.linalg.norm(u - ud) / np.linalg.norm(ud))
+    out["energy_rel_diff"] = abs(out["energy_mixed"] - out["energy_fp64"]) / abs(out["energy_fp64"])
+    out["note"] = ("prescribed edge motion: the energy is not conserved, drift is the work of the "
+                   "pulled edge" if config == "tri6" else "free vibration: drift is the "
+                   "integration error of each path")
+    return out
 
 
 def build_batch(akb, meshes, mats, vels, blocks, precision):

@@ -358,6 +358,7 @@ struct MatState {
   long offset = 0;         // first slot (element) of this material in r_e
   std::vector<double> grad_u, grad_u_prev, stress, stress_prev, pk2;
   std::vector<double> eps_p, eps_p_prev, iso, iso_prev, pe;
+  std::vector<double> c33;  // plane-stress neohookean out-of-plane stretch, initially 1
 };
 
 }  // namespace
@@ -403,6 +404,8 @@ void assign_materials(or_model *m) {
     s.stress.assign(nqp * dd, 0.);
     s.stress_prev.assign(nqp * dd, 0.);
     if (m->mats[k].finite()) s.pk2.assign(nqp * dd, 0.);
+    if (m->mats[k].law == OR_NEOHOOKEAN && m->mats[k].plane_stress && m->d == 2)
+      s.c33.assign(nqp, 1.);
     if (m->mats[k].law == OR_PLASTIC) {
       s.eps_p.assign(nqp * dd, 0.);
       s.eps_p_prev.assign(nqp * dd, 0.);
@@ -551,6 +554,23 @@ parallel_for(ne, m->threads, [&](long le) {
           double Egl[9];
           green_lagrange(d, g, Egl);
           elastic(d, mat.lambda, mat.mu, Egl, mat.sigma_th, S);
+        } else if (!s.c33.empty()) {
+          // plane stress: C33 by Newton iterations from the stored value on
+          // f(x) = lambda/2 (log x + log(C00 C11 - C01^2)) + mu (x - 1)
+          // (material_neohookean_inline_impl.hh:52-92, aka_math_tmpl.hh:191-208),
+          // then J = det F sqrt(C33)
+          const double F00 = 1. + g[0], F10 = g[1], F01 = g[2], F11 = 1. + g[3];
+          const double C00 = F00 * F00 + F10 * F10, C11 = F01 * F01 + F11 * F11;
+          const double C01 = F00 * F01 + F10 * F11;
+          const double lc = std::log(C00 * C11 - C01 * C01);
+          double x = s.c33[qp];
+          double fx = mat.lambda / 2. * (std::log(x) + lc) + mat.mu * (x - 1.);
+          for (int it = 0; std::fabs(fx) > 1e-5 && it < 100; ++it) {
+            x -= fx / (mat.lambda / (2. * x) + mat.mu);
+            fx = mat.lambda / 2. * (std::log(x) + lc) + mat.mu * (x - 1.);
+          }
+          s.c33[qp] = x;
+          neohookean(d, mat.lambda, mat.mu, g, x, S);
         } else {
           neohookean(d, mat.lambda, mat.mu, g, 1., S);
         }

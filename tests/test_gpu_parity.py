@@ -424,3 +424,51 @@ def test_finite_deformation_elastic_shares_the_finite_strain_launch():
     for k in range(2):
         assert np.array_equal(g.getMaterial(k).getInternal("piola_kirchhoff_2")(),
                               o.qp(k, orc.PK2)) or k == 0
+
+
+@pytest.mark.parametrize("kind", ["tet_cube_48k", "hex8_neohookean_16"])
+def test_mixed_precision_error_after_ten_thousand_steps(kind):
+    """FP32 element math with FP64 state against the plain FP64 path after
+    10^4 steps: relative L2 displacement <= 1e-5, and both paths conserve the
+    total energy of the free vibration to the same degree"""
+    if kind == "tet_cube_48k":
+        mesh, mat = akb.box_tet4(20), UNIT_ELASTIC
+        v0 = sinusoidal_velocity(mesh.nodes)
+    else:
+        mesh, mat = akb.box_hex8(16), UNIT_NEOHOOKEAN
+        v0 = random_field_velocity(mesh.nodes, seed=2024)
+    bl = blocked_face(mesh.nodes)
+    res = {}
+    for prec in ("mixed", "fp64"):
+        m = gpu_model(mesh, [mat], precision=prec)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        e0 = m.getEnergy("kinetic") + m.getEnergy("potential")
+        m.solveStep(10000)
+        e1 = m.getEnergy("kinetic") + m.getEnergy("potential")
+        res[prec] = (m.getDisplacement(), (e1 - e0) / e0)
+    u, ud = res["mixed"][0], res["fp64"][0]
+    assert np.linalg.norm(u - ud) / np.linalg.norm(ud) < 1e-5
+    assert abs(res["mixed"][1] - res["fp64"][1]) < 1e-6
+
+
+def test_plane_stress_neohookean_parity():
+    """plane-stress neohookean on _triangle_6: the per-point C33 Newton solve
+    (state carried between steps) against the oracle"""
+    mesh = akb.square_tri6(6)
+    x = mesh.nodes
+    mat = dict(UNIT_NEOHOOKEAN, Plane_Stress=True)
+    v0 = np.stack([0.2 * x[:, 0], -0.05 * x[:, 0] * x[:, 1]], axis=1)
+    bl = blocked_face(x, axis=0)
+    g, o = setup_pair(mesh, [mat], v0, bl)
+    g.solveStep(80)
+    o.step(80)
+    errs = compare(g, o, exact=False)
+    assert max(errs.values()) <= 1e-12
+    pk2, opk2 = g.getMaterial(0).getInternal("piola_kirchhoff_2")(), o.qp(0, orc.PK2)
+    assert np.max(np.abs(pk2 - opk2)) <= 1e-12 * np.max(np.abs(opk2))
+    gm, _ = setup_pair(mesh, [mat], v0, bl, precision="mixed")
+    gm.solveStep(80)
+    uo = o.get(orc.U)
+    assert np.linalg.norm(gm.getDisplacement() - uo) / np.linalg.norm(uo) < 1e-5

@@ -83,7 +83,6 @@ def test_dat_parser_reads_materials_and_expressions():
     ("material elastic [ E = abc ]", 6),
     ("material elastic [ Youngs = 1 ]", 6),
     ("material plastic_linear_isotropic_hardening [ E = 1\n finite_deformation = true ]", 8),
-    ("material neohookean [ E = 1\n Plane_Stress = true ]", 8),
 ])
 def test_dat_parser_errors(text, code):
     _, m = _tiny_model()

@@ -286,3 +286,27 @@ def test_finite_deformation_elastic_oracle_limits():
     ol.assemble_internal_forces()
     f, fl = o.get(orc.FINT), ol.get(orc.FINT)
     assert np.max(np.abs(f - fl)) <= 1e-6 * np.max(np.abs(fl))
+
+
+def test_plane_stress_neohookean_out_of_plane_solve():
+    """plane-stress neohookean: C33 starts at 1 and is only corrected when the
+    out-of-plane residual exceeds the Newton tolerance 1e-5 (the reference's
+    absolute tolerance), so a tiny strain gives exactly the plane-strain
+    forces; a finite strain relaxes the out-of-plane stress and gives a
+    softer in-plane response"""
+    from akantu2_b200 import square_tri6
+    mesh = square_tri6(2)
+    x = mesh.nodes
+    nh_ps = dict(type="neohookean", rho=1.0, E=1.0, nu=0.3, Plane_Stress=True)
+    nh_pe = dict(type="neohookean", rho=1.0, E=1.0, nu=0.3)
+
+    def forces(mat, eps):
+        o = orc.OracleModel(orc.TRI6, x, mesh.connectivity, [mat])
+        o.set(orc.U, x @ eps.T)
+        o.assemble_internal_forces()
+        return o.get(orc.FINT)
+    tiny = 1e-7 * np.array([[1.0, 0.3], [0.2, -0.5]])
+    assert np.array_equal(forces(nh_ps, tiny), forces(nh_pe, tiny))
+    stretch = np.array([[2e-2, 0.0], [0.0, 2e-2]])
+    fps, fpe = forces(nh_ps, stretch), forces(nh_pe, stretch)
+    assert np.linalg.norm(fps) < 0.9 * np.linalg.norm(fpe)
