@@ -1482,6 +1482,19 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   return AKB_OK;
 }
 
+int akb_model_apply_neumann_stress(akb_model *m, const int32_t *group_nodes, int64_t count,
+                                   const double *stress) {
+  AKB_TRY(check_model(m, true));
+  const int64_t nd = nodal_doubles(m);
+  std::vector<double> f(nd);
+  AKB_CUDA(cudaMemcpyAsync(f.data(), m->dfext, sizeof(double) * nd, cudaMemcpyDeviceToHost,
+                           m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  AKB_TRY(akb_mesh_neumann_forces(m->et, m->X.data(), m->N, m->conn.data(), m->E, group_nodes,
+                                  count, stress, f.data()));
+  return akb_model_set_nodal(m, AKB_EXTERNAL_FORCE, f.data(), nd * (int64_t)sizeof(double));
+}
+
 int akb_model_set_prescribed_velocity_ramp(akb_model *m, const int64_t *dofs, int64_t count,
                                            double v_max, int64_t ramp_steps) {
   AKB_TRY(check_model(m, true));

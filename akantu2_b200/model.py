@@ -66,6 +66,29 @@ class FixedValue:
         self.axis = axis
 
 
+class FromHigherDim:
+    """BC::Neumann::FromHigherDim(stress): the traction stress . n on the
+    boundary facets of a group (boundary_condition_functor.hh)."""
+
+    def __init__(self, stress):
+        self.stress = np.asarray(stress, dtype=np.float64)
+
+
+def neumann_forces(mesh, group_nodes, stress):
+    """Nodal forces [N, dim] of FromHigherDim(stress) on the boundary facets
+    whose nodes all belong to group_nodes (akb_mesh_neumann_forces)."""
+    d = mesh.spatial_dimension
+    nodes = np.ascontiguousarray(group_nodes, dtype=np.int32)
+    sig = np.asfortranarray(np.asarray(stress, dtype=np.float64).reshape(d, d))
+    sig_cm = np.ascontiguousarray(sig.T).reshape(-1)  # column-major
+    out = np.zeros((mesh.getNbNodes(), d))
+    _capi.check(_capi.lib().akb_mesh_neumann_forces(
+        TYPE_IDS[mesh.element_type], _capi.ptr(mesh.nodes), mesh.getNbNodes(),
+        _capi.ptr(mesh.connectivity), mesh.getNbElement(), _capi.ptr(nodes), nodes.size,
+        _capi.ptr(sig_cm), _capi.ptr(out)))
+    return out
+
+
 class Material:
     """View of one material of a model (src/model/solid_mechanics/material.hh)."""
 
@@ -241,10 +264,15 @@ class SolidMechanicsModel:
 
     def applyBC(self, bc, group):
         """applyBC(FixedValue(v, axis), group): blocks the axis of the group's
-        nodes and sets their displacement (boundary_condition_tmpl.hh)."""
+        nodes and sets their displacement; applyBC(FromHigherDim(stress),
+        group): adds the boundary traction to the external force
+        (boundary_condition_tmpl.hh)."""
         nodes = self.mesh.getNodeGroup(group) if isinstance(group, str) else np.asarray(group)
+        if isinstance(bc, FromHigherDim):
+            self.getExternalForce()[:] += neumann_forces(self.mesh, nodes, bc.stress)
+            return
         if not isinstance(bc, FixedValue):
-            raise TypeError("only BC::Dirichlet::FixedValue is provided")
+            raise TypeError("applyBC takes FixedValue or FromHigherDim")
         self.getBlockedDOFs()[nodes, bc.axis] = True
         self.getDisplacement()[nodes, bc.axis] = bc.value
 

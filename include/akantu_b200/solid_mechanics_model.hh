@@ -219,6 +219,14 @@ struct FixedValue {
   SpatialDirection axis;
 };
 }  // namespace Dirichlet
+namespace Neumann {
+// BC::Neumann::FromHigherDim(stress): traction stress . n on the group's
+// boundary facets, added to the external force (boundary_condition_tmpl.hh:100-164)
+struct FromHigherDim {
+  explicit FromHigherDim(const Array<Real> &stress_dim_x_dim) : stress(stress_dim_x_dim) {}
+  Array<Real> stress;  // (i, j) = stress_ij
+};
+}  // namespace Neumann
 }  // namespace BC
 
 class SolidMechanicsModel;
@@ -319,6 +327,17 @@ public:
       blocked(n, bc.axis) = true;
       u(n, bc.axis) = bc.value;
     }
+  }
+
+  // applyBC(BC::Neumann::FromHigherDim(stress), group)
+  void applyBC(const BC::Neumann::FromHigherDim &bc, const ID &group) {
+    syncUp();
+    std::vector<int32_t> nodes(mesh_.getNodeGroup(group).begin(), mesh_.getNodeGroup(group).end());
+    std::vector<Real> sig((size_t)dim_ * dim_);
+    for (Int i = 0; i < dim_; ++i)
+      for (Int j = 0; j < dim_; ++j) sig[i + dim_ * j] = bc.stress(i, j);  // column-major
+    check(akb_model_apply_neumann_stress(h_, nodes.data(), (int64_t)nodes.size(), sig.data()));
+    mirrors_.erase(AKB_EXTERNAL_FORCE);
   }
 
   void assembleInternalForces() {

@@ -181,6 +181,18 @@ int akb_model_get_qp_field(akb_model *model, int field, int material, double *ho
  * available for batches. */
 int akb_model_set_prescribed_velocity_ramp(akb_model *model, const int64_t *dofs,
                                            int64_t count, double v_max, int64_t ramp_steps);
+/* BC::Neumann::FromHigherDim(stress) on a node group (boundary_condition_tmpl.hh:100-164):
+ * the traction stress * n is integrated over every boundary facet whose nodes
+ * all belong to the group (n the outward normal) and added to forces
+ * [N][dim] (host arithmetic, no device needed).  stress: dim x dim,
+ * column-major. */
+int akb_mesh_neumann_forces(int element_type, const double *nodes, int64_t nb_nodes,
+                            const int32_t *connectivity, int64_t nb_elements,
+                            const int32_t *group_nodes, int64_t count, const double *stress,
+                            double *forces);
+/* the same added to the model's external force */
+int akb_model_apply_neumann_stress(akb_model *model, const int32_t *group_nodes, int64_t count,
+                                   const double *stress);
 /* ModelSolver::solveStep  model_solver.cc:267-280: enqueues nsteps explicit
  * steps on the model's stream (asynchronous; getters synchronise) */
 int akb_model_solve_step(akb_model *model, int64_t nsteps);

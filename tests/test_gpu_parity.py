@@ -472,3 +472,17 @@ def test_plane_stress_neohookean_parity():
     gm.solveStep(80)
     uo = o.get(orc.U)
     assert np.linalg.norm(gm.getDisplacement() - uo) / np.linalg.norm(uo) < 1e-5
+
+
+def test_neumann_stress_adds_to_external_force():
+    mesh = akb.box_hex8(3)
+    g = gpu_model(mesh, [UNIT_ELASTIC])
+    sigma = np.array([[1e-3, 2e-4, 0.0], [2e-4, -5e-4, 1e-4], [0.0, 1e-4, 3e-4]])
+    top = np.nonzero(np.isclose(mesh.nodes[:, 2], 1.0))[0]
+    g.getExternalForce()[:] = 1.0
+    g.applyBC(akb.FromHigherDim(sigma), top)
+    g.solveStep(0)
+    expected = 1.0 + akb.neumann_forces(mesh, top, sigma)
+    assert np.array_equal(g.getExternalForce(), expected)
+    # the top face's normal is +z: the resultant is the third column times the area
+    assert np.allclose((expected - 1.0).sum(axis=0), sigma[:, 2], rtol=1e-12, atol=1e-15)

@@ -310,3 +310,25 @@ def test_plane_stress_neohookean_out_of_plane_solve():
     stretch = np.array([[2e-2, 0.0], [0.0, 2e-2]])
     fps, fpe = forces(nh_ps, stretch), forces(nh_pe, stretch)
     assert np.linalg.norm(fps) < 0.9 * np.linalg.norm(fpe)
+
+
+@pytest.mark.parametrize("etype", TYPES)
+def test_neumann_traction_balances_internal_force(etype):
+    """BC::Neumann::FromHigherDim with the patch field's stress on the whole
+    boundary balances the internal force of that field at every node
+    (patch_test_linear_solid_mechanics_fixture.hh: checkForces)"""
+    from akantu2_b200 import neumann_forces
+    mesh = _patch_mesh(etype)
+    d = mesh.spatial_dimension
+    o = orc.OracleModel(OR_TYPE[etype], mesh.nodes, mesh.connectivity, [STEEL_PLANE_STRAIN])
+    o.set(orc.U, linear_field(mesh.nodes))
+    o.assemble_internal_forces()
+    sigma = o.qp(0, orc.STRESS)[0].reshape(d, d, order="F")
+    boundary = boundary_nodes(etype, mesh.connectivity)
+    fext = neumann_forces(mesh, boundary, sigma)
+    fint = o.get(orc.FINT)
+    scale = np.max(np.abs(fext))
+    assert scale > 0
+    assert np.max(np.abs(fint + fext)) <= 1e-9 * scale
+    # resultant of a uniform stress over a closed boundary is zero
+    assert np.max(np.abs(fext.sum(axis=0))) <= 1e-9 * scale
