@@ -52,6 +52,21 @@ inline unsigned grid_for(int64_t n, int threads = kThreads) {
     }                                                                     \
   } while (0)
 
+// threads per block of the staged node update: 128, 256 or 512
+#define AKB_DISPATCH_NODE_BLOCK(b, ...)                                  \
+  do {                                                                    \
+    if ((b) <= 128) {                                                     \
+      constexpr int NB = 128;                                             \
+      __VA_ARGS__;                                                        \
+    } else if ((b) <= 256) {                                              \
+      constexpr int NB = 256;                                             \
+      __VA_ARGS__;                                                        \
+    } else {                                                              \
+      constexpr int NB = 512;                                             \
+      __VA_ARGS__;                                                        \
+    }                                                                     \
+  } while (0)
+
 // cooperative launch of a persistent step kernel: as many blocks as fit on
 // the device at once (all resident, so the grid barrier can complete), fewer
 // when the mesh needs fewer

@@ -918,6 +918,32 @@ __global__ void __launch_bounds__(32 * NQ)
 // KAHAN selects a compensated FP64 sum (mixed path).
 enum { NU_CORRECT = 1, NU_PREDICT = 2, NU_FINT = 4, NU_FEXT_ZERO = 8 };
 
+// one slot into the internal-force sum, sign -1 (dof_manager.cc:65-120),
+// optionally compensated
+template <int D, bool KAHAN>
+__device__ __forceinline__ void accumulate_slot(const double *rv, double *acc, double *comp) {
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const double val = -1. * rv[c];
+    if constexpr (KAHAN) {
+      const double y = val - comp[c];
+      const double tt = acc[c] + y;
+      comp[c] = (tt - acc[c]) - y;
+      acc[c] = tt;
+    } else {
+      acc[c] = acc[c] + val;
+    }
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void node_apply(int64_t i, const double *acc, const double *fext,
+                                           const double *mass, const uint8_t *blocked,
+                                           double *fint, double *a, double *v, const double *u,
+                                           double *u_next, double dt, const int32_t *node_inst,
+                                           const double *inst_dt, int flags,
+                                           unsigned int *status);
+
 template <int D, class RT, bool KAHAN>
 __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
                                           const RT *re,
@@ -941,19 +967,21 @@ __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
   for (int32_t p = p0; p < p1; ++p) {
     double rv[D];
     load_slot<D>(re, p, rv);
-#pragma unroll
-    for (int c = 0; c < D; ++c) {
-      const double val = -1. * rv[c];
-      if constexpr (KAHAN) {
-        const double y = val - comp[c];
-        const double tt = acc[c] + y;
-        comp[c] = (tt - acc[c]) - y;
-        acc[c] = tt;
-      } else {
-        acc[c] = acc[c] + val;
-      }
-    }
+    accumulate_slot<D, KAHAN>(rv, acc, comp);
   }
+  node_apply<D>(i, acc, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst, inst_dt, flags,
+                status);
+}
+
+// the node update after the gather: f_int = acc, residual, solve, corrector
+// and predictor of node i
+template <int D>
+__device__ __forceinline__ void node_apply(int64_t i, const double *acc, const double *fext,
+                                           const double *mass, const uint8_t *blocked,
+                                           double *fint, double *a, double *v, const double *u,
+                                           double *u_next, double dt, const int32_t *node_inst,
+                                           const double *inst_dt, int flags,
+                                           unsigned int *status) {
   if (flags & NU_FINT) {
 #pragma unroll
     for (int c = 0; c < D; ++c) fint[i * D + c] = acc[c];
@@ -1011,6 +1039,78 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
   if (i >= N) return;
   node_body<D, RT, KAHAN>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst,
                           inst_dt, flags, status);
+}
+
+// Node update with the gather staged through shared memory: the slots of
+// BLOCK consecutive nodes are one contiguous range of the slot array, loaded
+// in chunks with coalesced vector loads (the direct form makes each thread
+// read its own node's slots, which a warp spreads over 32 separate ranges);
+// each thread then sums its node's slots from shared memory in the same order
+// as the direct form, so the results are identical.  Slot vectors are stored
+// at an XOR-swizzled index so that threads reading ranges a multiple of 8
+// vectors apart hit different banks.
+template <int D, class RT> struct SlotVec;
+template <> struct SlotVec<3, float> { using type = float4; static constexpr int per_slot = 1; };
+template <> struct SlotVec<2, float> { using type = float2; static constexpr int per_slot = 1; };
+template <> struct SlotVec<2, double> { using type = double2; static constexpr int per_slot = 1; };
+template <> struct SlotVec<3, double> { using type = double; static constexpr int per_slot = 3; };
+
+constexpr int kStagedBytes = 32768;
+
+__device__ __forceinline__ int swizzle(int w) { return w ^ ((w >> 3) & 7); }
+
+template <int D, class RT, bool KAHAN, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+    k_node_update_staged(int64_t N, const int32_t *__restrict__ ptr, const RT *__restrict__ re,
+                         const double *__restrict__ fext, const double *__restrict__ mass,
+                         const uint8_t *__restrict__ blocked, double *__restrict__ fint,
+                         double *__restrict__ a, double *__restrict__ v,
+                         const double *__restrict__ u, double *__restrict__ u_next, double dt,
+                         const int32_t *__restrict__ node_inst,
+                         const double *__restrict__ inst_dt, int flags,
+                         unsigned int *__restrict__ status) {
+  using V = typename SlotVec<D, RT>::type;
+  constexpr int WPS = SlotVec<D, RT>::per_slot;  // vectors per slot
+  constexpr int CAPW = kStagedBytes / (int)sizeof(V);
+  constexpr int CAP = CAPW / WPS;               // slots per chunk
+  __shared__ V sm[CAPW];
+  const int64_t i0 = (int64_t)blockIdx.x * BLOCK;
+  const int64_t i = i0 + threadIdx.x;
+  const int64_t iend = i0 + BLOCK < N ? i0 + BLOCK : N;
+  const int32_t pb = ptr[i0], pe = ptr[iend];
+  const int32_t p0 = i < N ? ptr[i] : pe, p1 = i < N ? ptr[i + 1] : pe;
+  const V *src = reinterpret_cast<const V *>(re);
+  double acc[D], comp[D];
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    acc[c] = 0.;
+    comp[c] = 0.;
+  }
+  for (int32_t cb = pb; cb < pe; cb += CAP) {
+    const int32_t ce = cb + CAP < pe ? cb + CAP : pe;
+    __syncthreads();
+    const int nw = (ce - cb) * WPS;
+    for (int w = threadIdx.x; w < nw; w += BLOCK) sm[swizzle(w)] = src[(int64_t)cb * WPS + w];
+    __syncthreads();
+    const int32_t lo = p0 > cb ? p0 : cb, hi = p1 < ce ? p1 : ce;
+    for (int32_t p = lo; p < hi; ++p) {
+      double rv[D];
+      const int w = (p - cb) * WPS;
+      if constexpr (WPS == 1) {
+        const V x = sm[swizzle(w)];
+        rv[0] = (double)x.x;
+        rv[1] = (double)x.y;
+        if constexpr (D == 3) rv[2] = (double)reinterpret_cast<const float4 &>(x).z;
+      } else {
+#pragma unroll
+        for (int c = 0; c < D; ++c) rv[c] = (double)sm[swizzle(w + c)];
+      }
+      accumulate_slot<D, KAHAN>(rv, acc, comp);
+    }
+  }
+  if (i >= N) return;
+  node_apply<D>(i, acc, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst, inst_dt, flags,
+                status);
 }
 
 // ---------------------------------------------------------------------------

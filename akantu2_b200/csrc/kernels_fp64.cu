@@ -122,8 +122,21 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
                                     double dt, int flags, unsigned int *status, int node_block,
-                                    cudaStream_t s) {
+                                    bool staged, cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
+  if (staged) {
+    AKB_DISPATCH_NODE_BLOCK(node_block, {
+      if (g.D == 3)
+        k_node_update_staged<3, double, false, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
+            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
+            g.inst_dt, flags, status);
+      else
+        k_node_update_staged<2, double, false, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
+            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
+            g.inst_dt, flags, status);
+    });
+    return cudaGetLastError();
+  }
   if (g.D == 3)
     k_node_update<3, double, false><<<grid_for(g.N, node_block), node_block, 0, s>>>(
         g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,

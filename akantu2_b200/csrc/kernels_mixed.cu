@@ -55,7 +55,9 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
                                         const MatParams &mp, const GroupArgs &ps,
                                         float *re, const ElemTuning &tn, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
-  if (g.D == 2)
+  // 2D elements and tetrahedra stream the FP32 copies of dN/dx (tetrahedra:
+  // unless the recomputed form is selected, points_per_iteration 0)
+  if (g.D == 2 || (g.et == ET_TET4 && fB && tn.qu != 0))
     return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, tn, s);
   if (g.et == ET_HEX8 && tn.qu > 0) {
     if (law == LAW_ELASTIC)
@@ -89,8 +91,11 @@ template <int LAW>
 cudaError_t persistent_mixed_law(const DevGeom &g, int qu, const StepArgs &sa,
                                  const QuadTable &tab, cudaStream_t s) {
   const int64_t work = std::max(g.E, g.N);
-  if (g.et == ET_TET4)
+  if (g.et == ET_TET4 && qu == 0)
     return launch_cooperative(k_persistent_steps<3, 4, 1, LAW, 1, float, float, true, 1>, work,
+                              sa, tab, s);
+  if (g.et == ET_TET4)
+    return launch_cooperative(k_persistent_steps<3, 4, 1, LAW, 0, float, float, true, 1>, work,
                               sa, tab, s);
   if (g.et == ET_HEX8 && qu == 1)
     return launch_cooperative(k_persistent_steps<3, 8, 8, LAW, 2, float, float, true, 1>, work,
@@ -117,8 +122,22 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,
                                      double *u_next, double dt, int flags,
-                                     unsigned int *status, int node_block, cudaStream_t s) {
+                                     unsigned int *status, int node_block, bool staged,
+                                     cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
+  if (staged) {
+    AKB_DISPATCH_NODE_BLOCK(node_block, {
+      if (g.D == 3)
+        k_node_update_staged<3, float, true, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
+            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
+            g.inst_dt, flags, status);
+      else
+        k_node_update_staged<2, float, true, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
+            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
+            g.inst_dt, flags, status);
+    });
+    return cudaGetLastError();
+  }
   if (g.D == 3)
     k_node_update<3, float, true><<<grid_for(g.N, node_block), node_block, 0, s>>>(
         g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,

@@ -78,17 +78,20 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
                                         float *re, const ElemTuning &tn, cudaStream_t s);
 // flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
 // the predictor of the next step reads u and writes u_next
-// node_block: threads per block of the node update (any multiple of 32 up to 1024)
+// node_block: threads per block of the node update (any multiple of 32 up to
+// 1024; 128, 256 or 512 when staged); staged: the gather goes through shared
+// memory (k_node_update_staged, same arithmetic)
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
                                     double dt, int flags, unsigned int *status, int node_block,
-                                    cudaStream_t s);
+                                    bool staged, cudaStream_t s);
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,
                                      double *u_next, double dt, int flags,
-                                     unsigned int *status, int node_block, cudaStream_t s);
+                                     unsigned int *status, int node_block, bool staged,
+                                     cudaStream_t s);
 
 // prescribed velocity ramp on a set of dofs (u indices node * D + c), written
 // into the displacement the next step starts from; acc and step live on the

@@ -246,6 +246,7 @@ struct akb_model {
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
   int node_block = 128;       // threads per block of the node update
+  bool node_staged = false;   // gather staged through shared memory
   // persistent multi-step kernel: 0 never (default: on B200 the 100-step
   // graphs of the two-kernel step are faster at every measured size), 1 for
   // small single-group meshes, 2 whenever the model allows it
@@ -446,11 +447,11 @@ int node_update(akb_model *m, bool correct) {
   if (m->precision == AKB_PRECISION_MIXED)
     e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass, m->dblocked,
                                  m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
-                                 m->node_block, m->stream);
+                                 m->node_block, m->node_staged, m->stream);
   else
     e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass, m->dblocked,
                                 m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
-                                m->node_block, m->stream);
+                                m->node_block, m->node_staged, m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
   if (correct) AKB_TRY(prescribe(m, u_next));
   m->fint_valid = !correct;
@@ -992,7 +993,10 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   for (auto &mt : m->mats)
     AKB_CUDA(launch_mass_elem(g, mt.e_begin, mt.e_count, mt.rho, tab, m->dwJ, me, s));
   AKB_CUDA(launch_gather_scalar(g, me, m->dmass, s));
-  if (precision == AKB_PRECISION_MIXED && d == 2) {
+  // FP32 copies of dN/dx and det J w: streamed by the mixed kernels of 2D
+  // elements and tetrahedra (a copy of the FP64 values, rounded once, is both
+  // as fast as recomputing the geometry in FP32 and more accurate)
+  if (precision == AKB_PRECISION_MIXED && (d == 2 || m->et == AKB_TETRAHEDRON_4)) {
     AKB_TRY(m->alloc(&m->fB, sizeof(float) * E * nq * nn * d));
     AKB_TRY(m->alloc(&m->fwJ, sizeof(float) * E * nq));
     AKB_CUDA(launch_to_float(m->dB, m->fB, E * nq * nn * d, s));
@@ -1473,7 +1477,8 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   t += r(std::max(re_bytes, 8 * E * nn));
   t += r(8 * std::max<int64_t>(std::max(E, N), 1)) + 8 * kReducePartials + 4 * 16;
   t += 4 * kBarrierWords;
-  if (precision == AKB_PRECISION_MIXED && d == 2) t += r(4 * E * nq * nn * d) + r(4 * E * nq);
+  if (precision == AKB_PRECISION_MIXED && (d == 2 || et == AKB_TETRAHEDRON_4))
+    t += r(4 * E * nq * nn * d) + r(4 * E * nq);
   const int64_t gs = precision == AKB_PRECISION_MIXED ? 4 : 8, ns = sym_comps((int)d);
   if (law == LAW_PLASTIC)
     t += 2 * (2 * r(8 * E * nq * ns) + r(gs * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
@@ -1629,7 +1634,8 @@ int akb_model_autotune(akb_model *m, int repeats) {
       if (q != 1) cand.insert(cand.end(), {{64, q, 1}, {256, q, 1}});
       if (q == 0) cand = {{128, 0, 1}, {64, 0, 1}, {256, 0, 1}};
     } else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64)) {
-      cand = {{64, 8}, {128, 8}, {256, 8}};
+      const int q = gr.tune.qu;
+      cand = {{64, q, 1}, {128, q, 1}, {256, q, 1}};
     }
     float best = 0.f;
     for (size_t k = 0; k < cand.size() && rc == AKB_OK; ++k) {
@@ -1645,23 +1651,26 @@ int akb_model_autotune(akb_model *m, int repeats) {
     const int flags = NU_CORRECT | NU_PREDICT | (m->fext_zero ? NU_FEXT_ZERO : 0);
     check(cudaMemcpyAsync(t_a, m->da, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "copy");
     check(cudaMemcpyAsync(t_v, m->dv, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "copy");
-    const int blocks[4] = {128, 256, 512, 1024};
+    // direct gather with 128 .. 1024 threads, staged gather with 128 .. 512
+    const int blocks[7] = {128, 256, 512, 1024, 128, 256, 512};
     float best = 0.f;
-    for (int k = 0; k < 4 && rc == AKB_OK; ++k) {
+    for (int k = 0; k < 7 && rc == AKB_OK; ++k) {
       float ms = 0.f;
+      const bool staged = k >= 4;
       auto launch = [&]() {
         if (m->precision == AKB_PRECISION_MIXED)
           return launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass,
                                           m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
-                                          flags, t_status, blocks[k], s);
+                                          flags, t_status, blocks[k], staged, s);
         return launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass,
                                        m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
-                                       flags, t_status, blocks[k], s);
+                                       flags, t_status, blocks[k], staged, s);
       };
       if (!time_it(launch, &ms)) break;
       if (k == 0 || ms < best) {
         best = ms;
         m->node_block = blocks[k];
+        m->node_staged = staged;
       }
     }
   }
@@ -1678,6 +1687,27 @@ int akb_model_autotune(akb_model *m, int repeats) {
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
   return rc;
+}
+
+int akb_model_set_node_shape(akb_model *m, int node_block, int staged) {
+  AKB_TRY(check_model(m, true));
+  if (staged && node_block != 128 && node_block != 256 && node_block != 512)
+    return fail(AKB_EINVAL, "the staged gather runs with 128, 256 or 512 threads");
+  if (node_block < 32 || node_block > 1024 || node_block % 32)
+    return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  m->node_block = node_block;
+  m->node_staged = staged != 0;
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_get_node_shape(const akb_model *m, int *node_block, int *staged) {
+  if (!m || !node_block || !staged) return fail(AKB_EINVAL, "null argument");
+  *node_block = m->node_block;
+  *staged = m->node_staged ? 1 : 0;
+  return AKB_OK;
 }
 
 int akb_model_get_launch_shape(const akb_model *m, int law, int *element_block,
@@ -1702,8 +1732,10 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
     return fail(AKB_EINVAL, "element_block must be 64, 128 or 256");
   const int q = points_per_iteration;
   const bool sf = m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED;
-  if (!sf && q != 8)
-    return fail(AKB_EINVAL, "points_per_iteration is 8 except for mixed-precision hexahedra");
+  const bool tet_mixed = m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_MIXED;
+  if (!sf && q != 8 && !(tet_mixed && q == 0))
+    return fail(AKB_EINVAL, "points_per_iteration is 8 (or 0 for the recomputed form of mixed "
+                            "tetrahedra and hexahedra)");
   if (sf && q != 0 && q != 1 && q != 2 && q != 8)
     return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
   if (sf && q == 1 && element_block != 128)

@@ -386,6 +386,16 @@ class SolidMechanicsModel:
                                                            int(points_per_iteration),
                                                            int(min_blocks), int(node_block)))
 
+    def setNodeShape(self, node_block, staged=False):
+        """Threads per block of the node update, and the staged (shared
+        memory) gather; results are unchanged by either."""
+        _capi.check(_capi.lib().akb_model_set_node_shape(self._h, int(node_block), int(staged)))
+
+    def getNodeShape(self):
+        b, st = ctypes.c_int(), ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_node_shape(self._h, ctypes.byref(b), ctypes.byref(st)))
+        return b.value, bool(st.value)
+
     def getDeviceBytes(self):
         """Device memory held by the model."""
         b = ctypes.c_int64()

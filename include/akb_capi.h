@@ -214,7 +214,8 @@ int akb_model_persistent_active(const akb_model *model, int *active);
 /* autotuner: times the candidate launch shapes of each law group's
  * element-force kernel (threads per block 64 / 128 / 256; for mixed
  * hexahedra also a register cap for 5 resident blocks of 128) and of the node
- * update (128 .. 1024 threads per block) on the model's current state,
+ * update (direct gather with 128 .. 1024 threads per block, staged gather
+ * with 128 .. 512) on the model's current state,
  * `repeats` launches each, and keeps the fastest.  The candidates compute
  * the same numbers, so the choice changes only the timing; the model's state
  * is not modified.  Captured step graphs are rebuilt.  The points per
@@ -231,6 +232,11 @@ int akb_model_get_launch_shape(const akb_model *model, int law, int *element_blo
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
                                int points_per_iteration, int min_blocks, int node_block);
+/* node update shape: threads per block, and staged = 1 to stage each block's
+ * slot range through shared memory (coalesced loads; 128, 256 or 512
+ * threads).  Both forms sum every node's slots in the same order. */
+int akb_model_set_node_shape(akb_model *model, int node_block, int staged);
+int akb_model_get_node_shape(const akb_model *model, int *node_block, int *staged);
 /* captures the graph that the next solve_step will launch (and enqueues the
  * predictor it starts from), so that the capture cost is not paid inside the
  * first solve_step; optional */

@@ -171,3 +171,33 @@ def test_persistent_batch_with_instance_time_steps():
         outs.append((b.getDisplacement().copy(), b.getVelocity().copy()))
     for a, c in zip(*outs):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("etype,precision,mat", [
+    ("_tetrahedron_4", "mixed", UNIT_ELASTIC), ("_tetrahedron_4", "fp64", UNIT_ELASTIC),
+    ("_hexahedron_8", "mixed", UNIT_NEOHOOKEAN), ("_hexahedron_8", "fp64", UNIT_ELASTIC),
+    ("_triangle_6", "mixed", UNIT_PLASTIC), ("_triangle_6", "fp64", UNIT_PLASTIC)])
+def test_staged_node_gather_is_bit_identical(etype, precision, mat):
+    """the shared-memory staged gather sums every node's slots in the order of
+    the direct gather: identical states, for every block size (small chunks
+    are exercised by the 512-thread blocks of tetrahedra, 24 slots a node)"""
+    mesh = {"_hexahedron_8": lambda: akb.box_hex8(6), "_triangle_6": lambda: akb.square_tri6(8),
+            "_tetrahedron_4": lambda: akb.box_tet4(8)}[etype]()
+    d = mesh.spatial_dimension
+    v0 = sinusoidal_velocity(mesh.nodes, 0.03) if d == 3 else \
+        np.stack([0.02 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
+    bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
+    runs = []
+    for shape in [(128, False), (128, True), (256, True), (512, True)]:
+        m = gpu_model(mesh, [mat], precision=precision)
+        m.setNodeShape(*shape)
+        assert m.getNodeShape() == shape
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.solveStep(123)
+        runs.append((m.getDisplacement().copy(), m.getVelocity().copy(),
+                     m.getInternalForce().copy()))
+    for other in runs[1:]:
+        for a, b in zip(runs[0], other):
+            assert np.array_equal(a, b)
