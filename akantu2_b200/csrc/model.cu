@@ -283,9 +283,26 @@ struct akb_model {
     return AKB_OK;
   }
   size_t device_bytes = 0;
+  // asynchronous nodal I/O: copy streams, double-buffered device staging and
+  // the events that order them against the step stream
+  struct AsyncIO {
+    cudaStream_t in = nullptr, out = nullptr;
+    double *stage_in[2] = {nullptr, nullptr}, *stage_out[2] = {nullptr, nullptr};
+    cudaEvent_t in_ready[2] = {nullptr, nullptr}, in_used[2] = {nullptr, nullptr};
+    cudaEvent_t out_ready[2] = {nullptr, nullptr}, out_done[2] = {nullptr, nullptr};
+    int in_k = 0;
+    int64_t out_tickets = 0;  // copies issued so far
+  } aio;
   ~akb_model() {
+    if (aio.in) cudaStreamSynchronize(aio.in);
+    if (aio.out) cudaStreamSynchronize(aio.out);
     for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
     for (void *p : allocs) cudaFreeAsync(p, stream);
+    for (int k = 0; k < 2; ++k)
+      for (cudaEvent_t e : {aio.in_ready[k], aio.in_used[k], aio.out_ready[k], aio.out_done[k]})
+        if (e) cudaEventDestroy(e);
+    if (aio.in) cudaStreamDestroy(aio.in);
+    if (aio.out) cudaStreamDestroy(aio.out);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1823,6 +1840,101 @@ int akb_model_profile_steps(akb_model *m, int64_t nsteps, double *total_ms, doub
 int akb_model_synchronize(akb_model *m) {
   AKB_TRY(check_model(m, true));
   AKB_CUDA(cudaStreamSynchronize(m->stream));
+  if (m->aio.in) AKB_CUDA(cudaStreamSynchronize(m->aio.in));
+  if (m->aio.out) AKB_CUDA(cudaStreamSynchronize(m->aio.out));
+  return AKB_OK;
+}
+
+namespace {
+int ensure_async_io(akb_model *m) {
+  auto &io = m->aio;
+  if (io.in) return AKB_OK;
+  const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(nodal_doubles(m), 1);
+  for (int k = 0; k < 2; ++k) {
+    AKB_TRY(m->alloc(&io.stage_in[k], bytes));
+    AKB_TRY(m->alloc(&io.stage_out[k], bytes));
+    for (cudaEvent_t *e : {&io.in_ready[k], &io.in_used[k], &io.out_ready[k], &io.out_done[k]})
+      AKB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  AKB_CUDA(cudaStreamSynchronize(m->stream));  // staging allocated before the copy streams use it
+  AKB_CUDA(cudaStreamCreateWithFlags(&io.out, cudaStreamNonBlocking));
+  AKB_CUDA(cudaStreamCreateWithFlags(&io.in, cudaStreamNonBlocking));
+  return AKB_OK;
+}
+}  // namespace
+
+int akb_model_set_nodal_async(akb_model *m, int field, const void *host, int64_t nbytes) {
+  AKB_TRY(check_model(m, true));
+  const int64_t nd = nodal_doubles(m);
+  if (nbytes != nd * (int64_t)sizeof(double)) return fail(AKB_EINVAL, "size must be N*dim doubles");
+  if (!host && nd > 0) return fail(AKB_EINVAL, "null host buffer");
+  double *dst = nullptr;
+  switch (field) {
+  case AKB_DISPLACEMENT:
+    AKB_TRY(snapshot_u(m));
+    dst = m->u();
+    m->predicted = false;
+    break;
+  case AKB_VELOCITY: dst = m->dv; m->predicted = false; break;
+  case AKB_ACCELERATION: dst = m->da; m->predicted = false; break;
+  case AKB_EXTERNAL_FORCE: dst = m->dfext; m->fext_zero = false; break;
+  default: return fail(AKB_EINVAL, "field is read-only or unknown");
+  }
+  AKB_TRY(ensure_async_io(m));
+  auto &io = m->aio;
+  const int k = io.in_k;
+  io.in_k ^= 1;
+  // the staging buffer k is free once the step stream consumed its last upload
+  AKB_CUDA(cudaStreamWaitEvent(io.in, io.in_used[k], 0));
+  AKB_CUDA(cudaMemcpyAsync(io.stage_in[k], host, nbytes, cudaMemcpyHostToDevice, io.in));
+  AKB_CUDA(cudaEventRecord(io.in_ready[k], io.in));
+  AKB_CUDA(cudaStreamWaitEvent(m->stream, io.in_ready[k], 0));
+  AKB_CUDA(cudaMemcpyAsync(dst, io.stage_in[k], nbytes, cudaMemcpyDeviceToDevice, m->stream));
+  AKB_CUDA(cudaEventRecord(io.in_used[k], m->stream));
+  return AKB_OK;
+}
+
+int akb_model_get_nodal_async(akb_model *m, int field, void *host, int64_t nbytes,
+                              int64_t *ticket) {
+  AKB_TRY(check_model(m, true));
+  const int64_t nd = nodal_doubles(m);
+  if (nbytes != nd * (int64_t)sizeof(double)) return fail(AKB_EINVAL, "size must be N*dim doubles");
+  if (!host && nd > 0) return fail(AKB_EINVAL, "null host buffer");
+  const double *src = nullptr;
+  switch (field) {
+  case AKB_DISPLACEMENT: src = m->u(); break;
+  case AKB_VELOCITY: src = m->dv; break;
+  case AKB_ACCELERATION: src = m->da; break;
+  case AKB_EXTERNAL_FORCE: src = m->dfext; break;
+  case AKB_INTERNAL_FORCE:
+    AKB_TRY(ensure_fint(m));
+    src = m->dfint;
+    break;
+  default: return fail(AKB_EINVAL, "field cannot be read asynchronously");
+  }
+  AKB_TRY(ensure_async_io(m));
+  auto &io = m->aio;
+  const int64_t t = io.out_tickets++;
+  const int k = (int)(t & 1);
+  // snapshot on the step stream (the field's buffer is reused by later
+  // steps), then the host copy on the copy stream, overlapping those steps
+  AKB_CUDA(cudaStreamWaitEvent(m->stream, io.out_done[k], 0));
+  AKB_CUDA(cudaMemcpyAsync(io.stage_out[k], src, nbytes, cudaMemcpyDeviceToDevice, m->stream));
+  AKB_CUDA(cudaEventRecord(io.out_ready[k], m->stream));
+  AKB_CUDA(cudaStreamWaitEvent(io.out, io.out_ready[k], 0));
+  AKB_CUDA(cudaMemcpyAsync(host, io.stage_out[k], nbytes, cudaMemcpyDeviceToHost, io.out));
+  AKB_CUDA(cudaEventRecord(io.out_done[k], io.out));
+  if (ticket) *ticket = t;
+  return AKB_OK;
+}
+
+int akb_model_wait_nodal_async(akb_model *m, int64_t ticket) {
+  AKB_TRY(check_model(m, true));
+  auto &io = m->aio;
+  if (ticket < 0 || ticket >= io.out_tickets) return fail(AKB_EINVAL, "unknown ticket");
+  if (ticket < io.out_tickets - 2)
+    return fail(AKB_EINVAL, "ticket older than the two copies in flight: use akb_model_synchronize");
+  AKB_CUDA(cudaEventSynchronize(io.out_done[ticket & 1]));
   return AKB_OK;
 }
 

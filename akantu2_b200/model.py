@@ -255,6 +255,26 @@ class SolidMechanicsModel:
         self._invalidate(["current_position"])
         return self._get("current_position")
 
+    def setNodalAsync(self, name, pinned):
+        """Asynchronous upload of a whole nodal array from a pinned host array
+        (akb_model_set_nodal_async); the array may be reused after the next
+        synchronize()."""
+        self._sync_up()
+        _capi.check(_capi.lib().akb_model_set_nodal_async(self._h, _FIELDS[name], _capi.ptr(pinned),
+                                                          pinned.nbytes))
+        self._invalidate([name, "current_position"])
+
+    def getNodalAsync(self, name, pinned):
+        """Asynchronous read of a nodal array into a pinned host array; returns
+        a ticket for waitNodalAsync (akb_model_get_nodal_async)."""
+        t = ctypes.c_int64()
+        _capi.check(_capi.lib().akb_model_get_nodal_async(self._h, _FIELDS[name], _capi.ptr(pinned),
+                                                          pinned.nbytes, ctypes.byref(t)))
+        return t.value
+
+    def waitNodalAsync(self, ticket):
+        _capi.check(_capi.lib().akb_model_wait_nodal_async(self._h, int(ticket)))
+
     def setNodal(self, name, values):
         """Direct upload of a whole nodal array."""
         self._sync_up()

@@ -469,24 +469,19 @@ def run_ours(args):
             "state_finite": m.getStatus() == 0 and bool(np.all(np.isfinite(m.getDisplacement()))),
         }
         if prec == precisions[0]:
-            # end to end through the C ABI with host buffers
-            from akantu2_b200._capi import PinnedArray
-            L = _capi.lib()
-            fext = PinnedArray(mesh.nodes.shape)
-            fext.array[:] = 0.0
-            uout = PinnedArray(mesh.nodes.shape)
-            nb = fext.array.nbytes
+            # end to end through the C ABI with pinned host buffers
+            nb = int(np.prod(mesh.nodes.shape)) * 8
             k_e2e = max(1, min(args.steps, 100))
-            barrier()
-            t0 = time.perf_counter()
-            for _ in range(k_e2e):
-                _capi.check(L.akb_model_set_nodal(m._h, _capi.EXTERNAL_FORCE, _capi.ptr(fext.array), nb))
-                _capi.check(L.akb_model_solve_step(m._h, 1))
-                _capi.check(L.akb_model_get_nodal(m._h, _capi.DISPLACEMENT, _capi.ptr(uout.array), nb))
-            secs = max_over_ranks(time.perf_counter() - t0)
-            results[prec]["e2e"] = {"value": world * E * k_e2e / secs, "unit": UNIT,
+            secs_sync, secs_async = e2e_legs(m, mesh.nodes.shape, k_e2e, barrier)
+            secs_sync, secs_async = max_over_ranks(secs_sync), max_over_ranks(secs_async)
+            results[prec]["e2e"] = {"value": world * E * k_e2e / secs_async, "unit": UNIT,
                                     "steps": k_e2e, "h2d_bytes_per_step": nb,
-                                    "d2h_bytes_per_step": nb}
+                                    "d2h_bytes_per_step": nb,
+                                    "mode": "pipelined: the external force of every step uploaded "
+                                            "and its displacement read back through the async "
+                                            "C ABI, each result waited for one step later, all "
+                                            "copies complete inside the timed region",
+                                    "synchronous_value": world * E * k_e2e / secs_sync}
         del m
     head = results[precisions[0]]
     accuracy = None
@@ -528,6 +523,47 @@ def run_ours(args):
             line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
         print(json.dumps(line), flush=True)
     rep.close()
+
+
+def e2e_legs(m, shape, k, barrier):
+    """End to end through the C ABI with pinned host buffers, k steps: every
+    step uploads the external force and reads the displacement back.
+    Synchronous: set_nodal / solve_step / get_nodal.  Pipelined: the async
+    forms with two host buffers per direction, the result of step j waited
+    for after step j + 1 is enqueued.  Returns both wall times (seconds)."""
+    from akantu2_b200 import _capi
+    from akantu2_b200._capi import PinnedArray
+    L = _capi.lib()
+    fext = [PinnedArray(shape) for _ in range(2)]
+    uout = [PinnedArray(shape) for _ in range(2)]
+    for f in fext:
+        f.array[:] = 0.0
+    nb = fext[0].array.nbytes
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        _capi.check(L.akb_model_set_nodal(m._h, _capi.EXTERNAL_FORCE, _capi.ptr(fext[0].array), nb))
+        _capi.check(L.akb_model_solve_step(m._h, 1))
+        _capi.check(L.akb_model_get_nodal(m._h, _capi.DISPLACEMENT, _capi.ptr(uout[0].array), nb))
+    secs_sync = time.perf_counter() - t0
+    barrier()
+    t0 = time.perf_counter()
+    import ctypes
+    ticket = ctypes.c_int64()
+    prev = None
+    for j in range(k):
+        _capi.check(L.akb_model_set_nodal_async(m._h, _capi.EXTERNAL_FORCE,
+                                                _capi.ptr(fext[j % 2].array), nb))
+        _capi.check(L.akb_model_solve_step(m._h, 1))
+        _capi.check(L.akb_model_get_nodal_async(m._h, _capi.DISPLACEMENT,
+                                                _capi.ptr(uout[j % 2].array), nb,
+                                                ctypes.byref(ticket)))
+        if prev is not None:
+            _capi.check(L.akb_model_wait_nodal_async(m._h, prev))
+        prev = ticket.value
+    _capi.check(L.akb_model_synchronize(m._h))
+    secs_async = time.perf_counter() - t0
+    return secs_sync, secs_async
 
 
 def accuracy_leg(akb, config, mesh, mat, v0, blocked, nsteps):
@@ -623,23 +659,15 @@ def run_batch(args):
             "state_finite": b.getStatus() == 0 and bool(np.all(np.isfinite(b.getDisplacement()))),
         }
         if prec == precisions[0]:
-            from akantu2_b200._capi import PinnedArray
-            L = _capi.lib()
-            fext = PinnedArray((N, 3))
-            fext.array[:] = 0.0
-            uout = PinnedArray((N, 3))
-            nb = fext.array.nbytes
+            nb = N * 3 * 8
             k_e2e = max(1, min(args.steps, 100))
-            barrier()
-            t0 = time.perf_counter()
-            for _ in range(k_e2e):
-                _capi.check(L.akb_model_set_nodal(b._h, _capi.EXTERNAL_FORCE, _capi.ptr(fext.array), nb))
-                _capi.check(L.akb_model_solve_step(b._h, 1))
-                _capi.check(L.akb_model_get_nodal(b._h, _capi.DISPLACEMENT, _capi.ptr(uout.array), nb))
-            secs = max_over_ranks(time.perf_counter() - t0)
-            results[prec]["e2e"] = {"value": world * E * k_e2e / secs, "unit": UNIT,
+            secs_sync, secs_async = e2e_legs(b, (N, 3), k_e2e, barrier)
+            secs_sync, secs_async = max_over_ranks(secs_sync), max_over_ranks(secs_async)
+            results[prec]["e2e"] = {"value": world * E * k_e2e / secs_async, "unit": UNIT,
                                     "steps": k_e2e, "h2d_bytes_per_step": nb,
-                                    "d2h_bytes_per_step": nb}
+                                    "d2h_bytes_per_step": nb,
+                                    "mode": "pipelined async C ABI copies (see e2e_legs)",
+                                    "synchronous_value": world * E * k_e2e / secs_sync}
         del b
     # unbatched baseline: every 16th instance alone (sizes spread over the
     # range), FP64, same step count with the same graphs

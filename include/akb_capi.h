@@ -163,6 +163,20 @@ int akb_model_get_nodal(akb_model *model, int field, void *host, int64_t nbytes)
  * step's prediction into the other one): its address is valid until the next
  * akb_model_solve_step; the other arrays keep their address. */
 int akb_model_nodal_device_pointer(akb_model *model, int field, void **device_ptr);
+/* asynchronous forms of set/get, for drivers that stream inputs and results
+ * every step (pinned host buffers, akb_host_alloc): the copies run on two
+ * copy streams of the model, double-buffered in device staging, so that they
+ * overlap the steps enqueued after them.  set: takes effect before the next
+ * step; the host buffer may be reused after the next akb_model_synchronize
+ * (an external force set this way is not tested for zero).  get: snapshots
+ * the field as of the steps enqueued so far and returns a ticket; the host
+ * buffer holds it once akb_model_wait_nodal_async(ticket) or
+ * akb_model_synchronize returns (only the two most recent tickets can be
+ * waited on individually). */
+int akb_model_set_nodal_async(akb_model *model, int field, const void *host, int64_t nbytes);
+int akb_model_get_nodal_async(akb_model *model, int field, void *host, int64_t nbytes,
+                              int64_t *ticket);
+int akb_model_wait_nodal_async(akb_model *model, int64_t ticket);
 
 /* Material::getStress/getGradU/getInternal<Real>(id)(type): count is the
  * number of doubles (akb_model_qp_field_size) */

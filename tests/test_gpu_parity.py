@@ -489,3 +489,45 @@ def test_neumann_stress_adds_to_external_force():
     assert np.array_equal(g.getExternalForce(), expected)
     # the top face's normal is +z: the resultant is the third column times the area
     assert np.allclose((expected - 1.0).sum(axis=0), sigma[:, 2], rtol=1e-12, atol=1e-15)
+
+
+def test_async_nodal_io_matches_synchronous_calls():
+    """per-step uploads and reads through the asynchronous forms give the
+    state and the host copies of the synchronous set / get sequence"""
+    from akantu2_b200._capi import PinnedArray
+    mesh = akb.box_tet4(6)
+    v0, bl = sinusoidal_velocity(mesh.nodes, 0.05), blocked_face(mesh.nodes)
+    rng = np.random.default_rng(4)
+    forces = [1e-4 * rng.standard_normal(mesh.nodes.shape) for _ in range(12)]
+    out = {}
+    for mode in ("sync", "async"):
+        m = gpu_model(mesh, [UNIT_ELASTIC], precision="mixed")
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        fin = [PinnedArray(mesh.nodes.shape) for _ in range(2)]
+        uo = [PinnedArray(mesh.nodes.shape) for _ in range(2)]
+        seen = []
+        prev = None
+        for j, f in enumerate(forces):
+            if mode == "sync":
+                m.setNodal("external_force", f)
+                m.solveStep(1)
+                seen.append(m.getDisplacement().copy())
+            else:
+                fin[j % 2].array[:] = f
+                m.setNodalAsync("external_force", fin[j % 2].array)
+                m.solveStep(1)
+                t = m.getNodalAsync("displacement", uo[j % 2].array)
+                if prev is not None:
+                    m.waitNodalAsync(prev[0])
+                    seen.append(uo[prev[1]].array.copy())
+                prev = (t, j % 2)
+                m.synchronize() if j == len(forces) - 1 else None
+        if mode == "async":
+            seen.append(uo[prev[1]].array.copy())
+        out[mode] = (seen, m.getVelocity().copy())
+    assert len(out["sync"][0]) == len(out["async"][0])
+    for a, b in zip(out["sync"][0], out["async"][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out["sync"][1], out["async"][1])
