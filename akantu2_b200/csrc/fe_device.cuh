@@ -47,6 +47,15 @@ template <class T> __device__ __forceinline__ void inv3(const T *m, T *r) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) r[i + 3 * j] = cof3(m, j, i) * id;
 }
+// adjugate r = det(m) m^-1 (r[i + 3 j] = cofactor (j, i)); returns det(m)
+// from the first-column cofactors
+template <class T> __device__ __forceinline__ T adj3(const T *m, T *r) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r[i + 3 * j] = cof3(m, j, i);
+  return r[0] * m[0] + r[3] * m[1] + r[6] * m[2];
+}
 template <class T> __device__ __forceinline__ void inv2(const T *m, T *r) {
   const T id = T(1) / det2(m);
   r[0] = m[3] * id;

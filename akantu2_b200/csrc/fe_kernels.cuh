@@ -787,20 +787,23 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
       Dp[1 + 3 * j] = wu[2][j] + sx * wu[3][j] + sz * wu[6][j] + sx * sz * wu[7][j];
       Dp[2 + 3 * j] = wu[4][j] + sx * wu[5][j] + sy * wu[6][j] + sx * sy * wu[7][j];
     }
-    const float det8 = det3(Jp);  // 512 det J
-    inv3(Jp, Ji);                 // J^-1 / 8
+    // adjugate: (8 J)^-1 = adj / det8, det8 = 512 det J
+    const float det8 = adj3(Jp, Ji);
+    const float rdet = 1.f / det8;
     // grad u (i, j) = sum_k J^-1(j, k) du_i/dxi_k  (the factors 8 cancel)
     float gr[9];
 #pragma unroll
     for (int j = 0; j < 3; ++j)
 #pragma unroll
       for (int i = 0; i < 3; ++i)
-        gr[i + 3 * j] = Ji[j] * Dp[0 + 3 * i] + Ji[j + 3] * Dp[1 + 3 * i] +
-                        Ji[j + 6] * Dp[2 + 3 * i];
-    const float w = det8 * (1.f / 512.f);  // 2 x 2 x 2 Gauss weights are 1
+        gr[i + 3 * j] = (Ji[j] * Dp[0 + 3 * i] + Ji[j + 3] * Dp[1 + 3 * i] +
+                         Ji[j + 6] * Dp[2 + 3 * i]) * rdet;
+    // the weight w = det J (2 x 2 x 2 Gauss weights are 1) cancels the 1/det
+    // of J^-1 in H = w P J^-1: the unweighted flux times the adjugate is
+    // accumulated and the remaining 1/512 applied once per element
     float P[9];
-    mixed_flux<3, LAW>(gr, w, mpe, ps, e_count, le, q, P);
-    // H(k, m) = sum_J P(k, J) J^-1(J, m), accumulated per mode
+    mixed_flux<3, LAW>(gr, 1.f, mpe, ps, e_count, le, q, P);
+    // H(k, m) = sum_J P(k, J) adj(J, m), accumulated per mode
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const float H0 = P[k] * Ji[0] + P[k + 3] * Ji[1] + P[k + 6] * Ji[2];
@@ -815,9 +818,11 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
       A[7][k] += sy * sz * H0 + sx * sz * H1 + sx * sy * H2;
     }
   }
+  constexpr float s0 = 1.f / 512.f, s1 = g1 / 512.f, s2 = g2 / 512.f;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    A[3][c] *= g1; A[5][c] *= g1; A[6][c] *= g1; A[7][c] *= g2;
+    A[1][c] *= s0; A[2][c] *= s0; A[4][c] *= s0;
+    A[3][c] *= s1; A[5][c] *= s1; A[6][c] *= s1; A[7][c] *= s2;
   }
   iwht8(A);
 #pragma unroll
@@ -990,36 +995,41 @@ __device__ __forceinline__ void node_apply(int64_t i, const double *acc, const d
   const double m = mass[i];
   const uint8_t bl = blocked[i];
   dt = node_dt(dt, node_inst, inst_dt, i);
-  const double hdt = .5 * dt;
+  const double hdt = __dmul_rn(.5, dt);
   bool bad = false;
 #pragma unroll
+  // explicit round-to-nearest products and sums: the nodal state arithmetic is
+  // the same (no contraction) in the FP64 and the mixed translation units,
+  // and the fused predictor equals k_predict
   for (int c = 0; c < D; ++c) {
     const int64_t k = i * D + c;
     const bool free_dof = !((bl >> c) & 1);
     const double ak = a[k];
     double vk = v[k];
-    if (free_dof) vk = vk + dt * ak;  // predicted velocity (newmark-beta.cc:69)
+    if (free_dof) vk = __dadd_rn(vk, __dmul_rn(dt, ak));  // predicted velocity (newmark-beta.cc:69)
     double r;
     if (flags & NU_FEXT_ZERO) {
       r = acc[c];
     } else {
-      r = 0. + 1. * fext[k];
-      r = r + 1. * acc[c];
+      r = __dadd_rn(0., __dmul_rn(1., fext[k]));
+      r = __dadd_rn(r, __dmul_rn(1., acc[c]));
     }
-    const double ma = 0. + -1. * ak;
-    r = r + m * ma;
+    const double ma = __dadd_rn(0., __dmul_rn(-1., ak));
+    r = __dadd_rn(r, __dmul_rn(m, ma));
     double an = ak;
     if (free_dof) {
-      const double x = 1. * (r / m);
-      vk = vk + hdt * x;
-      an = ak + 1. * x;
+      const double x = __dmul_rn(1., __ddiv_rn(r, m));
+      vk = __dadd_rn(vk, __dmul_rn(hdt, x));
+      an = __dadd_rn(ak, __dmul_rn(1., x));
       v[k] = vk;
       a[k] = an;
       bad |= !isfinite(an);
     }
     if (flags & NU_PREDICT) {
       const double uk = u[k];
-      u_next[k] = free_dof ? uk + (dt * vk + hdt * (dt * an)) : uk;
+      u_next[k] = free_dof ? __dadd_rn(uk, __dadd_rn(__dmul_rn(dt, vk),
+                                                     __dmul_rn(hdt, __dmul_rn(dt, an))))
+                           : uk;
     }
   }
   if (bad) atomicOr(status, 1u);
