@@ -93,6 +93,7 @@ def lib():
         "akb_stable_time_step_noalloc": (c_int, [c_int, vp, vp, vp, i64, c_dbl, vp, vp]),
         "akb_model_prepare_graphs": (c_int, [vp]),
         "akb_model_autotune": (c_int, [vp, c_int]),
+        "akb_model_set_stream_priority": (c_int, [vp, c_int]),
         "akb_model_set_nodal_async": (c_int, [vp, c_int, vp, i64]),
         "akb_model_get_nodal_async": (c_int, [vp, c_int, vp, i64, ctypes.POINTER(i64)]),
         "akb_model_wait_nodal_async": (c_int, [vp, i64]),

@@ -245,6 +245,8 @@ struct akb_model {
   };
   std::vector<StepGraph> graphs;
   int64_t graph_steps = 100;  // steps per captured graph (even; 0 disables)
+  int stream_priority = 0;    // of the model's stream, when priority_set
+  bool priority_set = false;
   int node_block = 128;       // threads per block of the node update
   bool node_staged = false;   // gather staged through shared memory
   // persistent multi-step kernel: 0 never (default: on B200 the 100-step
@@ -881,7 +883,10 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   }
   m->precision = precision;
   AKB_CUDA(cudaGetDevice(&m->device));
-  AKB_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  if (m->priority_set)
+    AKB_CUDA(cudaStreamCreateWithPriority(&m->stream, cudaStreamNonBlocking, m->stream_priority));
+  else
+    AKB_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
 
   const int nn = m->nn, d = m->dim;
   const int64_t E = m->E, N = m->N;
@@ -1772,6 +1777,16 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   AKB_CUDA(cudaStreamSynchronize(m->stream));
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_set_stream_priority(akb_model *m, int priority) {
+  AKB_TRY(check_model(m, false));
+  if (m->initialized) return fail(AKB_ESTATE, "the stream priority is set before initFull");
+  int least = 0, greatest = 0;
+  AKB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  m->stream_priority = std::min(std::max(priority, greatest), least);
+  m->priority_set = true;
   return AKB_OK;
 }
 

@@ -130,6 +130,13 @@ void akb_server::complete(Job *j) {
 
 void akb_server::build(Job *j) {
   int rc = akb_model_create(j->dim, j->et, j->X.data(), j->N, j->conn.data(), j->E, &j->m);
+  // short solves (few element-steps) on a high-priority stream: their kernels
+  // are scheduled ahead of the long ones', which keeps their latency low
+  if (rc == AKB_OK && (double)j->E * (double)j->steps < cfg.short_work) {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess)
+      rc = akb_model_set_stream_priority(j->m, greatest);
+  }
   if (rc == AKB_OK) rc = akb_model_add_material(j->m, j->mat_type.c_str(), j->mat_params.c_str());
   if (rc == AKB_OK && j->rule) rc = akb_model_set_quadrature_rule(j->m, j->rule);
   if (rc == AKB_OK) rc = akb_model_init_full(j->m, AKB_EXPLICIT_LUMPED_MASS, j->precision);
@@ -317,6 +324,7 @@ int akb_server_create(const akb_server_config *cfg, akb_server **out) {
   if (c.max_active <= 0) c.max_active = 64;
   if (c.chunk_steps <= 0) c.chunk_steps = 500;
   if (c.builders <= 0) c.builders = 4;
+  if (c.short_work <= 0.) c.short_work = 1e8;
   auto *s = new akb_server();
   s->cfg = c;
   s->t0 = std::chrono::steady_clock::now();

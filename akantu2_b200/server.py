@@ -15,7 +15,7 @@ from .mesh import Mesh, TYPE_IDS
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_active", ctypes.c_int),
                 ("device_bytes", ctypes.c_int64), ("chunk_steps", ctypes.c_int64),
-                ("builders", ctypes.c_int)]
+                ("builders", ctypes.c_int), ("short_work", ctypes.c_double)]
 
 
 class Request(ctypes.Structure):
@@ -64,8 +64,10 @@ class Server:
     arrays are filled when the solve completes; ``poll`` returns the
     completions (id, status, timings in seconds on the server's clock)."""
 
-    def __init__(self, device=0, max_active=64, device_bytes=0, chunk_steps=500, builders=4):
-        cfg = ServerConfig(device, max_active, int(device_bytes), int(chunk_steps), builders)
+    def __init__(self, device=0, max_active=64, device_bytes=0, chunk_steps=500, builders=4,
+                 short_work=1e8):
+        cfg = ServerConfig(device, max_active, int(device_bytes), int(chunk_steps), builders,
+                           float(short_work))
         self._h = ctypes.c_void_p()
         _capi.check(_capi.lib().akb_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self._outputs = {}

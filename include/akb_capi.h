@@ -215,6 +215,10 @@ int akb_model_solve_step(akb_model *model, int64_t nsteps);
  * parity, dt, zero external force) and replayed; steps that follow a host
  * edit of u, v, a, the blocked dofs or dt run eagerly first. */
 int akb_model_set_graph_steps(akb_model *model, int64_t steps);
+/* priority of the model's CUDA stream (cudaStreamCreateWithPriority; lower
+ * numbers run first, clamped to the device's range), before initFull; the
+ * serving loop gives short solves the higher priority */
+int akb_model_set_stream_priority(akb_model *model, int priority);
 /* persistent multi-step kernel: a model of one law group runs a whole
  * solve_step in one cooperative launch (all blocks resident, grid barriers
  * between the element and node phases, bounded waits reported in bit 1 of
@@ -333,6 +337,8 @@ typedef struct {
   int64_t chunk_steps;   /* steps enqueued per solve and scheduling pass
                             (<= 0: 500; multiples of 100 use the step graphs)  */
   int builders;          /* host threads preparing and finishing solves (<= 0: 4) */
+  double short_work;     /* solves of fewer element-steps (elements x steps) run on
+                            high-priority streams (<= 0: 1e8)                   */
 } akb_server_config;
 
 typedef struct {
