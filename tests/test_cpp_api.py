@@ -33,6 +33,35 @@ def test_example_compiles(tmp_path):
     assert exe.exists()
 
 
+def build_serving_example(tmp_path):
+    exe = tmp_path / "serve_boxes"
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "examples", "serve_boxes.cc"),
+           "-L", os.path.join(ROOT, "akantu2_b200"), "-lakb",
+           "-Wl,-rpath," + os.path.join(ROOT, "akantu2_b200"), "-o", str(exe)]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_serving_example_compiles(tmp_path):
+    assert build_serving_example(tmp_path).exists()
+
+
+@pytest.mark.gpu
+def test_serving_example_runs(tmp_path):
+    """every submitted solve completes, and solves of the same box agree"""
+    exe = build_serving_example(tmp_path)
+    out = subprocess.run([str(exe), "8", "200"], check=True, capture_output=True,
+                         text=True).stdout.splitlines()
+    assert len(out) == 8 and all(" failed " not in line for line in out)
+    by_size = {}
+    for line in out:
+        f = line.split()
+        by_size.setdefault(f[3], set()).add(f[7])
+    assert all(len(v) == 1 for v in by_size.values())  # same box, same result
+
+
 def _oracle_run(kind, cells, steps):
     mesh = akb.box_hex8(cells) if kind == "hex8" else akb.box_tet4(cells)
     x = mesh.nodes

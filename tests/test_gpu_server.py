@@ -108,3 +108,32 @@ def test_estimate_bounds_the_allocation():
         used = m.getDeviceBytes()
         est = akb.Server.estimate_bytes(mesh, mat, prec)
         assert used <= est <= used + 4096, (mesh.element_type, prec, used, est)
+
+
+def test_failed_solves_are_reported_and_do_not_disturb_others():
+    """a solve whose model cannot be built (an inverted element) completes
+    with the library's status and message; the others complete normally"""
+    good = akb.box_tet4(3)
+    bad = akb.box_tet4(3)
+    bad.connectivity[0, [1, 2]] = bad.connectivity[0, [2, 1]]  # negative Jacobian
+    mat = dict(type="elastic", E=1.0, nu=0.3, rho=1.0)
+    srv = akb.Server(max_active=4)
+    v = 0.01 * np.ones_like(good.nodes)
+    ids = {}
+    for name, mesh in (("good1", good), ("bad", bad), ("good2", good)):
+        rid, _ = srv.submit(mesh, mat, 150, velocity=v)
+        ids[rid] = name
+    done = {ids[c["id"]]: c for c in srv.drain(timeout=120)}
+    srv.close()
+    assert done["bad"]["status"] == 4 and "Negative jacobian" in done["bad"]["message"]
+    assert done["good1"]["status"] == 0 and done["good2"]["status"] == 0
+    assert np.array_equal(done["good1"]["outputs"]["displacement"],
+                          done["good2"]["outputs"]["displacement"])
+
+
+def test_submit_rejects_unknown_material():
+    srv = akb.Server()
+    with pytest.raises(akb.AkbError) as e:
+        srv.submit(akb.box_tet4(2), dict(type="no_such_law", E=1.0), 10)
+    assert e.value.name == "AKB_EMATERIAL"
+    srv.close()
