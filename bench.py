@@ -492,9 +492,14 @@ def run_ours(args):
         threads = os.cpu_count() or 1
         rate, steps, secs = cpu_rate(args.config, mesh, mat, v0, blocked, budget_s=20.0,
                                      max_steps=50, threads=threads)
+        # one thread, as the reference runs per MPI rank (a short sample)
+        rate1, steps1, secs1 = cpu_rate(args.config, mesh, mat, v0, blocked, budget_s=5.0,
+                                        max_steps=50, threads=1)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{steps} steps of the full {desc} in {secs:.1f} s "
-                         f"(CPU oracle, {threads} threads)"}
+                         f"(CPU oracle, {threads} threads)",
+               "one_thread": {"value": rate1, "unit": UNIT, "cores": 1,
+                              "sample": f"{steps1} steps in {secs1:.1f} s"}}
     if rank == 0:
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
