@@ -17,6 +17,29 @@ inline unsigned grid_for(int64_t n, int threads = kThreads) {
 }
 }  // namespace
 
+// a step kernel launch, with the programmatic-serialization attribute when pdl
+// is set (the kernel then overlaps the end of the previous kernel on the
+// stream; it waits for it in pdl_begin)
+template <class... KArgs, class... Args>
+inline cudaError_t launch_step(bool pdl, void (*kernel)(KArgs...), unsigned grid,
+                               unsigned block, cudaStream_t s, Args... args) {
+  if (!pdl) {
+    kernel<<<grid, block, 0, s>>>(args...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // ---- dispatch helpers ------------------------------------------------------
 #define AKB_DISPATCH_ELEM(g, ...)                                        \
   do {                                                                    \
@@ -102,27 +125,20 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
     constexpr bool PQ = std::is_same<T, double>::value && NQ == 8;
     if constexpr (PQ) {
       const unsigned grid = (unsigned)((ne + 31) / 32);
-      if (law == LAW_ELASTIC)
-        k_element_forces_pq<D, NN, NQ, LAW_ELASTIC>
-            <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
-      else if (law == LAW_NEOHOOKEAN)
-        k_element_forces_pq<D, NN, NQ, LAW_NEOHOOKEAN>
-            <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
-      else
-        k_element_forces_pq<D, NN, NQ, LAW_PLASTIC>
-            <<<grid, 32 * NQ, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+      auto kern = law == LAW_ELASTIC      ? k_element_forces_pq<D, NN, NQ, LAW_ELASTIC>
+                  : law == LAW_NEOHOOKEAN ? k_element_forces_pq<D, NN, NQ, LAW_NEOHOOKEAN>
+                                          : k_element_forces_pq<D, NN, NQ, LAW_PLASTIC>;
+      return launch_step(g.pdl, kern, grid, 32 * NQ, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
+                         mp, ps, re);
     } else {
       AKB_DISPATCH_BLOCK(tn.block, {
         const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-        if (law == LAW_ELASTIC)
-          k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>
-              <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
-        else if (law == LAW_NEOHOOKEAN)
-          k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>
-              <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
-        else
-          k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>
-              <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, B, wJ, u, mp, ps, re);
+        auto kern = law == LAW_ELASTIC ? k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>
+                    : law == LAW_NEOHOOKEAN
+                        ? k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>
+                        : k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;
+        return launch_step(g.pdl, kern, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
+                           mp, ps, re);
       });
     }
   });

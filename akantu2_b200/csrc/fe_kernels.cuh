@@ -24,6 +24,21 @@ namespace akb {
 constexpr int kMaxNQ = 8;
 constexpr int kMaxNN = 8;
 
+// Programmatic dependent launch of the step kernels: a step kernel launched
+// with the programmatic-serialization attribute may start while the kernel
+// before it on the stream finishes; it waits here (griddepcontrol.wait)
+// until that kernel has completed and its writes are visible, before it
+// reads anything.  Kernels of at most kEarlyTriggerBlocks blocks (one wave)
+// let the next kernel launch at once; larger grids let it launch when they
+// end, so that its waiting blocks do not hold SM slots their later waves
+// need.  Without the attribute both instructions do nothing.
+constexpr unsigned kEarlyTriggerBlocks = 1184;  // 148 SMs x 8
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (gridDim.x * gridDim.y <= kEarlyTriggerBlocks)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // natural-coordinate tables evaluated on the host (passed by value: they sit
 // in the kernel-parameter constant bank)
 struct QuadTable {
@@ -343,6 +358,7 @@ __global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
                           const double *__restrict__ a, double dt,
                           const int32_t *__restrict__ node_inst,
                           const double *__restrict__ inst_dt, double *__restrict__ u_pred) {
+  pdl_begin();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N * D) return;
   const int64_t node = i / D;
@@ -562,6 +578,7 @@ __global__ void __launch_bounds__(BLOCK)
                         const T *__restrict__ B, const T *__restrict__ wJ,
                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
                         RT *__restrict__ re) {
+  pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
   element_pe<D, NN, NQ, LAW, T, RT>(le, e_begin, e_count, E, conn, pos, B, wJ, u, mp, ps, re);
@@ -648,6 +665,7 @@ __global__ void __launch_bounds__(BLOCK)
                          const double *__restrict__ X, QuadTable tab,
                          const double *__restrict__ u, MatParams mp, GroupArgs ps,
                          float *__restrict__ re) {
+  pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
   element_geo<D, NN, NQ, LAW>(le, e_begin, e_count, E, conn, pos, X, tab, u, mp, ps, re);
@@ -837,6 +855,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                             const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                             const double *__restrict__ X, const double *__restrict__ u,
                             MatParams mp, GroupArgs ps, float *__restrict__ re) {
+  pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
   element_hex8sf<LAW, QU>(le, e_begin, e_count, E, conn, pos, X, u, mp, ps, re);
@@ -850,6 +869,7 @@ __global__ void __launch_bounds__(32 * NQ)
                         const double *__restrict__ B, const double *__restrict__ wJ,
                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
                         double *__restrict__ re) {
+  pdl_begin();
   constexpr int ND = NN * D;
   constexpr int CH = (ND + NQ - 1) / NQ;  // components reduced per round and thread
   __shared__ double us[ND][32];
@@ -1045,6 +1065,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               double dt, const int32_t *__restrict__ node_inst,
                               const double *__restrict__ inst_dt, int flags,
                               unsigned int *__restrict__ status) {
+  pdl_begin();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   node_body<D, RT, KAHAN>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst,
@@ -1079,6 +1100,7 @@ __global__ void __launch_bounds__(BLOCK)
                          const int32_t *__restrict__ node_inst,
                          const double *__restrict__ inst_dt, int flags,
                          unsigned int *__restrict__ status) {
+  pdl_begin();
   using V = typename SlotVec<D, RT>::type;
   constexpr int WPS = SlotVec<D, RT>::per_slot;  // vectors per slot
   constexpr int CAPW = kStagedBytes / (int)sizeof(V);

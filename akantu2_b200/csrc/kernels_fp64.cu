@@ -81,13 +81,9 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
                            const double *v, const double *a, double dt, double *u_pred,
                            cudaStream_t s) {
   if (g.N == 0) return cudaSuccess;
-  if (g.D == 3)
-    k_predict<3><<<grid_for(g.N * 3), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, g.node_inst,
-                                                        g.inst_dt, u_pred);
-  else
-    k_predict<2><<<grid_for(g.N * 2), kThreads, 0, s>>>(g.N, blocked, u, v, a, dt, g.node_inst,
-                                                        g.inst_dt, u_pred);
-  return cudaGetLastError();
+  auto kern = g.D == 3 ? k_predict<3> : k_predict<2>;
+  return launch_step(g.pdl, kern, grid_for(g.N * g.D), kThreads, s, g.N, blocked, u, v, a, dt,
+                     g.node_inst, g.inst_dt, u_pred);
 }
 
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
@@ -126,26 +122,17 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
   if (g.N == 0) return cudaSuccess;
   if (staged) {
     AKB_DISPATCH_NODE_BLOCK(node_block, {
-      if (g.D == 3)
-        k_node_update_staged<3, double, false, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
-            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
-            g.inst_dt, flags, status);
-      else
-        k_node_update_staged<2, double, false, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
-            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
-            g.inst_dt, flags, status);
+      auto kern = g.D == 3 ? k_node_update_staged<3, double, false, NB>
+                           : k_node_update_staged<2, double, false, NB>;
+      return launch_step(g.pdl, kern, grid_for(g.N, NB), NB, s, g.N, g.ptr, re, fext, mass,
+                         blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt, flags,
+                         status);
     });
-    return cudaGetLastError();
   }
-  if (g.D == 3)
-    k_node_update<3, double, false><<<grid_for(g.N, node_block), node_block, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
-        flags, status);
-  else
-    k_node_update<2, double, false><<<grid_for(g.N, node_block), node_block, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
-        flags, status);
-  return cudaGetLastError();
+  auto kern = g.D == 3 ? k_node_update<3, double, false> : k_node_update<2, double, false>;
+  return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
+                     fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
+                     flags, status);
 }
 
 // prescribed motion: before step k (k = 1, 2, ... since the motion was set)
@@ -158,6 +145,7 @@ __global__ void k_prescribe(int64_t count, const int64_t *__restrict__ dofs,
                             const double *__restrict__ u0, double v_max, double ramp_steps,
                             double dt, double *__restrict__ acc, int64_t *__restrict__ step,
                             double *__restrict__ u) {
+  pdl_begin();
   __shared__ double a_sh;
   if (threadIdx.x == 0) {
     const int64_t k = *step + 1;
@@ -173,9 +161,9 @@ __global__ void k_prescribe(int64_t count, const int64_t *__restrict__ dofs,
 }
 cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u0, double v_max,
                              int64_t ramp_steps, double dt, double *acc, int64_t *step,
-                             double *u, cudaStream_t s) {
-  k_prescribe<<<1, 512, 0, s>>>(count, dofs, u0, v_max, (double)ramp_steps, dt, acc, step, u);
-  return cudaGetLastError();
+                             double *u, bool pdl, cudaStream_t s) {
+  return launch_step(pdl, k_prescribe, 1, 512, s, count, dofs, u0, v_max, (double)ramp_steps,
+                     dt, acc, step, u);
 }
 
 // ---- fields and energies ---------------------------------------------------

@@ -11,8 +11,8 @@ template <int LAW, int BLOCK, int QU, int MINB = 1>
 void launch_hex8sf(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
                    const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
   const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-  k_element_forces_hex8sf<LAW, BLOCK, QU, MINB>
-      <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, u, mp, ps, re);
+  launch_step(g.pdl, k_element_forces_hex8sf<LAW, BLOCK, QU, MINB>, grid, BLOCK, s, e0, ne, g.E,
+              g.conn, g.pos, g.X, u, mp, ps, re);
 }
 
 // the shapes of the sum-factorised kernel: 64, 128 or 256 threads with 8 or
@@ -72,15 +72,11 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
     (void)ET;
     AKB_DISPATCH_BLOCK(tn.block, {
       const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-      if (law == LAW_ELASTIC)
-        k_element_forces_geo<D, NN, NQ, LAW_ELASTIC, BLOCK>
-            <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
-      else if (law == LAW_NEOHOOKEAN)
-        k_element_forces_geo<D, NN, NQ, LAW_NEOHOOKEAN, BLOCK>
-            <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
-      else
-        k_element_forces_geo<D, NN, NQ, LAW_PLASTIC, BLOCK>
-            <<<grid, BLOCK, 0, s>>>(e0, ne, g.E, g.conn, g.pos, g.X, tab, u, mp, ps, re);
+      auto kern = law == LAW_ELASTIC      ? k_element_forces_geo<D, NN, NQ, LAW_ELASTIC, BLOCK>
+                  : law == LAW_NEOHOOKEAN ? k_element_forces_geo<D, NN, NQ, LAW_NEOHOOKEAN, BLOCK>
+                                          : k_element_forces_geo<D, NN, NQ, LAW_PLASTIC, BLOCK>;
+      return launch_step(g.pdl, kern, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X, tab, u,
+                         mp, ps, re);
     });
   });
   return cudaGetLastError();
@@ -127,26 +123,17 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
   if (g.N == 0) return cudaSuccess;
   if (staged) {
     AKB_DISPATCH_NODE_BLOCK(node_block, {
-      if (g.D == 3)
-        k_node_update_staged<3, float, true, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
-            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
-            g.inst_dt, flags, status);
-      else
-        k_node_update_staged<2, float, true, NB><<<grid_for(g.N, NB), NB, 0, s>>>(
-            g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst,
-            g.inst_dt, flags, status);
+      auto kern = g.D == 3 ? k_node_update_staged<3, float, true, NB>
+                           : k_node_update_staged<2, float, true, NB>;
+      return launch_step(g.pdl, kern, grid_for(g.N, NB), NB, s, g.N, g.ptr, re, fext, mass,
+                         blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt, flags,
+                         status);
     });
-    return cudaGetLastError();
   }
-  if (g.D == 3)
-    k_node_update<3, float, true><<<grid_for(g.N, node_block), node_block, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
-        flags, status);
-  else
-    k_node_update<2, float, true><<<grid_for(g.N, node_block), node_block, 0, s>>>(
-        g.N, g.ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
-        flags, status);
-  return cudaGetLastError();
+  auto kern = g.D == 3 ? k_node_update<3, float, true> : k_node_update<2, float, true>;
+  return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
+                     fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
+                     flags, status);
 }
 
 }  // namespace akb

@@ -249,6 +249,9 @@ struct akb_model {
   bool priority_set = false;
   int node_block = 128;       // threads per block of the node update
   bool node_staged = false;   // gather staged through shared memory
+  // step kernels launched with programmatic stream serialization: each one
+  // is scheduled while its predecessor drains and waits for it on the device
+  bool pdl = false;
   // persistent multi-step kernel: 0 never (default: on B200 the 100-step
   // graphs of the two-kernel step are faster at every measured size), 1 for
   // small single-group meshes, 2 whenever the model allows it
@@ -268,6 +271,7 @@ struct akb_model {
     g.conn = dconn; g.X = dX; g.ptr = dptr; g.ent = dent; g.pos = dpos;
     g.node_inst = dnode_inst;
     g.inst_dt = dinst_dt;
+    g.pdl = pdl ? 1 : 0;
     return g;
   }
   // stream-ordered allocations on the model's stream: neither allocating
@@ -437,7 +441,7 @@ int prescribe(akb_model *m, double *u_start) {
   if (m->presc_count == 0) return AKB_OK;
   AKB_CUDA(launch_prescribe(m->presc_count, m->dpresc_dofs, m->dpresc_u0, m->presc_vmax,
                             m->presc_ramp, m->dt, m->dpresc_acc, m->dpresc_step, u_start,
-                            m->stream));
+                            m->pdl, m->stream));
   return AKB_OK;
 }
 
@@ -933,6 +937,10 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     }
     for (int64_t e = 0; e < E; ++e) m->perm[start[m->mat_user[e]]++] = e;
   }
+  // dependent launches: measured on B200 from 3k to 2M elements, 4-15 %
+  // shorter steps on meshes below ~50k elements and even above, except FP64
+  // hexahedra (the per-point kernel), whose 16^3 and 32^3 steps were slower
+  m->pdl = !(m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_FP64);
   std::vector<int64_t> iperm(E);  // user element -> internal element
   for (int64_t ie = 0; ie < E; ++ie) iperm[m->perm[ie]] = ie;
   std::vector<int32_t> conn_soa((size_t)nn * E);
@@ -1696,6 +1704,35 @@ int akb_model_autotune(akb_model *m, int repeats) {
       }
     }
   }
+  // dependent launch on or off: whole steps (element forces of every group,
+  // node update into the scratch state) in the chosen shapes
+  if (rc == AKB_OK) {
+    const int flags = NU_CORRECT | NU_PREDICT | (m->fext_zero ? NU_FEXT_ZERO : 0);
+    float ms[2] = {0.f, 0.f};
+    for (int pdl = 0; pdl < 2 && rc == AKB_OK; ++pdl) {
+      g.pdl = pdl;
+      auto step = [&]() {
+        cudaError_t e = cudaSuccess;
+        for (int r = 0; r < 8 && e == cudaSuccess; ++r) {
+          for (auto &gr : m->groups)
+            if (e == cudaSuccess) e = elem_launch(gr, gr.tune);
+          if (e != cudaSuccess) break;
+          if (m->precision == AKB_PRECISION_MIXED)
+            e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass,
+                                         m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
+                                         flags, t_status, m->node_block, m->node_staged, s);
+          else
+            e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass,
+                                        m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
+                                        flags, t_status, m->node_block, m->node_staged, s);
+        }
+        return e;
+      };
+      time_it(step, &ms[pdl]);
+    }
+    if (rc == AKB_OK) m->pdl = ms[1] < ms[0];
+    g.pdl = m->pdl ? 1 : 0;
+  }
   // the slot array again holds the forces of the current state, computed
   // with the chosen shapes
   for (auto &gr : m->groups)
@@ -1722,6 +1759,21 @@ int akb_model_set_node_shape(akb_model *m, int node_block, int staged) {
   m->node_staged = staged != 0;
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_set_dependent_launch(akb_model *m, int on) {
+  AKB_TRY(check_model(m, true));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  m->pdl = on != 0;
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_get_dependent_launch(const akb_model *m, int *on) {
+  if (!m || !on) return fail(AKB_EINVAL, "null argument");
+  *on = m->pdl ? 1 : 0;
   return AKB_OK;
 }
 

@@ -416,6 +416,16 @@ class SolidMechanicsModel:
         _capi.check(_capi.lib().akb_model_get_node_shape(self._h, ctypes.byref(b), ctypes.byref(st)))
         return b.value, bool(st.value)
 
+    def setDependentLaunch(self, on=True):
+        """Step kernels launched with programmatic stream serialization (each
+        scheduled while its predecessor drains); results are unchanged."""
+        _capi.check(_capi.lib().akb_model_set_dependent_launch(self._h, int(bool(on))))
+
+    def getDependentLaunch(self):
+        on = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_dependent_launch(self._h, ctypes.byref(on)))
+        return bool(on.value)
+
     def getDeviceBytes(self):
         """Device memory held by the model."""
         b = ctypes.c_int64()

@@ -255,6 +255,12 @@ int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
  * threads).  Both forms sum every node's slots in the same order. */
 int akb_model_set_node_shape(akb_model *model, int node_block, int staged);
 int akb_model_get_node_shape(const akb_model *model, int *node_block, int *staged);
+/* on = 1 launches the step kernels with programmatic stream serialization:
+ * a kernel is scheduled while the previous one drains and waits for its
+ * completion on the device before touching memory, which hides part of the
+ * launch gap on small meshes.  Results do not change. */
+int akb_model_set_dependent_launch(akb_model *model, int on);
+int akb_model_get_dependent_launch(const akb_model *model, int *on);
 /* captures the graph that the next solve_step will launch (and enqueues the
  * predictor it starts from), so that the capture cost is not paid inside the
  * first solve_step; optional */

@@ -201,3 +201,58 @@ def test_staged_node_gather_is_bit_identical(etype, precision, mat):
     for other in runs[1:]:
         for a, b in zip(runs[0], other):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("etype,precision,mat", [
+    ("_tetrahedron_4", "mixed", UNIT_ELASTIC), ("_tetrahedron_4", "fp64", UNIT_PLASTIC),
+    ("_hexahedron_8", "mixed", UNIT_NEOHOOKEAN), ("_hexahedron_8", "fp64", UNIT_ELASTIC),
+    ("_triangle_6", "mixed", UNIT_PLASTIC), ("_triangle_6", "fp64", UNIT_NEOHOOKEAN)])
+def test_dependent_launch_is_bit_identical(etype, precision, mat):
+    """programmatic stream serialization only changes when a step kernel is
+    scheduled, not what it computes: identical states with and without it,
+    through graphs, single steps, a velocity ramp on blocked dofs (one more
+    kernel per step) and both node-update forms"""
+    mesh = {"_hexahedron_8": lambda: akb.box_hex8(6), "_triangle_6": lambda: akb.square_tri6(8),
+            "_tetrahedron_4": lambda: akb.box_tet4(8)}[etype]()
+    d = mesh.spatial_dimension
+    v0 = sinusoidal_velocity(mesh.nodes, 0.03) if d == 3 else \
+        np.stack([0.02 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
+    bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
+    top = np.flatnonzero(np.isclose(mesh.nodes[:, d - 1], mesh.nodes[:, d - 1].max()))
+    runs = []
+    for pdl, staged in [(False, False), (True, False), (True, True)]:
+        m = gpu_model(mesh, [mat], precision=precision)
+        m.setDependentLaunch(pdl)
+        assert m.getDependentLaunch() == pdl
+        m.setNodeShape(128, staged)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.setPrescribedVelocityRamp(top, d - 1, 0.05, 40)
+        m.solveStep(3)
+        m.solveStep(207)
+        runs.append((m.getDisplacement().copy(), m.getVelocity().copy(),
+                     m.getInternalForce().copy(), m.getMaterial(0).getStress().copy()))
+    for other in runs[1:]:
+        for a, b in zip(runs[0], other):
+            assert np.array_equal(a, b)
+
+
+def test_dependent_launch_batch_is_bit_identical():
+    meshes = [akb.box_tet4(n) for n in (3, 5, 4)]
+    runs = []
+    for pdl in (False, True):
+        b = akb.BatchModel(meshes)
+        for e in (0.5, 1.0, 2.0):
+            b.addMaterial("elastic", rho=1.0, E=e, nu=0.3)
+        b.setInstanceMaterials(np.arange(3))
+        b.initFull(akb._explicit_lumped_mass, precision="mixed")
+        b.setDependentLaunch(pdl)
+        x = np.concatenate([m.nodes for m in meshes])
+        b.setNodal("velocity", sinusoidal_velocity(x, 0.03))
+        b.setNodal("blocked_dofs", blocked_face(x, axis=2))
+        b.setTimeSteps(0.8 * b.getStableTimeSteps())
+        b.solveStep(250)
+        runs.append((b.getDisplacement().copy(), b.getVelocity().copy()))
+    for a, c in zip(*runs):
+        assert np.array_equal(a, c)
