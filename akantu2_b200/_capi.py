@@ -103,6 +103,18 @@ def lib():
         "akb_model_get_dependent_launch": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_mesh_neumann_forces": (c_int, [c_int, vp, i64, vp, i64, vp, i64, vp, vp]),
         "akb_model_apply_neumann_stress": (c_int, [vp, vp, i64, vp]),
+        "akb_partition_elements": (c_int, [c_int, vp, i64, vp, i64, c_int, vp]),
+        "akb_subdomain_create": (c_int, [c_int, vp, i64, vp, i64, vp, c_int, c_int,
+                                         ctypes.POINTER(vp)]),
+        "akb_subdomain_sizes": (c_int, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                        ctypes.POINTER(i64), ctypes.POINTER(c_int)]),
+        "akb_subdomain_mesh": (c_int, [vp, vp, vp, vp, vp]),
+        "akb_subdomain_neighbor": (c_int, [vp, c_int, ctypes.POINTER(c_int), ctypes.POINTER(i64),
+                                           ctypes.POINTER(i64)]),
+        "akb_subdomain_lists": (c_int, [vp, c_int, vp, vp]),
+        "akb_subdomain_destroy": (None, [vp]),
+        "akb_model_halo_pack": (c_int, [vp, vp, i64, vp]),
+        "akb_model_halo_unpack": (c_int, [vp, vp, i64, vp]),
         "akb_model_set_persistent": (c_int, [vp, c_int]),
         "akb_model_persistent_active": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_model_set_prescribed_velocity_ramp": (c_int, [vp, vp, i64, c_dbl, i64]),

@@ -388,4 +388,23 @@ cudaError_t launch_reduce(const double *x, int64_t n, int op_min, double *partia
   return cudaGetLastError();
 }
 
+// ---- halo of a partitioned mesh: the predicted displacement of listed nodes --
+__global__ void k_halo(int64_t n, int d, bool unpack, const int32_t *__restrict__ idx,
+                       double *__restrict__ u, double *__restrict__ buf) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * d) return;
+  const int64_t node = idx[k / d], c = k % d;
+  if (unpack)
+    u[node * d + c] = buf[k];
+  else
+    buf[k] = u[node * d + c];
+}
+
+cudaError_t launch_halo(bool unpack, int d, int64_t n, const int32_t *idx, double *u, double *buf,
+                        cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_halo<<<(unsigned)((n * d + 255) / 256), 256, 0, s>>>(n, d, unpack, idx, u, buf);
+  return cudaGetLastError();
+}
+
 }  // namespace akb

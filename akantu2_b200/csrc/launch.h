@@ -137,4 +137,7 @@ constexpr int kReducePartials = 1024;
 cudaError_t launch_reduce(const double *x, int64_t n, int op_min, double *partials,
                           double *out, cudaStream_t s);
 
+// buf[k d + c] = u[idx[k] d + c] (pack) or the reverse (unpack), k < n
+cudaError_t launch_halo(bool unpack, int d, int64_t n, const int32_t *idx, double *u, double *buf,
+                        cudaStream_t s);
 }  // namespace akb

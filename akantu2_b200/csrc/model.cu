@@ -1762,6 +1762,24 @@ int akb_model_set_node_shape(akb_model *m, int node_block, int staged) {
   return AKB_OK;
 }
 
+// halo of a partitioned mesh: the prediction of the coming step (the
+// displacement its element forces read) of the listed local nodes
+int akb_model_halo_pack(akb_model *m, const int32_t *idx, int64_t n, double *buf) {
+  AKB_TRY(check_model(m, true));
+  if (n < 0 || (n > 0 && (!idx || !buf))) return fail(AKB_EINVAL, "bad arguments");
+  if (!m->predicted) AKB_TRY(predict(m));
+  AKB_CUDA(launch_halo(false, m->dim, n, idx, m->u_pred(), buf, m->stream));
+  return AKB_OK;
+}
+
+int akb_model_halo_unpack(akb_model *m, const int32_t *idx, int64_t n, const double *buf) {
+  AKB_TRY(check_model(m, true));
+  if (n < 0 || (n > 0 && (!idx || !buf))) return fail(AKB_EINVAL, "bad arguments");
+  if (!m->predicted) AKB_TRY(predict(m));
+  AKB_CUDA(launch_halo(true, m->dim, n, idx, m->u_pred(), const_cast<double *>(buf), m->stream));
+  return AKB_OK;
+}
+
 int akb_model_set_dependent_launch(akb_model *m, int on) {
   AKB_TRY(check_model(m, true));
   AKB_CUDA(cudaStreamSynchronize(m->stream));

@@ -207,6 +207,46 @@ int akb_mesh_neumann_forces(int element_type, const double *nodes, int64_t nb_no
 /* the same added to the model's external force */
 int akb_model_apply_neumann_stress(akb_model *model, const int32_t *group_nodes, int64_t count,
                                    const double *stress);
+
+/* ---- one mesh over several GPUs ----------------------------------------------
+ * Replaces the reference's distributed mesh (MeshPartitionScotch,
+ * mesh_partition_scotch.cc; ElementSynchronizer with the _smm_stress exchange,
+ * solid_mechanics_model.cc:333-370).  akb_partition_elements splits the
+ * elements by recursive coordinate bisection of their centroids (part[E],
+ * balanced counts, deterministic).  A node belongs to the lowest part among
+ * its elements; rank r's subdomain holds every element with a node r owns
+ * (a ghost layer evaluated redundantly) and every node of those elements,
+ * owned nodes first, then ghosts, each in ascending global order; elements in
+ * ascending global order.  Each owned node then sums the same slots in the
+ * same order as the whole mesh on one GPU, so a partitioned run is
+ * bit-identical to it when ghost nodes are blocked and, after every step,
+ * receive their owner's prediction: akb_model_halo_pack (the prediction of
+ * the coming step of the listed local nodes into buf[n][dim], device
+ * pointers, on the model's stream) on the owner, akb_model_halo_unpack on the
+ * holder.  Neighbor k's send list of rank r and receive list of the neighbor
+ * name the same global nodes in the same order. */
+int akb_partition_elements(int element_type, const double *nodes, int64_t nb_nodes,
+                           const int32_t *connectivity, int64_t nb_elements, int nparts,
+                           int32_t *part);
+typedef struct akb_subdomain akb_subdomain;
+int akb_subdomain_create(int element_type, const double *nodes, int64_t nb_nodes,
+                         const int32_t *connectivity, int64_t nb_elements, const int32_t *part,
+                         int nparts, int rank, akb_subdomain **out);
+int akb_subdomain_sizes(const akb_subdomain *sd, int64_t *nb_local_nodes, int64_t *nb_owned_nodes,
+                        int64_t *nb_local_elements, int *nb_neighbors);
+/* local nodes [n_local][dim], local connectivity [e_local][nodes per element]
+ * (local ids), and the global id of each local node and element; any output
+ * may be null */
+int akb_subdomain_mesh(const akb_subdomain *sd, double *nodes, int32_t *connectivity,
+                       int64_t *node_global, int64_t *element_global);
+int akb_subdomain_neighbor(const akb_subdomain *sd, int k, int *rank, int64_t *nb_send,
+                           int64_t *nb_recv);
+int akb_subdomain_lists(const akb_subdomain *sd, int k, int32_t *send_local,
+                        int32_t *recv_local);
+void akb_subdomain_destroy(akb_subdomain *sd);
+int akb_model_halo_pack(akb_model *model, const int32_t *local_nodes, int64_t count, double *buf);
+int akb_model_halo_unpack(akb_model *model, const int32_t *local_nodes, int64_t count,
+                          const double *buf);
 /* ModelSolver::solveStep  model_solver.cc:267-280: enqueues nsteps explicit
  * steps on the model's stream (asynchronous; getters synchronise) */
 int akb_model_solve_step(akb_model *model, int64_t nsteps);
