@@ -139,20 +139,24 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
 // the listed dofs get u = u0 + sum_{j <= k} dt v_max min(1, j / ramp_steps),
 // the cumulative displacement of a velocity ramped linearly to v_max over
 // ramp_steps steps.  One block: thread 0 advances the step counter and the
-// running sum, then the block writes the dofs into the displacement the
-// coming step starts from.
+// running sum (advance != 0; else the sum of the coming step is applied
+// again), then the block writes the dofs into the displacement the coming
+// step starts from.
 __global__ void k_prescribe(int64_t count, const int64_t *__restrict__ dofs,
                             const double *__restrict__ u0, double v_max, double ramp_steps,
                             double dt, double *__restrict__ acc, int64_t *__restrict__ step,
-                            double *__restrict__ u) {
+                            double *__restrict__ u, int advance) {
   pdl_begin();
   __shared__ double a_sh;
   if (threadIdx.x == 0) {
-    const int64_t k = *step + 1;
-    const double vk = v_max * fmin(1.0, (double)k / ramp_steps);
-    const double a = *acc + dt * vk;
-    *step = k;
-    *acc = a;
+    double a = *acc;
+    if (advance) {
+      const int64_t k = *step + 1;
+      const double vk = v_max * fmin(1.0, (double)k / ramp_steps);
+      a = a + dt * vk;
+      *step = k;
+      *acc = a;
+    }
     a_sh = a;
   }
   __syncthreads();
@@ -161,9 +165,9 @@ __global__ void k_prescribe(int64_t count, const int64_t *__restrict__ dofs,
 }
 cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u0, double v_max,
                              int64_t ramp_steps, double dt, double *acc, int64_t *step,
-                             double *u, bool pdl, cudaStream_t s) {
+                             double *u, bool advance, bool pdl, cudaStream_t s) {
   return launch_step(pdl, k_prescribe, 1, 512, s, count, dofs, u0, v_max, (double)ramp_steps,
-                     dt, acc, step, u);
+                     dt, acc, step, u, advance ? 1 : 0);
 }
 
 // ---- fields and energies ---------------------------------------------------

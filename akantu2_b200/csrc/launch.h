@@ -100,7 +100,7 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
 // device so that captured graphs replay it
 cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u0, double v_max,
                              int64_t ramp_steps, double dt, double *acc, int64_t *step,
-                             double *u, bool pdl, cudaStream_t s);
+                             double *u, bool advance, bool pdl, cudaStream_t s);
 
 // persistent multi-step kernel (one law group; sa describes the steps);
 // qu: points per iteration of mixed hexahedra (1 or 2)

@@ -262,6 +262,9 @@ struct akb_model {
   double presc_vmax = 0.;
   int64_t *dpresc_dofs = nullptr, *dpresc_step = nullptr;
   double *dpresc_u0 = nullptr, *dpresc_acc = nullptr;
+  // the prescribed value of the coming step is in place (a prediction made
+  // again after a host write re-applies it instead of advancing the ramp)
+  bool presc_ahead = false;
 
   double *u() const { return dU[ucur]; }
   double *u_pred() const { return dU[1 - ucur]; }
@@ -436,12 +439,14 @@ int element_forces(akb_model *m, bool in_step) {
   return AKB_OK;
 }
 
-// the prescribed dofs of the step that starts from u_start
-int prescribe(akb_model *m, double *u_start) {
+// the prescribed dofs of the step that starts from u_start: advanced to the
+// next step of the ramp, or the value of the coming step applied again
+int prescribe(akb_model *m, double *u_start, bool advance) {
   if (m->presc_count == 0) return AKB_OK;
   AKB_CUDA(launch_prescribe(m->presc_count, m->dpresc_dofs, m->dpresc_u0, m->presc_vmax,
                             m->presc_ramp, m->dt, m->dpresc_acc, m->dpresc_step, u_start,
-                            m->pdl, m->stream));
+                            advance, m->pdl, m->stream));
+  m->presc_ahead = true;
   return AKB_OK;
 }
 
@@ -450,7 +455,7 @@ int prescribe(akb_model *m, double *u_start) {
 int predict(akb_model *m) {
   AKB_CUDA(launch_predict(m->geom(), m->dblocked, m->u(), m->dv, m->da, m->dt, m->u_pred(),
                           m->stream));
-  AKB_TRY(prescribe(m, m->u_pred()));
+  AKB_TRY(prescribe(m, m->u_pred(), !m->presc_ahead));
   m->predicted = true;
   return AKB_OK;
 }
@@ -476,7 +481,7 @@ int node_update(akb_model *m, bool correct) {
                                 m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
                                 m->node_block, m->node_staged, m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
-  if (correct) AKB_TRY(prescribe(m, u_next));
+  if (correct) AKB_TRY(prescribe(m, u_next, true));
   m->fint_valid = !correct;
   return AKB_OK;
 }
@@ -1571,6 +1576,7 @@ int akb_model_set_prescribed_velocity_ramp(akb_model *m, const int64_t *dofs, in
   m->presc_count = count;
   m->presc_vmax = v_max;
   m->presc_ramp = ramp_steps;
+  m->presc_ahead = false;
   m->predicted = false;
   return AKB_OK;
 }

@@ -379,6 +379,29 @@ def test_device_prescribed_velocity_ramp_bitwise(graph_steps):
     assert np.array_equal(g.getMaterial(0).getInternal("inelastic_strain")(), o.qp(0, orc.EPS_P))
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_ramp_survives_host_writes(precision):
+    """a host write between steps makes the model predict again; the ramp
+    then applies the coming step's value again instead of advancing twice"""
+    mesh = akb.square_tri6(6)
+    x = mesh.nodes
+    right = np.flatnonzero(np.isclose(x[:, 0], 1.0))
+    blocked = np.zeros(x.shape, dtype=np.uint8)
+    blocked[np.isclose(x[:, 0], 0.0)] = 1
+    runs = []
+    for writes in (False, True):
+        g = gpu_model(mesh, [dict(UNIT_PLASTIC, sigma_y=2e-3)], precision=precision)
+        g.setNodal("blocked_dofs", blocked)
+        g.setTimeStep(0.8 * g.getStableTimeStep())
+        g.setPrescribedVelocityRamp(right, 0, 0.4, 30)
+        for chunk in (7, 1, 20, 45):
+            if writes:
+                g.setNodal("velocity", g.getVelocity().copy())
+            g.solveStep(chunk)
+        runs.append((g.getDisplacement().copy(), g.getVelocity().copy()))
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+
+
 UNIT_ELASTIC_FD = dict(type="elastic", name="svk", rho=1.0, E=1.0, nu=0.3,
                        finite_deformation=True)
 
