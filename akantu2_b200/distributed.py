@@ -302,6 +302,9 @@ class DistributedModel(_PartitionBase):
         sp = ctypes.c_void_p()
         _capi.check(_capi.lib().akb_model_stream(self.local.model._h, ctypes.byref(sp)))
         self._stream = torch.cuda.ExternalStream(sp.value, device=dev)
+        # every rank takes part in the group's first collective before the
+        # point-to-point exchanges between neighbors only
+        self.dist.barrier(group=self.group)
 
     def getStableTimeStep(self):
         import torch

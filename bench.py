@@ -76,6 +76,11 @@ def parse():
     p.add_argument("--precisions", default="mixed,fp64")
     p.add_argument("--accuracy-steps", type=int, default=10000,
                    help="steps of the mixed-vs-FP64 accuracy leg (0: skip)")
+    p.add_argument("--mode", default="replicas", choices=["replicas", "partitioned"],
+                   help="N > 1: independent replicas (weak scaling), or one mesh split over "
+                        "the ranks with a halo exchange every step (strong scaling)")
+    p.add_argument("--parts", type=int, default=0,
+                   help="partitioned, one process: subdomains advanced on the one GPU")
     return p.parse_args()
 
 
@@ -878,10 +883,91 @@ def run_serve(args):
         print(json.dumps(line), flush=True)
 
 
+def run_partitioned(args):
+    """One mesh of the configuration split into subdomains (coordinate
+    bisection, ghost layer, per-step halo exchange of the predicted
+    displacement).  Under torchrun: one subdomain per rank, the exchange over
+    NCCL on each model's stream, device time of the K steps (events on the
+    model's stream) taken as the maximum over ranks; strong scaling.  In one
+    process with --parts P: P subdomains advanced on the one GPU."""
+    rep = Replicas("nccl")
+    world, rank, local = rep.world, rep.rank, rep.local
+    import torch
+    import akantu2_b200 as akb
+    from akantu2_b200 import _capi
+    _capi.check(_capi.lib().akb_set_device(local))
+    mesh, mat, desc = workload(args.config, args.cells)
+    v0, blocked = initial_state(args.config, mesh)
+    prec = [p for p in args.precisions.split(",") if p][0]
+    if world > 1:
+        pm = akb.DistributedModel(mesh, device=local)
+        nparts = world
+    else:
+        nparts = max(1, args.parts)
+        pm = akb.PartitionedModel(mesh, nparts)
+    pm.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+    pm.initFull(akb._explicit_lumped_mass, precision=prec)
+    pm.setNodal("velocity", v0)
+    pm.setNodal("blocked_dofs", blocked)
+    pm.setTimeStep(0.8 * pm.getStableTimeStep())
+    if args.config == "tri6":
+        pm.setPrescribedVelocityRamp(np.isclose(mesh.nodes[:, 0], 1.0), 0, 1e-3, 5000)
+    pm.solveStep(max(3, args.warmup))
+    E = mesh.getNbElement()
+    models = [lc.model for lc in pm.locals]
+    for m in models:
+        m.synchronize()
+    rep.barrier()
+    # events on the first local model's stream; with one process and several
+    # subdomains every step ends with a host synchronisation of all models
+    sp = ctypes_stream(models[0])
+    stream = torch.cuda.ExternalStream(sp, device=torch.device("cuda", local))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        pm.solveStep(args.steps)
+        t1.record(stream)
+        t1.synchronize()
+    ms = rep.max(t0.elapsed_time(t1))
+    rep.barrier()
+    local_elems = [len(lc.sub.element_global) for lc in pm.locals]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": E * args.steps / (ms / 1e3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None,
+            "dtype": "f32 element math / f64 state" if prec == "mixed" else "f64",
+            "data": "synthetic (seeded random-field initial velocity)",
+            "config": {"workload": desc, "elements": E, "nodes": mesh.getNbNodes(),
+                       "precision": prec, "parallelism": f"partitioned x{nparts}",
+                       "subdomain_elements_rank0": local_elems,
+                       "l2": "inputs larger than L2 (no flush)"},
+            "clocks": clk.summary(),
+            # per step and subdomain: element forces, node update, the ramp
+            # (tri6), one halo pack and one unpack per neighbor (rank 0's
+            # subdomains)
+            "gpu_launches": args.steps * sum(2 + (1 if args.config == "tri6" else 0) +
+                                             2 * len(lc.sub.neighbors) for lc in pm.locals),
+        }
+        print(json.dumps(line), flush=True)
+    rep.close()
+
+
+def ctypes_stream(model):
+    import ctypes
+    from akantu2_b200 import _capi
+    sp = ctypes.c_void_p()
+    _capi.check(_capi.lib().akb_model_stream(model._h, ctypes.byref(sp)))
+    return sp.value
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "partitioned" and args.config in ("hex8", "tet", "tri6"):
+        run_partitioned(args)
     elif args.config == "serve":
         run_serve(args)
     elif args.config == "batch":
