@@ -544,6 +544,12 @@ int capture_graph(akb_model *m, bool any_plastic, akb_model::StepGraph **out = n
     cudaGraphDestroy(graph);
     if (e != cudaSuccess)
       return fail(AKB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    // uploaded now, so that its first launch costs what the later ones do
+    e = cudaGraphUpload(exec, m->stream);
+    if (e != cudaSuccess) {
+      cudaGraphExecDestroy(exec);
+      return fail(AKB_ECUDA, std::string("graph upload: ") + cudaGetErrorString(e));
+    }
     if (m->graphs.size() >= 8) {  // keep the cache small: drop the oldest
       cudaGraphExecDestroy(m->graphs.front().exec);
       m->graphs.erase(m->graphs.begin());
