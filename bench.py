@@ -76,6 +76,8 @@ def parse():
     p.add_argument("--precisions", default="mixed,fp64")
     p.add_argument("--accuracy-steps", type=int, default=10000,
                    help="steps of the mixed-vs-FP64 accuracy leg (0: skip)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch shapes (profiling captures)")
     p.add_argument("--mode", default="replicas", choices=["replicas", "partitioned"],
                    help="N > 1: independent replicas (weak scaling), or one mesh split over "
                         "the ranks with a halo exchange every step (strong scaling)")
@@ -445,7 +447,8 @@ def run_ours(args):
             m.setPrescribedVelocityRamp(np.isclose(mesh.nodes[:, 0], 1.0), 0, 1e-3, 5000)
         m.timeSteps(max(3, args.warmup))
         # launch shapes timed on this state (none of them changes results)
-        m.autotune(5)
+        if not args.no_autotune:
+            m.autotune(5)
         m.prepareGraphs()  # the step graph is captured before the clock starts
         footprint = m.getDeviceBytes()
         fits_l2 = footprint < L2_BYTES
@@ -676,7 +679,8 @@ def run_batch(args):
     for prec in precisions:
         b = build_batch(akb, meshes, mats, vels, blocks, prec)
         b.timeSteps(max(3, args.warmup))
-        b.autotune(5)
+        if not args.no_autotune:
+            b.autotune(5)
         b.prepareGraphs()
         barrier()
         with ClockSampler(local) as clk:
@@ -727,7 +731,8 @@ def run_batch(args):
         m.setNodal("blocked_dofs", blocks[k])
         m.setTimeStep(0.8 * m.getStableTimeStep())
         m.timeSteps(max(3, args.warmup))
-        m.autotune(5)
+        if not args.no_autotune:
+            m.autotune(5)
         m.prepareGraphs()
         alone_ms += m.timeSteps(args.steps)
         alone_e += meshes[k].getNbElement()
