@@ -133,6 +133,15 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
     } else {
       AKB_DISPATCH_BLOCK(tn.block, {
         const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
+        if constexpr (BLOCK == 128) {
+          // plastic groups: 128 threads with registers capped for 5 or 6 blocks per SM
+          if (law == LAW_PLASTIC && tn.minb > 1) {
+            auto kern = tn.minb >= 6 ? k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>
+                                     : k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;
+            return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
+                               mp, ps, re);
+          }
+        }
         auto kern = law == LAW_ELASTIC ? k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>
                     : law == LAW_NEOHOOKEAN
                         ? k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>

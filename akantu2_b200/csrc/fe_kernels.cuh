@@ -570,9 +570,10 @@ __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t 
 }
 
 // BLOCK: threads (= elements) per block, one of the launch shapes the
-// autotuner chooses from
-template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
+// autotuner chooses from; MINB > 1 caps the registers for that many resident
+// blocks per SM (plastic groups, whose state loads want more warps in flight)
+template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const T *__restrict__ B, const T *__restrict__ wJ,

@@ -942,6 +942,11 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
       // hiding more than registers)
       if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED)
         gr.tune = gr.law == LAW_PLASTIC ? ElemTuning{128, 1, 5} : ElemTuning{128, 2, 1};
+      // plastic quadratic triangles: registers capped for 6 (mixed) or 5
+      // (FP64) resident blocks, 22-24 % shorter element launches measured on
+      // the 512^2 square than uncapped
+      if (m->et == AKB_TRIANGLE_6 && gr.law == LAW_PLASTIC)
+        gr.tune = ElemTuning{128, 8, precision == AKB_PRECISION_MIXED ? 6 : 5};
       gr.nmat++;
       gr.e_count += mt.e_count;
       mt.group = (int)m->groups.size() - 1;
@@ -1678,6 +1683,8 @@ int akb_model_autotune(akb_model *m, int repeats) {
     } else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64)) {
       const int q = gr.tune.qu;
       cand = {{64, q, 1}, {128, q, 1}, {256, q, 1}};
+      if (gr.law == LAW_PLASTIC && m->et != AKB_HEXAHEDRON_8)
+        cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}});
     }
     float best = 0.f;
     for (size_t k = 0; k < cand.size() && rc == AKB_OK; ++k) {
@@ -1844,8 +1851,12 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
     return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
   if (sf && q == 1 && element_block != 128)
     return fail(AKB_EINVAL, "1 point per iteration runs with 128 threads");
-  if (min_blocks != 1 && !(sf && q != 0 && min_blocks == 5 && element_block == 128))
-    return fail(AKB_EINVAL, "min_blocks is 1, or 5 for the 128-thread mixed hexahedron kernel");
+  const bool capped_sf = sf && q != 0 && min_blocks == 5 && element_block == 128;
+  const bool capped_plastic = m->et != AKB_HEXAHEDRON_8 && law == LAW_PLASTIC &&
+                              (min_blocks == 5 || min_blocks == 6) && element_block == 128;
+  if (min_blocks != 1 && !capped_sf && !capped_plastic)
+    return fail(AKB_EINVAL, "min_blocks is 1; 5 for the 128-thread mixed hexahedron kernel; 5 or 6 "
+                            "for 128-thread plastic tetrahedra and triangles");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   bool found = false;

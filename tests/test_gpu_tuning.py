@@ -256,3 +256,32 @@ def test_dependent_launch_batch_is_bit_identical():
         runs.append((b.getDisplacement().copy(), b.getVelocity().copy()))
     for a, c in zip(*runs):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("etype,precision", [
+    ("_tetrahedron_4", "fp64"), ("_tetrahedron_4", "mixed"), ("_triangle_6", "fp64"),
+    ("_triangle_6", "mixed")])
+def test_plastic_register_caps_are_bit_identical(etype, precision):
+    """128-thread plastic kernels with registers capped for 5 or 6 resident
+    blocks per SM compute the same numbers"""
+    mesh = {"_triangle_6": lambda: akb.square_tri6(8), "_tetrahedron_4": lambda: akb.box_tet4(6)}[etype]()
+    d = mesh.spatial_dimension
+    mat = dict(UNIT_PLASTIC, sigma_y=2e-3)
+    v0 = sinusoidal_velocity(mesh.nodes, 0.05) if d == 3 else \
+        np.stack([0.05 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
+    bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
+    runs = []
+    for mb in (1, 5, 6):
+        m = gpu_model(mesh, [mat], precision=precision)
+        m.setLaunchShape(mat["type"], 128, 8, 128, mb)
+        assert m.getLaunchShape(mat["type"])[2] == mb
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.solveStep(150)
+        runs.append((m.getDisplacement().copy(), m.getVelocity().copy(),
+                     m.getMaterial(0).getInternal("inelastic_strain")().copy()))
+    assert np.max(np.abs(runs[0][2])) > 0, "the run must yield"
+    for other in runs[1:]:
+        for a, b in zip(runs[0], other):
+            assert np.array_equal(a, b)
