@@ -294,40 +294,78 @@ __device__ __forceinline__ void first_piola(const T *g, const T *S, T w, T *P) {
     }
 }
 
-// Weighted first Piola-Kirchhoff stress of the neohookean law from the
-// cofactors of F, for the mixed-precision path:
-//   P = F S = mu F + (lambda ln J - mu) F^-T,  F^-T = cof(F) / det F
-// (F C^-1 = F^-T), the same tensor as first_piola(g, neohookean_pk2(g)) in
-// exact arithmetic without forming C, its inverse or the product F S.
+// Weighted first Piola-Kirchhoff stress of the neohookean law for the
+// mixed-precision path,
+//   P = F S = mu F + (lambda ln J - mu) F^-T = mu F + c cof(F),
+//   c = (lambda ln J - mu) / det F   (F C^-1 = F^-T = cof(F) / det F),
+// the same tensor as first_piola(g, neohookean_pk2(g)) in exact arithmetic,
+// written in the displacement gradient H = F - I so that the O(1) parts
+// cancel analytically and small strains keep FP32's relative precision
+// (forming mu F and c cof(F) separately loses it: their identity parts cancel
+// to O(|H|)).  With t = tr H:
+//   3D (Cayley-Hamilton): cof(I + H) = I + K^T, K = (t + i2) I - (1 + t) H + H^2,
+//      i2 = (t^2 - tr H^2) / 2,  det F - 1 = t + i2 + det H;
+//   2D: cof(I + H) = I + K^T, K = t I - H,  det F - 1 = t + det H;
+//   P = (mu + c) I + mu H + c K^T,  mu + c = (mu (det F - 1) + lambda ln J) / det F,
+//   ln J = log1p(det F - 1) (+ ln C33 / 2 in plane stress).
+// explicitly rounded operations (never contracted or split by the compiler,
+// whatever the launch shape's register budget), FP32 and FP64
+__device__ __forceinline__ float op_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float op_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float op_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double op_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double op_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double op_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 template <int D, class T>
-__device__ __forceinline__ void neohookean_piola_cof(T lambda, T mu, const T *g, T w, T *P,
-                                                     double c33 = 0.) {
-  T F[D * D], cof[D * D];
-#pragma unroll
-  for (int j = 0; j < D; ++j)
-#pragma unroll
-    for (int i = 0; i < D; ++i) F[i + D * j] = (i == j ? T(1) : T(0)) + g[i + D * j];
+__device__ __forceinline__ void neohookean_piola(T lambda, T mu, const T *g, T w, T *P,
+                                                 double c33 = 0.) {
+  T K[D * D];
+  T dm1;
   if constexpr (D == 3) {
+    T H2[9];
 #pragma unroll
     for (int j = 0; j < 3; ++j)
 #pragma unroll
-      for (int i = 0; i < 3; ++i) cof[i + 3 * j] = cof3(F, i, j);
+      for (int i = 0; i < 3; ++i)
+        H2[i + 3 * j] = op_fma(g[i + 6], g[2 + 3 * j],
+                               op_fma(g[i + 3], g[1 + 3 * j], op_mul(g[i], g[3 * j])));
+    const T t = op_add(op_add(g[0], g[4]), g[8]);
+    const T trH2 = op_add(op_add(H2[0], H2[4]), H2[8]);
+    const T i2 = op_mul(T(0.5), op_fma(t, t, -trH2));
+    const T m0 = op_fma(g[4], g[8], -op_mul(g[5], g[7]));
+    const T m1 = op_fma(g[1], g[8], -op_mul(g[2], g[7]));
+    const T m2 = op_fma(g[1], g[5], -op_mul(g[2], g[4]));
+    const T detH = op_fma(g[6], m2, op_fma(-g[3], m1, op_mul(g[0], m0)));
+    dm1 = op_add(op_add(t, i2), detH);
+    const T a = op_add(t, i2), b = op_add(T(1), t);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) K[k] = op_fma(-b, g[k], H2[k]);
+    K[0] = op_add(K[0], a);
+    K[4] = op_add(K[4], a);
+    K[8] = op_add(K[8], a);
   } else {
-    cof[0] = F[3];
-    cof[1] = -F[2];
-    cof[2] = -F[1];
-    cof[3] = F[0];
+    const T t = op_add(g[0], g[3]);
+    dm1 = op_add(t, op_fma(g[0], g[3], -op_mul(g[1], g[2])));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) K[k] = -g[k];
+    K[0] = op_add(K[0], t);
+    K[3] = op_add(K[3], t);
   }
-  T det = F[0] * cof[0];
+  const T det = op_add(T(1), dm1);
+  T lnJ = log1p(dm1);
+  if (c33 > 0.) lnJ = op_add(lnJ, (T)(0.5 * log(c33)));
+  const T rdet = T(1) / det;
+  const T c = op_mul(op_fma(lambda, lnJ, -mu), rdet);
+  const T a0 = op_mul(op_fma(mu, dm1, op_mul(lambda, lnJ)), rdet);
 #pragma unroll
-  for (int i = 1; i < D; ++i) det += F[i] * cof[i];
-  // ln J = ln det F (+ ln C33 / 2 in plane stress)
-  T lnJ = log(det);
-  if (c33 > 0.) lnJ += (T)(0.5 * log(c33));
-  const T c = (lambda * lnJ - mu) / det;
-  const T mw = mu * w, cw = c * w;
+  for (int j = 0; j < D; ++j)
 #pragma unroll
-  for (int k = 0; k < D * D; ++k) P[k] = mw * F[k] + cw * cof[k];
+    for (int i = 0; i < D; ++i) {
+      T p = op_fma(c, K[j + D * i], op_mul(mu, g[i + D * j]));
+      if (i == j) p = op_add(p, a0);
+      P[i + D * j] = op_mul(w, p);
+    }
 }
 
 template <int D, class T> __device__ __forceinline__ void to_voigt(const T *S, T *Sv) {

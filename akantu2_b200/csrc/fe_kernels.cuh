@@ -454,7 +454,7 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
     }
   if constexpr (LAW == LAW_NEOHOOKEAN) {
     if constexpr (REL) {
-      // mixed path: r = (F S w) . dN/dx with F S from the cofactors of F
+      // mixed path: r = (F S w) . dN/dx with F S formed in the displacement gradient
       T P[D * D];
       if (mp.svk) {
         T S[D * D];
@@ -462,7 +462,7 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
         first_piola<D, T>(g, S, w, P);
       } else {
         const double c33 = point_c33<D, T>(mp, ps, ne, le, q, g);
-        neohookean_piola_cof<D, T>((T)mp.lambda, (T)mp.mu, g, w, P, c33);
+        neohookean_piola<D, T>((T)mp.lambda, (T)mp.mu, g, w, P, c33);
       }
 #pragma unroll
       for (int a = 0; a < NN; ++a)
@@ -729,7 +729,7 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
       finite_pk2<D, float>(mp, g, S);
       first_piola<D, float>(g, S, w, P);
     } else {
-      neohookean_piola_cof<D, float>((float)mp.lambda, (float)mp.mu, g, w, P);
+      neohookean_piola<D, float>((float)mp.lambda, (float)mp.mu, g, w, P);
     }
   } else if constexpr (LAW == LAW_ELASTIC) {
     float sig[D * D];
@@ -788,6 +788,25 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
   for (int m = 0; m < 8; ++m)
 #pragma unroll
     for (int c = 0; c < 3; ++c) A[m][c] = 0.f;
+  // a parallelepiped (affine element: no bilinear or trilinear geometry
+  // mode) has the same Jacobian at every point; its adjugate and 1/det are
+  // formed once.  The modes are tested for exact zeros, so the point-wise
+  // formulas below would give the same values at every point anyway.
+  bool affine = true;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    affine = affine && wx[3][c] == 0.f && wx[5][c] == 0.f && wx[6][c] == 0.f && wx[7][c] == 0.f;
+  float Ja[9], rdet_a = 0.f;
+  if (affine) {
+    float Jp[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      Jp[0 + 3 * j] = wx[1][j];
+      Jp[1 + 3 * j] = wx[2][j];
+      Jp[2 + 3 * j] = wx[4][j];
+    }
+    rdet_a = 1.f / adj3(Jp, Ja);
+  }
 #pragma unroll 1
   for (int qo = 0; qo < 8; qo += QU)
 #pragma unroll
@@ -795,20 +814,31 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
     const int q = qo + qi;
     // point q at (xi, eta, zeta) = g1 (sx, sy, sz), the order of the rule
     const float sx = (q & 1) ? 1.f : -1.f, sy = (q & 2) ? 1.f : -1.f, sz = (q & 4) ? 1.f : -1.f;
-    float Jp[9], Dp[9], Ji[9];
+    float Dp[9], Ji[9];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      // 8 d(X_j)/d(xi_k) at row k, 8 d(u_j)/d(xi_k) likewise
-      Jp[0 + 3 * j] = wx[1][j] + sy * wx[3][j] + sz * wx[5][j] + sy * sz * wx[7][j];
-      Jp[1 + 3 * j] = wx[2][j] + sx * wx[3][j] + sz * wx[6][j] + sx * sz * wx[7][j];
-      Jp[2 + 3 * j] = wx[4][j] + sx * wx[5][j] + sy * wx[6][j] + sx * sy * wx[7][j];
+      // 8 d(u_j)/d(xi_k) at row k
       Dp[0 + 3 * j] = wu[1][j] + sy * wu[3][j] + sz * wu[5][j] + sy * sz * wu[7][j];
       Dp[1 + 3 * j] = wu[2][j] + sx * wu[3][j] + sz * wu[6][j] + sx * sz * wu[7][j];
       Dp[2 + 3 * j] = wu[4][j] + sx * wu[5][j] + sy * wu[6][j] + sx * sy * wu[7][j];
     }
-    // adjugate: (8 J)^-1 = adj / det8, det8 = 512 det J
-    const float det8 = adj3(Jp, Ji);
-    const float rdet = 1.f / det8;
+    float rdet;
+    if (affine) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Ji[k] = Ja[k];
+      rdet = rdet_a;
+    } else {
+      // 8 d(X_j)/d(xi_k) at row k
+      float Jp[9];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        Jp[0 + 3 * j] = wx[1][j] + sy * wx[3][j] + sz * wx[5][j] + sy * sz * wx[7][j];
+        Jp[1 + 3 * j] = wx[2][j] + sx * wx[3][j] + sz * wx[6][j] + sx * sz * wx[7][j];
+        Jp[2 + 3 * j] = wx[4][j] + sx * wx[5][j] + sy * wx[6][j] + sx * sy * wx[7][j];
+      }
+      // adjugate: (8 J)^-1 = adj / det8, det8 = 512 det J
+      rdet = 1.f / adj3(Jp, Ji);
+    }
     // grad u (i, j) = sum_k J^-1(j, k) du_i/dxi_k  (the factors 8 cancel)
     float gr[9];
 #pragma unroll

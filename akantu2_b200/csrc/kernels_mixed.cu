@@ -39,6 +39,9 @@ void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t
     launch_hex8sf<LAW, 128, 2, 5>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.minb == 5)
     launch_hex8sf<LAW, 128, 8, 5>(g, e0, ne, u, mp, ps, re, s);
+  // 128 threads capped at 128 registers for 4 resident blocks (16 warps)
+  else if (tn.minb == 4 && tn.qu == 2)
+    launch_hex8sf<LAW, 128, 2, 4>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 1)
     launch_hex8sf<LAW, 128, 1>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 2)

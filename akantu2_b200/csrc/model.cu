@@ -936,12 +936,14 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
         m->groups.push_back(gr);
       }
       Group &gr = m->groups.back();
-      // mixed hexahedra, fastest forms measured at 128^3 on B200: 2 points
-      // per unrolled iteration (elastic, neohookean); 1 point with registers
-      // capped for 5 blocks per SM (plastic, whose state loads need latency
-      // hiding more than registers)
+      // mixed hexahedra, fastest forms measured at 128^3 on B200: all 8
+      // points unrolled (elastic); 2 points per iteration with registers
+      // capped for 4 blocks per SM (neohookean); 1 point capped for 5 blocks
+      // (plastic, whose state loads need latency hiding more than registers)
       if (m->et == AKB_HEXAHEDRON_8 && precision == AKB_PRECISION_MIXED)
-        gr.tune = gr.law == LAW_PLASTIC ? ElemTuning{128, 1, 5} : ElemTuning{128, 2, 1};
+        gr.tune = gr.law == LAW_PLASTIC      ? ElemTuning{128, 1, 5}
+                  : gr.law == LAW_NEOHOOKEAN ? ElemTuning{128, 2, 4}
+                                             : ElemTuning{128, 8, 1};
       // plastic quadratic triangles: registers capped for 6 (mixed) or 5
       // (FP64) resident blocks, 22-24 % shorter element launches measured on
       // the 512^2 square than uncapped
@@ -1679,6 +1681,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
       const int q = gr.tune.qu;
       cand = {{128, q, 1}, {128, q, 5}};
       if (q != 1) cand.insert(cand.end(), {{64, q, 1}, {256, q, 1}});
+      if (q == 2) cand.push_back({128, q, 4});
       if (q == 0) cand = {{128, 0, 1}, {64, 0, 1}, {256, 0, 1}};
     } else if (!(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64)) {
       const int q = gr.tune.qu;
@@ -1851,12 +1854,14 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
     return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
   if (sf && q == 1 && element_block != 128)
     return fail(AKB_EINVAL, "1 point per iteration runs with 128 threads");
-  const bool capped_sf = sf && q != 0 && min_blocks == 5 && element_block == 128;
+  const bool capped_sf = sf && q != 0 && element_block == 128 &&
+                         (min_blocks == 5 || (min_blocks == 4 && q == 2));
   const bool capped_plastic = m->et != AKB_HEXAHEDRON_8 && law == LAW_PLASTIC &&
                               (min_blocks == 5 || min_blocks == 6) && element_block == 128;
   if (min_blocks != 1 && !capped_sf && !capped_plastic)
-    return fail(AKB_EINVAL, "min_blocks is 1; 5 for the 128-thread mixed hexahedron kernel; 5 or 6 "
-                            "for 128-thread plastic tetrahedra and triangles");
+    return fail(AKB_EINVAL, "min_blocks is 1; 5 (or 4 with 2 points per iteration) for the "
+                            "128-thread mixed hexahedron kernel; 5 or 6 for 128-thread plastic "
+                            "tetrahedra and triangles");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   bool found = false;

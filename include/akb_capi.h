@@ -285,8 +285,9 @@ int akb_model_autotune(akb_model *model, int repeats);
  * hexahedra, where 0 selects the dN/dx form of the kernel instead of the
  * sum-factorised one (not bit-identical to it: a different FP32 evaluation);
  * min_blocks is 1 except for 128-thread kernels that cap their registers
- * for that many resident blocks per SM: 5 for the mixed hexahedron kernel,
- * 5 or 6 for plastic tetrahedra and triangles (same results) */
+ * for that many resident blocks per SM: 5 for the mixed hexahedron kernel
+ * (or 4 with 2 points per iteration), 5 or 6 for plastic tetrahedra and
+ * triangles (same results) */
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
