@@ -316,7 +316,7 @@ inline void plastic(int d, double lambda, double mu, double sigma_y, double h,
                     const double *ep_prev, double iso_cur, double iso_prev,
                     double dsth, double *s, double *ep, double *iso) {
   const int dd = d * d;
-  double gdu[9], str[9] = {0.}, dev[9], deps[9];
+  double gdu[9] = {0.}, str[9] = {0.}, dev[9], deps[9];
   for (int k = 0; k < dd; ++k) gdu[k] = g[k] - gp[k];
   elastic(d, lambda, mu, gdu, dsth, str);
   for (int k = 0; k < dd; ++k) str[k] = str[k] + sp[k];
