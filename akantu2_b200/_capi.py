@@ -20,7 +20,7 @@ TETRAHEDRON_4, HEXAHEDRON_8, TRIANGLE_6 = 0, 1, 2
 EXPLICIT_LUMPED_MASS = 0
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 (DISPLACEMENT, VELOCITY, ACCELERATION, EXTERNAL_FORCE, INTERNAL_FORCE, MASS,
- BLOCKED_DOFS, CURRENT_POSITION) = range(8)
+ BLOCKED_DOFS, CURRENT_POSITION, PREVIOUS_DISPLACEMENT, DISPLACEMENT_INCREMENT) = range(10)
 (GRAD_U, STRESS, PIOLA_KIRCHHOFF_2, INELASTIC_STRAIN, ISO_HARDENING,
  PLASTIC_ENERGY) = range(6)
 
@@ -100,6 +100,7 @@ def lib():
         "akb_model_set_node_shape": (c_int, [vp, c_int, c_int]),
         "akb_model_get_node_shape": (c_int, [vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
         "akb_model_set_dependent_launch": (c_int, [vp, c_int]),
+        "akb_model_set_increment_tracking": (c_int, [vp, c_int]),
         "akb_model_get_dependent_launch": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_mesh_neumann_forces": (c_int, [c_int, vp, i64, vp, i64, vp, i64, vp, vp]),
         "akb_model_apply_neumann_stress": (c_int, [vp, vp, i64, vp]),

@@ -411,4 +411,26 @@ cudaError_t launch_halo(bool unpack, int d, int64_t n, const int32_t *idx, doubl
   return cudaGetLastError();
 }
 
+// ---- previous displacement and increment of a step ---------------------------
+// u_n is the displacement the step starts from, u_np1 its prediction, which
+// the corrector does not change (its displacement coefficient is zero)
+__global__ void k_history(int64_t n, const double *__restrict__ u_n,
+                          const double *__restrict__ u_np1, double *__restrict__ prev,
+                          double *__restrict__ incr) {
+  pdl_begin();
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double a = u_n[k];
+  prev[k] = a;
+  incr[k] = u_np1[k] - a;
+}
+
+cudaError_t launch_history(const DevGeom &g, const double *u_n, const double *u_np1,
+                           double *prev, double *incr, cudaStream_t s) {
+  const int64_t n = g.N * g.D;
+  if (n == 0) return cudaSuccess;
+  return launch_step(g.pdl, k_history, (unsigned)((n + 255) / 256), 256, s, n, u_n, u_np1, prev,
+                     incr);
+}
+
 }  // namespace akb

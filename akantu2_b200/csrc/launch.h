@@ -140,4 +140,7 @@ cudaError_t launch_reduce(const double *x, int64_t n, int op_min, double *partia
 // buf[k d + c] = u[idx[k] d + c] (pack) or the reverse (unpack), k < n
 cudaError_t launch_halo(bool unpack, int d, int64_t n, const int32_t *idx, double *u, double *buf,
                         cudaStream_t s);
+// prev = u_n, incr = u_np1 - u_n over the N * D dofs
+cudaError_t launch_history(const DevGeom &g, const double *u_n, const double *u_np1,
+                           double *prev, double *incr, cudaStream_t s);
 }  // namespace akb

@@ -249,6 +249,9 @@ struct akb_model {
   bool priority_set = false;
   int node_block = 128;       // threads per block of the node update
   bool node_staged = false;   // gather staged through shared memory
+  // previous displacement and increment of the last step, when tracked
+  bool track_history = false;
+  double *dprev = nullptr, *dincr = nullptr;
   // step kernels launched with programmatic stream serialization: each one
   // is scheduled while its predecessor drains and waits for it on the device
   bool pdl = false;
@@ -499,6 +502,10 @@ int ensure_fint(akb_model *m) {
 int one_step(akb_model *m, bool any_plastic, cudaEvent_t e1 = nullptr,
              cudaEvent_t e2 = nullptr) {
   if (!m->predicted) AKB_TRY(predict(m));
+  // previous displacement and increment: the step goes from u() to its
+  // prediction u_pred()
+  if (m->track_history)
+    AKB_CUDA(launch_history(m->geom(), m->u(), m->u_pred(), m->dprev, m->dincr, m->stream));
   if (e1) AKB_CUDA(cudaEventRecord(e1, m->stream));
   AKB_TRY(element_forces(m, true));
   if (e2) AKB_CUDA(cudaEventRecord(e2, m->stream));
@@ -579,7 +586,8 @@ constexpr int kBarrierWords = 1 + 8192;
 constexpr int64_t kPersistentMaxElements = 1 << 18;
 
 bool use_persistent(const akb_model *m) {
-  if (m->persistent == 0 || m->groups.size() != 1 || m->presc_count > 0 || m->E == 0) return false;
+  if (m->persistent == 0 || m->groups.size() != 1 || m->presc_count > 0 || m->E == 0 ||
+      m->track_history) return false;
   const Group &gr = m->groups[0];
   // mixed hexahedra: the persistent kernel has the 1- and 2-point forms
   if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED && gr.tune.qu != 1 &&
@@ -1325,6 +1333,12 @@ int akb_model_get_nodal(akb_model *m, int field, void *host, int64_t nbytes) {
     AKB_TRY(ensure_fint(m));
     src = m->dfint;
     break;
+  case AKB_PREVIOUS_DISPLACEMENT:
+  case AKB_DISPLACEMENT_INCREMENT:
+    if (!m->track_history)
+      return fail(AKB_ESTATE, "increment tracking is off (akb_model_set_increment_tracking)");
+    src = field == AKB_PREVIOUS_DISPLACEMENT ? m->dprev : m->dincr;
+    break;
   default: return fail(AKB_EINVAL, "unknown nodal field");
   }
   AKB_CUDA(cudaMemcpyAsync(out, src, nbytes, cudaMemcpyDeviceToHost, s));
@@ -1344,6 +1358,12 @@ int akb_model_nodal_device_pointer(akb_model *m, int field, void **p) {
     AKB_TRY(ensure_fint(m));
     AKB_CUDA(cudaStreamSynchronize(m->stream));
     *p = m->dfint;
+    break;
+  case AKB_PREVIOUS_DISPLACEMENT:
+  case AKB_DISPLACEMENT_INCREMENT:
+    if (!m->track_history)
+      return fail(AKB_ESTATE, "increment tracking is off (akb_model_set_increment_tracking)");
+    *p = field == AKB_PREVIOUS_DISPLACEMENT ? m->dprev : m->dincr;
     break;
   default: return fail(AKB_EINVAL, "no device pointer for this field");
   }
@@ -1799,6 +1819,25 @@ int akb_model_halo_unpack(akb_model *m, const int32_t *idx, int64_t n, const dou
   if (n < 0 || (n > 0 && (!idx || !buf))) return fail(AKB_EINVAL, "bad arguments");
   if (!m->predicted) AKB_TRY(predict(m));
   AKB_CUDA(launch_halo(true, m->dim, n, idx, m->u_pred(), const_cast<double *>(buf), m->stream));
+  return AKB_OK;
+}
+
+int akb_model_set_increment_tracking(akb_model *m, int on) {
+  AKB_TRY(check_model(m, true));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  if (on && !m->dprev) {
+    AKB_TRY(m->alloc(&m->dprev, sizeof(double) * nodal_doubles(m)));
+    AKB_TRY(m->alloc(&m->dincr, sizeof(double) * nodal_doubles(m)));
+  }
+  if (on && !m->track_history) {
+    AKB_CUDA(cudaMemsetAsync(m->dprev, 0, sizeof(double) * nodal_doubles(m), m->stream));
+    AKB_CUDA(cudaMemsetAsync(m->dincr, 0, sizeof(double) * nodal_doubles(m), m->stream));
+    AKB_CUDA(cudaStreamSynchronize(m->stream));
+  }
+  m->track_history = on != 0;
+  // captured steps hold the launches of the previous setting
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
   return AKB_OK;
 }
 

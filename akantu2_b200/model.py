@@ -23,6 +23,8 @@ _FIELDS = {
     "acceleration": _capi.ACCELERATION, "external_force": _capi.EXTERNAL_FORCE,
     "internal_force": _capi.INTERNAL_FORCE, "mass": _capi.MASS,
     "blocked_dofs": _capi.BLOCKED_DOFS, "current_position": _capi.CURRENT_POSITION,
+    "previous_displacement": _capi.PREVIOUS_DISPLACEMENT,
+    "displacement_increment": _capi.DISPLACEMENT_INCREMENT,
 }
 _LAW_IDS = {"elastic": 0, "neohookean": 1, "plastic_linear_isotropic_hardening": 2,
             "plastic": 2}
@@ -249,6 +251,26 @@ class SolidMechanicsModel:
 
     def getBlockedDOFs(self):
         return self._get("blocked_dofs")
+
+    def setIncrementTracking(self, on=True):
+        """Keep the displacement each step starts from and its increment
+        (getPreviousDisplacement, getIncrement); off by default, one extra
+        launch per step when on (akb_model_set_increment_tracking)."""
+        self._sync_up()
+        _capi.check(_capi.lib().akb_model_set_increment_tracking(self._h, int(bool(on))))
+        self._invalidate(["previous_displacement", "displacement_increment"])
+
+    def getPreviousDisplacement(self):
+        """SolidMechanicsModel::getPreviousDisplacement: u at the start of
+        the last step (increment tracking on)."""
+        self._sync_up()
+        return self._get("previous_displacement")
+
+    def getIncrement(self):
+        """SolidMechanicsModel::getIncrement: u_{n+1} - u_n of the last step
+        (increment tracking on)."""
+        self._sync_up()
+        return self._get("displacement_increment")
 
     def getCurrentPosition(self):
         self._sync_up()

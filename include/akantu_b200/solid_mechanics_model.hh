@@ -303,6 +303,22 @@ public:
     return nodal(AKB_INTERNAL_FORCE, false);
   }
   const Array<Real> &getMass() { return nodal(AKB_MASS, false); }
+  // SolidMechanicsModel::getPreviousDisplacement / getIncrement
+  // (solid_mechanics_model.hh:284-293): kept while increment tracking is on
+  void setIncrementTracking(bool on = true) {
+    syncUp();
+    check(akb_model_set_increment_tracking(h_, on ? 1 : 0));
+    mirrors_.erase(AKB_PREVIOUS_DISPLACEMENT);
+    mirrors_.erase(AKB_DISPLACEMENT_INCREMENT);
+  }
+  const Array<Real> &getPreviousDisplacement() {
+    syncUp();
+    return nodal(AKB_PREVIOUS_DISPLACEMENT, false);
+  }
+  const Array<Real> &getIncrement() {
+    syncUp();
+    return nodal(AKB_DISPLACEMENT_INCREMENT, false);
+  }
   const Array<Real> &getCurrentPosition() {
     syncUp();
     mirrors_.erase(AKB_CURRENT_POSITION);

@@ -62,7 +62,12 @@ enum akb_nodal_field {
   AKB_INTERNAL_FORCE = 4,   /* double [N][dim] getInternalForce() (read only)*/
   AKB_MASS = 5,             /* double [N][dim] getMass()         (read only) */
   AKB_BLOCKED_DOFS = 6,     /* uint8  [N][dim] getBlockedDOFs()              */
-  AKB_CURRENT_POSITION = 7  /* double [N][dim] getCurrentPosition() (r/o)    */
+  AKB_CURRENT_POSITION = 7, /* double [N][dim] getCurrentPosition() (r/o)    */
+  /* displacement at the start of the last step and its change over it
+   * (getPreviousDisplacement / getIncrement, solid_mechanics_model.hh:284-293);
+   * read only, kept while increment tracking is on */
+  AKB_PREVIOUS_DISPLACEMENT = 8,
+  AKB_DISPLACEMENT_INCREMENT = 9
 };
 
 /* quadrature-point internals of one material, material-local element order,
@@ -297,6 +302,13 @@ int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
  * threads).  Both forms sum every node's slots in the same order. */
 int akb_model_set_node_shape(akb_model *model, int node_block, int staged);
 int akb_model_get_node_shape(const akb_model *model, int *node_block, int *staged);
+/* TimeStepSolverDefault::predictor / corrector bookkeeping
+ * (time_step_solver_default.cc:171-221): with tracking on, every step also
+ * stores the displacement it starts from (AKB_PREVIOUS_DISPLACEMENT) and
+ * u_{n+1} - u_n (AKB_DISPLACEMENT_INCREMENT), both FP64, one extra launch per
+ * step; off (the default) the step does neither and those fields are not
+ * available (AKB_ESTATE).  Turning it on zeroes both arrays. */
+int akb_model_set_increment_tracking(akb_model *model, int on);
 /* on = 1 launches the step kernels with programmatic stream serialization:
  * a kernel is scheduled while the previous one drains and waits for its
  * completion on the device before touching memory, which hides part of the

@@ -554,3 +554,46 @@ def test_async_nodal_io_matches_synchronous_calls():
     for a, b in zip(out["sync"][0], out["async"][0]):
         assert np.array_equal(a, b)
     assert np.array_equal(out["sync"][1], out["async"][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_previous_displacement_and_increment(precision):
+    """TimeStepSolverDefault's bookkeeping (time_step_solver_default.cc:171-221):
+    the previous displacement is u at the start of the last step and the
+    increment u_{n+1} - u_n, through single steps, a 100-step graph and a
+    host write between steps; tracking changes no state"""
+    mesh = akb.box_tet4(5)
+    v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
+
+    def model(track):
+        m = gpu_model(mesh, [UNIT_NEOHOOKEAN], precision=precision)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        if track:
+            m.setIncrementTracking(True)
+        return m
+
+    plain = model(False)
+    with pytest.raises(akb.AkbError):
+        plain.getIncrement()
+    history = [plain.getDisplacement().copy()]
+    for _ in range(152):
+        plain.solveStep(1)
+        history.append(plain.getDisplacement().copy())
+    tracked = model(True)
+    assert not np.any(tracked.getIncrement())
+    tracked.solveStep(1)
+    assert np.array_equal(tracked.getPreviousDisplacement(), history[0])
+    assert np.array_equal(tracked.getIncrement(), history[1] - history[0])
+    tracked.solveStep(150)  # one 100-step graph and 50 single steps
+    assert np.array_equal(tracked.getDisplacement(), history[151])
+    assert np.array_equal(tracked.getPreviousDisplacement(), history[150])
+    assert np.array_equal(tracked.getIncrement(), history[151] - history[150])
+    # a host write: the next step starts from the written displacement
+    u = tracked.getDisplacement()
+    u[:, 0] += 1e-4
+    written = u.copy()
+    tracked.solveStep(1)
+    assert np.array_equal(tracked.getPreviousDisplacement(), written)
+    assert np.array_equal(tracked.getIncrement(), tracked.getDisplacement() - written)
