@@ -71,3 +71,71 @@ def blocked_face(nodes, axis=2, value=0.0):
     b = np.zeros(nodes.shape, dtype=np.uint8)
     b[np.isclose(nodes[:, axis], value)] = 1
     return b
+
+
+# ---- travelling-wave bar (test_solid_mechanics_model_dynamics.cc) -----------------------
+# A 10 x 1 (x 1) bar of mesh size about 0.6, E = 1, nu = 0, rho = 1, a plane
+# P wave and S waves of wave vector k = (0.5, 0, 0) and amplitude A = 0.1; the
+# boundary nodes get the analytic displacement and velocity before every step
+# (their x component blocked), and the error after t = 5 is
+# sqrt(sum over nodes |u - u_exact|^2) / (number of nodes), at most 2e-3.  The
+# velocity expression is the reference test's (cosine of the phase).
+WAVE_MAT = dict(type="elastic", name="uniterial", rho=1.0, E=1.0, nu=0.0)
+WAVE_A, WAVE_K = 0.1, 0.5
+
+
+def wave_bar(etype):
+    import akantu2_b200 as akb
+    if etype == "_tetrahedron_4":
+        return akb.box_tet4(17, 2, 2, lengths=(10.0, 1.0, 1.0))
+    if etype == "_hexahedron_8":
+        return akb.box_hex8(17, 2, 2, lengths=(10.0, 1.0, 1.0))
+    return akb.square_tri6(17, 2, lengths=(10.0, 1.0))
+
+
+def wave_solution(X, t):
+    """(displacement, velocity) of the analytic waves at the points X, time t."""
+    d = X.shape[1]
+    lam, mu = 0.0, 0.5  # E = 1, nu = 0
+    cp, cs = np.sqrt(lam + 2 * mu), np.sqrt(mu)
+    wp, ws = WAVE_K * cp, WAVE_K * cs
+    ph_p = WAVE_K * X[:, 0] - wp * t
+    ph_s = WAVE_K * X[:, 0] - ws * t
+    kpush = np.zeros(d)
+    kpush[0] = WAVE_K
+    if d == 2:
+        shear = [np.array([0.0, WAVE_K])]
+    else:  # k x (0, 0, 1) and k x (0, 1, 0)
+        shear = [np.array([0.0, -WAVE_K, 0.0]), np.array([0.0, 0.0, WAVE_K])]
+    u = WAVE_A * np.outer(np.cos(ph_p), kpush)
+    v = WAVE_A * np.outer(wp * np.cos(ph_p), kpush)
+    for ks in shear:
+        u += WAVE_A * np.outer(np.cos(ph_s), ks)
+        v += WAVE_A * np.outer(ws * np.cos(ph_s), ks)
+    return u, v
+
+
+def run_wave(mesh, set_nodal, get_u, step, dt):
+    """Drives the wave test through plain callbacks; returns the maximum error."""
+    from akantu2_b200 import boundary_nodes
+    X = mesh.nodes
+    bnd = boundary_nodes(mesh.element_type, mesh.connectivity)
+    blocked = np.zeros(X.shape, dtype=np.uint8)
+    blocked[bnd, 0] = 1
+    u0, v0 = wave_solution(X, 0.0)
+    set_nodal("displacement", u0)
+    set_nodal("velocity", v0)
+    set_nodal("blocked_dofs", blocked)
+    steps = int(5.0 / dt)
+    t, err = 0.0, -1.0
+    for _ in range(steps):
+        ub, vb = wave_solution(X[bnd], t)
+        u, v = get_u()
+        u[bnd], v[bnd] = ub, vb
+        set_nodal("displacement", u)
+        set_nodal("velocity", v)
+        ue, _ = wave_solution(X, t)
+        err = max(err, np.sqrt(np.sum((u - ue) ** 2)) / X.shape[0])
+        step()
+        t += dt
+    return err, steps

@@ -597,3 +597,28 @@ def test_previous_displacement_and_increment(precision):
     tracked.solveStep(1)
     assert np.array_equal(tracked.getPreviousDisplacement(), written)
     assert np.array_equal(tracked.getIncrement(), tracked.getDisplacement() - written)
+
+
+@pytest.mark.parametrize("etype", ["_tetrahedron_4", "_hexahedron_8", "_triangle_6"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_travelling_wave_bar(etype, precision):
+    """the reference's explicit dynamics test (test_solid_mechanics_model_dynamics.cc)
+    through the C ABI, the boundary written by the host before every step:
+    error at most 2e-3, and the FP64 path equal to the oracle's run"""
+    from scenarios import WAVE_MAT, run_wave, wave_bar
+    mesh = wave_bar(etype)
+    g = gpu_model(mesh, [WAVE_MAT], precision=precision)
+    dt = g.getStableTimeStep() / 10
+    g.setTimeStep(dt)
+    err, steps = run_wave(mesh, g.setNodal,
+                          lambda: (g.getDisplacement().copy(), g.getVelocity().copy()),
+                          lambda: g.solveStep(1), dt)
+    assert steps >= 100 and 0 < err < 2e-3
+    if precision == "fp64":
+        fields = {"displacement": orc.U, "velocity": orc.V, "blocked_dofs": orc.BLOCKED}
+        o = oracle_model(mesh, [WAVE_MAT])
+        o.set_dt(dt)
+        err_o, _ = run_wave(mesh, lambda n, a: o.set(fields[n], a),
+                            lambda: (o.get(orc.U), o.get(orc.V)), lambda: o.step(1), dt)
+        assert err == err_o
+        assert np.array_equal(g.getDisplacement(), o.get(orc.U))

@@ -332,3 +332,20 @@ def test_neumann_traction_balances_internal_force(etype):
     assert np.max(np.abs(fint + fext)) <= 1e-9 * scale
     # resultant of a uniform stress over a closed boundary is zero
     assert np.max(np.abs(fext.sum(axis=0))) <= 1e-9 * scale
+
+
+@pytest.mark.parametrize("etype", ["_tetrahedron_4", "_hexahedron_8", "_triangle_6"])
+def test_travelling_wave_bar(etype):
+    """test_solid_mechanics_model_dynamics.cc on a generated bar of the same
+    size (its gmsh bars are not shipped): P and S waves driven by the analytic
+    solution on the boundary, error at most 2e-3 over t in [0, 5] with
+    dt = stable / 10 (test_solid_mechanics_model_fixture.hh:62-69)"""
+    from scenarios import OR_TYPE, WAVE_MAT, run_wave, wave_bar
+    fields = {"displacement": orc.U, "velocity": orc.V, "blocked_dofs": orc.BLOCKED}
+    mesh = wave_bar(etype)
+    o = orc.OracleModel(OR_TYPE[etype], mesh.nodes, mesh.connectivity, [WAVE_MAT])
+    dt = o.stable_dt() / 10
+    o.set_dt(dt)
+    err, steps = run_wave(mesh, lambda n, a: o.set(fields[n], a),
+                          lambda: (o.get(orc.U), o.get(orc.V)), lambda: o.step(1), dt)
+    assert steps >= 100 and 0 < err < 2e-3
