@@ -1000,7 +1000,19 @@ __device__ __forceinline__ void node_apply(int64_t i, const double *acc, const d
                                            const double *inst_dt, int flags,
                                            unsigned int *status);
 
-template <int D, class RT, bool KAHAN>
+// two consecutive float4 slots as one 32-byte load (sm_100 256-bit global
+// load); p even and the slot array 32-byte aligned
+__device__ __forceinline__ void load_slot_pair(const float *re, int64_t p, float *f) {
+  const float *q = re + 4 * p;
+  asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]),
+                 "=f"(f[6]), "=f"(f[7])
+               : "l"(q));
+}
+
+// WIDE: float4 slots read in 32-byte pairs (the launcher checks the slot
+// array's alignment); same slots, same order
+template <int D, class RT, bool KAHAN, bool WIDE = false>
 __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
                                           const RT *re,
                                           const double *fext,
@@ -1019,11 +1031,35 @@ __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
     comp[c] = 0.;
   }
   const int32_t p0 = ptr[i], p1 = ptr[i + 1];
+  if constexpr (WIDE && SlotStride<D, RT>::value == 4) {
+    int32_t p = p0;
+    if ((p & 1) && p < p1) {
+      double rv[D];
+      load_slot<D>(re, p, rv);
+      accumulate_slot<D, KAHAN>(rv, acc, comp);
+      ++p;
+    }
+#pragma unroll 2
+    for (; p + 1 < p1; p += 2) {
+      float f[8];
+      load_slot_pair(reinterpret_cast<const float *>(re), p, f);
+      double rv[3] = {(double)f[0], (double)f[1], (double)f[2]};
+      accumulate_slot<3, KAHAN>(rv, acc, comp);
+      double rw[3] = {(double)f[4], (double)f[5], (double)f[6]};
+      accumulate_slot<3, KAHAN>(rw, acc, comp);
+    }
+    if (p < p1) {
+      double rv[D];
+      load_slot<D>(re, p, rv);
+      accumulate_slot<D, KAHAN>(rv, acc, comp);
+    }
+  } else {
 #pragma unroll 4
-  for (int32_t p = p0; p < p1; ++p) {
-    double rv[D];
-    load_slot<D>(re, p, rv);
-    accumulate_slot<D, KAHAN>(rv, acc, comp);
+    for (int32_t p = p0; p < p1; ++p) {
+      double rv[D];
+      load_slot<D>(re, p, rv);
+      accumulate_slot<D, KAHAN>(rv, acc, comp);
+    }
   }
   node_apply<D>(i, acc, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst, inst_dt, flags,
                 status);
@@ -1086,7 +1122,7 @@ __device__ __forceinline__ void node_apply(int64_t i, const double *acc, const d
   if (bad) atomicOr(status, 1u);
 }
 
-template <int D, class RT, bool KAHAN>
+template <int D, class RT, bool KAHAN, bool WIDE = false>
 __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               const RT *__restrict__ re, const double *__restrict__ fext,
                               const double *__restrict__ mass,
@@ -1099,8 +1135,8 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
   pdl_begin();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  node_body<D, RT, KAHAN>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst,
-                          inst_dt, flags, status);
+  node_body<D, RT, KAHAN, WIDE>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt,
+                                node_inst, inst_dt, flags, status);
 }
 
 // Node update with the gather staged through shared memory: the slots of
