@@ -1000,17 +1000,16 @@ __device__ __forceinline__ void node_apply(int64_t i, const double *acc, const d
                                            const double *inst_dt, int flags,
                                            unsigned int *status);
 
-// two consecutive float4 slots as one 32-byte load (sm_100 256-bit global
-// load); p even and the slot array 32-byte aligned
-__device__ __forceinline__ void load_slot_pair(const float *re, int64_t p, float *f) {
-  const float *q = re + 4 * p;
+// 32 bytes of the slot array as one load (sm_100 256-bit global load): two
+// float4 slots of 3D or four float2 slots of 2D; the address 32-byte aligned
+__device__ __forceinline__ void load_32b(const float *q, float *f) {
   asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]),
                  "=f"(f[6]), "=f"(f[7])
                : "l"(q));
 }
 
-// WIDE: float4 slots read in 32-byte pairs (the launcher checks the slot
+// WIDE: FP32 slots read 32 bytes at a time (the launcher checks the slot
 // array's alignment); same slots, same order
 template <int D, class RT, bool KAHAN, bool WIDE = false>
 __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
@@ -1031,24 +1030,28 @@ __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
     comp[c] = 0.;
   }
   const int32_t p0 = ptr[i], p1 = ptr[i + 1];
-  if constexpr (WIDE && SlotStride<D, RT>::value == 4) {
+  if constexpr (WIDE && std::is_same<RT, float>::value) {
+    // floats per slot and slots per 32-byte load
+    constexpr int FS = SlotStride<D, RT>::value, PER = 8 / FS;
     int32_t p = p0;
-    if ((p & 1) && p < p1) {
+    for (; (p % PER) != 0 && p < p1; ++p) {
       double rv[D];
       load_slot<D>(re, p, rv);
       accumulate_slot<D, KAHAN>(rv, acc, comp);
-      ++p;
     }
 #pragma unroll 2
-    for (; p + 1 < p1; p += 2) {
+    for (; p + PER <= p1; p += PER) {
       float f[8];
-      load_slot_pair(reinterpret_cast<const float *>(re), p, f);
-      double rv[3] = {(double)f[0], (double)f[1], (double)f[2]};
-      accumulate_slot<3, KAHAN>(rv, acc, comp);
-      double rw[3] = {(double)f[4], (double)f[5], (double)f[6]};
-      accumulate_slot<3, KAHAN>(rw, acc, comp);
+      load_32b(reinterpret_cast<const float *>(re) + (int64_t)FS * p, f);
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        double rv[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) rv[c] = (double)f[k * FS + c];
+        accumulate_slot<D, KAHAN>(rv, acc, comp);
+      }
     }
-    if (p < p1) {
+    for (; p < p1; ++p) {
       double rv[D];
       load_slot<D>(re, p, rv);
       accumulate_slot<D, KAHAN>(rv, acc, comp);

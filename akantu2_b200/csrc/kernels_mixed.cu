@@ -133,10 +133,10 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                          status);
     });
   }
-  // 3D float4 slots: pairs of slots as 32-byte loads when the array allows it
-  const bool wide = g.D == 3 && ((uintptr_t)re & 31) == 0;
+  // slots read 32 bytes at a time when the array's alignment allows it
+  const bool wide = ((uintptr_t)re & 31) == 0;
   auto kern = g.D == 3 ? (wide ? k_node_update<3, float, true, true> : k_node_update<3, float, true>)
-                       : k_node_update<2, float, true>;
+                       : (wide ? k_node_update<2, float, true, true> : k_node_update<2, float, true>);
   return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
                      fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
                      flags, status);
