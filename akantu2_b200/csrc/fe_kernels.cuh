@@ -1009,7 +1009,13 @@ __device__ __forceinline__ void load_32b(const float *q, float *f) {
                : "l"(q));
 }
 
-// WIDE: FP32 slots read 32 bytes at a time (the launcher checks the slot
+__device__ __forceinline__ void load_32b(const double *q, double *f) {
+  asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(f[0]), "=d"(f[1]), "=d"(f[2]), "=d"(f[3])
+               : "l"(q));
+}
+
+// WIDE: slots read 32 bytes at a time (the launcher checks the slot
 // array's alignment); same slots, same order
 template <int D, class RT, bool KAHAN, bool WIDE = false>
 __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
@@ -1048,6 +1054,33 @@ __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
         double rv[D];
 #pragma unroll
         for (int c = 0; c < D; ++c) rv[c] = (double)f[k * FS + c];
+        accumulate_slot<D, KAHAN>(rv, acc, comp);
+      }
+    }
+    for (; p < p1; ++p) {
+      double rv[D];
+      load_slot<D>(re, p, rv);
+      accumulate_slot<D, KAHAN>(rv, acc, comp);
+    }
+  } else if constexpr (WIDE && std::is_same<RT, double>::value) {
+    // FP64 slots of D doubles: G slots fill D * G / 4 loads of 32 bytes
+    constexpr int G = D == 3 ? 4 : 2, NL = D * G / 4;
+    int32_t p = p0;
+    for (; (p % G) != 0 && p < p1; ++p) {
+      double rv[D];
+      load_slot<D>(re, p, rv);
+      accumulate_slot<D, KAHAN>(rv, acc, comp);
+    }
+    for (; p + G <= p1; p += G) {
+      double f[4 * NL];
+#pragma unroll
+      for (int l = 0; l < NL; ++l)
+        load_32b(reinterpret_cast<const double *>(re) + (int64_t)D * p + 4 * l, f + 4 * l);
+#pragma unroll
+      for (int k = 0; k < G; ++k) {
+        double rv[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) rv[c] = f[k * D + c];
         accumulate_slot<D, KAHAN>(rv, acc, comp);
       }
     }

@@ -129,7 +129,12 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
                          status);
     });
   }
-  auto kern = g.D == 3 ? k_node_update<3, double, false> : k_node_update<2, double, false>;
+  // slots read 32 bytes at a time when the array's alignment allows it
+  const bool wide = ((uintptr_t)re & 31) == 0;
+  auto kern = g.D == 3 ? (wide ? k_node_update<3, double, false, true>
+                               : k_node_update<3, double, false>)
+                       : (wide ? k_node_update<2, double, false, true>
+                               : k_node_update<2, double, false>);
   return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
                      fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
                      flags, status);
