@@ -551,12 +551,23 @@ __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t 
       }
     }
   }
+  // mixed tetrahedra stream dN/dx of nodes 1..3 only ([9][E]); node 0's are
+  // minus their sum (its relative displacement is zero, so only its force
+  // uses them)
+  constexpr bool TET_COMPACT = D == 3 && NN == 4 && NQ == 1 && REL;
   T r[ND];
 #pragma unroll 1
   for (int q = 0; q < NQ; ++q) {
     T b[ND];
+    if constexpr (TET_COMPACT) {
 #pragma unroll
-    for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)(q * ND + c) * E + e];
+      for (int c = 3; c < ND; ++c) b[c] = B[(int64_t)(c - 3) * E + e];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) b[j] = -((b[3 + j] + b[6 + j]) + b[9 + j]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)(q * ND + c) * E + e];
+    }
     const T w = wJ[(int64_t)q * E + e];
     T t[ND];
     element_law<D, NN, LAW, T, REL>(ue, b, w, mpe, ps, e_count, le, q, t);

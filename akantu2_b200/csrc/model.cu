@@ -1051,11 +1051,15 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   AKB_CUDA(launch_gather_scalar(g, me, m->dmass, s));
   // FP32 copies of dN/dx and det J w: streamed by the mixed kernels of 2D
   // elements and tetrahedra (a copy of the FP64 values, rounded once, is both
-  // as fast as recomputing the geometry in FP32 and more accurate)
+  // as fast as recomputing the geometry in FP32 and more accurate).
+  // Tetrahedra keep nodes 1..3 only, rows 3..11 of the [12][E] FP64 array:
+  // node 0's derivatives are minus their sum (the shape functions sum to 1)
   if (precision == AKB_PRECISION_MIXED && (d == 2 || m->et == AKB_TETRAHEDRON_4)) {
-    AKB_TRY(m->alloc(&m->fB, sizeof(float) * E * nq * nn * d));
+    const int64_t rows0 = m->et == AKB_TETRAHEDRON_4 ? 3 : 0;
+    const int64_t nb = E * (nq * nn * d - rows0);
+    AKB_TRY(m->alloc(&m->fB, sizeof(float) * nb));
     AKB_TRY(m->alloc(&m->fwJ, sizeof(float) * E * nq));
-    AKB_CUDA(launch_to_float(m->dB, m->fB, E * nq * nn * d, s));
+    AKB_CUDA(launch_to_float(m->dB + rows0 * E, m->fB, nb, s));
     AKB_CUDA(launch_to_float(m->dwJ, m->fwJ, E * nq, s));
   }
   const size_t gu_size = precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
@@ -1546,7 +1550,7 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   t += r(8 * std::max<int64_t>(std::max(E, N), 1)) + 8 * kReducePartials + 4 * 16;
   t += 4 * kBarrierWords;
   if (precision == AKB_PRECISION_MIXED && (d == 2 || et == AKB_TETRAHEDRON_4))
-    t += r(4 * E * nq * nn * d) + r(4 * E * nq);
+    t += r(4 * E * (nq * nn * d - (et == AKB_TETRAHEDRON_4 ? 3 : 0))) + r(4 * E * nq);
   const int64_t gs = precision == AKB_PRECISION_MIXED ? 4 : 8, ns = sym_comps((int)d);
   if (law == LAW_PLASTIC)
     t += 2 * (2 * r(8 * E * nq * ns) + r(gs * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
