@@ -101,6 +101,8 @@ def lib():
         "akb_model_get_node_shape": (c_int, [vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
         "akb_model_set_dependent_launch": (c_int, [vp, c_int]),
         "akb_model_set_increment_tracking": (c_int, [vp, c_int]),
+        "akb_model_set_affine_kernel": (c_int, [vp, c_int]),
+        "akb_model_get_affine_kernel": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_model_get_dependent_launch": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_mesh_neumann_forces": (c_int, [c_int, vp, i64, vp, i64, vp, i64, vp, vp]),
         "akb_model_apply_neumann_stress": (c_int, [vp, vp, i64, vp]),

@@ -757,8 +757,30 @@ __device__ __forceinline__ void mixed_flux(const float *g, float w, const MatPar
   }
 }
 
-// QU: quadrature points per unrolled iteration (1, 2, 4 or 8)
-template <int LAW, int QU>
+// relative FP32 coordinates of a hexahedron's nodes in the modal
+// (Walsh-Hadamard) basis, lexicographic corner order
+__device__ __forceinline__ void hex8_geometry_modes(int64_t e, int64_t E, const int32_t *conn,
+                                                    const double *X, float (*wx)[3]) {
+  constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+  double x0[3];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double x = X[node * 3 + i];
+      if (a == 0) x0[i] = x;
+      wx[lex[a]][i] = (float)(x - x0[i]);
+    }
+  }
+  wht8(wx);
+}
+
+// QU: quadrature points per unrolled iteration (1, 2, 4 or 8).  AFF: every
+// element of the launch is a parallelepiped (checked once per mesh), so the
+// per-point geometry and its registers are compiled out; the same arithmetic
+// as the general kernel's affine branch
+template <int LAW, int QU, bool AFF = false>
 __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int64_t e_count,
                                                int64_t E, const int32_t *conn,
                                                const int32_t *pos,
@@ -804,9 +826,11 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
   // formed once.  The modes are tested for exact zeros, so the point-wise
   // formulas below would give the same values at every point anyway.
   bool affine = true;
+  if constexpr (!AFF) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
-    affine = affine && wx[3][c] == 0.f && wx[5][c] == 0.f && wx[6][c] == 0.f && wx[7][c] == 0.f;
+    for (int c = 0; c < 3; ++c)
+      affine = affine && wx[3][c] == 0.f && wx[5][c] == 0.f && wx[6][c] == 0.f && wx[7][c] == 0.f;
+  }
   float Ja[9], rdet_a = 0.f;
   if (affine) {
     float Jp[9];
@@ -891,7 +915,7 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
 
 // MINB: blocks per SM the register allocation must allow (1: the compiler's
 // choice)
-template <int LAW, int BLOCK, int QU, int MINB>
+template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
@@ -900,7 +924,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
-  element_hex8sf<LAW, QU>(le, e_begin, e_count, E, conn, pos, X, u, mp, ps, re);
+  element_hex8sf<LAW, QU, AFF>(le, e_begin, e_count, E, conn, pos, X, u, mp, ps, re);
 }
 
 // FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q

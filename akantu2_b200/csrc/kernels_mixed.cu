@@ -7,47 +7,73 @@ namespace akb {
 
 namespace {
 
-template <int LAW, int BLOCK, int QU, int MINB = 1>
+template <int LAW, int BLOCK, int QU, int MINB = 1, bool AFF = false>
 void launch_hex8sf(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
                    const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
   const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-  launch_step(g.pdl, k_element_forces_hex8sf<LAW, BLOCK, QU, MINB>, grid, BLOCK, s, e0, ne, g.E,
-              g.conn, g.pos, g.X, u, mp, ps, re);
+  launch_step(g.pdl, k_element_forces_hex8sf<LAW, BLOCK, QU, MINB, AFF>, grid, BLOCK, s, e0, ne,
+              g.E, g.conn, g.pos, g.X, u, mp, ps, re);
 }
 
 // the shapes of the sum-factorised kernel: 64, 128 or 256 threads with 8 or
 // 2 points per iteration, 128 threads with 1
-template <int LAW, int QU>
+template <int LAW, int QU, bool AFF>
 void dispatch_hex8sf_block(int block, const DevGeom &g, int64_t e0, int64_t ne,
                            const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                            cudaStream_t s) {
   if (block == 64)
-    launch_hex8sf<LAW, 64, QU>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 64, QU, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
   else if (block == 256)
-    launch_hex8sf<LAW, 256, QU>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 256, QU, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
   else
-    launch_hex8sf<LAW, 128, QU>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, QU, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
 }
-template <int LAW>
+template <int LAW, bool AFF>
 void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
                      const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                      cudaStream_t s) {
   // 128 threads with the registers capped for 5 resident blocks (20 warps)
   if (tn.minb == 5 && tn.qu == 1)
-    launch_hex8sf<LAW, 128, 1, 5>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 1, 5, AFF>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.minb == 5 && tn.qu == 2)
-    launch_hex8sf<LAW, 128, 2, 5>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 2, 5, AFF>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.minb == 5)
-    launch_hex8sf<LAW, 128, 8, 5>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 8, 5, AFF>(g, e0, ne, u, mp, ps, re, s);
   // 128 threads capped at 128 registers for 4 resident blocks (16 warps)
   else if (tn.minb == 4 && tn.qu == 2)
-    launch_hex8sf<LAW, 128, 2, 4>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 2, 4, AFF>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 1)
-    launch_hex8sf<LAW, 128, 1>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 1, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 2)
-    dispatch_hex8sf_block<LAW, 2>(tn.block, g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf_block<LAW, 2, AFF>(tn.block, g, e0, ne, u, mp, ps, re, s);
   else
-    dispatch_hex8sf_block<LAW, 8>(tn.block, g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf_block<LAW, 8, AFF>(tn.block, g, e0, ne, u, mp, ps, re, s);
+}
+template <int LAW>
+void dispatch_hex8sf_mesh(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
+                          const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
+                          cudaStream_t s) {
+  if (g.affine)
+    dispatch_hex8sf<LAW, true>(tn, g, e0, ne, u, mp, ps, re, s);
+  else
+    dispatch_hex8sf<LAW, false>(tn, g, e0, ne, u, mp, ps, re, s);
+}
+
+// a hexahedron is a parallelepiped when its bilinear and trilinear geometry
+// modes are zero (the test of the element kernel, on the same FP32 values)
+__global__ void k_hex8_affine(int64_t E, const int32_t *__restrict__ conn,
+                              const double *__restrict__ X, unsigned int *__restrict__ flag) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  float wx[8][3];
+  hex8_geometry_modes(e, E, conn, X, wx);
+  constexpr float g1 = 0.577350269189625764509f, g2 = 1.f / 3.f;
+  bool affine = true;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    affine = affine && wx[3][c] * g1 == 0.f && wx[5][c] * g1 == 0.f && wx[6][c] * g1 == 0.f &&
+             wx[7][c] * g2 == 0.f;
+  if (!affine) atomicOr(flag, 1u);
 }
 
 }  // namespace
@@ -64,11 +90,11 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
     return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, tn, s);
   if (g.et == ET_HEX8 && tn.qu > 0) {
     if (law == LAW_ELASTIC)
-      dispatch_hex8sf<LAW_ELASTIC>(tn, g, e0, ne, u, mp, ps, re, s);
+      dispatch_hex8sf_mesh<LAW_ELASTIC>(tn, g, e0, ne, u, mp, ps, re, s);
     else if (law == LAW_NEOHOOKEAN)
-      dispatch_hex8sf<LAW_NEOHOOKEAN>(tn, g, e0, ne, u, mp, ps, re, s);
+      dispatch_hex8sf_mesh<LAW_NEOHOOKEAN>(tn, g, e0, ne, u, mp, ps, re, s);
     else
-      dispatch_hex8sf<LAW_PLASTIC>(tn, g, e0, ne, u, mp, ps, re, s);
+      dispatch_hex8sf_mesh<LAW_PLASTIC>(tn, g, e0, ne, u, mp, ps, re, s);
     return cudaGetLastError();
   }
   AKB_DISPATCH_ELEM(g, {
@@ -140,6 +166,13 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
   return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
                      fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
                      flags, status);
+}
+
+cudaError_t launch_hex8_affine_check(const DevGeom &g, unsigned int *flag, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess || g.E == 0) return e;
+  k_hex8_affine<<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X, flag);
+  return cudaGetLastError();
 }
 
 }  // namespace akb

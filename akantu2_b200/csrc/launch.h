@@ -41,6 +41,9 @@ struct DevGeom {
   const double *inst_dt = nullptr;     // [instances]
   // launch the step kernels with programmatic dependent launch (pdl_begin)
   int pdl = 0;
+  // every element is a parallelepiped (mixed hexahedra: the element kernel
+  // compiled without per-point geometry)
+  int affine = 0;
 };
 
 // ---- init ------------------------------------------------------------------
@@ -143,4 +146,6 @@ cudaError_t launch_halo(bool unpack, int d, int64_t n, const int32_t *idx, doubl
 // prev = u_n, incr = u_np1 - u_n over the N * D dofs
 cudaError_t launch_history(const DevGeom &g, const double *u_n, const double *u_np1,
                            double *prev, double *incr, cudaStream_t s);
+// flag = 1 if some hexahedron is not a parallelepiped (FP32 modal test)
+cudaError_t launch_hex8_affine_check(const DevGeom &g, unsigned int *flag, cudaStream_t s);
 }  // namespace akb

@@ -249,6 +249,9 @@ struct akb_model {
   bool priority_set = false;
   int node_block = 128;       // threads per block of the node update
   bool node_staged = false;   // gather staged through shared memory
+  // mixed hexahedra: every element a parallelepiped (found at initFull), and
+  // the kernel compiled for such meshes in use
+  bool all_affine = false, affine_kernel = false;
   // previous displacement and increment of the last step, when tracked
   bool track_history = false;
   double *dprev = nullptr, *dincr = nullptr;
@@ -278,6 +281,7 @@ struct akb_model {
     g.node_inst = dnode_inst;
     g.inst_dt = dinst_dt;
     g.pdl = pdl ? 1 : 0;
+    g.affine = affine_kernel ? 1 : 0;
     return g;
   }
   // stream-ordered allocations on the model's stream: neither allocating
@@ -1062,6 +1066,22 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_CUDA(launch_to_float(m->dB + rows0 * E, m->fB, nb, s));
     AKB_CUDA(launch_to_float(m->dwJ, m->fwJ, E * nq, s));
   }
+  // a mesh of parallelepipeds (structured and voxel meshes) runs the mixed
+  // hexahedron kernel compiled for them
+  if (precision == AKB_PRECISION_MIXED && m->et == AKB_HEXAHEDRON_8) {
+    unsigned int *flag = reinterpret_cast<unsigned int *>(m->dscratch), h = 1;
+    AKB_CUDA(launch_hex8_affine_check(g, flag, s));
+    AKB_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
+    m->all_affine = h == 0;
+    m->affine_kernel = m->all_affine;
+    // without per-point geometry the kernel fits 5 blocks per SM without
+    // spilling: the fastest shape for the elastic and neohookean laws
+    // (measured on the 128^3 box: 11 % and 7 % shorter launches)
+    if (m->all_affine)
+      for (auto &gr : m->groups)
+        if (gr.law != LAW_PLASTIC) gr.tune.minb = 5;
+  }
   const size_t gu_size = precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
   for (auto &mt : m->groups) {
     if (mt.law != LAW_PLASTIC) continue;
@@ -1842,6 +1862,24 @@ int akb_model_set_increment_tracking(akb_model *m, int on) {
   // captured steps hold the launches of the previous setting
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_set_affine_kernel(akb_model *m, int on) {
+  AKB_TRY(check_model(m, true));
+  if (on && !m->all_affine)
+    return fail(AKB_EUNSUPPORTED, "the mesh is not made of parallelepipeds only (or is not a "
+                                  "mixed-precision hexahedral mesh)");
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  m->affine_kernel = on != 0;
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_get_affine_kernel(const akb_model *m, int *on) {
+  if (!m || !on) return fail(AKB_EINVAL, "null argument");
+  *on = m->affine_kernel ? 1 : 0;
   return AKB_OK;
 }
 

@@ -252,6 +252,17 @@ class SolidMechanicsModel:
     def getBlockedDOFs(self):
         return self._get("blocked_dofs")
 
+    def setAffineKernel(self, on=True):
+        """Mixed hexahedra of a mesh of parallelepipeds: the element kernel
+        compiled without per-point geometry (the default for such meshes) or
+        the general one; the same numbers either way."""
+        _capi.check(_capi.lib().akb_model_set_affine_kernel(self._h, int(bool(on))))
+
+    def getAffineKernel(self):
+        on = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_affine_kernel(self._h, ctypes.byref(on)))
+        return bool(on.value)
+
     def setIncrementTracking(self, on=True):
         """Keep the displacement each step starts from and its increment
         (getPreviousDisplacement, getIncrement); off by default, one extra

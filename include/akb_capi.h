@@ -309,6 +309,13 @@ int akb_model_get_node_shape(const akb_model *model, int *node_block, int *stage
  * step; off (the default) the step does neither and those fields are not
  * available (AKB_ESTATE).  Turning it on zeroes both arrays. */
 int akb_model_set_increment_tracking(akb_model *model, int on);
+/* mixed-precision hexahedra: a mesh made of parallelepipeds only (found at
+ * init_full; structured and voxel meshes) runs an element kernel compiled
+ * without per-point geometry, which needs fewer registers; on = 0 returns to
+ * the general kernel.  Both compute the same numbers.  AKB_EUNSUPPORTED for
+ * other meshes. */
+int akb_model_set_affine_kernel(akb_model *model, int on);
+int akb_model_get_affine_kernel(const akb_model *model, int *on);
 /* on = 1 launches the step kernels with programmatic stream serialization:
  * a kernel is scheduled while the previous one drains and waits for its
  * completion on the device before touching memory, which hides part of the
