@@ -622,3 +622,25 @@ def test_travelling_wave_bar(etype, precision):
                             lambda: (o.get(orc.U), o.get(orc.V)), lambda: o.step(1), dt)
         assert err == err_o
         assert np.array_equal(g.getDisplacement(), o.get(orc.U))
+
+
+def test_nodes_with_many_elements_fp64_bitwise():
+    """a fan of 300 tetrahedra around one axis: two nodes with 300 slots each
+    (long node-CSR rows), the oracle's trajectory bit for bit"""
+    n = 300
+    th = 2 * np.pi * np.arange(n) / n
+    ring = np.stack([np.cos(th), np.sin(th), np.zeros(n)], axis=1)
+    nodes = np.vstack([[0.0, 0.0, 0.0], [0.0, 0.0, 1.0], ring])
+    conn = np.array([[0, 2 + k, 2 + (k + 1) % n, 1] for k in range(n)], dtype=np.int32)
+    X = nodes[conn]
+    vol = np.einsum("ij,ij->i", X[:, 1] - X[:, 0], np.cross(X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]))
+    conn[vol < 0] = conn[vol < 0][:, [0, 2, 1, 3]]
+    mesh = akb.Mesh(3, nodes, conn, "_tetrahedron_4")
+    v0 = np.zeros_like(nodes)
+    v0[2:, 2] = 0.01 * np.sin(3 * th)
+    bl = np.zeros(nodes.shape, np.uint8)
+    bl[0] = 1
+    g, o = setup_pair(mesh, [UNIT_ELASTIC], v0, bl)
+    g.solveStep(60)
+    o.step(60)
+    compare(g, o, exact=True)
