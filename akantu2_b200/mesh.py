@@ -47,7 +47,8 @@ class Mesh:
         return self
 
     def read(self, path, element_type=None):
-        """Mesh::read for gmsh 2.x ASCII files (src/io/mesh_io/mesh_io_msh.cc)."""
+        """Mesh::read for gmsh 2.x and 4.x ASCII files (src/io/mesh_io/mesh_io_msh.cc);
+        the file's physical groups become node groups (getNodeGroup)."""
         types = [element_type] if element_type else [t for t, d in DIM.items()
                                                      if d == self.spatial_dimension]
         L = _capi.lib()
@@ -65,9 +66,22 @@ class Mesh:
                 conn = np.zeros((ne.value, npe.value), dtype=np.int32)
                 tags = np.zeros(ne.value, dtype=np.int32)
                 _capi.check(L.akb_mesh_copy(h, _capi.ptr(nodes), _capi.ptr(conn), _capi.ptr(tags)))
+                ng = ctypes.c_int()
+                _capi.check(L.akb_mesh_nb_groups(h, ctypes.byref(ng)))
+                groups = {}
+                for k in range(ng.value):
+                    name = ctypes.create_string_buffer(256)
+                    gdim, count = ctypes.c_int(), ctypes.c_int64()
+                    _capi.check(L.akb_mesh_group(h, k, name, 256, ctypes.byref(gdim),
+                                                 ctypes.byref(count), None))
+                    members = np.zeros(count.value, dtype=np.int32)
+                    _capi.check(L.akb_mesh_group(h, k, None, 0, None, None, _capi.ptr(members)))
+                    groups[name.value.decode()] = members.astype(np.int64)
             finally:
                 L.akb_mesh_free(h)
-            return self.set(nodes, conn, t, tags)
+            self.set(nodes, conn, t, tags)
+            self.node_groups.update(groups)
+            return self
         raise ValueError(f"{path}: no element of a supported type")
 
     # -- akantu-style accessors ------------------------------------------------

@@ -152,8 +152,9 @@ class Mesh {
 public:
   explicit Mesh(Int spatial_dimension) : dim_(spatial_dimension), nodes_(0, spatial_dimension) {}
 
-  // Mesh::read for gmsh 2.x ASCII files: the elements of the type matching
-  // the dimension (_triangle_6 in 2D; _hexahedron_8, else _tetrahedron_4 in 3D)
+  // Mesh::read for gmsh 2.x and 4.x ASCII files: the elements of the type
+  // matching the dimension (_triangle_6 in 2D; _hexahedron_8, else
+  // _tetrahedron_4 in 3D); the file's physical groups become node groups
   void read(const std::string &path, ElementType type = _not_defined) {
     std::vector<ElementType> types;
     if (type != _not_defined) types = {type};
@@ -173,6 +174,16 @@ public:
       conn_ = Array<Idx>(ne, npe);
       tags_ = Array<Idx>(ne, 1);
       check(akb_mesh_copy(m, nodes_.data(), conn_.data(), tags_.data()));
+      int ng = 0;
+      check(akb_mesh_nb_groups(m, &ng));
+      for (int k = 0; k < ng; ++k) {
+        char name[256];
+        int64_t count = 0;
+        check(akb_mesh_group(m, k, name, sizeof(name), nullptr, &count, nullptr));
+        std::vector<int32_t> members((size_t)count);
+        check(akb_mesh_group(m, k, nullptr, 0, nullptr, nullptr, members.data()));
+        groups_[name] = std::set<Idx>(members.begin(), members.end());
+      }
       akb_mesh_free(m);
       type_ = t;
       return;

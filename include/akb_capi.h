@@ -95,11 +95,15 @@ int akb_set_device(int device);
 int akb_host_alloc(size_t bytes, void **ptr);
 int akb_host_free(void *ptr);
 
-/* ---- mesh input (src/io/mesh_io/mesh_io_msh.cc, gmsh 2.x ASCII) ---------- */
+/* ---- mesh input (src/io/mesh_io/mesh_io_msh.cc, gmsh 2.x and 4.x ASCII) -- */
 typedef struct akb_mesh akb_mesh;
-/* reads the nodes and the elements of `element_type` from a .msh file
- * (Mesh::read, src/mesh/mesh.hh:121); node order is the file's, elements are
- * numbered in order of appearance; physical tags are kept per element */
+/* reads the nodes and the elements of `element_type` from a .msh file of
+ * format 2.x, 4.0 or 4.1 (Mesh::read, src/mesh/mesh.hh:121; the reference's
+ * populateReaders2 / populateReaders4); node order is the file's, elements are
+ * numbered in order of appearance; the first physical tag is kept per
+ * element.  Every element of any type with a physical tag (volumes, facets,
+ * edges, points) adds its nodes to that physical group, named by
+ * $PhysicalNames or "msh_block_<tag>" (mesh_io_msh.cc:483-529). */
 int akb_mesh_read_msh(const char *path, int spatial_dimension, int element_type,
                       akb_mesh **mesh);
 int akb_mesh_sizes(const akb_mesh *mesh, int64_t *nb_nodes, int64_t *nb_elements,
@@ -107,6 +111,11 @@ int akb_mesh_sizes(const akb_mesh *mesh, int64_t *nb_nodes, int64_t *nb_elements
 /* copies nodes [N][dim], connectivity [E][n] and physical tag [E] */
 int akb_mesh_copy(const akb_mesh *mesh, double *nodes, int32_t *connectivity,
                   int32_t *physical_tag);
+/* physical groups of the file, in name order: name, dimension and nodes
+ * (0-based node indices; any output may be null, query nb_nodes first) */
+int akb_mesh_nb_groups(const akb_mesh *mesh, int *count);
+int akb_mesh_group(const akb_mesh *mesh, int k, char *name, size_t name_size, int *dimension,
+                   int64_t *nb_nodes, int32_t *nodes);
 void akb_mesh_free(akb_mesh *mesh);
 
 /* ---- model --------------------------------------------------------------- */
