@@ -7,12 +7,16 @@ from .mesh import (Mesh, _hexahedron_8, _tetrahedron_4, _triangle_6, box_hex8, b
                    boundary_nodes, gaussian_random_field, square_tri6)
 from .server import Server
 from .distributed import DistributedModel, PartitionedModel, Subdomain, partition_elements
-from .model import (BatchModel, FixedValue, FromHigherDim, neumann_forces, Material, SolidMechanicsModel, _explicit_lumped_mass, _x, _y,
-                    _z, getStaticParser, parseInput)
+from .model import (BatchModel, ElementDataMaterialSelector, FixedValue, FromHigherDim,
+                    MaterialSelector, MeshDataMaterialSelector, MeshDataMaterialSelectorInt,
+                    MeshDataMaterialSelectorString, neumann_forces, Material, SolidMechanicsModel,
+                    _explicit_lumped_mass, _x, _y, _z, getStaticParser, parseInput)
 
 __all__ = [
     "AkbError", "BatchModel", "Server", "LIB_PATH", "lib", "Mesh", "_hexahedron_8", "_tetrahedron_4", "_triangle_6",
     "box_hex8", "box_tet4", "boundary_nodes", "gaussian_random_field", "square_tri6", "FixedValue", "FromHigherDim", "neumann_forces", "Material",
     "SolidMechanicsModel", "_explicit_lumped_mass", "_x", "_y", "_z", "getStaticParser",
     "parseInput", "DistributedModel", "PartitionedModel", "Subdomain", "partition_elements",
+    "MaterialSelector", "ElementDataMaterialSelector", "MeshDataMaterialSelector",
+    "MeshDataMaterialSelectorString", "MeshDataMaterialSelectorInt",
 ]

@@ -61,6 +61,8 @@ def lib():
         "akb_mesh_nb_groups": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_mesh_group": (c_int, [vp, c_int, ctypes.c_char_p, ctypes.c_size_t,
                                    ctypes.POINTER(c_int), ctypes.POINTER(i64), vp]),
+        "akb_mesh_nb_element_names": (c_int, [vp, ctypes.POINTER(c_int)]),
+        "akb_mesh_element_names": (c_int, [vp, c_int, ctypes.c_char_p, ctypes.c_size_t, vp]),
         "akb_mesh_copy": (c_int, [vp, vp, vp, vp]),
         "akb_mesh_free": (None, [vp]),
         "akb_model_create": (c_int, [c_int, c_int, vp, i64, vp, i64, pp]),

@@ -34,6 +34,12 @@ struct akb_mesh {
   std::vector<int32_t> tag;
   // physical groups: name -> (dimension, node indices)
   std::map<std::string, std::pair<int, std::set<int32_t>>> groups;
+  // the "physical_names" element data of the read type: distinct names, and
+  // each element's index into them; absent (has_names false) for a format 2
+  // file without $PhysicalNames, as in the reference
+  bool has_names = false;
+  std::vector<std::string> names;
+  std::vector<int32_t> name_of;
 };
 
 namespace {
@@ -98,7 +104,20 @@ struct Reader {
     if (type == gt) {
       if ((int)idx.size() != m->nn) return akb::fail(AKB_EPARSE, "wrong number of element nodes");
       m->conn.insert(m->conn.end(), idx.begin(), idx.end());
-      m->tag.push_back(phys.empty() ? 0 : phys[0]);
+      const int first = phys.empty() ? 0 : phys[0];
+      m->tag.push_back(first);
+      // the element's physical name: format 2 names every tag, unnamed ones
+      // by their number (mesh_io.cc:97-110); format 4 names an element only
+      // when its entity's first tag has a name (mesh_io_msh.cc:669-676)
+      auto it = names.find(first);
+      std::string name;
+      if (it != names.end() && !phys.empty())
+        name = it->second;
+      else if (version < 4000)
+        name = std::to_string(first);
+      auto pos = std::find(m->names.begin(), m->names.end(), name);
+      m->name_of.push_back((int32_t)(pos - m->names.begin()));
+      if (pos == m->names.end()) m->names.push_back(name);
     }
     return AKB_OK;
   }
@@ -267,6 +286,7 @@ extern "C" int akb_mesh_read_msh(const char *path, int dim, int et, akb_mesh **o
     }
   }
   if (version == 0) return bail(AKB_EPARSE, "missing $MeshFormat");
+  m->has_names = version >= 4000 || !rd.names.empty();
   *out = m;
   return AKB_OK;
 }
@@ -308,6 +328,27 @@ extern "C" int akb_mesh_group(const akb_mesh *m, int k, char *name, size_t name_
   if (dim) *dim = it->second.first;
   if (nb_nodes) *nb_nodes = (int64_t)it->second.second.size();
   if (nodes) std::copy(it->second.second.begin(), it->second.second.end(), nodes);
+  return AKB_OK;
+}
+
+extern "C" int akb_mesh_nb_element_names(const akb_mesh *m, int *count) {
+  if (!m || !count) return akb::fail(AKB_EINVAL, "null argument");
+  *count = m->has_names ? (int)m->names.size() : -1;
+  return AKB_OK;
+}
+
+extern "C" int akb_mesh_element_names(const akb_mesh *m, int k, char *name, size_t name_size,
+                                      int32_t *name_of_element) {
+  if (!m) return akb::fail(AKB_EINVAL, "null mesh");
+  if (!m->has_names) return akb::fail(AKB_EINVAL, "the file gives no physical names");
+  if (name && name_size > 0) {
+    if (k < 0 || k >= (int)m->names.size()) return akb::fail(AKB_EINVAL, "name index out of range");
+    const std::string &s = m->names[k];
+    const size_t n = std::min(name_size - 1, s.size());
+    std::copy(s.begin(), s.begin() + n, name);
+    name[n] = '\0';
+  }
+  if (name_of_element) std::copy(m->name_of.begin(), m->name_of.end(), name_of_element);
   return AKB_OK;
 }
 

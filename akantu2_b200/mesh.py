@@ -32,6 +32,7 @@ class Mesh:
         self.connectivity = np.zeros((0, 0), dtype=np.int32)
         self.physical_tags = np.zeros(0, dtype=np.int32)
         self.node_groups = {}
+        self.mesh_data = {}
         if nodes is not None:
             self.set(nodes, connectivity, element_type)
 
@@ -77,10 +78,26 @@ class Mesh:
                     members = np.zeros(count.value, dtype=np.int32)
                     _capi.check(L.akb_mesh_group(h, k, None, 0, None, None, _capi.ptr(members)))
                     groups[name.value.decode()] = members.astype(np.int64)
+                nb_names = ctypes.c_int()
+                _capi.check(L.akb_mesh_nb_element_names(h, ctypes.byref(nb_names)))
+                names = None
+                if nb_names.value >= 0:
+                    table = []
+                    for k in range(nb_names.value):
+                        buf = ctypes.create_string_buffer(256)
+                        _capi.check(L.akb_mesh_element_names(h, k, buf, 256, None))
+                        table.append(buf.value.decode())
+                    index = np.zeros(ne.value, dtype=np.int32)
+                    _capi.check(L.akb_mesh_element_names(h, 0, None, 0, _capi.ptr(index)))
+                    names = np.array(table, dtype=object)[index] if table else \
+                        np.zeros(0, dtype=object)
             finally:
                 L.akb_mesh_free(h)
             self.set(nodes, conn, t, tags)
             self.node_groups.update(groups)
+            self.mesh_data = {"tag_0": self.physical_tags}
+            if names is not None:
+                self.mesh_data["physical_names"] = names
             return self
         raise ValueError(f"{path}: no element of a supported type")
 
@@ -105,6 +122,13 @@ class Mesh:
 
     def getUpperBounds(self):
         return self.nodes.max(axis=0)
+
+    def getData(self, name, element_type=None):
+        """Element data read from the file (Mesh::getData): "tag_0", the first
+        physical tag, and "physical_names", each element's physical name."""
+        if name not in self.mesh_data:
+            raise KeyError(f"the mesh has no element data '{name}'")
+        return self.mesh_data[name]
 
     def createNodeGroup(self, name, nodes):
         self.node_groups[name] = np.unique(np.asarray(nodes, dtype=np.int64))

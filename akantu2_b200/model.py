@@ -91,6 +91,79 @@ def neumann_forces(mesh, group_nodes, stress):
     return out
 
 
+class MaterialSelector:
+    """Element -> material index (ConstitutiveLawSelector,
+    src/model/common/constitutive_laws/constitutive_law_selector.hh:45-86):
+    the fallback value, or a fallback selector, for every element."""
+
+    def __init__(self):
+        self.fallback_value = 0
+        self.fallback_selector = None
+
+    def setFallback(self, f):
+        if isinstance(f, MaterialSelector):
+            self.fallback_selector = f
+        else:
+            self.fallback_value = int(f)
+
+    def getFallbackValue(self):
+        return self.fallback_value
+
+    def _fallback(self, model, elements):
+        if self.fallback_selector is not None:
+            return self.fallback_selector.select(model)[elements]
+        return np.full(len(elements), self.fallback_value, dtype=np.int32)
+
+    def select(self, model):
+        """the material index of every element of the model's mesh"""
+        return self._fallback(model, np.arange(model.mesh.getNbElement()))
+
+
+class ElementDataMaterialSelector(MaterialSelector):
+    """ElementDataConstitutiveLawSelector (constitutive_law_selector.hh:119-142,
+    constitutive_law_selector_tmpl.hh:8-20): a string datum is the name of the
+    element's material, an integer datum its index; an element whose name
+    names no material takes the fallback."""
+
+    def __init__(self, element_data, model=None, first_index=1):
+        super().__init__()
+        self.element_data = np.asarray(element_data)
+        self.first_index = first_index
+
+    def _data(self, model):
+        return self.element_data
+
+    def select(self, model):
+        data = self._data(model)
+        n = model.mesh.getNbElement()
+        if len(data) != n:
+            raise ValueError("element data must have one entry per element")
+        if data.dtype.kind in "iu":
+            return data.astype(np.int32)
+        index = {model.getMaterial(i).getName(): i for i in range(model.getNbMaterials())}
+        out = np.array([index.get(str(d), -1) for d in data], dtype=np.int32)
+        miss = np.nonzero(out < 0)[0]
+        if len(miss):
+            out[miss] = self._fallback(model, miss)
+        return out
+
+
+class MeshDataMaterialSelector(ElementDataMaterialSelector):
+    """MeshDataConstitutiveLawSelector (constitutive_law_selector.hh:144-150):
+    the selector of the mesh's element data of that name, e.g.
+    MeshDataMaterialSelector("physical_names", model) for a gmsh file whose
+    physical names are the material names."""
+
+    def __init__(self, name, model, first_index=1):
+        super().__init__(model.mesh.getData(name), model, first_index)
+        self.name = name
+
+
+# the reference's Python names (python/py_constitutive_law_selector.cc:95-96)
+MeshDataMaterialSelectorString = MeshDataMaterialSelector
+MeshDataMaterialSelectorInt = MeshDataMaterialSelector
+
+
 class Material:
     """View of one material of a model (src/model/solid_mechanics/material.hh)."""
 
@@ -125,6 +198,10 @@ class Material:
         if field in (_capi.ISO_HARDENING, _capi.PLASTIC_ENERGY):
             return out.reshape(-1, 1)
         return out.reshape(-1, m.dim * m.dim)
+
+    def getElementFilter(self, element_type=None):
+        """elements of the mesh that this material holds"""
+        return np.nonzero(self._model._element_materials() == self._index)[0]
 
     def getStress(self, element_type=None):
         return self._qp(_capi.STRESS)
@@ -183,6 +260,20 @@ class SolidMechanicsModel:
         self._mat = np.ascontiguousarray(material_of_element, dtype=np.int32)
         _capi.check(_capi.lib().akb_model_set_element_materials(self._h, _capi.ptr(self._mat)))
 
+    def setMaterialSelector(self, selector):
+        """setMaterialSelector (constitutive_laws_handler.hh:251): applied at
+        initFull, once the materials are known"""
+        if self._initialized:
+            raise _capi.AkbError(7, "the material selector must be set before initFull")
+        self._selector = selector
+
+    def getMaterialSelector(self):
+        return getattr(self, "_selector", None)
+
+    def _element_materials(self):
+        mat = getattr(self, "_mat", None)
+        return np.zeros(self.mesh.getNbElement(), np.int32) if mat is None else mat
+
     def setQuadratureRule(self, rule):
         """0: the reference's default order; 1: the 6-point rule of _triangle_6."""
         _capi.check(_capi.lib().akb_model_set_quadrature_rule(self._h, rule))
@@ -194,6 +285,8 @@ class SolidMechanicsModel:
         if not self._materials_added:
             for text in _static_parser.texts:
                 _capi.check(L.akb_model_load_materials(self._h, text.encode()))
+        if getattr(self, "_selector", None) is not None:
+            self.setElementMaterials(self._selector.select(self))
         prec = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}[precision]
         _capi.check(L.akb_model_init_full(self._h, _capi.EXPLICIT_LUMPED_MASS, prec))
         self._initialized = True

@@ -25,6 +25,7 @@
 #define AKANTU_B200_SOLID_MECHANICS_MODEL_HH_
 
 #include <cstdint>
+#include <deque>
 #include <fstream>
 #include <map>
 #include <memory>
@@ -32,6 +33,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../akb_capi.h"
@@ -184,6 +186,21 @@ public:
         check(akb_mesh_group(m, k, nullptr, 0, nullptr, nullptr, members.data()));
         groups_[name] = std::set<Idx>(members.begin(), members.end());
       }
+      int nb_names = 0;
+      check(akb_mesh_nb_element_names(m, &nb_names));
+      has_physical_names_ = nb_names >= 0;
+      physical_names_.clear();
+      if (has_physical_names_ && ne > 0) {
+        std::vector<std::string> table((size_t)nb_names);
+        for (int k = 0; k < nb_names; ++k) {
+          char name[256];
+          check(akb_mesh_element_names(m, k, name, sizeof(name), nullptr));
+          table[k] = name;
+        }
+        std::vector<int32_t> index((size_t)ne);
+        check(akb_mesh_element_names(m, 0, nullptr, 0, index.data()));
+        for (int32_t i : index) physical_names_.push_back(table[i]);
+      }
       akb_mesh_free(m);
       type_ = t;
       return;
@@ -206,6 +223,20 @@ public:
   const Array<Idx> &getConnectivity(ElementType = _not_defined) const { return conn_; }
   const Array<Idx> &getPhysicalTags() const { return tags_; }
 
+  // element data read from the file (Mesh::getData): "physical_names"
+  // (std::string, each element's physical name) and "tag_0" (Idx, its first
+  // physical tag)
+  template <typename T> std::vector<T> getData(const ID &name, ElementType = _not_defined) const {
+    if constexpr (std::is_same_v<T, std::string>) {
+      if (name != "physical_names" || !has_physical_names_)
+        throw Exception(AKB_EINVAL, "the mesh has no element data " + name);
+      return physical_names_;
+    } else {
+      if (name != "tag_0") throw Exception(AKB_EINVAL, "the mesh has no element data " + name);
+      return std::vector<T>(tags_.data(), tags_.data() + tags_.size());
+    }
+  }
+
   // named node groups (src/mesh/group_manager.hh), used by applyBC
   void createNodeGroup(const ID &name, const std::vector<Idx> &nodes) {
     groups_[name] = std::set<Idx>(nodes.begin(), nodes.end());
@@ -218,6 +249,8 @@ private:
   Array<Real> nodes_;
   Array<Idx> conn_{0, 4}, tags_{0, 1};
   std::map<ID, std::set<Idx>> groups_;
+  bool has_physical_names_ = false;
+  std::vector<std::string> physical_names_;
 };
 
 namespace BC {
@@ -242,6 +275,48 @@ struct FromHigherDim {
 
 class SolidMechanicsModel;
 
+/* ---- material selection (src/model/common/constitutive_laws/
+ * constitutive_law_selector.hh:45-150) ----------------------------------------- */
+struct Element {
+  ElementType type = _not_defined;
+  Idx element = 0;
+};
+
+class MaterialSelector : public std::enable_shared_from_this<MaterialSelector> {
+public:
+  virtual ~MaterialSelector() = default;
+  virtual Idx operator()(const Element &element) {
+    return fallback_selector_ ? (*fallback_selector_)(element) : fallback_value_;
+  }
+  void setFallback(Idx f) { fallback_value_ = f; }
+  void setFallback(const std::shared_ptr<MaterialSelector> &f) { fallback_selector_ = f; }
+  Idx getFallbackValue() const { return fallback_value_; }
+
+private:
+  Idx fallback_value_ = 0;
+  std::shared_ptr<MaterialSelector> fallback_selector_;
+};
+
+// a string datum is the name of the element's material (an element whose
+// name names no material takes the fallback), an integer datum its index
+template <typename T> class ElementDataMaterialSelector : public MaterialSelector {
+public:
+  ElementDataMaterialSelector(std::vector<T> data, SolidMechanicsModel &model, Idx first_index = 1)
+      : data_(std::move(data)), model_(&model), first_index_(first_index) {}
+  inline Idx operator()(const Element &element) override;
+  Idx getFirstIndex() const { return first_index_; }
+
+private:
+  std::vector<T> data_;
+  SolidMechanicsModel *model_;
+  Idx first_index_;
+};
+
+template <typename T> class MeshDataMaterialSelector : public ElementDataMaterialSelector<T> {
+public:
+  inline MeshDataMaterialSelector(const ID &name, SolidMechanicsModel &model, Idx first_index = 1);
+};
+
 /* ---- Material view ---------------------------------------------------------- */
 class Material {
 public:
@@ -249,6 +324,8 @@ public:
   inline Real get(const ID &param) const;
   Real getRho() const { return get("rho"); }
   inline ID getName() const;
+  // the mesh elements that this material holds
+  inline Array<Idx> getElementFilter(ElementType = _not_defined) const;
   // quadrature-point internals, material-local element order, [nq][dim*dim]
   inline Array<Real> getStress(ElementType = _not_defined);
   inline Array<Real> getGradU(ElementType = _not_defined);
@@ -279,7 +356,30 @@ public:
   void initFull(AnalysisMethodArg arg = {_explicit_lumped_mass, AKB_PRECISION_FP64}) {
     for (const auto &text : getStaticParser().texts())
       check(akb_model_load_materials(h_, text.c_str()));
+    applySelector();
     check(akb_model_init_full(h_, arg.method, arg.precision));
+  }
+
+  // element -> material index, before initFull
+  void setElementMaterials(const std::vector<Idx> &material_of_element) {
+    check(akb_model_set_element_materials(h_, material_of_element.data()));
+    element_materials_ = material_of_element;
+  }
+  // applied by initFull, once the materials are known
+  void setMaterialSelector(std::shared_ptr<MaterialSelector> selector) {
+    selector_ = std::move(selector);
+  }
+  MaterialSelector *getMaterialSelector() { return selector_.get(); }
+  // material index of a name, -1 when no material has that name
+  Int getMaterialIndex(const ID &name) {
+    for (Int i = 0; i < getNbMaterials(); ++i)
+      if (getMaterial(i).getName() == name) return i;
+    return -1;
+  }
+  const std::vector<Idx> &getElementMaterials() {
+    if (element_materials_.size() != (size_t)mesh_.getNbElement())
+      element_materials_.assign((size_t)mesh_.getNbElement(), 0);
+    return element_materials_;
   }
   // FP32 element math with FP64 nodal state (see akb_precision)
   void initFullMixedPrecision() { check(akb_model_load_and_init_mixed()); }
@@ -409,9 +509,9 @@ public:
     return materials_[i];
   }
   Material &getMaterial(const ID &name) {
-    for (Int i = 0; i < getNbMaterials(); ++i)
-      if (getMaterial(i).getName() == name) return getMaterial(i);
-    throw Exception(AKB_EMATERIAL, "no material named " + name);
+    const Int i = getMaterialIndex(name);
+    if (i < 0) throw Exception(AKB_EMATERIAL, "no material named " + name);
+    return getMaterial(i);
   }
 
   Int getSpatialDimension() const { return dim_; }
@@ -439,7 +539,15 @@ private:
       int rc = akb_model_load_materials(h_, text.c_str());
       if (rc != AKB_OK) return rc;
     }
+    applySelector();
     return akb_model_init_full(h_, AKB_EXPLICIT_LUMPED_MASS, AKB_PRECISION_MIXED);
+  }
+
+  void applySelector() {
+    if (!selector_) return;
+    std::vector<Idx> mat((size_t)mesh_.getNbElement());
+    for (size_t e = 0; e < mat.size(); ++e) mat[e] = (*selector_)(Element{mesh_.getElementType(), (Idx)e});
+    setElementMaterials(mat);
   }
 
   Array<Real> &nodal(int field, bool writable) {
@@ -461,8 +569,38 @@ private:
   std::set<int> handed_out_;
   std::unique_ptr<Array<bool>> blocked_;
   bool blocked_dirty_ = false;
-  std::vector<Material> materials_;
+  std::deque<Material> materials_;  // references stay valid as it grows
+  std::shared_ptr<MaterialSelector> selector_;
+  std::vector<Idx> element_materials_;
 };
+
+template <typename T> Idx ElementDataMaterialSelector<T>::operator()(const Element &element) {
+  if (element.element < 0 || (size_t)element.element >= data_.size())
+    return MaterialSelector::operator()(element);
+  if constexpr (std::is_same_v<T, std::string>) {
+    const Int i = model_->getMaterialIndex(data_[element.element]);
+    return i >= 0 ? (Idx)i : MaterialSelector::operator()(element);
+  } else {
+    return (Idx)data_[element.element];
+  }
+}
+
+template <typename T>
+MeshDataMaterialSelector<T>::MeshDataMaterialSelector(const ID &name, SolidMechanicsModel &model,
+                                                      Idx first_index)
+    : ElementDataMaterialSelector<T>(model.getMesh().template getData<T>(name), model,
+                                     first_index) {}
+
+inline Array<Idx> Material::getElementFilter(ElementType) const {
+  const auto &mat = model_->getElementMaterials();
+  Int n = 0;
+  for (Idx m : mat) n += m == index_;
+  Array<Idx> out(n, 1);
+  Int k = 0;
+  for (size_t e = 0; e < mat.size(); ++e)
+    if (mat[e] == index_) out(k++, 0) = (Idx)e;
+  return out;
+}
 
 inline Real Material::get(const ID &param) const {
   Real v = 0;

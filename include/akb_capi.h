@@ -116,6 +116,14 @@ int akb_mesh_copy(const akb_mesh *mesh, double *nodes, int32_t *connectivity,
 int akb_mesh_nb_groups(const akb_mesh *mesh, int *count);
 int akb_mesh_group(const akb_mesh *mesh, int k, char *name, size_t name_size, int *dimension,
                    int64_t *nb_nodes, int32_t *nodes);
+/* the "physical_names" element data of the read type (mesh_io_msh.cc:669-676,
+ * mesh_io.cc:89-113, read by MeshDataMaterialSelector<std::string>): count =
+ * the number of distinct names, -1 when the file gives none (format 2 without
+ * $PhysicalNames); akb_mesh_element_names copies name k and/or, for each
+ * element, the index of its name [E] */
+int akb_mesh_nb_element_names(const akb_mesh *mesh, int *count);
+int akb_mesh_element_names(const akb_mesh *mesh, int k, char *name, size_t name_size,
+                           int32_t *name_of_element);
 void akb_mesh_free(akb_mesh *mesh);
 
 /* ---- model --------------------------------------------------------------- */

@@ -202,3 +202,173 @@ def test_cpp_mesh_read_groups(tmp_path):
     out = subprocess.run([str(exe), str(p)], check=True, capture_output=True,
                          text=True).stdout.split()
     assert [int(v) for v in out] == [len(x), len(conn), len(x), int(np.sum(x[:, 2] == 0)), 1]
+
+
+# -- material selection by physical name ------------------------------------------
+REGIONS = {1: "steel", 2: "rubber", 3: "glass"}  # physical tag 4 has no name
+
+
+def write_regions(path, version):
+    """a row of 8 hexahedra in four volume entities (physical tags 1 2 3 4,
+    two elements each): element k lies in entity k // 2 + 1"""
+    mesh = akb.box_hex8(8, 1, 1)
+    x, conn = mesh.nodes, mesh.connectivity
+    fmt = lambda v: " ".join("%.17g" % c for c in v)
+    out = ["$MeshFormat", f"{version} 0 8", "$EndMeshFormat",
+           "$PhysicalNames", str(len(REGIONS))]
+    out += [f'3 {t} "{n}"' for t, n in REGIONS.items()] + ["$EndPhysicalNames"]
+    if version == "2.2":
+        out += ["$Nodes", str(len(x))] + [f"{i + 1} {fmt(x[i])}" for i in range(len(x))]
+        out += ["$EndNodes", "$Elements", str(len(conn))]
+        out += [f"{k + 1} 5 2 {k // 2 + 1} {k // 2 + 1} " + " ".join(str(n + 1) for n in c)
+                for k, c in enumerate(conn)]
+    else:
+        out += ["$Entities", "0 0 0 4"]
+        out += [f"{t} 0 0 0 1 1 1 1 {t} 0" for t in range(1, 5)] + ["$EndEntities"]
+        out += ["$Nodes", f"1 {len(x)} 1 {len(x)}", f"3 1 0 {len(x)}"]
+        out += [str(i + 1) for i in range(len(x))] + [fmt(v) for v in x] + ["$EndNodes"]
+        out += ["$Elements", f"4 {len(conn)} 1 {len(conn)}"]
+        for t in range(1, 5):
+            out.append(f"3 {t} 5 2")
+            out += [f"{k + 1} " + " ".join(str(n + 1) for n in conn[k])
+                    for k in (2 * t - 2, 2 * t - 1)]
+    out += ["$EndElements"]
+    path.write_text("\n".join(out) + "\n")
+
+
+def _model_with_materials(mesh):
+    model = akb.SolidMechanicsModel(mesh)
+    for name, E in (("steel", 2.0), ("rubber", 0.5), ("glass", 1.5)):
+        model.addMaterial("elastic", name=name, rho=1.0, E=E, nu=0.3)
+    return model
+
+
+@pytest.mark.parametrize("version", ["2.2", "4.1"])
+def test_physical_names_data(tmp_path, version):
+    p = tmp_path / "regions.msh"
+    write_regions(p, version)
+    mesh = akb.Mesh(3).read(p)
+    names = list(mesh.getData("physical_names"))
+    unnamed = "4" if version == "2.2" else ""  # format 4 leaves it empty
+    assert names == ["steel"] * 2 + ["rubber"] * 2 + ["glass"] * 2 + [unnamed] * 2
+    assert list(mesh.getData("tag_0")) == [1, 1, 2, 2, 3, 3, 4, 4]
+
+
+def test_no_physical_names_data_in_format_2(tmp_path):
+    p = tmp_path / "box.msh"
+    write_msh(p, "2.2", names=False)
+    mesh = akb.Mesh(3).read(p)
+    with pytest.raises(KeyError):
+        mesh.getData("physical_names")
+
+
+@pytest.mark.parametrize("version", ["2.2", "4.1"])
+def test_mesh_data_material_selector(tmp_path, version):
+    p = tmp_path / "regions.msh"
+    write_regions(p, version)
+    model = _model_with_materials(akb.Mesh(3).read(p))
+    sel = akb.MeshDataMaterialSelector("physical_names", model)
+    # the unnamed region names no material: the fallback value, then a
+    # fallback selector
+    assert list(sel.select(model)) == [0, 0, 1, 1, 2, 2, 0, 0]
+    sel.setFallback(2)
+    assert list(sel.select(model)) == [0, 0, 1, 1, 2, 2, 2, 2]
+    by_tag = akb.MeshDataMaterialSelectorInt("tag_0", model)
+    assert list(by_tag.select(model)) == [1, 1, 2, 2, 3, 3, 4, 4]
+    fb = akb.ElementDataMaterialSelector(np.array([1, 1, 1, 1, 1, 1, 2, 1]))
+    sel.setFallback(fb)
+    assert list(sel.select(model)) == [0, 0, 1, 1, 2, 2, 2, 1]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("version", ["2.2", "4.1"])
+def test_selector_at_init_full(tmp_path, version):
+    """initFull applies the selector: each material holds its region's
+    elements, and the run is bit-identical to one given the same element
+    materials directly"""
+    p = tmp_path / "regions.msh"
+    write_regions(p, version)
+    runs = []
+    for use_selector in (True, False):
+        mesh = akb.Mesh(3).read(p)
+        model = _model_with_materials(mesh)
+        if use_selector:
+            model.setMaterialSelector(akb.MeshDataMaterialSelector("physical_names", model))
+        else:
+            model.setElementMaterials([0, 0, 1, 1, 2, 2, 0, 0])
+        model.initFull(_analysis_method=akb._explicit_lumped_mass)
+        if use_selector:
+            assert list(model.getMaterial("steel").getElementFilter()) == [0, 1, 6, 7]
+            assert list(model.getMaterial("rubber").getElementFilter()) == [2, 3]
+            assert list(model.getMaterial("glass").getElementFilter()) == [4, 5]
+        x = mesh.nodes
+        model.getBlockedDOFs()[x[:, 0] == 0.0] = True
+        model.getVelocity()[:, 0] = 0.01 * x[:, 0]
+        model.setTimeStep(0.5 * model.getStableTimeStep())
+        model.solveStep(50)
+        runs.append(model.getDisplacement().copy())
+    assert np.array_equal(runs[0], runs[1])
+    assert np.abs(runs[0]).max() > 0
+
+
+CPP_SELECTOR = r"""
+#include <akantu_b200/solid_mechanics_model.hh>
+#include <cstdio>
+#include <cstring>
+using namespace akantu_b200;
+int main(int argc, char **argv) {
+  Mesh mesh(3);
+  mesh.read(argv[1]);
+  for (const auto &n : mesh.getData<std::string>("physical_names")) std::printf("[%s]", n.c_str());
+  for (Idx t : mesh.getData<Idx>("tag_0")) std::printf(" %d", (int)t);
+  std::printf("\n");
+  if (argc < 3) return 0;
+  initialize(argv[2], argc, argv);
+  SolidMechanicsModel model(mesh);
+  auto selector = std::make_shared<MeshDataMaterialSelector<std::string>>("physical_names", model);
+  model.setMaterialSelector(selector);
+  model.initFull(_analysis_method = _explicit_lumped_mass);
+  for (const char *name : {"steel", "rubber", "glass"}) {
+    auto filter = model.getMaterial(name).getElementFilter(_hexahedron_8);
+    std::printf("%s", name);
+    for (Int k = 0; k < filter.size(); ++k) std::printf(" %d", (int)filter(k, 0));
+    std::printf("\n");
+  }
+  return 0;
+}
+"""
+
+DAT = "".join(f"material elastic [\n  name = {n}\n  rho = 1\n  E = {E}\n  nu = 0.3\n]\n"
+              for n, E in (("steel", 2.0), ("rubber", 0.5), ("glass", 1.5)))
+
+
+def _build_selector_example(tmp_path):
+    src = tmp_path / "selector.cc"
+    src.write_text(CPP_SELECTOR)
+    exe = tmp_path / "selector"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-L",
+                    os.path.join(ROOT, "akantu2_b200"), "-lakb",
+                    "-Wl,-rpath," + os.path.join(ROOT, "akantu2_b200"), "-o", str(exe)],
+                   check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_cpp_mesh_data(tmp_path):
+    exe = _build_selector_example(tmp_path)
+    p = tmp_path / "regions.msh"
+    write_regions(p, "4.1")
+    out = subprocess.run([str(exe), str(p)], check=True, capture_output=True, text=True).stdout
+    assert out.strip() == "[steel][steel][rubber][rubber][glass][glass][][] 1 1 2 2 3 3 4 4"
+
+
+@pytest.mark.gpu
+def test_cpp_selector_at_init_full(tmp_path):
+    exe = _build_selector_example(tmp_path)
+    p = tmp_path / "regions.msh"
+    write_regions(p, "2.2")
+    dat = tmp_path / "materials.dat"
+    dat.write_text(DAT)
+    out = subprocess.run([str(exe), str(p), str(dat)], check=True, capture_output=True,
+                         text=True).stdout.splitlines()
+    assert out[1:] == ["steel 0 1 6 7", "rubber 2 3", "glass 4 5"]
