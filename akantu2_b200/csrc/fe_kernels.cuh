@@ -776,17 +776,34 @@ __device__ __forceinline__ void hex8_geometry_modes(int64_t e, int64_t E, const 
   wht8(wx);
 }
 
+// the Jacobian adjugate and 1/det of a parallelepiped from its geometry
+// modes (wx after wht8: modes 1, 2 and 4 are 8 dX/dxi, 8 dX/deta, 8 dX/dzeta)
+__device__ __forceinline__ float hex8_affine_adjugate(const float (*wx)[3], float *Ja) {
+  float Jp[9];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    Jp[0 + 3 * j] = wx[1][j];
+    Jp[1 + 3 * j] = wx[2][j];
+    Jp[2 + 3 * j] = wx[4][j];
+  }
+  return 1.f / adj3(Jp, Ja);
+}
+
 // QU: quadrature points per unrolled iteration (1, 2, 4 or 8).  AFF: every
 // element of the launch is a parallelepiped (checked once per mesh), so the
 // per-point geometry and its registers are compiled out; the same arithmetic
-// as the general kernel's affine branch
-template <int LAW, int QU, bool AFF = false>
+// as the general kernel's affine branch.  GEO (with AFF): the adjugate and
+// 1/det of each element are read from geo [10][E], formed once by
+// k_hex8_affine_geometry with the same arithmetic, instead of gathering the
+// element's coordinates every step
+template <int LAW, int QU, bool AFF = false, bool GEO = false>
 __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int64_t e_count,
                                                int64_t E, const int32_t *conn,
                                                const int32_t *pos,
-                                               const double *X,
+                                               const double *X, const float *geo,
                                                const double *u, const MatParams &mp,
                                                const GroupArgs &ps, float *re) {
+  static_assert(AFF || !GEO, "the geometry table holds parallelepipeds only");
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
   // reference node a sits at lexicographic corner lex[a] = [sx>0] + 2[sy>0] + 4[sz>0]
@@ -798,22 +815,32 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
     const int64_t node = conn[(int64_t)a * E + e];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const double x = X[node * 3 + i], uu = u[node * 3 + i];
-      if (a == 0) {
-        x0[i] = x;
-        u0[i] = uu;
-      }
-      wx[lex[a]][i] = (float)(x - x0[i]);
+      const double uu = u[node * 3 + i];
+      if (a == 0) u0[i] = uu;
       wu[lex[a]][i] = (float)(uu - u0[i]);
+      if constexpr (!GEO) {
+        const double x = X[node * 3 + i];
+        if (a == 0) x0[i] = x;
+        wx[lex[a]][i] = (float)(x - x0[i]);
+      }
     }
   }
-  wht8(wx);
+  float Ja[9], rdet_a = 0.f;
+  if constexpr (GEO) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ja[k] = geo[(int64_t)k * E + e];
+    rdet_a = geo[(int64_t)9 * E + e];
+  } else {
+    wht8(wx);
+  }
   wht8(wu);
   constexpr float g1 = 0.577350269189625764509f;  // Gauss coordinate 1/sqrt(3)
   constexpr float g2 = 1.f / 3.f;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    wx[3][c] *= g1; wx[5][c] *= g1; wx[6][c] *= g1; wx[7][c] *= g2;
+    if constexpr (!GEO) {
+      wx[3][c] *= g1; wx[5][c] *= g1; wx[6][c] *= g1; wx[7][c] *= g2;
+    }
     wu[3][c] *= g1; wu[5][c] *= g1; wu[6][c] *= g1; wu[7][c] *= g2;
   }
   float A[8][3];
@@ -831,17 +858,8 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
     for (int c = 0; c < 3; ++c)
       affine = affine && wx[3][c] == 0.f && wx[5][c] == 0.f && wx[6][c] == 0.f && wx[7][c] == 0.f;
   }
-  float Ja[9], rdet_a = 0.f;
-  if (affine) {
-    float Jp[9];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      Jp[0 + 3 * j] = wx[1][j];
-      Jp[1 + 3 * j] = wx[2][j];
-      Jp[2 + 3 * j] = wx[4][j];
-    }
-    rdet_a = 1.f / adj3(Jp, Ja);
-  }
+  if constexpr (!GEO)
+    if (affine) rdet_a = hex8_affine_adjugate(wx, Ja);
 #pragma unroll 1
   for (int qo = 0; qo < 8; qo += QU)
 #pragma unroll
@@ -862,7 +880,7 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
 #pragma unroll
       for (int k = 0; k < 9; ++k) Ji[k] = Ja[k];
       rdet = rdet_a;
-    } else {
+    } else if constexpr (!AFF) {
       // 8 d(X_j)/d(xi_k) at row k
       float Jp[9];
 #pragma unroll
@@ -915,16 +933,17 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
 
 // MINB: blocks per SM the register allocation must allow (1: the compiler's
 // choice)
-template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false>
+template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false, bool GEO = false>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                            const double *__restrict__ X, const double *__restrict__ u,
-                            MatParams mp, GroupArgs ps, float *__restrict__ re) {
+                            const double *__restrict__ X, const float *__restrict__ geo,
+                            const double *__restrict__ u, MatParams mp, GroupArgs ps,
+                            float *__restrict__ re) {
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count) return;
-  element_hex8sf<LAW, QU, AFF>(le, e_begin, e_count, E, conn, pos, X, u, mp, ps, re);
+  element_hex8sf<LAW, QU, AFF, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
 }
 
 // FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q
@@ -1403,7 +1422,7 @@ __global__ void __launch_bounds__(kPersistentThreads)
         element_geo<D, NN, NQ, LAW>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, tab, up, mp, ps,
                                     reinterpret_cast<float *>(re));
       else
-        element_hex8sf<LAW, QU>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, up, mp, ps,
+        element_hex8sf<LAW, QU>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, nullptr, up, mp, ps,
                                 reinterpret_cast<float *>(re));
     }
     if (!grid_barrier(sa.bar, ++gen, sa.status)) return;

@@ -7,56 +7,63 @@ namespace akb {
 
 namespace {
 
-template <int LAW, int BLOCK, int QU, int MINB = 1, bool AFF = false>
+template <int LAW, int BLOCK, int QU, int MINB = 1, bool AFF = false, bool GEO = false>
 void launch_hex8sf(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
                    const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
   const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-  launch_step(g.pdl, k_element_forces_hex8sf<LAW, BLOCK, QU, MINB, AFF>, grid, BLOCK, s, e0, ne,
-              g.E, g.conn, g.pos, g.X, u, mp, ps, re);
+  launch_step(g.pdl, k_element_forces_hex8sf<LAW, BLOCK, QU, MINB, AFF, GEO>, grid, BLOCK, s, e0,
+              ne, g.E, g.conn, g.pos, g.X, g.geo, u, mp, ps, re);
 }
 
 // the shapes of the sum-factorised kernel: 64, 128 or 256 threads with 8 or
 // 2 points per iteration, 128 threads with 1
-template <int LAW, int QU, bool AFF>
+template <int LAW, int QU, bool AFF, bool GEO>
 void dispatch_hex8sf_block(int block, const DevGeom &g, int64_t e0, int64_t ne,
                            const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                            cudaStream_t s) {
   if (block == 64)
-    launch_hex8sf<LAW, 64, QU, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 64, QU, 1, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   else if (block == 256)
-    launch_hex8sf<LAW, 256, QU, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 256, QU, 1, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   else
-    launch_hex8sf<LAW, 128, QU, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, QU, 1, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
 }
-template <int LAW, bool AFF>
+template <int LAW, bool AFF, bool GEO>
 void dispatch_hex8sf(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
                      const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                      cudaStream_t s) {
-  // 128 threads with the registers capped for 5 resident blocks (20 warps)
-  if (tn.minb == 5 && tn.qu == 1)
-    launch_hex8sf<LAW, 128, 1, 5, AFF>(g, e0, ne, u, mp, ps, re, s);
+  // 128 threads with the registers capped for 6 or 5 resident blocks (24 or
+  // 20 warps)
+  if (tn.minb == 6 && tn.qu == 1)
+    launch_hex8sf<LAW, 128, 1, 6, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.minb == 6 && tn.qu == 2)
+    launch_hex8sf<LAW, 128, 2, 6, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
+  else if (tn.minb == 5 && tn.qu == 1)
+    launch_hex8sf<LAW, 128, 1, 5, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.minb == 5 && tn.qu == 2)
-    launch_hex8sf<LAW, 128, 2, 5, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 2, 5, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.minb == 5)
-    launch_hex8sf<LAW, 128, 8, 5, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 8, 5, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   // 128 threads capped at 128 registers for 4 resident blocks (16 warps)
   else if (tn.minb == 4 && tn.qu == 2)
-    launch_hex8sf<LAW, 128, 2, 4, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 2, 4, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 1)
-    launch_hex8sf<LAW, 128, 1, 1, AFF>(g, e0, ne, u, mp, ps, re, s);
+    launch_hex8sf<LAW, 128, 1, 1, AFF, GEO>(g, e0, ne, u, mp, ps, re, s);
   else if (tn.qu == 2)
-    dispatch_hex8sf_block<LAW, 2, AFF>(tn.block, g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf_block<LAW, 2, AFF, GEO>(tn.block, g, e0, ne, u, mp, ps, re, s);
   else
-    dispatch_hex8sf_block<LAW, 8, AFF>(tn.block, g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf_block<LAW, 8, AFF, GEO>(tn.block, g, e0, ne, u, mp, ps, re, s);
 }
 template <int LAW>
 void dispatch_hex8sf_mesh(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
                           const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                           cudaStream_t s) {
-  if (g.affine)
-    dispatch_hex8sf<LAW, true>(tn, g, e0, ne, u, mp, ps, re, s);
+  if (g.affine && g.geo)
+    dispatch_hex8sf<LAW, true, true>(tn, g, e0, ne, u, mp, ps, re, s);
+  else if (g.affine)
+    dispatch_hex8sf<LAW, true, false>(tn, g, e0, ne, u, mp, ps, re, s);
   else
-    dispatch_hex8sf<LAW, false>(tn, g, e0, ne, u, mp, ps, re, s);
+    dispatch_hex8sf<LAW, false, false>(tn, g, e0, ne, u, mp, ps, re, s);
 }
 
 // a hexahedron is a parallelepiped when its bilinear and trilinear geometry
@@ -74,6 +81,20 @@ __global__ void k_hex8_affine(int64_t E, const int32_t *__restrict__ conn,
     affine = affine && wx[3][c] * g1 == 0.f && wx[5][c] * g1 == 0.f && wx[6][c] * g1 == 0.f &&
              wx[7][c] * g2 == 0.f;
   if (!affine) atomicOr(flag, 1u);
+}
+
+// the adjugate and 1/det of every element of a mesh of parallelepipeds, into
+// geo [10][E]: the values the element kernel forms from the same modes
+__global__ void k_hex8_affine_geometry(int64_t E, const int32_t *__restrict__ conn,
+                                       const double *__restrict__ X, float *__restrict__ geo) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  float wx[8][3], Ja[9];
+  hex8_geometry_modes(e, E, conn, X, wx);
+  const float rdet = hex8_affine_adjugate(wx, Ja);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) geo[(int64_t)k * E + e] = Ja[k];
+  geo[(int64_t)9 * E + e] = rdet;
 }
 
 }  // namespace
@@ -166,6 +187,12 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
   return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
                      fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
                      flags, status);
+}
+
+cudaError_t launch_hex8_affine_geometry(const DevGeom &g, float *geo, cudaStream_t s) {
+  if (g.E == 0) return cudaSuccess;
+  k_hex8_affine_geometry<<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X, geo);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_hex8_affine_check(const DevGeom &g, unsigned int *flag, cudaStream_t s) {

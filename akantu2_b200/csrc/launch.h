@@ -44,6 +44,8 @@ struct DevGeom {
   // every element is a parallelepiped (mixed hexahedra: the element kernel
   // compiled without per-point geometry)
   int affine = 0;
+  // with affine: the adjugate and 1/det of each element [10][E], or null
+  const float *geo = nullptr;
 };
 
 // ---- init ------------------------------------------------------------------
@@ -147,5 +149,7 @@ cudaError_t launch_halo(bool unpack, int d, int64_t n, const int32_t *idx, doubl
 cudaError_t launch_history(const DevGeom &g, const double *u_n, const double *u_np1,
                            double *prev, double *incr, cudaStream_t s);
 // flag = 1 if some hexahedron is not a parallelepiped (FP32 modal test)
+// adjugate and 1/det of every element of a mesh of parallelepipeds, [10][E]
+cudaError_t launch_hex8_affine_geometry(const DevGeom &g, float *geo, cudaStream_t s);
 cudaError_t launch_hex8_affine_check(const DevGeom &g, unsigned int *flag, cudaStream_t s);
 }  // namespace akb

@@ -250,8 +250,11 @@ struct akb_model {
   int node_block = 128;       // threads per block of the node update
   bool node_staged = false;   // gather staged through shared memory
   // mixed hexahedra: every element a parallelepiped (found at initFull), and
-  // the kernel compiled for such meshes in use
-  bool all_affine = false, affine_kernel = false;
+  // the kernel in use: 0 the general one, 1 the one compiled for such meshes,
+  // 2 the same reading each element's adjugate and 1/det from dgeo [10][E]
+  bool all_affine = false;
+  int affine_kernel = 0;
+  float *dgeo = nullptr;
   // previous displacement and increment of the last step, when tracked
   bool track_history = false;
   double *dprev = nullptr, *dincr = nullptr;
@@ -282,6 +285,7 @@ struct akb_model {
     g.inst_dt = dinst_dt;
     g.pdl = pdl ? 1 : 0;
     g.affine = affine_kernel ? 1 : 0;
+    g.geo = affine_kernel == 2 ? dgeo : nullptr;
     return g;
   }
   // stream-ordered allocations on the model's stream: neither allocating
@@ -1074,13 +1078,20 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, s));
     AKB_CUDA(cudaStreamSynchronize(s));
     m->all_affine = h == 0;
-    m->affine_kernel = m->all_affine;
+    m->affine_kernel = 0;
     // without per-point geometry the kernel fits 5 blocks per SM without
     // spilling: the fastest shape for the elastic and neohookean laws
-    // (measured on the 128^3 box: 11 % and 7 % shorter launches)
-    if (m->all_affine)
+    // (measured on the 128^3 box: 11 % and 7 % shorter launches).  Reading
+    // each element's adjugate and 1/det from a table formed here, instead of
+    // gathering its coordinates every step, shortens the neohookean launch
+    // by a further 4 % for 40 bytes per element
+    if (m->all_affine) {
+      AKB_TRY(m->alloc(&m->dgeo, sizeof(float) * 10 * m->E));
+      AKB_CUDA(launch_hex8_affine_geometry(g, m->dgeo, s));
+      m->affine_kernel = 2;
       for (auto &gr : m->groups)
         if (gr.law != LAW_PLASTIC) gr.tune.minb = 5;
+    }
   }
   const size_t gu_size = precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
   for (auto &mt : m->groups) {
@@ -1575,6 +1586,8 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   if (law == LAW_PLASTIC)
     t += 2 * (2 * r(8 * E * nq * ns) + r(gs * E * nq * d * d) + r(8 * E * nq)) + r(8 * E * nq);
   if (law == LAW_NEOHOOKEAN && d == 2) t += r(8 * E * nq);  // plane-stress C33
+  // mixed hexahedra: the adjugate table of a mesh of parallelepipeds
+  if (precision == AKB_PRECISION_MIXED && et == AKB_HEXAHEDRON_8) t += r(4 * 10 * E);
   *bytes = t;
   return AKB_OK;
 }
@@ -1724,6 +1737,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
     if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
       const int q = gr.tune.qu;
       cand = {{128, q, 1}, {128, q, 5}};
+      if (q == 1 || q == 2) cand.push_back({128, q, 6});
       if (q != 1) cand.insert(cand.end(), {{64, q, 1}, {256, q, 1}});
       if (q == 2) cand.push_back({128, q, 4});
       if (q == 0) cand = {{128, 0, 1}, {64, 0, 1}, {256, 0, 1}};
@@ -1867,11 +1881,16 @@ int akb_model_set_increment_tracking(akb_model *m, int on) {
 
 int akb_model_set_affine_kernel(akb_model *m, int on) {
   AKB_TRY(check_model(m, true));
+  if (on < 0 || on > 2) return fail(AKB_EINVAL, "affine kernel mode is 0, 1 or 2");
   if (on && !m->all_affine)
     return fail(AKB_EUNSUPPORTED, "the mesh is not made of parallelepipeds only (or is not a "
                                   "mixed-precision hexahedral mesh)");
+  if (on == 2 && !m->dgeo) {
+    AKB_TRY(m->alloc(&m->dgeo, sizeof(float) * 10 * m->E));
+    AKB_CUDA(launch_hex8_affine_geometry(m->geom(), m->dgeo, m->stream));
+  }
   AKB_CUDA(cudaStreamSynchronize(m->stream));
-  m->affine_kernel = on != 0;
+  m->affine_kernel = on;
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
   return AKB_OK;
@@ -1879,7 +1898,7 @@ int akb_model_set_affine_kernel(akb_model *m, int on) {
 
 int akb_model_get_affine_kernel(const akb_model *m, int *on) {
   if (!m || !on) return fail(AKB_EINVAL, "null argument");
-  *on = m->affine_kernel ? 1 : 0;
+  *on = m->affine_kernel;
   return AKB_OK;
 }
 
@@ -1936,13 +1955,14 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   if (sf && q == 1 && element_block != 128)
     return fail(AKB_EINVAL, "1 point per iteration runs with 128 threads");
   const bool capped_sf = sf && q != 0 && element_block == 128 &&
-                         (min_blocks == 5 || (min_blocks == 4 && q == 2));
+                         (min_blocks == 5 || (min_blocks == 4 && q == 2) ||
+                          (min_blocks == 6 && (q == 1 || q == 2)));
   const bool capped_plastic = m->et != AKB_HEXAHEDRON_8 && law == LAW_PLASTIC &&
                               (min_blocks == 5 || min_blocks == 6) && element_block == 128;
   if (min_blocks != 1 && !capped_sf && !capped_plastic)
-    return fail(AKB_EINVAL, "min_blocks is 1; 5 (or 4 with 2 points per iteration) for the "
-                            "128-thread mixed hexahedron kernel; 5 or 6 for 128-thread plastic "
-                            "tetrahedra and triangles");
+    return fail(AKB_EINVAL, "min_blocks is 1; 5 (or 4 with 2 points per iteration, 6 with 1 or "
+                            "2) for the 128-thread mixed hexahedron kernel; 5 or 6 for "
+                            "128-thread plastic tetrahedra and triangles");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   bool found = false;

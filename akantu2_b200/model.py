@@ -347,14 +347,17 @@ class SolidMechanicsModel:
 
     def setAffineKernel(self, on=True):
         """Mixed hexahedra of a mesh of parallelepipeds: the element kernel
-        compiled without per-point geometry (the default for such meshes) or
-        the general one; the same numbers either way."""
-        _capi.check(_capi.lib().akb_model_set_affine_kernel(self._h, int(bool(on))))
+        compiled without per-point geometry (True or 1), the same reading each
+        element's adjugate and 1/det from a table formed once (2), or the
+        general kernel (False or 0); the same numbers in every mode."""
+        mode = on if isinstance(on, int) and not isinstance(on, bool) else int(bool(on))
+        _capi.check(_capi.lib().akb_model_set_affine_kernel(self._h, mode))
 
     def getAffineKernel(self):
+        """0 (general kernel), 1 or 2 (the modes of setAffineKernel)"""
         on = ctypes.c_int()
         _capi.check(_capi.lib().akb_model_get_affine_kernel(self._h, ctypes.byref(on)))
-        return bool(on.value)
+        return on.value
 
     def setIncrementTracking(self, on=True):
         """Keep the displacement each step starts from and its increment

@@ -308,8 +308,8 @@ int akb_model_autotune(akb_model *model, int repeats);
  * sum-factorised one (not bit-identical to it: a different FP32 evaluation);
  * min_blocks is 1 except for 128-thread kernels that cap their registers
  * for that many resident blocks per SM: 5 for the mixed hexahedron kernel
- * (or 4 with 2 points per iteration), 5 or 6 for plastic tetrahedra and
- * triangles (same results) */
+ * (4 with 2 points per iteration, 6 with 1 or 2), 5 or 6 for plastic
+ * tetrahedra and triangles (same results) */
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
@@ -328,9 +328,11 @@ int akb_model_get_node_shape(const akb_model *model, int *node_block, int *stage
 int akb_model_set_increment_tracking(akb_model *model, int on);
 /* mixed-precision hexahedra: a mesh made of parallelepipeds only (found at
  * init_full; structured and voxel meshes) runs an element kernel compiled
- * without per-point geometry, which needs fewer registers; on = 0 returns to
- * the general kernel.  Both compute the same numbers.  AKB_EUNSUPPORTED for
- * other meshes. */
+ * without per-point geometry, which needs fewer registers (on = 1); on = 2
+ * also forms each element's Jacobian adjugate and 1/det once, into a table
+ * of 40 bytes per element that the kernel streams instead of gathering the
+ * element's coordinates every step; on = 0 returns to the general kernel.
+ * All three compute the same numbers.  AKB_EUNSUPPORTED for other meshes. */
 int akb_model_set_affine_kernel(akb_model *model, int on);
 int akb_model_get_affine_kernel(const akb_model *model, int *on);
 /* on = 1 launches the step kernels with programmatic stream serialization:

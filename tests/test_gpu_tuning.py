@@ -314,17 +314,20 @@ def test_plastic_register_caps_are_bit_identical(etype, precision):
 @pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC])
 def test_affine_kernel_is_bit_identical(mat):
     """a box of parallelepipeds runs the element kernel compiled without
-    per-point geometry by default; the general kernel computes the same
-    numbers in every launch shape"""
+    per-point geometry by default; that kernel reading the geometry table
+    (mode 2) and the general kernel compute the same numbers in every launch
+    shape"""
     mesh = akb.box_hex8(5, 4, 6, lengths=(1.0, 0.7, 1.3))
     v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
     mat = dict(mat, sigma_y=2e-3) if "sigma_y" in mat else mat
     runs = []
-    for affine in (True, False):
-        for shape in ((128, 2, 4), (128, 2, 5), (128, 1, 5), (128, 8, 1)):
+    for affine in (2, 1, 0):
+        for shape in ((128, 2, 4), (128, 2, 5), (128, 2, 6), (128, 1, 5), (128, 1, 6),
+                      (128, 8, 1)):
             m = gpu_model(mesh, [mat], precision="mixed")
-            assert m.getAffineKernel()
+            assert m.getAffineKernel() in (1, 2)
             m.setAffineKernel(affine)
+            assert m.getAffineKernel() == affine
             m.setLaunchShape(mat["type"], shape[0], shape[1], 128, shape[2])
             m.setNodal("velocity", v0)
             m.setNodal("blocked_dofs", bl)
@@ -343,7 +346,8 @@ def test_affine_kernel_only_for_parallelepipeds():
     mesh.nodes[np.all((mesh.nodes > 0.1) & (mesh.nodes < 0.9), axis=1)] += 0.01
     m = gpu_model(mesh, [UNIT_ELASTIC], precision="mixed")
     assert not m.getAffineKernel()
-    with pytest.raises(akb.AkbError):
-        m.setAffineKernel(True)
+    for mode in (True, 2):
+        with pytest.raises(akb.AkbError):
+            m.setAffineKernel(mode)
     assert not gpu_model(akb.box_hex8(3), [UNIT_ELASTIC], precision="fp64").getAffineKernel()
     assert not gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision="mixed").getAffineKernel()
