@@ -15,7 +15,8 @@ dt = 0.8 x stable.  One step = one central-difference step of the whole mesh.
   fp64       the same for the plain FP64 path
   e2e        through the C ABI with host buffers: every step uploads the
              external force from pinned memory, runs the step and reads the
-             displacement back (wall clock, synchronised)
+             displacement back (wall clock, synchronised); pcie_bound: the
+             same two copies alone, issued together, as the floor of that step
   roofline   element-force kernel: algorithmic bytes / its event-timed duration
   cpu_baseline  the CPU oracle (restatement of the reference path) on the host
              cores, bounded sample of the same workload
@@ -507,7 +508,8 @@ def run_ours(args):
                                             "and its displacement read back through the async "
                                             "C ABI, each result waited for one step later, all "
                                             "copies complete inside the timed region",
-                                    "synchronous_value": world * E * k_e2e / secs_sync}
+                                    "synchronous_value": world * E * k_e2e / secs_sync,
+                                    "pcie_bound": e2e_bound(nb, nb, secs_async, k_e2e)}
         del m
     head = results[precisions[0]]
     accuracy = None
@@ -615,6 +617,48 @@ def e2e_legs(m, shape, k, barrier):
     return secs_sync, secs_async
 
 
+def pcie_bound(h2d_bytes, d2h_bytes, reps=20):
+    """The end-to-end leg's copy floor on this box: one host-to-device and
+    one device-to-host copy of the step's sizes, pinned, issued together on
+    two streams, timed with CUDA events; milliseconds per pair."""
+    import torch
+    h = [torch.empty(b, dtype=torch.uint8, pin_memory=True) for b in (h2d_bytes, d2h_bytes)]
+    d = [torch.empty(b, dtype=torch.uint8, device="cuda") for b in (h2d_bytes, d2h_bytes)]
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    main = torch.cuda.current_stream()
+
+    def pairs(n):
+        up.wait_stream(main)
+        down.wait_stream(main)
+        for _ in range(n):
+            with torch.cuda.stream(up):
+                d[0].copy_(h[0], non_blocking=True)
+            with torch.cuda.stream(down):
+                h[1].copy_(d[1], non_blocking=True)
+        main.wait_stream(up)
+        main.wait_stream(down)
+
+    pairs(3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    pairs(reps)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def e2e_bound(nb_up, nb_down, secs, steps):
+    """the copy floor against the measured end-to-end step"""
+    floor = pcie_bound(nb_up, nb_down)
+    step_ms = 1e3 * secs / steps
+    return {"copy_pair_ms": floor, "step_ms": step_ms, "frac": floor / step_ms,
+            "gbs_per_direction": max(nb_up, nb_down) / floor / 1e6,
+            "how": "one pinned host-to-device and one device-to-host copy of the step's sizes "
+                   "issued together on two streams, CUDA-event timed: the floor of a step "
+                   "that moves both"}
+
+
 def accuracy_leg(akb, config, mesh, mat, v0, blocked, nsteps):
     """The mixed path against the plain FP64 path (bit-identical to the CPU
     oracle for elastic / plastic, within 1e-12 for neohookean) after nsteps
@@ -718,7 +762,8 @@ def run_batch(args):
                                     "steps": k_e2e, "h2d_bytes_per_step": nb,
                                     "d2h_bytes_per_step": nb,
                                     "mode": "pipelined async C ABI copies (see e2e_legs)",
-                                    "synchronous_value": world * E * k_e2e / secs_sync}
+                                    "synchronous_value": world * E * k_e2e / secs_sync,
+                                    "pcie_bound": e2e_bound(nb, nb, secs_async, k_e2e)}
         del b
     # unbatched baseline: every 16th instance alone (sizes spread over the
     # range), FP64, same step count with the same graphs
