@@ -95,7 +95,7 @@ def lib():
         "akb_model_assemble_internal_forces": (c_int, [vp]),
         "akb_model_get_energy": (c_int, [vp, ctypes.c_char_p, ctypes.POINTER(c_dbl)]),
         "akb_model_get_status": (c_int, [vp, ctypes.POINTER(c_int)]),
-        "akb_stable_time_step_noalloc": (c_int, [c_int, vp, vp, vp, i64, c_dbl, vp, vp]),
+        "akb_stable_time_step_noalloc": (c_int, [c_int, vp, vp, i64, vp, i64, c_dbl, vp, vp]),
         "akb_model_prepare_graphs": (c_int, [vp]),
         "akb_model_autotune": (c_int, [vp, c_int]),
         "akb_model_set_stream_priority": (c_int, [vp, c_int]),

@@ -475,25 +475,33 @@ int akb_server_destroy(akb_server *server);
  * material, for callers that cannot let the library call cudaMalloc: an
  * application whose device memory all comes from its own pool or arena, or
  * code computing the time step inside a loop where runtime allocation is not
- * allowed.  All arguments are device pointers owned by the caller:
- *   nodes, displacement  double [N][dim]; connectivity int32 [E][n] (the
- *   reference's node order); dt_out one double, receives min_e h_e / celerity
- *   (DBL_MAX when nb_elements == 0); stream a cudaStream_t (NULL: default).
+ * allowed.  All arrays are device pointers owned by the caller:
+ *   nodes, displacement  double [nb_nodes][dim]; connectivity int32 [E][n]
+ *   (the reference's node order); dt_out one double, receives
+ *   min_e h_e / celerity (DBL_MAX when nb_elements == 0); stream a
+ *   cudaStream_t (NULL: the default stream).
+ * Every connectivity index must lie in [0, nb_nodes).  An element with an
+ * index outside that range reads no node, and dt_out then receives NaN
+ * (the check runs on the device, so the call itself still returns AKB_OK).
+ * celerity must be finite and positive (AKB_EINVAL otherwise).
  * The work is enqueued on `stream`; synchronise it before reading dt_out.
- * The scratch (per-element values and reduction partials) is a file-scope
- * device array of AKB_NOALLOC_MAX_ELEMENTS + 1024 doubles (8 MiB) that every
- * GPU loading the library holds until the process exits; larger element
- * counts are rejected with AKB_EINVAL.  Every call shares that array and
- * overwrites all of it that it reads, so nothing carries over between calls,
- * but calls that overlap on the GPU (different streams, threads or
- * processes sharing the module) race on it.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress, with that device
- * current); make that first call before any stream capture begins. */
+ * The scratch (per-element values, reduction partials and the index-check
+ * word) is a file-scope device array of AKB_NOALLOC_MAX_ELEMENTS + 1025
+ * doubles (8 MiB) that every GPU loading the library holds until the
+ * process exits; larger element counts are rejected with AKB_EINVAL.  Every
+ * call shares that array and clears or overwrites all of it that it reads,
+ * so nothing carries over between calls, but calls that overlap on the GPU
+ * (different streams, threads or processes sharing the module) race on it.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current) and keeps it; make that
+ * first call before any stream capture begins.  cudaDeviceReset unloads the
+ * module and invalidates the kept address: do not call this entry point
+ * again in a process after resetting a device it ran on. */
 #define AKB_NOALLOC_MAX_ELEMENTS (1 << 20)
 int akb_stable_time_step_noalloc(int element_type, const double *nodes,
-                                 const double *displacement, const int32_t *connectivity,
-                                 int64_t nb_elements, double celerity, double *dt_out,
-                                 void *stream);
+                                 const double *displacement, int64_t nb_nodes,
+                                 const int32_t *connectivity, int64_t nb_elements,
+                                 double celerity, double *dt_out, void *stream);
 
 #ifdef __cplusplus
 }
