@@ -22,7 +22,7 @@ PRECISION_FP64, PRECISION_MIXED = 0, 1
 (DISPLACEMENT, VELOCITY, ACCELERATION, EXTERNAL_FORCE, INTERNAL_FORCE, MASS,
  BLOCKED_DOFS, CURRENT_POSITION, PREVIOUS_DISPLACEMENT, DISPLACEMENT_INCREMENT) = range(10)
 (GRAD_U, STRESS, PIOLA_KIRCHHOFF_2, INELASTIC_STRAIN, ISO_HARDENING,
- PLASTIC_ENERGY) = range(6)
+ PLASTIC_ENERGY, EIGEN_GRAD_U) = range(7)
 
 
 class AkbError(RuntimeError):
@@ -86,6 +86,7 @@ def lib():
         "akb_model_nodal_device_pointer": (c_int, [vp, c_int, pp]),
         "akb_model_qp_field_size": (c_int, [vp, c_int, c_int, ctypes.POINTER(i64)]),
         "akb_model_get_qp_field": (c_int, [vp, c_int, c_int, vp, i64]),
+        "akb_model_set_qp_field": (c_int, [vp, c_int, c_int, vp, i64]),
         "akb_model_solve_step": (c_int, [vp, i64]),
         "akb_model_set_graph_steps": (c_int, [vp, i64]),
         "akb_model_synchronize": (c_int, [vp]),

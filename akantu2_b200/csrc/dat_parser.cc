@@ -127,9 +127,23 @@ bool parse_dat(const std::string &text, ParsedFile &out, std::string &err) {
       ++p;
     return src.substr(b, p - b);
   };
-  // value: rest of the logical line (until newline, ']' or '[' at depth 0)
+  // value: rest of the logical line (until newline, ']' or '[' at depth 0),
+  // or a bracketed matrix / vector "[...]" up to its closing bracket (it may
+  // span lines)
   auto read_value = [&]() {
     size_t b = p;
+    if (p < n && src[p] == '[') {
+      int brackets = 0;
+      while (p < n) {
+        if (src[p] == '[') ++brackets;
+        if (src[p] == ']' && --brackets == 0) {
+          ++p;
+          break;
+        }
+        ++p;
+      }
+      return trim(src.substr(b, p - b));
+    }
     int depth = 0;
     while (p < n && src[p] != '\n') {
       if (src[p] == '(') ++depth;

@@ -22,6 +22,9 @@ struct MatParams {
   double lambda, mu, sigma_y, h, sigma_th, rho;
   int svk;
   int c33;  // plane-stress neohookean: J includes the out-of-plane stretch sqrt(C33)
+  // plastic law: thermal term of the trial stress, previous sigma_th minus
+  // current sigma_th (material_linear_isotropic_hardening_inline_impl.hh:31-34)
+  double dsth;
 };
 
 // ---- small dense algebra, column-major m[i + j*D] ---------------------------

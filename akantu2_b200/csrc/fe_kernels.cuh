@@ -104,7 +104,20 @@ struct GroupArgs {
   double *c33;               // [q][ne] plane-stress neohookean out-of-plane stretch
                              // (updated in place by every stress evaluation), or null
   int update_energy;         // 1 inside solveStep (afterSolveStep), 0 otherwise
+  // eigen gradient of the displacement [q][d*d][ne] (double), subtracted from
+  // the gradient before the law (material.cc:147), or null when zero
+  const double *eig;
 };
+
+// grad u -= eigen_grad_u at point (le, q) of a launch over ne elements
+template <int D, class T>
+__device__ __forceinline__ void subtract_eigen(const GroupArgs &ps, int64_t ne, int64_t le, int q,
+                                               T *g) {
+  if (ps.eig) {
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) g[k] = g[k] - (T)ps.eig[(int64_t)(q * D * D + k) * ne + le];
+  }
+}
 
 // plane-stress C33 of point (le, q), solved from its stored value and stored
 // back (PlaneStressToolbox::computeStress runs computeThirdAxisDeformation on
@@ -412,7 +425,7 @@ __device__ __forceinline__ void plastic_point(const MatParams &mp, const GroupAr
   }
   const int64_t qi = (int64_t)q * ne + le;
   plastic_update<D>(mp.lambda, mp.mu, mp.sigma_y, mp.h, gd, gp, sp, epp, ps.iso_cur_in[qi],
-                    ps.iso_prev[qi], 0., s, ep, &iso);
+                    ps.iso_prev[qi], mp.dsth, s, ep, &iso);
   if (ps.update_energy) {
     // MaterialPlastic::updateEnergies (material_plastic.cc:85-103)
     double wp = 0.;
@@ -452,6 +465,7 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
       for (int a = 1; a < NN; ++a) s = s + ue[a * D + i] * b[a * D + j];
       g[i + D * j] = s;
     }
+  subtract_eigen<D, T>(ps, ne, le, q, g);
   if constexpr (LAW == LAW_NEOHOOKEAN) {
     if constexpr (REL) {
       // mixed path: r = (F S w) . dN/dx with F S formed in the displacement gradient
@@ -900,6 +914,7 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
       for (int i = 0; i < 3; ++i)
         gr[i + 3 * j] = (Ji[j] * Dp[0 + 3 * i] + Ji[j + 3] * Dp[1 + 3 * i] +
                          Ji[j + 6] * Dp[2 + 3 * i]) * rdet;
+    subtract_eigen<3, float>(ps, e_count, le, q, gr);
     // the weight w = det J (2 x 2 x 2 Gauss weights are 1) cancels the 1/det
     // of J^-1 in H = w P J^-1: the unweighted flux times the adjugate is
     // accumulated and the remaining 1/512 applied once per element
@@ -1449,6 +1464,7 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const double *__restrict__ B,
                             const double *__restrict__ u, MatParams mp,
                             const double *__restrict__ c33, int64_t c33_ld,
+                            const double *__restrict__ eig,
                             double *__restrict__ grad_out, double *__restrict__ stress_out) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e_count * NQ) return;
@@ -1474,6 +1490,10 @@ __global__ void k_qp_fields(int64_t e_begin, int64_t e_count, int64_t E,
       for (int a = 1; a < NN; ++a) acc = acc + ue[a * D + i] * b[a * D + j];
       g[i + D * j] = acc;
     }
+  if (eig) {
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) g[k] = g[k] - eig[(int64_t)(q * D * D + k) * c33_ld + le];
+  }
   if constexpr (LAW == LAW_NEOHOOKEAN)
     finite_pk2<D, double>(mp, g, s, (c33 && mp.c33) ? c33[(int64_t)q * c33_ld + le] : 0.);
   else

@@ -178,17 +178,17 @@ cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u
 // ---- fields and energies ---------------------------------------------------
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,
-                             const double *c33, int64_t c33_ld, double *grad, double *stress,
-                             cudaStream_t s) {
+                             const double *c33, int64_t c33_ld, const double *eig,
+                             double *grad, double *stress, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
     if (law == LAW_NEOHOOKEAN)
       k_qp_fields<D, NN, NQ, LAW_NEOHOOKEAN><<<grid_for(ne * NQ), kThreads, 0, s>>>(
-          e0, ne, g.E, g.conn, B, u, mp, c33, c33_ld, grad, stress);
+          e0, ne, g.E, g.conn, B, u, mp, c33, c33_ld, eig, grad, stress);
     else
       k_qp_fields<D, NN, NQ, LAW_ELASTIC><<<grid_for(ne * NQ), kThreads, 0, s>>>(
-          e0, ne, g.E, g.conn, B, u, mp, c33, c33_ld, grad, stress);
+          e0, ne, g.E, g.conn, B, u, mp, c33, c33_ld, eig, grad, stress);
   });
   return cudaGetLastError();
 }

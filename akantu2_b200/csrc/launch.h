@@ -116,11 +116,12 @@ cudaError_t launch_persistent_mixed(const DevGeom &g, int law, int qu, const Ste
                                     const QuadTable &tab, cudaStream_t s);
 
 // ---- fields and energies ---------------------------------------------------
-// c33: stored plane-stress stretches of the material's points ([q][c33_ld]), or null
+// c33: stored plane-stress stretches of the material's points ([q][c33_ld]),
+// eig: their eigen gradients ([q][d*d][c33_ld]); either may be null
 cudaError_t launch_qp_fields(const DevGeom &g, int law, int64_t e0, int64_t ne,
                              const double *B, const double *u, const MatParams &mp,
-                             const double *c33, int64_t c33_ld, double *grad, double *stress,
-                             cudaStream_t s);
+                             const double *c33, int64_t c33_ld, const double *eig,
+                             double *grad, double *stress, cudaStream_t s);
 // per-dof kinetic terms (m > eps ? v v m : 0) summed per node -> out[N]
 cudaError_t launch_ekin_terms(const DevGeom &g, const double *v, const double *mass,
                               double *out, cudaStream_t s);

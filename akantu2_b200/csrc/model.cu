@@ -49,6 +49,16 @@ struct Material {
   // kernels with the elastic law applied to the Green-Lagrange strain
   bool svk = false;
   double lambda = 0., mu = 0., sigma_th = 0.;
+  // eigen_grad_u parameter (material.cc:35-51), column-major d x d; every
+  // point of the material starts from it (Material::updateInternalParameters)
+  double eig[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  bool has_eig = false;
+  double eig_in[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};  // as parsed, 3 x 3
+  int eig_rows = 0, eig_cols = 0;                           // parsed size
+  // sigma_th internal and its saved previous value (material_thermal.cc:33-34):
+  // a stress evaluation sets th_cur = sigma_th, the start of a step saves
+  // th_prev = th_cur; the plastic trial stress takes th_prev - th_cur
+  double th_prev = 0., th_cur = 0., dsth = 0.;
   int64_t e_begin = 0, e_count = 0;  // internal element range
   int group = 0;                     // law group holding the range
 
@@ -62,7 +72,7 @@ struct Material {
     sigma_th = -E / (1. - 2. * nu) * alpha * delta_T;
   }
   MatParams params() const {
-    return MatParams{lambda, mu, sigma_y, h, sigma_th, rho, svk ? 1 : 0, c33 ? 1 : 0};
+    return MatParams{lambda, mu, sigma_y, h, sigma_th, rho, svk ? 1 : 0, c33 ? 1 : 0, dsth};
   }
   bool c33 = false;  // plane-stress neohookean (set by initFull in 2D)
   double celerity() const { return std::sqrt((lambda + 2 * mu) / rho); }
@@ -88,6 +98,9 @@ struct Group {
   // plane-stress neohookean: out-of-plane stretch C33 per point, initially 1
   // (third_axis_deformation, plane_stress_toolbox_tmpl.hh:46)
   double *c33 = nullptr;
+  // eigen gradient of every point [q][d*d][e_count], or null while every
+  // material of the group has a zero one
+  double *eig = nullptr;
 };
 
 // independent components of a symmetric d x d tensor, and the map from
@@ -212,6 +225,7 @@ struct akb_model {
   QuadTable tab;  // quadrature tables of the element type
   int32_t *dconn = nullptr, *dptr = nullptr, *dent = nullptr, *dpos = nullptr;
   MatParams *dmtab = nullptr;  // all materials, for groups of several
+  std::vector<double> mtab_dsth;  // the dsth values dmtab holds
   int32_t *dmslot = nullptr;   // [E] material of each internal element
   int32_t *dnode_inst = nullptr, *dperm = nullptr;  // batch: [N] instance, [E] user id
   double *dinst_dt = nullptr, *dinst_min = nullptr;  // batch: [ninst]
@@ -329,10 +343,76 @@ struct akb_model {
 
 namespace {
 
+// a matrix parameter, rows of a bracketed list "[[a, b, c], [d, e, f], ...]"
+// (the .dat grammar of parsable matrices, algebraic_parser.hh:363-380);
+// entries are expressions.  rows[i][j] is entry (i, j).
+bool parse_matrix(const std::string &val, std::vector<std::vector<double>> &rows) {
+  size_t p = 0;
+  auto ws = [&]() {
+    while (p < val.size() && std::isspace((unsigned char)val[p])) ++p;
+  };
+  ws();
+  if (p >= val.size() || val[p] != '[') return false;
+  ++p;
+  rows.clear();
+  for (;;) {
+    ws();
+    if (p >= val.size() || val[p] != '[') return false;
+    ++p;
+    std::vector<double> row;
+    for (;;) {
+      size_t b = p;
+      int depth = 0;
+      while (p < val.size() && !(depth == 0 && (val[p] == ',' || val[p] == ']'))) {
+        if (val[p] == '(') ++depth;
+        if (val[p] == ')') --depth;
+        ++p;
+      }
+      if (p >= val.size()) return false;
+      double x;
+      if (!eval_value(val.substr(b, p - b), x)) return false;
+      row.push_back(x);
+      if (val[p++] == ']') break;
+    }
+    rows.push_back(row);
+    ws();
+    if (p < val.size() && val[p] == ',') {
+      ++p;
+      continue;
+    }
+    if (p < val.size() && val[p] == ']') {
+      ++p;
+      break;
+    }
+    return false;
+  }
+  ws();
+  return p == val.size();
+}
+
 int apply_param(Material &m, const std::string &key, const std::string &val) {
   if (key == "name") {
     m.name = val;
     return AKB_OK;
+  }
+  if (key == "eigen_grad_u") {
+    // a matrix (its leading d x d block is used, ParameterTyped<Matrix>::setAuto,
+    // parameter_registry_tmpl.hh:203-217), or a scalar 0
+    std::vector<std::vector<double>> rows;
+    double z;
+    if (parse_matrix(val, rows)) {
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          const double x = (i < (int)rows.size() && j < (int)rows[i].size()) ? rows[i][j] : 0.;
+          m.eig_in[i + 3 * j] = x;  // column-major; the d x d block is taken at initFull
+        }
+      m.eig_rows = (int)rows.size();
+      m.eig_cols = 3;
+      for (auto &r : rows) m.eig_cols = std::min(m.eig_cols, (int)r.size());
+      return AKB_OK;
+    }
+    if (eval_value(val, z) && z == 0.) return AKB_OK;
+    return fail(AKB_EPARSE, "eigen_grad_u must be a matrix [[...], ...] (got '" + val + "')");
   }
   double v;
   if (!eval_value(val, v))
@@ -346,9 +426,7 @@ int apply_param(Material &m, const std::string &key, const std::string &val) {
   else if (key == "delta_T") m.delta_T = v;
   else if (key == "Plane_Stress") m.plane_stress = v != 0.;
   else if (key == "finite_deformation") m.finite_deformation = v != 0.;
-  else if (key == "eigen_grad_u") {
-    if (v != 0.) return fail(AKB_EUNSUPPORTED, "a non-zero eigen_grad_u is not supported");
-  } else
+  else
     return fail(AKB_EPARSE, "unknown material parameter '" + key + "'");
   return AKB_OK;
 }
@@ -374,8 +452,6 @@ int make_material(akb_model *m, const std::string &type, const std::string &name
   }
   if (mat.law == LAW_PLASTIC && mat.finite_deformation)
     return fail(AKB_EUNSUPPORTED, "finite-strain plasticity is not supported by this path");
-  if (mat.law == LAW_PLASTIC && mat.alpha * mat.delta_T != 0.)
-    return fail(AKB_EUNSUPPORTED, "thermal stress with plasticity is not supported");
   m->mats.push_back(mat);
   return AKB_OK;
 }
@@ -410,6 +486,7 @@ GroupArgs group_args(akb_model *m, const Group &mt, bool in_step) {
     ps.mslot = m->dmslot + mt.e_begin;
   }
   ps.c33 = mt.c33;
+  ps.eig = mt.eig;
   if (mt.law != LAW_PLASTIC) return ps;
   const int c = m->cur;
   // inside a step the new state goes to the other buffer; a standalone
@@ -430,9 +507,55 @@ GroupArgs group_args(akb_model *m, const Group &mt, bool in_step) {
   return ps;
 }
 
+// the device table of per-material parameters (groups of several materials)
+// follows the materials' dsth values
+int sync_mtab(akb_model *m) {
+  if (!m->dmtab) return AKB_OK;
+  const size_t nm = m->mats.size();
+  bool same = m->mtab_dsth.size() == nm;
+  for (size_t k = 0; same && k < nm; ++k)
+    same = std::memcmp(&m->mtab_dsth[k], &m->mats[k].dsth, sizeof(double)) == 0;
+  if (same) return AKB_OK;
+  std::vector<MatParams> tab(nm);
+  m->mtab_dsth.resize(nm);
+  for (size_t k = 0; k < nm; ++k) {
+    tab[k] = m->mats[k].params();
+    m->mtab_dsth[k] = m->mats[k].dsth;
+  }
+  // pageable source: the call returns once the data is staged
+  AKB_CUDA(cudaMemcpyAsync(m->dmtab, tab.data(), sizeof(MatParams) * nm, cudaMemcpyHostToDevice,
+                           m->stream));
+  return AKB_OK;
+}
+
+// sigma_th of the plastic materials for one stress evaluation: a step first
+// saves the previous value (Material::savePreviousState, material.cc:737),
+// then MaterialThermal::computeStress sets the current one
+// (material_thermal.hh:89-95); the trial stress of the radial return takes
+// previous - current (material_linear_isotropic_hardening_inline_impl.hh:31-34)
+int thermal_eval(akb_model *m, bool in_step) {
+  for (auto &mt : m->mats) {
+    if (mt.law != LAW_PLASTIC) continue;
+    if (in_step) mt.th_prev = mt.th_cur;
+    mt.th_cur = mt.sigma_th;
+    mt.dsth = mt.th_prev - mt.th_cur;
+  }
+  return sync_mtab(m);
+}
+
+// every step from now on has a zero thermal term (the current sigma_th is
+// the material's and the last evaluation had none): steps may be replayed
+// from captured graphs, whose launches bake the parameters in
+bool thermal_steady(const akb_model *m) {
+  for (auto &mt : m->mats)
+    if (mt.law == LAW_PLASTIC && (mt.th_cur != mt.sigma_th || mt.dsth != 0.)) return false;
+  return true;
+}
+
 // elemental forces at the predicted displacement (inside a step) or at the
 // model's displacement (standalone assembly)
 int element_forces(akb_model *m, bool in_step) {
+  AKB_TRY(thermal_eval(m, in_step));
   DevGeom g = m->geom();
   const double *u = in_step ? m->u_pred() : m->u();
   for (auto &gr : m->groups) {
@@ -541,6 +664,15 @@ int capture_graph(akb_model *m, bool any_plastic, akb_model::StepGraph **out = n
   if (!g) {
     const int ucur0 = m->ucur, cur0 = m->cur;
     const int64_t steps0 = m->steps_done;
+    // graphs replay steps without a thermal term (thermal_steady): capture
+    // them from that state, with the device table already matching it
+    std::vector<Material> mats0 = m->mats;
+    for (auto &mt : m->mats)
+      if (mt.law == LAW_PLASTIC) {
+        mt.th_prev = mt.th_cur = mt.sigma_th;
+        mt.dsth = 0.;
+      }
+    AKB_TRY(sync_mtab(m));
     AKB_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
     int rc = AKB_OK;
     for (int64_t s = 0; s < m->graph_steps && rc == AKB_OK; ++s) rc = one_step(m, any_plastic);
@@ -549,6 +681,11 @@ int capture_graph(akb_model *m, bool any_plastic, akb_model::StepGraph **out = n
     m->ucur = ucur0;
     m->cur = cur0;
     m->steps_done = steps0;
+    for (size_t k = 0; k < m->mats.size(); ++k) {
+      m->mats[k].th_prev = mats0[k].th_prev;
+      m->mats[k].th_cur = mats0[k].th_cur;
+      m->mats[k].dsth = mats0[k].dsth;
+    }
     if (rc != AKB_OK || e != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
       if (rc != AKB_OK) return rc;
@@ -579,6 +716,13 @@ int capture_graph(akb_model *m, bool any_plastic, akb_model::StepGraph **out = n
 int run_graph(akb_model *m, bool any_plastic) {
   akb_model::StepGraph *g = nullptr;
   AKB_TRY(capture_graph(m, any_plastic, &g));
+  // the steps of the graph leave the sigma_th history steady
+  for (auto &mt : m->mats)
+    if (mt.law == LAW_PLASTIC) {
+      mt.th_prev = mt.th_cur = mt.sigma_th;
+      mt.dsth = 0.;
+    }
+  AKB_TRY(sync_mtab(m));
   AKB_CUDA(cudaGraphLaunch(g->exec, m->stream));
   m->steps_done += g->steps;
   m->fint_valid = false;
@@ -693,8 +837,37 @@ int eval_qp_fields(akb_model *m, const Material &mt) {
   const double *u = m->snap_valid ? m->dusnap : m->u();
   const Group &gr = m->groups[mt.group];
   const double *c33 = gr.c33 ? gr.c33 + (mt.e_begin - gr.e_begin) : nullptr;
+  const double *eig = gr.eig ? gr.eig + (mt.e_begin - gr.e_begin) : nullptr;
   AKB_CUDA(launch_qp_fields(m->geom(), mt.law, mt.e_begin, mt.e_count, m->dB, u, mt.params(),
-                            c33, gr.e_count, m->dqp_a, m->dqp_b, m->stream));
+                            c33, gr.e_count, eig, m->dqp_a, m->dqp_b, m->stream));
+  return AKB_OK;
+}
+
+// the group's eigen-gradient array [q][d*d][e_count], allocated if needed
+// and set to each material's eigen_grad_u parameter at every point.  Graphs
+// captured before the array existed read no eigen gradient: they are dropped.
+int fill_group_eigen(akb_model *m, int gi) {
+  Group &gr = m->groups[gi];
+  const int dd = m->dim * m->dim;
+  const int64_t ne = gr.e_count, rows = (int64_t)m->nq * dd;
+  if (!gr.eig) {
+    AKB_TRY(m->alloc(&gr.eig, sizeof(double) * std::max<int64_t>(rows * ne, 1)));
+    for (auto &g : m->graphs) cudaGraphExecDestroy(g.exec);
+    m->graphs.clear();
+  }
+  std::vector<double> h((size_t)(rows * ne), 0.);
+  for (auto &mt : m->mats) {
+    if (mt.group != gi || !mt.has_eig) continue;
+    const int64_t off = mt.e_begin - gr.e_begin;
+    for (int q = 0; q < m->nq; ++q)
+      for (int k = 0; k < dd; ++k)
+        std::fill(h.begin() + (size_t)((q * dd + k) * ne + off),
+                  h.begin() + (size_t)((q * dd + k) * ne + off + mt.e_count), mt.eig[k]);
+  }
+  if (!h.empty())
+    AKB_CUDA(cudaMemcpyAsync(gr.eig, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice,
+                             m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
   return AKB_OK;
 }
 
@@ -911,6 +1084,18 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   for (auto &mt : m->mats) {
     mt.update(m->dim);
     mt.c33 = m->dim == 2 && mt.law == LAW_NEOHOOKEAN && !mt.svk && mt.plane_stress;
+    if (mt.eig_rows > 0) {
+      const int d = m->dim;
+      if (mt.eig_rows < d || mt.eig_cols < d)
+        return fail(AKB_EINVAL, "material '" + mt.name + "': eigen_grad_u needs at least " +
+                                    std::to_string(d) + " x " + std::to_string(d) + " entries");
+      mt.has_eig = false;
+      for (int j = 0; j < d; ++j)
+        for (int i = 0; i < d; ++i) {
+          mt.eig[i + d * j] = mt.eig_in[i + 3 * j];
+          mt.has_eig |= mt.eig[i + d * j] != 0.;
+        }
+    }
   }
   m->precision = precision;
   AKB_CUDA(cudaGetDevice(&m->device));
@@ -1119,12 +1304,21 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     AKB_TRY(m->alloc(&gr.c33, sizeof(double) * nqp));
     AKB_CUDA(launch_fill(gr.c33, 1.0, nqp, s));
   }
+  // eigen gradients: every point of a material starts from its parameter
+  // (Material::updateInternalParameters, material.cc:61-71)
+  for (size_t gi = 0; gi < m->groups.size(); ++gi) {
+    bool need = false;
+    for (auto &mt : m->mats) need |= mt.group == (int)gi && mt.has_eig;
+    if (need) AKB_TRY(fill_group_eigen(m, (int)gi));
+  }
   // groups of several materials read per-element parameters
   bool multi = false;
   for (auto &gr : m->groups) multi |= gr.nmat > 1;
   if (multi) {
     std::vector<MatParams> mtab(nm);
     for (int k = 0; k < nm; ++k) mtab[k] = m->mats[k].params();
+    m->mtab_dsth.assign(nm, 0.);
+    for (int k = 0; k < nm; ++k) m->mtab_dsth[k] = m->mats[k].dsth;
     std::vector<int32_t> mslot(E);
     for (int64_t ie = 0; ie < E; ++ie) mslot[ie] = m->mat_user[m->perm[ie]];
     AKB_TRY(m->alloc(&m->dmtab, sizeof(MatParams) * nm));
@@ -1412,6 +1606,7 @@ int akb_model_qp_field_size(akb_model *m, int field, int k, int64_t *count) {
   const int64_t nqp = m->mats[k].e_count * m->nq;
   switch (field) {
   case AKB_GRAD_U: case AKB_STRESS: case AKB_PIOLA_KIRCHHOFF_2: case AKB_INELASTIC_STRAIN:
+  case AKB_EIGEN_GRAD_U:
     *count = nqp * m->dim * m->dim;
     return AKB_OK;
   case AKB_ISO_HARDENING: case AKB_PLASTIC_ENERGY:
@@ -1432,7 +1627,16 @@ int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t
   const double *src = nullptr;
   int comps = dd;
   int64_t ld = mt.e_count;  // row length of the device array [q][comp][ld]
-  if (mt.law == LAW_PLASTIC) {
+  if (field == AKB_EIGEN_GRAD_U) {
+    const Group &gr = m->groups[mt.group];
+    if (!gr.eig) {  // never set: every point holds the (zero) parameter
+      for (int64_t p = 0; p < nqp; ++p)
+        for (int kk = 0; kk < dd; ++kk) host[p * dd + kk] = mt.eig[kk];
+      return AKB_OK;
+    }
+    src = gr.eig + (mt.e_begin - gr.e_begin);
+    ld = gr.e_count;
+  } else if (mt.law == LAW_PLASTIC) {
     const Group &gr = m->groups[mt.group];
     const int c = m->cur;
     const int64_t off = mt.e_begin - gr.e_begin, ns = sym_comps(m->dim);
@@ -1502,11 +1706,45 @@ int akb_model_get_qp_field(akb_model *m, int field, int k, double *host, int64_t
   return AKB_OK;
 }
 
+int akb_model_set_qp_field(akb_model *m, int field, int k, const double *host, int64_t count) {
+  int64_t need = 0;
+  AKB_TRY(akb_model_qp_field_size(m, field, k, &need));
+  if (field != AKB_EIGEN_GRAD_U)
+    return fail(AKB_EINVAL, "only eigen_grad_u can be written");
+  if (count != need) return fail(AKB_EINVAL, "count does not match the field size");
+  if (!host && need > 0) return fail(AKB_EINVAL, "null host buffer");
+  const Material &mt = m->mats[k];
+  Group &gr = m->groups[mt.group];
+  if (!gr.eig) AKB_TRY(fill_group_eigen(m, mt.group));
+  const int dd = m->dim * m->dim;
+  const int64_t ne = mt.e_count, rows = (int64_t)m->nq * dd;
+  // reference order [element][q][comp] -> device [q][comp][element]
+  std::vector<double> soa((size_t)(rows * ne));
+  for (int64_t le = 0; le < ne; ++le)
+    for (int q = 0; q < m->nq; ++q)
+      for (int c = 0; c < dd; ++c)
+        soa[(size_t)((q * dd + c) * ne + le)] = host[(le * m->nq + q) * dd + c];
+  if (ne > 0)
+    AKB_CUDA(cudaMemcpy2DAsync(gr.eig + (mt.e_begin - gr.e_begin), sizeof(double) * gr.e_count,
+                               soa.data(), sizeof(double) * ne, sizeof(double) * ne,
+                               (size_t)rows, cudaMemcpyHostToDevice, m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
 int akb_model_solve_step(akb_model *m, int64_t nsteps) {
   AKB_TRY(check_model(m, true));
   if (nsteps < 0) return fail(AKB_EINVAL, "negative step count");
   bool any_plastic = false;
   for (auto &mt : m->mats) any_plastic |= mt.law == LAW_PLASTIC;
+  // a step with a thermal term in the plastic trial stress (the first after
+  // initFull or a standalone assembly of a heated material) runs eagerly
+  if (nsteps > 0 && !thermal_steady(m)) {
+    AKB_TRY(one_step(m, any_plastic));
+    --nsteps;
+    m->forces_evaluated = true;
+    m->snap_valid = false;
+  }
   if (nsteps > 0 && use_persistent(m)) {
     AKB_TRY(run_persistent(m, nsteps, any_plastic));
     m->forces_evaluated = true;

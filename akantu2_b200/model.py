@@ -209,13 +209,30 @@ class Material:
     def getGradU(self, element_type=None):
         return self._qp(_capi.GRAD_U)
 
+    _INTERNALS = {"stress": _capi.STRESS, "grad_u": _capi.GRAD_U,
+                  "piola_kirchhoff_2": _capi.PIOLA_KIRCHHOFF_2,
+                  "inelastic_strain": _capi.INELASTIC_STRAIN,
+                  "iso_hardening": _capi.ISO_HARDENING, "plastic_energy": _capi.PLASTIC_ENERGY,
+                  "eigen_grad_u": _capi.EIGEN_GRAD_U}
+
     def getInternal(self, name):
-        ids = {"stress": _capi.STRESS, "grad_u": _capi.GRAD_U,
-               "piola_kirchhoff_2": _capi.PIOLA_KIRCHHOFF_2,
-               "inelastic_strain": _capi.INELASTIC_STRAIN,
-               "iso_hardening": _capi.ISO_HARDENING, "plastic_energy": _capi.PLASTIC_ENERGY}
-        fid = ids[name]
+        fid = self._INTERNALS[name]
         return lambda element_type=None: self._qp(fid)
+
+    def setInternal(self, name, values, element_type=None):
+        """Writes a quadrature-point internal ([points][dim*dim], the getter's
+        layout); the reference assigns getInternal<Real>(name)(type) in place
+        (test_solid_mechanics_model_material_eigenstrain.cc:127-136).  Only
+        "eigen_grad_u" is writable."""
+        m = self._model
+        fid = self._INTERNALS[name]
+        n = ctypes.c_int64()
+        L = _capi.lib()
+        _capi.check(L.akb_model_qp_field_size(m._h, fid, self._index, ctypes.byref(n)))
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if a.size != n.value:
+            raise ValueError(f"{name} holds {n.value} values, got {a.size}")
+        _capi.check(L.akb_model_set_qp_field(m._h, fid, self._index, _capi.ptr(a), n.value))
 
 
 class SolidMechanicsModel:
@@ -251,6 +268,10 @@ class SolidMechanicsModel:
         def fmt(v):
             if isinstance(v, (bool, np.bool_)):
                 return "true" if v else "false"
+            if isinstance(v, (list, tuple, np.ndarray)):  # a matrix: rows in brackets
+                rows = np.atleast_2d(np.asarray(v, dtype=np.float64))
+                return "[" + ", ".join("[" + ", ".join(repr(float(x)) for x in r) + "]"
+                                       for r in rows) + "]"
             return repr(float(v)) if isinstance(v, (int, float, np.floating)) else str(v)
         text = "\n".join(f"{k} = {fmt(v)}" for k, v in params.items())
         _capi.check(_capi.lib().akb_model_add_material(self._h, type.encode(), text.encode()))

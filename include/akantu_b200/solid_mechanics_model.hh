@@ -330,9 +330,14 @@ public:
   inline Array<Real> getStress(ElementType = _not_defined);
   inline Array<Real> getGradU(ElementType = _not_defined);
   inline Array<Real> getInternal(const ID &name, ElementType = _not_defined);
+  // writes an internal in the getter's layout (only "eigen_grad_u"); the
+  // reference assigns getInternal<Real>(name)(type) in place
+  inline void setInternal(const ID &name, const Array<Real> &values,
+                          ElementType = _not_defined);
 
 private:
   inline Array<Real> qp(int field);
+  static inline int internalId(const ID &name);
   SolidMechanicsModel *model_;
   int index_;
 };
@@ -625,12 +630,24 @@ inline Array<Real> Material::qp(int field) {
 }
 inline Array<Real> Material::getStress(ElementType) { return qp(AKB_STRESS); }
 inline Array<Real> Material::getGradU(ElementType) { return qp(AKB_GRAD_U); }
-inline Array<Real> Material::getInternal(const ID &name, ElementType) {
+inline int Material::internalId(const ID &name) {
   static const std::map<ID, int> ids = {
       {"stress", AKB_STRESS}, {"grad_u", AKB_GRAD_U},
       {"piola_kirchhoff_2", AKB_PIOLA_KIRCHHOFF_2}, {"inelastic_strain", AKB_INELASTIC_STRAIN},
-      {"iso_hardening", AKB_ISO_HARDENING}, {"plastic_energy", AKB_PLASTIC_ENERGY}};
-  return qp(ids.at(name));
+      {"iso_hardening", AKB_ISO_HARDENING}, {"plastic_energy", AKB_PLASTIC_ENERGY},
+      {"eigen_grad_u", AKB_EIGEN_GRAD_U}};
+  return ids.at(name);
+}
+inline Array<Real> Material::getInternal(const ID &name, ElementType) {
+  return qp(internalId(name));
+}
+inline void Material::setInternal(const ID &name, const Array<Real> &values, ElementType) {
+  const int field = internalId(name);
+  int64_t n = 0;
+  check(akb_model_qp_field_size(model_->handle(), field, index_, &n));
+  if ((int64_t)(values.size() * values.getNbComponent()) != n)
+    throw Exception(AKB_EINVAL, "setInternal: size mismatch for " + name);
+  check(akb_model_set_qp_field(model_->handle(), field, index_, values.data(), n));
 }
 
 /* ---- Server: many solves resident on one GPU ----------------------------- */

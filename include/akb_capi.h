@@ -78,7 +78,11 @@ enum akb_qp_field {
   AKB_PIOLA_KIRCHHOFF_2 = 2,    /* [nq_m][dim*dim] neohookean                 */
   AKB_INELASTIC_STRAIN = 3,     /* [nq_m][dim*dim] plastic                    */
   AKB_ISO_HARDENING = 4,        /* [nq_m]          plastic                    */
-  AKB_PLASTIC_ENERGY = 5        /* [nq_m]          plastic, cumulative        */
+  AKB_PLASTIC_ENERGY = 5,       /* [nq_m]          plastic, cumulative        */
+  /* [nq_m][dim*dim] eigen gradient subtracted from grad u before the law
+   * (material.cc:147); initially the material's eigen_grad_u parameter at
+   * every point (material.cc:61-71), writable per point */
+  AKB_EIGEN_GRAD_U = 6
 };
 
 /* ---- library ------------------------------------------------------------ */
@@ -204,6 +208,12 @@ int akb_model_wait_nodal_async(akb_model *model, int64_t ticket);
  * number of doubles (akb_model_qp_field_size) */
 int akb_model_qp_field_size(akb_model *model, int field, int material, int64_t *count);
 int akb_model_get_qp_field(akb_model *model, int field, int material, double *host,
+                           int64_t count);
+/* writes a quadrature-point internal of one material, the same layout as the
+ * getter: Material::getInternal<Real>("eigen_grad_u")(type) assigned in
+ * place (e.g. test_solid_mechanics_model_material_eigenstrain.cc:127-136);
+ * only AKB_EIGEN_GRAD_U is writable (AKB_EINVAL otherwise) */
+int akb_model_set_qp_field(akb_model *model, int field, int material, const double *host,
                            int64_t count);
 
 /* prescribed motion on the device, for the imposed-displacement loop of a

@@ -252,6 +252,8 @@ struct Mat {
   double rho, E, nu, sigma_y, h, alpha, delta_T;
   int plane_stress;
   double lambda, mu, sigma_th;
+  // sigma_th internal and its saved previous value (material_thermal.cc:33-34)
+  double th_prev = 0., th_cur = 0.;
   void update() {
     lambda = nu * E / ((1 + nu) * (1 - 2 * nu));
     mu = E / (2 * (1 + nu));
@@ -359,6 +361,7 @@ struct MatState {
   std::vector<double> grad_u, grad_u_prev, stress, stress_prev, pk2;
   std::vector<double> eps_p, eps_p_prev, iso, iso_prev, pe;
   std::vector<double> c33;  // plane-stress neohookean out-of-plane stretch, initially 1
+  std::vector<double> eig;  // eigen_grad_u per point [qp][d*d], empty when zero
 };
 
 }  // namespace
@@ -493,8 +496,13 @@ parallel_for((long)s.elems.size(), m->threads, [&](long le) {
 void element_forces(or_model *m, int k, bool history_step) {
   const int n = m->n, nq = m->nq, d = m->d, dd = d * d;
   MatState &s = m->st[k];
-  const Mat &mat = m->mats[k];
+  Mat &mat = m->mats[k];
   const long ne = (long)s.elems.size();
+  // MaterialThermal::computeStress sets the current sigma_th
+  // (material_thermal.hh:89-95); the plastic trial stress takes the saved
+  // previous value minus it (material_linear_isotropic_hardening_inline_impl.hh:31-34)
+  mat.th_cur = mat.sigma_th;
+  const double dsth = mat.th_prev - mat.th_cur;
 parallel_for(ne, m->threads, [&](long le) {
     const long e = s.elems[le];
     const int32_t *cn = &m->conn[e * n];
@@ -515,18 +523,18 @@ parallel_for(ne, m->threads, [&](long le) {
           for (int a = 1; a < n; ++a) t = t + ue[a * d + i] * B[a * d + j];
           g[i + d * j] = t;
         }
+      // gradu -= eigengradu (material.cc:147)
+      if (!s.eig.empty())
+        for (int c = 0; c < dd; ++c) g[c] = g[c] - s.eig[qp * dd + c];
       double rq[24];
       if (!mat.finite()) {
         double *sig = &s.stress[qp * dd];
         if (mat.law == OR_ELASTIC) {
           elastic(d, mat.lambda, mat.mu, g, mat.sigma_th, sig);
         } else {
-          // for a uniform temperature field, previous sigma_th equals the
-          // current one after the first step; alpha * delta_T = 0 in all
-          // supported inputs so the difference is zero
           plastic(d, mat.lambda, mat.mu, mat.sigma_y, mat.h, g,
                   &s.grad_u_prev[qp * dd], &s.stress_prev[qp * dd],
-                  &s.eps_p_prev[qp * dd], s.iso[qp], s.iso_prev[qp], 0.,
+                  &s.eps_p_prev[qp * dd], s.iso[qp], s.iso_prev[qp], dsth,
                   sig, &s.eps_p[qp * dd], &s.iso[qp]);
           if (history_step) {
             // MaterialPlastic::updateEnergies (material_plastic.cc:85-103)
@@ -634,6 +642,7 @@ void internal_forces(or_model *m, bool history_step) {
 }
 
 void save_previous(or_model *m) {
+  for (auto &mt : m->mats) mt.th_prev = mt.th_cur;
   for (auto &s : m->st) {
     s.grad_u_prev = s.grad_u;
     s.stress_prev = s.stress;
@@ -831,6 +840,12 @@ void or_model_get_nodal(or_model *m, int field, void *data) {
 long or_model_qp_size(or_model *m, int mat) {
   return (long)m->st[mat].elems.size() * m->nq;
 }
+void or_model_set_eigen_grad_u(or_model *m, int mat, const double *values) {
+  MatState &s = m->st[mat];
+  const size_t n = s.elems.size() * (size_t)m->nq * m->d * m->d;
+  s.eig.assign(values, values + n);
+}
+
 void or_model_get_qp(or_model *m, int mat, int field, double *out) {
   const MatState &s = m->st[mat];
   const std::vector<double> *src = nullptr;

@@ -100,6 +100,9 @@ void or_model_set_nodal(or_model *m, int field, const void *data);
 void or_model_get_nodal(or_model *m, int field, void *data);
 long or_model_qp_size(or_model *m, int mat);
 void or_model_get_qp(or_model *m, int mat, int field, double *out);
+/* eigen_grad_u of every point of material mat, [qp][dim*dim] in the qp
+ * getter's order (material.cc:35-51,147: subtracted from grad u) */
+void or_model_set_eigen_grad_u(or_model *m, int mat, const double *values);
 void or_model_set_threads(or_model *m, int nthreads);
 void or_model_solve_step(or_model *m, long nsteps);
 /* recompute internal forces (and stresses) at the current displacement */

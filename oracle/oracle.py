@@ -53,6 +53,7 @@ def lib():
         L.or_model_qp_size.restype = ctypes.c_long
         L.or_model_qp_size.argtypes = [vp, ctypes.c_int]
         L.or_model_get_qp.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+        L.or_model_set_eigen_grad_u.argtypes = [vp, ctypes.c_int, vp]
         L.or_model_set_threads.argtypes = [vp, ctypes.c_int]
         L.or_model_solve_step.argtypes = [vp, ctypes.c_long]
         L.or_model_assemble_internal_forces.argtypes = [vp]
@@ -180,6 +181,14 @@ class OracleModel:
             self._m = None
             raise RuntimeError(f"oracle init failed ({rc})")
         self.nb_materials = len(materials)
+        # eigen_grad_u parameter: every point of the material starts from it
+        # (Material::updateInternalParameters); its leading d x d block is used
+        for k, mat in enumerate(materials):
+            if "eigen_grad_u" in mat:
+                M = np.asarray(mat["eigen_grad_u"], dtype=np.float64)[:self.dim, :self.dim]
+                col = M.reshape(self.dim, self.dim).ravel(order="F")
+                n = lib().or_model_qp_size(self._m, k)
+                self.set_eigen_grad_u(k, np.tile(col, (n, 1)))
 
     def __del__(self):
         if getattr(self, "_m", None):
@@ -216,6 +225,12 @@ class OracleModel:
         a = np.zeros((n, comp))
         lib().or_model_get_qp(self._m, mat, field, _p(a))
         return a
+
+    def set_eigen_grad_u(self, mat, values):
+        """per-point eigen gradient of one material, [points][dim*dim]"""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        assert a.size == lib().or_model_qp_size(self._m, mat) * self.dim * self.dim
+        lib().or_model_set_eigen_grad_u(self._m, mat, _p(a))
 
     def step(self, n=1):
         lib().or_model_solve_step(self._m, n)

@@ -15,7 +15,7 @@ import pytest
 
 from oracle import oracle as orc
 from scenarios import (OR_TYPE, PATCH_ALPHA, STEEL_LUMPED, STEEL_PLANE_STRAIN,
-                       STEEL_PLANE_STRESS, TYPES, golden, linear_field)
+                       STEEL_PLANE_STRESS, TYPES, golden, linear_field, oracle_model)
 
 from akantu2_b200.mesh import Mesh, boundary_nodes
 
@@ -349,3 +349,78 @@ def test_travelling_wave_bar(etype):
     err, steps = run_wave(mesh, lambda n, a: o.set(fields[n], a),
                           lambda: (o.get(orc.U), o.get(orc.V)), lambda: o.step(1), dt)
     assert steps >= 100 and 0 < err < 2e-3
+
+
+# ---- eigen gradient and thermal stress with plasticity -------------------------------
+def _eigen_prescribed_stress(eig, d, E=2.1e11, nu=0.3):
+    """test_solid_mechanics_model_material_eigenstrain.cc:44-75: the stress of
+    the linear field alpha minus the eigen gradient, plane strain in 2D"""
+    pstrain = PATCH_ALPHA[:d, 1:1 + d]
+    strain = (pstrain + pstrain.T) / 2.0 - eig
+    lam = nu * E / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    return np.eye(d) * np.trace(strain) * lam + 2.0 * mu * strain
+
+
+@pytest.mark.parametrize("etype", ["_tetrahedron_4", "_hexahedron_8", "_triangle_6"])
+@pytest.mark.parametrize("per_point", [False, True])
+def test_eigen_grad_u_stress_matches_reference_check(etype, per_point):
+    """The reference's eigenstrain test: every node displaced by the linear
+    field alpha, eigen_grad_u = 0.1 in every entry, the stress at every point
+    equal to the analytic one within 1e-13 (infinity norm); here through the
+    material parameter, or written point by point as the test does."""
+    mesh = _patch_mesh(etype)
+    d = mesh.spatial_dimension
+    eig = np.full((d, d), 0.1)
+    mat = dict(STEEL_PLANE_STRAIN, rho=7800.0)
+    if not per_point:
+        mat = dict(mat, eigen_grad_u=eig)
+    o = oracle_model(mesh, [mat])
+    if per_point:
+        n = orc.lib().or_model_qp_size(o._m, 0)
+        o.set_eigen_grad_u(0, np.tile(eig.ravel(order="F"), (n, 1)))
+    o.set(orc.U, linear_field(mesh.nodes))
+    o.assemble_internal_forces()
+    expected = _eigen_prescribed_stress(eig, d)
+    for s in o.qp(0, orc.STRESS):
+        S = s.reshape(d, d, order="F")
+        assert np.max(np.abs(S - expected)) / np.max(np.abs(S)) <= 1e-13
+    g = o.qp(0, orc.GRAD_U)[0].reshape(d, d, order="F")
+    assert np.allclose(g, PATCH_ALPHA[:d, 1:1 + d] - eig, rtol=0, atol=1e-14)
+
+
+def test_plastic_thermal_term_follows_the_sigma_th_history():
+    """Heated plastic material (alpha delta_T != 0) in plane strain: the trial
+    stress of the first step after initFull adds (previous sigma_th - current
+    sigma_th) = -sigma_th to its 2 x 2 diagonal, which the 3 x 3 deviator (zero
+    out-of-plane entry) turns into an effective stress |sigma_th|: with
+    sigma_y below it the points yield at zero displacement.  A standalone
+    assembly takes the same term (its previous value is still the initial
+    zero) and updates the internals as the step would
+    (material_thermal.cc:33-34, material_thermal.hh:89-95,
+    material_linear_isotropic_hardening_inline_impl.hh:31-84)."""
+    mesh = _patch_mesh("_triangle_6")
+    mat = dict(type="plastic_linear_isotropic_hardening", name="hot", rho=1.0, E=1.0, nu=0.3,
+               sigma_y=1e-3, h=0.1, alpha=1e-3, delta_T=2.0)
+    sth = -1.0 / (1 - 0.6) * 1e-3 * 2.0
+    mu = 1.0 / 2.6
+    dp = (abs(sth) - 1e-3) / (3 * mu + 0.1)
+
+    def run(pre_assemble, steps):
+        o = oracle_model(mesh, [mat])
+        o.set_dt(1e-9)
+        if pre_assemble:
+            o.assemble_internal_forces()
+        o.step(steps)
+        return o
+
+    o = run(False, 1)
+    iso = o.qp(0, orc.ISO)
+    assert np.allclose(iso, 0.1 * dp, rtol=1e-12, atol=0)
+    eps = o.qp(0, orc.EPS_P)
+    # delta eps_p = 1.5 dp dev / sigma_eff on the 2 x 2 block: dev = -sth / 3 I
+    assert np.allclose(eps[:, [0, 3]], 1.5 * dp * (-sth / 3) / abs(sth), rtol=1e-12, atol=0)
+    assert np.all(eps[:, [1, 2]] == 0)
+    o2 = run(True, 0)
+    assert np.array_equal(o2.qp(0, orc.ISO), iso)
+    assert np.array_equal(o2.qp(0, orc.EPS_P), eps)
