@@ -456,6 +456,21 @@ int make_material(akb_model *m, const std::string &type, const std::string &name
   return AKB_OK;
 }
 
+// every double of x is +0.0 (a -0.0 counts as nonzero, which only costs the
+// step the read of f_ext): an OR over 64-bit words, 512 at a time
+bool all_zero_bits(const void *x, size_t n) {
+  const uint64_t *w = static_cast<const uint64_t *>(x);
+  size_t i = 0;
+  for (; i + 512 <= n; i += 512) {
+    uint64_t acc = 0;
+    for (size_t j = 0; j < 512; ++j) acc |= w[i + j];
+    if (acc) return false;
+  }
+  uint64_t acc = 0;
+  for (; i < n; ++i) acc |= w[i];
+  return acc == 0;
+}
+
 int check_model(akb_model *m, bool need_init) {
   if (!m) return fail(AKB_EINVAL, "null model");
   if (need_init && !m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
@@ -1506,11 +1521,10 @@ int akb_model_set_nodal(akb_model *m, int field, const void *host, int64_t nbyte
     break;
   case AKB_VELOCITY: dst = m->dv; m->predicted = false; break;
   case AKB_ACCELERATION: dst = m->da; m->predicted = false; break;
-  case AKB_EXTERNAL_FORCE: {
+  case AKB_EXTERNAL_FORCE:
     dst = m->dfext;
-    const double *h = (const double *)host;
-    m->fext_zero = std::all_of(h, h + nd, [](double x) { return x == 0.; });
-  } break;
+    m->fext_zero = all_zero_bits(host, (size_t)nd);
+    break;
   default: return fail(AKB_EINVAL, "field is read-only or unknown");
   }
   AKB_CUDA(cudaMemcpyAsync(dst, host, nbytes, cudaMemcpyHostToDevice, m->stream));

@@ -74,6 +74,10 @@ def parse():
     p.add_argument("--builders", type=int, default=8, help="serve: host build threads")
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-e2e-fp64", action="store_true",
+                   help="skip the end-to-end leg of the FP64 path")
+    p.add_argument("--no-extras", action="store_true",
+                   help="default configuration: skip the compact tri6 and batch records")
     p.add_argument("--precisions", default="mixed,fp64")
     p.add_argument("--accuracy-steps", type=int, default=10000,
                    help="steps of the mixed-vs-FP64 accuracy leg (0: skip)")
@@ -233,6 +237,21 @@ def read_traffic(config, precision):
         return t.get(f"{config}_{precision}")
     except Exception:
         return None
+
+
+def roofline_entry(kern_bytes, elem_ms, peak, peak_kind, traffic):
+    """the element-force kernel against the measured HBM peak: the formula's
+    algorithmic bytes per launch, and (when an ncu capture gave the kernel's
+    DRAM bytes per launch) the measured DRAM traffic per launch time"""
+    secs = elem_ms / 1e3
+    r = {"bound": "hbm", "kernel": "k_element_forces",
+         "achieved": kern_bytes / secs / 1e9, "peak": peak, "unit": "GB/s",
+         "frac": kern_bytes / secs / 1e9 / peak, "traffic": traffic,
+         "peak_source": f"{peak_kind} hbm_gbs"}
+    if traffic:
+        r["dram_achieved"] = traffic / secs / 1e9
+        r["dram_frac"] = traffic / secs / 1e9 / peak
+    return r
 
 
 class ClockSampler:
@@ -423,8 +442,9 @@ def run_reference(args):
 
 
 # ---- GPU leg ----------------------------------------------------------------------------
-def run_ours(args):
-    rep = Replicas("nccl")
+def run_ours(args, rep=None, emit=True, extra=False):
+    own = rep is None
+    rep = rep or Replicas("nccl")
     world, rank, local = rep.world, rep.rank, rep.local
     barrier, max_over_ranks = rep.barrier, rep.max
     import akantu2_b200 as akb
@@ -472,11 +492,8 @@ def run_ours(args):
             "phase_ms_per_step": {"predictor": phases[0] / nprof,
                                   "element_forces": phases[1] / nprof,
                                   "node_update": phases[2] / nprof},
-            "roofline": {"bound": "hbm", "kernel": "k_element_forces",
-                         "achieved": kern_b / (elem_ms / 1e3) / 1e9, "peak": peak,
-                         "unit": "GB/s", "frac": kern_b / (elem_ms / 1e3) / 1e9 / peak,
-                         "traffic": read_traffic(args.config, prec),
-                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "roofline": roofline_entry(kern_b, elem_ms, peak, peak_kind,
+                                       read_traffic(args.config, prec)),
             "roofline_step": {"bytes_per_element_step": step_b / E,
                               "achieved": step_b / (ms / args.steps / 1e3) / 1e9,
                               "frac": step_b / (ms / args.steps / 1e3) / 1e9 / peak},
@@ -495,10 +512,10 @@ def run_ours(args):
             # the state after the timed steps must be finite (device status word)
             "state_finite": m.getStatus() == 0 and bool(np.all(np.isfinite(m.getDisplacement()))),
         }
-        if prec == precisions[0]:
+        if (prec == precisions[0] and not extra) or (prec == "fp64" and not args.no_e2e_fp64):
             # end to end through the C ABI with pinned host buffers
             nb = int(np.prod(mesh.nodes.shape)) * 8
-            k_e2e = max(1, min(args.steps, 100))
+            k_e2e = max(1, min(args.steps, 100 if prec == precisions[0] else 20))
             secs_sync, secs_async = e2e_legs(m, mesh.nodes.shape, k_e2e, barrier)
             secs_sync, secs_async = max_over_ranks(secs_sync), max_over_ranks(secs_async)
             results[prec]["e2e"] = {"value": world * E * k_e2e / secs_async, "unit": UNIT,
@@ -513,10 +530,11 @@ def run_ours(args):
         del m
     head = results[precisions[0]]
     accuracy = None
-    if rank == 0 and args.accuracy_steps > 0 and set(precisions) >= {"mixed", "fp64"}:
+    if rank == 0 and not extra and args.accuracy_steps > 0 and \
+            set(precisions) >= {"mixed", "fp64"}:
         accuracy = accuracy_leg(akb, args.config, mesh, mat, v0, blocked, args.accuracy_steps)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not extra:
         threads = os.cpu_count() or 1
         rate, steps, secs = cpu_rate(args.config, mesh, mat, v0, blocked, budget_s=20.0,
                                      max_steps=50, threads=threads)
@@ -553,10 +571,15 @@ def run_ours(args):
             line[prec] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
                           "roofline": r["roofline"], "roofline_step": r["roofline_step"],
                           "phase_ms_per_step": r["phase_ms_per_step"]}
+            if "e2e" in r:
+                line[prec]["e2e"] = r["e2e"]
         if "fp64" in results and precisions[0] != "fp64":
             line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
-        print(json.dumps(line), flush=True)
-    rep.close()
+        if emit:
+            print(json.dumps(line), flush=True)
+    if own:
+        rep.close()
+    return line if rank == 0 else None
 
 
 L2_BYTES = 126 * 10**6  # B200 L2
@@ -590,29 +613,43 @@ def e2e_legs(m, shape, k, barrier):
     for f in fext:
         f.array[:] = 0.0
     nb = fext[0].array.nbytes
+    import ctypes
+    ticket = ctypes.c_int64()
+
+    def sync_steps(n):
+        for _ in range(n):
+            _capi.check(L.akb_model_set_nodal(m._h, _capi.EXTERNAL_FORCE,
+                                              _capi.ptr(fext[0].array), nb))
+            _capi.check(L.akb_model_solve_step(m._h, 1))
+            _capi.check(L.akb_model_get_nodal(m._h, _capi.DISPLACEMENT,
+                                              _capi.ptr(uout[0].array), nb))
+
+    def async_steps(n):
+        prev = None
+        for j in range(n):
+            _capi.check(L.akb_model_set_nodal_async(m._h, _capi.EXTERNAL_FORCE,
+                                                    _capi.ptr(fext[j % 2].array), nb))
+            _capi.check(L.akb_model_solve_step(m._h, 1))
+            _capi.check(L.akb_model_get_nodal_async(m._h, _capi.DISPLACEMENT,
+                                                    _capi.ptr(uout[j % 2].array), nb,
+                                                    ctypes.byref(ticket)))
+            if prev is not None:
+                _capi.check(L.akb_model_wait_nodal_async(m._h, prev))
+            prev = ticket.value
+        _capi.check(L.akb_model_synchronize(m._h))
+
+    # untimed warm-up of both legs: the first asynchronous call creates the
+    # copy streams and the staging buffers, and the first touches of the
+    # pinned buffers fault their pages in
+    sync_steps(3)
+    async_steps(3)
     barrier()
     t0 = time.perf_counter()
-    for _ in range(k):
-        _capi.check(L.akb_model_set_nodal(m._h, _capi.EXTERNAL_FORCE, _capi.ptr(fext[0].array), nb))
-        _capi.check(L.akb_model_solve_step(m._h, 1))
-        _capi.check(L.akb_model_get_nodal(m._h, _capi.DISPLACEMENT, _capi.ptr(uout[0].array), nb))
+    sync_steps(k)
     secs_sync = time.perf_counter() - t0
     barrier()
     t0 = time.perf_counter()
-    import ctypes
-    ticket = ctypes.c_int64()
-    prev = None
-    for j in range(k):
-        _capi.check(L.akb_model_set_nodal_async(m._h, _capi.EXTERNAL_FORCE,
-                                                _capi.ptr(fext[j % 2].array), nb))
-        _capi.check(L.akb_model_solve_step(m._h, 1))
-        _capi.check(L.akb_model_get_nodal_async(m._h, _capi.DISPLACEMENT,
-                                                _capi.ptr(uout[j % 2].array), nb,
-                                                ctypes.byref(ticket)))
-        if prev is not None:
-            _capi.check(L.akb_model_wait_nodal_async(m._h, prev))
-        prev = ticket.value
-    _capi.check(L.akb_model_synchronize(m._h))
+    async_steps(k)
     secs_async = time.perf_counter() - t0
     return secs_sync, secs_async
 
@@ -704,8 +741,9 @@ def build_batch(akb, meshes, mats, vels, blocks, precision):
     return b
 
 
-def run_batch(args):
-    rep = Replicas("nccl")
+def run_batch(args, rep=None, emit=True, extra=False):
+    own = rep is None
+    rep = rep or Replicas("nccl")
     world, rank, local = rep.world, rep.rank, rep.local
     barrier, max_over_ranks = rep.barrier, rep.max
     import akantu2_b200 as akb
@@ -741,11 +779,8 @@ def run_batch(args):
             "phase_ms_per_step": {"predictor": phases[0] / nprof,
                                   "element_forces": phases[1] / nprof,
                                   "node_update": phases[2] / nprof},
-            "roofline": {"bound": "hbm", "kernel": "k_element_forces",
-                         "achieved": kern_b / (elem_ms / 1e3) / 1e9, "peak": peak,
-                         "unit": "GB/s", "frac": kern_b / (elem_ms / 1e3) / 1e9 / peak,
-                         "traffic": read_traffic("batch", prec),
-                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "roofline": roofline_entry(kern_b, elem_ms, peak, peak_kind,
+                                       read_traffic("batch", prec)),
             "roofline_step": {"bytes_per_element_step": step_b / E,
                               "achieved": step_b / (ms / args.steps / 1e3) / 1e9,
                               "frac": step_b / (ms / args.steps / 1e3) / 1e9 / peak},
@@ -753,7 +788,7 @@ def run_batch(args):
             "gpu_launches": args.steps * 2,
             "state_finite": b.getStatus() == 0 and bool(np.all(np.isfinite(b.getDisplacement()))),
         }
-        if prec == precisions[0]:
+        if prec == precisions[0] and not extra:
             nb = N * 3 * 8
             k_e2e = max(1, min(args.steps, 100))
             secs_sync, secs_async = e2e_legs(b, (N, 3), k_e2e, barrier)
@@ -768,7 +803,7 @@ def run_batch(args):
     # unbatched baseline: every 16th instance alone (sizes spread over the
     # range), FP64, same step count with the same graphs
     alone_e, alone_ms = 0, 0.0
-    for k in range(0, len(meshes), max(1, len(meshes) // 16)):
+    for k in (range(0, len(meshes), max(1, len(meshes) // 16)) if not extra else []):
         m = akb.SolidMechanicsModel(meshes[k])
         m.addMaterial(mats[k]["type"], **{kk: v for kk, v in mats[k].items() if kk != "type"})
         m.initFull(akb._explicit_lumped_mass, precision="fp64")
@@ -782,10 +817,10 @@ def run_batch(args):
         alone_ms += m.timeSteps(args.steps)
         alone_e += meshes[k].getNbElement()
         del m
-    unbatched = alone_e * args.steps / (alone_ms / 1e3)
+    unbatched = alone_e * args.steps / (alone_ms / 1e3) if alone_ms > 0 else None
     head = results[precisions[0]]
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not extra:
         threads = os.cpu_count() or 1
         cpu = cpu_batch_rate(meshes, mats, vels, blocks, threads, budget_s=20.0)
     if rank == 0:
@@ -815,9 +850,13 @@ def run_batch(args):
                           "phase_ms_per_step": r["phase_ms_per_step"]}
         if "fp64" in results and precisions[0] != "fp64":
             line["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
-        line["speedup_vs_unbatched_fp64"] = head["value"] / unbatched
-        print(json.dumps(line), flush=True)
-    rep.close()
+        if unbatched:
+            line["speedup_vs_unbatched_fp64"] = head["value"] / unbatched
+        if emit:
+            print(json.dumps(line), flush=True)
+    if own:
+        rep.close()
+    return line if rank == 0 else None
 
 
 def cpu_serve_rate(reqs, threads, budget_s):
@@ -1020,6 +1059,39 @@ def ctypes_stream(model):
     return sp.value
 
 
+def compact(line):
+    """the figures of a configuration's line kept as a sub-record"""
+    keys = ("value", "ms_per_step", "roofline", "roofline_step", "phase_ms_per_step",
+            "speedup_vs_fp64", "clocks", "state_finite", "tuning")
+    out = {k: line[k] for k in keys if k in line}
+    out["workload"] = line["config"]["workload"]
+    out["elements"] = line["config"]["elements"]
+    if "fp64" in line:
+        out["fp64"] = {k: line["fp64"][k] for k in ("value", "ms_per_step", "roofline")
+                       if k in line["fp64"]}
+    return out
+
+
+def run_default_with_extras(args):
+    """The default run on one GPU: the hexahedral configuration's line, with
+    compact records of the plastic triangle square and of the 256-mesh batch
+    (mixed and FP64 each, 20 timed steps after the same warm-up, autotuned
+    shapes; no CPU, accuracy or end-to-end legs for those two) appended to
+    the same JSON line."""
+    import copy
+    rep = Replicas("nccl")
+    line = run_ours(args, rep=rep, emit=False)
+    extras = {}
+    for config, runner in (("tri6", run_ours), ("batch", run_batch)):
+        a = copy.copy(args)
+        a.config, a.steps, a.no_cpu, a.accuracy_steps, a.no_e2e_fp64 = config, 20, True, 0, True
+        a.precisions = "mixed,fp64"
+        extras[config] = compact(runner(a, rep=rep, emit=False, extra=True))
+    line["configs"] = extras
+    print(json.dumps(line), flush=True)
+    rep.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1030,6 +1102,9 @@ def main():
         run_serve(args)
     elif args.config == "batch":
         run_batch(args)
+    elif args.config == "hex8" and not args.no_extras and not args.cells and \
+            int(os.environ.get("WORLD_SIZE", "1")) == 1:
+        run_default_with_extras(args)
     else:
         run_ours(args)
 

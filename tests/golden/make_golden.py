@@ -1,6 +1,7 @@
 """Generates the golden fixtures of tests/golden/ from the reference's own test
-data.  Run once in a container that has the reference tree (REF below); the
-fixtures it writes are committed, the GPU host never reads the reference.
+data.  Run once in a container that has the reference tree, giving its root
+as the argument; the fixtures it writes are committed, the GPU host never
+reads the reference.
 
   fe_<type>.npz     meshes of test/test_fe_engine/_<type>.msh with
                     - the per-element inradius of test/test_fe_engine/_<type>.csv
@@ -12,7 +13,7 @@ fixtures it writes are committed, the GPU host never reads the reference.
   patch_<type>.npz  meshes of test/test_model/patch_tests/data/_<type>.msh
                     (patch tests and lumped-mass test)
 
-usage: python tests/golden/make_golden.py [REF]
+usage: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import contextlib
 import io
@@ -21,7 +22,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+REF = sys.argv[1]
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 GMSH_TYPE = {"_tetrahedron_4": (4, 4, 3), "_hexahedron_8": (5, 8, 3), "_triangle_6": (9, 6, 2)}
