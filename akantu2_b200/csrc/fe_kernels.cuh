@@ -946,6 +946,223 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
   for (int a = 0; a < 8; ++a) store_slot<3>(re, pos[(int64_t)a * E + e], A[lex[a]]);
 }
 
+// ---- sum-factorised hexahedra on packed FP32 pairs ---------------------------
+// sm_100 executes two FP32 operations of one thread as one packed
+// instruction (add / mul / fma .rn .f32x2), each lane rounded exactly like
+// the scalar operation.  The two Gauss points of an element that differ only
+// in xi (q and q + 1: the same eta and zeta) are evaluated as the two lanes
+// of one pair: their derivative rows, gradient, flux and projection are
+// packed operations, the per-element constants (adjugate, Lame constants)
+// broadcast to both lanes.  Lane x is the point at xi = -1/sqrt(3), lane y
+// the point at +1/sqrt(3).
+__device__ __forceinline__ float2 pb(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pneg(float2 a) { return make_float2(-a.x, -a.y); }
+
+// weighted first Piola-Kirchhoff stress of the neohookean law for a pair of
+// points (weight 1): the operations of neohookean_piola, lane by lane
+__device__ __forceinline__ void neohookean_piola_x2(float lambda, float mu, const float2 *g,
+                                                    float2 *P) {
+  float2 H2[9], K[9];
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      H2[i + 3 * j] = pfma(g[i + 6], g[2 + 3 * j], pfma(g[i + 3], g[1 + 3 * j], pmul(g[i], g[3 * j])));
+  const float2 t = padd(padd(g[0], g[4]), g[8]);
+  const float2 trH2 = padd(padd(H2[0], H2[4]), H2[8]);
+  const float2 i2 = pmul(pb(0.5f), pfma(t, t, pneg(trH2)));
+  const float2 m0 = pfma(g[4], g[8], pneg(pmul(g[5], g[7])));
+  const float2 m1 = pfma(g[1], g[8], pneg(pmul(g[2], g[7])));
+  const float2 m2 = pfma(g[1], g[5], pneg(pmul(g[2], g[4])));
+  const float2 detH = pfma(g[6], m2, pfma(pneg(g[3]), m1, pmul(g[0], m0)));
+  const float2 a = padd(t, i2);
+  const float2 dm1 = padd(a, detH);
+  const float2 nb = pneg(padd(pb(1.f), t));
+#pragma unroll
+  for (int k = 0; k < 9; ++k) K[k] = pfma(nb, g[k], H2[k]);
+  K[0] = padd(K[0], a);
+  K[4] = padd(K[4], a);
+  K[8] = padd(K[8], a);
+  const float2 det = padd(pb(1.f), dm1);
+  const float2 lnJ = make_float2(log1pf(dm1.x), log1pf(dm1.y));
+  const float2 rdet = make_float2(1.f / det.x, 1.f / det.y);
+  const float2 c = pmul(pfma(pb(lambda), lnJ, pb(-mu)), rdet);
+  const float2 a0 = pmul(pfma(pb(mu), dm1, pmul(pb(lambda), lnJ)), rdet);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float2 p = pfma(c, K[j + 3 * i], pmul(pb(mu), g[i + 3 * j]));
+      if (i == j) p = padd(p, a0);
+      P[i + 3 * j] = p;
+    }
+}
+
+// Cauchy stress of the elastic law for a pair of points
+// (material_elastic_inline_impl.hh:31-48), sigma_th included
+__device__ __forceinline__ void elastic_stress_x2(float lambda, float mu, float sth,
+                                                  const float2 *g, float2 *s) {
+  const float2 tr = padd(padd(g[0], g[4]), g[8]);
+  const float2 dia = pfma(pb(lambda), tr, pb(sth));
+  const float2 two_mu = pb(2.f * mu);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float2 v = pmul(two_mu, pmul(pb(.5f), padd(g[j + 3 * i], g[i + 3 * j])));
+      s[i + 3 * j] = (i == j) ? padd(v, dia) : v;
+    }
+}
+
+// PU pairs per unrolled iteration (1, 2 or 4); meshes of parallelepipeds
+// only (one adjugate per element, from the geometry table with GEO); the
+// elastic and neohookean laws (the plastic state is FP64 per point)
+template <int LAW, int PU, bool GEO>
+__device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, int64_t e_count,
+                                                  int64_t E, const int32_t *conn,
+                                                  const int32_t *pos, const double *X,
+                                                  const float *geo, const double *u,
+                                                  const MatParams &mp, const GroupArgs &ps,
+                                                  float *re) {
+  static_assert(LAW != LAW_PLASTIC, "plastic hexahedra use the scalar kernel");
+  const int64_t e = e_begin + le;
+  const MatParams mpe = group_params(mp, ps, le);
+  constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+  float wu[8][3];
+  double u0[3];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double uu = u[node * 3 + i];
+      if (a == 0) u0[i] = uu;
+      wu[lex[a]][i] = (float)(uu - u0[i]);
+    }
+  }
+  float Ja[9], rdet;
+  if constexpr (GEO) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ja[k] = geo[(int64_t)k * E + e];
+    rdet = geo[(int64_t)9 * E + e];
+  } else {
+    float wx[8][3];
+    hex8_geometry_modes(e, E, conn, X, wx);
+    rdet = hex8_affine_adjugate(wx, Ja);
+  }
+  wht8(wu);
+  constexpr float g1 = 0.577350269189625764509f;
+  constexpr float g2 = 1.f / 3.f;
+  // the modes carry the 1/det of the gradient (adj / det) and the Gauss
+  // coordinates of their bilinear and trilinear terms
+  const float rg1 = rdet * g1, rg2 = rdet * g2;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    wu[1][c] *= rdet; wu[2][c] *= rdet; wu[4][c] *= rdet;
+    wu[3][c] *= rg1; wu[5][c] *= rg1; wu[6][c] *= rg1; wu[7][c] *= rg2;
+  }
+  float A[8][3];
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) A[m][c] = 0.f;
+  const float lam = (float)mpe.lambda, mu = (float)mpe.mu, sth = (float)mpe.sigma_th;
+#pragma unroll 1
+  for (int po = 0; po < 4; po += PU)
+#pragma unroll
+  for (int pi = 0; pi < PU; ++pi) {
+    const int pr = po + pi;  // pair: points 2 pr (lane x) and 2 pr + 1 (lane y)
+    const float sy = (pr & 1) ? 1.f : -1.f, sz = (pr & 2) ? 1.f : -1.f;
+    // 8 du_j/dxi_k: row 0 is the same for both points; rows 1 and 2 are
+    // r -+ s (xi = -+1/sqrt(3))
+    float2 D1[3], D2[3];
+    float D0[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      D0[j] = (wu[1][j] + sy * wu[3][j]) + sz * (wu[5][j] + sy * wu[7][j]);
+      const float r1 = wu[2][j] + sz * wu[6][j], s1 = wu[3][j] + sz * wu[7][j];
+      const float r2 = wu[4][j] + sy * wu[6][j], s2 = wu[5][j] + sy * wu[7][j];
+      D1[j] = make_float2(r1 - s1, r1 + s1);
+      D2[j] = make_float2(r2 - s2, r2 + s2);
+    }
+    // grad u (i, j) = sum_k adj(j, k) 8 du_i/dxi_k / det
+    float2 gr[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        gr[i + 3 * j] = pfma(pb(Ja[j + 6]), D2[i], pfma(pb(Ja[j + 3]), D1[i], pb(Ja[j] * D0[i])));
+    if (ps.eig) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int64_t i0 = (int64_t)((2 * pr) * 9 + k) * e_count + le;
+        gr[k] = make_float2(gr[k].x - (float)ps.eig[i0], gr[k].y - (float)ps.eig[i0 + 9 * e_count]);
+      }
+    }
+    float2 P[9];
+    if constexpr (LAW == LAW_NEOHOOKEAN) {
+      if (mpe.svk) {
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+          float gl[9], S[9], Pl[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) gl[k] = l ? gr[k].y : gr[k].x;
+          finite_pk2<3, float>(mpe, gl, S);
+          first_piola<3, float>(gl, S, 1.f, Pl);
+#pragma unroll
+          for (int k = 0; k < 9; ++k) (l ? P[k].y : P[k].x) = Pl[k];
+        }
+      } else {
+        neohookean_piola_x2(lam, mu, gr, P);
+      }
+    } else {
+      elastic_stress_x2(lam, mu, sth, gr, P);
+    }
+    // H(k, m) = sum_J P(k, J) adj(J, m), folded into the modes: with
+    // S = H.x + H.y and T = H.y - H.x (the xi sign of lane y is +1)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float2 H0 = pfma(P[k + 6], pb(Ja[2]), pfma(P[k + 3], pb(Ja[1]), pmul(P[k], pb(Ja[0]))));
+      const float2 H1 = pfma(P[k + 6], pb(Ja[5]), pfma(P[k + 3], pb(Ja[4]), pmul(P[k], pb(Ja[3]))));
+      const float2 H2 = pfma(P[k + 6], pb(Ja[8]), pfma(P[k + 3], pb(Ja[7]), pmul(P[k], pb(Ja[6]))));
+      const float S0 = H0.x + H0.y, S1 = H1.x + H1.y, S2 = H2.x + H2.y;
+      const float T1 = H1.y - H1.x, T2 = H2.y - H2.x;
+      A[1][k] += S0;
+      A[2][k] += S1;
+      A[4][k] += S2;
+      A[3][k] += sy * S0 + T1;
+      A[5][k] += sz * S0 + T2;
+      A[6][k] += sz * S1 + sy * S2;
+      A[7][k] += sy * sz * S0 + sz * T1 + sy * T2;
+    }
+  }
+  constexpr float s0 = 1.f / 512.f, s1 = g1 / 512.f, s2 = g2 / 512.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    A[1][c] *= s0; A[2][c] *= s0; A[4][c] *= s0;
+    A[3][c] *= s1; A[5][c] *= s1; A[6][c] *= s1; A[7][c] *= s2;
+  }
+  iwht8(A);
+#pragma unroll
+  for (int a = 0; a < 8; ++a) store_slot<3>(re, pos[(int64_t)a * E + e], A[lex[a]]);
+}
+
+template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_element_forces_hex8sf_x2(int64_t e_begin, int64_t e_count, int64_t E,
+                               const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                               const double *__restrict__ X, const float *__restrict__ geo,
+                               const double *__restrict__ u, MatParams mp, GroupArgs ps,
+                               float *__restrict__ re) {
+  pdl_begin();
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count) return;
+  element_hex8sf_x2<LAW, PU, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
+}
+
 // MINB: blocks per SM the register allocation must allow (1: the compiler's
 // choice)
 template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false, bool GEO = false>

@@ -25,6 +25,9 @@ struct ElemTuning {
   int qu = 8;
   int minb = 1;
 };
+// points_per_iteration flag of the mixed hexahedron kernel: the points are
+// evaluated as packed FP32 pairs (2, 4 or 8 points per iteration)
+constexpr int kPackedPoints = 256;
 
 // device view of the mesh, internal element order
 struct DevGeom {
@@ -83,6 +86,14 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
                                         const float *fwJ, const double *u,
                                         const MatParams &mp, const GroupArgs &ps,
                                         float *re, const ElemTuning &tn, cudaStream_t s);
+// mixed hexahedra of a mesh of parallelepipeds, elastic or neohookean law:
+// the sum-factorised kernel on packed FP32 pairs of points; points per
+// unrolled iteration 2, 4 or 8; minb: resident blocks per SM the registers
+// are capped for (1, 4 or 5); 128 threads
+cudaError_t launch_element_forces_hex8_x2(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                          const double *u, const MatParams &mp,
+                                          const GroupArgs &ps, float *re, int points,
+                                          int minb, cudaStream_t s);
 // flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
 // the predictor of the next step reads u and writes u_next
 // node_block: threads per block of the node update (any multiple of 32 up to

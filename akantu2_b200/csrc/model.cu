@@ -2143,6 +2143,15 @@ int akb_model_set_affine_kernel(akb_model *m, int on) {
   }
   AKB_CUDA(cudaStreamSynchronize(m->stream));
   m->affine_kernel = on;
+  // the packed form exists for meshes of parallelepipeds only: without the
+  // kernel compiled for them, the scalar form with the same points per
+  // iteration (2 or 8; 4 becomes 2) and a register cap that does not spill
+  if (!on)
+    for (auto &gr : m->groups)
+      if (gr.tune.qu & AKB_POINTS_PACKED) {
+        const int pts = gr.tune.qu & ~AKB_POINTS_PACKED;
+        gr.tune = ElemTuning{128, pts == 8 ? 8 : 2, pts == 8 ? 1 : 4};
+      }
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
   return AKB_OK;
@@ -2199,19 +2208,30 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   const int q = points_per_iteration;
   const bool sf = m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED;
   const bool tet_mixed = m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_MIXED;
-  if (!sf && q != 8 && !(tet_mixed && q == 0))
+  if (q & AKB_POINTS_PACKED) {
+    // packed FP32 pairs: mixed hexahedra of a mesh of parallelepipeds with the
+    // kernel compiled for them, elastic or neohookean, 128 threads
+    const int pts = q & ~AKB_POINTS_PACKED;
+    if (!sf || !m->affine_kernel || law == LAW_PLASTIC)
+      return fail(AKB_EINVAL, "packed points need mixed hexahedra of a mesh of parallelepipeds "
+                              "(affine kernel on), elastic or neohookean");
+    if (pts != 2 && pts != 4 && pts != 8)
+      return fail(AKB_EINVAL, "packed points per iteration must be 2, 4 or 8");
+    if (element_block != 128 || (min_blocks != 1 && min_blocks != 4 && min_blocks != 5))
+      return fail(AKB_EINVAL, "packed points run with 128 threads and min_blocks 1, 4 or 5");
+  } else if (!sf && q != 8 && !(tet_mixed && q == 0))
     return fail(AKB_EINVAL, "points_per_iteration is 8 (or 0 for the recomputed form of mixed "
                             "tetrahedra and hexahedra)");
-  if (sf && q != 0 && q != 1 && q != 2 && q != 8)
+  if (sf && !(q & AKB_POINTS_PACKED) && q != 0 && q != 1 && q != 2 && q != 8)
     return fail(AKB_EINVAL, "points_per_iteration must be 0, 1, 2 or 8");
   if (sf && q == 1 && element_block != 128)
     return fail(AKB_EINVAL, "1 point per iteration runs with 128 threads");
-  const bool capped_sf = sf && q != 0 && element_block == 128 &&
+  const bool capped_sf = sf && q != 0 && element_block == 128 && !(q & AKB_POINTS_PACKED) &&
                          (min_blocks == 5 || (min_blocks == 4 && q == 2) ||
                           (min_blocks == 6 && (q == 1 || q == 2)));
   const bool capped_plastic = m->et != AKB_HEXAHEDRON_8 && law == LAW_PLASTIC &&
                               (min_blocks == 5 || min_blocks == 6) && element_block == 128;
-  if (min_blocks != 1 && !capped_sf && !capped_plastic)
+  if (min_blocks != 1 && !capped_sf && !capped_plastic && !(q & AKB_POINTS_PACKED))
     return fail(AKB_EINVAL, "min_blocks is 1; 5 (or 4 with 2 points per iteration, 6 with 1 or "
                             "2) for the 128-thread mixed hexahedron kernel; 5 or 6 for "
                             "128-thread plastic tetrahedra and triangles");

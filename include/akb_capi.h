@@ -320,6 +320,11 @@ int akb_model_autotune(akb_model *model, int repeats);
  * for that many resident blocks per SM: 5 for the mixed hexahedron kernel
  * (4 with 2 points per iteration, 6 with 1 or 2), 5 or 6 for plastic
  * tetrahedra and triangles (same results) */
+/* flag of points_per_iteration (mixed hexahedra of a mesh of parallelepipeds,
+ * elastic or neohookean, 128 threads, min_blocks 1, 4 or 5): the Gauss
+ * points are evaluated as packed FP32 pairs, 2, 4 or 8 points per iteration
+ * (e.g. AKB_POINTS_PACKED | 2); a different FP32 evaluation order again */
+#define AKB_POINTS_PACKED 256
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
