@@ -144,6 +144,9 @@ def lib():
         "akb_batch_nb_instances": (c_int, [vp, ctypes.POINTER(c_int)]),
         "akb_batch_instance_offsets": (c_int, [vp, vp, vp]),
         "akb_batch_set_instance_materials": (c_int, [vp, vp]),
+        "akb_batch_set_instance_steps": (c_int, [vp, vp]),
+        "akb_batch_instance_steps_left": (c_int, [vp, vp]),
+        "akb_batch_copy_instance_nodal": (c_int, [vp, c_int, c_int, vp, i64]),
         "akb_batch_get_stable_time_steps": (c_int, [vp, vp]),
         "akb_batch_set_time_steps": (c_int, [vp, vp]),
         "akb_batch_get_time_steps": (c_int, [vp, vp]),

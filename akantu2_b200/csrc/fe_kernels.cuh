@@ -107,7 +107,18 @@ struct GroupArgs {
   // eigen gradient of the displacement [q][d*d][ne] (double), subtracted from
   // the gradient before the law (material.cc:147), or null when zero
   const double *eig;
+  // batches whose instances stop after their own step counts: instance of
+  // each element of the launch [ne], the step count at which each instance
+  // stops, and the device's step counter (all null otherwise)
+  const int32_t *einst;
+  const int64_t *inst_end;
+  const int64_t *step;
 };
+
+// the element's instance still advances in this step
+__device__ __forceinline__ bool element_active(const GroupArgs &ps, int64_t le) {
+  return !ps.inst_end || *ps.step < ps.inst_end[ps.einst[le]];
+}
 
 // grad u -= eigen_grad_u at point (le, q) of a launch over ne elements
 template <int D, class T>
@@ -606,7 +617,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                         RT *__restrict__ re) {
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
+  if (le >= e_count || !element_active(ps, le)) return;
   element_pe<D, NN, NQ, LAW, T, RT>(le, e_begin, e_count, E, conn, pos, B, wJ, u, mp, ps, re);
 }
 
@@ -693,7 +704,7 @@ __global__ void __launch_bounds__(BLOCK)
                          float *__restrict__ re) {
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
+  if (le >= e_count || !element_active(ps, le)) return;
   element_geo<D, NN, NQ, LAW>(le, e_begin, e_count, E, conn, pos, X, tab, u, mp, ps, re);
 }
 
@@ -962,30 +973,34 @@ __device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 pneg(float2 a) { return make_float2(-a.x, -a.y); }
 
 // weighted first Piola-Kirchhoff stress of the neohookean law for a pair of
-// points (weight 1): the operations of neohookean_piola, lane by lane
+// points (weight 1), P = mu F + c cof(F), written in the displacement
+// gradient H = F - I like neohookean_piola, with the cofactor expansion
+//   adj(I + H) = I + t I - H + adj(H)       (t = tr H; Cayley-Hamilton)
+// whose quadratic part adj(H) is formed from the 2 x 2 minors of H directly
+// (18 operations instead of the 27 of H^2), and
+//   det F - 1 = t + i2 + det H,  i2 = tr adj(H),  det H = H(0, :) . adj(H)(:, 0)
 __device__ __forceinline__ void neohookean_piola_x2(float lambda, float mu, const float2 *g,
                                                     float2 *P) {
-  float2 H2[9], K[9];
+  float2 adj[9];
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-      H2[i + 3 * j] = pfma(g[i + 6], g[2 + 3 * j], pfma(g[i + 3], g[1 + 3 * j], pmul(g[i], g[3 * j])));
+    for (int i = 0; i < 3; ++i) {
+      // adj(H)(i, j) = cofactor (j, i) of H
+      const int j1 = (j + 1) % 3, j2 = (j + 2) % 3, i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+      adj[i + 3 * j] = pfma(g[j1 + 3 * i1], g[j2 + 3 * i2], pneg(pmul(g[j1 + 3 * i2], g[j2 + 3 * i1])));
+    }
   const float2 t = padd(padd(g[0], g[4]), g[8]);
-  const float2 trH2 = padd(padd(H2[0], H2[4]), H2[8]);
-  const float2 i2 = pmul(pb(0.5f), pfma(t, t, pneg(trH2)));
-  const float2 m0 = pfma(g[4], g[8], pneg(pmul(g[5], g[7])));
-  const float2 m1 = pfma(g[1], g[8], pneg(pmul(g[2], g[7])));
-  const float2 m2 = pfma(g[1], g[5], pneg(pmul(g[2], g[4])));
-  const float2 detH = pfma(g[6], m2, pfma(pneg(g[3]), m1, pmul(g[0], m0)));
-  const float2 a = padd(t, i2);
-  const float2 dm1 = padd(a, detH);
-  const float2 nb = pneg(padd(pb(1.f), t));
+  const float2 i2 = padd(padd(adj[0], adj[4]), adj[8]);
+  const float2 detH = pfma(g[6], adj[2], pfma(g[3], adj[1], pmul(g[0], adj[0])));
+  const float2 dm1 = padd(padd(t, i2), detH);
+  // K = adj(I + H) - I = adj(H) - H + t I; cof(F) = I + K^T
+  float2 K[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) K[k] = pfma(nb, g[k], H2[k]);
-  K[0] = padd(K[0], a);
-  K[4] = padd(K[4], a);
-  K[8] = padd(K[8], a);
+  for (int k = 0; k < 9; ++k) K[k] = padd(adj[k], pneg(g[k]));
+  K[0] = padd(K[0], t);
+  K[4] = padd(K[4], t);
+  K[8] = padd(K[8], t);
   const float2 det = padd(pb(1.f), dm1);
   const float2 lnJ = make_float2(log1pf(dm1.x), log1pf(dm1.y));
   const float2 rdet = make_float2(1.f / det.x, 1.f / det.y);
@@ -1007,7 +1022,7 @@ __device__ __forceinline__ void elastic_stress_x2(float lambda, float mu, float 
                                                   const float2 *g, float2 *s) {
   const float2 tr = padd(padd(g[0], g[4]), g[8]);
   const float2 dia = pfma(pb(lambda), tr, pb(sth));
-  const float2 two_mu = pb(2.f * mu);
+  const float2 two_mu = pb(__fmul_rn(2.f, mu));
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
@@ -1020,6 +1035,11 @@ __device__ __forceinline__ void elastic_stress_x2(float lambda, float mu, float 
 // PU pairs per unrolled iteration (1, 2 or 4); meshes of parallelepipeds
 // only (one adjugate per element, from the geometry table with GEO); the
 // elastic and neohookean laws (the plastic state is FP64 per point)
+// PU pairs per unrolled iteration (1, 2 or 4); meshes of parallelepipeds
+// only (one adjugate per element, from the geometry table with GEO); the
+// elastic and neohookean laws (the plastic state is FP64 per point).  Every
+// FP32 operation is explicitly rounded (scalar __f*_rn or packed .rn), so
+// neither the points per iteration nor the register cap changes a result.
 template <int LAW, int PU, bool GEO>
 __device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, int64_t e_count,
                                                   int64_t E, const int32_t *conn,
@@ -1058,11 +1078,16 @@ __device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, i
   constexpr float g2 = 1.f / 3.f;
   // the modes carry the 1/det of the gradient (adj / det) and the Gauss
   // coordinates of their bilinear and trilinear terms
-  const float rg1 = rdet * g1, rg2 = rdet * g2;
+  const float rg1 = __fmul_rn(rdet, g1), rg2 = __fmul_rn(rdet, g2);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    wu[1][c] *= rdet; wu[2][c] *= rdet; wu[4][c] *= rdet;
-    wu[3][c] *= rg1; wu[5][c] *= rg1; wu[6][c] *= rg1; wu[7][c] *= rg2;
+    wu[1][c] = __fmul_rn(wu[1][c], rdet);
+    wu[2][c] = __fmul_rn(wu[2][c], rdet);
+    wu[4][c] = __fmul_rn(wu[4][c], rdet);
+    wu[3][c] = __fmul_rn(wu[3][c], rg1);
+    wu[5][c] = __fmul_rn(wu[5][c], rg1);
+    wu[6][c] = __fmul_rn(wu[6][c], rg1);
+    wu[7][c] = __fmul_rn(wu[7][c], rg2);
   }
   float A[8][3];
 #pragma unroll
@@ -1075,31 +1100,35 @@ __device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, i
 #pragma unroll
   for (int pi = 0; pi < PU; ++pi) {
     const int pr = po + pi;  // pair: points 2 pr (lane x) and 2 pr + 1 (lane y)
+    // sign products are exact: sy, sz = +-1
     const float sy = (pr & 1) ? 1.f : -1.f, sz = (pr & 2) ? 1.f : -1.f;
-    // 8 du_j/dxi_k: row 0 is the same for both points; rows 1 and 2 are
-    // r -+ s (xi = -+1/sqrt(3))
+    // du_j/dxi_k (times 8 / det): row 0 is the same for both points; rows 1
+    // and 2 are r -+ s (xi = -+1/sqrt(3))
     float2 D1[3], D2[3];
     float D0[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      D0[j] = (wu[1][j] + sy * wu[3][j]) + sz * (wu[5][j] + sy * wu[7][j]);
-      const float r1 = wu[2][j] + sz * wu[6][j], s1 = wu[3][j] + sz * wu[7][j];
-      const float r2 = wu[4][j] + sy * wu[6][j], s2 = wu[5][j] + sy * wu[7][j];
-      D1[j] = make_float2(r1 - s1, r1 + s1);
-      D2[j] = make_float2(r2 - s2, r2 + s2);
+      D0[j] = __fadd_rn(__fadd_rn(wu[1][j], sy * wu[3][j]),
+                        sz * __fadd_rn(wu[5][j], sy * wu[7][j]));
+      const float r1 = __fadd_rn(wu[2][j], sz * wu[6][j]), s1 = __fadd_rn(wu[3][j], sz * wu[7][j]);
+      const float r2 = __fadd_rn(wu[4][j], sy * wu[6][j]), s2 = __fadd_rn(wu[5][j], sy * wu[7][j]);
+      D1[j] = make_float2(__fadd_rn(r1, -s1), __fadd_rn(r1, s1));
+      D2[j] = make_float2(__fadd_rn(r2, -s2), __fadd_rn(r2, s2));
     }
-    // grad u (i, j) = sum_k adj(j, k) 8 du_i/dxi_k / det
+    // grad u (i, j) = sum_k adj(j, k) du_i/dxi_k / det
     float2 gr[9];
 #pragma unroll
     for (int j = 0; j < 3; ++j)
 #pragma unroll
       for (int i = 0; i < 3; ++i)
-        gr[i + 3 * j] = pfma(pb(Ja[j + 6]), D2[i], pfma(pb(Ja[j + 3]), D1[i], pb(Ja[j] * D0[i])));
+        gr[i + 3 * j] = pfma(pb(Ja[j + 6]), D2[i],
+                             pfma(pb(Ja[j + 3]), D1[i], pb(__fmul_rn(Ja[j], D0[i]))));
     if (ps.eig) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         const int64_t i0 = (int64_t)((2 * pr) * 9 + k) * e_count + le;
-        gr[k] = make_float2(gr[k].x - (float)ps.eig[i0], gr[k].y - (float)ps.eig[i0 + 9 * e_count]);
+        gr[k] = make_float2(__fadd_rn(gr[k].x, -(float)ps.eig[i0]),
+                            __fadd_rn(gr[k].y, -(float)ps.eig[i0 + 9 * e_count]));
       }
     }
     float2 P[9];
@@ -1128,22 +1157,28 @@ __device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, i
       const float2 H0 = pfma(P[k + 6], pb(Ja[2]), pfma(P[k + 3], pb(Ja[1]), pmul(P[k], pb(Ja[0]))));
       const float2 H1 = pfma(P[k + 6], pb(Ja[5]), pfma(P[k + 3], pb(Ja[4]), pmul(P[k], pb(Ja[3]))));
       const float2 H2 = pfma(P[k + 6], pb(Ja[8]), pfma(P[k + 3], pb(Ja[7]), pmul(P[k], pb(Ja[6]))));
-      const float S0 = H0.x + H0.y, S1 = H1.x + H1.y, S2 = H2.x + H2.y;
-      const float T1 = H1.y - H1.x, T2 = H2.y - H2.x;
-      A[1][k] += S0;
-      A[2][k] += S1;
-      A[4][k] += S2;
-      A[3][k] += sy * S0 + T1;
-      A[5][k] += sz * S0 + T2;
-      A[6][k] += sz * S1 + sy * S2;
-      A[7][k] += sy * sz * S0 + sz * T1 + sy * T2;
+      const float S0 = __fadd_rn(H0.x, H0.y), S1 = __fadd_rn(H1.x, H1.y),
+                  S2 = __fadd_rn(H2.x, H2.y);
+      const float T1 = __fadd_rn(H1.y, -H1.x), T2 = __fadd_rn(H2.y, -H2.x);
+      A[1][k] = __fadd_rn(A[1][k], S0);
+      A[2][k] = __fadd_rn(A[2][k], S1);
+      A[4][k] = __fadd_rn(A[4][k], S2);
+      A[3][k] = __fadd_rn(A[3][k], __fadd_rn(sy * S0, T1));
+      A[5][k] = __fadd_rn(A[5][k], __fadd_rn(sz * S0, T2));
+      A[6][k] = __fadd_rn(A[6][k], __fadd_rn(sz * S1, sy * S2));
+      A[7][k] = __fadd_rn(A[7][k], __fadd_rn(__fadd_rn((sy * sz) * S0, sz * T1), sy * T2));
     }
   }
   constexpr float s0 = 1.f / 512.f, s1 = g1 / 512.f, s2 = g2 / 512.f;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    A[1][c] *= s0; A[2][c] *= s0; A[4][c] *= s0;
-    A[3][c] *= s1; A[5][c] *= s1; A[6][c] *= s1; A[7][c] *= s2;
+    A[1][c] = __fmul_rn(A[1][c], s0);
+    A[2][c] = __fmul_rn(A[2][c], s0);
+    A[4][c] = __fmul_rn(A[4][c], s0);
+    A[3][c] = __fmul_rn(A[3][c], s1);
+    A[5][c] = __fmul_rn(A[5][c], s1);
+    A[6][c] = __fmul_rn(A[6][c], s1);
+    A[7][c] = __fmul_rn(A[7][c], s2);
   }
   iwht8(A);
 #pragma unroll
@@ -1159,7 +1194,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                                float *__restrict__ re) {
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
+  if (le >= e_count || !element_active(ps, le)) return;
   element_hex8sf_x2<LAW, PU, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
 }
 
@@ -1174,7 +1209,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                             float *__restrict__ re) {
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-  if (le >= e_count) return;
+  if (le >= e_count || !element_active(ps, le)) return;
   element_hex8sf<LAW, QU, AFF, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
 }
 
@@ -1194,7 +1229,7 @@ __global__ void __launch_bounds__(32 * NQ)
   const int lane = threadIdx.x & 31;
   const int q = threadIdx.x >> 5;
   const int64_t le = (int64_t)blockIdx.x * 32 + lane;
-  const bool active = le < e_count;
+  const bool active = le < e_count && element_active(ps, le);
   const int64_t e = e_begin + le;
   if (active) {
     for (int a = q; a < NN; a += NQ) {
@@ -1459,6 +1494,43 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
   if (i >= N) return;
   node_body<D, RT, KAHAN, WIDE>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt,
                                 node_inst, inst_dt, flags, status);
+}
+
+// Node update of a batch whose instances stop after their own step counts:
+// a node of a stopped instance keeps its state; the displacement buffer that
+// becomes the model's displacement after this step (u, the prediction's
+// buffer) takes the value of the other one (u_next), which holds the
+// instance's last displacement, so that both buffers hold it from then on
+template <int D, class RT, bool KAHAN>
+__global__ void k_node_update_retire(int64_t N, const int32_t *__restrict__ ptr,
+                                     const RT *__restrict__ re, const double *__restrict__ fext,
+                                     const double *__restrict__ mass,
+                                     const uint8_t *__restrict__ blocked,
+                                     double *__restrict__ fint, double *__restrict__ a,
+                                     double *__restrict__ v, double *u, double *u_next, double dt,
+                                     const int32_t *__restrict__ node_inst,
+                                     const double *__restrict__ inst_dt,
+                                     const int64_t *__restrict__ inst_end,
+                                     const int64_t *__restrict__ step, int flags,
+                                     unsigned int *__restrict__ status) {
+  pdl_begin();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  if (*step >= inst_end[node_inst[i]]) {
+    if (flags & NU_PREDICT) {
+#pragma unroll
+      for (int c = 0; c < D; ++c) u[i * D + c] = u_next[i * D + c];
+    }
+    return;
+  }
+  node_body<D, RT, KAHAN, false>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt,
+                                 node_inst, inst_dt, flags, status);
+}
+
+// the step counter of a batch with stopping instances, after each step
+static __global__ void k_step_advance(int64_t *step) {
+  pdl_begin();
+  *step += 1;
 }
 
 // Node update with the gather staged through shared memory: the slots of

@@ -119,6 +119,12 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
                                     double *a, double *v, const double *u, double *u_next,
                                     double dt, int flags, unsigned int *status, int node_block,
                                     bool staged, cudaStream_t s) {
+  if (g.N > 0 && g.inst_end) {
+    auto kern = g.D == 3 ? k_node_update_retire<3, double, false> : k_node_update_retire<2, double, false>;
+    return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
+                       fext, mass, blocked, fint, a, v, const_cast<double *>(u), u_next, dt,
+                       g.node_inst, g.inst_dt, g.inst_end, (const int64_t *)g.step, flags, status);
+  }
   if (g.N == 0) return cudaSuccess;
   if (staged) {
     AKB_DISPATCH_NODE_BLOCK(node_block, {
@@ -173,6 +179,10 @@ cudaError_t launch_prescribe(int64_t count, const int64_t *dofs, const double *u
                              double *u, bool advance, bool pdl, cudaStream_t s) {
   return launch_step(pdl, k_prescribe, 1, 512, s, count, dofs, u0, v_max, (double)ramp_steps,
                      dt, acc, step, u, advance ? 1 : 0);
+}
+
+cudaError_t launch_step_advance(const DevGeom &g, cudaStream_t s) {
+  return launch_step(g.pdl, k_step_advance, 1, 1, s, g.step);
 }
 
 // ---- fields and energies ---------------------------------------------------

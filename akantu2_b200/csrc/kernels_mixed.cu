@@ -172,6 +172,12 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                                      double *u_next, double dt, int flags,
                                      unsigned int *status, int node_block, bool staged,
                                      cudaStream_t s) {
+  if (g.N > 0 && g.inst_end) {
+    auto kern = g.D == 3 ? k_node_update_retire<3, float, true> : k_node_update_retire<2, float, true>;
+    return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
+                       fext, mass, blocked, fint, a, v, const_cast<double *>(u), u_next, dt,
+                       g.node_inst, g.inst_dt, g.inst_end, (const int64_t *)g.step, flags, status);
+  }
   if (g.N == 0) return cudaSuccess;
   if (staged) {
     AKB_DISPATCH_NODE_BLOCK(node_block, {

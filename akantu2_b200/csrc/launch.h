@@ -49,6 +49,10 @@ struct DevGeom {
   int affine = 0;
   // with affine: the adjugate and 1/det of each element [10][E], or null
   const float *geo = nullptr;
+  // batch whose instances stop after their own step counts: the step count
+  // at which each instance stops and the device step counter (null otherwise)
+  const int64_t *inst_end = nullptr;
+  int64_t *step = nullptr;
 };
 
 // ---- init ------------------------------------------------------------------
@@ -110,6 +114,9 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                                      double *u_next, double dt, int flags,
                                      unsigned int *status, int node_block, bool staged,
                                      cudaStream_t s);
+
+// the device step counter of a batch with stopping instances, + 1
+cudaError_t launch_step_advance(const DevGeom &g, cudaStream_t s);
 
 // prescribed velocity ramp on a set of dofs (u indices node * D + c), written
 // into the displacement the next step starts from; acc and step live on the

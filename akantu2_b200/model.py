@@ -687,3 +687,30 @@ class BatchModel(SolidMechanicsModel):
         dt = np.zeros(self.nb_instances)
         _capi.check(_capi.lib().akb_batch_get_time_steps(self._h, _capi.ptr(dt)))
         return dt
+
+    def setInstanceSteps(self, steps):
+        """From the current step on, instance k advances exactly steps[k] more
+        steps (negative: its limit stays as it is, initially none), then
+        keeps its u, v and a while the others go on
+        (akb_batch_set_instance_steps)."""
+        self._sync_up()
+        st = np.ascontiguousarray(steps, dtype=np.int64)
+        if st.shape != (self.nb_instances,):
+            raise ValueError("one step count per instance")
+        _capi.check(_capi.lib().akb_batch_set_instance_steps(self._h, _capi.ptr(st)))
+
+    def getInstanceStepsLeft(self):
+        left = np.zeros(self.nb_instances, dtype=np.int64)
+        _capi.check(_capi.lib().akb_batch_instance_steps_left(self._h, _capi.ptr(left)))
+        return left
+
+    def getInstanceNodal(self, field, k):
+        """one instance's displacement, velocity or acceleration, copied
+        after the steps enqueued so far"""
+        sl = self.instance_nodes(k)
+        out = np.zeros((sl.stop - sl.start, self.dim))
+        L = _capi.lib()
+        _capi.check(L.akb_batch_copy_instance_nodal(self._h, _FIELDS[field], int(k),
+                                                    _capi.ptr(out), out.nbytes))
+        _capi.check(L.akb_model_synchronize(self._h))
+        return out

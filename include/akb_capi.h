@@ -413,6 +413,23 @@ int akb_batch_instance_offsets(const akb_model *model, int64_t *node_offsets,
                                int64_t *element_offsets);
 /* material index of every element of instance k (before initFull) */
 int akb_batch_set_instance_materials(akb_model *model, const int32_t *material_of_instance);
+/* Instances that stop after their own step counts (the serving loop's
+ * batches): from the current step on, instance k advances exactly steps[k]
+ * more steps (steps[k] < 0: its limit stays as it is, initially none) and
+ * then keeps its state (u, v, a;
+ * its plastic internals are not maintained) while the others go on; the
+ * captured step graphs stay valid (each step's kernels read the device's
+ * step counter).  Called again, it sets new counts from the current step. */
+int akb_batch_set_instance_steps(akb_model *model, const int64_t *steps);
+/* steps each instance still advances (-1: no limit set) */
+int akb_batch_instance_steps_left(const akb_model *model, int64_t *left);
+/* enqueues on the model's stream a copy of one instance's nodal field
+ * (AKB_DISPLACEMENT, AKB_VELOCITY or AKB_ACCELERATION; N_k * dim doubles) to
+ * host memory, after the steps enqueued so far; synchronise the model's
+ * stream (or an event recorded on it) before reading the buffer, which
+ * should be pinned for the copy to be asynchronous */
+int akb_batch_copy_instance_nodal(akb_model *model, int field, int instance, void *host,
+                                  int64_t nbytes);
 /* getStableTimeStep of every instance -> dt[nb_instances] */
 int akb_batch_get_stable_time_steps(akb_model *model, double *dt);
 /* setTimeStep per instance (akb_model_set_time_step sets them all) */

@@ -136,3 +136,39 @@ def test_batch_time_steps_and_offsets():
     assert np.array_equal(b.getTimeSteps(), 0.8 * dts)
     with pytest.raises(ValueError):
         b.setTimeSteps(dts[:2])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("graph_steps", [0, 10])
+def test_instances_stop_after_their_own_steps(precision, graph_steps):
+    """a batch whose instances stop after their own step counts (the serving
+    loop's batches): each instance's u, v and a equal the same mesh run
+    alone for exactly that many steps, bit for bit, while the others go on;
+    limits set again later count from then"""
+    meshes, mats, vels = _instances(seed=13, count=5)
+    b = _batch(meshes, mats, vels, precision)
+    dts = b.getStableTimeSteps()
+    b.setTimeSteps(0.8 * dts)
+    b.setGraphSteps(graph_steps)
+    steps = np.array([7, 33, 0, -1, 24], dtype=np.int64)
+    b.setInstanceSteps(steps)
+    assert np.array_equal(b.getInstanceStepsLeft(), [7, 33, 0, np.iinfo(np.int64).max, 24])
+    b.solveStep(29)
+    left = b.getInstanceStepsLeft()
+    assert np.array_equal(left[[0, 1, 2, 4]], [0, 4, 0, 0])
+    b.solveStep(21)  # 50 steps in all
+    # instance 3 has no limit: 50 steps; a new limit for it from now on
+    b.setInstanceSteps(np.array([-1, -1, -1, 6, -1], dtype=np.int64))
+    b.solveStep(13)
+    expected = {0: 7, 1: 33, 2: 0, 3: 56, 4: 24}
+    for k, mesh in enumerate(meshes):
+        alone = gpu_model(mesh, [mats[k]], precision=precision)
+        alone.setNodal("velocity", vels[k])
+        alone.setNodal("blocked_dofs", blocked_face(mesh.nodes))
+        alone.setTimeStep(0.8 * dts[k])
+        alone.solveStep(expected[k])
+        sl = b.instance_nodes(k)
+        for name in ("displacement", "velocity", "acceleration"):
+            got = getattr(b, _getter(name))()[sl]
+            assert np.array_equal(got, getattr(alone, _getter(name))()), (k, name)
+            assert np.array_equal(b.getInstanceNodal(name, k), got), (k, name)

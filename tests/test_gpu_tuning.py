@@ -351,3 +351,68 @@ def test_affine_kernel_only_for_parallelepipeds():
             m.setAffineKernel(mode)
     assert not gpu_model(akb.box_hex8(3), [UNIT_ELASTIC], precision="fp64").getAffineKernel()
     assert not gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision="mixed").getAffineKernel()
+
+
+PACK = 256  # AKB_POINTS_PACKED
+
+
+@pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
+def test_hex8_packed_pairs_are_the_default_and_bit_identical(mat):
+    """meshes of parallelepipeds evaluate elastic and neohookean points as
+    packed FP32 pairs by default; every packed shape (points per iteration,
+    register cap) and both affine kernel modes give the same numbers"""
+    mesh = akb.box_hex8(5, 4, 6, lengths=(1.0, 0.7, 1.3))
+    v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
+    m = gpu_model(mesh, [mat], precision="mixed")
+    b, q, mb, n = m.getLaunchShape(mat["type"])
+    assert q == PACK | 8 and b == 128
+    runs = []
+    for affine in (2, 1):
+        for pts in (2, 4, 8):
+            for minb in (1, 4, 5):
+                m = gpu_model(mesh, [mat], precision="mixed")
+                m.setAffineKernel(affine)
+                m.setLaunchShape(mat["type"], 128, PACK | pts, 128, minb)
+                m.setNodal("velocity", v0)
+                m.setNodal("blocked_dofs", bl)
+                m.setTimeStep(0.8 * m.getStableTimeStep())
+                m.solveStep(130)
+                runs.append(((affine, pts, minb), m.getDisplacement().copy(),
+                             m.getVelocity().copy(), m.getInternalForce().copy()))
+    for other in runs[1:]:
+        for a, b_ in zip(runs[0][1:], other[1:]):
+            assert np.array_equal(a, b_), (runs[0][0], other[0])
+
+
+@pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
+def test_hex8_packed_pairs_accuracy(mat):
+    """the packed form against the FP64 oracle and the scalar form after 500
+    steps (relative L2 of the displacement)"""
+    mesh = akb.box_hex8(8)
+    v0, bl = random_field_velocity(mesh.nodes, seed=21), blocked_face(mesh.nodes)
+    g, o = setup_pair(mesh, [mat], v0, bl, precision="mixed")
+    assert g.getLaunchShape(mat["type"])[1] & PACK
+    g.solveStep(500)
+    o.step(500)
+    uo = o.get(orc.U)
+    u = g.getDisplacement()
+    assert np.linalg.norm(u - uo) / np.linalg.norm(uo) < 1e-5
+    scalar = _run(mesh, mat, "mixed", v0, bl, 500, shape=(128, 2, 256, 5)).getDisplacement()
+    assert np.linalg.norm(scalar - u) / np.linalg.norm(uo) < 1e-5
+
+
+def test_hex8_packed_shape_rules():
+    mesh = akb.box_hex8(3)
+    m = gpu_model(mesh, [UNIT_NEOHOOKEAN], precision="mixed")
+    with pytest.raises(akb.AkbError):
+        m.setLaunchShape("neohookean", 64, PACK | 8, 128, 1)  # 128 threads only
+    with pytest.raises(akb.AkbError):
+        m.setLaunchShape("neohookean", 128, PACK | 3, 128, 1)
+    m.setAffineKernel(0)  # no packed form for the general kernel: scalar again
+    b, q, mb, n = m.getLaunchShape("neohookean")
+    assert not (q & PACK)
+    with pytest.raises(akb.AkbError):
+        m.setLaunchShape("neohookean", 128, PACK | 8, 128, 4)
+    p = gpu_model(mesh, [UNIT_PLASTIC], precision="mixed")
+    with pytest.raises(akb.AkbError):
+        p.setLaunchShape("plastic_linear_isotropic_hardening", 128, PACK | 2, 128, 5)
