@@ -135,6 +135,8 @@ def lib():
         "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
         "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,
                                               ctypes.POINTER(i64)]),
+        "akb_estimate_batch_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,
+                                                    c_int, ctypes.POINTER(i64)]),
         "akb_server_create": (c_int, [vp, pp]),
         "akb_server_submit": (c_int, [vp, vp, ctypes.POINTER(i64)]),
         "akb_server_poll": (c_int, [vp, vp, c_int, ctypes.POINTER(c_int), c_dbl]),

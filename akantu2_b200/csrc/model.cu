@@ -1928,6 +1928,20 @@ int akb_estimate_device_bytes(int et, int rule, int64_t N, int64_t E, int law, i
   return AKB_OK;
 }
 
+int akb_estimate_batch_device_bytes(int et, int rule, int64_t N, int64_t E, int nb_instances,
+                                    int law, int precision, int64_t *bytes) {
+  AKB_TRY(akb_estimate_device_bytes(et, rule, N, E, law, precision, bytes));
+  if (nb_instances < 1) return fail(AKB_EINVAL, "a batch has at least one instance");
+  auto r = [](int64_t b) { return std::max<int64_t>(b, 16); };
+  const int64_t ni = nb_instances;
+  // instance of each node, user id and instance of each element, material
+  // slot of each element; per-instance time steps, minima, element offsets,
+  // stop steps; the material table and the step counter
+  *bytes += r(4 * N) + 3 * r(4 * E) + 3 * r(8 * ni) + r(8 * (ni + 1)) +
+            r((int64_t)sizeof(MatParams) * ni) + r(8);
+  return AKB_OK;
+}
+
 int akb_model_apply_neumann_stress(akb_model *m, const int32_t *group_nodes, int64_t count,
                                    const double *stress) {
   AKB_TRY(check_model(m, true));

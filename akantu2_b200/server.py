@@ -15,7 +15,10 @@ from .mesh import Mesh, TYPE_IDS
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_active", ctypes.c_int),
                 ("device_bytes", ctypes.c_int64), ("chunk_steps", ctypes.c_int64),
-                ("builders", ctypes.c_int), ("short_work", ctypes.c_double)]
+                ("builders", ctypes.c_int), ("short_work", ctypes.c_double),
+                ("no_batching", ctypes.c_int), ("batch_max_instances", ctypes.c_int),
+                ("batch_max_request_elements", ctypes.c_int64),
+                ("batch_max_elements", ctypes.c_int64)]
 
 
 class Request(ctypes.Structure):
@@ -35,7 +38,7 @@ class Completion(ctypes.Structure):
                 ("t_admit", ctypes.c_double), ("t_start", ctypes.c_double),
                 ("t_end", ctypes.c_double), ("nb_elements", ctypes.c_int64),
                 ("nb_steps", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
-                ("dt", ctypes.c_double)]
+                ("dt", ctypes.c_double), ("batched", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):
@@ -58,16 +61,19 @@ def _params_text(params):
 
 
 class Server:
-    """Continuous-batching solve server on one GPU.
+    """Continuous-batching solve server on one GPU (small solves of the same
+    kind share batch models whose instances stop and report one by one).
 
     ``submit`` returns an id and a dict whose "displacement" (and "velocity")
     arrays are filled when the solve completes; ``poll`` returns the
     completions (id, status, timings in seconds on the server's clock)."""
 
     def __init__(self, device=0, max_active=64, device_bytes=0, chunk_steps=500, builders=4,
-                 short_work=1e8):
+                 short_work=1e8, batching=True, batch_max_instances=256,
+                 batch_max_request_elements=1 << 17, batch_max_elements=1 << 23):
         cfg = ServerConfig(device, max_active, int(device_bytes), int(chunk_steps), builders,
-                           float(short_work))
+                           float(short_work), 0 if batching else 1, int(batch_max_instances),
+                           int(batch_max_request_elements), int(batch_max_elements))
         self._h = ctypes.c_void_p()
         _capi.check(_capi.lib().akb_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self._outputs = {}
@@ -129,6 +135,7 @@ class Server:
                         "t_submit": c.t_submit, "t_admit": c.t_admit, "t_start": c.t_start,
                         "t_end": c.t_end, "nb_elements": c.nb_elements, "nb_steps": c.nb_steps,
                         "device_bytes": c.device_bytes, "dt": c.dt,
+                        "batched": bool(c.batched),
                         "outputs": self._outputs.pop(c.id, None)})
         return res
 

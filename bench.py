@@ -72,6 +72,8 @@ def parse():
     p.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     p.add_argument("--max-active", type=int, default=64, help="serve: resident solves")
     p.add_argument("--builders", type=int, default=8, help="serve: host build threads")
+    p.add_argument("--no-batching", action="store_true",
+                   help="serve: every request gets a model of its own")
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e-fp64", action="store_true",
@@ -928,7 +930,7 @@ def run_serve(args):
     warm.drain()
     warm.close()
     srv = akb.Server(device=local, max_active=args.max_active, chunk_steps=500,
-                     builders=args.builders)
+                     builders=args.builders, batching=not args.no_batching)
     done = []
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
@@ -961,6 +963,7 @@ def run_serve(args):
                                    f"{args.rate}/s, tet4/hex8 boxes of 1e3..1e6 elements, "
                                    "3 laws, 500..5000 steps",
                        "precision": precision, "max_active": args.max_active,
+                       "batching": not args.no_batching,
                        "chunk_steps": 500, "parallelism": f"replicas x{world}"},
             "latency_s": {"p50": float(np.percentile(lat, 50)),
                           "p99": float(np.percentile(lat, 99)),
@@ -971,6 +974,8 @@ def run_serve(args):
                         "p99": float(np.percentile(build, 99))},
             "run_s": {"p50": float(np.percentile(run, 50)), "p99": float(np.percentile(run, 99))},
             "requests_per_s": len(done) / span, "element_steps": work, "wall_s": wall,
+            "batched_requests": int(sum(c.get("batched", False) for c in done)),
+            "batching": not args.no_batching,
             "failed": len(bad), "clocks": clk.summary(),
             "e2e": {"value": world * work / span, "unit": UNIT,
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,

@@ -370,6 +370,12 @@ int akb_model_device_bytes(const akb_model *model, int64_t *bytes);
  * for admission by memory footprint */
 int akb_estimate_device_bytes(int element_type, int quadrature_rule, int64_t nb_nodes,
                               int64_t nb_elements, int law, int precision, int64_t *bytes);
+/* the same for a batch of nb_instances meshes with N nodes and E elements in
+ * all, one material per instance, instances stopping after their own step
+ * counts (akb_batch_set_instance_steps) */
+int akb_estimate_batch_device_bytes(int element_type, int quadrature_rule, int64_t nb_nodes,
+                                    int64_t nb_elements, int nb_instances, int law,
+                                    int precision, int64_t *bytes);
 int akb_model_synchronize(akb_model *model);
 /* SolidMechanicsModel::assembleInternalForces  solid_mechanics_model.cc:333-370 */
 int akb_model_assemble_internal_forces(akb_model *model);
@@ -439,14 +445,20 @@ int akb_batch_get_time_steps(const akb_model *model, double *dt);
 /* ---- serving: many solves resident on one GPU ---------------------------- */
 /* No reference counterpart (the reference runs one model per process).  A
  * server admits submitted solves in arrival order while their estimated
- * device memory (akb_estimate_device_bytes) fits in its budget and fewer
- * than max_active are resident; each admitted solve gets its own model and
- * stream, is prepared by a builder thread (tables, lumped mass, stable time
- * step, step graph) and then advanced chunk by chunk by the scheduler thread
- * together with every other resident solve, so that their kernels overlap on
- * the device.  Arrivals are folded into the running set as soon as memory
- * and a slot are free.  A solve's result does not depend on what else runs
- * (each solve is computed exactly as by a model of its own). */
+ * device memory (akb_estimate_device_bytes, akb_estimate_batch_device_bytes)
+ * fits in its budget and fewer than max_active are resident.  Solves of at
+ * most batch_max_request_elements elements are admitted in batches: the
+ * queue's head with every queued solve of the same element type, quadrature
+ * rule, law and precision (limits above) becomes one batch model whose
+ * instances each stop after their own step count
+ * (akb_batch_set_instance_steps) and are reported as soon as they end, while
+ * the batch goes on; larger solves get a model of their own.  Builder threads
+ * prepare the models (tables, lumped mass, stable time steps, step graphs),
+ * the scheduler thread advances every resident batch and solve chunk by chunk
+ * on its own stream, so that their kernels overlap on the device; arrivals are
+ * admitted as soon as memory and a slot are free.  A solve's result does not
+ * depend on what else runs (each is computed exactly as by a model of its
+ * own). */
 typedef struct akb_server akb_server;
 typedef struct {
   int device;            /* CUDA device                                        */
@@ -457,6 +469,10 @@ typedef struct {
   int builders;          /* host threads preparing and finishing solves (<= 0: 4) */
   double short_work;     /* solves of fewer element-steps (elements x steps) run on
                             high-priority streams (<= 0: 1e8)                   */
+  int no_batching;       /* 1: every solve gets a model of its own             */
+  int batch_max_instances;            /* solves per batch (<= 0: 256)          */
+  int64_t batch_max_request_elements; /* larger solves run alone (<= 0: 2^17)  */
+  int64_t batch_max_elements;         /* elements per batch (<= 0: 2^23)       */
 } akb_server_config;
 
 typedef struct {
@@ -483,6 +499,7 @@ typedef struct {
   double t_submit, t_admit, t_start, t_end; /* seconds on the server's clock   */
   int64_t nb_elements, nb_steps, device_bytes;
   double dt;
+  int batched;                   /* 1: advanced as an instance of a batch      */
 } akb_completion;
 
 typedef struct {

@@ -44,10 +44,14 @@ def _alone(req):
     return m.getDisplacement(), m.getVelocity()
 
 
-def test_results_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("batching", [True, False])
+def test_results_same_alone_and_in_the_mix(batching):
+    """every result equals the same solve run by a model of its own, bit for
+    bit, whether it ran as an instance of a batch (requests of one kind
+    sharing a batch model, each stopping after its own step count) or alone"""
     rng = np.random.default_rng(3)
     reqs = [_request(k, rng) for k in range(14)]
-    srv = akb.Server(max_active=5, chunk_steps=100, builders=3)
+    srv = akb.Server(max_active=5, chunk_steps=100, builders=3, batching=batching)
     ids = {}
     for k, r in enumerate(reqs):
         rid, out = srv.submit(r["mesh"], r["material"], r["steps"], velocity=r["velocity"],
@@ -58,6 +62,7 @@ def test_results_same_alone_and_in_the_mix():
     done = srv.drain(timeout=300)
     srv.close()
     assert sorted(c["id"] for c in done) == sorted(ids)
+    assert any(c["batched"] for c in done) == batching
     for c in done:
         assert c["status"] == 0, c["message"]
         assert c["t_submit"] <= c["t_admit"] <= c["t_start"] <= c["t_end"]
@@ -137,3 +142,53 @@ def test_submit_rejects_unknown_material():
         srv.submit(akb.box_tet4(2), dict(type="no_such_law", E=1.0), 10)
     assert e.value.name == "AKB_EMATERIAL"
     srv.close()
+
+
+def test_batched_admission_of_many_small_solves():
+    """40 small solves of a few kinds arriving together: they share batch
+    models (up to the instance limit), each result bit-identical to the solve
+    alone, reported as soon as its own steps are done"""
+    rng = np.random.default_rng(11)
+    reqs = []
+    for k in range(40):
+        r = _request(3 * (k % 2), rng)  # tetrahedra (k even) and hexahedra
+        r["precision"] = ("fp64", "mixed")[(k // 2) % 2]
+        reqs.append(r)
+    srv = akb.Server(max_active=40, chunk_steps=500, builders=2, batch_max_instances=12)
+    ids = {}
+    for k, r in enumerate(reqs):
+        rid, out = srv.submit(r["mesh"], r["material"], r["steps"], velocity=r["velocity"],
+                              blocked=r["blocked"], precision=r["precision"], want_velocity=True)
+        ids[rid] = (k, out)
+    done = srv.drain(timeout=300)
+    srv.close()
+    assert sum(c["batched"] for c in done) >= 30
+    for c in done:
+        assert c["status"] == 0, c["message"]
+        k, out = ids[c["id"]]
+        u, v = _alone(reqs[k])
+        assert np.array_equal(out["displacement"], u), f"request {k}"
+        assert np.array_equal(out["velocity"], v), f"request {k}"
+
+
+def test_batch_estimate_bounds_the_allocation():
+    import ctypes
+    from akantu2_b200 import _capi
+    for meshes, mat, prec in [([akb.box_tet4(n) for n in (2, 3, 4)], UNIT_ELASTIC, "fp64"),
+                              ([akb.box_hex8(n) for n in (2, 4)], UNIT_NEOHOOKEAN, "mixed"),
+                              ([akb.square_tri6(n) for n in (3, 5)], UNIT_PLASTIC, "mixed")]:
+        b = akb.BatchModel(meshes)
+        for k in range(len(meshes)):
+            b.addMaterial(mat["type"], **{kk: v for kk, v in mat.items() if kk != "type"})
+        b.setInstanceMaterials(np.arange(len(meshes)))
+        b.initFull(akb._explicit_lumped_mass, precision=prec)
+        b.setInstanceSteps(np.full(len(meshes), 10, dtype=np.int64))
+        used = b.getDeviceBytes()
+        est = ctypes.c_int64()
+        law = {"elastic": 0, "neohookean": 1, "plastic_linear_isotropic_hardening": 2}[mat["type"]]
+        _capi.check(_capi.lib().akb_estimate_batch_device_bytes(
+            _capi.TETRAHEDRON_4 if meshes[0].element_type == "_tetrahedron_4" else
+            (_capi.HEXAHEDRON_8 if meshes[0].element_type == "_hexahedron_8" else
+             _capi.TRIANGLE_6), 0, b.mesh.getNbNodes(), b.mesh.getNbElement(), len(meshes),
+            law, 0 if prec == "fp64" else 1, ctypes.byref(est)))
+        assert used <= est.value <= used + 8192, (meshes[0].element_type, prec, used, est.value)
