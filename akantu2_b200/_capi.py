@@ -135,6 +135,12 @@ def lib():
         "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
         "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,
                                               ctypes.POINTER(i64)]),
+        "akb_exchange_create": (c_int, [vp, c_int, pp]),
+        "akb_exchange_add_link": (c_int, [vp, c_int, c_int, vp, vp, i64]),
+        "akb_exchange_set_graph_steps": (c_int, [vp, i64]),
+        "akb_exchange_solve_step": (c_int, [vp, i64]),
+        "akb_exchange_synchronize": (c_int, [vp]),
+        "akb_exchange_destroy": (c_int, [vp]),
         "akb_estimate_batch_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,
                                                     c_int, ctypes.POINTER(i64)]),
         "akb_server_create": (c_int, [vp, pp]),

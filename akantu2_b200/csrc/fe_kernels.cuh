@@ -1516,7 +1516,8 @@ __global__ void k_node_update_retire(int64_t N, const int32_t *__restrict__ ptr,
   pdl_begin();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  if (*step >= inst_end[node_inst[i]]) {
+  // a batch of one instance has no node -> instance table
+  if (*step >= inst_end[node_inst ? node_inst[i] : 0]) {
     if (flags & NU_PREDICT) {
 #pragma unroll
       for (int c = 0; c < D; ++c) u[i * D + c] = u_next[i * D + c];

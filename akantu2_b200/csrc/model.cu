@@ -2608,3 +2608,355 @@ int akb_model_get_status(akb_model *m, int *flags) {
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------------ */
+/* Halo exchange between the subdomain models of one process                */
+/* ------------------------------------------------------------------------ */
+// Replaces the reference's per-step ElementSynchronizer exchange
+// (solid_mechanics_model.cc:333-370, _smm_stress) for subdomains that one
+// process drives, on one or several GPUs.  Every step, for each directed
+// link (owner -> holder): the owner's stream gathers the prediction of the
+// listed nodes into the link buffer (and copies it to the holder's GPU when
+// the two differ), records an event; the holder's stream waits for it and
+// scatters the values into its own prediction; then every model runs its
+// step on its own stream.  The subdomains' kernels overlap on the device: a
+// model waits only for its own neighbors' packs.  A link's buffer is reused
+// the next step only after the holder has read it (a second event).  With all
+// models on one GPU, runs of graph_steps steps are captured as one CUDA graph
+// (fork from a stream of the exchange into the models' streams, join back),
+// so a step costs no host work at all.
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    else prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct akb_exchange {
+  std::vector<akb_model *> parts;  // not owned
+  struct Link {
+    int from = 0, to = 0;
+    int64_t n = 0;
+    int32_t *send_idx = nullptr, *recv_idx = nullptr;  // on the owner's / holder's GPU
+    double *send_buf = nullptr, *recv_buf = nullptr;   // the same buffer on one GPU
+    cudaEvent_t packed = nullptr, consumed = nullptr;
+    bool consumed_pending = false;  // `consumed` recorded since the last pack
+  };
+  std::vector<Link> links;
+  std::vector<void *> dev_allocs;  // (device, pointer) freed at destruction
+  std::vector<int> dev_of_alloc;
+  int device = 0;
+  bool one_device = true;
+  cudaStream_t main = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> joins;
+  int64_t graph_steps = 100;
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> ucur, cur;
+    std::vector<double> dt;
+    std::vector<char> fext_zero;
+    int64_t steps = 0;
+  };
+  std::vector<Graph> graphs;
+  ~akb_exchange() {
+    if (main) cudaStreamSynchronize(main);
+    for (auto *m : parts)
+      if (m && m->stream) cudaStreamSynchronize(m->stream);
+    for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+    for (auto &l : links) {
+      if (l.packed) cudaEventDestroy(l.packed);
+      if (l.consumed) cudaEventDestroy(l.consumed);
+    }
+    for (size_t k = 0; k < dev_allocs.size(); ++k) {
+      DeviceGuard g(dev_of_alloc[k]);
+      cudaFree(dev_allocs[k]);
+    }
+    for (auto e : joins) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (done) cudaEventDestroy(done);
+    if (main) cudaStreamDestroy(main);
+  }
+  template <class P> int alloc(int dev, P **p, size_t bytes) {
+    DeviceGuard g(dev);
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? AKB_ENOMEM : AKB_ECUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    dev_allocs.push_back(q);
+    dev_of_alloc.push_back(dev);
+    *p = (P *)q;
+    return AKB_OK;
+  }
+};
+
+namespace {
+
+bool any_plastic_of(const akb_model *m) {
+  for (auto &mt : m->mats)
+    if (mt.law == LAW_PLASTIC) return true;
+  return false;
+}
+
+// one step of every model with its halo exchange, enqueued on the models'
+// streams (inside or outside a capture)
+int exchange_step(akb_exchange *x) {
+  for (auto *m : x->parts) {
+    DeviceGuard g(m->device);
+    if (!m->predicted) AKB_TRY(predict(m));
+  }
+  for (auto &l : x->links) {
+    akb_model *a = x->parts[l.from], *b = x->parts[l.to];
+    DeviceGuard g(a->device);
+    if (l.consumed_pending) AKB_CUDA(cudaStreamWaitEvent(a->stream, l.consumed, 0));
+    AKB_CUDA(launch_halo(false, a->dim, l.n, l.send_idx, a->u_pred(), l.send_buf, a->stream));
+    if (l.recv_buf != l.send_buf)
+      AKB_CUDA(cudaMemcpyPeerAsync(l.recv_buf, b->device, l.send_buf, a->device,
+                                   sizeof(double) * l.n * a->dim, a->stream));
+    AKB_CUDA(cudaEventRecord(l.packed, a->stream));
+  }
+  for (auto &l : x->links) {
+    akb_model *b = x->parts[l.to];
+    DeviceGuard g(b->device);
+    AKB_CUDA(cudaStreamWaitEvent(b->stream, l.packed, 0));
+    AKB_CUDA(launch_halo(true, b->dim, l.n, l.recv_idx, b->u_pred(), l.recv_buf, b->stream));
+    AKB_CUDA(cudaEventRecord(l.consumed, b->stream));
+    l.consumed_pending = true;
+  }
+  for (auto *m : x->parts) {
+    DeviceGuard g(m->device);
+    AKB_TRY(one_step(m, any_plastic_of(m)));
+  }
+  return AKB_OK;
+}
+
+// graph_steps steps of every model as one graph (one GPU), captured when
+// the models' parities, time steps and external-force flags are new
+int exchange_graph(akb_exchange *x) {
+  const size_t P = x->parts.size();
+  akb_exchange::Graph *g = nullptr;
+  for (auto &c : x->graphs) {
+    bool same = c.steps == x->graph_steps;
+    for (size_t k = 0; same && k < P; ++k) {
+      const akb_model *m = x->parts[k];
+      same = c.ucur[k] == m->ucur && c.cur[k] == m->cur && c.dt[k] == m->dt &&
+             c.fext_zero[k] == (char)m->fext_zero;
+    }
+    if (same) g = &c;
+  }
+  DeviceGuard dg(x->device);
+  if (!g) {
+    akb_exchange::Graph ng;
+    for (auto *m : x->parts) {
+      ng.ucur.push_back(m->ucur);
+      ng.cur.push_back(m->cur);
+      ng.dt.push_back(m->dt);
+      ng.fext_zero.push_back((char)m->fext_zero);
+    }
+    ng.steps = x->graph_steps;
+    std::vector<int64_t> steps0(P);
+    for (size_t k = 0; k < P; ++k) steps0[k] = x->parts[k]->steps_done;
+    std::vector<bool> pending0;
+    for (auto &l : x->links) {
+      pending0.push_back(l.consumed_pending);
+      l.consumed_pending = false;  // the fork orders the graph after earlier work
+    }
+    AKB_CUDA(cudaStreamBeginCapture(x->main, cudaStreamCaptureModeThreadLocal));
+    int rc = AKB_OK;
+    if (cudaEventRecord(x->fork, x->main) != cudaSuccess) rc = fail(AKB_ECUDA, "capture fork");
+    for (auto *m : x->parts)
+      if (rc == AKB_OK && cudaStreamWaitEvent(m->stream, x->fork, 0) != cudaSuccess)
+        rc = fail(AKB_ECUDA, "capture fork");
+    for (int64_t s = 0; s < x->graph_steps && rc == AKB_OK; ++s) rc = exchange_step(x);
+    for (size_t k = 0; k < P && rc == AKB_OK; ++k)
+      if (cudaEventRecord(x->joins[k], x->parts[k]->stream) != cudaSuccess ||
+          cudaStreamWaitEvent(x->main, x->joins[k], 0) != cudaSuccess)
+        rc = fail(AKB_ECUDA, "capture join");
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(x->main, &graph);
+    // capturing executes nothing: the models' step state goes back
+    for (size_t k = 0; k < P; ++k) {
+      akb_model *m = x->parts[k];
+      m->ucur = ng.ucur[k];
+      m->cur = ng.cur[k];
+      m->steps_done = steps0[k];
+    }
+    for (size_t k = 0; k < x->links.size(); ++k) x->links[k].consumed_pending = pending0[k];
+    if (rc != AKB_OK || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc != AKB_OK) return rc;
+      return fail(AKB_ECUDA, std::string("exchange capture: ") + cudaGetErrorString(e));
+    }
+    e = cudaGraphInstantiate(&ng.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e == cudaSuccess) e = cudaGraphUpload(ng.exec, x->main);
+    if (e != cudaSuccess)
+      return fail(AKB_ECUDA, std::string("exchange graph: ") + cudaGetErrorString(e));
+    if (x->graphs.size() >= 8) {
+      cudaGraphExecDestroy(x->graphs.front().exec);
+      x->graphs.erase(x->graphs.begin());
+    }
+    x->graphs.push_back(std::move(ng));
+    g = &x->graphs.back();
+  }
+  // the graph after everything enqueued on the models' streams, and their
+  // later work after the graph
+  for (size_t k = 0; k < P; ++k) {
+    AKB_CUDA(cudaEventRecord(x->joins[k], x->parts[k]->stream));
+    AKB_CUDA(cudaStreamWaitEvent(x->main, x->joins[k], 0));
+  }
+  AKB_CUDA(cudaGraphLaunch(g->exec, x->main));
+  AKB_CUDA(cudaEventRecord(x->done, x->main));
+  for (auto *m : x->parts) {
+    AKB_CUDA(cudaStreamWaitEvent(m->stream, x->done, 0));
+    m->steps_done += g->steps;
+    m->fint_valid = false;
+  }
+  // the graph's last unpacks precede its end, which the models' streams wait for
+  for (auto &l : x->links) l.consumed_pending = false;
+  return AKB_OK;
+}
+
+bool exchange_steady(const akb_exchange *x) {
+  for (auto *m : x->parts)
+    if (!thermal_steady(m) || !m->predicted) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int akb_exchange_create(akb_model *const *parts, int nparts, akb_exchange **out) {
+  if (!out || !parts || nparts < 1) return fail(AKB_EINVAL, "bad arguments");
+  *out = nullptr;
+  for (int k = 0; k < nparts; ++k) {
+    AKB_TRY(check_model(parts[k], true));
+    if (parts[k]->is_batch) return fail(AKB_EINVAL, "a batch cannot be a subdomain");
+    if (parts[k]->dim != parts[0]->dim) return fail(AKB_EINVAL, "subdomains of different dimensions");
+  }
+  auto *x = new akb_exchange();
+  x->parts.assign(parts, parts + nparts);
+  x->device = parts[0]->device;
+  for (auto *m : x->parts) x->one_device = x->one_device && m->device == x->device;
+  int rc = AKB_OK;
+  {
+    DeviceGuard g(x->device);
+    if (cudaStreamCreateWithFlags(&x->main, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&x->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&x->done, cudaEventDisableTiming) != cudaSuccess)
+      rc = fail(AKB_ECUDA, "exchange stream / events");
+    x->joins.assign(nparts, nullptr);
+    for (auto &e : x->joins)
+      if (rc == AKB_OK && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(AKB_ECUDA, "exchange events");
+  }
+  if (rc != AKB_OK) {
+    delete x;
+    return rc;
+  }
+  *out = x;
+  return AKB_OK;
+}
+
+int akb_exchange_add_link(akb_exchange *x, int from, int to, const int32_t *send_local,
+                          const int32_t *recv_local, int64_t count) {
+  if (!x) return fail(AKB_EINVAL, "null exchange");
+  const int P = (int)x->parts.size();
+  if (from < 0 || from >= P || to < 0 || to >= P || from == to)
+    return fail(AKB_EINVAL, "link ends out of range");
+  if (count < 0 || (count > 0 && (!send_local || !recv_local)))
+    return fail(AKB_EINVAL, "bad node lists");
+  akb_model *a = x->parts[from], *b = x->parts[to];
+  for (int64_t i = 0; i < count; ++i)
+    if (send_local[i] < 0 || send_local[i] >= a->N || recv_local[i] < 0 || recv_local[i] >= b->N)
+      return fail(AKB_EINVAL, "node list refers to a missing node");
+  akb_exchange::Link l;
+  l.from = from;
+  l.to = to;
+  l.n = count;
+  const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(count * a->dim, 1);
+  AKB_TRY(x->alloc(a->device, &l.send_idx, sizeof(int32_t) * std::max<int64_t>(count, 1)));
+  AKB_TRY(x->alloc(b->device, &l.recv_idx, sizeof(int32_t) * std::max<int64_t>(count, 1)));
+  AKB_TRY(x->alloc(a->device, &l.send_buf, bytes));
+  if (a->device == b->device) {
+    l.recv_buf = l.send_buf;
+  } else {
+    AKB_TRY(x->alloc(b->device, &l.recv_buf, bytes));
+  }
+  {
+    DeviceGuard g(a->device);
+    if (count > 0)
+      AKB_CUDA(cudaMemcpy(l.send_idx, send_local, sizeof(int32_t) * count, cudaMemcpyHostToDevice));
+    AKB_CUDA(cudaEventCreateWithFlags(&l.packed, cudaEventDisableTiming));
+  }
+  {
+    DeviceGuard g(b->device);
+    if (count > 0)
+      AKB_CUDA(cudaMemcpy(l.recv_idx, recv_local, sizeof(int32_t) * count, cudaMemcpyHostToDevice));
+    AKB_CUDA(cudaEventCreateWithFlags(&l.consumed, cudaEventDisableTiming));
+  }
+  x->links.push_back(l);
+  for (auto &g : x->graphs) cudaGraphExecDestroy(g.exec);
+  x->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_exchange_set_graph_steps(akb_exchange *x, int64_t steps) {
+  if (!x) return fail(AKB_EINVAL, "null exchange");
+  if (steps < 0 || (steps & 1)) return fail(AKB_EINVAL, "graph steps must be even and >= 0");
+  x->graph_steps = steps;
+  return AKB_OK;
+}
+
+int akb_exchange_solve_step(akb_exchange *x, int64_t nsteps) {
+  if (!x) return fail(AKB_EINVAL, "null exchange");
+  if (nsteps < 0) return fail(AKB_EINVAL, "negative step count");
+  int64_t left = nsteps;
+  const int64_t G = x->graph_steps;
+  // steps whose models must first predict, or whose plastic trial stress
+  // has a thermal term, run eagerly; then whole graphs on one GPU
+  while (left > 0 && (!x->one_device || G == 0 || left < G || !exchange_steady(x))) {
+    AKB_TRY(exchange_step(x));
+    --left;
+    if (x->one_device && G > 0 && left >= G && exchange_steady(x)) break;
+  }
+  while (G > 0 && left >= G && x->one_device) {
+    AKB_TRY(exchange_graph(x));
+    left -= G;
+  }
+  for (; left > 0; --left) AKB_TRY(exchange_step(x));
+  if (nsteps > 0)
+    for (auto *m : x->parts) {
+      m->forces_evaluated = true;
+      m->snap_valid = false;
+    }
+  return AKB_OK;
+}
+
+int akb_exchange_synchronize(akb_exchange *x) {
+  if (!x) return fail(AKB_EINVAL, "null exchange");
+  for (auto *m : x->parts) {
+    DeviceGuard g(m->device);
+    AKB_CUDA(cudaStreamSynchronize(m->stream));
+  }
+  DeviceGuard g(x->device);
+  AKB_CUDA(cudaStreamSynchronize(x->main));
+  return AKB_OK;
+}
+
+int akb_exchange_destroy(akb_exchange *x) {
+  delete x;
+  return AKB_OK;
+}
+
+}  // extern "C"

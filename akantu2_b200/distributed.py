@@ -20,8 +20,10 @@ Each owned node sums the same elemental forces in the same order as the whole
 mesh on one GPU, so a partitioned run is bit-identical to the serial one
 (FP64 and mixed alike).
 
-PartitionedModel advances all subdomains on the current GPU (the exchange is a
-device gather/scatter between the subdomain models).  DistributedModel is one
+PartitionedModel advances all subdomains on the current GPU through the
+library's exchange (akb_exchange: per-step gather / scatter between the
+subdomain models on their own streams, ordered by events, replayed as CUDA
+graphs of 100 steps).  DistributedModel is one
 subdomain per torch.distributed rank: with NCCL the halo buffers stay on the
 device and the send/receive run on the model's stream; with gloo they are
 staged through host memory.
@@ -198,47 +200,68 @@ class PartitionedModel(_PartitionBase):
         self._setup(mesh, [Subdomain(mesh, self.part, nparts, r) for r in range(nparts)])
 
     def initFull(self, _analysis_method=_explicit_lumped_mass, precision="fp64"):
-        import torch
         self._init_locals(_analysis_method, precision)
-        dev = torch.device("cuda", torch.cuda.current_device())
-        # buffer of each directed pair (owner r -> holder s), shared by r's
-        # pack and s's unpack
-        self._bufs = {}
-        self._idx = []
+        # the per-step exchange in the library (akb_exchange): one link per
+        # directed pair (owner r -> holder s), the send list of r and the
+        # receive list of s naming the same global nodes in the same order
+        L = _capi.lib()
+        handles = (ctypes.c_void_p * len(self.locals))(*[lc.model._h.value for lc in self.locals])
+        self._x = ctypes.c_void_p()
+        _capi.check(L.akb_exchange_create(handles, len(self.locals), ctypes.byref(self._x)))
+        recv_of = {}
+        for lc in self.locals:
+            for r, send, recv in lc.sub.neighbors:
+                recv_of[(r, lc.sub.rank)] = recv
         for lc in self.locals:
             r = lc.sub.rank
-            lists = []
-            for s, send, recv in lc.sub.neighbors:
-                if (r, s) not in self._bufs:
-                    self._bufs[(r, s)] = torch.empty(max(len(send), 1) * self.dim,
-                                                     dtype=torch.float64, device=dev)
-                lists.append((s, torch.from_numpy(send).to(dev), len(send),
-                              torch.from_numpy(recv).to(dev), len(recv)))
-            self._idx.append(lists)
-        torch.cuda.synchronize()
+            for s, send, _ in lc.sub.neighbors:
+                recv = np.ascontiguousarray(recv_of[(r, s)], dtype=np.int32)
+                send = np.ascontiguousarray(send, dtype=np.int32)
+                assert len(send) == len(recv)
+                _capi.check(L.akb_exchange_add_link(self._x, r, s, _capi.ptr(send),
+                                                    _capi.ptr(recv), len(send)))
+
+    def setGraphSteps(self, steps):
+        _capi.check(_capi.lib().akb_exchange_set_graph_steps(self._x, int(steps)))
 
     def getStableTimeStep(self):
         return min(lc.model.getStableTimeStep() for lc in self.locals)
 
-    def _exchange(self):
-        for lc, lists in zip(self.locals, self._idx):
-            r = lc.sub.rank
-            for s, send, ns, _, _ in lists:
-                lc.pack(send.data_ptr(), self._bufs[(r, s)].data_ptr(), ns)
-        for lc in self.locals:
-            lc.model.synchronize()
-        for lc, lists in zip(self.locals, self._idx):
-            s = lc.sub.rank
-            for r, _, _, recv, nr in lists:
-                lc.unpack(recv.data_ptr(), self._bufs[(r, s)].data_ptr(), nr)
-        for lc in self.locals:
-            lc.model.synchronize()
-
     def solveStep(self, nsteps=1):
-        for _ in range(int(nsteps)):
-            self._exchange()
-            for lc in self.locals:
-                lc.model.solveStep(1)
+        for lc in self.locals:
+            lc.model._sync_up()
+        _capi.check(_capi.lib().akb_exchange_solve_step(self._x, int(nsteps)))
+        for lc in self.locals:
+            lc.model._invalidate()
+
+    def timeSteps(self, nsteps):
+        """nsteps steps of all subdomains timed on the device (ms), between
+        events on the first subdomain's stream after a full synchronisation"""
+        import torch
+        L = _capi.lib()
+        _capi.check(L.akb_exchange_synchronize(self._x))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sp = ctypes.c_void_p()
+        _capi.check(L.akb_model_stream(self.locals[0].model._h, ctypes.byref(sp)))
+        st = torch.cuda.ExternalStream(sp.value)
+        e0.record(st)
+        # every subdomain's stream starts after e0 through the exchange's fork
+        self.solveStep(nsteps)
+        for lc in self.locals[1:]:
+            sp2 = ctypes.c_void_p()
+            _capi.check(L.akb_model_stream(lc.model._h, ctypes.byref(sp2)))
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.ExternalStream(sp2.value))
+            st.wait_event(ev)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def __del__(self):
+        x = getattr(self, "_x", None)
+        if x:
+            _capi.lib().akb_exchange_destroy(x)
+            self._x = None
 
     def getNodal(self, name):
         ids, vals = self._owned(name)

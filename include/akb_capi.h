@@ -279,6 +279,30 @@ void akb_subdomain_destroy(akb_subdomain *sd);
 int akb_model_halo_pack(akb_model *model, const int32_t *local_nodes, int64_t count, double *buf);
 int akb_model_halo_unpack(akb_model *model, const int32_t *local_nodes, int64_t count,
                           const double *buf);
+/* The per-step halo exchange of subdomain models driven by one process
+ * (replaces the reference's ElementSynchronizer _smm_stress exchange,
+ * solid_mechanics_model.cc:333-370): the models, initialised with their
+ * ghost nodes blocked, are advanced together; every step each link gathers
+ * the owner's prediction of its send list (akb_subdomain_lists) and scatters
+ * it into the holder's prediction of its receive list, on the models' streams
+ * ordered by events (peer copies between GPUs), the subdomains' kernels
+ * overlapping on the device.  With all models on one GPU, runs of
+ * graph_steps (even, default 100) steps are captured as one CUDA graph.  The
+ * models are not owned and must outlive the exchange; while it is in use,
+ * step them only through it.  Bit-identical to the whole mesh on one model. */
+typedef struct akb_exchange akb_exchange;
+int akb_exchange_create(akb_model *const *models, int nb_models, akb_exchange **out);
+/* owner `from` sends the prediction of its local nodes send_local[count] to
+ * model `to`, which writes it to its local nodes recv_local[count] (host
+ * arrays, copied) */
+int akb_exchange_add_link(akb_exchange *exchange, int from, int to, const int32_t *send_local,
+                          const int32_t *recv_local, int64_t count);
+int akb_exchange_set_graph_steps(akb_exchange *exchange, int64_t steps);
+/* enqueues nsteps steps of every model (asynchronous) */
+int akb_exchange_solve_step(akb_exchange *exchange, int64_t nsteps);
+int akb_exchange_synchronize(akb_exchange *exchange);
+int akb_exchange_destroy(akb_exchange *exchange);
+
 /* ModelSolver::solveStep  model_solver.cc:267-280: enqueues nsteps explicit
  * steps on the model's stream (asynchronous; getters synchronise) */
 int akb_model_solve_step(akb_model *model, int64_t nsteps);

@@ -172,3 +172,22 @@ def test_instances_stop_after_their_own_steps(precision, graph_steps):
             got = getattr(b, _getter(name))()[sl]
             assert np.array_equal(got, getattr(alone, _getter(name))()), (k, name)
             assert np.array_equal(b.getInstanceNodal(name, k), got), (k, name)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_single_instance_batch_stops_after_its_steps(precision):
+    """a batch of one instance (no node -> instance table) with a step limit,
+    as the serving loop builds when one request arrives alone"""
+    meshes, mats, vels = _instances(seed=21, count=1)
+    b = _batch(meshes, mats, vels, precision)
+    dt = b.getStableTimeSteps()
+    b.setTimeSteps(0.8 * dt)
+    b.setInstanceSteps(np.array([37], dtype=np.int64))
+    b.solveStep(150)
+    alone = gpu_model(meshes[0], [mats[0]], precision=precision)
+    alone.setNodal("velocity", vels[0])
+    alone.setNodal("blocked_dofs", blocked_face(meshes[0].nodes))
+    alone.setTimeStep(0.8 * dt[0])
+    alone.solveStep(37)
+    for name in ("displacement", "velocity", "acceleration"):
+        assert np.array_equal(getattr(b, _getter(name))(), getattr(alone, _getter(name))()), name
