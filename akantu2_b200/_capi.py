@@ -18,7 +18,7 @@ ERRORS = {
 
 TETRAHEDRON_4, HEXAHEDRON_8, TRIANGLE_6 = 0, 1, 2
 EXPLICIT_LUMPED_MASS = 0
-PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FAST = 0, 1, 2
 (DISPLACEMENT, VELOCITY, ACCELERATION, EXTERNAL_FORCE, INTERNAL_FORCE, MASS,
  BLOCKED_DOFS, CURRENT_POSITION, PREVIOUS_DISPLACEMENT, DISPLACEMENT_INCREMENT) = range(10)
 (GRAD_U, STRESS, PIOLA_KIRCHHOFF_2, INELASTIC_STRAIN, ISO_HARDENING,

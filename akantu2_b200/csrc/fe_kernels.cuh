@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(BLOCK)
 // dN/dx form of k_element_forces_geo in exact arithmetic, with about 40% fewer
 // floating-point operations per point.  The factors 1/8 cancel between the
 // Jacobian and its inverse and are folded into det J.
-__device__ __forceinline__ void wht8(float (*v)[3]) {
+template <class T> __device__ __forceinline__ void wht8(T (*v)[3]) {
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -732,13 +732,13 @@ __device__ __forceinline__ void wht8(float (*v)[3]) {
         const int h = l | (1 << d);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const float a = v[l][c], b = v[h][c];
+          const T a = v[l][c], b = v[h][c];
           v[l][c] = a + b;
           v[h][c] = b - a;
         }
       }
 }
-__device__ __forceinline__ void iwht8(float (*v)[3]) {
+template <class T> __device__ __forceinline__ void iwht8(T (*v)[3]) {
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -747,45 +747,48 @@ __device__ __forceinline__ void iwht8(float (*v)[3]) {
         const int h = l | (1 << d);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const float a = v[l][c], b = v[h][c];
+          const T a = v[l][c], b = v[h][c];
           v[l][c] = a - b;
           v[h][c] = a + b;
         }
       }
 }
 
-// weighted flux P of one point for the mixed path: r_a = P . dN_a/dx
-template <int D, int LAW>
-__device__ __forceinline__ void mixed_flux(const float *g, float w, const MatParams &mp,
+// weighted flux P of one point for the sum-factorised kernels: r_a = P . dN_a/dx
+// (FP32 element math on the mixed path, FP64 on the fast FP64 path: the
+// same formulas, first Piola-Kirchhoff stress in the displacement gradient)
+template <int D, int LAW, class T = float>
+__device__ __forceinline__ void mixed_flux(const T *g, T w, const MatParams &mp,
                                            const GroupArgs &ps, int64_t ne, int64_t le, int q,
-                                           float *P) {
+                                           T *P) {
   if constexpr (LAW == LAW_NEOHOOKEAN) {
     if (mp.svk) {
-      float S[D * D];
-      finite_pk2<D, float>(mp, g, S);
-      first_piola<D, float>(g, S, w, P);
+      T S[D * D];
+      finite_pk2<D, T>(mp, g, S);
+      first_piola<D, T>(g, S, w, P);
     } else {
-      neohookean_piola<D, float>((float)mp.lambda, (float)mp.mu, g, w, P);
+      neohookean_piola<D, T>((T)mp.lambda, (T)mp.mu, g, w, P);
     }
   } else if constexpr (LAW == LAW_ELASTIC) {
-    float sig[D * D];
-    elastic_stress<D, float>((float)mp.lambda, (float)mp.mu, g, (float)mp.sigma_th, sig);
+    T sig[D * D];
+    elastic_stress<D, T>((T)mp.lambda, (T)mp.mu, g, (T)mp.sigma_th, sig);
 #pragma unroll
     for (int k = 0; k < D * D; ++k) P[k] = sig[k] * w;
   } else {
     double gd[D * D], sd[D * D];
 #pragma unroll
     for (int k = 0; k < D * D; ++k) gd[k] = (double)g[k];
-    plastic_point<D, float>(mp, ps, ne, le, q, gd, sd);
+    plastic_point<D, T>(mp, ps, ne, le, q, gd, sd);
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) P[k] = (float)sd[k] * w;
+    for (int k = 0; k < D * D; ++k) P[k] = (T)sd[k] * w;
   }
 }
 
 // relative FP32 coordinates of a hexahedron's nodes in the modal
 // (Walsh-Hadamard) basis, lexicographic corner order
+template <class T>
 __device__ __forceinline__ void hex8_geometry_modes(int64_t e, int64_t E, const int32_t *conn,
-                                                    const double *X, float (*wx)[3]) {
+                                                    const double *X, T (*wx)[3]) {
   constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
   double x0[3];
 #pragma unroll
@@ -795,7 +798,7 @@ __device__ __forceinline__ void hex8_geometry_modes(int64_t e, int64_t E, const 
     for (int i = 0; i < 3; ++i) {
       const double x = X[node * 3 + i];
       if (a == 0) x0[i] = x;
-      wx[lex[a]][i] = (float)(x - x0[i]);
+      wx[lex[a]][i] = (T)(x - x0[i]);
     }
   }
   wht8(wx);
@@ -803,15 +806,16 @@ __device__ __forceinline__ void hex8_geometry_modes(int64_t e, int64_t E, const 
 
 // the Jacobian adjugate and 1/det of a parallelepiped from its geometry
 // modes (wx after wht8: modes 1, 2 and 4 are 8 dX/dxi, 8 dX/deta, 8 dX/dzeta)
-__device__ __forceinline__ float hex8_affine_adjugate(const float (*wx)[3], float *Ja) {
-  float Jp[9];
+template <class T>
+__device__ __forceinline__ T hex8_affine_adjugate(const T (*wx)[3], T *Ja) {
+  T Jp[9];
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     Jp[0 + 3 * j] = wx[1][j];
     Jp[1 + 3 * j] = wx[2][j];
     Jp[2 + 3 * j] = wx[4][j];
   }
-  return 1.f / adj3(Jp, Ja);
+  return T(1) / adj3(Jp, Ja);
 }
 
 // QU: quadrature points per unrolled iteration (1, 2, 4 or 8).  AFF: every
@@ -821,19 +825,19 @@ __device__ __forceinline__ float hex8_affine_adjugate(const float (*wx)[3], floa
 // 1/det of each element are read from geo [10][E], formed once by
 // k_hex8_affine_geometry with the same arithmetic, instead of gathering the
 // element's coordinates every step
-template <int LAW, int QU, bool AFF = false, bool GEO = false>
+template <int LAW, int QU, bool AFF = false, bool GEO = false, class T = float>
 __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int64_t e_count,
                                                int64_t E, const int32_t *conn,
                                                const int32_t *pos,
-                                               const double *X, const float *geo,
+                                               const double *X, const T *geo,
                                                const double *u, const MatParams &mp,
-                                               const GroupArgs &ps, float *re) {
+                                               const GroupArgs &ps, T *re) {
   static_assert(AFF || !GEO, "the geometry table holds parallelepipeds only");
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
   // reference node a sits at lexicographic corner lex[a] = [sx>0] + 2[sy>0] + 4[sz>0]
   constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
-  float wx[8][3], wu[8][3];
+  T wx[8][3], wu[8][3];
   double x0[3], u0[3];
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
@@ -842,15 +846,15 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
     for (int i = 0; i < 3; ++i) {
       const double uu = u[node * 3 + i];
       if (a == 0) u0[i] = uu;
-      wu[lex[a]][i] = (float)(uu - u0[i]);
+      wu[lex[a]][i] = (T)(uu - u0[i]);
       if constexpr (!GEO) {
         const double x = X[node * 3 + i];
         if (a == 0) x0[i] = x;
-        wx[lex[a]][i] = (float)(x - x0[i]);
+        wx[lex[a]][i] = (T)(x - x0[i]);
       }
     }
   }
-  float Ja[9], rdet_a = 0.f;
+  T Ja[9], rdet_a = T(0);
   if constexpr (GEO) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) Ja[k] = geo[(int64_t)k * E + e];
@@ -859,8 +863,10 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
     wht8(wx);
   }
   wht8(wu);
-  constexpr float g1 = 0.577350269189625764509f;  // Gauss coordinate 1/sqrt(3)
-  constexpr float g2 = 1.f / 3.f;
+  // Gauss coordinate 1/sqrt(3), rounded once to T
+  constexpr T g1 = std::is_same<T, float>::value ? T(0.577350269189625764509f)
+                                                 : T(0.577350269189625764509);
+  constexpr T g2 = T(1) / T(3);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if constexpr (!GEO) {
@@ -868,11 +874,11 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
     }
     wu[3][c] *= g1; wu[5][c] *= g1; wu[6][c] *= g1; wu[7][c] *= g2;
   }
-  float A[8][3];
+  T A[8][3];
 #pragma unroll
   for (int m = 0; m < 8; ++m)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) A[m][c] = 0.f;
+    for (int c = 0; c < 3; ++c) A[m][c] = T(0);
   // a parallelepiped (affine element: no bilinear or trilinear geometry
   // mode) has the same Jacobian at every point; its adjugate and 1/det are
   // formed once.  The modes are tested for exact zeros, so the point-wise
@@ -881,7 +887,8 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
   if constexpr (!AFF) {
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      affine = affine && wx[3][c] == 0.f && wx[5][c] == 0.f && wx[6][c] == 0.f && wx[7][c] == 0.f;
+      affine = affine && wx[3][c] == T(0) && wx[5][c] == T(0) && wx[6][c] == T(0) &&
+               wx[7][c] == T(0);
   }
   if constexpr (!GEO)
     if (affine) rdet_a = hex8_affine_adjugate(wx, Ja);
@@ -891,8 +898,8 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
   for (int qi = 0; qi < QU; ++qi) {
     const int q = qo + qi;
     // point q at (xi, eta, zeta) = g1 (sx, sy, sz), the order of the rule
-    const float sx = (q & 1) ? 1.f : -1.f, sy = (q & 2) ? 1.f : -1.f, sz = (q & 4) ? 1.f : -1.f;
-    float Dp[9], Ji[9];
+    const T sx = (q & 1) ? T(1) : T(-1), sy = (q & 2) ? T(1) : T(-1), sz = (q & 4) ? T(1) : T(-1);
+    T Dp[9], Ji[9];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       // 8 d(u_j)/d(xi_k) at row k
@@ -900,14 +907,14 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
       Dp[1 + 3 * j] = wu[2][j] + sx * wu[3][j] + sz * wu[6][j] + sx * sz * wu[7][j];
       Dp[2 + 3 * j] = wu[4][j] + sx * wu[5][j] + sy * wu[6][j] + sx * sy * wu[7][j];
     }
-    float rdet;
+    T rdet;
     if (affine) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) Ji[k] = Ja[k];
       rdet = rdet_a;
     } else if constexpr (!AFF) {
       // 8 d(X_j)/d(xi_k) at row k
-      float Jp[9];
+      T Jp[9];
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         Jp[0 + 3 * j] = wx[1][j] + sy * wx[3][j] + sz * wx[5][j] + sy * sz * wx[7][j];
@@ -915,28 +922,28 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
         Jp[2 + 3 * j] = wx[4][j] + sx * wx[5][j] + sy * wx[6][j] + sx * sy * wx[7][j];
       }
       // adjugate: (8 J)^-1 = adj / det8, det8 = 512 det J
-      rdet = 1.f / adj3(Jp, Ji);
+      rdet = T(1) / adj3(Jp, Ji);
     }
     // grad u (i, j) = sum_k J^-1(j, k) du_i/dxi_k  (the factors 8 cancel)
-    float gr[9];
+    T gr[9];
 #pragma unroll
     for (int j = 0; j < 3; ++j)
 #pragma unroll
       for (int i = 0; i < 3; ++i)
         gr[i + 3 * j] = (Ji[j] * Dp[0 + 3 * i] + Ji[j + 3] * Dp[1 + 3 * i] +
                          Ji[j + 6] * Dp[2 + 3 * i]) * rdet;
-    subtract_eigen<3, float>(ps, e_count, le, q, gr);
+    subtract_eigen<3, T>(ps, e_count, le, q, gr);
     // the weight w = det J (2 x 2 x 2 Gauss weights are 1) cancels the 1/det
     // of J^-1 in H = w P J^-1: the unweighted flux times the adjugate is
     // accumulated and the remaining 1/512 applied once per element
-    float P[9];
-    mixed_flux<3, LAW>(gr, 1.f, mpe, ps, e_count, le, q, P);
+    T P[9];
+    mixed_flux<3, LAW, T>(gr, T(1), mpe, ps, e_count, le, q, P);
     // H(k, m) = sum_J P(k, J) adj(J, m), accumulated per mode
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const float H0 = P[k] * Ji[0] + P[k + 3] * Ji[1] + P[k + 6] * Ji[2];
-      const float H1 = P[k] * Ji[3] + P[k + 3] * Ji[4] + P[k + 6] * Ji[5];
-      const float H2 = P[k] * Ji[6] + P[k + 3] * Ji[7] + P[k + 6] * Ji[8];
+      const T H0 = P[k] * Ji[0] + P[k + 3] * Ji[1] + P[k + 6] * Ji[2];
+      const T H1 = P[k] * Ji[3] + P[k + 3] * Ji[4] + P[k + 6] * Ji[5];
+      const T H2 = P[k] * Ji[6] + P[k + 3] * Ji[7] + P[k + 6] * Ji[8];
       A[1][k] += H0;
       A[2][k] += H1;
       A[4][k] += H2;
@@ -946,7 +953,7 @@ __device__ __forceinline__ void element_hex8sf(int64_t le, int64_t e_begin, int6
       A[7][k] += sy * sz * H0 + sx * sz * H1 + sx * sy * H2;
     }
   }
-  constexpr float s0 = 1.f / 512.f, s1 = g1 / 512.f, s2 = g2 / 512.f;
+  constexpr T s0 = T(1) / T(512), s1 = g1 / T(512), s2 = g2 / T(512);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     A[1][c] *= s0; A[2][c] *= s0; A[4][c] *= s0;
@@ -1200,17 +1207,19 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 
 // MINB: blocks per SM the register allocation must allow (1: the compiler's
 // choice)
-template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false, bool GEO = false>
+template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false, bool GEO = false,
+          class T = float>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf(int64_t e_begin, int64_t e_count, int64_t E,
                             const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                            const double *__restrict__ X, const float *__restrict__ geo,
+                            const double *__restrict__ X, const T *__restrict__ geo,
                             const double *__restrict__ u, MatParams mp, GroupArgs ps,
-                            float *__restrict__ re) {
+                            T *__restrict__ re) {
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
-  element_hex8sf<LAW, QU, AFF, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
+  element_hex8sf<LAW, QU, AFF, GEO, T>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps,
+                                       re);
 }
 
 // FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q
@@ -1727,8 +1736,9 @@ __global__ void __launch_bounds__(kPersistentThreads)
         element_geo<D, NN, NQ, LAW>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, tab, up, mp, ps,
                                     reinterpret_cast<float *>(re));
       else
-        element_hex8sf<LAW, QU>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X, nullptr, up, mp, ps,
-                                reinterpret_cast<float *>(re));
+        element_hex8sf<LAW, QU, false, false, float>(le, 0, sa.E, sa.E, sa.conn, sa.pos, sa.X,
+                                                     static_cast<const float *>(nullptr), up,
+                                                     mp, ps, reinterpret_cast<float *>(re));
     }
     if (!grid_barrier(sa.bar, ++gen, sa.status)) return;
     for (int64_t i = t0; i < sa.N; i += stride)

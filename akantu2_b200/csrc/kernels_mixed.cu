@@ -68,30 +68,34 @@ void dispatch_hex8sf_mesh(const ElemTuning &tn, const DevGeom &g, int64_t e0, in
 
 // a hexahedron is a parallelepiped when its bilinear and trilinear geometry
 // modes are zero (the test of the element kernel, on the same FP32 values)
+template <class T>
 __global__ void k_hex8_affine(int64_t E, const int32_t *__restrict__ conn,
                               const double *__restrict__ X, unsigned int *__restrict__ flag) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
-  float wx[8][3];
+  T wx[8][3];
   hex8_geometry_modes(e, E, conn, X, wx);
-  constexpr float g1 = 0.577350269189625764509f, g2 = 1.f / 3.f;
+  constexpr T g1 = std::is_same<T, float>::value ? T(0.577350269189625764509f)
+                                                 : T(0.577350269189625764509);
+  constexpr T g2 = T(1) / T(3);
   bool affine = true;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
-    affine = affine && wx[3][c] * g1 == 0.f && wx[5][c] * g1 == 0.f && wx[6][c] * g1 == 0.f &&
-             wx[7][c] * g2 == 0.f;
+    affine = affine && wx[3][c] * g1 == T(0) && wx[5][c] * g1 == T(0) &&
+             wx[6][c] * g1 == T(0) && wx[7][c] * g2 == T(0);
   if (!affine) atomicOr(flag, 1u);
 }
 
 // the adjugate and 1/det of every element of a mesh of parallelepipeds, into
 // geo [10][E]: the values the element kernel forms from the same modes
+template <class T>
 __global__ void k_hex8_affine_geometry(int64_t E, const int32_t *__restrict__ conn,
-                                       const double *__restrict__ X, float *__restrict__ geo) {
+                                       const double *__restrict__ X, T *__restrict__ geo) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
-  float wx[8][3], Ja[9];
+  T wx[8][3], Ja[9];
   hex8_geometry_modes(e, E, conn, X, wx);
-  const float rdet = hex8_affine_adjugate(wx, Ja);
+  const T rdet = hex8_affine_adjugate(wx, Ja);
 #pragma unroll
   for (int k = 0; k < 9; ++k) geo[(int64_t)k * E + e] = Ja[k];
   geo[(int64_t)9 * E + e] = rdet;
@@ -199,14 +203,68 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
 
 cudaError_t launch_hex8_affine_geometry(const DevGeom &g, float *geo, cudaStream_t s) {
   if (g.E == 0) return cudaSuccess;
-  k_hex8_affine_geometry<<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X, geo);
+  k_hex8_affine_geometry<float><<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X,
+                                                                             geo);
   return cudaGetLastError();
+}
+
+cudaError_t launch_hex8_affine_geometry_fp64(const DevGeom &g, double *geo, cudaStream_t s) {
+  if (g.E == 0) return cudaSuccess;
+  k_hex8_affine_geometry<double><<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X,
+                                                                              geo);
+  return cudaGetLastError();
+}
+
+// FP64 hexahedra by the sum-factorised kernel with contraction allowed (the
+// fast FP64 path): 128 threads, QU points per unrolled iteration, registers
+// capped for MINB blocks; meshes of parallelepipeds read their FP64 adjugate
+// table, the others form their geometry per point
+template <int LAW, int QU, int MINB>
+cudaError_t launch_sf64(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
+                        const MatParams &mp, const GroupArgs &ps, double *re, const double *geo,
+                        cudaStream_t s) {
+  const unsigned grid = (unsigned)((ne + 127) / 128);
+  if (geo)
+    return launch_step(g.pdl, k_element_forces_hex8sf<LAW, 128, QU, MINB, true, true, double>,
+                       grid, 128, s, e0, ne, g.E, g.conn, g.pos, g.X, geo, u, mp, ps, re);
+  return launch_step(g.pdl, k_element_forces_hex8sf<LAW, 128, QU, MINB, false, false, double>,
+                     grid, 128, s, e0, ne, g.E, g.conn, g.pos, g.X, geo, u, mp, ps, re);
+}
+
+template <int LAW>
+cudaError_t dispatch_sf64(const ElemTuning &tn, const DevGeom &g, int64_t e0, int64_t ne,
+                          const double *u, const MatParams &mp, const GroupArgs &ps, double *re,
+                          const double *geo, cudaStream_t s) {
+  if (tn.qu == 1) return launch_sf64<LAW, 1, 1>(g, e0, ne, u, mp, ps, re, geo, s);
+  if (tn.qu == 8) return launch_sf64<LAW, 8, 1>(g, e0, ne, u, mp, ps, re, geo, s);
+  if (tn.minb == 2) return launch_sf64<LAW, 2, 2>(g, e0, ne, u, mp, ps, re, geo, s);
+  if (tn.minb == 3) return launch_sf64<LAW, 2, 3>(g, e0, ne, u, mp, ps, re, geo, s);
+  return launch_sf64<LAW, 2, 1>(g, e0, ne, u, mp, ps, re, geo, s);
+}
+
+cudaError_t launch_element_forces_fp64_sf(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                          const double *u, const MatParams &mp,
+                                          const GroupArgs &ps, double *re, const double *geo,
+                                          const ElemTuning &tn, cudaStream_t s) {
+  if (ne == 0) return cudaSuccess;
+  if (g.et != ET_HEX8) return cudaErrorInvalidValue;
+  if (law == LAW_ELASTIC) return dispatch_sf64<LAW_ELASTIC>(tn, g, e0, ne, u, mp, ps, re, geo, s);
+  if (law == LAW_NEOHOOKEAN)
+    return dispatch_sf64<LAW_NEOHOOKEAN>(tn, g, e0, ne, u, mp, ps, re, geo, s);
+  return dispatch_sf64<LAW_PLASTIC>(tn, g, e0, ne, u, mp, ps, re, geo, s);
 }
 
 cudaError_t launch_hex8_affine_check(const DevGeom &g, unsigned int *flag, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), s);
   if (e != cudaSuccess || g.E == 0) return e;
-  k_hex8_affine<<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X, flag);
+  k_hex8_affine<float><<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X, flag);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hex8_affine_check_fp64(const DevGeom &g, unsigned int *flag, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess || g.E == 0) return e;
+  k_hex8_affine<double><<<(unsigned)((g.E + 255) / 256), 256, 0, s>>>(g.E, g.conn, g.X, flag);
   return cudaGetLastError();
 }
 

@@ -171,4 +171,16 @@ cudaError_t launch_history(const DevGeom &g, const double *u_n, const double *u_
 // adjugate and 1/det of every element of a mesh of parallelepipeds, [10][E]
 cudaError_t launch_hex8_affine_geometry(const DevGeom &g, float *geo, cudaStream_t s);
 cudaError_t launch_hex8_affine_check(const DevGeom &g, unsigned int *flag, cudaStream_t s);
+// the same check and table in FP64 (fast FP64 path)
+cudaError_t launch_hex8_affine_check_fp64(const DevGeom &g, unsigned int *flag, cudaStream_t s);
+cudaError_t launch_hex8_affine_geometry_fp64(const DevGeom &g, double *geo, cudaStream_t s);
+// fast FP64 path, hexahedra: the sum-factorised element kernel in FP64 with
+// contraction allowed (not the operation order of the CPU path: within
+// 1e-12 of it); geo: the FP64 adjugate table of a mesh of parallelepipeds,
+// or null (geometry formed per point); tn.qu 1, 2 or 8 points per
+// iteration, tn.minb 1, 2 or 3 (with 2 points)
+cudaError_t launch_element_forces_fp64_sf(const DevGeom &g, int law, int64_t e0, int64_t ne,
+                                          const double *u, const MatParams &mp,
+                                          const GroupArgs &ps, double *re, const double *geo,
+                                          const ElemTuning &tn, cudaStream_t s);
 }  // namespace akb

@@ -276,6 +276,12 @@ struct akb_model {
   bool all_affine = false;
   int affine_kernel = 0;
   float *dgeo = nullptr;
+  // fast FP64 path (AKB_PRECISION_FP64_FAST): FP64 state and element math,
+  // hexahedra by the sum-factorised kernel with contraction allowed, reading
+  // the FP64 adjugate table of a mesh of parallelepipeds (dgeo64) or forming
+  // their geometry per point
+  bool fast64 = false;
+  double *dgeo64 = nullptr;
   // previous displacement and increment of the last step, when tracked
   bool track_history = false;
   double *dprev = nullptr, *dincr = nullptr;
@@ -594,6 +600,9 @@ int element_forces(akb_model *m, bool in_step) {
     if (m->precision == AKB_PRECISION_MIXED)
       e = launch_element_forces_mixed(g, gr.law, gr.e_begin, gr.e_count, m->tab, m->fB, m->fwJ,
                                       u, mp, ps, (float *)m->dre, gr.tune, m->stream);
+    else if (m->fast64 && m->et == AKB_HEXAHEDRON_8)
+      e = launch_element_forces_fp64_sf(g, gr.law, gr.e_begin, gr.e_count, u, mp, ps,
+                                        (double *)m->dre, m->dgeo64, gr.tune, m->stream);
     else
       e = launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ, u, mp,
                                      ps, (double *)m->dre, gr.tune, m->stream);
@@ -769,7 +778,7 @@ constexpr int64_t kPersistentMaxElements = 1 << 18;
 
 bool use_persistent(const akb_model *m) {
   if (m->persistent == 0 || m->groups.size() != 1 || m->presc_count > 0 || m->E == 0 ||
-      m->track_history || m->dinst_end) return false;
+      m->track_history || m->dinst_end || m->fast64) return false;
   const Group &gr = m->groups[0];
   // mixed hexahedra: the persistent kernel has the 1- and 2-point forms
   if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED && gr.tune.qu != 1 &&
@@ -1103,8 +1112,13 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
   if (m->initialized) return fail(AKB_ESTATE, "initFull called twice");
   if (method != AKB_EXPLICIT_LUMPED_MASS)
     return fail(AKB_EUNSUPPORTED, "only _explicit_lumped_mass is provided");
-  if (precision != AKB_PRECISION_FP64 && precision != AKB_PRECISION_MIXED)
+  if (precision != AKB_PRECISION_FP64 && precision != AKB_PRECISION_MIXED &&
+      precision != AKB_PRECISION_FP64_FAST)
     return fail(AKB_EINVAL, "unknown precision");
+  // the fast FP64 path is the FP64 path everywhere but in the element
+  // kernel of hexahedra
+  m->fast64 = precision == AKB_PRECISION_FP64_FAST;
+  if (m->fast64) precision = AKB_PRECISION_FP64;
   if (m->mats.empty()) return fail(AKB_EMATERIAL, "no material defined (parse a .dat first)");
   if (m->mat_user.empty()) m->mat_user.assign(m->E, 0);
   for (int32_t k : m->mat_user)
@@ -1313,6 +1327,18 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
         if (gr.law == LAW_ELASTIC) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 5};
         else if (gr.law == LAW_NEOHOOKEAN) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 4};
     }
+  }
+  if (m->fast64 && m->et == AKB_HEXAHEDRON_8) {
+    unsigned int *flag = reinterpret_cast<unsigned int *>(m->dscratch), h = 1;
+    AKB_CUDA(launch_hex8_affine_check_fp64(g, flag, s));
+    AKB_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, s));
+    AKB_CUDA(cudaStreamSynchronize(s));
+    if (h == 0) {
+      AKB_TRY(m->alloc(&m->dgeo64, sizeof(double) * 10 * m->E));
+      AKB_CUDA(launch_hex8_affine_geometry_fp64(g, m->dgeo64, s));
+    }
+    for (auto &gr : m->groups) gr.tune = ElemTuning{128, 2, 1};
+    m->pdl = true;
   }
   const size_t gu_size = precision == AKB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
   for (auto &mt : m->groups) {
@@ -2077,6 +2103,9 @@ int akb_model_autotune(akb_model *m, int repeats) {
     if (m->precision == AKB_PRECISION_MIXED)
       return launch_element_forces_mixed(g, gr.law, gr.e_begin, gr.e_count, m->tab, m->fB,
                                          m->fwJ, m->u(), mp, ps, (float *)m->dre, tn, s);
+    if (m->fast64 && m->et == AKB_HEXAHEDRON_8)
+      return launch_element_forces_fp64_sf(g, gr.law, gr.e_begin, gr.e_count, m->u(), mp, ps,
+                                           (double *)m->dre, m->dgeo64, tn, s);
     return launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ,
                                       m->u(), mp, ps, (double *)m->dre, tn, s);
   };
@@ -2088,7 +2117,12 @@ int akb_model_autotune(akb_model *m, int repeats) {
     // threads per block only: the points per iteration of the mixed
     // hexahedron kernel change the FP32 rounding and stay as set
     std::vector<ElemTuning> cand;
-    if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED &&
+    if (m->fast64 && m->et == AKB_HEXAHEDRON_8) {
+      // the register cap only (points per iteration change the rounding)
+      const int q = gr.tune.qu;
+      cand = {{128, q, 1}};
+      if (q == 2) cand.insert(cand.end(), {{128, 2, 2}, {128, 2, 3}});
+    } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED &&
         (gr.tune.qu & AKB_POINTS_PACKED)) {
       const int q = gr.tune.qu;
       cand = {{128, q, 1}, {128, q, 4}, {128, q, 5}};

@@ -308,7 +308,8 @@ class SolidMechanicsModel:
                 _capi.check(L.akb_model_load_materials(self._h, text.encode()))
         if getattr(self, "_selector", None) is not None:
             self.setElementMaterials(self._selector.select(self))
-        prec = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}[precision]
+        prec = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED,
+                "fp64_fast": _capi.PRECISION_FP64_FAST}[precision]
         _capi.check(L.akb_model_init_full(self._h, _capi.EXPLICIT_LUMPED_MASS, prec))
         self._initialized = True
         self.precision = precision

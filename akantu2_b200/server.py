@@ -49,7 +49,8 @@ class ServerStats(ctypes.Structure):
                 ("device_bytes_budget", ctypes.c_int64), ("now", ctypes.c_double)]
 
 
-_PRECISION = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}
+_PRECISION = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED,
+              "fp64_fast": _capi.PRECISION_FP64_FAST}
 
 
 def _params_text(params):

@@ -50,7 +50,12 @@ enum akb_analysis_method { AKB_EXPLICIT_LUMPED_MASS = 0 };
 /* arithmetic of the element kernels; nodal state is FP64 in both */
 enum akb_precision {
   AKB_PRECISION_FP64 = 0,  /* plain FP64, same operation order as the CPU path */
-  AKB_PRECISION_MIXED = 1  /* FP32 element math, FP64 nodal state + gather   */
+  AKB_PRECISION_MIXED = 1, /* FP32 element math, FP64 nodal state + gather   */
+  /* FP64 everywhere; hexahedra by a sum-factorised FP64 element kernel with
+   * contraction allowed: not the CPU path's operation order, within 1e-12 of
+   * it, faster (the plain FP64 path streams dN/dx; this one reads a
+   * per-element adjugate table or recomputes the geometry) */
+  AKB_PRECISION_FP64_FAST = 2
 };
 
 /* nodal arrays, src/model/solid_mechanics/solid_mechanics_model.hh:270-321 */
