@@ -7,7 +7,10 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libakb.so")
+# AKB_BOUNDS_CHECK=1 in the environment loads the bounds-checking build
+# (libakb_checked.so: every index of the step kernels checked on the device)
+LIB_PATH = os.path.join(_HERE, "libakb_checked.so" if os.environ.get("AKB_BOUNDS_CHECK") == "1"
+                        else "libakb.so")
 
 AKB_OK = 0
 ERRORS = {
@@ -135,6 +138,9 @@ def lib():
         "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
         "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,
                                               ctypes.POINTER(i64)]),
+        "akb_bounds_checked": (c_int, []),
+        "akb_model_debug_write_index": (c_int, [vp, c_int, i64, ctypes.c_int32]),
+        "akb_model_set_persistent_wait_test": (c_int, [vp, ctypes.c_uint, c_int, ctypes.c_uint]),
         "akb_exchange_create": (c_int, [vp, c_int, pp]),
         "akb_exchange_add_link": (c_int, [vp, c_int, c_int, vp, vp, i64]),
         "akb_exchange_set_graph_steps": (c_int, [vp, i64]),

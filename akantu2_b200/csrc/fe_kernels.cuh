@@ -113,7 +113,34 @@ struct GroupArgs {
   const int32_t *einst;
   const int64_t *inst_end;
   const int64_t *step;
+  // index checks of the bounds-checking build (AKB_BOUNDS_CHECK): node count,
+  // slot count and the model's status word
+  int64_t nb_nodes, nb_slots;
+  unsigned int *status;
 };
+
+// AKB_BOUNDS_CHECK builds check every index an element reads before using it:
+// node ids in [0, nb_nodes), slot positions in [0, nb_slots); an element with
+// an index out of range sets status bit 2 and is skipped (no access through
+// the bad index)
+constexpr unsigned int ST_INDEX_RANGE = 4u;
+template <int NN>
+__device__ __forceinline__ bool element_indices_ok(const GroupArgs &ps, const int32_t *conn,
+                                                   const int32_t *pos, int64_t E, int64_t e) {
+#ifdef AKB_BOUNDS_CHECK
+  bool ok = true;
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    const int32_t n = conn[(int64_t)a * E + e], p = pos[(int64_t)a * E + e];
+    ok = ok && n >= 0 && n < ps.nb_nodes && p >= 0 && p < ps.nb_slots;
+  }
+  if (!ok && ps.status) atomicOr(ps.status, ST_INDEX_RANGE);
+  return ok;
+#else
+  (void)ps, (void)conn, (void)pos, (void)E, (void)e;
+  return true;
+#endif
+}
 
 // the element's instance still advances in this step
 __device__ __forceinline__ bool element_active(const GroupArgs &ps, int64_t le) {
@@ -618,6 +645,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
+  if (!element_indices_ok<NN>(ps, conn, pos, E, e_begin + le)) return;
   element_pe<D, NN, NQ, LAW, T, RT>(le, e_begin, e_count, E, conn, pos, B, wJ, u, mp, ps, re);
 }
 
@@ -705,6 +733,7 @@ __global__ void __launch_bounds__(BLOCK)
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
+  if (!element_indices_ok<NN>(ps, conn, pos, E, e_begin + le)) return;
   element_geo<D, NN, NQ, LAW>(le, e_begin, e_count, E, conn, pos, X, tab, u, mp, ps, re);
 }
 
@@ -1202,6 +1231,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
+  if (!element_indices_ok<8>(ps, conn, pos, E, e_begin + le)) return;
   element_hex8sf_x2<LAW, PU, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
 }
 
@@ -1218,6 +1248,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
+  if (!element_indices_ok<8>(ps, conn, pos, E, e_begin + le)) return;
   element_hex8sf<LAW, QU, AFF, GEO, T>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps,
                                        re);
 }
@@ -1238,7 +1269,8 @@ __global__ void __launch_bounds__(32 * NQ)
   const int lane = threadIdx.x & 31;
   const int q = threadIdx.x >> 5;
   const int64_t le = (int64_t)blockIdx.x * 32 + lane;
-  const bool active = le < e_count && element_active(ps, le);
+  const bool active = le < e_count && element_active(ps, le) &&
+                      element_indices_ok<NN>(ps, conn, pos, E, e_begin + le);
   const int64_t e = e_begin + le;
   if (active) {
     for (int a = q; a < NN; a += NQ) {
@@ -1343,6 +1375,22 @@ __device__ __forceinline__ void load_32b(const double *q, double *f) {
   asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
                : "=d"(f[0]), "=d"(f[1]), "=d"(f[2]), "=d"(f[3])
                : "l"(q));
+}
+
+// AKB_BOUNDS_CHECK builds: node i's slot range lies within the CSR
+// (0 <= ptr[i] <= ptr[i + 1] <= ptr[N]); a node whose range does not sets
+// status bit 2 and is skipped
+__device__ __forceinline__ bool node_range_ok(const int32_t *ptr, int64_t N, int64_t i,
+                                              unsigned int *status) {
+#ifdef AKB_BOUNDS_CHECK
+  const int32_t p0 = ptr[i], p1 = ptr[i + 1], pn = ptr[N];
+  if (p0 >= 0 && p0 <= p1 && p1 <= pn) return true;
+  atomicOr(status, 4u);
+  return false;
+#else
+  (void)ptr, (void)N, (void)i, (void)status;
+  return true;
+#endif
 }
 
 // WIDE: slots read 32 bytes at a time (the launcher checks the slot
@@ -1500,7 +1548,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               unsigned int *__restrict__ status) {
   pdl_begin();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || !node_range_ok(ptr, N, i, status)) return;
   node_body<D, RT, KAHAN, WIDE>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt,
                                 node_inst, inst_dt, flags, status);
 }
@@ -1524,7 +1572,7 @@ __global__ void k_node_update_retire(int64_t N, const int32_t *__restrict__ ptr,
                                      unsigned int *__restrict__ status) {
   pdl_begin();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || !node_range_ok(ptr, N, i, status)) return;
   // a batch of one instance has no node -> instance table
   if (*step >= inst_end[node_inst ? node_inst[i] : 0]) {
     if (flags & NU_PREDICT) {
@@ -1645,6 +1693,12 @@ struct StepArgs {
   int64_t nsteps;
   unsigned int *status;
   unsigned int *bar;   // [1 + blocks]: release generation, then one arrival flag per block
+  // the barrier's bound on its waits (sleeps of about 32 ns each), and a
+  // failure-path setting: block late_block (>= 0) first sleeps late_us
+  // microseconds, so that a short bound runs out (status bit 1)
+  unsigned int spin_limit;
+  int late_block;
+  unsigned int late_us;
 };
 
 constexpr int kPersistentThreads = 256;
@@ -1657,7 +1711,7 @@ constexpr unsigned int ST_BARRIER_TIMEOUT = 2u;
 // the release, which the other blocks wait for.  Returns false (status bit 1
 // set) when a wait ran out.
 __device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int gen,
-                                             unsigned int *status) {
+                                             unsigned int *status, unsigned int spin_limit) {
   __shared__ int ok;
   volatile unsigned int *release = bar;
   volatile unsigned int *arrive = bar + 1;
@@ -1673,7 +1727,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int gen
       for (unsigned int b = threadIdx.x; b < gridDim.x && fine; b += 32) {
         unsigned int spins = 0;
         while (arrive[b] != gen) {
-          if (++spins > kBarrierSpinLimit) {
+          if (++spins > spin_limit) {
             fine = false;
             break;
           }
@@ -1690,7 +1744,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int gen
   } else if (threadIdx.x == 0) {
     unsigned int spins = 0;
     while (*release != gen) {
-      if (++spins > kBarrierSpinLimit) {
+      if (++spins > spin_limit) {
         atomicOr(status, ST_BARRIER_TIMEOUT);
         break;
       }
@@ -1725,6 +1779,8 @@ __global__ void __launch_bounds__(kPersistentThreads)
   double *up = sa.u_pred, *uo = sa.u_other;
   RT *re = static_cast<RT *>(sa.re);
   unsigned int gen = 0;
+  if ((int)blockIdx.x == sa.late_block && threadIdx.x == 0)
+    for (unsigned int k = 0; k < sa.late_us; ++k) __nanosleep(1000);
   for (int64_t s = 0; s < sa.nsteps; ++s) {
     for (int64_t le = t0; le < sa.E; le += stride) {
       const MatParams &mp = sa.mp;
@@ -1740,11 +1796,11 @@ __global__ void __launch_bounds__(kPersistentThreads)
                                                      static_cast<const float *>(nullptr), up,
                                                      mp, ps, reinterpret_cast<float *>(re));
     }
-    if (!grid_barrier(sa.bar, ++gen, sa.status)) return;
+    if (!grid_barrier(sa.bar, ++gen, sa.status, sa.spin_limit)) return;
     for (int64_t i = t0; i < sa.N; i += stride)
       node_body<D, RT, KAHAN>(i, sa.ptr, re, sa.fext, sa.mass, sa.blocked, sa.fint, sa.a, sa.v,
                               up, uo, sa.dt, sa.node_inst, sa.inst_dt, sa.flags, sa.status);
-    if (!grid_barrier(sa.bar, ++gen, sa.status)) return;
+    if (!grid_barrier(sa.bar, ++gen, sa.status, sa.spin_limit)) return;
     double *tu = up;
     up = uo;
     uo = tu;

@@ -183,6 +183,9 @@ cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const do
                        g.node_inst, g.inst_dt, g.inst_end, (const int64_t *)g.step, flags, status);
   }
   if (g.N == 0) return cudaSuccess;
+#ifdef AKB_BOUNDS_CHECK
+  staged = false;  // the bounds-checking build checks each node's own slot range
+#endif
   if (staged) {
     AKB_DISPATCH_NODE_BLOCK(node_block, {
       auto kern = g.D == 3 ? k_node_update_staged<3, float, true, NB>

@@ -293,6 +293,11 @@ struct akb_model {
   // small single-group meshes, 2 whenever the model allows it
   int persistent = 0;
   unsigned int *dbar = nullptr;  // grid-barrier counters
+  // the persistent kernel's bound on a barrier wait, and the failure-path
+  // setting that makes one block arrive late (akb_model_set_persistent_wait_test)
+  unsigned int bar_spin_limit = kBarrierSpinLimit;
+  int bar_late_block = -1;
+  unsigned int bar_late_us = 0;
   // prescribed velocity ramp on a set of dofs (akb_model_set_prescribed_velocity_ramp)
   int64_t presc_count = 0, presc_ramp = 1;
   double presc_vmax = 0.;
@@ -517,6 +522,9 @@ GroupArgs group_args(akb_model *m, const Group &mt, bool in_step) {
   }
   ps.c33 = mt.c33;
   ps.eig = mt.eig;
+  ps.nb_nodes = m->N;
+  ps.nb_slots = m->E * m->nn;
+  ps.status = m->dstatus;
   if (m->dinst_end) {
     ps.einst = m->delem_inst + mt.e_begin;
     ps.inst_end = m->dinst_end;
@@ -777,6 +785,9 @@ constexpr int kBarrierWords = 1 + 8192;
 constexpr int64_t kPersistentMaxElements = 1 << 18;
 
 bool use_persistent(const akb_model *m) {
+#ifdef AKB_BOUNDS_CHECK
+  return false;  // the bounds-checking build runs the checked two-kernel step only
+#endif
   if (m->persistent == 0 || m->groups.size() != 1 || m->presc_count > 0 || m->E == 0 ||
       m->track_history || m->dinst_end || m->fast64) return false;
   const Group &gr = m->groups[0];
@@ -838,6 +849,9 @@ int run_persistent(akb_model *m, int64_t nsteps, bool any_plastic) {
     sa.nsteps = n;
     sa.status = m->dstatus;
     sa.bar = m->dbar;
+    sa.spin_limit = m->bar_spin_limit;
+    sa.late_block = m->bar_late_block;
+    sa.late_us = m->bar_late_us;
     AKB_CUDA(cudaMemsetAsync(m->dbar, 0, kBarrierWords * sizeof(unsigned int), m->stream));
     cudaError_t e = m->precision == AKB_PRECISION_MIXED
                         ? launch_persistent_mixed(g, gr.law, gr.tune.qu, sa, m->tab, m->stream)
@@ -2034,6 +2048,16 @@ int akb_model_set_persistent(akb_model *m, int mode) {
   return AKB_OK;
 }
 
+int akb_model_set_persistent_wait_test(akb_model *m, unsigned int spin_limit, int late_block,
+                                       unsigned int late_us) {
+  AKB_TRY(check_model(m, true));
+  if (late_us > 1000000u) return fail(AKB_EINVAL, "late_us is at most one second");
+  m->bar_spin_limit = spin_limit ? spin_limit : kBarrierSpinLimit;
+  m->bar_late_block = late_block;
+  m->bar_late_us = late_block >= 0 ? late_us : 0u;
+  return AKB_OK;
+}
+
 int akb_model_persistent_active(const akb_model *m, int *active) {
   if (!m || !active) return fail(AKB_EINVAL, "null argument");
   if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
@@ -2628,6 +2652,43 @@ int akb_model_get_energy(akb_model *m, const char *id, double *value) {
   }
   *value = total;
   return AKB_OK;
+}
+
+int akb_bounds_checked(void) {
+#ifdef AKB_BOUNDS_CHECK
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+int akb_model_debug_write_index(akb_model *m, int which, int64_t position, int32_t value) {
+#ifndef AKB_BOUNDS_CHECK
+  (void)m, (void)which, (void)position, (void)value;
+  return fail(AKB_EUNSUPPORTED, "index writes exist in the bounds-checking build only");
+#else
+  AKB_TRY(check_model(m, true));
+  int32_t *arr = nullptr;
+  int64_t n = 0;
+  if (which == 0) {
+    arr = m->dconn;
+    n = m->E * m->nn;
+  } else if (which == 1) {
+    arr = m->dpos;
+    n = m->E * m->nn;
+  } else if (which == 2) {
+    arr = m->dptr;
+    n = m->N + 1;
+  } else {
+    return fail(AKB_EINVAL, "which is 0 (connectivity), 1 (slot positions) or 2 (CSR offsets)");
+  }
+  if (position < 0 || position >= n) return fail(AKB_EINVAL, "position out of range");
+  AKB_CUDA(cudaMemcpyAsync(arr + position, &value, sizeof(int32_t), cudaMemcpyHostToDevice,
+                           m->stream));
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  // graphs and predictions stay valid: the kernels read the array in place
+  return AKB_OK;
+#endif
 }
 
 int akb_model_get_status(akb_model *m, int *flags) {

@@ -329,6 +329,14 @@ int akb_model_set_stream_priority(akb_model *model, int priority);
  * most 2^18 elements; 2: whenever the model allows it.  Not used with a
  * prescribed motion or several constitutive laws. */
 int akb_model_set_persistent(akb_model *model, int mode);
+/* Failure path of the persistent kernel's grid barrier, for tests: every
+ * wait of the barrier gives up after spin_limit sleeps of about 32 ns (0: the
+ * default bound, about a second), sets bit 1 of the status word
+ * (akb_model_get_status) and ends the launch; block late_block (>= 0; -1:
+ * none) first sleeps late_us microseconds (at most 10^6), so that a short
+ * bound runs out.  The state of a launch that gave up is not a step's. */
+int akb_model_set_persistent_wait_test(akb_model *model, unsigned int spin_limit,
+                                       int late_block, unsigned int late_us);
 int akb_model_persistent_active(const akb_model *model, int *active);
 /* autotuner: times the candidate launch shapes of each law group's
  * element-force kernel (threads per block 64 / 128 / 256; for mixed
@@ -470,6 +478,20 @@ int akb_batch_get_stable_time_steps(akb_model *model, double *dt);
 /* setTimeStep per instance (akb_model_set_time_step sets them all) */
 int akb_batch_set_time_steps(akb_model *model, const double *dt);
 int akb_batch_get_time_steps(const akb_model *model, double *dt);
+
+/* ---- bounds-checking build ----------------------------------------------- */
+/* libakb_checked.so is this library built with AKB_BOUNDS_CHECK: its step
+ * kernels check every index they read (node ids of the connectivity, slot
+ * positions, each node's CSR slot range) before using it; an element or node
+ * with an index out of range is skipped and sets bit 2 of the status word
+ * (akb_model_get_status).  It stands in for a memory checker.  The persistent
+ * kernel and the staged node gather are not used by it.  1 in that build. */
+int akb_bounds_checked(void);
+/* bounds-checking build only (AKB_EUNSUPPORTED otherwise): overwrites one
+ * entry of an index array on the device from the host, for tests of the
+ * checks: which 0 connectivity [n][E] (internal order), 1 slot positions
+ * [n][E], 2 CSR offsets [N + 1] */
+int akb_model_debug_write_index(akb_model *model, int which, int64_t position, int32_t value);
 
 /* ---- serving: many solves resident on one GPU ---------------------------- */
 /* No reference counterpart (the reference runs one model per process).  A

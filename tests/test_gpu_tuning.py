@@ -420,3 +420,44 @@ def test_hex8_packed_shape_rules():
     p = gpu_model(mesh, [UNIT_PLASTIC], precision="mixed")
     with pytest.raises(akb.AkbError):
         p.setLaunchShape("plastic_linear_isotropic_hardening", 128, PACK | 2, 128, 5)
+
+
+def test_persistent_barrier_wait_runs_out_and_reports():
+    """the failure path of the persistent kernel's grid barrier: with a short
+    bound on its waits and one block arriving late, a wait runs out, the
+    launch ends and status bit 1 reports it; the context stays usable and the
+    default bound steps normally again (bit-identical to the step graphs from
+    the same state)"""
+    import time
+    from akantu2_b200 import _capi
+    mesh = akb.box_tet4(10)  # 6,000 elements: 24 blocks of the persistent grid
+    v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
+    m = gpu_model(mesh, [UNIT_ELASTIC])
+    m.setPersistent(2)
+    assert m.persistentActive()
+    m.setNodal("velocity", v0)
+    m.setNodal("blocked_dofs", bl)
+    dt = 0.8 * m.getStableTimeStep()
+    m.setTimeStep(dt)
+    L = _capi.lib()
+    # waits bounded at 64 sleeps (about 2 us); block 1 starts 20 ms late
+    _capi.check(L.akb_model_set_persistent_wait_test(m._h, 64, 1, 20000))
+    t0 = time.perf_counter()
+    m.solveStep(5)
+    status = m.getStatus()
+    assert status & 2, status
+    assert time.perf_counter() - t0 < 10.0
+    _capi.check(L.akb_model_set_persistent_wait_test(m._h, 0, -1, 0))
+    # a fresh state written by the host, then steps with the default bound
+    zero = np.zeros_like(mesh.nodes)
+    for name, val in (("displacement", zero), ("velocity", v0), ("acceleration", zero)):
+        m.setNodal(name, val)
+    m.solveStep(40)
+    assert m.getStatus() == 0
+    ref = gpu_model(mesh, [UNIT_ELASTIC])
+    ref.setNodal("velocity", v0)
+    ref.setNodal("blocked_dofs", bl)
+    ref.setTimeStep(dt)
+    ref.solveStep(40)
+    assert np.array_equal(m.getDisplacement(), ref.getDisplacement())
+    assert np.array_equal(m.getVelocity(), ref.getVelocity())

@@ -195,3 +195,16 @@ def test_boundary_of_reference_patch_meshes():
         x = g["nodes"]
         on_hull = np.any(np.isclose(x, x.min(0)) | np.isclose(x, x.max(0)), axis=1)
         assert set(b) == set(np.nonzero(on_hull)[0])
+
+
+def test_both_library_builds_export_the_checked_entry_points():
+    import ctypes
+    import os
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "akantu2_b200")
+    for name, checked in (("libakb.so", 0), ("libakb_checked.so", 1)):
+        L = ctypes.CDLL(os.path.join(here, name))
+        assert L.akb_bounds_checked() == checked
+        for sym in ("akb_model_debug_write_index", "akb_exchange_create",
+                    "akb_batch_set_instance_steps", "akb_model_set_qp_field"):
+            assert hasattr(L, sym), (name, sym)
