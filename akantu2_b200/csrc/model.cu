@@ -2370,6 +2370,28 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   if (element_block != 64 && element_block != 128 && element_block != 256)
     return fail(AKB_EINVAL, "element_block must be 64, 128 or 256");
   const int q = points_per_iteration;
+  if (m->fast64 && m->et == AKB_HEXAHEDRON_8) {
+    // the FP64 sum-factorised kernel: 128 threads, 1, 2 or 8 points per
+    // iteration, registers capped for 2 or 3 blocks with 2 points
+    if (element_block != 128 || (q != 1 && q != 2 && q != 8) ||
+        (min_blocks != 1 && !(q == 2 && (min_blocks == 2 || min_blocks == 3))))
+      return fail(AKB_EINVAL, "fast FP64 hexahedra: 128 threads, 1, 2 or 8 points per "
+                              "iteration, min_blocks 1 (or 2, 3 with 2 points)");
+    if (node_block < 32 || node_block > 1024 || node_block % 32)
+      return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
+    bool found = false;
+    for (auto &gr : m->groups)
+      if (gr.law == law) {
+        gr.tune = ElemTuning{element_block, q, min_blocks};
+        found = true;
+      }
+    if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
+    m->node_block = node_block;
+    AKB_CUDA(cudaStreamSynchronize(m->stream));
+    for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+    m->graphs.clear();
+    return AKB_OK;
+  }
   const bool sf = m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED;
   const bool tet_mixed = m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_MIXED;
   if (q & AKB_POINTS_PACKED) {
