@@ -358,31 +358,35 @@ def test_affine_kernel_only_for_parallelepipeds():
 
 
 PACK = 256  # AKB_POINTS_PACKED
+PIPE = 512  # AKB_POINTS_PIPELINED
 
 
 @pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
 def test_hex8_packed_pairs_are_the_default_and_bit_identical(mat):
     """meshes of parallelepipeds evaluate elastic and neohookean points as
     packed FP32 pairs by default; every packed shape (points per iteration,
-    register cap) and both affine kernel modes give the same numbers"""
+    register cap, the pipelined gather) and both affine kernel modes give the
+    same numbers"""
     mesh = akb.box_hex8(5, 4, 6, lengths=(1.0, 0.7, 1.3))
     v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
     m = gpu_model(mesh, [mat], precision="mixed")
     b, q, mb, n = m.getLaunchShape(mat["type"])
     assert q == PACK | 8 and b == 128
     runs = []
-    for affine in (2, 1):
-        for pts in (2, 4, 8):
-            for minb in (1, 4, 5):
-                m = gpu_model(mesh, [mat], precision="mixed")
-                m.setAffineKernel(affine)
-                m.setLaunchShape(mat["type"], 128, PACK | pts, 128, minb)
-                m.setNodal("velocity", v0)
-                m.setNodal("blocked_dofs", bl)
-                m.setTimeStep(0.8 * m.getStableTimeStep())
-                m.solveStep(130)
-                runs.append(((affine, pts, minb), m.getDisplacement().copy(),
-                             m.getVelocity().copy(), m.getInternalForce().copy()))
+    shapes = [(affine, PACK | pts, minb) for affine in (2, 1) for pts in (2, 4, 8)
+              for minb in (1, 4, 5)]
+    # the gather software-pipelined through shared memory (adjugate table)
+    shapes += [(2, PACK | PIPE | pts, minb) for pts in (2, 4, 8) for minb in (3, 4)]
+    for affine, q, minb in shapes:
+        m = gpu_model(mesh, [mat], precision="mixed")
+        m.setAffineKernel(affine)
+        m.setLaunchShape(mat["type"], 128, q, 128, minb)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.solveStep(130)
+        runs.append(((affine, q, minb), m.getDisplacement().copy(), m.getVelocity().copy(),
+                     m.getInternalForce().copy()))
     for other in runs[1:]:
         for a, b_ in zip(runs[0][1:], other[1:]):
             assert np.array_equal(a, b_), (runs[0][0], other[0])
@@ -412,6 +416,13 @@ def test_hex8_packed_shape_rules():
         m.setLaunchShape("neohookean", 64, PACK | 8, 128, 1)  # 128 threads only
     with pytest.raises(akb.AkbError):
         m.setLaunchShape("neohookean", 128, PACK | 3, 128, 1)
+    with pytest.raises(akb.AkbError):
+        m.setLaunchShape("neohookean", 128, PIPE | 2, 128, 4)  # pipelined needs packed
+    with pytest.raises(akb.AkbError):
+        m.setLaunchShape("neohookean", 128, PACK | PIPE | 2, 128, 5)
+    m.setAffineKernel(1)  # coordinates gathered: no table, no pipelined form
+    with pytest.raises(akb.AkbError):
+        m.setLaunchShape("neohookean", 128, PACK | PIPE | 2, 128, 4)
     m.setAffineKernel(0)  # no packed form for the general kernel: scalar again
     b, q, mb, n = m.getLaunchShape("neohookean")
     assert not (q & PACK)
