@@ -1236,85 +1236,6 @@ __device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, i
   element_hex8sf_x2_core<LAW, PU, GEO>(wu, le, e_begin, e_count, E, conn, pos, X, geo, mp, ps, re);
 }
 
-// asynchronous 8-byte copy global -> shared (cp.async, no cluster, no
-// multicast), its group commit and wait
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// The packed kernel with its displacement gather software-pipelined: a grid
-// of resident blocks, each thread advancing elements le, le + stride, ...;
-// while it computes element k, the 24 displacement components of element
-// k + 1 are on their way into its own slots of shared memory (cp.async, two
-// stages) and the connectivity of element k + 2 into registers, so the
-// dependent gather (connectivity, then displacement) leaves the critical
-// path.  Shared memory [2][24][128] doubles (48 KB per block); every thread
-// reads only the slots it filled.  Same arithmetic as k_element_forces_hex8sf_x2.
-constexpr int kPipeThreads = 128;
-constexpr size_t kPipeSmem = sizeof(double) * 2 * 24 * kPipeThreads;
-template <int LAW, int PU, int MINB>
-__global__ void __launch_bounds__(kPipeThreads, MINB)
-    k_element_forces_hex8sf_x2p(int64_t e_begin, int64_t e_count, int64_t E,
-                                const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                                const float *__restrict__ geo, const double *__restrict__ u,
-                                MatParams mp, GroupArgs ps, float *__restrict__ re) {
-  extern __shared__ double su[];
-  pdl_begin();
-  constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
-  const int t = threadIdx.x;
-  const int64_t stride = (int64_t)gridDim.x * kPipeThreads;
-  int64_t le = (int64_t)blockIdx.x * kPipeThreads + t;
-  int32_t cn[8];
-  auto load_conn = [&](int64_t l) {
-    if (l < e_count) {
-#pragma unroll
-      for (int a = 0; a < 8; ++a) cn[a] = conn[(int64_t)a * E + e_begin + l];
-    }
-  };
-  auto issue = [&](int64_t l, int b) {
-    if (l < e_count) {
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-          cp_async8(&su[(b * 24 + a * 3 + i) * kPipeThreads + t], u + (int64_t)cn[a] * 3 + i);
-    }
-    cp_async_commit();  // an empty group past the end keeps the count
-  };
-  load_conn(le);
-  issue(le, 0);
-  load_conn(le + stride);
-  int b = 0;
-  for (; le < e_count; le += stride) {
-    issue(le + stride, b ^ 1);
-    load_conn(le + 2 * stride);
-    cp_async_wait<1>();  // element le's displacements are in stage b
-    if (element_active(ps, le)) {
-      float wu[8][3];
-      double u0[3];
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const double uu = su[(b * 24 + a * 3 + i) * kPipeThreads + t];
-          if (a == 0) u0[i] = uu;
-          wu[lex[a]][i] = (float)(uu - u0[i]);
-        }
-      element_hex8sf_x2_core<LAW, PU, true>(wu, le, e_begin, e_count, E, conn, pos, nullptr,
-                                            geo, mp, ps, re);
-    }
-    b ^= 1;
-  }
-  cp_async_wait<0>();
-}
-
 template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf_x2(int64_t e_begin, int64_t e_count, int64_t E,

@@ -28,9 +28,6 @@ struct ElemTuning {
 // points_per_iteration flag of the mixed hexahedron kernel: the points are
 // evaluated as packed FP32 pairs (2, 4 or 8 points per iteration)
 constexpr int kPackedPoints = 256;
-// with kPackedPoints: the displacement gather software-pipelined through
-// shared memory (cp.async), a grid of resident blocks (min_blocks 3 or 4)
-constexpr int kPipelinedPoints = 512;
 
 // device view of the mesh, internal element order
 struct DevGeom {

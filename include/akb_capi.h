@@ -362,12 +362,6 @@ int akb_model_autotune(akb_model *model, int repeats);
  * points are evaluated as packed FP32 pairs, 2, 4 or 8 points per iteration
  * (e.g. AKB_POINTS_PACKED | 2); a different FP32 evaluation order again */
 #define AKB_POINTS_PACKED 256
-/* with AKB_POINTS_PACKED, on a mesh of parallelepipeds reading its adjugate
- * table (affine kernel 2): the element's displacement gather is
- * software-pipelined through shared memory (asynchronous copies of the next
- * element's displacements while the current one is computed), a grid of
- * resident blocks, min_blocks 3 or 4; the same arithmetic as the packed form */
-#define AKB_POINTS_PIPELINED 512
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,

@@ -53,7 +53,7 @@ def test_fp64_fast_register_caps_are_bit_identical():
         m = akb.SolidMechanicsModel(mesh)
         m.addMaterial("neohookean", rho=1.0, E=1.0, nu=0.3)
         m.initFull(akb._explicit_lumped_mass, precision="fp64_fast")
-        assert m.getLaunchShape("neohookean")[1] == 2
+        assert m.getLaunchShape("neohookean")[1:3] == (2, 3)
         m.setLaunchShape("neohookean", 128, 2, 256, minb)
         m.setNodal("velocity", v0)
         m.setNodal("blocked_dofs", bl)

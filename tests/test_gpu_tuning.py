@@ -358,15 +358,13 @@ def test_affine_kernel_only_for_parallelepipeds():
 
 
 PACK = 256  # AKB_POINTS_PACKED
-PIPE = 512  # AKB_POINTS_PIPELINED
 
 
 @pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
 def test_hex8_packed_pairs_are_the_default_and_bit_identical(mat):
     """meshes of parallelepipeds evaluate elastic and neohookean points as
     packed FP32 pairs by default; every packed shape (points per iteration,
-    register cap, the pipelined gather) and both affine kernel modes give the
-    same numbers"""
+    register cap) and both affine kernel modes give the same numbers"""
     mesh = akb.box_hex8(5, 4, 6, lengths=(1.0, 0.7, 1.3))
     v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
     m = gpu_model(mesh, [mat], precision="mixed")
@@ -375,8 +373,6 @@ def test_hex8_packed_pairs_are_the_default_and_bit_identical(mat):
     runs = []
     shapes = [(affine, PACK | pts, minb) for affine in (2, 1) for pts in (2, 4, 8)
               for minb in (1, 4, 5)]
-    # the gather software-pipelined through shared memory (adjugate table)
-    shapes += [(2, PACK | PIPE | pts, minb) for pts in (2, 4, 8) for minb in (3, 4)]
     for affine, q, minb in shapes:
         m = gpu_model(mesh, [mat], precision="mixed")
         m.setAffineKernel(affine)
@@ -416,13 +412,6 @@ def test_hex8_packed_shape_rules():
         m.setLaunchShape("neohookean", 64, PACK | 8, 128, 1)  # 128 threads only
     with pytest.raises(akb.AkbError):
         m.setLaunchShape("neohookean", 128, PACK | 3, 128, 1)
-    with pytest.raises(akb.AkbError):
-        m.setLaunchShape("neohookean", 128, PIPE | 2, 128, 4)  # pipelined needs packed
-    with pytest.raises(akb.AkbError):
-        m.setLaunchShape("neohookean", 128, PACK | PIPE | 2, 128, 5)
-    m.setAffineKernel(1)  # coordinates gathered: no table, no pipelined form
-    with pytest.raises(akb.AkbError):
-        m.setLaunchShape("neohookean", 128, PACK | PIPE | 2, 128, 4)
     m.setAffineKernel(0)  # no packed form for the general kernel: scalar again
     b, q, mb, n = m.getLaunchShape("neohookean")
     assert not (q & PACK)
