@@ -134,6 +134,10 @@ def lib():
                                                ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                                ctypes.POINTER(c_int)]),
         "akb_model_set_launch_shape": (c_int, [vp, c_int, c_int, c_int, c_int, c_int]),
+        "akb_model_set_prefetch": (c_int, [vp, c_int, c_int]),
+        "akb_model_get_prefetch": (c_int, [vp, c_int, ctypes.POINTER(c_int)]),
+        "akb_model_set_recompute_geometry": (c_int, [vp, c_int, c_int]),
+        "akb_model_get_recompute_geometry": (c_int, [vp, c_int, ctypes.POINTER(c_int)]),
         "akb_model_stream": (c_int, [vp, pp]),
         "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
         "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "fe_kernels.cuh"
@@ -112,11 +113,38 @@ inline cudaError_t launch_cooperative(K kernel, int64_t work, const StepArgs &sa
   return cudaLaunchCooperativeKernel((const void *)kernel, grid, kPersistentThreads, args, 0, s);
 }
 
+// elements one wave of resident blocks of kernel covers: its occupancy
+// times the SM count (0 if the query fails)
+template <class K>
+int64_t wave_elements(K kernel, int block) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess)
+    return 0;
+  return (int64_t)sms * per_sm * block;
+}
+
+// L2 prefetch distance, in elements, of `waves` waves of resident blocks of
+// the kernel K (0: none); the wave is queried once per kernel (the GPUs of a
+// node are of one model)
+template <auto K>
+int64_t prefetch_distance(int waves, int block) {
+  if (waves <= 0) return 0;
+  static std::atomic<int64_t> wave{-1};
+  int64_t w = wave.load(std::memory_order_relaxed);
+  if (w < 0) wave.store(w = wave_elements(K, block), std::memory_order_relaxed);
+  return waves * w;
+}
+
+// tab: the quadrature tables, for the kernels that recompute dN/dx and
+// det J w from the coordinates (tn.rec; tetrahedra and triangles)
 template <class T, class RT>
 inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const T *B, const T *wJ, const double *u,
                                        const MatParams &mp, const GroupArgs &ps, RT *re,
-                                       const ElemTuning &tn, cudaStream_t s) {
+                                       const ElemTuning &tn, const QuadTable *tab,
+                                       cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   AKB_DISPATCH_ELEM(g, {
     (void)ET;
@@ -133,21 +161,49 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
     } else {
       AKB_DISPATCH_BLOCK(tn.block, {
         const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
+        if constexpr (ET != ET_HEX8) {
+          if (tn.rec && tab) {
+            if constexpr (BLOCK == 128) {
+              if (law == LAW_PLASTIC && tn.minb > 1) {
+                constexpr auto k6 = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>;
+                constexpr auto k5 = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;
+                const int64_t pf = tn.minb >= 6 ? prefetch_distance<k6>(tn.pf, 128)
+                                                : prefetch_distance<k5>(tn.pf, 128);
+                return launch_step(g.pdl, tn.minb >= 6 ? k6 : k5, grid, 128, s, e0, ne, g.E,
+                                   g.conn, g.pos, g.X, *tab, u, mp, ps, re, pf);
+              }
+            }
+            constexpr auto ke = k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>;
+            constexpr auto kn = k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>;
+            constexpr auto kp = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;
+            const int64_t pf = law == LAW_ELASTIC      ? prefetch_distance<ke>(tn.pf, BLOCK)
+                               : law == LAW_NEOHOOKEAN ? prefetch_distance<kn>(tn.pf, BLOCK)
+                                                       : prefetch_distance<kp>(tn.pf, BLOCK);
+            auto kern = law == LAW_ELASTIC ? ke : law == LAW_NEOHOOKEAN ? kn : kp;
+            return launch_step(g.pdl, kern, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X,
+                               *tab, u, mp, ps, re, pf);
+          }
+        }
         if constexpr (BLOCK == 128) {
           // plastic groups: 128 threads with registers capped for 5 or 6 blocks per SM
           if (law == LAW_PLASTIC && tn.minb > 1) {
-            auto kern = tn.minb >= 6 ? k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>
-                                     : k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;
-            return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
-                               mp, ps, re);
+            constexpr auto k6 = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>;
+            constexpr auto k5 = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;
+            const int64_t pf = tn.minb >= 6 ? prefetch_distance<k6>(tn.pf, 128)
+                                            : prefetch_distance<k5>(tn.pf, 128);
+            return launch_step(g.pdl, tn.minb >= 6 ? k6 : k5, grid, 128, s, e0, ne, g.E, g.conn,
+                               g.pos, B, wJ, u, mp, ps, re, pf);
           }
         }
-        auto kern = law == LAW_ELASTIC ? k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>
-                    : law == LAW_NEOHOOKEAN
-                        ? k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>
-                        : k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;
+        constexpr auto ke = k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>;
+        constexpr auto kn = k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>;
+        constexpr auto kp = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;
+        const int64_t pf = law == LAW_ELASTIC      ? prefetch_distance<ke>(tn.pf, BLOCK)
+                           : law == LAW_NEOHOOKEAN ? prefetch_distance<kn>(tn.pf, BLOCK)
+                                                   : prefetch_distance<kp>(tn.pf, BLOCK);
+        auto kern = law == LAW_ELASTIC ? ke : law == LAW_NEOHOOKEAN ? kn : kp;
         return launch_step(g.pdl, kern, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
-                           mp, ps, re);
+                           mp, ps, re, pf);
       });
     }
   });

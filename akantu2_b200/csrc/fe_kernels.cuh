@@ -39,6 +39,23 @@ __device__ __forceinline__ void pdl_begin() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// L2 prefetch (cp.async.bulk.prefetch.L2: nothing reaches the SM) of the
+// bytes [lo, hi) of an array occupying [base, end).  The range is widened to
+// 16-byte boundaries, as the instruction requires, and clipped to the
+// array's own 16-byte-aligned span, so no byte outside the array is named.
+__device__ __forceinline__ void prefetch_l2(const void *base, const void *end, const void *lo,
+                                            const void *hi) {
+  const uint64_t b0 = ((uint64_t)__cvta_generic_to_global(base) + 15) & ~(uint64_t)15;
+  const uint64_t b1 = (uint64_t)__cvta_generic_to_global(end) & ~(uint64_t)15;
+  uint64_t a = (uint64_t)__cvta_generic_to_global(lo) & ~(uint64_t)15;
+  uint64_t z = ((uint64_t)__cvta_generic_to_global(hi) + 15) & ~(uint64_t)15;
+  if (a < b0) a = b0;
+  if (z > b1) z = b1;
+  if (z > a)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(z - a))
+                 : "memory");
+}
+
 // natural-coordinate tables evaluated on the host (passed by value: they sit
 // in the kernel-parameter constant bank)
 struct QuadTable {
@@ -198,8 +215,88 @@ __device__ __forceinline__ MatParams group_params(const MatParams &mp, const Gro
 
 // ---------------------------------------------------------------------------
 // K0: dN/dx and det J * w  (element_class_tmpl.hh:296-395,
-// integrator_gauss_inline_impl.hh:176-195,378-398).  One thread per (e, q),
-// element fastest.  bad receives the smallest e*NQ + q with det J < 0.
+// integrator_gauss_inline_impl.hh:176-195,378-398).
+//
+// point_geometry: one quadrature point from the element's nodal coordinates
+// Xe [NN][D] and dN/ds at the point, dn(k, a): J = dN/ds X, det J
+// by first-row expansion, J^-1 through the adjugate (det from the
+// first-column cofactors), dN/dx = J^-1 dN/ds, wJ = det J w.  Every product,
+// sum and quotient is explicitly rounded, so the translation units built with
+// and without contraction compute the same bits: the step kernels that
+// recompute the geometry instead of streaming it reproduce the precomputed
+// tables exactly.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double cof3_rn(const double *m, int i, int j) {
+  const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+  return sub_rn(mul_rn(m[i1 + 3 * j1], m[i2 + 3 * j2]), mul_rn(m[i1 + 3 * j2], m[i2 + 3 * j1]));
+}
+template <int D, int NN, class DN>
+__device__ __forceinline__ double point_geometry(const double *Xe, const DN &dn, double w,
+                                                 double *Bq, double *wJq) {
+  double J[D * D], Ji[D * D];
+#pragma unroll
+  for (int k = 0; k < D; ++k)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      double s = mul_rn(dn(k, 0), Xe[j]);
+#pragma unroll
+      for (int a = 1; a < NN; ++a) s = add_rn(s, mul_rn(dn(k, a), Xe[a * D + j]));
+      J[k + D * j] = s;
+    }
+  double det;
+  if constexpr (D == 3) {
+    const double *m = J;
+    det = add_rn(sub_rn(mul_rn(m[0], sub_rn(mul_rn(m[4], m[8]), mul_rn(m[7], m[5]))),
+                        mul_rn(m[3], sub_rn(mul_rn(m[1], m[8]), mul_rn(m[7], m[2])))),
+                 mul_rn(m[6], sub_rn(mul_rn(m[1], m[5]), mul_rn(m[4], m[2]))));
+    const double c0 = cof3_rn(m, 0, 0), c1 = cof3_rn(m, 1, 0), c2 = cof3_rn(m, 2, 0);
+    const double dc = add_rn(add_rn(mul_rn(c0, m[0]), mul_rn(c1, m[1])), mul_rn(c2, m[2]));
+    const double id = __ddiv_rn(1., dc);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Ji[i + 3 * j] = mul_rn(cof3_rn(m, j, i), id);
+  } else {
+    det = sub_rn(mul_rn(J[0], J[3]), mul_rn(J[1], J[2]));
+    const double id = __ddiv_rn(1., det);
+    Ji[0] = mul_rn(J[3], id);
+    Ji[1] = mul_rn(-J[1], id);
+    Ji[2] = mul_rn(-J[2], id);
+    Ji[3] = mul_rn(J[0], id);
+  }
+#pragma unroll
+  for (int a = 0; a < NN; ++a)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      double s = mul_rn(Ji[j], dn(0, a));
+#pragma unroll
+      for (int k = 1; k < D; ++k) s = add_rn(s, mul_rn(Ji[j + D * k], dn(k, a)));
+      Bq[a * D + j] = s;
+    }
+  *wJq = mul_rn(det, w);
+  return det;
+}
+
+// dN/ds at one point: the host-evaluated table of the element type
+struct TableDn {
+  const double *p;  // dnds of the point, [k][kMaxNN]
+  __device__ __forceinline__ double operator()(int k, int a) const { return p[k * kMaxNN + a]; }
+};
+// dN/ds of the linear tetrahedron (the same at every point; N3 = xi, N1 =
+// eta, N2 = zeta, N0 = 1 - xi - eta - zeta) at compile time: the products
+// with its 1 and -1 entries fold to exact copies and negations, its 0 entries
+// stay multiplications (0 x X keeps the signs of zeros the table-driven sums
+// give), so it computes what TableDn over the tetrahedron's table computes
+struct Tet4Dn {
+  __device__ __forceinline__ constexpr double operator()(int k, int a) const {
+    return a == 0 ? -1. : (a == (k == 0 ? 3 : k) ? 1. : 0.);
+  }
+};
+
+// One thread per (e, q), element fastest.  bad receives the smallest
+// e*NQ + q with det J < 0.
 template <int D, int NN, int NQ>
 __global__ void k_precompute(const double *__restrict__ X, const int32_t *__restrict__ conn,
                              int64_t E, QuadTable tab, double *__restrict__ B,
@@ -215,36 +312,13 @@ __global__ void k_precompute(const double *__restrict__ X, const int32_t *__rest
 #pragma unroll
     for (int i = 0; i < D; ++i) Xe[a * D + i] = X[node * D + i];
   }
-  const double *dn = &tab.dnds[q * 3 * kMaxNN];
-  double J[D * D], Ji[D * D];
+  double Bq[NN * D], wq;
+  const double det =
+      point_geometry<D, NN>(Xe, TableDn{&tab.dnds[q * 3 * kMaxNN]}, tab.w[q], Bq, &wq);
 #pragma unroll
-  for (int k = 0; k < D; ++k)
-#pragma unroll
-    for (int j = 0; j < D; ++j) {
-      double s = dn[k * kMaxNN] * Xe[j];
-#pragma unroll
-      for (int a = 1; a < NN; ++a) s = s + dn[k * kMaxNN + a] * Xe[a * D + j];
-      J[k + D * j] = s;
-    }
-  double det;
-  if constexpr (D == 3) {
-    det = det3(J);
-    inv3(J, Ji);
-  } else {
-    det = det2(J);
-    inv2(J, Ji);
-  }
-#pragma unroll
-  for (int a = 0; a < NN; ++a)
-#pragma unroll
-    for (int j = 0; j < D; ++j) {
-      double s = Ji[j] * dn[a];
-#pragma unroll
-      for (int k = 1; k < D; ++k) s = s + Ji[j + D * k] * dn[k * kMaxNN + a];
-      B[(int64_t)((q * NN + a) * D + j) * E + e] = s;
-    }
+  for (int c = 0; c < NN * D; ++c) B[(int64_t)(q * NN * D + c) * E + e] = Bq[c];
   if (det < 0) atomicMin(bad, (unsigned long long)(e * NQ + q));
-  wJ[t] = det * tab.w[q];
+  wJ[t] = wq;
 }
 
 // ---------------------------------------------------------------------------
@@ -575,20 +649,28 @@ __device__ __forceinline__ void element_law(const T *ue, const T *b, T w, const 
   }
 }
 
-// element le of a launch over [e_begin, e_begin + e_count): streamed dN/dx
-template <int D, int NN, int NQ, int LAW, class T, class RT>
+// element le of a launch over [e_begin, e_begin + e_count): dN/dx and
+// det J w streamed from the precomputed tables B, wJ, or with REC recomputed
+// from the nodal coordinates X by the precomputation's own arithmetic
+// (point_geometry, FP64, then rounded to T like the tables' FP32 copies):
+// the same numbers either way, REC reading the L2-resident coordinates
+// instead of streaming (NQ x NN x D + NQ) values per element from DRAM
+template <int D, int NN, int NQ, int LAW, class T, class RT, bool REC = false>
 __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t e_count,
                                            int64_t E, const int32_t *conn,
                                            const int32_t *pos,
                                            const T *B, const T *wJ,
                                            const double *u, const MatParams &mp,
-                                           const GroupArgs &ps, RT *re) {
+                                           const GroupArgs &ps, RT *re,
+                                           const double *X = nullptr,
+                                           const QuadTable *tab = nullptr) {
   constexpr int ND = NN * D;
   constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
   const int64_t e = e_begin + le;
   const MatParams mpe = group_params(mp, ps, le);
   T ue[ND];
   double u0[D];
+  double Xe[REC ? ND : 1];
 #pragma unroll
   for (int a = 0; a < NN; ++a) {
     const int64_t node = conn[(int64_t)a * E + e];
@@ -601,6 +683,7 @@ __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t 
       } else {
         ue[a * D + i] = x;
       }
+      if constexpr (REC) Xe[a * D + i] = X[node * D + i];
     }
   }
   // mixed tetrahedra stream dN/dx of nodes 1..3 only ([9][E]); node 0's are
@@ -611,16 +694,30 @@ __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t 
 #pragma unroll 1
   for (int q = 0; q < NQ; ++q) {
     T b[ND];
+    T w;
+    if constexpr (REC) {
+      double Bq[ND], wq;
+      if constexpr (D == 3 && NN == 4)
+        point_geometry<D, NN>(Xe, Tet4Dn{}, tab->w[q], Bq, &wq);
+      else
+        point_geometry<D, NN>(Xe, TableDn{&tab->dnds[q * 3 * kMaxNN]}, tab->w[q], Bq, &wq);
+#pragma unroll
+      for (int c = TET_COMPACT ? 3 : 0; c < ND; ++c) b[c] = (T)Bq[c];
+      w = (T)wq;
+    } else {
+      if constexpr (TET_COMPACT) {
+#pragma unroll
+        for (int c = 3; c < ND; ++c) b[c] = B[(int64_t)(c - 3) * E + e];
+      } else {
+#pragma unroll
+        for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)(q * ND + c) * E + e];
+      }
+      w = wJ[(int64_t)q * E + e];
+    }
     if constexpr (TET_COMPACT) {
 #pragma unroll
-      for (int c = 3; c < ND; ++c) b[c] = B[(int64_t)(c - 3) * E + e];
-#pragma unroll
       for (int j = 0; j < 3; ++j) b[j] = -((b[3 + j] + b[6 + j]) + b[9 + j]);
-    } else {
-#pragma unroll
-      for (int c = 0; c < ND; ++c) b[c] = B[(int64_t)(q * ND + c) * E + e];
     }
-    const T w = wJ[(int64_t)q * E + e];
     T t[ND];
     element_law<D, NN, LAW, T, REL>(ue, b, w, mpe, ps, e_count, le, q, t);
     // integrate: sum over q in increasing order (integrator_gauss_inline_impl.hh:401-418)
@@ -632,6 +729,62 @@ __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t 
   for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
 }
 
+// The element-indexed rows the warp pf elements further on reads, prefetched
+// into L2 (one row segment of 32 elements per lane and pass): connectivity,
+// slot positions, dN/dx and det J w, the material slot, and the previous
+// plastic state of every point ([row][e_count] arrays of the group).  L2 is
+// the device's point of coherence, so a prefetch can never return stale
+// data: it is issued before the dependent-launch wait.
+template <int D, int NN, int NQ, int LAW, class T>
+__device__ __forceinline__ void prefetch_pe_rows(int64_t pf, int64_t e_begin, int64_t e_count,
+                                                 int64_t E, const int32_t *conn,
+                                                 const int32_t *pos, const T *B, const T *wJ,
+                                                 const GroupArgs &ps) {
+  constexpr int ND = NN * D, DD = D * D, NS = SymComps<D>::value;
+  constexpr bool TET_COMPACT = D == 3 && NN == 4 && NQ == 1 && !std::is_same<T, double>::value;
+  constexpr int NB = TET_COMPACT ? 9 : NQ * ND;
+  constexpr int NPL = LAW == LAW_PLASTIC ? NQ * (2 * NS + DD + 2) : 0;
+  constexpr int kRows = 2 * NN + NB + NQ + 1 + NPL;
+  const int64_t w0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31) + pf;
+  if (w0 >= e_count) return;
+  const int64_t w1 = w0 + 32 < e_count ? w0 + 32 : e_count;
+  for (int r = threadIdx.x & 31; r < kRows; r += 32) {
+    // array, its entry count and size, and the entry of local element 0
+    const char *b = nullptr;
+    int64_t n = 0, at = 0;
+    int esz = 4;
+    int k = r;
+    if (k < NN) {
+      b = (const char *)conn, n = NN * E, at = k * E + e_begin;
+    } else if ((k -= NN) < NN) {
+      b = (const char *)pos, n = NN * E, at = k * E + e_begin;
+    } else if ((k -= NN) < NB) {
+      b = (const char *)B, n = NB * E, at = k * E + e_begin, esz = sizeof(T);
+    } else if ((k -= NB) < NQ) {
+      b = (const char *)wJ, n = NQ * E, at = k * E + e_begin, esz = sizeof(T);
+    } else if ((k -= NQ) < 1) {
+      b = (const char *)ps.mslot, n = e_count;  // per-element material slot, or none
+    } else if (LAW == LAW_PLASTIC) {
+      k -= 1;
+      esz = 8;
+      if (k < NQ * NS) {
+        b = (const char *)ps.sig_prev, n = NQ * NS * e_count, at = k * e_count;
+      } else if ((k -= NQ * NS) < NQ * NS) {
+        b = (const char *)ps.eps_prev, n = NQ * NS * e_count, at = k * e_count;
+      } else if ((k -= NQ * NS) < NQ * DD) {
+        esz = sizeof(T);
+        b = (const char *)ps.gu_prev, n = NQ * DD * e_count, at = k * e_count;
+      } else if ((k -= NQ * DD) < NQ) {
+        b = (const char *)ps.iso_prev, n = NQ * e_count, at = k * e_count;
+      } else {
+        k -= NQ;
+        b = (const char *)ps.iso_cur_in, n = NQ * e_count, at = k * e_count;
+      }
+    }
+    if (b) prefetch_l2(b, b + n * esz, b + (at + w0) * esz, b + (at + w1) * esz);
+  }
+}
+
 // BLOCK: threads (= elements) per block, one of the launch shapes the
 // autotuner chooses from; MINB > 1 caps the registers for that many resident
 // blocks per SM (plastic groups, whose state loads want more warps in flight)
@@ -641,12 +794,32 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const T *__restrict__ B, const T *__restrict__ wJ,
                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
-                        RT *__restrict__ re) {
+                        RT *__restrict__ re, int64_t pf) {
+  if (pf > 0) prefetch_pe_rows<D, NN, NQ, LAW, T>(pf, e_begin, e_count, E, conn, pos, B, wJ, ps);
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
   if (!element_indices_ok<NN>(ps, conn, pos, E, e_begin + le)) return;
   element_pe<D, NN, NQ, LAW, T, RT>(le, e_begin, e_count, E, conn, pos, B, wJ, u, mp, ps, re);
+}
+
+// k_element_forces_pe with the geometry recomputed from the coordinates
+// (element_pe REC): the same numbers, no dN/dx and det J w streamed
+template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_element_forces_pr(int64_t e_begin, int64_t e_count, int64_t E,
+                        const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                        const double *__restrict__ X, const QuadTable tab,
+                        const double *__restrict__ u, MatParams mp, GroupArgs ps,
+                        RT *__restrict__ re, int64_t pf) {
+  if (pf > 0)
+    prefetch_pe_rows<D, NN, NQ, LAW, T>(pf, e_begin, e_count, E, conn, pos, nullptr, nullptr, ps);
+  pdl_begin();
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count || !element_active(ps, le)) return;
+  if (!element_indices_ok<NN>(ps, conn, pos, E, e_begin + le)) return;
+  element_pe<D, NN, NQ, LAW, T, RT, true>(le, e_begin, e_count, E, conn, pos, nullptr, nullptr, u,
+                                          mp, ps, re, X, &tab);
 }
 
 // Mixed path: FP32 element math with the shape derivatives recomputed from
@@ -1070,9 +1243,6 @@ __device__ __forceinline__ void elastic_stress_x2(float lambda, float mu, float 
 
 // PU pairs per unrolled iteration (1, 2 or 4); meshes of parallelepipeds
 // only (one adjugate per element, from the geometry table with GEO); the
-// elastic and neohookean laws (the plastic state is FP64 per point)
-// PU pairs per unrolled iteration (1, 2 or 4); meshes of parallelepipeds
-// only (one adjugate per element, from the geometry table with GEO); the
 // elastic and neohookean laws (the plastic state is FP64 per point).  Every
 // FP32 operation is explicitly rounded (scalar __f*_rn or packed .rn), so
 // neither the points per iteration nor the register cap changes a result.
@@ -1236,13 +1406,42 @@ __device__ __forceinline__ void element_hex8sf_x2(int64_t le, int64_t e_begin, i
   element_hex8sf_x2_core<LAW, PU, GEO>(wu, le, e_begin, e_count, E, conn, pos, X, geo, mp, ps, re);
 }
 
+// The rows of the per-element tables (connectivity and slot positions, 8
+// each; with GEO the 10 of the adjugate table) that the warp pf elements
+// further on will read, prefetched into L2 by one lane per row: with pf one
+// wave of resident blocks, the blocks that follow find them there instead
+// of in DRAM.  L2 is the device's point of coherence, so the prefetch is
+// issued before the dependent-launch wait.
+template <bool GEO>
+__device__ __forceinline__ void prefetch_hex8_rows(int64_t pf, int64_t e_begin, int64_t e_count,
+                                                   int64_t E, const int32_t *conn,
+                                                   const int32_t *pos, const float *geo) {
+  const int lane = threadIdx.x & 31;
+  constexpr int kRows = GEO ? 26 : 16;
+  const int64_t w0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31) + pf;
+  if (lane >= kRows || w0 >= e_count) return;
+  const int64_t w1 = w0 + 32 < e_count ? w0 + 32 : e_count;
+  const char *b;
+  int64_t r, n;
+  if (lane < 8) {
+    b = (const char *)conn, r = lane, n = 8;
+  } else if (lane < 16) {
+    b = (const char *)pos, r = lane - 8, n = 8;
+  } else {
+    b = (const char *)geo, r = lane - 16, n = 10;
+  }
+  static_assert(sizeof(int32_t) == 4 && sizeof(float) == 4, "4-byte table entries");
+  prefetch_l2(b, b + n * E * 4, b + (r * E + e_begin + w0) * 4, b + (r * E + e_begin + w1) * 4);
+}
+
 template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf_x2(int64_t e_begin, int64_t e_count, int64_t E,
                                const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                                const double *__restrict__ X, const float *__restrict__ geo,
                                const double *__restrict__ u, MatParams mp, GroupArgs ps,
-                               float *__restrict__ re) {
+                               float *__restrict__ re, int64_t pf) {
+  if (pf > 0) prefetch_hex8_rows<GEO>(pf, e_begin, e_count, E, conn, pos, geo);
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;

@@ -89,8 +89,9 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
                                        const MatParams &mp, const GroupArgs &ps,
-                                       double *re, const ElemTuning &tn, cudaStream_t s) {
-  return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, tn, s);
+                                       double *re, const ElemTuning &tn, const QuadTable &tab,
+                                       cudaStream_t s) {
+  return element_forces_impl<double, double>(g, law, e0, ne, B, wJ, u, mp, ps, re, tn, &tab, s);
 }
 
 cudaError_t launch_persistent_fp64(const DevGeom &g, int law, int qu, const StepArgs &sa,

@@ -11,10 +11,13 @@ namespace {
 
 template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
 cudaError_t launch_x2(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
-                      const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
+                      const MatParams &mp, const GroupArgs &ps, float *re, int pf_waves,
+                      cudaStream_t s) {
   const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-  return launch_step(g.pdl, k_element_forces_hex8sf_x2<LAW, BLOCK, PU, MINB, GEO>, grid, BLOCK,
-                     s, e0, ne, g.E, g.conn, g.pos, g.X, g.geo, u, mp, ps, re);
+  constexpr auto kernel = k_element_forces_hex8sf_x2<LAW, BLOCK, PU, MINB, GEO>;
+  const int64_t pf = prefetch_distance<kernel>(pf_waves, BLOCK);
+  return launch_step(g.pdl, kernel, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X, g.geo, u,
+                     mp, ps, re, pf);
 }
 
 // 128 threads, registers capped for minb resident blocks per SM (1: the
@@ -22,9 +25,9 @@ cudaError_t launch_x2(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
 template <int LAW, bool GEO>
 cudaError_t dispatch_x2(int pu, int minb, const DevGeom &g, int64_t e0, int64_t ne,
                         const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
-                        cudaStream_t s) {
+                        int pf, cudaStream_t s) {
 #define AKB_X2(PU, MINB)                                                      \
-  if (pu == PU && minb == MINB) return launch_x2<LAW, 128, PU, MINB, GEO>(g, e0, ne, u, mp, ps, re, s);
+  if (pu == PU && minb == MINB) return launch_x2<LAW, 128, PU, MINB, GEO>(g, e0, ne, u, mp, ps, re, pf, s);
   AKB_X2(1, 1) AKB_X2(2, 1) AKB_X2(4, 1)
   AKB_X2(1, 4) AKB_X2(2, 4) AKB_X2(4, 4)
   AKB_X2(1, 5) AKB_X2(2, 5) AKB_X2(4, 5)
@@ -37,16 +40,16 @@ cudaError_t dispatch_x2(int pu, int minb, const DevGeom &g, int64_t e0, int64_t 
 cudaError_t launch_element_forces_hex8_x2(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                           const double *u, const MatParams &mp,
                                           const GroupArgs &ps, float *re, int points,
-                                          int minb, cudaStream_t s) {
+                                          int minb, int pf_waves, cudaStream_t s) {
   if (ne == 0) return cudaSuccess;
   if (!g.affine || law == LAW_PLASTIC) return cudaErrorInvalidValue;
   const int pu = points / 2;
   const bool geo = g.geo != nullptr;
   if (law == LAW_ELASTIC)
-    return geo ? dispatch_x2<LAW_ELASTIC, true>(pu, minb, g, e0, ne, u, mp, ps, re, s)
-               : dispatch_x2<LAW_ELASTIC, false>(pu, minb, g, e0, ne, u, mp, ps, re, s);
-  return geo ? dispatch_x2<LAW_NEOHOOKEAN, true>(pu, minb, g, e0, ne, u, mp, ps, re, s)
-             : dispatch_x2<LAW_NEOHOOKEAN, false>(pu, minb, g, e0, ne, u, mp, ps, re, s);
+    return geo ? dispatch_x2<LAW_ELASTIC, true>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s)
+               : dispatch_x2<LAW_ELASTIC, false>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s);
+  return geo ? dispatch_x2<LAW_NEOHOOKEAN, true>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s)
+             : dispatch_x2<LAW_NEOHOOKEAN, false>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s);
 }
 
 }  // namespace akb

@@ -112,9 +112,11 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
   // 2D elements and tetrahedra stream the FP32 copies of dN/dx (tetrahedra:
   // unless the recomputed form is selected, points_per_iteration 0)
   if (g.D == 2 || (g.et == ET_TET4 && fB && tn.qu != 0))
-    return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, tn, s);
+    return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, tn, &tab,
+                                              s);
   if (g.et == ET_HEX8 && (tn.qu & kPackedPoints))
-    return launch_element_forces_hex8_x2(g, law, e0, ne, u, mp, ps, re, tn.qu & 0xff, tn.minb, s);
+    return launch_element_forces_hex8_x2(g, law, e0, ne, u, mp, ps, re, tn.qu & 0xff, tn.minb,
+                                         tn.pf, s);
   if (g.et == ET_HEX8 && tn.qu > 0) {
     if (law == LAW_ELASTIC)
       dispatch_hex8sf_mesh<LAW_ELASTIC>(tn, g, e0, ne, u, mp, ps, re, s);

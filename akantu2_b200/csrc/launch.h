@@ -24,6 +24,15 @@ struct ElemTuning {
   int block = 128;
   int qu = 8;
   int minb = 1;
+  // packed hexahedron kernel and the one-thread-per-element kernel of
+  // tetrahedra and triangles: distance, in waves of resident blocks, at which
+  // each warp prefetches the per-element table rows of a later warp into L2
+  // (0: no prefetch); the results do not depend on it
+  int pf = 0;
+  // tetrahedra and triangles (one thread per element): 1 recomputes dN/dx and
+  // det J w from the coordinates by the precomputation's arithmetic instead
+  // of streaming the tables (the same numbers)
+  int rec = 0;
 };
 // points_per_iteration flag of the mixed hexahedron kernel: the points are
 // evaluated as packed FP32 pairs (2, 4 or 8 points per iteration)
@@ -81,7 +90,8 @@ cudaError_t launch_predict(const DevGeom &g, const uint8_t *blocked, const doubl
 cudaError_t launch_element_forces_fp64(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                        const double *B, const double *wJ, const double *u,
                                        const MatParams &mp, const GroupArgs &ps,
-                                       double *re, const ElemTuning &tn, cudaStream_t s);
+                                       double *re, const ElemTuning &tn, const QuadTable &tab,
+                                       cudaStream_t s);
 // mixed path: 3D elements recompute their shape derivatives in FP32 from g.X
 // and the table; 2D elements stream FP32 copies (fB, fwJ) of the precomputed
 // ones (their state traffic dominates, the recomputation would not pay)
@@ -97,7 +107,7 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
 cudaError_t launch_element_forces_hex8_x2(const DevGeom &g, int law, int64_t e0, int64_t ne,
                                           const double *u, const MatParams &mp,
                                           const GroupArgs &ps, float *re, int points,
-                                          int minb, cudaStream_t s);
+                                          int minb, int pf_waves, cudaStream_t s);
 // flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
 // the predictor of the next step reads u and writes u_next
 // node_block: threads per block of the node update (any multiple of 32 up to

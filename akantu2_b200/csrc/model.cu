@@ -613,7 +613,7 @@ int element_forces(akb_model *m, bool in_step) {
                                         (double *)m->dre, m->dgeo64, gr.tune, m->stream);
     else
       e = launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ, u, mp,
-                                     ps, (double *)m->dre, gr.tune, m->stream);
+                                     ps, (double *)m->dre, gr.tune, m->tab, m->stream);
     if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("element forces: ") + cudaGetErrorString(e));
   }
   return AKB_OK;
@@ -1209,6 +1209,19 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
       // the 512^2 square than uncapped
       if (m->et == AKB_TRIANGLE_6 && gr.law == LAW_PLASTIC)
         gr.tune = ElemTuning{128, 8, precision == AKB_PRECISION_MIXED ? 6 : 5};
+      // elastic and neohookean tetrahedra: the next wave's table rows
+      // prefetched into L2, and in FP64 the geometry recomputed from the
+      // coordinates instead of streaming 104 bytes of dN/dx and det J w per
+      // element (measured on the 256-cube batch in one sweep: element launch
+      // 9 % shorter mixed, 15 % shorter FP64; the recomputation alone made
+      // the mixed launch 35 % longer, at 80 instead of 56 registers: it stays
+      // off there).  Plastic triangles keep
+      // neither: one wave of their per-point state is most of L2, and the
+      // prefetch lengthened their launches by a fifth
+      if (m->et == AKB_TETRAHEDRON_4 && gr.law != LAW_PLASTIC) {
+        gr.tune.pf = 1;
+        gr.tune.rec = precision == AKB_PRECISION_FP64 ? 1 : 0;
+      }
       gr.nmat++;
       gr.e_count += mt.e_count;
       mt.group = (int)m->groups.size() - 1;
@@ -1332,14 +1345,17 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     // The elastic and neohookean laws then evaluate their points as packed
     // FP32 pairs, all 8 unrolled: measured on the 128^3 box, 0.149 instead
     // of 0.167 ms (elastic, registers capped for 5 blocks) and 0.178 instead
-    // of 0.196 ms (neohookean, capped for 4) against the best scalar shapes
+    // of 0.196 ms (neohookean, capped for 4) against the best scalar shapes;
+    // with the next wave's table rows prefetched into L2, 13 % shorter again
+    // (one sweep, both laws; two waves ahead gained less, three nothing)
     if (m->all_affine) {
       AKB_TRY(m->alloc(&m->dgeo, sizeof(float) * 10 * m->E));
       AKB_CUDA(launch_hex8_affine_geometry(g, m->dgeo, s));
       m->affine_kernel = 2;
       for (auto &gr : m->groups)
-        if (gr.law == LAW_ELASTIC) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 5};
-        else if (gr.law == LAW_NEOHOOKEAN) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 4};
+        if (gr.law == LAW_ELASTIC) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 5, 1};
+        else if (gr.law == LAW_NEOHOOKEAN)
+          gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 4, 1};
     }
   }
   if (m->fast64 && m->et == AKB_HEXAHEDRON_8) {
@@ -2068,6 +2084,14 @@ int akb_model_persistent_active(const akb_model *m, int *active) {
   return AKB_OK;
 }
 
+// the element kernels with an L2 prefetch of later warps' rows: the packed
+// hexahedron kernel, and the one-thread-per-element kernel of tetrahedra
+// and triangles (not its recomputed-geometry form, points_per_iteration 0)
+static bool prefetching_kernel(const akb_model *m, const Group &gr) {
+  if (m->et == AKB_HEXAHEDRON_8) return (gr.tune.qu & AKB_POINTS_PACKED) != 0;
+  return !(m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_MIXED && gr.tune.qu == 0);
+}
+
 int akb_model_autotune(akb_model *m, int repeats) {
   AKB_TRY(check_model(m, true));
   if (repeats < 1) return fail(AKB_EINVAL, "repeats must be >= 1");
@@ -2134,7 +2158,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
       return launch_element_forces_fp64_sf(g, gr.law, gr.e_begin, gr.e_count, m->u(), mp, ps,
                                            (double *)m->dre, m->dgeo64, tn, s);
     return launch_element_forces_fp64(g, gr.law, gr.e_begin, gr.e_count, m->dB, m->dwJ,
-                                      m->u(), mp, ps, (double *)m->dre, tn, s);
+                                      m->u(), mp, ps, (double *)m->dre, tn, m->tab, s);
   };
   for (auto &gr : m->groups) {
     if (rc != AKB_OK) break;
@@ -2151,8 +2175,12 @@ int akb_model_autotune(akb_model *m, int repeats) {
       if (q == 2) cand.insert(cand.end(), {{128, 2, 2}, {128, 2, 3}});
     } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED &&
         (gr.tune.qu & AKB_POINTS_PACKED)) {
+      // register cap and L2 prefetch distance
       const int q = gr.tune.qu;
-      cand = {{128, q, 1}, {128, q, 4}, {128, q, 5}};
+      cand = {{128, q, 4, gr.tune.pf}};
+      for (int minb : {1, 4, 5})
+        for (int pf : {0, 1, 2})
+          if (minb != 4 || pf != gr.tune.pf) cand.push_back({128, q, minb, pf});
     } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
       const int q = gr.tune.qu;
       cand = {{128, q, 1}, {128, q, 5}};
@@ -2165,6 +2193,22 @@ int akb_model_autotune(akb_model *m, int repeats) {
       cand = {{64, q, 1}, {128, q, 1}, {256, q, 1}};
       if (gr.law == LAW_PLASTIC && m->et != AKB_HEXAHEDRON_8)
         cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}});
+      // each with and without the L2 prefetch of the next wave's rows, and
+      // (tetrahedra and triangles) with the geometry streamed or recomputed
+      if (prefetching_kernel(m, gr)) {
+        const size_t n = cand.size();
+        for (size_t k = 0; k < n; ++k) {
+          cand[k].pf = 0;
+          cand[k].rec = 0;
+          for (int v = 1; v < 4; ++v) {
+            cand.push_back(cand[k]);
+            cand.back().pf = v & 1;
+            cand.back().rec = v >> 1;
+          }
+        }
+      }
+      // the shape in use first (kept on ties)
+      cand.insert(cand.begin(), gr.tune);
     }
     float best = 0.f;
     for (size_t k = 0; k < cand.size() && rc == AKB_OK; ++k) {
@@ -2428,7 +2472,12 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   bool found = false;
   for (auto &gr : m->groups)
     if (gr.law == law) {
-      gr.tune = ElemTuning{element_block, q, min_blocks};
+      // the L2 prefetch and the recomputed geometry carry over where the new
+      // shape's kernel has them
+      const ElemTuning old = gr.tune;
+      gr.tune = ElemTuning{element_block, q, min_blocks, old.pf, old.rec};
+      if (!prefetching_kernel(m, gr)) gr.tune.pf = 0;
+      if (!prefetching_kernel(m, gr) || m->et == AKB_HEXAHEDRON_8) gr.tune.rec = 0;
       found = true;
     }
   if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
@@ -2437,6 +2486,67 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
   return AKB_OK;
+}
+
+int akb_model_set_prefetch(akb_model *m, int law, int waves) {
+  AKB_TRY(check_model(m, true));
+  if (waves < 0 || waves > 4) return fail(AKB_EINVAL, "waves must be in [0, 4]");
+  bool found = false;
+  for (auto &gr : m->groups)
+    if (gr.law == law) {
+      if (!prefetching_kernel(m, gr) && waves != 0)
+        return fail(AKB_EINVAL, "the L2 prefetch is a setting of the packed hexahedron kernel "
+                                "(points_per_iteration with AKB_POINTS_PACKED) and of the "
+                                "tetrahedron and triangle kernels");
+      gr.tune.pf = waves;
+      found = true;
+    }
+  if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_set_recompute_geometry(akb_model *m, int law, int on) {
+  AKB_TRY(check_model(m, true));
+  if (on != 0 && on != 1) return fail(AKB_EINVAL, "on must be 0 or 1");
+  bool found = false;
+  for (auto &gr : m->groups)
+    if (gr.law == law) {
+      if (on && (m->et == AKB_HEXAHEDRON_8 || !prefetching_kernel(m, gr)))
+        return fail(AKB_EINVAL, "the recomputed geometry is a setting of the tetrahedron and "
+                                "triangle kernels that stream dN/dx");
+      gr.tune.rec = on;
+      found = true;
+    }
+  if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
+  AKB_CUDA(cudaStreamSynchronize(m->stream));
+  for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
+  m->graphs.clear();
+  return AKB_OK;
+}
+
+int akb_model_get_recompute_geometry(const akb_model *m, int law, int *on) {
+  if (!m) return fail(AKB_EINVAL, "null model");
+  if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  for (auto &gr : m->groups)
+    if (gr.law == law) {
+      if (on) *on = gr.tune.rec;
+      return AKB_OK;
+    }
+  return fail(AKB_EINVAL, "no material of this law in the model");
+}
+
+int akb_model_get_prefetch(const akb_model *m, int law, int *waves) {
+  if (!m) return fail(AKB_EINVAL, "null model");
+  if (!m->initialized) return fail(AKB_ESTATE, "initFull has not been called");
+  for (auto &gr : m->groups)
+    if (gr.law == law) {
+      if (waves) *waves = gr.tune.pf;
+      return AKB_OK;
+    }
+  return fail(AKB_EINVAL, "no material of this law in the model");
 }
 
 int akb_model_set_stream_priority(akb_model *m, int priority) {

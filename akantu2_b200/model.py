@@ -557,6 +557,30 @@ class SolidMechanicsModel:
                                                            int(points_per_iteration),
                                                            int(min_blocks), int(node_block)))
 
+    def setPrefetch(self, law, waves):
+        """L2 prefetch distance (waves of resident blocks, 0 = off) of the
+        packed hexahedron kernel of the law group `law`; results are
+        unchanged by it."""
+        _capi.check(_capi.lib().akb_model_set_prefetch(self._h, _LAW_IDS[law], int(waves)))
+
+    def getPrefetch(self, law):
+        w = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_prefetch(self._h, _LAW_IDS[law], ctypes.byref(w)))
+        return w.value
+
+    def setRecomputeGeometry(self, law, on=True):
+        """Tetrahedra and triangles: recompute dN/dx and det J w from the
+        coordinates every step (the precomputation's arithmetic) instead of
+        streaming the tables; results are unchanged by it."""
+        _capi.check(_capi.lib().akb_model_set_recompute_geometry(self._h, _LAW_IDS[law],
+                                                                 int(bool(on))))
+
+    def getRecomputeGeometry(self, law):
+        w = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_recompute_geometry(self._h, _LAW_IDS[law],
+                                                                 ctypes.byref(w)))
+        return bool(w.value)
+
     def setNodeShape(self, node_block, staged=False):
         """Threads per block of the node update, and the staged (shared
         memory) gather; results are unchanged by either."""

@@ -981,7 +981,10 @@ def run_serve(args):
             "requests_per_s": len(done) / span, "element_steps": work, "wall_s": wall,
             "batched_requests": int(sum(c.get("batched", False) for c in done)),
             "batching": not args.no_batching,
-            "failed": len(bad), "clocks": clk.summary(),
+            "failed": len(bad),
+            "failures": [{k: c.get(k) for k in ("status", "message", "nb_elements", "nb_steps",
+                                                "batched")} for c in bad[:5]],
+            "clocks": clk.summary(),
             "e2e": {"value": world * work / span, "unit": UNIT,
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "note": "each request uploads its mesh and initial state and reads its "

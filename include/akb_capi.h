@@ -362,6 +362,25 @@ int akb_model_autotune(akb_model *model, int repeats);
  * points are evaluated as packed FP32 pairs, 2, 4 or 8 points per iteration
  * (e.g. AKB_POINTS_PACKED | 2); a different FP32 evaluation order again */
 #define AKB_POINTS_PACKED 256
+/* L2 prefetch of the packed hexahedron kernel (points_per_iteration with
+ * AKB_POINTS_PACKED): each warp prefetches into L2 the connectivity,
+ * slot-position and adjugate rows that the warp `waves` waves of resident
+ * blocks further on reads (0: none; at most 4).  The results do not depend
+ * on it; the autotuner also tries 0, 1 and 2.  Captured step graphs are
+ * rebuilt.  No reference counterpart (a launch setting of this library). */
+int akb_model_set_prefetch(akb_model *model, int law, int waves);
+int akb_model_get_prefetch(const akb_model *model, int law, int *waves);
+/* geometry of the tetrahedron and triangle element kernels (one thread per
+ * element): 0 streams the precomputed dN/dx and det J w every step (FP32
+ * copies on the mixed path), 1 recomputes them from the nodal coordinates
+ * with the precomputation's own FP64 arithmetic (explicitly rounded, then
+ * rounded to FP32 on the mixed path), reading the coordinates instead of the
+ * tables.  The same numbers either way; the autotuner tries both.  Not for
+ * hexahedra, nor for the FP32 recomputed form of mixed tetrahedra
+ * (points_per_iteration 0).  No reference counterpart (a launch setting of
+ * this library; the reference precomputes, fe_engine_template_tmpl.hh). */
+int akb_model_set_recompute_geometry(akb_model *model, int law, int on);
+int akb_model_get_recompute_geometry(const akb_model *model, int law, int *on);
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,

@@ -370,6 +370,7 @@ def test_hex8_packed_pairs_are_the_default_and_bit_identical(mat):
     m = gpu_model(mesh, [mat], precision="mixed")
     b, q, mb, n = m.getLaunchShape(mat["type"])
     assert q == PACK | 8 and b == 128
+    assert m.getPrefetch(mat["type"]) == 1
     runs = []
     shapes = [(affine, PACK | pts, minb) for affine in (2, 1) for pts in (2, 4, 8)
               for minb in (1, 4, 5)]
@@ -403,6 +404,152 @@ def test_hex8_packed_pairs_accuracy(mat):
     assert np.linalg.norm(u - uo) / np.linalg.norm(uo) < 1e-5
     scalar = _run(mesh, mat, "mixed", v0, bl, 500, shape=(128, 2, 256, 5)).getDisplacement()
     assert np.linalg.norm(scalar - u) / np.linalg.norm(uo) < 1e-5
+
+
+def test_hex8_packed_l2_prefetch_is_bit_identical():
+    """the L2 prefetch distance of the packed kernel (0 = off, 1, 2 and 4
+    waves of resident blocks) changes no number: a box large enough for the
+    prefetching warps to exist, two law groups (the second starting past
+    element 0, a table offset), the default shapes and both register caps"""
+    mesh = akb.box_hex8(60)
+    E = mesh.getNbElement()
+    assert E > 2 * 148 * 5 * 128  # two waves of the 5-block cap
+    mat_of_elem = (np.arange(E) >= E // 3).astype(np.int32)
+    mats = [UNIT_ELASTIC, UNIT_NEOHOOKEAN]
+    v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
+    runs = []
+    for minb in (4, 5):
+        for pf in (0, 1, 2, 4):
+            m = gpu_model(mesh, mats, mat_of_elem=mat_of_elem, precision="mixed")
+            for law in ("elastic", "neohookean"):
+                m.setLaunchShape(law, 128, PACK | 8, 128, minb)
+                m.setPrefetch(law, pf)
+                assert m.getPrefetch(law) == pf
+            m.setNodal("velocity", v0)
+            m.setNodal("blocked_dofs", bl)
+            m.setTimeStep(0.8 * m.getStableTimeStep())
+            m.solveStep(130)
+            runs.append(((minb, pf), m.getDisplacement().copy(), m.getVelocity().copy(),
+                         m.getInternalForce().copy()))
+            del m
+    for other in runs[1:]:
+        for a, b_ in zip(runs[0][1:], other[1:]):
+            assert np.array_equal(a, b_), (runs[0][0], other[0])
+
+
+@pytest.mark.parametrize("case", ["tet4_elastic", "tet4_neohookean", "tri6_plastic3",
+                                  "tri6_plastic6", "tri6_elastic6"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_recomputed_geometry_and_prefetch_are_bit_identical(case, precision):
+    """tetrahedra and triangles: dN/dx and det J w recomputed from the
+    coordinates every step (the precomputation's explicitly rounded FP64
+    arithmetic) instead of streamed, and the L2 prefetch of later warps' rows,
+    on or off: every combination, with the plastic register caps, gives the
+    same nodal fields and plastic internals"""
+    etype, law = case.split("_")
+    qp_rule = 1 if law.endswith("6") else 0
+    law = law.rstrip("36")
+    if etype == "tet4":
+        mesh = akb.box_tet4(30)  # 162,000 elements: the prefetching warps exist
+        mat = dict(UNIT_ELASTIC if law == "elastic" else UNIT_NEOHOOKEAN)
+        v0 = sinusoidal_velocity(mesh.nodes, 0.02)
+        bl = blocked_face(mesh.nodes)
+    else:
+        mesh = akb.square_tri6(200)  # 80,000 elements
+        mat = dict(UNIT_PLASTIC, sigma_y=2e-3) if law == "plastic" else dict(UNIT_ELASTIC)
+        x = mesh.nodes
+        v0 = np.zeros_like(x)
+        v0[:, 0] = 0.05 * x[:, 0] * x[:, 1]
+        bl = np.zeros(x.shape, dtype=np.uint8)
+        bl[np.isclose(x[:, 0], 0.0)] = 1
+    name = LAW_NAME[mat["type"]]
+    shapes = [(128, 1, 0, 0), (128, 1, 1, 0), (128, 1, 0, 1), (128, 1, 1, 1), (64, 1, 1, 1),
+              (256, 1, 1, 1)]
+    if law == "plastic":
+        shapes += [(128, 5, 1, 1), (128, 6, 1, 1), (128, 6, 0, 1)]
+    runs = []
+    for block, minb, rec, pf in shapes:
+        m = gpu_model(mesh, [mat], precision=precision, qp_rule=qp_rule)
+        m.setLaunchShape(mat["type"], block, 8, 256, minb)
+        m.setRecomputeGeometry(mat["type"], rec)
+        m.setPrefetch(mat["type"], pf)
+        assert m.getRecomputeGeometry(mat["type"]) == bool(rec)
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.solveStep(120)
+        fields = [m.getDisplacement().copy(), m.getVelocity().copy(),
+                  m.getAcceleration().copy(), m.getInternalForce().copy()]
+        if name == "plastic":
+            mt = m.getMaterial(0)
+            fields += [mt.getStress().copy(), mt.getInternal("inelastic_strain")().copy()]
+        runs.append(((block, minb, rec, pf), fields))
+        del m
+    if name == "plastic":
+        assert np.max(np.abs(runs[0][1][5])) > 0, "the square must yield"
+    for other in runs[1:]:
+        for a, b_ in zip(runs[0][1], other[1]):
+            assert np.array_equal(a, b_), (runs[0][0], other[0])
+
+
+def test_recomputed_geometry_batch_is_bit_identical():
+    """a tetrahedral batch (per-instance materials and time steps) with the
+    geometry recomputed and the prefetch on, against the streamed tables"""
+    import bench
+    meshes, mats, vels, blocks = bench.batch_workload(12)
+    runs = []
+    for rec, pf in ((0, 0), (1, 1), (1, 0)):
+        for precision in ("fp64", "mixed"):
+            b = bench.build_batch(akb, meshes, mats, vels, blocks, precision)
+            b.setRecomputeGeometry("elastic", rec)
+            b.setPrefetch("elastic", pf)
+            b.solveStep(130)
+            runs.append(((rec, pf, precision), b.getDisplacement().copy(), b.getVelocity().copy()))
+            del b
+    for other in runs[2:]:
+        ref = runs[0] if other[0][2] == "fp64" else runs[1]
+        for a, b_ in zip(ref[1:], other[1:]):
+            assert np.array_equal(a, b_), (ref[0], other[0])
+
+
+def test_geometry_and_prefetch_defaults():
+    """elastic and neohookean tetrahedra prefetch the next wave's rows; in
+    FP64 they recompute the geometry; plastic triangles do neither"""
+    for precision in ("fp64", "mixed"):
+        t = gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision=precision)
+        assert t.getPrefetch("elastic") == 1
+        assert t.getRecomputeGeometry("elastic") == (precision == "fp64")
+        p = gpu_model(akb.square_tri6(3), [UNIT_PLASTIC], precision=precision)
+        law = UNIT_PLASTIC["type"]
+        assert p.getPrefetch(law) == 0 and not p.getRecomputeGeometry(law)
+
+
+def test_recomputed_geometry_setting_rules():
+    h = gpu_model(akb.box_hex8(3), [UNIT_ELASTIC], precision="fp64")
+    with pytest.raises(akb.AkbError):
+        h.setRecomputeGeometry("elastic", True)
+    t = gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision="mixed")
+    assert not t.getRecomputeGeometry("elastic")
+    t.setRecomputeGeometry("elastic", True)
+    t.setLaunchShape("elastic", 128, 0, 128, 1)  # the FP32 recomputed form
+    with pytest.raises(akb.AkbError):
+        t.setRecomputeGeometry("elastic", True)
+
+
+def test_l2_prefetch_setting_rules():
+    m = gpu_model(akb.box_hex8(3), [UNIT_NEOHOOKEAN], precision="mixed")
+    with pytest.raises(akb.AkbError):
+        m.setPrefetch("neohookean", 5)
+    with pytest.raises(akb.AkbError):
+        m.setPrefetch("elastic", 1)  # no such law group
+    m.setLaunchShape("neohookean", 128, 2, 128, 5)  # the scalar kernel: no prefetch
+    assert m.getPrefetch("neohookean") == 0
+    with pytest.raises(akb.AkbError):
+        m.setPrefetch("neohookean", 1)
+    m.setPrefetch("neohookean", 0)
+    f = gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision="fp64")
+    with pytest.raises(akb.AkbError):
+        f.setPrefetch("elastic", 1)
 
 
 def test_hex8_packed_shape_rules():
