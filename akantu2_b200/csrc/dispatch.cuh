@@ -167,19 +167,30 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
               if (law == LAW_PLASTIC && tn.minb > 1) {
                 constexpr auto k6 = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>;
                 constexpr auto k5 = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;
-                const int64_t pf = tn.minb >= 6 ? prefetch_distance<k6>(tn.pf, 128)
-                                                : prefetch_distance<k5>(tn.pf, 128);
-                return launch_step(g.pdl, tn.minb >= 6 ? k6 : k5, grid, 128, s, e0, ne, g.E,
-                                   g.conn, g.pos, g.X, *tab, u, mp, ps, re, pf);
+                constexpr auto k6p =
+                    k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6, true>;
+                constexpr auto k5p =
+                    k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5, true>;
+                const int64_t pf = tn.minb >= 6 ? prefetch_distance<k6p>(tn.pf, 128)
+                                                : prefetch_distance<k5p>(tn.pf, 128);
+                auto kern = tn.minb >= 6 ? (pf > 0 ? k6p : k6) : (pf > 0 ? k5p : k5);
+                return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, g.X,
+                                   *tab, u, mp, ps, re, pf);
               }
             }
             constexpr auto ke = k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>;
             constexpr auto kn = k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>;
             constexpr auto kp = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;
-            const int64_t pf = law == LAW_ELASTIC      ? prefetch_distance<ke>(tn.pf, BLOCK)
-                               : law == LAW_NEOHOOKEAN ? prefetch_distance<kn>(tn.pf, BLOCK)
-                                                       : prefetch_distance<kp>(tn.pf, BLOCK);
-            auto kern = law == LAW_ELASTIC ? ke : law == LAW_NEOHOOKEAN ? kn : kp;
+            constexpr auto kep = k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK, 1, true>;
+            constexpr auto knp =
+                k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK, 1, true>;
+            constexpr auto kpp = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK, 1, true>;
+            const int64_t pf = law == LAW_ELASTIC      ? prefetch_distance<kep>(tn.pf, BLOCK)
+                               : law == LAW_NEOHOOKEAN ? prefetch_distance<knp>(tn.pf, BLOCK)
+                                                       : prefetch_distance<kpp>(tn.pf, BLOCK);
+            auto kern = law == LAW_ELASTIC      ? (pf > 0 ? kep : ke)
+                        : law == LAW_NEOHOOKEAN ? (pf > 0 ? knp : kn)
+                                                : (pf > 0 ? kpp : kp);
             return launch_step(g.pdl, kern, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X,
                                *tab, u, mp, ps, re, pf);
           }
@@ -189,19 +200,27 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
           if (law == LAW_PLASTIC && tn.minb > 1) {
             constexpr auto k6 = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>;
             constexpr auto k5 = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;
-            const int64_t pf = tn.minb >= 6 ? prefetch_distance<k6>(tn.pf, 128)
-                                            : prefetch_distance<k5>(tn.pf, 128);
-            return launch_step(g.pdl, tn.minb >= 6 ? k6 : k5, grid, 128, s, e0, ne, g.E, g.conn,
-                               g.pos, B, wJ, u, mp, ps, re, pf);
+            constexpr auto k6p = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6, true>;
+            constexpr auto k5p = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5, true>;
+            const int64_t pf = tn.minb >= 6 ? prefetch_distance<k6p>(tn.pf, 128)
+                                            : prefetch_distance<k5p>(tn.pf, 128);
+            auto kern = tn.minb >= 6 ? (pf > 0 ? k6p : k6) : (pf > 0 ? k5p : k5);
+            return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
+                               mp, ps, re, pf);
           }
         }
         constexpr auto ke = k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>;
         constexpr auto kn = k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>;
         constexpr auto kp = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;
-        const int64_t pf = law == LAW_ELASTIC      ? prefetch_distance<ke>(tn.pf, BLOCK)
-                           : law == LAW_NEOHOOKEAN ? prefetch_distance<kn>(tn.pf, BLOCK)
-                                                   : prefetch_distance<kp>(tn.pf, BLOCK);
-        auto kern = law == LAW_ELASTIC ? ke : law == LAW_NEOHOOKEAN ? kn : kp;
+        constexpr auto kep = k_element_forces_pe<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK, 1, true>;
+        constexpr auto knp = k_element_forces_pe<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK, 1, true>;
+        constexpr auto kpp = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK, 1, true>;
+        const int64_t pf = law == LAW_ELASTIC      ? prefetch_distance<kep>(tn.pf, BLOCK)
+                           : law == LAW_NEOHOOKEAN ? prefetch_distance<knp>(tn.pf, BLOCK)
+                                                   : prefetch_distance<kpp>(tn.pf, BLOCK);
+        auto kern = law == LAW_ELASTIC      ? (pf > 0 ? kep : ke)
+                    : law == LAW_NEOHOOKEAN ? (pf > 0 ? knp : kn)
+                                            : (pf > 0 ? kpp : kp);
         return launch_step(g.pdl, kern, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
                            mp, ps, re, pf);
       });

@@ -505,7 +505,8 @@ __global__ void k_predict(int64_t N, const uint8_t *__restrict__ blocked,
 // u B^T, the law, and the weighted elemental force t = (B^T sigma or
 // B(grad u)^T S) * wJ_q.  Two launch shapes use it:
 //  - k_element_forces_pe: one thread per element, loop over q, accumulate t
-//    in registers in increasing q (all mixed kernels; FP64 tet4 / tri6);
+//    in registers in increasing q (mixed tetrahedra and triangles; FP64 tet4
+//    / tri6);
 //  - k_element_forces_pq: one thread per (element, q) for FP64 hexahedra,
 //    32 elements per warp (lanes = elements, warps = quadrature points), the
 //    per-q contributions summed in increasing q through shared memory laid
@@ -788,14 +789,18 @@ __device__ __forceinline__ void prefetch_pe_rows(int64_t pf, int64_t e_begin, in
 // BLOCK: threads (= elements) per block, one of the launch shapes the
 // autotuner chooses from; MINB > 1 caps the registers for that many resident
 // blocks per SM (plastic groups, whose state loads want more warps in flight)
-template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK, int MINB = 1>
+// PF: the instance with the L2 prefetch (pf > 0); the one without has no
+// prefetch code at all
+template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK, int MINB = 1,
+          bool PF = false>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_pe(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const T *__restrict__ B, const T *__restrict__ wJ,
                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
                         RT *__restrict__ re, int64_t pf) {
-  if (pf > 0) prefetch_pe_rows<D, NN, NQ, LAW, T>(pf, e_begin, e_count, E, conn, pos, B, wJ, ps);
+  if constexpr (PF)
+    prefetch_pe_rows<D, NN, NQ, LAW, T>(pf, e_begin, e_count, E, conn, pos, B, wJ, ps);
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
@@ -805,14 +810,15 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 
 // k_element_forces_pe with the geometry recomputed from the coordinates
 // (element_pe REC): the same numbers, no dN/dx and det J w streamed
-template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK, int MINB = 1>
+template <int D, int NN, int NQ, int LAW, class T, class RT, int BLOCK, int MINB = 1,
+          bool PF = false>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_pr(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                         const double *__restrict__ X, const QuadTable tab,
                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
                         RT *__restrict__ re, int64_t pf) {
-  if (pf > 0)
+  if constexpr (PF)
     prefetch_pe_rows<D, NN, NQ, LAW, T>(pf, e_begin, e_count, E, conn, pos, nullptr, nullptr, ps);
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
@@ -1434,14 +1440,16 @@ __device__ __forceinline__ void prefetch_hex8_rows(int64_t pf, int64_t e_begin, 
   prefetch_l2(b, b + n * E * 4, b + (r * E + e_begin + w0) * 4, b + (r * E + e_begin + w1) * 4);
 }
 
-template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
+// PF: the instance with the prefetch (pf > 0); the one without has no
+// prefetch code at all
+template <int LAW, int BLOCK, int PU, int MINB, bool GEO, bool PF = false>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_element_forces_hex8sf_x2(int64_t e_begin, int64_t e_count, int64_t E,
                                const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
                                const double *__restrict__ X, const float *__restrict__ geo,
                                const double *__restrict__ u, MatParams mp, GroupArgs ps,
                                float *__restrict__ re, int64_t pf) {
-  if (pf > 0) prefetch_hex8_rows<GEO>(pf, e_begin, e_count, E, conn, pos, geo);
+  if constexpr (PF) prefetch_hex8_rows<GEO>(pf, e_begin, e_count, E, conn, pos, geo);
   pdl_begin();
   const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
   if (le >= e_count || !element_active(ps, le)) return;
@@ -1467,19 +1475,30 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                                        re);
 }
 
-// FP64, one thread per (element, q): blockDim = 32 * NQ, warp w = point q
-template <int D, int NN, int NQ, int LAW>
+// One thread per (element, q): blockDim = 32 * NQ, warp w = point q, lane =
+// element; FP64 hexahedra.  The warps gather the element's nodal
+// displacements into shared memory (FP64; with an FP32 element type T they
+// are taken relative to node 0 there, as the per-element kernel does), each
+// thread evaluates its point, and the points' contributions are summed in
+// increasing q through shared memory laid out [q][component][lane] (free of
+// bank conflicts): the per-element kernel's sums, bit for bit.  One thread
+// per point of plastic triangles, in either precision, was measured slower
+// than the per-element kernel (0.152 against 0.091 ms mixed, 0.181 against
+// 0.126 ms FP64 on the 512^2 square: a third of the elements in flight per
+// SM) and is not offered.
+template <int D, int NN, int NQ, int LAW, class T = double, class RT = double>
 __global__ void __launch_bounds__(32 * NQ)
     k_element_forces_pq(int64_t e_begin, int64_t e_count, int64_t E,
                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
-                        const double *__restrict__ B, const double *__restrict__ wJ,
+                        const T *__restrict__ B, const T *__restrict__ wJ,
                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
-                        double *__restrict__ re) {
+                        RT *__restrict__ re) {
   pdl_begin();
   constexpr int ND = NN * D;
+  constexpr bool REL = !std::is_same<T, double>::value;  // relative gather in FP32
   constexpr int CH = (ND + NQ - 1) / NQ;  // components reduced per round and thread
   __shared__ double us[ND][32];
-  __shared__ double red[NQ][NQ][32];
+  __shared__ T red[NQ][NQ][32];
   const int lane = threadIdx.x & 31;
   const int q = threadIdx.x >> 5;
   const int64_t le = (int64_t)blockIdx.x * 32 + lane;
@@ -1494,17 +1513,20 @@ __global__ void __launch_bounds__(32 * NQ)
     }
   }
   __syncthreads();
-  double t[ND];
+  T t[ND];
   if (active) {
-    double ue[ND], b[ND];
+    T ue[ND], b[ND];
 #pragma unroll
     for (int c = 0; c < ND; ++c) {
-      ue[c] = us[c][lane];
+      if constexpr (REL)
+        ue[c] = (T)(us[c][lane] - us[c % D][lane]);
+      else
+        ue[c] = us[c][lane];
       b[c] = B[(int64_t)(q * ND + c) * E + e];
     }
-    const double w = wJ[(int64_t)q * E + e];
+    const T w = wJ[(int64_t)q * E + e];
     const MatParams mpe = group_params(mp, ps, le);
-    element_law<D, NN, LAW, double, false>(ue, b, w, mpe, ps, e_count, le, q, t);
+    element_law<D, NN, LAW, T, REL>(ue, b, w, mpe, ps, e_count, le, q, t);
   }
   // sum over q in increasing order, NQ components per round
 #pragma unroll
@@ -1519,11 +1541,11 @@ __global__ void __launch_bounds__(32 * NQ)
     __syncthreads();
     const int c = round * NQ + q;
     if (active && c < ND) {
-      double s = red[0][q][lane];
+      T s = red[0][q][lane];
 #pragma unroll
       for (int qq = 1; qq < NQ; ++qq) s = s + red[qq][q][lane];
       const int a = c / D;
-      re[(int64_t)pos[(int64_t)a * E + e] * SlotStride<D, double>::value + (c - a * D)] = s;
+      re[(int64_t)pos[(int64_t)a * E + e] * SlotStride<D, RT>::value + (c - a * D)] = (RT)s;
     }
     __syncthreads();
   }
@@ -1568,13 +1590,64 @@ __device__ __forceinline__ void accumulate_slot(const double *rv, double *acc, d
   }
 }
 
+// the node update after the gather: f_int = acc, residual, solve, corrector
+// and predictor of node i (its nodal state is loaded after the gather: loaded
+// before it, with the slots, the update was measured slower, 0.120 against
+// 0.107 ms on the 128^3 hexahedral box, at 66 instead of 50 registers)
 template <int D>
 __device__ __forceinline__ void node_apply(int64_t i, const double *acc, const double *fext,
                                            const double *mass, const uint8_t *blocked,
                                            double *fint, double *a, double *v, const double *u,
                                            double *u_next, double dt, const int32_t *node_inst,
                                            const double *inst_dt, int flags,
-                                           unsigned int *status);
+                                           unsigned int *status) {
+  if (flags & NU_FINT) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) fint[i * D + c] = acc[c];
+  }
+  if (!(flags & NU_CORRECT)) return;
+  const double m = mass[i];
+  const uint8_t bl = blocked[i];
+  dt = node_dt(dt, node_inst, inst_dt, i);
+  const double hdt = __dmul_rn(.5, dt);
+  bool bad = false;
+  // explicit round-to-nearest products and sums: the nodal state arithmetic is
+  // the same (no contraction) in the FP64 and the mixed translation units,
+  // and the fused predictor equals k_predict
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const int64_t k = i * D + c;
+    const bool free_dof = !((bl >> c) & 1);
+    const double ak = a[k];
+    double vk = v[k];
+    if (free_dof) vk = __dadd_rn(vk, __dmul_rn(dt, ak));  // predicted velocity (newmark-beta.cc:69)
+    double r;
+    if (flags & NU_FEXT_ZERO) {
+      r = acc[c];
+    } else {
+      r = __dadd_rn(0., __dmul_rn(1., fext[k]));
+      r = __dadd_rn(r, __dmul_rn(1., acc[c]));
+    }
+    const double ma = __dadd_rn(0., __dmul_rn(-1., ak));
+    r = __dadd_rn(r, __dmul_rn(m, ma));
+    double an = ak;
+    if (free_dof) {
+      const double x = __dmul_rn(1., __ddiv_rn(r, m));
+      vk = __dadd_rn(vk, __dmul_rn(hdt, x));
+      an = __dadd_rn(ak, __dmul_rn(1., x));
+      v[k] = vk;
+      a[k] = an;
+      bad |= !isfinite(an);
+    }
+    if (flags & NU_PREDICT) {
+      const double uk = u[k];
+      u_next[k] = free_dof ? __dadd_rn(uk, __dadd_rn(__dmul_rn(dt, vk),
+                                                     __dmul_rn(hdt, __dmul_rn(dt, an))))
+                           : uk;
+    }
+  }
+  if (bad) atomicOr(status, 1u);
+}
 
 // 32 bytes of the slot array as one load (sm_100 256-bit global load): two
 // float4 slots of 3D or four float2 slots of 2D; the address 32-byte aligned
@@ -1693,65 +1766,11 @@ __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
                 status);
 }
 
-// the node update after the gather: f_int = acc, residual, solve, corrector
-// and predictor of node i
-template <int D>
-__device__ __forceinline__ void node_apply(int64_t i, const double *acc, const double *fext,
-                                           const double *mass, const uint8_t *blocked,
-                                           double *fint, double *a, double *v, const double *u,
-                                           double *u_next, double dt, const int32_t *node_inst,
-                                           const double *inst_dt, int flags,
-                                           unsigned int *status) {
-  if (flags & NU_FINT) {
-#pragma unroll
-    for (int c = 0; c < D; ++c) fint[i * D + c] = acc[c];
-  }
-  if (!(flags & NU_CORRECT)) return;
-  const double m = mass[i];
-  const uint8_t bl = blocked[i];
-  dt = node_dt(dt, node_inst, inst_dt, i);
-  const double hdt = __dmul_rn(.5, dt);
-  bool bad = false;
-#pragma unroll
-  // explicit round-to-nearest products and sums: the nodal state arithmetic is
-  // the same (no contraction) in the FP64 and the mixed translation units,
-  // and the fused predictor equals k_predict
-  for (int c = 0; c < D; ++c) {
-    const int64_t k = i * D + c;
-    const bool free_dof = !((bl >> c) & 1);
-    const double ak = a[k];
-    double vk = v[k];
-    if (free_dof) vk = __dadd_rn(vk, __dmul_rn(dt, ak));  // predicted velocity (newmark-beta.cc:69)
-    double r;
-    if (flags & NU_FEXT_ZERO) {
-      r = acc[c];
-    } else {
-      r = __dadd_rn(0., __dmul_rn(1., fext[k]));
-      r = __dadd_rn(r, __dmul_rn(1., acc[c]));
-    }
-    const double ma = __dadd_rn(0., __dmul_rn(-1., ak));
-    r = __dadd_rn(r, __dmul_rn(m, ma));
-    double an = ak;
-    if (free_dof) {
-      const double x = __dmul_rn(1., __ddiv_rn(r, m));
-      vk = __dadd_rn(vk, __dmul_rn(hdt, x));
-      an = __dadd_rn(ak, __dmul_rn(1., x));
-      v[k] = vk;
-      a[k] = an;
-      bad |= !isfinite(an);
-    }
-    if (flags & NU_PREDICT) {
-      const double uk = u[k];
-      u_next[k] = free_dof ? __dadd_rn(uk, __dadd_rn(__dmul_rn(dt, vk),
-                                                     __dmul_rn(hdt, __dmul_rn(dt, an))))
-                           : uk;
-    }
-  }
-  if (bad) atomicOr(status, 1u);
-}
 
+// launched with up to 1024 threads per block (the autotuner's candidates):
+// at most 64 registers
 template <int D, class RT, bool KAHAN, bool WIDE = false>
-__global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
+__global__ void __launch_bounds__(1024) k_node_update(int64_t N, const int32_t *__restrict__ ptr,
                               const RT *__restrict__ re, const double *__restrict__ fext,
                               const double *__restrict__ mass,
                               const uint8_t *__restrict__ blocked, double *__restrict__ fint,
@@ -1773,7 +1792,7 @@ __global__ void k_node_update(int64_t N, const int32_t *__restrict__ ptr,
 // buffer) takes the value of the other one (u_next), which holds the
 // instance's last displacement, so that both buffers hold it from then on
 template <int D, class RT, bool KAHAN>
-__global__ void k_node_update_retire(int64_t N, const int32_t *__restrict__ ptr,
+__global__ void __launch_bounds__(1024) k_node_update_retire(int64_t N, const int32_t *__restrict__ ptr,
                                      const RT *__restrict__ re, const double *__restrict__ fext,
                                      const double *__restrict__ mass,
                                      const uint8_t *__restrict__ blocked,

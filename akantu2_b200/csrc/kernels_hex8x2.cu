@@ -14,10 +14,11 @@ cudaError_t launch_x2(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
                       const MatParams &mp, const GroupArgs &ps, float *re, int pf_waves,
                       cudaStream_t s) {
   const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
-  constexpr auto kernel = k_element_forces_hex8sf_x2<LAW, BLOCK, PU, MINB, GEO>;
-  const int64_t pf = prefetch_distance<kernel>(pf_waves, BLOCK);
-  return launch_step(g.pdl, kernel, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X, g.geo, u,
-                     mp, ps, re, pf);
+  constexpr auto k0 = k_element_forces_hex8sf_x2<LAW, BLOCK, PU, MINB, GEO, false>;
+  constexpr auto k1 = k_element_forces_hex8sf_x2<LAW, BLOCK, PU, MINB, GEO, true>;
+  const int64_t pf = prefetch_distance<k1>(pf_waves, BLOCK);
+  return launch_step(g.pdl, pf > 0 ? k1 : k0, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X,
+                     g.geo, u, mp, ps, re, pf);
 }
 
 // 128 threads, registers capped for minb resident blocks per SM (1: the

@@ -1209,18 +1209,18 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
       // the 512^2 square than uncapped
       if (m->et == AKB_TRIANGLE_6 && gr.law == LAW_PLASTIC)
         gr.tune = ElemTuning{128, 8, precision == AKB_PRECISION_MIXED ? 6 : 5};
-      // elastic and neohookean tetrahedra: the next wave's table rows
-      // prefetched into L2, and in FP64 the geometry recomputed from the
-      // coordinates instead of streaming 104 bytes of dN/dx and det J w per
-      // element (measured on the 256-cube batch in one sweep: element launch
-      // 9 % shorter mixed, 15 % shorter FP64; the recomputation alone made
-      // the mixed launch 35 % longer, at 80 instead of 56 registers: it stays
-      // off there).  Plastic triangles keep
-      // neither: one wave of their per-point state is most of L2, and the
-      // prefetch lengthened their launches by a fifth
-      if (m->et == AKB_TETRAHEDRON_4 && gr.law != LAW_PLASTIC) {
+      // FP64 elastic and neohookean tetrahedra: the geometry recomputed from
+      // the coordinates instead of streaming 104 bytes of dN/dx and det J w
+      // per element, and the next wave's table rows prefetched into L2
+      // (256-cube batch, element launch 0.835 against 0.993 ms).  Mixed
+      // tetrahedra keep the streamed FP32 copies without prefetch (0.455 ms;
+      // prefetching 0.476, recomputing 0.538: 80 instead of 56 registers),
+      // and so do triangles (the prefetch made their launches a third longer:
+      // one wave of the plastic per-point state is most of L2)
+      if (m->et == AKB_TETRAHEDRON_4 && gr.law != LAW_PLASTIC &&
+          precision == AKB_PRECISION_FP64) {
         gr.tune.pf = 1;
-        gr.tune.rec = precision == AKB_PRECISION_FP64 ? 1 : 0;
+        gr.tune.rec = 1;
       }
       gr.nmat++;
       gr.e_count += mt.e_count;
@@ -1345,17 +1345,17 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
     // The elastic and neohookean laws then evaluate their points as packed
     // FP32 pairs, all 8 unrolled: measured on the 128^3 box, 0.149 instead
     // of 0.167 ms (elastic, registers capped for 5 blocks) and 0.178 instead
-    // of 0.196 ms (neohookean, capped for 4) against the best scalar shapes;
-    // with the next wave's table rows prefetched into L2, 13 % shorter again
-    // (one sweep, both laws; two waves ahead gained less, three nothing)
+    // of 0.196 ms (neohookean, capped for 4) against the best scalar shapes.
+    // The L2 prefetch of the next wave's table rows made both launches
+    // longer (0.218 against 0.184 ms neohookean, 0.171 against 0.147
+    // elastic): off
     if (m->all_affine) {
       AKB_TRY(m->alloc(&m->dgeo, sizeof(float) * 10 * m->E));
       AKB_CUDA(launch_hex8_affine_geometry(g, m->dgeo, s));
       m->affine_kernel = 2;
       for (auto &gr : m->groups)
-        if (gr.law == LAW_ELASTIC) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 5, 1};
-        else if (gr.law == LAW_NEOHOOKEAN)
-          gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 4, 1};
+        if (gr.law == LAW_ELASTIC) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 5};
+        else if (gr.law == LAW_NEOHOOKEAN) gr.tune = ElemTuning{128, AKB_POINTS_PACKED | 8, 4};
     }
   }
   if (m->fast64 && m->et == AKB_HEXAHEDRON_8) {
@@ -2195,7 +2195,9 @@ int akb_model_autotune(akb_model *m, int repeats) {
         cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}});
       // each with and without the L2 prefetch of the next wave's rows, and
       // (tetrahedra and triangles) with the geometry streamed or recomputed
-      if (prefetching_kernel(m, gr)) {
+      Group probe = gr;
+      probe.tune = cand[0];
+      if (prefetching_kernel(m, probe)) {
         const size_t n = cand.size();
         for (size_t k = 0; k < n; ++k) {
           cand[k].pf = 0;

@@ -9,8 +9,9 @@
 // requests, within the memory budget) and prepares one batch model for all of
 // them (akb_batch_create: one element launch and one node launch per step
 // advance every instance, each with its own material, time step and step
-// count).  Larger requests, and every request when batching is off, get a
-// model of their own.
+// count).  Larger requests, a request with no queued partner of its kind
+// (under light load: a model of its own builds and steps faster than a batch
+// of one), and every request when batching is off, get a model of their own.
 //
 // The scheduler thread keeps every running unit (batch or single solve) two
 // chunks ahead: a chunk is a solve_step of up to chunk_steps steps (100-step
@@ -513,14 +514,28 @@ void akb_server::builder_loop() {
           cv_work.wait_for(lock, std::chrono::milliseconds(2));
           continue;
         }
-        reserved += c->est_bytes;
-        const double t = now();
-        for (Job *jj : c->jobs) {
-          jj->phase = BUILDING;
-          jj->t_admit = t;
+        if (c->jobs.size() == 1 &&
+            (reserved == 0 || reserved + c->jobs[0]->est_bytes <= cfg.device_bytes)) {
+          // nothing to share a batch with (the load is light): a model of its
+          // own, which builds and steps faster than a batch of one
+          j = c->jobs[0];
+          delete c;
+          c = nullptr;
+          reserved += j->est_bytes;
+          active++;
+          n_building++;
+          j->phase = BUILDING;
+          j->t_admit = now();
+        } else {
+          reserved += c->est_bytes;
+          const double t = now();
+          for (Job *jj : c->jobs) {
+            jj->phase = BUILDING;
+            jj->t_admit = t;
+          }
+          active += (int)c->jobs.size();
+          n_building += (int64_t)c->jobs.size();
         }
-        active += (int)c->jobs.size();
-        n_building += (int64_t)c->jobs.size();
       } else {
         j = queue.front();
         queue.pop_front();

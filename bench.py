@@ -88,6 +88,8 @@ def parse():
     p.add_argument("--mode", default="replicas", choices=["replicas", "partitioned"],
                    help="N > 1: independent replicas (weak scaling), or one mesh split over "
                         "the ranks with a halo exchange every step (strong scaling)")
+    p.add_argument("--qp-rule", type=int, default=0,
+                   help="tri6: quadrature rule (0: the reference's default, 3 points; 1: 6 points)")
     p.add_argument("--parts", type=int, default=0,
                    help="partitioned, one process: subdomains advanced on the one GPU")
     return p.parse_args()
@@ -209,11 +211,15 @@ def serve_mesh(kind, cells):
 
 # algorithmic bytes (formula of the specification, per element-step), and the
 # element-force kernel's own share
-def algorithmic_bytes(config, mesh, precision):
+def quadrature_points(config, qp_rule=0):
+    return {"hex8": 8, "tet": 1, "tri6": 6 if qp_rule else 3, "batch": 1}[config]
+
+
+def algorithmic_bytes(config, mesh, precision, qp_rule=0):
     E, N = mesh.getNbElement(), mesh.getNbNodes()
     n = mesh.connectivity.shape[1]
     d = mesh.spatial_dimension
-    Q = {"hex8": 8, "tet": 1, "tri6": 3, "batch": 1}[config]
+    Q = quadrature_points(config, qp_rule)
     s_e = 8 if precision.startswith("fp64") else 4
     S = (3 * d * d + 1) * 8 if config == "tri6" else 0
     elem = E * (4 * n + Q * (d * n + 1) * s_e + 2 * Q * S)
@@ -454,6 +460,8 @@ def run_ours(args, rep=None, emit=True, extra=False):
     _capi.check(_capi.lib().akb_set_device(local))
 
     mesh, mat, desc = workload(args.config, args.cells)
+    if args.config == "tri6":
+        desc += f", {quadrature_points('tri6', args.qp_rule)} Gauss points per triangle"
     v0, blocked = initial_state(args.config, mesh)
     E = mesh.getNbElement()
     results = {}
@@ -462,6 +470,8 @@ def run_ours(args, rep=None, emit=True, extra=False):
     for prec in precisions:
         m = akb.SolidMechanicsModel(mesh)
         m.addMaterial(mat["type"], **{k: v for k, v in mat.items() if k != "type"})
+        if args.config == "tri6" and args.qp_rule:
+            m.setQuadratureRule(args.qp_rule)
         m.initFull(akb._explicit_lumped_mass, precision=prec)
         m.setNodal("velocity", v0)
         m.setNodal("blocked_dofs", blocked)
@@ -485,7 +495,7 @@ def run_ours(args, rep=None, emit=True, extra=False):
         ms = max_over_ranks(ms)
         nprof = min(args.steps, 20)
         tot, phases = m.profileSteps(nprof)
-        step_b, kern_b = algorithmic_bytes(args.config, mesh, prec)
+        step_b, kern_b = algorithmic_bytes(args.config, mesh, prec, args.qp_rule)
         elem_ms = phases[1] / nprof
         peak, peak_kind = read_peaks()
         results[prec] = {
@@ -495,6 +505,7 @@ def run_ours(args, rep=None, emit=True, extra=False):
                                   "element_forces": phases[1] / nprof,
                                   "node_update": phases[2] / nprof},
             "roofline": roofline_entry(kern_b, elem_ms, peak, peak_kind,
+                                       None if args.qp_rule else
                                        read_traffic(args.config, prec)),
             "roofline_step": {"bytes_per_element_step": step_b / E,
                               "achieved": step_b / (ms / args.steps / 1e3) / 1e9,
@@ -562,7 +573,7 @@ def run_ours(args, rep=None, emit=True, extra=False):
                            "fp64_fast": "FP64, hexahedra by the sum-factorised kernel with "
                                         "contraction (within 1e-12 of the CPU path)"},
             "config": {"workload": desc, "elements": E, "nodes": mesh.getNbNodes(),
-                       "quadrature_points": {"hex8": 8, "tet": 1, "tri6": 3}[args.config],
+                       "quadrature_points": quadrature_points(args.config, args.qp_rule),
                        "precision": precisions[0], "parallelism": f"replicas x{world}",
                        "l2": head["l2"]},
             "e2e": head.get("e2e"), "roofline": head["roofline"],
@@ -1100,11 +1111,16 @@ def run_default_with_extras(args):
     rep = Replicas("nccl")
     line = run_ours(args, rep=rep, emit=False)
     extras = {}
-    for config, runner in (("tri6", run_ours), ("batch", run_batch)):
+    # the plastic square with the reference's default 3-point rule and with
+    # the 6-point rule its configuration names
+    for name, config, rule, runner in (("tri6", "tri6", 0, run_ours),
+                                       ("tri6_6points", "tri6", 1, run_ours),
+                                       ("batch", "batch", 0, run_batch)):
         a = copy.copy(args)
         a.config, a.steps, a.no_cpu, a.accuracy_steps, a.no_e2e_fp64 = config, 20, True, 0, True
         a.precisions = "mixed,fp64"
-        extras[config] = compact(runner(a, rep=rep, emit=False, extra=True))
+        a.qp_rule = rule
+        extras[name] = compact(runner(a, rep=rep, emit=False, extra=True))
     line["configs"] = extras
     print(json.dumps(line), flush=True)
     rep.close()

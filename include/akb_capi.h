@@ -522,7 +522,8 @@ int akb_model_debug_write_index(akb_model *model, int which, int64_t position, i
  * rule, law and precision (limits above) becomes one batch model whose
  * instances each stop after their own step count
  * (akb_batch_set_instance_steps) and are reported as soon as they end, while
- * the batch goes on; larger solves get a model of their own.  Builder threads
+ * the batch goes on; larger solves, and a solve with no queued partner of its
+ * kind, get a model of their own.  Builder threads
  * prepare the models (tables, lumped mass, stable time steps, step graphs),
  * the scheduler thread advances every resident batch and solve chunk by chunk
  * on its own stream, so that their kernels overlap on the device; arrivals are

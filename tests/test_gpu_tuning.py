@@ -370,7 +370,7 @@ def test_hex8_packed_pairs_are_the_default_and_bit_identical(mat):
     m = gpu_model(mesh, [mat], precision="mixed")
     b, q, mb, n = m.getLaunchShape(mat["type"])
     assert q == PACK | 8 and b == 128
-    assert m.getPrefetch(mat["type"]) == 1
+    assert m.getPrefetch(mat["type"]) == 0
     runs = []
     shapes = [(affine, PACK | pts, minb) for affine in (2, 1) for pts in (2, 4, 8)
               for minb in (1, 4, 5)]
@@ -463,14 +463,14 @@ def test_recomputed_geometry_and_prefetch_are_bit_identical(case, precision):
         bl = np.zeros(x.shape, dtype=np.uint8)
         bl[np.isclose(x[:, 0], 0.0)] = 1
     name = LAW_NAME[mat["type"]]
-    shapes = [(128, 1, 0, 0), (128, 1, 1, 0), (128, 1, 0, 1), (128, 1, 1, 1), (64, 1, 1, 1),
-              (256, 1, 1, 1)]
+    shapes = [(128, 8, 1, 0, 0), (128, 8, 1, 1, 0), (128, 8, 1, 0, 1), (128, 8, 1, 1, 1),
+              (64, 8, 1, 1, 1), (256, 8, 1, 1, 1)]
     if law == "plastic":
-        shapes += [(128, 5, 1, 1), (128, 6, 1, 1), (128, 6, 0, 1)]
+        shapes += [(128, 8, 5, 1, 1), (128, 8, 6, 1, 1), (128, 8, 6, 0, 1)]
     runs = []
-    for block, minb, rec, pf in shapes:
+    for block, q, minb, rec, pf in shapes:
         m = gpu_model(mesh, [mat], precision=precision, qp_rule=qp_rule)
-        m.setLaunchShape(mat["type"], block, 8, 256, minb)
+        m.setLaunchShape(mat["type"], block, q, 256, minb)
         m.setRecomputeGeometry(mat["type"], rec)
         m.setPrefetch(mat["type"], pf)
         assert m.getRecomputeGeometry(mat["type"]) == bool(rec)
@@ -483,7 +483,7 @@ def test_recomputed_geometry_and_prefetch_are_bit_identical(case, precision):
         if name == "plastic":
             mt = m.getMaterial(0)
             fields += [mt.getStress().copy(), mt.getInternal("inelastic_strain")().copy()]
-        runs.append(((block, minb, rec, pf), fields))
+        runs.append(((block, q, minb, rec, pf), fields))
         del m
     if name == "plastic":
         assert np.max(np.abs(runs[0][1][5])) > 0, "the square must yield"
@@ -513,11 +513,12 @@ def test_recomputed_geometry_batch_is_bit_identical():
 
 
 def test_geometry_and_prefetch_defaults():
-    """elastic and neohookean tetrahedra prefetch the next wave's rows; in
-    FP64 they recompute the geometry; plastic triangles do neither"""
+    """FP64 elastic and neohookean tetrahedra recompute the geometry and
+    prefetch the next wave's rows; mixed tetrahedra and plastic triangles do
+    neither"""
     for precision in ("fp64", "mixed"):
         t = gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision=precision)
-        assert t.getPrefetch("elastic") == 1
+        assert t.getPrefetch("elastic") == (1 if precision == "fp64" else 0)
         assert t.getRecomputeGeometry("elastic") == (precision == "fp64")
         p = gpu_model(akb.square_tri6(3), [UNIT_PLASTIC], precision=precision)
         law = UNIT_PLASTIC["type"]
@@ -547,7 +548,7 @@ def test_l2_prefetch_setting_rules():
     with pytest.raises(akb.AkbError):
         m.setPrefetch("neohookean", 1)
     m.setPrefetch("neohookean", 0)
-    f = gpu_model(akb.box_tet4(3), [UNIT_ELASTIC], precision="fp64")
+    f = gpu_model(akb.box_hex8(3), [UNIT_ELASTIC], precision="fp64")  # per-point kernel
     with pytest.raises(akb.AkbError):
         f.setPrefetch("elastic", 1)
 
