@@ -50,7 +50,14 @@ def test_results_same_alone_and_in_the_mix(batching):
     bit, whether it ran as an instance of a batch (requests of one kind
     sharing a batch model, each stopping after its own step count) or alone"""
     rng = np.random.default_rng(3)
-    reqs = [_request(k, rng) for k in range(14)]
+    # seven pairs of one kind each (element type, law, precision) arriving
+    # together: a solve with no queued partner of its kind runs alone
+    reqs = []
+    for k in range(14):
+        r = _request(k // 2, rng)
+        if k % 2:
+            r["material"], r["precision"] = reqs[-1]["material"], reqs[-1]["precision"]
+        reqs.append(r)
     srv = akb.Server(max_active=5, chunk_steps=100, builders=3, batching=batching)
     ids = {}
     for k, r in enumerate(reqs):
