@@ -69,7 +69,10 @@ struct QuadTable {
 // elemental-force slots: the D components of one (element, node) force at
 // slot p.  FP32 3D slots are padded to one 16-byte float4 (one vector store
 // in the element kernel, one vector load in the node gather); the others
-// hold D values without padding.
+// hold D values without padding.  Unpadded 12-byte slots (three scalar
+// stores, the node's range read in aligned 16-byte chunks) were measured: the
+// element launches took 58 % (128^3 hexahedra) and 55 % (tet batch) longer,
+// for a 5 % shorter hexahedral node update and a 15 % longer batch one.
 template <int D, class RT> struct SlotStride {
   static constexpr int value = (D == 3 && sizeof(RT) == 4) ? 4 : D;
 };
