@@ -1464,87 +1464,6 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   element_hex8sf_x2<LAW, PU, GEO>(le, e_begin, e_count, E, conn, pos, X, geo, u, mp, ps, re);
 }
 
-// 4-byte asynchronous copy global -> shared (cp.async, no register holds the
-// value), and its group commit / wait
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Persistent form of the packed hexahedron kernel: a grid of resident blocks
-// walks the elements with the grid as stride.  Each thread copies the
-// connectivity, slot positions and (GEO) adjugate entries of its next element
-// into shared memory with cp.async while it computes the current one, so the
-// only global latency left on an element's path is its displacement gather;
-// the same arithmetic as k_element_forces_hex8sf_x2, bit for bit.  Each
-// thread reads back only what it copied itself (after its own wait_group), so
-// no barrier is needed; a buffer is refilled only after the loads of the
-// element that used it have been consumed (program order, "memory" clobbers).
-template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
-__global__ void __launch_bounds__(BLOCK, MINB)
-    k_element_forces_hex8sf_x2s(int64_t e_begin, int64_t e_count, int64_t E,
-                                const int32_t *__restrict__ conn,
-                                const int32_t *__restrict__ pos, const double *__restrict__ X,
-                                const float *__restrict__ geo, const double *__restrict__ u,
-                                MatParams mp, GroupArgs ps, float *__restrict__ re) {
-  constexpr int NG = GEO ? 10 : 1;
-  __shared__ int32_t s_cn[2][8][BLOCK];
-  __shared__ int32_t s_pv[2][8][BLOCK];
-  __shared__ float s_gv[2][NG][BLOCK];
-  const int t = threadIdx.x;
-  const int64_t stride = (int64_t)gridDim.x * BLOCK;
-  auto stage = [&](int b, int64_t l) {
-    const int64_t e = e_begin + l;
-#pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      cp_async4(&s_cn[b][a][t], conn + (int64_t)a * E + e);
-      cp_async4(&s_pv[b][a][t], pos + (int64_t)a * E + e);
-    }
-    if constexpr (GEO) {
-#pragma unroll
-      for (int k = 0; k < 10; ++k) cp_async4(&s_gv[b][k][t], geo + (int64_t)k * E + e);
-    }
-  };
-  // the tables do not change between steps: the first copies may overlap
-  // the previous kernel (dependent launch)
-  int64_t le = (int64_t)blockIdx.x * BLOCK + t;
-  if (le < e_count) stage(0, le);
-  cp_async_commit();
-  pdl_begin();
-  constexpr int lex[8] = {0, 1, 3, 2, 4, 5, 7, 6};
-  int b = 0;
-  for (; le < e_count; le += stride, b ^= 1) {
-    const int64_t ln = le + stride;
-    if (ln < e_count) stage(b ^ 1, ln);
-    cp_async_commit();
-    cp_async_wait<1>();  // the current element's copies have landed
-    if (!element_active(ps, le)) continue;
-    if (!element_indices_ok<8>(ps, conn, pos, E, e_begin + le)) continue;
-    float wu[8][3];
-    double u0[3];
-#pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const int64_t node = s_cn[b][a][t];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const double uu = u[node * 3 + i];
-        if (a == 0) u0[i] = uu;
-        wu[lex[a]][i] = (float)(uu - u0[i]);
-      }
-    }
-    element_hex8sf_x2_core<LAW, PU, GEO>(wu, le, e_count, &s_cn[b][0][t], BLOCK,
-                                         &s_pv[b][0][t], BLOCK, X, &s_gv[b][0][t], BLOCK, mp,
-                                         ps, re);
-  }
-  cp_async_wait<0>();
-}
-
 // MINB: blocks per SM the register allocation must allow (1: the compiler's
 // choice)
 template <int LAW, int BLOCK, int QU, int MINB, bool AFF = false, bool GEO = false,

@@ -21,35 +21,12 @@ cudaError_t launch_x2(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
                      g.geo, u, mp, ps, re, pf);
 }
 
-// the persistent form: one wave of resident blocks (queried once per
-// instance), or fewer when the group is smaller
-template <int LAW, int BLOCK, int PU, int MINB, bool GEO>
-cudaError_t launch_x2s(const DevGeom &g, int64_t e0, int64_t ne, const double *u,
-                       const MatParams &mp, const GroupArgs &ps, float *re, cudaStream_t s) {
-  constexpr auto kernel = k_element_forces_hex8sf_x2s<LAW, BLOCK, PU, MINB, GEO>;
-  static std::atomic<int64_t> wave{-1};
-  int64_t w = wave.load(std::memory_order_relaxed);
-  if (w < 0) wave.store(w = wave_elements(kernel, BLOCK) / BLOCK, std::memory_order_relaxed);
-  if (w <= 0) return cudaErrorInvalidConfiguration;
-  const int64_t want = (ne + BLOCK - 1) / BLOCK;
-  const unsigned grid = (unsigned)(want < w ? want : w);
-  return launch_step(g.pdl, kernel, grid, BLOCK, s, e0, ne, g.E, g.conn, g.pos, g.X, g.geo, u,
-                     mp, ps, re);
-}
-
 // 128 threads, registers capped for minb resident blocks per SM (1: the
-// compiler's choice); pu pairs per unrolled iteration; staged: the
-// persistent form with the tables copied ahead into shared memory
+// compiler's choice); pu pairs per unrolled iteration
 template <int LAW, bool GEO>
-cudaError_t dispatch_x2(int pu, int minb, bool staged, const DevGeom &g, int64_t e0, int64_t ne,
+cudaError_t dispatch_x2(int pu, int minb, const DevGeom &g, int64_t e0, int64_t ne,
                         const double *u, const MatParams &mp, const GroupArgs &ps, float *re,
                         int pf, cudaStream_t s) {
-  if (staged) {
-    if (pu == 4 && minb == 4) return launch_x2s<LAW, 128, 4, 4, GEO>(g, e0, ne, u, mp, ps, re, s);
-    if (pu == 4 && minb == 5) return launch_x2s<LAW, 128, 4, 5, GEO>(g, e0, ne, u, mp, ps, re, s);
-    if (pu == 4 && minb == 3) return launch_x2s<LAW, 128, 4, 3, GEO>(g, e0, ne, u, mp, ps, re, s);
-    return cudaErrorInvalidValue;
-  }
 #define AKB_X2(PU, MINB)                                                      \
   if (pu == PU && minb == MINB) return launch_x2<LAW, 128, PU, MINB, GEO>(g, e0, ne, u, mp, ps, re, pf, s);
   AKB_X2(1, 1) AKB_X2(2, 1) AKB_X2(4, 1)
@@ -65,17 +42,15 @@ cudaError_t launch_element_forces_hex8_x2(const DevGeom &g, int law, int64_t e0,
                                           const double *u, const MatParams &mp,
                                           const GroupArgs &ps, float *re, int points,
                                           int minb, int pf_waves, cudaStream_t s) {
-  const bool staged = (points & kStagedTables) != 0;
-  points &= 0xff;
   if (ne == 0) return cudaSuccess;
   if (!g.affine || law == LAW_PLASTIC) return cudaErrorInvalidValue;
   const int pu = points / 2;
   const bool geo = g.geo != nullptr;
   if (law == LAW_ELASTIC)
-    return geo ? dispatch_x2<LAW_ELASTIC, true>(pu, minb, staged, g, e0, ne, u, mp, ps, re, pf_waves, s)
-               : dispatch_x2<LAW_ELASTIC, false>(pu, minb, staged, g, e0, ne, u, mp, ps, re, pf_waves, s);
-  return geo ? dispatch_x2<LAW_NEOHOOKEAN, true>(pu, minb, staged, g, e0, ne, u, mp, ps, re, pf_waves, s)
-             : dispatch_x2<LAW_NEOHOOKEAN, false>(pu, minb, staged, g, e0, ne, u, mp, ps, re, pf_waves, s);
+    return geo ? dispatch_x2<LAW_ELASTIC, true>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s)
+               : dispatch_x2<LAW_ELASTIC, false>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s);
+  return geo ? dispatch_x2<LAW_NEOHOOKEAN, true>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s)
+             : dispatch_x2<LAW_NEOHOOKEAN, false>(pu, minb, g, e0, ne, u, mp, ps, re, pf_waves, s);
 }
 
 }  // namespace akb

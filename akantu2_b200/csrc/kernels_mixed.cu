@@ -115,8 +115,7 @@ cudaError_t launch_element_forces_mixed(const DevGeom &g, int law, int64_t e0, i
     return element_forces_impl<float, float>(g, law, e0, ne, fB, fwJ, u, mp, ps, re, tn, &tab,
                                               s);
   if (g.et == ET_HEX8 && (tn.qu & kPackedPoints))
-    return launch_element_forces_hex8_x2(g, law, e0, ne, u, mp, ps, re,
-                                         tn.qu & (0xff | kStagedTables), tn.minb,
+    return launch_element_forces_hex8_x2(g, law, e0, ne, u, mp, ps, re, tn.qu & 0xff, tn.minb,
                                          tn.pf, s);
   if (g.et == ET_HEX8 && tn.qu > 0) {
     if (law == LAW_ELASTIC)

@@ -37,9 +37,6 @@ struct ElemTuning {
 // points_per_iteration flag of the mixed hexahedron kernel: the points are
 // evaluated as packed FP32 pairs (2, 4 or 8 points per iteration)
 constexpr int kPackedPoints = 256;
-// with kPackedPoints: the persistent form, each element's tables copied into
-// shared memory while the previous one is computed (8 points, 3 to 5 blocks)
-constexpr int kStagedTables = 512;
 
 // device view of the mesh, internal element order
 struct DevGeom {

@@ -2088,8 +2088,7 @@ int akb_model_persistent_active(const akb_model *m, int *active) {
 // hexahedron kernel, and the one-thread-per-element kernel of tetrahedra
 // and triangles (not its recomputed-geometry form, points_per_iteration 0)
 static bool prefetching_kernel(const akb_model *m, const Group &gr) {
-  if (m->et == AKB_HEXAHEDRON_8)
-    return (gr.tune.qu & AKB_POINTS_PACKED) && !(gr.tune.qu & AKB_POINTS_STAGED);
+  if (m->et == AKB_HEXAHEDRON_8) return (gr.tune.qu & AKB_POINTS_PACKED) != 0;
   return !(m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_MIXED && gr.tune.qu == 0);
 }
 
@@ -2176,14 +2175,11 @@ int akb_model_autotune(akb_model *m, int repeats) {
       if (q == 2) cand.insert(cand.end(), {{128, 2, 2}, {128, 2, 3}});
     } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED &&
         (gr.tune.qu & AKB_POINTS_PACKED)) {
-      // register cap and L2 prefetch distance, and with 8 points the staged
-      // persistent form
-      const int q = gr.tune.qu & ~AKB_POINTS_STAGED;
+      // register cap and L2 prefetch distance
+      const int q = gr.tune.qu;
       cand = {gr.tune};
       for (int minb : {1, 4, 5})
         for (int pf : {0, 1, 2}) cand.push_back({128, q, minb, pf});
-      if ((q & 0xff) == 8)
-        for (int minb : {3, 4, 5}) cand.push_back({128, q | AKB_POINTS_STAGED, minb, 0});
     } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
       const int q = gr.tune.qu;
       cand = {{128, q, 1}, {128, q, 5}};
@@ -2445,24 +2441,17 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
   }
   const bool sf = m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED;
   const bool tet_mixed = m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_MIXED;
-  if (q & AKB_POINTS_STAGED && !(q & AKB_POINTS_PACKED))
-    return fail(AKB_EINVAL, "AKB_POINTS_STAGED is a form of the packed kernel (AKB_POINTS_PACKED)");
   if (q & AKB_POINTS_PACKED) {
     // packed FP32 pairs: mixed hexahedra of a mesh of parallelepipeds with the
     // kernel compiled for them, elastic or neohookean, 128 threads
-    const int pts = q & ~(AKB_POINTS_PACKED | AKB_POINTS_STAGED);
+    const int pts = q & ~AKB_POINTS_PACKED;
     if (!sf || !m->affine_kernel || law == LAW_PLASTIC)
       return fail(AKB_EINVAL, "packed points need mixed hexahedra of a mesh of parallelepipeds "
                               "(affine kernel on), elastic or neohookean");
     if (pts != 2 && pts != 4 && pts != 8)
       return fail(AKB_EINVAL, "packed points per iteration must be 2, 4 or 8");
-    if (q & AKB_POINTS_STAGED) {
-      if (pts != 8 || element_block != 128 || min_blocks < 3 || min_blocks > 5)
-        return fail(AKB_EINVAL, "the staged packed form runs 8 points with 128 threads and "
-                                "min_blocks 3, 4 or 5");
-    } else if (element_block != 128 || (min_blocks != 1 && min_blocks != 4 && min_blocks != 5)) {
+    if (element_block != 128 || (min_blocks != 1 && min_blocks != 4 && min_blocks != 5))
       return fail(AKB_EINVAL, "packed points run with 128 threads and min_blocks 1, 4 or 5");
-    }
   } else if (!sf && q != 8 && !(tet_mixed && q == 0))
     return fail(AKB_EINVAL, "points_per_iteration is 8 (or 0 for the recomputed form of mixed "
                             "tetrahedra and hexahedra)");

@@ -362,12 +362,6 @@ int akb_model_autotune(akb_model *model, int repeats);
  * points are evaluated as packed FP32 pairs, 2, 4 or 8 points per iteration
  * (e.g. AKB_POINTS_PACKED | 2); a different FP32 evaluation order again */
 #define AKB_POINTS_PACKED 256
-/* flag of points_per_iteration, with AKB_POINTS_PACKED | 8 and min_blocks
- * 3, 4 or 5: the persistent form of the packed kernel (a grid of resident
- * blocks; each element's connectivity, slot positions and adjugate entries
- * copied into shared memory while the previous element is computed).  The
- * same numbers as the packed form. */
-#define AKB_POINTS_STAGED 512
 /* L2 prefetch of the packed hexahedron kernel (points_per_iteration with
  * AKB_POINTS_PACKED): each warp prefetches into L2 the connectivity,
  * slot-position and adjugate rows that the warp `waves` waves of resident

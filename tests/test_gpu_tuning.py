@@ -537,74 +537,6 @@ def test_recomputed_geometry_setting_rules():
         t.setRecomputeGeometry("elastic", True)
 
 
-STAGED = 512  # AKB_POINTS_STAGED
-
-
-def test_hex8_staged_packed_form_is_bit_identical():
-    """the persistent form of the packed kernel (tables copied into shared
-    memory one element ahead, a grid of resident blocks striding over the
-    elements) gives the packed form's numbers: a box of several waves, two
-    law groups (the second starting past element 0), every register cap"""
-    mesh = akb.box_hex8(60)
-    E = mesh.getNbElement()
-    mat_of_elem = (np.arange(E) >= E // 3).astype(np.int32)
-    mats = [UNIT_ELASTIC, UNIT_NEOHOOKEAN]
-    v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
-    runs = []
-    for q, minb in ((PACK | 8, 4), (PACK | STAGED | 8, 3), (PACK | STAGED | 8, 4),
-                    (PACK | STAGED | 8, 5)):
-        m = gpu_model(mesh, mats, mat_of_elem=mat_of_elem, precision="mixed")
-        for law in ("elastic", "neohookean"):
-            m.setLaunchShape(law, 128, q, 128, minb)
-            assert m.getLaunchShape(law)[1] == q
-        m.setNodal("velocity", v0)
-        m.setNodal("blocked_dofs", bl)
-        m.setTimeStep(0.8 * m.getStableTimeStep())
-        m.solveStep(130)
-        runs.append(((q, minb), m.getDisplacement().copy(), m.getVelocity().copy(),
-                     m.getInternalForce().copy()))
-        del m
-    for other in runs[1:]:
-        for a, b_ in zip(runs[0][1:], other[1:]):
-            assert np.array_equal(a, b_), (runs[0][0], other[0])
-
-
-def test_hex8_staged_packed_form_stopping_batch():
-    """a batch of hexahedral boxes whose instances stop after their own step
-    counts: the staged form skips the stopped instances' elements exactly as
-    the packed form does"""
-    meshes = [akb.box_hex8(n) for n in (6, 9, 4)]
-    runs = []
-    for q, minb in ((PACK | 8, 4), (PACK | STAGED | 8, 4)):
-        b = akb.BatchModel(meshes)
-        b.addMaterial("neohookean", name="a", rho=1.0, E=1.0, nu=0.3)
-        b.setInstanceMaterials(np.zeros(len(meshes), dtype=np.int32))
-        b.initFull(akb._explicit_lumped_mass, precision="mixed")
-        b.setNodal("velocity", np.concatenate([sinusoidal_velocity(m.nodes, 0.02) for m in meshes]))
-        b.setNodal("blocked_dofs", np.concatenate([blocked_face(m.nodes) for m in meshes]))
-        b.setTimeSteps(0.8 * b.getStableTimeSteps())
-        b.setLaunchShape("neohookean", 128, q, 128, minb)
-        b.setInstanceSteps([60, 150, 110])
-        b.solveStep(150)
-        runs.append((b.getDisplacement().copy(), b.getVelocity().copy()))
-        del b
-    for a, b_ in zip(runs[0], runs[1]):
-        assert np.array_equal(a, b_)
-
-
-def test_staged_form_setting_rules():
-    m = gpu_model(akb.box_hex8(3), [UNIT_NEOHOOKEAN], precision="mixed")
-    with pytest.raises(akb.AkbError):
-        m.setLaunchShape("neohookean", 128, STAGED | 8, 128, 4)  # not packed
-    with pytest.raises(akb.AkbError):
-        m.setLaunchShape("neohookean", 128, PACK | STAGED | 2, 128, 4)  # 8 points only
-    with pytest.raises(akb.AkbError):
-        m.setLaunchShape("neohookean", 128, PACK | STAGED | 8, 128, 1)
-    m.setLaunchShape("neohookean", 128, PACK | STAGED | 8, 128, 4)
-    with pytest.raises(akb.AkbError):
-        m.setPrefetch("neohookean", 1)  # no prefetch in the staged form
-
-
 def test_l2_prefetch_setting_rules():
     m = gpu_model(akb.box_hex8(3), [UNIT_NEOHOOKEAN], precision="mixed")
     with pytest.raises(akb.AkbError):
