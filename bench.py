@@ -268,7 +268,11 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the raw samples (the line carries their summary); AKB_CLOCKS_DIR
+        # keeps them somewhere else than the system's temporary directory
+        import tempfile
+        self.path = os.path.join(os.environ.get("AKB_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"akb_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
