@@ -2175,11 +2175,14 @@ int akb_model_autotune(akb_model *m, int repeats) {
       if (q == 2) cand.insert(cand.end(), {{128, 2, 2}, {128, 2, 3}});
     } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED &&
         (gr.tune.qu & AKB_POINTS_PACKED)) {
-      // register cap and L2 prefetch distance
-      const int q = gr.tune.qu;
+      // points per iteration and register cap (every FP32 operation of the
+      // packed form is explicitly rounded: the same numbers in every shape),
+      // and the L2 prefetch of the shape in use
       cand = {gr.tune};
-      for (int minb : {1, 4, 5})
-        for (int pf : {0, 1, 2}) cand.push_back({128, q, minb, pf});
+      for (int pts : {2, 4, 8})
+        for (int minb : {1, 4, 5}) cand.push_back({128, AKB_POINTS_PACKED | pts, minb, 0});
+      cand.push_back(gr.tune);
+      cand.back().pf = gr.tune.pf ? 0 : 1;
     } else if (m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_MIXED) {
       const int q = gr.tune.qu;
       cand = {{128, q, 1}, {128, q, 5}};

@@ -340,14 +340,16 @@ int akb_model_set_persistent_wait_test(akb_model *model, unsigned int spin_limit
 int akb_model_persistent_active(const akb_model *model, int *active);
 /* autotuner: times the candidate launch shapes of each law group's
  * element-force kernel (threads per block 64 / 128 / 256; for mixed
- * hexahedra also a register cap for 5 resident blocks of 128) and of the node
+ * hexahedra also a register cap for 5 resident blocks of 128; the L2
+ * prefetch; for tetrahedra and triangles the recomputed geometry) and of the node
  * update (direct gather with 128 .. 1024 threads per block, staged gather
  * with 128 .. 512) on the model's current state,
  * `repeats` launches each, and keeps the fastest.  The candidates compute
  * the same numbers, so the choice changes only the timing; the model's state
  * is not modified.  Captured step graphs are rebuilt.  The points per
  * iteration of the mixed hexahedron kernel (set_launch_shape) are not tuned:
- * they change the FP32 rounding. */
+ * they change the FP32 rounding; those of its packed form
+ * (AKB_POINTS_PACKED), whose every operation is explicitly rounded, are. */
 int akb_model_autotune(akb_model *model, int repeats);
 /* the launch shape in use for the law group of `law` (0 elastic, 1
  * neohookean, 2 plastic); points_per_iteration is 8 except for mixed
