@@ -196,7 +196,14 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
           }
         }
         if constexpr (BLOCK == 128) {
-          // plastic groups: 128 threads with registers capped for 5 or 6 blocks per SM
+          // plastic groups: 128 threads with registers capped for 5 to 8 blocks per
+          // SM (7 and 8 without the prefetch)
+          if (law == LAW_PLASTIC && tn.minb >= 7 && tn.pf == 0) {
+            auto kern = tn.minb >= 8 ? k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 8>
+                                     : k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 7>;
+            return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
+                               mp, ps, re, (int64_t)0);
+          }
           if (law == LAW_PLASTIC && tn.minb > 1) {
             constexpr auto k6 = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 6>;
             constexpr auto k5 = k_element_forces_pe<D, NN, NQ, LAW_PLASTIC, T, RT, 128, 5>;

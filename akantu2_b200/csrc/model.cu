@@ -2194,7 +2194,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
       const int q = gr.tune.qu;
       cand = {{64, q, 1}, {128, q, 1}, {256, q, 1}};
       if (gr.law == LAW_PLASTIC && m->et != AKB_HEXAHEDRON_8)
-        cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}});
+        cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}, {128, q, 7}, {128, q, 8}});
       // each with and without the L2 prefetch of the next wave's rows, and
       // (tetrahedra and triangles) with the geometry streamed or recomputed
       Group probe = gr;
@@ -2204,6 +2204,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
         for (size_t k = 0; k < n; ++k) {
           cand[k].pf = 0;
           cand[k].rec = 0;
+          if (cand[k].minb >= 7) continue;  // the 7- and 8-block caps: streamed, no prefetch
           for (int v = 1; v < 4; ++v) {
             cand.push_back(cand[k]);
             cand.back().pf = v & 1;
@@ -2466,10 +2467,10 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
                          (min_blocks == 5 || (min_blocks == 4 && q == 2) ||
                           (min_blocks == 6 && (q == 1 || q == 2)));
   const bool capped_plastic = m->et != AKB_HEXAHEDRON_8 && law == LAW_PLASTIC &&
-                              (min_blocks == 5 || min_blocks == 6) && element_block == 128;
+                              min_blocks >= 5 && min_blocks <= 8 && element_block == 128;
   if (min_blocks != 1 && !capped_sf && !capped_plastic && !(q & AKB_POINTS_PACKED))
     return fail(AKB_EINVAL, "min_blocks is 1; 5 (or 4 with 2 points per iteration, 6 with 1 or "
-                            "2) for the 128-thread mixed hexahedron kernel; 5 or 6 for "
+                            "2) for the 128-thread mixed hexahedron kernel; 5 to 8 for "
                             "128-thread plastic tetrahedra and triangles");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");

@@ -290,7 +290,7 @@ def test_dependent_launch_batch_is_bit_identical():
     ("_tetrahedron_4", "fp64"), ("_tetrahedron_4", "mixed"), ("_triangle_6", "fp64"),
     ("_triangle_6", "mixed")])
 def test_plastic_register_caps_are_bit_identical(etype, precision):
-    """128-thread plastic kernels with registers capped for 5 or 6 resident
+    """128-thread plastic kernels with registers capped for 5 to 8 resident
     blocks per SM compute the same numbers"""
     mesh = {"_triangle_6": lambda: akb.square_tri6(8), "_tetrahedron_4": lambda: akb.box_tet4(6)}[etype]()
     d = mesh.spatial_dimension
@@ -299,9 +299,11 @@ def test_plastic_register_caps_are_bit_identical(etype, precision):
         np.stack([0.05 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
     bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
     runs = []
-    for mb in (1, 5, 6):
+    for mb in (1, 5, 6, 7, 8):
         m = gpu_model(mesh, [mat], precision=precision)
         m.setLaunchShape(mat["type"], 128, 8, 128, mb)
+        m.setPrefetch(mat["type"], 0)
+        m.setRecomputeGeometry(mat["type"], False)
         assert m.getLaunchShape(mat["type"])[2] == mb
         m.setNodal("velocity", v0)
         m.setNodal("blocked_dofs", bl)
