@@ -26,6 +26,8 @@ PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FAST = 0, 1, 2
  BLOCKED_DOFS, CURRENT_POSITION, PREVIOUS_DISPLACEMENT, DISPLACEMENT_INCREMENT) = range(10)
 (GRAD_U, STRESS, PIOLA_KIRCHHOFF_2, INELASTIC_STRAIN, ISO_HARDENING,
  PLASTIC_ENERGY, EIGEN_GRAD_U) = range(7)
+# AKB_ASYNC_READS_IN_FLIGHT: asynchronous reads that can be waited on one by one
+ASYNC_READS_IN_FLIGHT = 4
 
 
 class AkbError(RuntimeError):
@@ -138,6 +140,8 @@ def lib():
         "akb_model_get_prefetch": (c_int, [vp, c_int, ctypes.POINTER(c_int)]),
         "akb_model_set_recompute_geometry": (c_int, [vp, c_int, c_int]),
         "akb_model_get_recompute_geometry": (c_int, [vp, c_int, ctypes.POINTER(c_int)]),
+        "akb_model_set_streamed_points": (c_int, [vp, c_int, c_int]),
+        "akb_model_get_streamed_points": (c_int, [vp, c_int, ctypes.POINTER(c_int)]),
         "akb_model_stream": (c_int, [vp, pp]),
         "akb_model_device_bytes": (c_int, [vp, ctypes.POINTER(i64)]),
         "akb_estimate_device_bytes": (c_int, [c_int, c_int, i64, i64, c_int, c_int,

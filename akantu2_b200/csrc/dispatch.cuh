@@ -21,17 +21,19 @@ inline unsigned grid_for(int64_t n, int threads = kThreads) {
 // a step kernel launch, with the programmatic-serialization attribute when pdl
 // is set (the kernel then overlaps the end of the previous kernel on the
 // stream; it waits for it in pdl_begin)
+// (smem: bytes of dynamic shared memory)
 template <class... KArgs, class... Args>
-inline cudaError_t launch_step(bool pdl, void (*kernel)(KArgs...), unsigned grid,
-                               unsigned block, cudaStream_t s, Args... args) {
+inline cudaError_t launch_step_smem(bool pdl, void (*kernel)(KArgs...), unsigned grid,
+                                    unsigned block, size_t smem, cudaStream_t s,
+                                    Args... args) {
   if (!pdl) {
-    kernel<<<grid, block, 0, s>>>(args...);
+    kernel<<<grid, block, smem, s>>>(args...);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(block);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -39,6 +41,12 @@ inline cudaError_t launch_step(bool pdl, void (*kernel)(KArgs...), unsigned grid
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_step(bool pdl, void (*kernel)(KArgs...), unsigned grid,
+                               unsigned block, cudaStream_t s, Args... args) {
+  return launch_step_smem(pdl, kernel, grid, block, 0, s, args...);
 }
 
 // ---- dispatch helpers ------------------------------------------------------
@@ -153,6 +161,24 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
     constexpr bool PQ = std::is_same<T, double>::value && NQ == 8;
     if constexpr (PQ) {
       const unsigned grid = (unsigned)((ne + 31) / 32);
+      if (tn.pqs) {
+        auto kern = law == LAW_ELASTIC      ? k_element_forces_pqs<D, NN, NQ, LAW_ELASTIC>
+                    : law == LAW_NEOHOOKEAN ? k_element_forces_pqs<D, NN, NQ, LAW_NEOHOOKEAN>
+                                            : k_element_forces_pqs<D, NN, NQ, LAW_PLASTIC>;
+        constexpr size_t smem = sizeof(double) * 32 * (NN * D) * (1 + NQ);
+        // above the 48 KB default: allowed once per kernel (a host-side
+        // attribute, no stream work)
+        static std::atomic<int> opted[3] = {0, 0, 0};
+        const int li = law == LAW_ELASTIC ? 0 : law == LAW_NEOHOOKEAN ? 1 : 2;
+        if (!opted[li].load(std::memory_order_relaxed)) {
+          const cudaError_t ea =
+              cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+          if (ea != cudaSuccess) return ea;
+          opted[li].store(1, std::memory_order_relaxed);
+        }
+        return launch_step_smem(g.pdl, kern, grid, 32 * NQ, smem, s, e0, ne, g.E, g.conn, g.pos,
+                                B, wJ, u, mp, ps, re);
+      }
       auto kern = law == LAW_ELASTIC      ? k_element_forces_pq<D, NN, NQ, LAW_ELASTIC>
                   : law == LAW_NEOHOOKEAN ? k_element_forces_pq<D, NN, NQ, LAW_NEOHOOKEAN>
                                           : k_element_forces_pq<D, NN, NQ, LAW_PLASTIC>;

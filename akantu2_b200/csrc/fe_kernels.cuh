@@ -1558,6 +1558,133 @@ __global__ void __launch_bounds__(32 * NQ)
   }
 }
 
+// one FP64 value of a dN/dx table, loaded where it is used: the asm keeps
+// the compiler from holding a point's whole row in registers between the
+// gradient and the force, which read it at two places
+__device__ __forceinline__ double ld_table(const double *p) {
+  double v;
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+// The FP64 law of one (element, point), the operations of
+// element_law<D, NN, LAW, double, false> in the same order, streamed: the
+// nodal displacements are read from the block's staging us[c][lane], the
+// point's dN/dx row b_a = B[(q ND + a D + j) E + e] is loaded node by node
+// where the gradient and the force use it, and each force component c is
+// handed to put(c, value) as soon as it is formed.  Nothing of size NN x D
+// stays in registers, which leaves room for more resident warps.
+template <int D, int NN, int LAW, class Put>
+__device__ __forceinline__ void element_law_streamed(const double (*us)[32], int lane,
+                                                     const double *Bq, int64_t E, double w,
+                                                     const MatParams &mp, const GroupArgs &ps,
+                                                     int64_t ne, int64_t le, int q, Put put) {
+  // grad u = u B^T (shape_functions_inline_impl.hh:303-310): g(i, j) =
+  // u_0,i b_0,j, then + u_a,i b_a,j for a ascending
+  double g[D * D];
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    double ba[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) ba[j] = Bq[(int64_t)(a * D + j) * E];
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const double p = us[a * D + i][lane] * ba[j];
+        g[i + D * j] = (a == 0) ? p : g[i + D * j] + p;
+      }
+  }
+  subtract_eigen<D, double>(ps, ne, le, q, g);
+  if constexpr (LAW == LAW_NEOHOOKEAN) {
+    double S[D * D];
+    finite_pk2<D, double>(mp, g, S, point_c33<D, double>(mp, ps, ne, le, q, g));
+    double Sv[D == 3 ? 6 : 3];
+    to_voigt<D, double>(S, Sv);
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      double ba[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) ba[j] = ld_table(Bq + (int64_t)(a * D + j) * E);
+#pragma unroll
+      for (int k = 0; k < D; ++k) put(a * D + k, finite_force_component<D, double>(ba, g, Sv, k) * w);
+    }
+  } else {
+    double sig[D * D];
+    if constexpr (LAW == LAW_ELASTIC) {
+      elastic_stress<D, double>(mp.lambda, mp.mu, g, mp.sigma_th, sig);
+    } else {
+      plastic_point<D, double>(mp, ps, ne, le, q, g, sig);
+    }
+    // sigma B, d x n (shape_lagrange_inline_impl.hh:402-408), times wJ_q
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      double ba[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) ba[j] = ld_table(Bq + (int64_t)(a * D + j) * E);
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        double s = sig[i] * ba[0];
+#pragma unroll
+        for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * ba[j];
+        put(a * D + i, s * w);
+      }
+    }
+  }
+}
+
+// k_element_forces_pq with the streamed law: the same thread layout (warp =
+// point, lane = element), the same gather, the same sums over q in
+// increasing order, bit for bit; every point's NN x D force components go to
+// shared memory [q][component][lane] as they are formed and are summed in
+// one round.  Dynamic shared memory: (NN D + NQ NN D) x 32 doubles (55,296
+// bytes for hexahedra in 3D, above the 48 KB of static shared memory).
+template <int D, int NN, int NQ, int LAW>
+__global__ void __launch_bounds__(32 * NQ)
+    k_element_forces_pqs(int64_t e_begin, int64_t e_count, int64_t E,
+                         const int32_t *__restrict__ conn, const int32_t *__restrict__ pos,
+                         const double *__restrict__ B, const double *__restrict__ wJ,
+                         const double *__restrict__ u, MatParams mp, GroupArgs ps,
+                         double *__restrict__ re) {
+  pdl_begin();
+  constexpr int ND = NN * D;
+  extern __shared__ double pqs_smem[];
+  double(*us)[32] = reinterpret_cast<double(*)[32]>(pqs_smem);
+  double(*red)[ND][32] = reinterpret_cast<double(*)[ND][32]>(pqs_smem + ND * 32);
+  const int lane = threadIdx.x & 31;
+  const int q = threadIdx.x >> 5;
+  const int64_t le = (int64_t)blockIdx.x * 32 + lane;
+  const bool active = le < e_count && element_active(ps, le) &&
+                      element_indices_ok<NN>(ps, conn, pos, E, e_begin + le);
+  const int64_t e = e_begin + le;
+  if (active) {
+    for (int a = q; a < NN; a += NQ) {
+      const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+      for (int i = 0; i < D; ++i) us[a * D + i][lane] = u[node * D + i];
+    }
+  }
+  __syncthreads();
+  if (active) {
+    const double w = wJ[(int64_t)q * E + e];
+    const MatParams mpe = group_params(mp, ps, le);
+    element_law_streamed<D, NN, LAW>(us, lane, B + (int64_t)q * ND * E + e, E, w, mpe, ps,
+                                     e_count, le, q,
+                                     [&](int c, double v) { red[q][c][lane] = v; });
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int c = q; c < ND; c += NQ) {
+      double s = red[0][c][lane];
+#pragma unroll
+      for (int qq = 1; qq < NQ; ++qq) s = s + red[qq][c][lane];
+      const int a = c / D;
+      re[(int64_t)pos[(int64_t)a * E + e] * SlotStride<D, double>::value + (c - a * D)] = s;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K5: node gather + residual + lumped solve + corrector
 //   f_int = sum_slots (-1) r_e           (dof_manager.cc:65-120)

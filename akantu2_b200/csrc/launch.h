@@ -33,6 +33,10 @@ struct ElemTuning {
   // det J w from the coordinates by the precomputation's arithmetic instead
   // of streaming the tables (the same numbers)
   int rec = 0;
+  // plain FP64 hexahedra (one thread per point): 1 runs the streamed law
+  // (k_element_forces_pqs: dN/dx rows loaded node by node where used, force
+  // components sent to shared memory as formed); the same numbers
+  int pqs = 0;
 };
 // points_per_iteration flag of the mixed hexahedron kernel: the points are
 // evaluated as packed FP32 pairs (2, 4 or 8 points per iteration)

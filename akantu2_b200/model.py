@@ -408,7 +408,8 @@ class SolidMechanicsModel:
 
     def setNodalAsync(self, name, pinned):
         """Asynchronous upload of a whole nodal array from a pinned host array
-        (akb_model_set_nodal_async); the array may be reused after the next
+        (akb_model_set_nodal_async); the array may be reused once a read
+        enqueued after the next step has been waited for, or after the next
         synchronize()."""
         self._sync_up()
         _capi.check(_capi.lib().akb_model_set_nodal_async(self._h, _FIELDS[name], _capi.ptr(pinned),
@@ -417,7 +418,10 @@ class SolidMechanicsModel:
 
     def getNodalAsync(self, name, pinned):
         """Asynchronous read of a nodal array into a pinned host array; returns
-        a ticket for waitNodalAsync (akb_model_get_nodal_async)."""
+        a ticket for waitNodalAsync (akb_model_get_nodal_async).  The
+        ASYNC_READS_IN_FLIGHT most recent tickets can be waited on one by one:
+        waiting for each step's read that many steps minus one later lets the
+        copies of consecutive steps run back to back."""
         t = ctypes.c_int64()
         _capi.check(_capi.lib().akb_model_get_nodal_async(self._h, _FIELDS[name], _capi.ptr(pinned),
                                                           pinned.nbytes, ctypes.byref(t)))
@@ -579,6 +583,20 @@ class SolidMechanicsModel:
         w = ctypes.c_int()
         _capi.check(_capi.lib().akb_model_get_recompute_geometry(self._h, _LAW_IDS[law],
                                                                  ctypes.byref(w)))
+        return bool(w.value)
+
+    def setStreamedPoints(self, law, on=True):
+        """Plain FP64 hexahedra: the per-point kernel with the streamed law
+        (dN/dx rows loaded where used, forces sent to shared memory as formed;
+        fewer registers) or with the point's row and forces held in
+        registers; results are unchanged by it."""
+        _capi.check(_capi.lib().akb_model_set_streamed_points(self._h, _LAW_IDS[law],
+                                                              int(bool(on))))
+
+    def getStreamedPoints(self, law):
+        w = ctypes.c_int()
+        _capi.check(_capi.lib().akb_model_get_streamed_points(self._h, _LAW_IDS[law],
+                                                              ctypes.byref(w)))
         return bool(w.value)
 
     def setNodeShape(self, node_block, staged=False):

@@ -76,6 +76,9 @@ def parse():
                    help="serve: every request gets a model of its own")
     p.add_argument("--cells", type=int, default=0, help="override the mesh resolution")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--e2e-lag", type=int, default=3,
+                   help="end-to-end leg: steps between a step's read and the wait for it "
+                        "(1 .. AKB_ASYNC_READS_IN_FLIGHT - 1)")
     p.add_argument("--no-e2e-fp64", action="store_true",
                    help="skip the end-to-end leg of the FP64 path")
     p.add_argument("--no-extras", action="store_true",
@@ -209,8 +212,8 @@ def serve_mesh(kind, cells):
     return _MESH_CACHE[key]
 
 
-# algorithmic bytes (formula of the specification, per element-step), and the
-# element-force kernel's own share
+# algorithmic bytes per element-step (fixed formula over the arrays the step
+# must read and write), and the element-force kernel's own share
 def quadrature_points(config, qp_rule=0):
     return {"hex8": 8, "tet": 1, "tri6": 6 if qp_rule else 3, "batch": 1}[config]
 
@@ -533,15 +536,17 @@ def run_ours(args, rep=None, emit=True, extra=False):
             # end to end through the C ABI with pinned host buffers
             nb = int(np.prod(mesh.nodes.shape)) * 8
             k_e2e = max(1, min(args.steps, 100 if prec == precisions[0] else 20))
-            secs_sync, secs_async = e2e_legs(m, mesh.nodes.shape, k_e2e, barrier)
+            secs_sync, secs_async = e2e_legs(m, mesh.nodes.shape, k_e2e, barrier,
+                                             args.e2e_lag)
             secs_sync, secs_async = max_over_ranks(secs_sync), max_over_ranks(secs_async)
             results[prec]["e2e"] = {"value": world * E * k_e2e / secs_async, "unit": UNIT,
                                     "steps": k_e2e, "h2d_bytes_per_step": nb,
                                     "d2h_bytes_per_step": nb,
                                     "mode": "pipelined: the external force of every step uploaded "
                                             "and its displacement read back through the async "
-                                            "C ABI, each result waited for one step later, all "
-                                            "copies complete inside the timed region",
+                                            f"C ABI, each result waited for {args.e2e_lag} "
+                                            "step(s) later, all copies complete inside the "
+                                            "timed region",
                                     "synchronous_value": world * E * k_e2e / secs_sync,
                                     "pcie_bound": e2e_bound(nb, nb, secs_async, k_e2e)}
         del m
@@ -621,17 +626,21 @@ def flushed_steps(m, k, device):
     return total
 
 
-def e2e_legs(m, shape, k, barrier):
+def e2e_legs(m, shape, k, barrier, lag=None):
     """End to end through the C ABI with pinned host buffers, k steps: every
     step uploads the external force and reads the displacement back.
     Synchronous: set_nodal / solve_step / get_nodal.  Pipelined: the async
-    forms with two host buffers per direction, the result of step j waited
-    for after step j + 1 is enqueued.  Returns both wall times (seconds)."""
+    forms, the result of step j waited for after step j + lag is enqueued
+    (lag + 1 host buffers per direction; by default lag =
+    AKB_ASYNC_READS_IN_FLIGHT - 1, so that the copies of consecutive steps
+    run back to back).  Returns both wall times (seconds)."""
     from akantu2_b200 import _capi
     from akantu2_b200._capi import PinnedArray
     L = _capi.lib()
-    fext = [PinnedArray(shape) for _ in range(2)]
-    uout = [PinnedArray(shape) for _ in range(2)]
+    if lag is None:
+        lag = _capi.ASYNC_READS_IN_FLIGHT - 1
+    fext = [PinnedArray(shape) for _ in range(lag + 1)]
+    uout = [PinnedArray(shape) for _ in range(lag + 1)]
     for f in fext:
         f.array[:] = 0.0
     nb = fext[0].array.nbytes
@@ -647,17 +656,18 @@ def e2e_legs(m, shape, k, barrier):
                                               _capi.ptr(uout[0].array), nb))
 
     def async_steps(n):
-        prev = None
+        issued = []
         for j in range(n):
+            b = j % (lag + 1)
             _capi.check(L.akb_model_set_nodal_async(m._h, _capi.EXTERNAL_FORCE,
-                                                    _capi.ptr(fext[j % 2].array), nb))
+                                                    _capi.ptr(fext[b].array), nb))
             _capi.check(L.akb_model_solve_step(m._h, 1))
             _capi.check(L.akb_model_get_nodal_async(m._h, _capi.DISPLACEMENT,
-                                                    _capi.ptr(uout[j % 2].array), nb,
+                                                    _capi.ptr(uout[b].array), nb,
                                                     ctypes.byref(ticket)))
-            if prev is not None:
-                _capi.check(L.akb_model_wait_nodal_async(m._h, prev))
-            prev = ticket.value
+            issued.append(ticket.value)
+            if len(issued) > lag:
+                _capi.check(L.akb_model_wait_nodal_async(m._h, issued.pop(0)))
         _capi.check(L.akb_model_synchronize(m._h))
 
     # untimed warm-up of both legs: the first asynchronous call creates the
@@ -813,7 +823,7 @@ def run_batch(args, rep=None, emit=True, extra=False):
         if prec == precisions[0] and not extra:
             nb = N * 3 * 8
             k_e2e = max(1, min(args.steps, 100))
-            secs_sync, secs_async = e2e_legs(b, (N, 3), k_e2e, barrier)
+            secs_sync, secs_async = e2e_legs(b, (N, 3), k_e2e, barrier, args.e2e_lag)
             secs_sync, secs_async = max_over_ranks(secs_sync), max_over_ranks(secs_async)
             results[prec]["e2e"] = {"value": world * E * k_e2e / secs_async, "unit": UNIT,
                                     "steps": k_e2e, "h2d_bytes_per_step": nb,

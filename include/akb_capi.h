@@ -196,14 +196,21 @@ int akb_model_get_nodal(akb_model *model, int field, void *host, int64_t nbytes)
 int akb_model_nodal_device_pointer(akb_model *model, int field, void **device_ptr);
 /* asynchronous forms of set/get, for drivers that stream inputs and results
  * every step (pinned host buffers, akb_host_alloc): the copies run on two
- * copy streams of the model, double-buffered in device staging, so that they
- * overlap the steps enqueued after them.  set: takes effect before the next
- * step; the host buffer may be reused after the next akb_model_synchronize
- * (an external force set this way is not tested for zero).  get: snapshots
- * the field as of the steps enqueued so far and returns a ticket; the host
- * buffer holds it once akb_model_wait_nodal_async(ticket) or
- * akb_model_synchronize returns (only the two most recent tickets can be
- * waited on individually). */
+ * copy streams of the model through device staging (two upload buffers,
+ * AKB_ASYNC_READS_IN_FLIGHT read buffers), so that they overlap the steps
+ * enqueued after them.  set: takes effect before the next step; the host
+ * buffer may be reused once a read enqueued after that step has been waited
+ * for, or after the next akb_model_synchronize (an external force set this
+ * way is not tested for zero).  get: snapshots the field as of the steps
+ * enqueued so far and returns a ticket; the host buffer holds it once
+ * akb_model_wait_nodal_async(ticket) or akb_model_synchronize returns (only
+ * the AKB_ASYNC_READS_IN_FLIGHT most recent tickets can be waited on
+ * individually).  A driver that waits for each step's read one step later
+ * leaves the copies of a single step to overlap the computation; waiting
+ * AKB_ASYNC_READS_IN_FLIGHT - 1 steps later lets the copies of consecutive
+ * steps run back to back, so that a step costs the slower of its copies and
+ * its computation. */
+#define AKB_ASYNC_READS_IN_FLIGHT 4
 int akb_model_set_nodal_async(akb_model *model, int field, const void *host, int64_t nbytes);
 int akb_model_get_nodal_async(akb_model *model, int field, void *host, int64_t nbytes,
                               int64_t *ticket);
@@ -383,6 +390,17 @@ int akb_model_get_prefetch(const akb_model *model, int law, int *waves);
  * this library; the reference precomputes, fe_engine_template_tmpl.hh). */
 int akb_model_set_recompute_geometry(akb_model *model, int law, int on);
 int akb_model_get_recompute_geometry(const akb_model *model, int law, int *on);
+/* form of the plain FP64 hexahedron kernel (one thread per Gauss point):
+ * 1 (the default of the neohookean and plastic laws; elastic 0) evaluates
+ * the law streamed, each point's dN/dx row loaded node by node where the
+ * gradient and the force read it and every force component written to
+ * shared memory as soon as it is formed, which needs about half the
+ * registers; 0 holds the point's row and forces in registers.  The same
+ * operations in the same order either way (bit-identical); the autotuner
+ * tries both.  Only plain FP64 hexahedra.  No reference counterpart (a
+ * launch setting of this library). */
+int akb_model_set_streamed_points(akb_model *model, int law, int on);
+int akb_model_get_streamed_points(const akb_model *model, int law, int *on);
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,

@@ -1,7 +1,7 @@
 """The fast FP64 path (AKB_PRECISION_FP64_FAST): FP64 state and element math,
 hexahedra by the sum-factorised element kernel with contraction allowed.  It
-does not keep the CPU path's operation order, so it is held to the 1e-12
-relative bar of the specification against the oracle (max |gpu - cpu| / max
+does not keep the CPU path's operation order, so it is held to a 1e-12
+relative bar against the oracle (max |gpu - cpu| / max
 |cpu| over each nodal array) after 1,000 steps, on a box of parallelepipeds
 (the per-element adjugate table) and on a distorted box (geometry per point),
 for the elastic and neohookean laws; the plastic law, whose yield test can

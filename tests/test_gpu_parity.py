@@ -3,8 +3,8 @@
 The FP64 kernels are compiled without contraction and follow the oracle's
 operation order, so elastic and plastic runs are expected to be bit-identical;
 the neohookean law calls log(), whose last bit may differ between the CUDA
-and glibc implementations, so those runs are held to the 1e-12 relative bar
-of the specification (max |gpu - cpu| / max |cpu| over each nodal array).
+and glibc implementations, so those runs are held to a 1e-12 relative bar
+(max |gpu - cpu| / max |cpu| over each nodal array).
 """
 import numpy as np
 import pytest
@@ -514,9 +514,12 @@ def test_neumann_stress_adds_to_external_force():
     assert np.allclose((expected - 1.0).sum(axis=0), sigma[:, 2], rtol=1e-12, atol=1e-15)
 
 
-def test_async_nodal_io_matches_synchronous_calls():
+@pytest.mark.parametrize("lag", [1, 3])
+def test_async_nodal_io_matches_synchronous_calls(lag):
     """per-step uploads and reads through the asynchronous forms give the
-    state and the host copies of the synchronous set / get sequence"""
+    state and the host copies of the synchronous set / get sequence, each
+    read waited for lag steps later (up to AKB_ASYNC_READS_IN_FLIGHT - 1;
+    lag + 1 host buffers per direction)"""
     from akantu2_b200._capi import PinnedArray
     mesh = akb.box_tet4(6)
     v0, bl = sinusoidal_velocity(mesh.nodes, 0.05), blocked_face(mesh.nodes)
@@ -528,32 +531,56 @@ def test_async_nodal_io_matches_synchronous_calls():
         m.setNodal("velocity", v0)
         m.setNodal("blocked_dofs", bl)
         m.setTimeStep(0.8 * m.getStableTimeStep())
-        fin = [PinnedArray(mesh.nodes.shape) for _ in range(2)]
-        uo = [PinnedArray(mesh.nodes.shape) for _ in range(2)]
+        fin = [PinnedArray(mesh.nodes.shape) for _ in range(lag + 1)]
+        uo = [PinnedArray(mesh.nodes.shape) for _ in range(lag + 1)]
         seen = []
-        prev = None
+        pending = []
         for j, f in enumerate(forces):
             if mode == "sync":
                 m.setNodal("external_force", f)
                 m.solveStep(1)
                 seen.append(m.getDisplacement().copy())
             else:
-                fin[j % 2].array[:] = f
-                m.setNodalAsync("external_force", fin[j % 2].array)
+                b = j % (lag + 1)
+                fin[b].array[:] = f
+                m.setNodalAsync("external_force", fin[b].array)
                 m.solveStep(1)
-                t = m.getNodalAsync("displacement", uo[j % 2].array)
-                if prev is not None:
-                    m.waitNodalAsync(prev[0])
-                    seen.append(uo[prev[1]].array.copy())
-                prev = (t, j % 2)
-                m.synchronize() if j == len(forces) - 1 else None
+                pending.append((m.getNodalAsync("displacement", uo[b].array), b))
+                if len(pending) > lag:
+                    t, bo = pending.pop(0)
+                    m.waitNodalAsync(t)
+                    seen.append(uo[bo].array.copy())
         if mode == "async":
-            seen.append(uo[prev[1]].array.copy())
+            m.synchronize()
+            seen += [uo[bo].array.copy() for _, bo in pending]
         out[mode] = (seen, m.getVelocity().copy())
     assert len(out["sync"][0]) == len(out["async"][0])
     for a, b in zip(out["sync"][0], out["async"][0]):
         assert np.array_equal(a, b)
     assert np.array_equal(out["sync"][1], out["async"][1])
+
+
+def test_async_reads_in_flight_limit():
+    """the AKB_ASYNC_READS_IN_FLIGHT most recent reads can be waited on one
+    by one; an older ticket is rejected (akb_model_synchronize covers it)"""
+    from akantu2_b200 import _capi
+    from akantu2_b200._capi import PinnedArray
+    n = _capi.ASYNC_READS_IN_FLIGHT
+    mesh = akb.box_tet4(4)
+    m = gpu_model(mesh, [UNIT_ELASTIC], precision="mixed")
+    m.setTimeStep(0.8 * m.getStableTimeStep())
+    bufs = [PinnedArray(mesh.nodes.shape) for _ in range(n + 1)]
+    tickets = []
+    for b in bufs:
+        m.solveStep(1)
+        tickets.append(m.getNodalAsync("displacement", b.array))
+    with pytest.raises(akb.AkbError) as e:
+        m.waitNodalAsync(tickets[0])
+    assert e.value.name == "AKB_EINVAL"
+    for t in tickets[1:]:
+        m.waitNodalAsync(t)
+    m.synchronize()
+    assert np.array_equal(bufs[-1].array, m.getDisplacement())
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

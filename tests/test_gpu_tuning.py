@@ -611,3 +611,68 @@ def test_persistent_barrier_wait_runs_out_and_reports():
     ref.solveStep(40)
     assert np.array_equal(m.getDisplacement(), ref.getDisplacement())
     assert np.array_equal(m.getVelocity(), ref.getVelocity())
+
+
+@pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN, UNIT_PLASTIC])
+@pytest.mark.parametrize("eigen", [False, True])
+def test_hex8_fp64_streamed_points_are_bit_identical(mat, eigen):
+    """plain FP64 hexahedra: the per-point kernel with the streamed law (dN/dx
+    rows loaded where used, forces written to shared memory as formed) and
+    with the point's row and forces held in registers give the same nodal
+    fields and internals, on a partly distorted box with two materials of
+    the law, with and without an eigen gradient; the streamed form is the
+    default of the neohookean and plastic laws"""
+    mesh = akb.box_hex8(9)  # 729 elements: 23 blocks of 32, the last one partial
+    x = mesh.nodes
+    rng = np.random.default_rng(5)
+    inner = np.all((x > 1e-9) & (x < 1 - 1e-9), axis=1) & (x[:, 2] > 0.4)
+    x[inner] += rng.uniform(-0.1, 0.1, size=(inner.sum(), 3)) / 9
+    v0, bl = sinusoidal_velocity(x, 0.04), blocked_face(x)
+    m1 = dict(mat, sigma_y=2e-3) if "sigma_y" in mat else dict(mat)
+    m2 = dict(m1, name=m1["name"] + "_b", E=1.7, nu=0.25)
+    if eigen:
+        m1["eigen_grad_u"] = 0.01 * np.arange(9.0).reshape(3, 3)
+    mat_of_elem = (np.arange(mesh.connectivity.shape[0]) % 3 == 0).astype(np.int32)
+    name = LAW_NAME[mat["type"]]
+    runs = []
+    for streamed in (True, False):
+        m = gpu_model(mesh, [m1, m2], mat_of_elem=mat_of_elem, precision="fp64")
+        assert m.getStreamedPoints(mat["type"]) == (name != "elastic")
+        m.setStreamedPoints(mat["type"], streamed)
+        assert m.getStreamedPoints(mat["type"]) == streamed
+        m.setNodal("velocity", v0)
+        m.setNodal("blocked_dofs", bl)
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        m.solveStep(37)    # single launches, then a 100-step graph
+        m.solveStep(100)
+        fields = [m.getDisplacement().copy(), m.getVelocity().copy(),
+                  m.getAcceleration().copy(), m.getInternalForce().copy()]
+        for k in range(2):
+            mt = m.getMaterial(k)
+            fields.append(mt.getGradU().copy())
+            if name == "plastic":
+                fields += [mt.getStress().copy(), mt.getInternal("inelastic_strain")().copy()]
+        runs.append(fields)
+        del m
+    if name == "plastic":
+        assert np.max(np.abs(runs[0][6])) > 0, "the box must yield"
+    for a, b_ in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b_)
+
+
+def test_hex8_fp64_streamed_points_setting_rules():
+    """the streamed law is a setting of plain FP64 hexahedra only; the
+    autotuner keeps the state and picks one of the two forms"""
+    for etype, precision in (("hex8", "mixed"), ("hex8", "fp64_fast"), ("tet4", "fp64")):
+        mesh = akb.box_hex8(3) if etype == "hex8" else akb.box_tet4(3)
+        m = gpu_model(mesh, [UNIT_ELASTIC], precision=precision)
+        assert not m.getStreamedPoints("elastic")
+        with pytest.raises(akb.AkbError):
+            m.setStreamedPoints("elastic", True)
+        m.setStreamedPoints("elastic", False)
+    mesh = akb.box_hex8(6)
+    v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
+    ref = _run(mesh, UNIT_NEOHOOKEAN, "fp64", v0, bl, 60)
+    tuned = _run(mesh, UNIT_NEOHOOKEAN, "fp64", v0, bl, 60, autotune_at=20)
+    assert np.array_equal(ref.getDisplacement(), tuned.getDisplacement())
+    assert np.array_equal(ref.getVelocity(), tuned.getVelocity())
