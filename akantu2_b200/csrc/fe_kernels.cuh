@@ -1814,27 +1814,87 @@ __device__ __forceinline__ bool node_range_ok(const int32_t *ptr, int64_t N, int
 #endif
 }
 
-// WIDE: slots read 32 bytes at a time (the launcher checks the slot
-// array's alignment); same slots, same order
-template <int D, class RT, bool KAHAN, bool WIDE = false>
-__device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
-                                          const RT *re,
-                                          const double *fext,
-                                          const double *mass,
-                                          const uint8_t *blocked,
-                                          double *fint, double *a,
-                                          double *v, const double *u,
-                                          double *u_next, double dt,
-                                          const int32_t *node_inst,
-                                          const double *inst_dt, int flags,
-                                          unsigned int *status) {
-  double acc[D], comp[D];
+// A node's inputs to the update, loaded ahead of its slot gather by the
+// state-first node update (the values node_apply reads itself)
+template <int D> struct NodeState {
+  double m;
+  uint8_t bl;
+  double a[D], v[D], f[D], u[D];
+};
+
+template <int D>
+__device__ __forceinline__ void load_node_state(NodeState<D> &st, int64_t i, const double *fext,
+                                                const double *a, const double *v,
+                                                const double *u, int flags) {
 #pragma unroll
   for (int c = 0; c < D; ++c) {
-    acc[c] = 0.;
-    comp[c] = 0.;
+    const int64_t k = i * D + c;
+    st.a[c] = a[k];
+    st.v[c] = v[k];
+    st.f[c] = (flags & NU_FEXT_ZERO) ? 0. : fext[k];
+    st.u[c] = (flags & NU_PREDICT) ? u[k] : 0.;
   }
-  const int32_t p0 = ptr[i], p1 = ptr[i + 1];
+}
+
+// node_apply on preloaded inputs: the same operations in the same order
+template <int D>
+__device__ __forceinline__ void node_apply_state(int64_t i, const double *acc,
+                                                 const NodeState<D> &st, double *fint, double *a,
+                                                 double *v, double *u_next, double dt,
+                                                 const int32_t *node_inst,
+                                                 const double *inst_dt, int flags,
+                                                 unsigned int *status) {
+  if (flags & NU_FINT) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) fint[i * D + c] = acc[c];
+  }
+  if (!(flags & NU_CORRECT)) return;
+  const double m = st.m;
+  const uint8_t bl = st.bl;
+  dt = node_dt(dt, node_inst, inst_dt, i);
+  const double hdt = __dmul_rn(.5, dt);
+  bool bad = false;
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const int64_t k = i * D + c;
+    const bool free_dof = !((bl >> c) & 1);
+    const double ak = st.a[c];
+    double vk = st.v[c];
+    if (free_dof) vk = __dadd_rn(vk, __dmul_rn(dt, ak));
+    double r;
+    if (flags & NU_FEXT_ZERO) {
+      r = acc[c];
+    } else {
+      r = __dadd_rn(0., __dmul_rn(1., st.f[c]));
+      r = __dadd_rn(r, __dmul_rn(1., acc[c]));
+    }
+    const double ma = __dadd_rn(0., __dmul_rn(-1., ak));
+    r = __dadd_rn(r, __dmul_rn(m, ma));
+    double an = ak;
+    if (free_dof) {
+      const double x = __dmul_rn(1., __ddiv_rn(r, m));
+      vk = __dadd_rn(vk, __dmul_rn(hdt, x));
+      an = __dadd_rn(ak, __dmul_rn(1., x));
+      v[k] = vk;
+      a[k] = an;
+      bad |= !isfinite(an);
+    }
+    if (flags & NU_PREDICT) {
+      const double uk = st.u[c];
+      u_next[k] = free_dof ? __dadd_rn(uk, __dadd_rn(__dmul_rn(dt, vk),
+                                                     __dmul_rn(hdt, __dmul_rn(dt, an))))
+                           : uk;
+    }
+  }
+  if (bad) atomicOr(status, 1u);
+}
+
+// the node's slots p0 .. p1 summed in increasing slot order into acc (comp:
+// the compensation of the Kahan sum); WIDE: slots read 32 bytes at a time
+// (the launcher checks the slot array's alignment), same slots, same order
+template <int D, class RT, bool KAHAN, bool WIDE>
+__device__ __forceinline__ void gather_slots(int32_t p0, int32_t p1, const RT *re, double *acc,
+                                             double *comp) {
   if constexpr (WIDE && std::is_same<RT, float>::value) {
     // floats per slot and slots per 32-byte load
     constexpr int FS = SlotStride<D, RT>::value, PER = 8 / FS;
@@ -1896,6 +1956,29 @@ __device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
       accumulate_slot<D, KAHAN>(rv, acc, comp);
     }
   }
+}
+
+// the gather and the node update of node i (WIDE: 32-byte slot loads)
+template <int D, class RT, bool KAHAN, bool WIDE = false>
+__device__ __forceinline__ void node_body(int64_t i, const int32_t *ptr,
+                                          const RT *re,
+                                          const double *fext,
+                                          const double *mass,
+                                          const uint8_t *blocked,
+                                          double *fint, double *a,
+                                          double *v, const double *u,
+                                          double *u_next, double dt,
+                                          const int32_t *node_inst,
+                                          const double *inst_dt, int flags,
+                                          unsigned int *status) {
+  double acc[D], comp[D];
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    acc[c] = 0.;
+    comp[c] = 0.;
+  }
+  const int32_t p0 = ptr[i], p1 = ptr[i + 1];
+  gather_slots<D, RT, KAHAN, WIDE>(p0, p1, re, acc, comp);
   node_apply<D>(i, acc, fext, mass, blocked, fint, a, v, u, u_next, dt, node_inst, inst_dt, flags,
                 status);
 }
@@ -1918,6 +2001,45 @@ __global__ void __launch_bounds__(1024) k_node_update(int64_t N, const int32_t *
   if (i >= N || !node_range_ok(ptr, N, i, status)) return;
   node_body<D, RT, KAHAN, WIDE>(i, ptr, re, fext, mass, blocked, fint, a, v, u, u_next, dt,
                                 node_inst, inst_dt, flags, status);
+}
+
+// State-first form of k_node_update (the same numbers): the node's slot
+// range, mass and blocked flags, which no step changes, are read before the
+// wait on the preceding kernel (a dependent launch starts them under that
+// kernel's tail), and its a, v, f_ext and u before the slot gather, so that
+// they are in flight together with it rather than after it
+template <int D, class RT, bool KAHAN, bool WIDE = false>
+__global__ void __launch_bounds__(1024)
+    k_node_update_early(int64_t N, const int32_t *__restrict__ ptr, const RT *__restrict__ re,
+                        const double *__restrict__ fext, const double *__restrict__ mass,
+                        const uint8_t *__restrict__ blocked, double *__restrict__ fint,
+                        double *__restrict__ a, double *__restrict__ v,
+                        const double *__restrict__ u, double *__restrict__ u_next, double dt,
+                        const int32_t *__restrict__ node_inst, const double *__restrict__ inst_dt,
+                        int flags, unsigned int *__restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = i < N;
+  int32_t p0 = 0, p1 = 0;
+  NodeState<D> st;
+  st.m = 1.;
+  st.bl = 0;
+  if (in) {
+    p0 = ptr[i];
+    p1 = ptr[i + 1];
+    st.m = mass[i];
+    st.bl = blocked[i];
+  }
+  pdl_begin();
+  if (!in || !node_range_ok(ptr, N, i, status)) return;
+  if (flags & NU_CORRECT) load_node_state<D>(st, i, fext, a, v, u, flags);
+  double acc[D], comp[D];
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    acc[c] = 0.;
+    comp[c] = 0.;
+  }
+  gather_slots<D, RT, KAHAN, WIDE>(p0, p1, re, acc, comp);
+  node_apply_state<D>(i, acc, st, fint, a, v, u_next, dt, node_inst, inst_dt, flags, status);
 }
 
 // Node update of a batch whose instances stop after their own step counts:

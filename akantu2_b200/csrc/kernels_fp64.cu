@@ -119,7 +119,7 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
                                     double dt, int flags, unsigned int *status, int node_block,
-                                    bool staged, cudaStream_t s) {
+                                    int form, cudaStream_t s) {
   if (g.N > 0 && g.inst_end) {
     auto kern = g.D == 3 ? k_node_update_retire<3, double, false> : k_node_update_retire<2, double, false>;
     return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
@@ -128,9 +128,9 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
   }
   if (g.N == 0) return cudaSuccess;
 #ifdef AKB_BOUNDS_CHECK
-  staged = false;  // the bounds-checking build checks each node's own slot range
+  if (form == 1) form = 0;  // the bounds-checking build checks each node's own slot range
 #endif
-  if (staged) {
+  if (form == 1) {
     AKB_DISPATCH_NODE_BLOCK(node_block, {
       auto kern = g.D == 3 ? k_node_update_staged<3, double, false, NB>
                            : k_node_update_staged<2, double, false, NB>;
@@ -145,6 +145,11 @@ cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const do
                                : k_node_update<3, double, false>)
                        : (wide ? k_node_update<2, double, false, true>
                                : k_node_update<2, double, false>);
+  if (form == 2)
+    kern = g.D == 3 ? (wide ? k_node_update_early<3, double, false, true>
+                            : k_node_update_early<3, double, false>)
+                    : (wide ? k_node_update_early<2, double, false, true>
+                            : k_node_update_early<2, double, false>);
   return launch_step(g.pdl, kern, grid_for(g.N, node_block), node_block, s, g.N, g.ptr, re,
                      fext, mass, blocked, fint, a, v, u, u_next, dt, g.node_inst, g.inst_dt,
                      flags, status);

@@ -115,18 +115,19 @@ cudaError_t launch_element_forces_hex8_x2(const DevGeom &g, int law, int64_t e0,
 // flags: NU_CORRECT | NU_PREDICT | NU_FINT | NU_FEXT_ZERO (fe_kernels.cuh);
 // the predictor of the next step reads u and writes u_next
 // node_block: threads per block of the node update (any multiple of 32 up to
-// 1024; 128, 256 or 512 when staged); staged: the gather goes through shared
-// memory (k_node_update_staged, same arithmetic)
+// 1024; 128, 256 or 512 when staged); form: 0 the direct gather, 1 the gather
+// staged through shared memory (k_node_update_staged), 2 the direct gather
+// with the node's state read first (k_node_update_early); same arithmetic
 cudaError_t launch_node_update_fp64(const DevGeom &g, const double *re, const double *fext,
                                     const double *mass, const uint8_t *blocked, double *fint,
                                     double *a, double *v, const double *u, double *u_next,
                                     double dt, int flags, unsigned int *status, int node_block,
-                                    bool staged, cudaStream_t s);
+                                    int form, cudaStream_t s);
 cudaError_t launch_node_update_mixed(const DevGeom &g, const float *re, const double *fext,
                                      const double *mass, const uint8_t *blocked,
                                      double *fint, double *a, double *v, const double *u,
                                      double *u_next, double dt, int flags,
-                                     unsigned int *status, int node_block, bool staged,
+                                     unsigned int *status, int node_block, int form,
                                      cudaStream_t s);
 
 // the device step counter of a batch with stopping instances, + 1

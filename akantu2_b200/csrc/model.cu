@@ -269,7 +269,7 @@ struct akb_model {
   int stream_priority = 0;    // of the model's stream, when priority_set
   bool priority_set = false;
   int node_block = 128;       // threads per block of the node update
-  bool node_staged = false;   // gather staged through shared memory
+  int node_form = 0;  // node update: 0 direct, 1 staged gather, 2 state first
   // mixed hexahedra: every element a parallelepiped (found at initFull), and
   // the kernel in use: 0 the general one, 1 the one compiled for such meshes,
   // 2 the same reading each element's adjugate and 1/det from dgeo [10][E]
@@ -660,11 +660,11 @@ int node_update(akb_model *m, bool correct) {
   if (m->precision == AKB_PRECISION_MIXED)
     e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass, m->dblocked,
                                  m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
-                                 m->node_block, m->node_staged, m->stream);
+                                 m->node_block, m->node_form, m->stream);
   else
     e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass, m->dblocked,
                                 m->dfint, m->da, m->dv, u, u_next, m->dt, flags, m->dstatus,
-                                m->node_block, m->node_staged, m->stream);
+                                m->node_block, m->node_form, m->stream);
   if (e != cudaSuccess) return fail(AKB_ECUDA, std::string("node update: ") + cudaGetErrorString(e));
   if (correct) AKB_TRY(prescribe(m, u_next, true));
   m->fint_valid = !correct;
@@ -2246,12 +2246,14 @@ int akb_model_autotune(akb_model *m, int repeats) {
     const int flags = NU_CORRECT | NU_PREDICT | (m->fext_zero ? NU_FEXT_ZERO : 0);
     check(cudaMemcpyAsync(t_a, m->da, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "copy");
     check(cudaMemcpyAsync(t_v, m->dv, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "copy");
-    // direct gather with 128 .. 1024 threads, staged gather with 128 .. 512
-    const int blocks[7] = {128, 256, 512, 1024, 128, 256, 512};
+    // direct gather with 128 .. 1024 threads, staged gather with 128 .. 512,
+    // state first with 128 .. 512
+    const int blocks[10] = {128, 256, 512, 1024, 128, 256, 512, 128, 256, 512};
+    const int forms[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 2};
     float best = 0.f;
-    for (int k = 0; k < 7 && rc == AKB_OK; ++k) {
+    for (int k = 0; k < 10 && rc == AKB_OK; ++k) {
       float ms = 0.f;
-      const bool staged = k >= 4;
+      const int staged = forms[k];
       auto launch = [&]() {
         if (m->precision == AKB_PRECISION_MIXED)
           return launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass,
@@ -2265,7 +2267,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
       if (k == 0 || ms < best) {
         best = ms;
         m->node_block = blocks[k];
-        m->node_staged = staged;
+        m->node_form = staged;
       }
     }
   }
@@ -2285,11 +2287,11 @@ int akb_model_autotune(akb_model *m, int repeats) {
           if (m->precision == AKB_PRECISION_MIXED)
             e = launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass,
                                          m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
-                                         flags, t_status, m->node_block, m->node_staged, s);
+                                         flags, t_status, m->node_block, m->node_form, s);
           else
             e = launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass,
                                         m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
-                                        flags, t_status, m->node_block, m->node_staged, s);
+                                        flags, t_status, m->node_block, m->node_form, s);
         }
         return e;
       };
@@ -2315,13 +2317,14 @@ int akb_model_autotune(akb_model *m, int repeats) {
 
 int akb_model_set_node_shape(akb_model *m, int node_block, int staged) {
   AKB_TRY(check_model(m, true));
-  if (staged && node_block != 128 && node_block != 256 && node_block != 512)
+  if (staged < 0 || staged > 2) return fail(AKB_EINVAL, "staged must be 0, 1 or 2");
+  if (staged == 1 && node_block != 128 && node_block != 256 && node_block != 512)
     return fail(AKB_EINVAL, "the staged gather runs with 128, 256 or 512 threads");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   AKB_CUDA(cudaStreamSynchronize(m->stream));
   m->node_block = node_block;
-  m->node_staged = staged != 0;
+  m->node_form = staged;
   for (auto &x : m->graphs) cudaGraphExecDestroy(x.exec);
   m->graphs.clear();
   return AKB_OK;
@@ -2413,7 +2416,7 @@ int akb_model_get_dependent_launch(const akb_model *m, int *on) {
 int akb_model_get_node_shape(const akb_model *m, int *node_block, int *staged) {
   if (!m || !node_block || !staged) return fail(AKB_EINVAL, "null argument");
   *node_block = m->node_block;
-  *staged = m->node_staged ? 1 : 0;
+  *staged = m->node_form;
   return AKB_OK;
 }
 

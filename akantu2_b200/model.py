@@ -599,15 +599,17 @@ class SolidMechanicsModel:
                                                               ctypes.byref(w)))
         return bool(w.value)
 
-    def setNodeShape(self, node_block, staged=False):
-        """Threads per block of the node update, and the staged (shared
-        memory) gather; results are unchanged by either."""
+    def setNodeShape(self, node_block, staged=0):
+        """Threads per block of the node update, and its form: 0 the direct
+        gather, 1 (True) the gather staged through shared memory, 2 the direct
+        gather with each node's state read first; results are unchanged by
+        either."""
         _capi.check(_capi.lib().akb_model_set_node_shape(self._h, int(node_block), int(staged)))
 
     def getNodeShape(self):
         b, st = ctypes.c_int(), ctypes.c_int()
         _capi.check(_capi.lib().akb_model_get_node_shape(self._h, ctypes.byref(b), ctypes.byref(st)))
-        return b.value, bool(st.value)
+        return b.value, st.value
 
     def setDependentLaunch(self, on=True):
         """Step kernels launched with programmatic stream serialization (each

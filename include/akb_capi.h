@@ -405,9 +405,12 @@ int akb_model_get_launch_shape(const akb_model *model, int law, int *element_blo
                                int *points_per_iteration, int *min_blocks, int *node_block);
 int akb_model_set_launch_shape(akb_model *model, int law, int element_block,
                                int points_per_iteration, int min_blocks, int node_block);
-/* node update shape: threads per block, and staged = 1 to stage each block's
- * slot range through shared memory (coalesced loads; 128, 256 or 512
- * threads).  Both forms sum every node's slots in the same order. */
+/* node update shape: threads per block, and its form: staged = 1 stages
+ * each block's slot range through shared memory (coalesced loads; 128, 256
+ * or 512 threads); staged = 2 keeps the direct gather but reads each node's
+ * slot range, mass and blocked flags before the wait on the preceding kernel
+ * and its state (a, v, u, f_ext) before the gather; 0 the direct gather.
+ * Every form sums every node's slots in the same order. */
 int akb_model_set_node_shape(akb_model *model, int node_block, int staged);
 int akb_model_get_node_shape(const akb_model *model, int *node_block, int *staged);
 /* TimeStepSolverDefault::predictor / corrector bookkeeping

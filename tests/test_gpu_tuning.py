@@ -206,9 +206,10 @@ def test_persistent_batch_with_instance_time_steps():
     ("_hexahedron_8", "mixed", UNIT_NEOHOOKEAN), ("_hexahedron_8", "fp64", UNIT_ELASTIC),
     ("_triangle_6", "mixed", UNIT_PLASTIC), ("_triangle_6", "fp64", UNIT_PLASTIC)])
 def test_staged_node_gather_is_bit_identical(etype, precision, mat):
-    """the shared-memory staged gather sums every node's slots in the order of
-    the direct gather: identical states, for every block size (small chunks
-    are exercised by the 512-thread blocks of tetrahedra, 24 slots a node)"""
+    """the shared-memory staged gather, and the direct gather with the node's
+    state read first (form 2), sum every node's slots in the order of the
+    direct gather: identical states, for every block size (small chunks are
+    exercised by the 512-thread blocks of tetrahedra, 24 slots a node)"""
     mesh = {"_hexahedron_8": lambda: akb.box_hex8(6), "_triangle_6": lambda: akb.square_tri6(8),
             "_tetrahedron_4": lambda: akb.box_tet4(8)}[etype]()
     d = mesh.spatial_dimension
@@ -216,7 +217,7 @@ def test_staged_node_gather_is_bit_identical(etype, precision, mat):
         np.stack([0.02 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
     bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
     runs = []
-    for shape in [(128, False), (128, True), (256, True), (512, True)]:
+    for shape in [(128, 0), (128, 1), (256, 1), (512, 1), (128, 2), (512, 2)]:
         m = gpu_model(mesh, [mat], precision=precision)
         m.setNodeShape(*shape)
         assert m.getNodeShape() == shape
@@ -248,7 +249,7 @@ def test_dependent_launch_is_bit_identical(etype, precision, mat):
     bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
     top = np.flatnonzero(np.isclose(mesh.nodes[:, d - 1], mesh.nodes[:, d - 1].max()))
     runs = []
-    for pdl, staged in [(False, False), (True, False), (True, True)]:
+    for pdl, staged in [(False, 0), (True, 0), (True, 1), (True, 2), (False, 2)]:
         m = gpu_model(mesh, [mat], precision=precision)
         m.setDependentLaunch(pdl)
         assert m.getDependentLaunch() == pdl
