@@ -166,15 +166,19 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
                     : law == LAW_NEOHOOKEAN ? k_element_forces_pqs<D, NN, NQ, LAW_NEOHOOKEAN>
                                             : k_element_forces_pqs<D, NN, NQ, LAW_PLASTIC>;
         constexpr size_t smem = sizeof(double) * 32 * (NN * D) * (1 + NQ);
-        // above the 48 KB default: allowed once per kernel (a host-side
-        // attribute, no stream work)
-        static std::atomic<int> opted[3] = {0, 0, 0};
+        // above the 48 KB default: allowed once per kernel and device (a
+        // host-side attribute of the current device, no stream work)
+        static std::atomic<unsigned long long> opted[3] = {0ull, 0ull, 0ull};
         const int li = law == LAW_ELASTIC ? 0 : law == LAW_NEOHOOKEAN ? 1 : 2;
-        if (!opted[li].load(std::memory_order_relaxed)) {
+        int dev = 0;
+        const cudaError_t ed = cudaGetDevice(&dev);
+        if (ed != cudaSuccess) return ed;
+        const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+        if (!(opted[li].load(std::memory_order_relaxed) & bit)) {
           const cudaError_t ea =
               cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
           if (ea != cudaSuccess) return ea;
-          opted[li].store(1, std::memory_order_relaxed);
+          opted[li].fetch_or(bit, std::memory_order_relaxed);
         }
         return launch_step_smem(g.pdl, kern, grid, 32 * NQ, smem, s, e0, ne, g.E, g.conn, g.pos,
                                 B, wJ, u, mp, ps, re);

@@ -2253,21 +2253,21 @@ int akb_model_autotune(akb_model *m, int repeats) {
     float best = 0.f;
     for (int k = 0; k < 10 && rc == AKB_OK; ++k) {
       float ms = 0.f;
-      const int staged = forms[k];
+      const int form = forms[k];
       auto launch = [&]() {
         if (m->precision == AKB_PRECISION_MIXED)
           return launch_node_update_mixed(g, (const float *)m->dre, m->dfext, m->dmass,
                                           m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
-                                          flags, t_status, blocks[k], staged, s);
+                                          flags, t_status, blocks[k], form, s);
         return launch_node_update_fp64(g, (const double *)m->dre, m->dfext, m->dmass,
                                        m->dblocked, m->dfint, t_a, t_v, m->u(), t_u, m->dt,
-                                       flags, t_status, blocks[k], staged, s);
+                                       flags, t_status, blocks[k], form, s);
       };
       if (!time_it(launch, &ms)) break;
       if (k == 0 || ms < best) {
         best = ms;
         m->node_block = blocks[k];
-        m->node_form = staged;
+        m->node_form = form;
       }
     }
   }
