@@ -191,6 +191,19 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
     } else {
       AKB_DISPATCH_BLOCK(tn.block, {
         const unsigned grid = (unsigned)((ne + BLOCK - 1) / BLOCK);
+        if constexpr (ET == ET_TRI6 && BLOCK == 128) {
+          // plastic triangles, streamed law: 128 threads, registers capped
+          // for 1 (none), 5, 6, 7 or 8 resident blocks; tables streamed
+          if (law == LAW_PLASTIC && tn.pqs && !tn.rec) {
+            auto kern = tn.minb >= 8   ? k_element_forces_pe_streamed<D, NN, NQ, T, RT, 128, 8>
+                        : tn.minb == 7 ? k_element_forces_pe_streamed<D, NN, NQ, T, RT, 128, 7>
+                        : tn.minb == 6 ? k_element_forces_pe_streamed<D, NN, NQ, T, RT, 128, 6>
+                        : tn.minb == 5 ? k_element_forces_pe_streamed<D, NN, NQ, T, RT, 128, 5>
+                                       : k_element_forces_pe_streamed<D, NN, NQ, T, RT, 128, 1>;
+            return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, B, wJ, u,
+                               mp, ps, re, (int64_t)0);
+          }
+        }
         if constexpr (ET != ET_HEX8) {
           if (tn.rec && tab) {
             if constexpr (BLOCK == 128) {

@@ -733,6 +733,139 @@ __device__ __forceinline__ void element_pe(int64_t le, int64_t e_begin, int64_t 
   for (int a = 0; a < NN; ++a) store_slot<D>(re, pos[(int64_t)a * E + e], &r[a * D]);
 }
 
+// one value of a dN/dx table, loaded where it is used: the asm keeps the
+// compiler from holding a point's whole row in registers between the
+// gradient and the force, which read it at two places
+__device__ __forceinline__ float ld_table(const float *p) {
+  float v;
+  asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_table(const double *p) {
+  double v;
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+// element_pe for the plastic law, streamed: the same operations in the same
+// order, with less held in registers across the radial return (its FP64
+// state is the register peak of the kernel): each point gathers the nodal
+// displacements again (the same values: u does not change within the step),
+// loads its dN/dx row node by node where the gradient and the force use it,
+// and the element's force sum over the points lives in shared memory
+// rs[c sst] instead of registers
+template <int D, int NN, int NQ, class T, class RT>
+__device__ __forceinline__ void element_pe_plastic_streamed(int64_t le, int64_t e_begin,
+                                                            int64_t e_count, int64_t E,
+                                                            const int32_t *conn,
+                                                            const int32_t *pos, const T *B,
+                                                            const T *wJ, const double *u,
+                                                            const MatParams &mp,
+                                                            const GroupArgs &ps, RT *re, T *rs,
+                                                            int sst) {
+  constexpr int ND = NN * D;
+  constexpr bool REL = !std::is_same<T, double>::value;
+  const int64_t e = e_begin + le;
+  const MatParams mpe = group_params(mp, ps, le);
+#pragma unroll 1
+  for (int q = 0; q < NQ; ++q) {
+    T ue[ND];
+    double u0[D];
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      const int64_t node = conn[(int64_t)a * E + e];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const double x = u[node * D + i];
+        if constexpr (REL) {
+          if (a == 0) u0[i] = x;
+          ue[a * D + i] = (T)(x - u0[i]);
+        } else {
+          ue[a * D + i] = x;
+        }
+      }
+    }
+    const T *Bq = B + (int64_t)q * ND * E + e;
+    // grad u = u B^T, s = u_0 b_0 then s + u_a b_a (the expression of element_law)
+    T g[D * D];
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      T ba[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) ba[j] = Bq[(int64_t)(a * D + j) * E];
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+          g[i + D * j] = (a == 0) ? ue[i] * ba[j] : g[i + D * j] + ue[a * D + i] * ba[j];
+    }
+    subtract_eigen<D, T>(ps, e_count, le, q, g);
+    T sig[D * D];
+    {
+      double gd[D * D], sd[D * D];
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) gd[k] = (double)g[k];
+      plastic_point<D, T>(mpe, ps, e_count, le, q, gd, sd);
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) sig[k] = (T)sd[k];
+    }
+    const T w = wJ[(int64_t)q * E + e];
+    if constexpr (REL) {
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) sig[k] *= w;
+    }
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      T ba[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) ba[j] = ld_table(Bq + (int64_t)(a * D + j) * E);
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        T t;
+        if constexpr (REL) {
+          T s = sig[i] * ba[0];
+#pragma unroll
+          for (int j = 1; j < D; ++j) s += sig[i + D * j] * ba[j];
+          t = s;
+        } else {
+          T s = sig[i] * ba[0];
+#pragma unroll
+          for (int j = 1; j < D; ++j) s = s + sig[i + D * j] * ba[j];
+          t = s * w;
+        }
+        // integrate: sum over q in increasing order
+        T &r = rs[(a * D + i) * sst];
+        r = (q == 0) ? t : r + t;
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NN; ++a) {
+    T ra[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) ra[i] = rs[(a * D + i) * sst];
+    store_slot<D>(re, pos[(int64_t)a * E + e], ra);
+  }
+}
+
+// k_element_forces_pe with the streamed plastic law (the same numbers)
+template <int D, int NN, int NQ, class T, class RT, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_element_forces_pe_streamed(int64_t e_begin, int64_t e_count, int64_t E,
+                                 const int32_t *__restrict__ conn,
+                                 const int32_t *__restrict__ pos, const T *__restrict__ B,
+                                 const T *__restrict__ wJ, const double *__restrict__ u,
+                                 MatParams mp, GroupArgs ps, RT *__restrict__ re, int64_t pf) {
+  (void)pf;
+  __shared__ T s_r[NN * D * BLOCK];
+  pdl_begin();
+  const int64_t le = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+  if (le >= e_count || !element_active(ps, le)) return;
+  if (!element_indices_ok<NN>(ps, conn, pos, E, e_begin + le)) return;
+  element_pe_plastic_streamed<D, NN, NQ, T, RT>(le, e_begin, e_count, E, conn, pos, B, wJ, u, mp,
+                                                ps, re, s_r + threadIdx.x, BLOCK);
+}
+
 // The element-indexed rows the warp pf elements further on reads, prefetched
 // into L2 (one row segment of 32 elements per lane and pass): connectivity,
 // slot positions, dN/dx and det J w, the material slot, and the previous
@@ -1556,15 +1689,6 @@ __global__ void __launch_bounds__(32 * NQ)
     }
     __syncthreads();
   }
-}
-
-// one FP64 value of a dN/dx table, loaded where it is used: the asm keeps
-// the compiler from holding a point's whole row in registers between the
-// gradient and the force, which read it at two places
-__device__ __forceinline__ double ld_table(const double *p) {
-  double v;
-  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
-  return v;
 }
 
 // The FP64 law of one (element, point), the operations of

@@ -33,9 +33,12 @@ struct ElemTuning {
   // det J w from the coordinates by the precomputation's arithmetic instead
   // of streaming the tables (the same numbers)
   int rec = 0;
-  // plain FP64 hexahedra (one thread per point): 1 runs the streamed law
-  // (k_element_forces_pqs: dN/dx rows loaded node by node where used, force
-  // components sent to shared memory as formed); the same numbers
+  // the streamed law (the same numbers): plain FP64 hexahedra, one thread
+  // per point (k_element_forces_pqs: dN/dx rows loaded node by node where
+  // used, force components sent to shared memory as formed); plastic
+  // triangles, one thread per element (k_element_forces_pe_streamed: the
+  // displacements gathered per point, dN/dx loaded where used, the force sum
+  // in shared memory), with the streamed tables (rec 0, no prefetch)
   int pqs = 0;
 };
 // points_per_iteration flag of the mixed hexahedron kernel: the points are

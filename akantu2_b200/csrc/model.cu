@@ -1214,6 +1214,13 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
       // the 512^2 square than uncapped
       if (m->et == AKB_TRIANGLE_6 && gr.law == LAW_PLASTIC)
         gr.tune = ElemTuning{128, 8, precision == AKB_PRECISION_MIXED ? 6 : 5};
+      // mixed plastic triangles: the streamed law with 7 blocks, measured on
+      // the 512^2 square: 0.0845 against 0.0875 ms (3 points), 0.1434 against
+      // 0.1481 ms (6 points); FP64 keeps the held form (0.1246 ms, 5 blocks)
+      if (m->et == AKB_TRIANGLE_6 && gr.law == LAW_PLASTIC && precision == AKB_PRECISION_MIXED) {
+        gr.tune.minb = 7;
+        gr.tune.pqs = 1;
+      }
       // FP64 elastic and neohookean tetrahedra: the geometry recomputed from
       // the coordinates instead of streaming 104 bytes of dN/dx and det J w
       // per element, and the next wave's table rows prefetched into L2
@@ -2212,6 +2219,13 @@ int akb_model_autotune(akb_model *m, int repeats) {
       cand = {{64, q, 1}, {128, q, 1}, {256, q, 1}};
       if (gr.law == LAW_PLASTIC && m->et != AKB_HEXAHEDRON_8)
         cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}, {128, q, 7}, {128, q, 8}});
+      // plastic triangles: the streamed law with each register cap
+      std::vector<ElemTuning> streamed;
+      if (gr.law == LAW_PLASTIC && m->et == AKB_TRIANGLE_6)
+        for (int mb : {1, 5, 6, 7, 8}) {
+          streamed.push_back({128, q, mb});
+          streamed.back().pqs = 1;
+        }
       // each with and without the L2 prefetch of the next wave's rows, and
       // (tetrahedra and triangles) with the geometry streamed or recomputed
       Group probe = gr;
@@ -2229,6 +2243,7 @@ int akb_model_autotune(akb_model *m, int repeats) {
           }
         }
       }
+      cand.insert(cand.end(), streamed.begin(), streamed.end());
       // the shape in use first (kept on ties)
       cand.insert(cand.begin(), gr.tune);
     }
@@ -2501,6 +2516,8 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
       // shape's kernel has them
       const ElemTuning old = gr.tune;
       gr.tune = ElemTuning{element_block, q, min_blocks, old.pf, old.rec, old.pqs};
+      // the streamed law of plastic triangles runs with 128 threads
+      if (m->et == AKB_TRIANGLE_6 && element_block != 128) gr.tune.pqs = 0;
       if (!prefetching_kernel(m, gr)) gr.tune.pf = 0;
       if (!prefetching_kernel(m, gr) || m->et == AKB_HEXAHEDRON_8) gr.tune.rec = 0;
       found = true;
@@ -2524,6 +2541,8 @@ int akb_model_set_prefetch(akb_model *m, int law, int waves) {
                                 "(points_per_iteration with AKB_POINTS_PACKED) and of the "
                                 "tetrahedron and triangle kernels");
       gr.tune.pf = waves;
+      // a prefetching kernel replaces the streamed law of plastic triangles
+      if (waves > 0 && m->et == AKB_TRIANGLE_6) gr.tune.pqs = 0;
       found = true;
     }
   if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
@@ -2543,6 +2562,8 @@ int akb_model_set_recompute_geometry(akb_model *m, int law, int on) {
         return fail(AKB_EINVAL, "the recomputed geometry is a setting of the tetrahedron and "
                                 "triangle kernels that stream dN/dx");
       gr.tune.rec = on;
+      // so does the recomputed geometry
+      if (on && m->et == AKB_TRIANGLE_6) gr.tune.pqs = 0;
       found = true;
     }
   if (!found) return fail(AKB_EINVAL, "no material of this law in the model");
@@ -2555,12 +2576,19 @@ int akb_model_set_recompute_geometry(akb_model *m, int law, int on) {
 int akb_model_set_streamed_points(akb_model *m, int law, int on) {
   AKB_TRY(check_model(m, true));
   if (on != 0 && on != 1) return fail(AKB_EINVAL, "on must be 0 or 1");
-  if (on && !(m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64 && !m->fast64))
-    return fail(AKB_EINVAL, "the streamed per-point law is a setting of plain FP64 hexahedra");
+  const bool hex64 = m->et == AKB_HEXAHEDRON_8 && m->precision == AKB_PRECISION_FP64 && !m->fast64;
+  const bool tri_plastic = m->et == AKB_TRIANGLE_6 && law == LAW_PLASTIC;
+  if (on && !hex64 && !tri_plastic)
+    return fail(AKB_EINVAL, "the streamed law is a setting of plain FP64 hexahedra and of plastic "
+                            "triangles");
   bool found = false;
   for (auto &gr : m->groups)
     if (gr.law == law) {
+      if (on && tri_plastic && (gr.tune.block != 128 || gr.tune.rec))
+        return fail(AKB_EINVAL, "the streamed law of plastic triangles runs with 128 threads and "
+                                "the streamed dN/dx tables (recompute_geometry 0)");
       gr.tune.pqs = on;
+      if (on && tri_plastic) gr.tune.pf = 0;
       found = true;
     }
   if (!found) return fail(AKB_EINVAL, "no material of this law in the model");

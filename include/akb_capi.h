@@ -390,15 +390,20 @@ int akb_model_get_prefetch(const akb_model *model, int law, int *waves);
  * this library; the reference precomputes, fe_engine_template_tmpl.hh). */
 int akb_model_set_recompute_geometry(akb_model *model, int law, int on);
 int akb_model_get_recompute_geometry(const akb_model *model, int law, int *on);
-/* form of the plain FP64 hexahedron kernel (one thread per Gauss point):
- * 1 (the default of the neohookean and plastic laws; elastic 0) evaluates
- * the law streamed, each point's dN/dx row loaded node by node where the
+/* streamed form of an element kernel, for plain FP64 hexahedra and for
+ * plastic triangles.  Plain FP64 hexahedra (one thread per Gauss point): 1
+ * (the default of the neohookean and plastic laws; elastic 0) evaluates the
+ * law streamed, each point's dN/dx row loaded node by node where the
  * gradient and the force read it and every force component written to
  * shared memory as soon as it is formed, which needs about half the
- * registers; 0 holds the point's row and forces in registers.  The same
- * operations in the same order either way (bit-identical); the autotuner
- * tries both.  Only plain FP64 hexahedra.  No reference counterpart (a
- * launch setting of this library). */
+ * registers; 0 holds the point's row and forces in registers.  Plastic
+ * triangles (one thread per element, 128 threads, the streamed dN/dx
+ * tables): 1 gathers the displacements again for each point, loads dN/dx
+ * where used and keeps the element's force sum in shared memory, so that
+ * less stays in registers across the FP64 radial return; setting the L2
+ * prefetch or the recomputed geometry turns it off.  The same operations in
+ * the same order either way (bit-identical); the autotuner tries both.  No
+ * reference counterpart (a launch setting of this library). */
 int akb_model_set_streamed_points(akb_model *model, int law, int on);
 int akb_model_get_streamed_points(const akb_model *model, int law, int *on);
 int akb_model_get_launch_shape(const akb_model *model, int law, int *element_block,

@@ -117,7 +117,7 @@ def test_autotune_leaves_the_state_alone(etype, precision, mat):
             assert np.array_equal(plain.getMaterial(0).getInternal(f)(),
                                   tuned.getMaterial(0).getInternal(f)()), f
     b, q, mb, n = tuned.getLaunchShape(mat["type"])
-    assert b in (64, 128, 256) and mb in (1, 4, 5, 6) and n in (128, 256, 512, 1024)
+    assert b in (64, 128, 256) and mb in (1, 4, 5, 6, 7, 8) and n in (128, 256, 512, 1024)
 
 
 @pytest.mark.parametrize("mat", [UNIT_ELASTIC, UNIT_NEOHOOKEAN])
@@ -292,7 +292,8 @@ def test_dependent_launch_batch_is_bit_identical():
     ("_triangle_6", "mixed")])
 def test_plastic_register_caps_are_bit_identical(etype, precision):
     """128-thread plastic kernels with registers capped for 5 to 8 resident
-    blocks per SM compute the same numbers"""
+    blocks per SM compute the same numbers, and so does the streamed law of
+    plastic triangles with each cap"""
     mesh = {"_triangle_6": lambda: akb.square_tri6(8), "_tetrahedron_4": lambda: akb.box_tet4(6)}[etype]()
     d = mesh.spatial_dimension
     mat = dict(UNIT_PLASTIC, sigma_y=2e-3)
@@ -300,12 +301,17 @@ def test_plastic_register_caps_are_bit_identical(etype, precision):
         np.stack([0.05 * mesh.nodes[:, 0], np.zeros(mesh.getNbNodes())], axis=1)
     bl = blocked_face(mesh.nodes, axis=2 if d == 3 else 0)
     runs = []
-    for mb in (1, 5, 6, 7, 8):
+    shapes = [(mb, False) for mb in (1, 5, 6, 7, 8)]
+    if etype == "_triangle_6":
+        shapes += [(mb, True) for mb in (1, 5, 6, 7, 8)]
+    for mb, streamed in shapes:
         m = gpu_model(mesh, [mat], precision=precision)
         m.setLaunchShape(mat["type"], 128, 8, 128, mb)
         m.setPrefetch(mat["type"], 0)
         m.setRecomputeGeometry(mat["type"], False)
+        m.setStreamedPoints(mat["type"], streamed)
         assert m.getLaunchShape(mat["type"])[2] == mb
+        assert m.getStreamedPoints(mat["type"]) == streamed
         m.setNodal("velocity", v0)
         m.setNodal("blocked_dofs", bl)
         m.setTimeStep(0.8 * m.getStableTimeStep())
@@ -664,13 +670,25 @@ def test_hex8_fp64_streamed_points_are_bit_identical(mat, eigen):
 def test_hex8_fp64_streamed_points_setting_rules():
     """the streamed law is a setting of plain FP64 hexahedra only; the
     autotuner keeps the state and picks one of the two forms"""
-    for etype, precision in (("hex8", "mixed"), ("hex8", "fp64_fast"), ("tet4", "fp64")):
-        mesh = akb.box_hex8(3) if etype == "hex8" else akb.box_tet4(3)
+    for etype, precision in (("hex8", "mixed"), ("hex8", "fp64_fast"), ("tet4", "fp64"),
+                             ("tri6", "mixed")):
+        mesh = {"hex8": akb.box_hex8, "tet4": akb.box_tet4, "tri6": akb.square_tri6}[etype](3)
         m = gpu_model(mesh, [UNIT_ELASTIC], precision=precision)
         assert not m.getStreamedPoints("elastic")
         with pytest.raises(akb.AkbError):
             m.setStreamedPoints("elastic", True)
         m.setStreamedPoints("elastic", False)
+    # plastic triangles: 128 threads and the streamed tables; a prefetch turns it off
+    p = gpu_model(akb.square_tri6(3), [UNIT_PLASTIC], precision="mixed")
+    law = UNIT_PLASTIC["type"]
+    p.setStreamedPoints(law, True)
+    assert p.getStreamedPoints(law)
+    p.setPrefetch(law, 1)
+    assert not p.getStreamedPoints(law)
+    p.setPrefetch(law, 0)
+    p.setLaunchShape(law, 64, 8, 128, 1)
+    with pytest.raises(akb.AkbError):
+        p.setStreamedPoints(law, True)
     mesh = akb.box_hex8(6)
     v0, bl = sinusoidal_velocity(mesh.nodes, 0.03), blocked_face(mesh.nodes)
     ref = _run(mesh, UNIT_NEOHOOKEAN, "fp64", v0, bl, 60)
