@@ -221,6 +221,33 @@ inline cudaError_t element_forces_impl(const DevGeom &g, int law, int64_t e0, in
                                    *tab, u, mp, ps, re, pf);
               }
             }
+            if constexpr (ET == ET_TET4 && BLOCK == 128 && std::is_same<T, double>::value) {
+              // FP64 elastic and neohookean tetrahedra: registers capped for 6
+              // or 7 resident blocks (80 / 72 instead of 90 registers)
+              if (law != LAW_PLASTIC && (tn.minb == 6 || tn.minb == 7)) {
+                const bool el = law == LAW_ELASTIC, m7 = tn.minb == 7;
+                constexpr auto e6 = k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, 128, 6>;
+                constexpr auto e7 = k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, 128, 7>;
+                constexpr auto n6 = k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, 128, 6>;
+                constexpr auto n7 = k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, 128, 7>;
+                constexpr auto e6p =
+                    k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, 128, 6, true>;
+                constexpr auto e7p =
+                    k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, 128, 7, true>;
+                constexpr auto n6p =
+                    k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, 128, 6, true>;
+                constexpr auto n7p =
+                    k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, 128, 7, true>;
+                const int64_t pf = el ? (m7 ? prefetch_distance<e7p>(tn.pf, 128)
+                                            : prefetch_distance<e6p>(tn.pf, 128))
+                                      : (m7 ? prefetch_distance<n7p>(tn.pf, 128)
+                                            : prefetch_distance<n6p>(tn.pf, 128));
+                auto kern = el ? (m7 ? (pf > 0 ? e7p : e7) : (pf > 0 ? e6p : e6))
+                               : (m7 ? (pf > 0 ? n7p : n7) : (pf > 0 ? n6p : n6));
+                return launch_step(g.pdl, kern, grid, 128, s, e0, ne, g.E, g.conn, g.pos, g.X,
+                                   *tab, u, mp, ps, re, pf);
+              }
+            }
             constexpr auto ke = k_element_forces_pr<D, NN, NQ, LAW_ELASTIC, T, RT, BLOCK>;
             constexpr auto kn = k_element_forces_pr<D, NN, NQ, LAW_NEOHOOKEAN, T, RT, BLOCK>;
             constexpr auto kp = k_element_forces_pr<D, NN, NQ, LAW_PLASTIC, T, RT, BLOCK>;

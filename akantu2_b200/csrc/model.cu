@@ -1233,6 +1233,10 @@ int akb_model_init_full(akb_model *m, int method, int precision) {
           precision == AKB_PRECISION_FP64) {
         gr.tune.pf = 1;
         gr.tune.rec = 1;
+        // registers capped for 6 resident blocks (80 instead of 90, no
+        // spill): 256-cube batch element launch 0.781-0.802 against
+        // 0.836-0.865 ms
+        gr.tune.minb = 6;
       }
       // plain FP64 hexahedra, neohookean and plastic: the streamed per-point
       // law (64 instead of 126 and 128 instead of 168 registers), measured on
@@ -2219,6 +2223,11 @@ int akb_model_autotune(akb_model *m, int repeats) {
       cand = {{64, q, 1}, {128, q, 1}, {256, q, 1}};
       if (gr.law == LAW_PLASTIC && m->et != AKB_HEXAHEDRON_8)
         cand.insert(cand.end(), {{128, q, 5}, {128, q, 6}, {128, q, 7}, {128, q, 8}});
+      // FP64 elastic and neohookean tetrahedra: register caps of the kernel
+      // with the recomputed geometry (the streamed form ignores them)
+      if (gr.law != LAW_PLASTIC && m->et == AKB_TETRAHEDRON_4 &&
+          m->precision == AKB_PRECISION_FP64)
+        cand.insert(cand.end(), {{128, q, 6}, {128, q, 7}});
       // plastic triangles: the streamed law with each register cap
       std::vector<ElemTuning> streamed;
       if (gr.law == LAW_PLASTIC && m->et == AKB_TRIANGLE_6)
@@ -2235,7 +2244,8 @@ int akb_model_autotune(akb_model *m, int repeats) {
         for (size_t k = 0; k < n; ++k) {
           cand[k].pf = 0;
           cand[k].rec = 0;
-          if (cand[k].minb >= 7) continue;  // the 7- and 8-block caps: streamed, no prefetch
+          // the 7- and 8-block caps of plastic groups: streamed tables, no prefetch
+          if (cand[k].minb >= 7 && gr.law == LAW_PLASTIC) continue;
           for (int v = 1; v < 4; ++v) {
             cand.push_back(cand[k]);
             cand.back().pf = v & 1;
@@ -2503,10 +2513,16 @@ int akb_model_set_launch_shape(akb_model *m, int law, int element_block,
                           (min_blocks == 6 && (q == 1 || q == 2)));
   const bool capped_plastic = m->et != AKB_HEXAHEDRON_8 && law == LAW_PLASTIC &&
                               min_blocks >= 5 && min_blocks <= 8 && element_block == 128;
-  if (min_blocks != 1 && !capped_sf && !capped_plastic && !(q & AKB_POINTS_PACKED))
+  // FP64 elastic and neohookean tetrahedra with the recomputed geometry
+  const bool capped_tet64 = m->et == AKB_TETRAHEDRON_4 && m->precision == AKB_PRECISION_FP64 &&
+                            law != LAW_PLASTIC && (min_blocks == 6 || min_blocks == 7) &&
+                            element_block == 128;
+  if (min_blocks != 1 && !capped_sf && !capped_plastic && !capped_tet64 &&
+      !(q & AKB_POINTS_PACKED))
     return fail(AKB_EINVAL, "min_blocks is 1; 5 (or 4 with 2 points per iteration, 6 with 1 or "
                             "2) for the 128-thread mixed hexahedron kernel; 5 to 8 for "
-                            "128-thread plastic tetrahedra and triangles");
+                            "128-thread plastic tetrahedra and triangles; 6 or 7 for 128-thread "
+                            "FP64 elastic and neohookean tetrahedra");
   if (node_block < 32 || node_block > 1024 || node_block % 32)
     return fail(AKB_EINVAL, "node_block must be a multiple of 32 in [32, 1024]");
   bool found = false;

@@ -476,6 +476,10 @@ def test_recomputed_geometry_and_prefetch_are_bit_identical(case, precision):
               (64, 8, 1, 1, 1), (256, 8, 1, 1, 1)]
     if law == "plastic":
         shapes += [(128, 8, 5, 1, 1), (128, 8, 6, 1, 1), (128, 8, 6, 0, 1)]
+    if etype == "tet4" and precision == "fp64":
+        # FP64 elastic and neohookean tetrahedra: the recomputed-geometry kernel
+        # with registers capped for 6 and 7 blocks, with and without prefetch
+        shapes += [(128, 8, 6, 1, 1), (128, 8, 6, 1, 0), (128, 8, 7, 1, 1), (128, 8, 7, 1, 0)]
     runs = []
     for block, q, minb, rec, pf in shapes:
         m = gpu_model(mesh, [mat], precision=precision, qp_rule=qp_rule)
