@@ -95,7 +95,11 @@ def parse():
                    help="tri6: quadrature rule (0: the reference's default, 3 points; 1: 6 points)")
     p.add_argument("--parts", type=int, default=0,
                    help="partitioned, one process: subdomains advanced on the one GPU")
-    return p.parse_args()
+    args = p.parse_args()
+    # the library keeps AKB_ASYNC_READS_IN_FLIGHT reads waitable one by one
+    if not 1 <= args.e2e_lag <= 3:
+        p.error("--e2e-lag must be in 1 .. 3 (AKB_ASYNC_READS_IN_FLIGHT - 1)")
+    return args
 
 
 # ---- workloads ---------------------------------------------------------------------
